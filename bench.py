@@ -1,0 +1,316 @@
+"""Benchmark of the particle-mesh step on B200: prints ONE JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+A step is one leapfrog step of QUANTIZER's main loop (main.c:375-481 with a
+fixed dt): kick-drift, reset, CIC deposit, head Poisson solve to the
+reference's thresholds, gradient, CIC gather, kick.  Metric: particle-steps/s.
+
+* value  -- whole-job throughput with the state resident in HBM; the device
+  time of exactly K steps (CUDA events on the library stream), L2 flushed
+  between steps by writing a 256 MiB buffer (outside the timed events).
+* e2e    -- the same metric through the C ABI with HOST buffers: every step
+  copies the particle state (x, v, a, m) from pinned host memory to the device
+  and reads the advanced state (x, v, a) back, as the drop-in does for the
+  reference's main loop.
+* roofline -- the dominant kernel category from a profiled pass of the same
+  workload (per-launch CUDA events), algorithmic bytes / device time against
+  the measured HBM copy bandwidth of MEASURED_PEAKS.json.
+* cpu_baseline -- the reference's own FP64 code (compiled unmodified,
+  oracle/_ref/qz_ref_driver) on the box's host, 1 thread (its default).
+
+--impl reference times the reference's CPU implementation of the same workload
+with all host threads (OpenMP), on rank 0 only.
+
+Multi-GPU (torchrun): the head-only path has no exchange step, so each rank
+runs an independent replica (different seed); value = all ranks' particle
+steps / max-over-ranks device time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # Plummer N=10,000, a=0.05, head 32^3, FP64, dt = 1e-3 t_cr, 100 steps
+    "plummer10k_head32": dict(n=10000, a=0.05, lmin=5, steps=100, precision=0),
+}
+DEFAULT_WORKLOAD = "plummer10k_head32"
+METRIC = "particle-steps/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference_cpu(wl: dict, steps: int, threads: int, seed: int) -> dict:
+    """The reference's FP64 path (oracle/_ref/qz_ref_driver) on this host."""
+    from oracle import oracle as O
+    from quantizer_b200 import ics
+    if not os.path.exists(O.REF_DRIVER):
+        return {"kind": "port"} | run_port_cpu(wl, steps, seed)
+    ic = ics.plummer(wl["n"], a=wl["a"], seed=seed)
+    dt = 1e-3 * ics.crossing_time(wl["a"])
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ic.bin")
+        ics.write_ic(p, ic)
+        r = O.run_reference(p, td, lmin=wl["lmin"], steps=steps, dt=dt, threads=threads)
+    return {"kind": "reference", "value": wl["n"] * steps / r["loop_s"], "seconds": r["loop_s"],
+            "steps": steps}
+
+
+def run_port_cpu(wl: dict, steps: int, seed: int) -> dict:
+    import numpy as np
+    from oracle import oracle as O
+    from quantizer_b200 import ics
+    ic = ics.plummer(wl["n"], a=wl["a"], seed=seed)
+    dt = 1e-3 * ics.crossing_time(wl["a"])
+    s = O.OracleSim(ic, O.params(wl["lmin"], total_mass=float(np.cumsum(ic["m"])[-1])))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step(dt)
+    t = time.perf_counter() - t0
+    return {"value": wl["n"] * steps / t, "seconds": t, "steps": steps}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    K = args.steps if args.steps is not None else wl["steps"]
+    W = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": args.workload, "particles": wl["n"], "head_grid": 2 ** wl["lmin"],
+              "lmax_minus_lmin": 0, "dt": "1e-3 crossing time", "precision":
+              "fp64" if wl["precision"] == 0 else "fp32-in-fp64", "residual_tol": 1e-10,
+              "l2": "flushed between timed steps (256 MiB write)", "replicas": world}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        r = run_reference_cpu(wl, K, threads, seed=1)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+                "n_gpus": args.gpus, "steps": K, "warmup": 0,
+                "ms_per_step": 1e3 * r["seconds"] / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": threads,
+                                 "kind": r.get("kind", "reference"),
+                                 "sample": f"{K} steps of the workload (whole step loop)"},
+                "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from quantizer_b200 import core, ics
+
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ic = ics.plummer(wl["n"], a=wl["a"], seed=1 + rank)
+    dt = 1e-3 * ics.crossing_time(wl["a"])
+    sim = core.Simulation(ic, wl["lmin"], precision=wl["precision"])
+    ext = torch.cuda.ExternalStream(sim.stream, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    sim.init_forces()
+    for _ in range(W):
+        sim.step(dt, 1)
+
+    def timed_steps(fn, k):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(k)]
+        for i in range(k):
+            with torch.cuda.stream(ext):
+                flush.add_(1.0)
+                evs[i][0].record(ext)
+            fn()
+            evs[i][1].record(ext)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs)
+
+    # ---- device-resident timed region -------------------------------------------------
+    st0 = sim.stats()
+    barrier()
+    with ClockSampler(local) as clk:
+        ms = timed_steps(lambda: sim.step(dt, 1), K)
+    barrier()
+    st1 = sim.stats()
+    launches = int(st1.kernel_launches - st0.kernel_launches)
+    vcycles = int(st1.vcycles_total - st0.vcycles_total)
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * wl["n"] * K / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers --------------------------------
+    p = sim.particles()
+    host = {}
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m"):
+        buf = torch.empty(wl["n"], dtype=torch.float64, pin_memory=True).numpy()
+        buf[:] = p[k] if k != "m" else ic["m"]
+        host[k] = buf
+    Ke = K
+    barrier()
+    ms_e2e = timed_steps(lambda: sim.step_host(host, dt), Ke)
+    barrier()
+    t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * wl["n"] * Ke / (float(t.item()) / 1e3)
+
+    # ---- profiled pass: per-kernel-category device time --------------------------------
+    Kp = min(K, 20)
+    core.profile_reset(sim)
+    core.profile_enable(sim, True)
+    sim.set_particles({**p, "m": ic["m"]})
+    sim.set_accelerations(p["ax"], p["ay"], p["az"])
+    sim.step(dt, Kp)
+    prof = core.profile_read(sim)
+    core.profile_enable(sim, False)
+    dom = max(prof, key=lambda c: prof[c][1])
+    n_l, ms_l, by_l = prof[dom]
+    pk = peaks()
+    achieved = (by_l / (ms_l / 1e3)) / 1e9 if ms_l > 0 else 0.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
+    if os.path.exists(tf):
+        for ln in open(tf):
+            f = ln.split()
+            if len(f) >= 3 and f[0] == args.workload and f[1] == dom:
+                traffic = float(f[2])
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                "peak_source": pk["source"], "launches": n_l,
+                "avg_launch_us": 1e3 * ms_l / max(n_l, 1),
+                "algorithmic_bytes_per_launch": by_l / max(n_l, 1)}
+    kernels = {c: {"launches": v[0], "ms": round(v[1], 4),
+                   "GBps": round((v[2] / (v[1] / 1e3)) / 1e9, 1) if v[1] > 0 else 0.0}
+               for c, v in prof.items() if v[0]}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            r = run_reference_cpu(wl, wl["steps"], 1, seed=1)
+            cpu = {"value": r["value"], "unit": METRIC, "cores": 1, "kind": r.get("kind", "reference"),
+                   "sample": f"{r['steps']} steps of the same workload, reference default 1 thread"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        n = wl["n"]
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 80 * n,
+                        "d2h_bytes_per_step": 72 * n},
+                "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
+                "vcycles_per_step": vcycles / K, "clocks": clk.summary(), "kernels": kernels}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

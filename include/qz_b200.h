@@ -1,0 +1,179 @@
+/*
+ * qz_b200.h -- C ABI of the B200 particle-mesh library (libqzb200.so).
+ *
+ * Plain pointers and sizes only.  All state lives in device memory owned by an
+ * opaque qz_sim; host pointers passed to qz_set_* / qz_get_* are copied
+ * through pinned staging buffers.  Every entry point returns QZ_SUCCESS (0)
+ * or QZ_FAILURE (1), the reference's int convention (headers/common.h:81-82);
+ * qz_last_error() gives the message.  There is no CPU fallback: without a
+ * CUDA device every compute entry point fails.
+ *
+ * The per-stage functions mirror the reference's hot-path entry points one to
+ * one (citations are QUANTIZER file:line of the routine each replaces):
+ *   qz_grid_density          grid_density          source/grid_density.c:269-306
+ *   qz_potential             potential             source/potential.c:29-51
+ *                            potential_head_node   source/potential_head_node.c:99-179
+ *   qz_grid_acceleration     grid_acceleration     source/grid_acceleration.c:694-738
+ *   qz_particle_acceleration particle_acceleration source/particle_acceleration.c:522-573
+ *   qz_particle_updating_A   particle_updating_A   source/particle_updating.c:2584-2675
+ *   qz_particle_updating_B   particle_updating_B   source/particle_updating.c:2787-2837
+ *   qz_reset                 reset                 source/reset.c:29-64
+ * and the array-level kernels mirror the force_methods/ routines:
+ *   qz_gauss_saidel          gauss_saidel          source/force_methods/gauss_saidel.c:29-55
+ *   qz_jacobi                jacobi                source/force_methods/jacobi.c:29-82
+ *   qz_multigrid             multigrid             source/force_methods/multigrid.c:106-229
+ *   qz_ptcl_idx_to_box_idx   ptcl_idx_to_box_idx   source/ptcl_idx_to_box_idx.c:30-139
+ */
+#ifndef QZ_B200_H
+#define QZ_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define QZ_API __attribute__((visibility("default")))
+#else
+#define QZ_API
+#endif
+
+#define QZ_SUCCESS 0
+#define QZ_FAILURE 1
+
+/* Smoother ordering of the Gauss-Seidel sweeps. */
+#define QZ_GS_REDBLACK 0 /* two-colour sweeps: the fast path */
+#define QZ_GS_LEX 1      /* lexicographic order as the reference, by wavefronts */
+
+/* Arithmetic of the head Poisson solve. */
+#define QZ_PREC_FP64 0  /* every stage in FP64 (the plain drop-in) */
+#define QZ_PREC_MIXED 1 /* FP32 V-cycles inside FP64 defect correction */
+
+/* Head grid fields for qz_get_head_field / qz_set_head_field. */
+#define QZ_FIELD_POT 0
+#define QZ_FIELD_POT_OLD 1
+#define QZ_FIELD_DENSITY 2
+#define QZ_FIELD_AX 3
+#define QZ_FIELD_AY 4
+#define QZ_FIELD_AZ 5
+
+typedef struct qz_config {
+    int lmin;           /* head level: 2^lmin cells per side (global_variables.c:252) */
+    int lmax;           /* finest level; lmax == lmin is the head-only path */
+    double G;           /* gravitational constant (_G_) */
+    double total_mass;  /* GL_total_mass_initial: analytic boundary and mean density */
+    int bdry;           /* 0 periodic, 1 reflexive (bdry_cond_type) */
+    int smoother;       /* 0 Gauss-Seidel, 1 Jacobi (solverPreS/PostS/finddphic) */
+    int gs_order;       /* QZ_GS_REDBLACK or QZ_GS_LEX */
+    int cycle;          /* 0 V, 1 F, 2 W (multigrid_cycle) */
+    int n_pre, n_post, n_coarse; /* _NiterPreS_, _NiterPostS_, _Niterfinddphic_ */
+    double w_sor;       /* _w_SOR_HEAD_ */
+    double tol, tol2;   /* residual and ratio thresholds of poisson_error */
+    int check_every;    /* iter_between_check_potential_solution */
+    int max_iter;       /* _MAX_NUMBER_OF_ITERATIONS_IN_POISSON_EQUATION_ */
+    int check_method;   /* check_poisson_error_method 0/1/2 */
+    int precision;      /* QZ_PREC_FP64 or QZ_PREC_MIXED */
+    int inner_cycles;   /* mixed precision: FP32 V-cycles per FP64 correction */
+    int force_stencil;  /* 0 = 3-point (only value supported) */
+} qz_config;
+
+typedef struct qz_stats {
+    long long vcycles_total;   /* V-cycles (FP64 or FP32 inner) since creation */
+    int last_vcycles;          /* V-cycles of the last potential solve */
+    int last_converged;        /* 1 if the last solve met both thresholds */
+    long long kernel_launches; /* kernels this library launched since creation */
+    long long steps;           /* completed qz_step steps */
+    int error_flags;           /* device-side bounds / sanity flags seen (bit set) */
+} qz_stats;
+
+typedef struct qz_sim qz_sim;
+
+/* Kernel categories of the per-launch profiler (qz_profile_*). */
+#define QZ_PROF_SMOOTH 0     /* Gauss-Seidel / Jacobi sweeps */
+#define QZ_PROF_RESTRICT 1   /* residual at injected points -> coarse rhs */
+#define QZ_PROF_PROLONG 2    /* trilinear prolongation + correction */
+#define QZ_PROF_CHECK 3      /* convergence test and pot_old update */
+#define QZ_PROF_DEPOSIT 4    /* cell keys, segments, cell sums, point sums */
+#define QZ_PROF_SORT 5       /* radix sort and scans of the deposit */
+#define QZ_PROF_GRADIENT 6   /* finite-difference grid acceleration */
+#define QZ_PROF_GATHER 7     /* CIC force gather */
+#define QZ_PROF_LEAPFROG 8   /* kick-drift and kick */
+#define QZ_PROF_OTHER 9      /* boundary fill, copies, mixed-precision residual */
+#define QZ_PROF_CATEGORIES 10
+
+/* Configuration with the reference defaults (global_variables.c:300-341). */
+QZ_API int qz_default_config(qz_config *cfg, int lmin);
+
+/* Create a simulation for up to n_capacity particles on the current device. */
+QZ_API int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out);
+QZ_API int qz_destroy(qz_sim *sim);
+
+/* Host <-> device particle state (SoA, float64, length n). */
+QZ_API int qz_set_particles(qz_sim *sim, long n, const double *x, const double *y, const double *z,
+                     const double *vx, const double *vy, const double *vz, const double *m);
+/* Any output pointer may be NULL; ax/ay/az are the particle accelerations. */
+QZ_API int qz_get_particles(qz_sim *sim, double *x, double *y, double *z, double *vx, double *vy,
+                     double *vz, double *ax, double *ay, double *az);
+/* Sets the particle accelerations (the state the next kick starts from);
+ * after it, qz_step does not recompute step-0 forces. */
+QZ_API int qz_set_particle_accel(qz_sim *sim, const double *ax, const double *ay, const double *az);
+QZ_API long qz_num_particles(const qz_sim *sim);
+
+/* Head grid fields: (2^lmin + 3)^3 float64 values, index i + j*D + k*D*D. */
+QZ_API long qz_head_grid_points(const qz_sim *sim);
+QZ_API int qz_get_head_field(qz_sim *sim, int which, double *out);
+QZ_API int qz_set_head_field(qz_sim *sim, int which, const double *in);
+
+/* Per-stage entry points (device-resident state, stream-ordered). */
+QZ_API int qz_initial_potential_head(qz_sim *sim); /* initial_potential_and_acceleration_head.c:30-375 */
+QZ_API int qz_reset(qz_sim *sim);
+QZ_API int qz_grid_density(qz_sim *sim);
+QZ_API int qz_potential(qz_sim *sim);
+QZ_API int qz_grid_acceleration(qz_sim *sim);
+QZ_API int qz_particle_acceleration(qz_sim *sim);
+QZ_API int qz_particle_updating_A(qz_sim *sim, double dt);
+QZ_API int qz_particle_updating_B(qz_sim *sim, double dt);
+
+/* poisson_error.c:290-347 for the head node (type 0): ratio test against
+ * pot_old, then the residual test; pot_old <- pot when not converged.
+ * *converged receives 1 or 0. */
+QZ_API int qz_poisson_error(qz_sim *sim, int *converged);
+
+/* Step 0 force computation (main.c:296-338) and whole leapfrog steps
+ * (main.c:375-481 with a fixed dt). */
+QZ_API int qz_init_forces(qz_sim *sim);
+QZ_API int qz_step(qz_sim *sim, double dt, int nsteps);
+
+/* Synchronise the library stream and report statistics. */
+QZ_API int qz_synchronize(qz_sim *sim);
+QZ_API int qz_get_stats(qz_sim *sim, qz_stats *out);
+/* The cudaStream_t the library launches on (for event timing by callers). */
+QZ_API void *qz_stream(qz_sim *sim);
+QZ_API const char *qz_last_error(void);
+
+/* Per-launch profiler: when enabled, every kernel launch is bracketed by CUDA
+ * events on the library stream and booked to its category with the
+ * algorithmic bytes it must move.  qz_profile_read synchronises and returns
+ * the category's launches, summed device time (ms) and algorithmic bytes. */
+QZ_API int qz_profile_enable(qz_sim *sim, int on);
+QZ_API int qz_profile_reset(qz_sim *sim);
+QZ_API int qz_profile_read(qz_sim *sim, int category, long long *launches, double *total_ms,
+                           double *bytes);
+
+/* Array-level kernels on host arrays of gridsize^3 float64 values (copied to
+ * the device and back), the reference's force_methods signatures plus the
+ * parameters the reference reads from globals. */
+QZ_API int qz_gauss_saidel(double *phi, const double *rho, int gridsize, int iter_max, double w,
+                    int gs_order);
+QZ_API int qz_jacobi(double *phi, const double *rho, int gridsize, int iter_max, double w);
+QZ_API int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, int gridsize,
+                 int type_multigrid);
+
+/* Batched ptcl_idx_to_box_idx for one non-periodic node geometry. */
+QZ_API int qz_ptcl_idx_to_box_idx(int lv, int box_ts_x, int box_ts_y, int box_ts_z,
+                           int box_real_dim_x, int box_real_dim_y, long n, const double *x,
+                           const double *y, const double *z, int *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,308 @@
+"""Python host mirror of the reference's hot-path interface over libqzb200.
+
+``Simulation`` exposes the reference's per-step entry points by their own
+names (grid_density, potential, grid_acceleration, particle_acceleration,
+particle_updating_A/B, reset; main.c:369-481) on device-resident state, and
+``step`` runs whole leapfrog steps.  Module functions mirror the array-level
+force_methods routines (gauss_saidel, jacobi, multigrid) and
+ptcl_idx_to_box_idx.  Every call goes through the C ABI of
+include/qz_b200.h; there is no CPU fallback -- a missing library or a
+machine without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libqzb200.so")
+
+QZ_GS_REDBLACK = 0
+QZ_GS_LEX = 1
+QZ_PREC_FP64 = 0
+QZ_PREC_MIXED = 1
+FIELDS = {"pot": 0, "pot_old": 1, "d": 2, "ax": 3, "ay": 4, "az": 5}
+
+_P = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("lmin", C.c_int), ("lmax", C.c_int), ("G", C.c_double), ("total_mass", C.c_double),
+        ("bdry", C.c_int), ("smoother", C.c_int), ("gs_order", C.c_int), ("cycle", C.c_int),
+        ("n_pre", C.c_int), ("n_post", C.c_int), ("n_coarse", C.c_int), ("w_sor", C.c_double),
+        ("tol", C.c_double), ("tol2", C.c_double), ("check_every", C.c_int),
+        ("max_iter", C.c_int), ("check_method", C.c_int), ("precision", C.c_int),
+        ("inner_cycles", C.c_int), ("force_stencil", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("vcycles_total", C.c_longlong), ("last_vcycles", C.c_int), ("last_converged", C.c_int),
+        ("kernel_launches", C.c_longlong), ("steps", C.c_longlong), ("error_flags", C.c_int),
+    ]
+
+
+class QZError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libqzb200.so (built in-tree by quantizer_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise QZError(f"{LIB_PATH} is missing: run `python -m quantizer_b200.build` "
+                      "(the CUDA library has no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "qz_default_config": ([C.POINTER(Config), C.c_int], C.c_int),
+        "qz_create": ([C.POINTER(Config), C.c_long, C.POINTER(vp)], C.c_int),
+        "qz_destroy": ([vp], C.c_int),
+        "qz_set_particles": ([vp, C.c_long] + [_P] * 7, C.c_int),
+        "qz_get_particles": ([vp] + [_P] * 9, C.c_int),
+        "qz_set_particle_accel": ([vp] + [_P] * 3, C.c_int),
+        "qz_num_particles": ([vp], C.c_long),
+        "qz_head_grid_points": ([vp], C.c_long),
+        "qz_get_head_field": ([vp, C.c_int, _P], C.c_int),
+        "qz_set_head_field": ([vp, C.c_int, _P], C.c_int),
+        "qz_initial_potential_head": ([vp], C.c_int),
+        "qz_reset": ([vp], C.c_int),
+        "qz_grid_density": ([vp], C.c_int),
+        "qz_potential": ([vp], C.c_int),
+        "qz_grid_acceleration": ([vp], C.c_int),
+        "qz_particle_acceleration": ([vp], C.c_int),
+        "qz_particle_updating_A": ([vp, C.c_double], C.c_int),
+        "qz_particle_updating_B": ([vp, C.c_double], C.c_int),
+        "qz_init_forces": ([vp], C.c_int),
+        "qz_step": ([vp, C.c_double, C.c_int], C.c_int),
+        "qz_synchronize": ([vp], C.c_int),
+        "qz_get_stats": ([vp, C.POINTER(Stats)], C.c_int),
+        "qz_stream": ([vp], vp),
+        "qz_last_error": ([], C.c_char_p),
+        "qz_gauss_saidel": ([_P, _P, C.c_int, C.c_int, C.c_double, C.c_int], C.c_int),
+        "qz_jacobi": ([_P, _P, C.c_int, C.c_int, C.c_double], C.c_int),
+        "qz_multigrid": ([C.POINTER(Config), _P, _P, C.c_int, C.c_int], C.c_int),
+        "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return [n for n in dir(load()) if n.startswith("qz_")]
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = load().qz_last_error().decode(errors="replace")
+        raise QZError(msg or "libqzb200 call failed")
+
+
+def _p(a: np.ndarray):
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_P)
+    return a.ctypes.data_as(_I)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def config(lmin: int, **kw) -> Config:
+    c = Config()
+    _check(load().qz_default_config(C.byref(c), lmin))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    return c
+
+
+def sequential_mass(m: np.ndarray) -> float:
+    """Total mass summed in index order, as the reference's input stage does."""
+    return float(np.cumsum(np.asarray(m, dtype=np.float64))[-1]) if len(m) else 0.0
+
+
+class Simulation:
+    """Head-node particle-mesh simulation held on the current CUDA device."""
+
+    def __init__(self, ic: dict, lmin: int, capacity: int | None = None, **cfg):
+        self.lib = load()
+        n = len(ic["x"])
+        cfg.setdefault("total_mass", sequential_mass(ic["m"]))
+        self.cfg = config(lmin, **cfg)
+        h = C.c_void_p()
+        _check(self.lib.qz_create(C.byref(self.cfg), capacity or n, C.byref(h)))
+        self.h = h
+        self.lmin = lmin
+        self.set_particles(ic)
+
+    # -- state ---------------------------------------------------------------------
+    def set_particles(self, ic: dict) -> None:
+        arrs = [_f64(ic[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+        _check(self.lib.qz_set_particles(self.h, arrs[0].size, *[_p(a) for a in arrs]))
+
+    def set_accelerations(self, ax, ay, az) -> None:
+        a = [_f64(v) for v in (ax, ay, az)]
+        _check(self.lib.qz_set_particle_accel(self.h, *[_p(v) for v in a]))
+
+    def step_host(self, state: dict, dt: float) -> None:
+        """One leapfrog step on host arrays, as the drop-in serves the
+        reference's main loop: the state (x..vz, ax..az, m) is copied to the
+        device, advanced, and x..vz, ax..az are copied back into `state`."""
+        self.set_particles(state)
+        self.set_accelerations(state["ax"], state["ay"], state["az"])
+        _check(self.lib.qz_step(self.h, dt, 1))
+        _check(self.lib.qz_get_particles(self.h, *[_p(state[k]) for k in
+                                                   ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]))
+
+    @property
+    def n(self) -> int:
+        return int(self.lib.qz_num_particles(self.h))
+
+    def particles(self) -> dict:
+        n = self.n
+        out = {k: np.empty(n) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+        _check(self.lib.qz_get_particles(self.h, *[_p(out[k]) for k in
+                                                   ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]))
+        return out
+
+    def field(self, name: str) -> np.ndarray:
+        g = int(self.lib.qz_head_grid_points(self.h))
+        out = np.empty(g)
+        _check(self.lib.qz_get_head_field(self.h, FIELDS[name], _p(out)))
+        return out
+
+    def set_field(self, name: str, values: np.ndarray) -> None:
+        a = _f64(values)
+        _check(self.lib.qz_set_head_field(self.h, FIELDS[name], _p(a)))
+
+    def stats(self) -> Stats:
+        s = Stats()
+        _check(self.lib.qz_get_stats(self.h, C.byref(s)))
+        return s
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.qz_stream(self.h) or 0)
+
+    # -- the reference's entry points ------------------------------------------------
+    def reset(self): _check(self.lib.qz_reset(self.h))
+    def grid_density(self): _check(self.lib.qz_grid_density(self.h))
+    def potential(self): _check(self.lib.qz_potential(self.h))
+    def grid_acceleration(self): _check(self.lib.qz_grid_acceleration(self.h))
+    def particle_acceleration(self): _check(self.lib.qz_particle_acceleration(self.h))
+    def particle_updating_A(self, dt): _check(self.lib.qz_particle_updating_A(self.h, dt))
+    def particle_updating_B(self, dt): _check(self.lib.qz_particle_updating_B(self.h, dt))
+    def initial_potential_head(self): _check(self.lib.qz_initial_potential_head(self.h))
+
+    def init_forces(self) -> None:
+        _check(self.lib.qz_init_forces(self.h))
+
+    def step(self, dt: float, nsteps: int = 1) -> None:
+        _check(self.lib.qz_step(self.h, dt, nsteps))
+
+    def synchronize(self) -> None:
+        _check(self.lib.qz_synchronize(self.h))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.qz_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+# -- array-level routines ---------------------------------------------------------------
+def gauss_saidel(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0,
+                 order: int = QZ_GS_REDBLACK) -> np.ndarray:
+    n = round(phi.size ** (1 / 3))
+    out = _f64(phi).copy()
+    r = _f64(rho)
+    _check(load().qz_gauss_saidel(_p(out), _p(r), n, iters, w, order))
+    return out
+
+
+def jacobi(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0) -> np.ndarray:
+    n = round(phi.size ** (1 / 3))
+    out = _f64(phi).copy()
+    r = _f64(rho)
+    _check(load().qz_jacobi(_p(out), _p(r), n, iters, w))
+    return out
+
+
+def multigrid(phi: np.ndarray, rho: np.ndarray, cycle: int = 0, **cfg) -> np.ndarray:
+    n = round(phi.size ** (1 / 3))
+    c = config(2, **cfg)
+    out = _f64(phi).copy()
+    r = _f64(rho)
+    _check(load().qz_multigrid(C.byref(c), _p(out), _p(r), n, cycle))
+    return out
+
+
+def ptcl_idx_to_box_idx(lv: int, box_ts: tuple, box_real_dim: tuple, x, y, z) -> np.ndarray:
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    out = np.empty(x.size, dtype=np.int32)
+    _check(load().qz_ptcl_idx_to_box_idx(lv, box_ts[0], box_ts[1], box_ts[2], box_real_dim[0],
+                                         box_real_dim[1], x.size, _p(x), _p(y), _p(z), _p(out)))
+    return out
+
+
+# -- per-launch profiler ---------------------------------------------------------------
+PROF_CATEGORIES = ("smooth", "restrict", "prolong", "check", "deposit", "sort", "gradient",
+                   "gather", "leapfrog", "other")
+
+
+def _prof_sig(lib):
+    if getattr(lib, "_prof_ready", False):
+        return
+    lib.qz_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    lib.qz_profile_reset.argtypes = [C.c_void_p]
+    lib.qz_profile_read.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib._prof_ready = True
+
+
+def profile_enable(sim: Simulation, on: bool = True) -> None:
+    _prof_sig(sim.lib)
+    _check(sim.lib.qz_profile_enable(sim.h, 1 if on else 0))
+
+
+def profile_reset(sim: Simulation) -> None:
+    _prof_sig(sim.lib)
+    _check(sim.lib.qz_profile_reset(sim.h))
+
+
+def profile_read(sim: Simulation) -> dict:
+    """{category: (launches, total_ms, algorithmic_bytes)} since the last reset."""
+    _prof_sig(sim.lib)
+    out = {}
+    for i, name in enumerate(PROF_CATEGORIES):
+        n, ms, b = C.c_longlong(), C.c_double(), C.c_double()
+        _check(sim.lib.qz_profile_read(sim.h, i, C.byref(n), C.byref(ms), C.byref(b)))
+        out[name] = (int(n.value), float(ms.value), float(b.value))
+    return out

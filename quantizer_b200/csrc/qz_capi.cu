@@ -1,0 +1,728 @@
+// qz_capi.cu -- the extern "C" surface of libqzb200 (include/qz_b200.h):
+// context lifecycle, host <-> device copies through pinned staging buffers,
+// per-stage entry points in the reference's main-loop order, and array-level
+// wrappers of the force_methods routines.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "qz_internal.cuh"
+
+namespace qz {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+bool check_cuda(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess)
+        return true;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+cudaEvent_t prof_event(qz_sim *s)
+{
+    if (!s->ev_pool.empty())
+    {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Books the elapsed time of every pending launch to its category and returns
+// the events to the pool (the stream must be idle).
+void prof_collect(qz_sim *s)
+{
+    for (auto &r : s->prof_pending)
+    {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.b, r.e) == cudaSuccess)
+        {
+            s->prof_launches[r.cat]++;
+            s->prof_ms[r.cat] += ms;
+            s->prof_bytes[r.cat] += r.bytes;
+        }
+        s->ev_pool.push_back(r.b);
+        s->ev_pool.push_back(r.e);
+    }
+    s->prof_pending.clear();
+    cudaGetLastError();
+}
+
+long radix_tiles(long n);
+void launch_box_idx(cudaStream_t st, long n, int lv, int tsx, int tsy, int tsz, int dimx,
+                    int dimy, const double *x, const double *y, const double *z, int *out);
+
+template <typename T>
+static bool dmalloc(T **p, size_t count, const char *what)
+{
+    *p = nullptr;
+    if (count == 0)
+        count = 1;
+    return check_cuda(cudaMalloc((void **)p, count * sizeof(T)), what);
+}
+
+static void dfree(void *p)
+{
+    if (p)
+        cudaFree(p);
+}
+
+// Allocates the multigrid hierarchy below a fine level of n0 points per side:
+// levels exist while the recursion of multigrid.c:175-191 reaches them
+// (coarse size >= 4).
+static bool build_levels(qz_sim *s, int n0)
+{
+    const bool mixed = s->cfg.precision == QZ_PREC_MIXED;
+    const bool jac = s->cfg.smoother == 1;
+    s->levels.clear();
+    Level l0;
+    l0.n = n0;
+    s->levels.push_back(l0);
+    int n = n0;
+    while (true)
+    {
+        int nc = (n + 1) / 2;
+        if (nc < 4)
+            break;
+        Level l;
+        l.n = nc;
+        size_t pts = (size_t)nc * nc * nc;
+        if (!dmalloc(&l.phi, pts, "mg phi") || !dmalloc(&l.rho, pts, "mg rho"))
+            return false;
+        cudaMemset(l.rho, 0, pts * sizeof(double));
+        if (mixed && (!dmalloc(&l.phif, pts, "mg phi32") || !dmalloc(&l.rhof, pts, "mg rho32")))
+            return false;
+        if (mixed)
+            cudaMemset(l.rhof, 0, pts * sizeof(float));
+        s->levels.push_back(l);
+        n = nc;
+    }
+    for (auto &l : s->levels)
+    {
+        size_t pts = (size_t)l.n * l.n * l.n;
+        if (jac && !dmalloc(&l.scr, pts, "jacobi scratch"))
+            return false;
+        if (jac && mixed && !dmalloc(&l.scrf, pts, "jacobi scratch32"))
+            return false;
+    }
+    if (mixed)
+    {
+        size_t pts = (size_t)n0 * n0 * n0;
+        if (!dmalloc(&s->rf, pts, "rf") || !dmalloc(&s->ef, pts, "ef"))
+            return false;
+        cudaMemset(s->rf, 0, pts * sizeof(float));
+        cudaMemset(s->ef, 0, pts * sizeof(float));
+    }
+    return true;
+}
+
+static void free_levels(qz_sim *s)
+{
+    for (size_t i = 0; i < s->levels.size(); i++)
+    {
+        Level &l = s->levels[i];
+        if (i > 0)
+        {
+            dfree(l.phi);
+            dfree(l.rho);
+            dfree(l.phif);
+            dfree(l.rhof);
+        }
+        dfree(l.scr);
+        dfree(l.scrf);
+    }
+    s->levels.clear();
+    dfree(s->rf);
+    dfree(s->ef);
+    s->rf = s->ef = nullptr;
+}
+
+static bool ensure_stage(qz_sim *s, size_t bytes)
+{
+    if (s->h_stage_bytes >= bytes)
+        return true;
+    if (s->h_stage)
+        cudaFreeHost(s->h_stage);
+    s->h_stage = nullptr;
+    s->h_stage_bytes = 0;
+    if (!check_cuda(cudaMallocHost((void **)&s->h_stage, bytes), "pinned staging"))
+        return false;
+    s->h_stage_bytes = bytes;
+    return true;
+}
+
+// Copies `count` doubles host -> device through the pinned stage (when the
+// host pointer is pageable) on the library stream.
+static bool h2d(qz_sim *s, double *dst, const double *src, long count)
+{
+    if (count <= 0)
+        return true;
+    size_t bytes = (size_t)count * sizeof(double);
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost)
+        return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream),
+                          "h2d");
+    cudaGetLastError();
+    if (!ensure_stage(s, bytes))
+        return false;
+    if (!check_cuda(cudaStreamSynchronize(s->stream), "h2d sync"))
+        return false;
+    memcpy(s->h_stage, src, bytes);
+    return check_cuda(cudaMemcpyAsync(dst, s->h_stage, bytes, cudaMemcpyHostToDevice, s->stream),
+                      "h2d");
+}
+
+static bool d2h(qz_sim *s, double *dst, const double *src, long count)
+{
+    if (count <= 0 || !dst)
+        return true;
+    size_t bytes = (size_t)count * sizeof(double);
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost)
+        return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream),
+                          "d2h") &&
+               check_cuda(cudaStreamSynchronize(s->stream), "d2h sync");
+    cudaGetLastError();
+    if (!ensure_stage(s, bytes))
+        return false;
+    if (!check_cuda(cudaMemcpyAsync(s->h_stage, src, bytes, cudaMemcpyDeviceToHost, s->stream),
+                    "d2h") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "d2h sync"))
+        return false;
+    memcpy(dst, s->h_stage, bytes);
+    return true;
+}
+
+static int check_flags(qz_sim *s)
+{
+    if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
+                                    cudaMemcpyDeviceToHost, s->stream),
+                    "flags") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "flags sync"))
+        return QZ_FAILURE;
+    int e = s->h_flags[F_ERROR];
+    s->stats.error_flags |= e;
+    if (e)
+    {
+        cudaMemsetAsync(s->flags + F_ERROR, 0, sizeof(int), s->stream);
+        set_error("device bounds check failed (flags 0x%x): a particle left the unit box", e);
+        return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+} // namespace qz
+
+using namespace qz;
+
+extern "C" {
+
+const char *qz_last_error(void) { return g_err; }
+
+int qz_default_config(qz_config *c, int lmin)
+{
+    if (!c)
+        return QZ_FAILURE;
+    memset(c, 0, sizeof *c);
+    c->lmin = lmin;
+    c->lmax = lmin;
+    c->G = 1.0;
+    c->total_mass = 1.0;
+    c->bdry = 1;
+    c->smoother = 0;
+    c->gs_order = QZ_GS_REDBLACK;
+    c->cycle = 0;
+    c->n_pre = 2;
+    c->n_post = 2;
+    c->n_coarse = 2;
+    c->w_sor = 1.0;
+    c->tol = 1.0e-10;
+    c->tol2 = 1.0e-10;
+    c->check_every = 5;
+    c->max_iter = 5000;
+    c->check_method = 0;
+    c->precision = QZ_PREC_FP64;
+    c->inner_cycles = 1;
+    c->force_stencil = 0;
+    return QZ_SUCCESS;
+}
+
+int qz_destroy(qz_sim *s)
+{
+    if (!s)
+        return QZ_SUCCESS;
+    if (s->stream)
+        cudaStreamSynchronize(s->stream);
+    prof_collect(s);
+    for (cudaEvent_t e : s->ev_pool)
+        cudaEventDestroy(e);
+    s->ev_pool.clear();
+    void *ptrs[] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m,
+                    s->pot, s->pot_old, s->d, s->gax, s->gay, s->gaz, s->sort.k0, s->sort.k1,
+                    s->sort.v0, s->sort.v1, s->sort.hist, s->seg_head, s->seg_id, s->seg_start,
+                    s->seg_cell, s->cell_seg, s->cell_sums, s->scan_tmp, s->red, s->flags};
+    for (void *p : ptrs)
+        dfree(p);
+    free_levels(s);
+    if (s->h_flags)
+        cudaFreeHost(s->h_flags);
+    if (s->h_stage)
+        cudaFreeHost(s->h_stage);
+    if (s->stream)
+        cudaStreamDestroy(s->stream);
+    delete s;
+    return QZ_SUCCESS;
+}
+
+int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
+{
+    if (!cfg || !out || n_capacity < 0)
+    {
+        set_error("qz_create: bad arguments");
+        return QZ_FAILURE;
+    }
+    *out = nullptr;
+    if (cfg->lmin < 2 || cfg->lmin > 9)
+    {
+        set_error("qz_create: lmin=%d outside the supported range 2..9", cfg->lmin);
+        return QZ_FAILURE;
+    }
+    if (cfg->lmax != cfg->lmin)
+    {
+        set_error("qz_create: this context runs the head-only path (lmax == lmin)");
+        return QZ_FAILURE;
+    }
+    if (cfg->bdry != 0 && cfg->bdry != 1)
+    {
+        set_error("qz_create: bdry=%d not supported (0 periodic, 1 reflexive)", cfg->bdry);
+        return QZ_FAILURE;
+    }
+    if (cfg->force_stencil != 0 || cfg->smoother < 0 || cfg->smoother > 1 || cfg->cycle < 0 ||
+        cfg->cycle > 2 || n_capacity > (1L << 30))
+    {
+        set_error("qz_create: unsupported configuration");
+        return QZ_FAILURE;
+    }
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    {
+        cudaGetLastError();
+        set_error("qz_create: no CUDA device is available (this library has no CPU path)");
+        return QZ_FAILURE;
+    }
+    qz_sim *s = new qz_sim();
+    s->cfg = *cfg;
+    cudaGetDevice(&s->device);
+    if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream"))
+    {
+        delete s;
+        return QZ_FAILURE;
+    }
+    s->cap = n_capacity;
+    s->L = cfg->lmin;
+    s->D = (1L << s->L) + 3;
+    s->gpts = s->D * s->D * s->D;
+    const long B = (1L << s->L) + 2;
+    const long cap = n_capacity > 0 ? n_capacity : 1;
+    bool ok = dmalloc(&s->x, cap, "x") && dmalloc(&s->y, cap, "y") && dmalloc(&s->z, cap, "z") &&
+              dmalloc(&s->vx, cap, "vx") && dmalloc(&s->vy, cap, "vy") &&
+              dmalloc(&s->vz, cap, "vz") && dmalloc(&s->ax, cap, "ax") &&
+              dmalloc(&s->ay, cap, "ay") && dmalloc(&s->az, cap, "az") && dmalloc(&s->m, cap, "m");
+    ok = ok && dmalloc(&s->pot, s->gpts, "pot") && dmalloc(&s->pot_old, s->gpts, "pot_old") &&
+         dmalloc(&s->d, s->gpts, "d") && dmalloc(&s->gax, s->gpts, "gax") &&
+         dmalloc(&s->gay, s->gpts, "gay") && dmalloc(&s->gaz, s->gpts, "gaz");
+    long tiles = radix_tiles(cap);
+    ok = ok && dmalloc(&s->sort.k0, cap, "keys") && dmalloc(&s->sort.k1, cap, "keys") &&
+         dmalloc(&s->sort.v0, cap, "vals") && dmalloc(&s->sort.v1, cap, "vals") &&
+         dmalloc(&s->sort.hist, 256 * tiles, "hist");
+    ok = ok && dmalloc(&s->seg_head, cap, "seg") && dmalloc(&s->seg_id, cap, "seg") &&
+         dmalloc(&s->seg_start, cap + 1, "seg") && dmalloc(&s->seg_cell, cap, "seg") &&
+         dmalloc(&s->cell_seg, B * B * B, "cell_seg") && dmalloc(&s->cell_sums, 8 * cap, "cs");
+    s->red_blocks = 296;
+    ok = ok && dmalloc(&s->red, s->red_blocks + 8, "red") && dmalloc(&s->flags, F_COUNT, "flags");
+    ok = ok && check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned");
+    s->sort.cap = cap;
+    s->sort.tiles_cap = tiles;
+    if (ok)
+    {
+        cudaMemset(s->flags, 0, F_COUNT * sizeof(int));
+        size_t gb = s->gpts * sizeof(double);
+        cudaMemset(s->pot_old, 0, gb);
+        cudaMemset(s->d, 0, gb);
+        s->fine_phi = head_view(s, s->pot);
+        s->fine_rho = head_view(s, s->d);
+        ok = build_levels(s, (1 << s->L) + 1);
+    }
+    if (ok)
+        ok = head_initial(s) == QZ_SUCCESS;
+    if (ok)
+        ok = check_cuda(cudaStreamSynchronize(s->stream), "create sync") &&
+             check_cuda(cudaDeviceSynchronize(), "create device sync");
+    if (!ok)
+    {
+        char keep[512];
+        snprintf(keep, sizeof keep, "%s", g_err);
+        qz_destroy(s);
+        set_error("%s", keep);
+        return QZ_FAILURE;
+    }
+    *out = s;
+    return QZ_SUCCESS;
+}
+
+int qz_set_particles(qz_sim *s, long n, const double *x, const double *y, const double *z,
+                     const double *vx, const double *vy, const double *vz, const double *m)
+{
+    if (!s || n < 0 || n > s->cap)
+    {
+        set_error("qz_set_particles: n=%ld exceeds capacity", n);
+        return QZ_FAILURE;
+    }
+    s->n = n;
+    bool ok = h2d(s, s->x, x, n) && h2d(s, s->y, y, n) && h2d(s, s->z, z, n) &&
+              h2d(s, s->vx, vx, n) && h2d(s, s->vy, vy, n) && h2d(s, s->vz, vz, n) &&
+              h2d(s, s->m, m, n);
+    if (ok)
+    {
+        size_t b = (size_t)(n > 0 ? n : 1) * sizeof(double);
+        ok = check_cuda(cudaMemsetAsync(s->ax, 0, b, s->stream), "memset") &&
+             check_cuda(cudaMemsetAsync(s->ay, 0, b, s->stream), "memset") &&
+             check_cuda(cudaMemsetAsync(s->az, 0, b, s->stream), "memset");
+    }
+    s->forces_ready = false;
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_set_particle_accel(qz_sim *s, const double *ax, const double *ay, const double *az)
+{
+    if (!s)
+        return QZ_FAILURE;
+    // accelerations supplied by the caller: the next step starts from them
+    bool ok = h2d(s, s->ax, ax, s->n) && h2d(s, s->ay, ay, s->n) && h2d(s, s->az, az, s->n);
+    s->forces_ready = ok;
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_get_particles(qz_sim *s, double *x, double *y, double *z, double *vx, double *vy,
+                     double *vz, double *ax, double *ay, double *az)
+{
+    if (!s)
+        return QZ_FAILURE;
+    long n = s->n;
+    bool ok = d2h(s, x, s->x, n) && d2h(s, y, s->y, n) && d2h(s, z, s->z, n) &&
+              d2h(s, vx, s->vx, n) && d2h(s, vy, s->vy, n) && d2h(s, vz, s->vz, n) &&
+              d2h(s, ax, s->ax, n) && d2h(s, ay, s->ay, n) && d2h(s, az, s->az, n);
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+long qz_num_particles(const qz_sim *s) { return s ? s->n : 0; }
+
+long qz_head_grid_points(const qz_sim *s) { return s ? s->gpts : 0; }
+
+static double *field_ptr(qz_sim *s, int which)
+{
+    switch (which)
+    {
+    case QZ_FIELD_POT: return s->pot;
+    case QZ_FIELD_POT_OLD: return s->pot_old;
+    case QZ_FIELD_DENSITY: return s->d;
+    case QZ_FIELD_AX: return s->gax;
+    case QZ_FIELD_AY: return s->gay;
+    case QZ_FIELD_AZ: return s->gaz;
+    default: return nullptr;
+    }
+}
+
+int qz_get_head_field(qz_sim *s, int which, double *out)
+{
+    double *f = s ? field_ptr(s, which) : nullptr;
+    if (!f || !out)
+    {
+        set_error("qz_get_head_field: bad field %d", which);
+        return QZ_FAILURE;
+    }
+    return d2h(s, out, f, s->gpts) ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_set_head_field(qz_sim *s, int which, const double *in)
+{
+    double *f = s ? field_ptr(s, which) : nullptr;
+    if (!f || !in)
+    {
+        set_error("qz_set_head_field: bad field %d", which);
+        return QZ_FAILURE;
+    }
+    return h2d(s, f, in, s->gpts) ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_initial_potential_head(qz_sim *s) { return s ? head_initial(s) : QZ_FAILURE; }
+
+// reset.c:29-64: particle accelerations and head density to zero.
+int qz_reset(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    size_t b = (size_t)(s->n > 0 ? s->n : 1) * sizeof(double);
+    bool ok = check_cuda(cudaMemsetAsync(s->ax, 0, b, s->stream), "reset") &&
+              check_cuda(cudaMemsetAsync(s->ay, 0, b, s->stream), "reset") &&
+              check_cuda(cudaMemsetAsync(s->az, 0, b, s->stream), "reset") &&
+              check_cuda(cudaMemsetAsync(s->d, 0, s->gpts * sizeof(double), s->stream), "reset");
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_grid_density(qz_sim *s) { return s ? deposit_head(s) : QZ_FAILURE; }
+
+int qz_potential(qz_sim *s) { return s ? potential_head(s) : QZ_FAILURE; }
+
+int qz_poisson_error(qz_sim *s, int *converged)
+{
+    if (!s || !converged)
+        return QZ_FAILURE;
+    return poisson_error_head(s, converged);
+}
+
+int qz_grid_acceleration(qz_sim *s) { return s ? grid_accel_head(s) : QZ_FAILURE; }
+
+int qz_particle_acceleration(qz_sim *s) { return s ? gather_head(s) : QZ_FAILURE; }
+
+int qz_particle_updating_A(qz_sim *s, double dt) { return s ? kick_drift(s, dt) : QZ_FAILURE; }
+
+int qz_particle_updating_B(qz_sim *s, double dt) { return s ? kick(s, dt) : QZ_FAILURE; }
+
+int qz_init_forces(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    if (qz_reset(s) || deposit_head(s) || potential_head(s) || grid_accel_head(s) ||
+        gather_head(s) || check_flags(s))
+        return QZ_FAILURE;
+    s->forces_ready = true;
+    return QZ_SUCCESS;
+}
+
+int qz_step(qz_sim *s, double dt, int nsteps)
+{
+    if (!s)
+        return QZ_FAILURE;
+    if (!s->forces_ready && qz_init_forces(s))
+        return QZ_FAILURE;
+    for (int q = 0; q < nsteps; q++)
+    {
+        if (kick_drift(s, dt) || qz_reset(s) || deposit_head(s) || potential_head(s) ||
+            grid_accel_head(s) || gather_head(s) || kick(s, dt))
+            return QZ_FAILURE;
+        s->stats.steps++;
+    }
+    return check_flags(s);
+}
+
+int qz_synchronize(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    return check_cuda(cudaStreamSynchronize(s->stream), "synchronize") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int qz_get_stats(qz_sim *s, qz_stats *out)
+{
+    if (!s || !out)
+        return QZ_FAILURE;
+    *out = s->stats;
+    return QZ_SUCCESS;
+}
+
+void *qz_stream(qz_sim *s) { return s ? (void *)s->stream : nullptr; }
+
+int qz_profile_enable(qz_sim *s, int on)
+{
+    if (!s)
+        return QZ_FAILURE;
+    if (!check_cuda(cudaStreamSynchronize(s->stream), "profile sync"))
+        return QZ_FAILURE;
+    prof_collect(s);
+    s->prof = on != 0;
+    return QZ_SUCCESS;
+}
+
+int qz_profile_reset(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    if (!check_cuda(cudaStreamSynchronize(s->stream), "profile sync"))
+        return QZ_FAILURE;
+    prof_collect(s);
+    for (int c = 0; c < QZ_PROF_CATEGORIES; c++)
+    {
+        s->prof_launches[c] = 0;
+        s->prof_ms[c] = 0.0;
+        s->prof_bytes[c] = 0.0;
+    }
+    return QZ_SUCCESS;
+}
+
+int qz_profile_read(qz_sim *s, int cat, long long *launches, double *total_ms, double *bytes)
+{
+    if (!s || cat < 0 || cat >= QZ_PROF_CATEGORIES)
+        return QZ_FAILURE;
+    if (!check_cuda(cudaStreamSynchronize(s->stream), "profile sync"))
+        return QZ_FAILURE;
+    prof_collect(s);
+    if (launches)
+        *launches = s->prof_launches[cat];
+    if (total_ms)
+        *total_ms = s->prof_ms[cat];
+    if (bytes)
+        *bytes = s->prof_bytes[cat];
+    return QZ_SUCCESS;
+}
+
+// ---- array-level wrappers ------------------------------------------------------------
+// A minimal context whose fine level is a dense gridsize^3 device copy of the
+// caller's arrays.
+static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, double **drho)
+{
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    {
+        cudaGetLastError();
+        set_error("no CUDA device is available (this library has no CPU path)");
+        return nullptr;
+    }
+    qz_sim *s = new qz_sim();
+    s->cfg = *cfg;
+    cudaGetDevice(&s->device);
+    size_t pts = (size_t)gridsize * gridsize * gridsize;
+    if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream") ||
+        !dmalloc(dphi, pts, "phi") || !dmalloc(drho, pts, "rho") ||
+        !check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned"))
+    {
+        qz_destroy(s);
+        return nullptr;
+    }
+    s->fine_phi = dense_view(*dphi, gridsize);
+    s->fine_rho = dense_view(*drho, gridsize);
+    if (!build_levels(s, gridsize))
+    {
+        qz_destroy(s);
+        return nullptr;
+    }
+    return s;
+}
+
+static int run_dense(const qz_config *cfg, double *phi, const double *rho, int gridsize,
+                     int (*body)(qz_sim *, void *), void *arg)
+{
+    if (!phi || !rho || gridsize < 3)
+    {
+        set_error("bad grid arguments");
+        return QZ_FAILURE;
+    }
+    double *dphi = nullptr, *drho = nullptr;
+    qz_sim *s = dense_context(cfg, gridsize, &dphi, &drho);
+    if (!s)
+        return QZ_FAILURE;
+    long pts = (long)gridsize * gridsize * gridsize;
+    int rc = (h2d(s, dphi, phi, pts) && h2d(s, drho, rho, pts)) ? body(s, arg) : QZ_FAILURE;
+    if (rc == QZ_SUCCESS && !d2h(s, phi, dphi, pts))
+        rc = QZ_FAILURE;
+    dfree(dphi);
+    dfree(drho);
+    qz_destroy(s);
+    return rc;
+}
+
+struct SmoothArg {
+    int iters;
+};
+static int smooth_body(qz_sim *s, void *a)
+{
+    return smooth(s, s->fine_phi, s->fine_rho, ((SmoothArg *)a)->iters);
+}
+struct CycleArg {
+    int type;
+};
+static int cycle_body(qz_sim *s, void *a) { return vcycle(s, 0, ((CycleArg *)a)->type); }
+
+int qz_gauss_saidel(double *phi, const double *rho, int gridsize, int iter_max, double w,
+                    int gs_order)
+{
+    qz_config c;
+    qz_default_config(&c, 2);
+    c.smoother = 0;
+    c.w_sor = w;
+    c.gs_order = gs_order;
+    SmoothArg a{iter_max};
+    return run_dense(&c, phi, rho, gridsize, smooth_body, &a);
+}
+
+int qz_jacobi(double *phi, const double *rho, int gridsize, int iter_max, double w)
+{
+    qz_config c;
+    qz_default_config(&c, 2);
+    c.smoother = 1;
+    c.w_sor = w;
+    SmoothArg a{iter_max};
+    return run_dense(&c, phi, rho, gridsize, smooth_body, &a);
+}
+
+int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, int gridsize,
+                 int type_multigrid)
+{
+    if (!cfg)
+        return QZ_FAILURE;
+    qz_config c = *cfg;
+    c.precision = QZ_PREC_FP64;
+    CycleArg a{type_multigrid};
+    return run_dense(&c, phi, rho, gridsize, cycle_body, &a);
+}
+
+int qz_ptcl_idx_to_box_idx(int lv, int tsx, int tsy, int tsz, int dimx, int dimy, long n,
+                           const double *x, const double *y, const double *z, int *out)
+{
+    if (n <= 0)
+        return QZ_SUCCESS;
+    if (!x || !y || !z || !out)
+        return QZ_FAILURE;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    {
+        cudaGetLastError();
+        set_error("no CUDA device is available (this library has no CPU path)");
+        return QZ_FAILURE;
+    }
+    double *d[3] = {nullptr, nullptr, nullptr};
+    int *dout = nullptr;
+    const double *h[3] = {x, y, z};
+    bool ok = true;
+    for (int c = 0; c < 3 && ok; c++)
+        ok = dmalloc(&d[c], n, "box idx") &&
+             check_cuda(cudaMemcpy(d[c], h[c], n * sizeof(double), cudaMemcpyHostToDevice),
+                        "box idx h2d");
+    ok = ok && dmalloc(&dout, n, "box idx");
+    if (ok)
+    {
+        launch_box_idx(0, n, lv, tsx, tsy, tsz, dimx, dimy, d[0], d[1], d[2], dout);
+        ok = check_cuda(cudaGetLastError(), "box idx") &&
+             check_cuda(cudaMemcpy(out, dout, n * sizeof(int), cudaMemcpyDeviceToHost),
+                        "box idx d2h");
+    }
+    for (int c = 0; c < 3; c++)
+        dfree(d[c]);
+    dfree(dout);
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+} // extern "C"

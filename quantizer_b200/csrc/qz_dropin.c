@@ -1,0 +1,449 @@
+/*
+ * qz_dropin.c -- libqz_dropin.so: the reference's hot-path symbols
+ * (include/qz_dropin.h) implemented on libqzb200's device pipeline.
+ *
+ * At the first call the shim finds the reference's globals in the host
+ * program (dlsym on the running image), creates a qz_sim from the parameters
+ * the reference's global_variables() set, and uploads the particle arrays and
+ * the head node's grid fields.  Afterwards the device copy is authoritative:
+ * each entry point runs on the device and writes the arrays it changed back
+ * to the host globals before returning (write-through), so host code that
+ * reads them (timestep, observables, snapshots) always sees current values.
+ *
+ * Scope of this build: the head-only path (lmax == lmin) with reflexive or
+ * periodic boundaries, Gauss-Seidel or Jacobi smoothing, the 3-point force
+ * stencil.  Other configurations are rejected with the reference's error
+ * convention (message + _FAILURE_).
+ *
+ * Environment: QZ_GS_ORDER=lex selects the reference's lexicographic
+ * Gauss-Seidel order for the head solve (default red-black);
+ * QZ_PRECISION=mixed selects FP32 cycles inside FP64 defect correction.
+ */
+#define _GNU_SOURCE
+#include <dlfcn.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/qz_b200.h"
+#include "../../include/qz_dropin.h"
+#include "qz_ref_abi.h"
+
+#define REF_SUCCESS 0
+#define REF_FAILURE 1
+
+/* The reference's globals the hot path reads (headers/common.h:105-260). */
+static struct {
+    double **ptcl_mass, **ptcl_x, **ptcl_y, **ptcl_z, **ptcl_vx, **ptcl_vy, **ptcl_vz;
+    double **ptcl_ax, **ptcl_ay, **ptcl_az;
+    int *no_ptcl_final, *no_ptcl_initial, *lmin, *lmax, *bdry_cond_type;
+    double *G, *total_mass_initial;
+    struct node **ptr_tree;
+    int *niter_pre, *niter_post, *niter_coarse, *solver_pre, *solver_post, *solver_coarse;
+    int *cycle, *check_every, *max_iter, *check_method, *head_pot_method, *force_stencil;
+    double *w_sor_head, *tol, *tol2;
+    int resolved;
+} R;
+
+static qz_sim *g_sim = NULL;
+static int g_failed = 0;
+
+static void *need(const char *name, int *ok)
+{
+    void *p = dlsym(RTLD_DEFAULT, name);
+    if (!p)
+    {
+        printf("\nERROR (drop-in): the host program does not export the global '%s' "
+               "(link it with -Wl,--export-dynamic)\n", name);
+        *ok = 0;
+    }
+    return p;
+}
+
+static int resolve(void)
+{
+    if (R.resolved)
+        return 1;
+    int ok = 1;
+    R.ptcl_mass = need("GL_ptcl_mass", &ok);
+    R.ptcl_x = need("GL_ptcl_x", &ok);
+    R.ptcl_y = need("GL_ptcl_y", &ok);
+    R.ptcl_z = need("GL_ptcl_z", &ok);
+    R.ptcl_vx = need("GL_ptcl_vx", &ok);
+    R.ptcl_vy = need("GL_ptcl_vy", &ok);
+    R.ptcl_vz = need("GL_ptcl_vz", &ok);
+    R.ptcl_ax = need("GL_ptcl_ax", &ok);
+    R.ptcl_ay = need("GL_ptcl_ay", &ok);
+    R.ptcl_az = need("GL_ptcl_az", &ok);
+    R.no_ptcl_final = need("GL_no_ptcl_final", &ok);
+    R.no_ptcl_initial = need("GL_no_ptcl_initial", &ok);
+    R.lmin = need("lmin", &ok);
+    R.lmax = need("lmax", &ok);
+    R.bdry_cond_type = need("bdry_cond_type", &ok);
+    R.G = need("_G_", &ok);
+    R.total_mass_initial = need("GL_total_mass_initial", &ok);
+    R.ptr_tree = need("GL_ptr_tree", &ok);
+    R.niter_pre = need("_NiterPreS_", &ok);
+    R.niter_post = need("_NiterPostS_", &ok);
+    R.niter_coarse = need("_Niterfinddphic_", &ok);
+    R.solver_pre = need("solverPreS", &ok);
+    R.solver_post = need("solverPostS", &ok);
+    R.solver_coarse = need("solverfinddphic", &ok);
+    R.cycle = need("multigrid_cycle", &ok);
+    R.check_every = need("iter_between_check_potential_solution", &ok);
+    R.max_iter = need("_MAX_NUMBER_OF_ITERATIONS_IN_POISSON_EQUATION_", &ok);
+    R.check_method = need("check_poisson_error_method", &ok);
+    R.head_pot_method = need("head_pot_method", &ok);
+    R.force_stencil = need("force_stencil", &ok);
+    R.w_sor_head = need("_w_SOR_HEAD_", &ok);
+    R.tol = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_", &ok);
+    R.tol2 = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_2", &ok);
+    R.resolved = ok;
+    return ok;
+}
+
+static void fill_config(qz_config *c)
+{
+    qz_default_config(c, *R.lmin);
+    c->lmax = *R.lmax;
+    c->G = *R.G;
+    c->total_mass = *R.total_mass_initial;
+    c->bdry = *R.bdry_cond_type;
+    c->smoother = *R.solver_pre;
+    c->cycle = *R.cycle;
+    c->n_pre = *R.niter_pre;
+    c->n_post = *R.niter_post;
+    c->n_coarse = *R.niter_coarse;
+    c->w_sor = *R.w_sor_head;
+    c->tol = *R.tol;
+    c->tol2 = *R.tol2;
+    c->check_every = *R.check_every;
+    c->max_iter = *R.max_iter;
+    c->check_method = *R.check_method;
+    c->force_stencil = *R.force_stencil;
+    const char *o = getenv("QZ_GS_ORDER");
+    c->gs_order = (o && !strcmp(o, "lex")) ? QZ_GS_LEX : QZ_GS_REDBLACK;
+    const char *p = getenv("QZ_PRECISION");
+    c->precision = (p && !strcmp(p, "mixed")) ? QZ_PREC_MIXED : QZ_PREC_FP64;
+}
+
+static int fail(const char *what)
+{
+    printf("\nERROR (drop-in): %s: %s\n", what, qz_last_error());
+    g_failed = 1;
+    return REF_FAILURE;
+}
+
+static int upload_all(void)
+{
+    struct node *h = *R.ptr_tree;
+    long n = *R.no_ptcl_final;
+    if (qz_set_particles(g_sim, n, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
+                         *R.ptcl_vz, *R.ptcl_mass) ||
+        qz_set_particle_accel(g_sim, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az) ||
+        qz_set_head_field(g_sim, QZ_FIELD_POT, h->ptr_pot) ||
+        qz_set_head_field(g_sim, QZ_FIELD_POT_OLD, h->ptr_pot_old) ||
+        qz_set_head_field(g_sim, QZ_FIELD_DENSITY, h->ptr_d) ||
+        qz_set_head_field(g_sim, QZ_FIELD_AX, h->ptr_ax) ||
+        qz_set_head_field(g_sim, QZ_FIELD_AY, h->ptr_ay) ||
+        qz_set_head_field(g_sim, QZ_FIELD_AZ, h->ptr_az))
+        return fail("upload of the host state");
+    return REF_SUCCESS;
+}
+
+/* Creates the device context on first use. */
+static int ensure(void)
+{
+    if (g_sim)
+        return REF_SUCCESS;
+    if (g_failed)
+        return REF_FAILURE;
+    if (!resolve())
+    {
+        g_failed = 1;
+        return REF_FAILURE;
+    }
+    if (*R.lmin != *R.lmax)
+    {
+        printf("\nERROR (drop-in): lmax > lmin (refinement) is not supported by this build\n");
+        g_failed = 1;
+        return REF_FAILURE;
+    }
+    if (*R.head_pot_method != 0 || *R.solver_pre != *R.solver_post ||
+        *R.solver_pre != *R.solver_coarse || *R.solver_pre > 1)
+    {
+        printf("\nERROR (drop-in): head solver configuration not supported "
+               "(multigrid with Gauss-Seidel or Jacobi smoothing only)\n");
+        g_failed = 1;
+        return REF_FAILURE;
+    }
+    qz_config c;
+    fill_config(&c);
+    if (qz_create(&c, *R.no_ptcl_initial, &g_sim))
+    {
+        g_sim = NULL;
+        return fail("device context");
+    }
+    return upload_all();
+}
+
+static int head_field_back(int which, double *dst)
+{
+    if (qz_get_head_field(g_sim, which, dst))
+        return fail("head field read-back");
+    return REF_SUCCESS;
+}
+
+/* grid_density.c:269-306 */
+void grid_density(void)
+{
+    if (ensure())
+        return;
+    if (qz_grid_density(g_sim))
+    {
+        fail("grid_density");
+        return;
+    }
+    head_field_back(QZ_FIELD_DENSITY, (*R.ptr_tree)->ptr_d);
+}
+
+/* potential_head_node.c:99-179 */
+int potential_head_node(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_potential(g_sim))
+    {
+        printf("\n\n Error running potential_head_node() function \n\n ");
+        return fail("potential_head_node");
+    }
+    struct node *h = *R.ptr_tree;
+    if (head_field_back(QZ_FIELD_POT, h->ptr_pot) || head_field_back(QZ_FIELD_POT_OLD, h->ptr_pot_old))
+        return REF_FAILURE;
+    return REF_SUCCESS;
+}
+
+/* potential_branches.c:401-532: nothing to solve without refinement. */
+int potential_branches(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    return REF_SUCCESS;
+}
+
+/* potential.c:29-51 */
+int potential(void)
+{
+    if (potential_head_node())
+        return REF_FAILURE;
+    if (*R.lmin < *R.lmax && potential_branches())
+        return REF_FAILURE;
+    return REF_SUCCESS;
+}
+
+/* grid_acceleration.c:694-738 */
+int grid_acceleration(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_grid_acceleration(g_sim))
+        return fail("grid_acceleration");
+    struct node *h = *R.ptr_tree;
+    if (head_field_back(QZ_FIELD_AX, h->ptr_ax) || head_field_back(QZ_FIELD_AY, h->ptr_ay) ||
+        head_field_back(QZ_FIELD_AZ, h->ptr_az))
+        return REF_FAILURE;
+    return REF_SUCCESS;
+}
+
+/* particle_acceleration.c:522-573 */
+int particle_acceleration(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_particle_acceleration(g_sim) ||
+        qz_get_particles(g_sim, NULL, NULL, NULL, NULL, NULL, NULL, *R.ptcl_ax, *R.ptcl_ay,
+                         *R.ptcl_az))
+        return fail("particle_acceleration");
+    return REF_SUCCESS;
+}
+
+/* particle_updating.c:2584-2675 */
+int particle_updating_A(double dt)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_particle_updating_A(g_sim, dt) ||
+        qz_get_particles(g_sim, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
+                         *R.ptcl_vz, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az))
+        return fail("particle_updating_A");
+    return REF_SUCCESS;
+}
+
+/* particle_updating.c:2787-2837 */
+void particle_updating_B(double dt)
+{
+    if (ensure())
+        return;
+    if (qz_particle_updating_B(g_sim, dt) ||
+        qz_get_particles(g_sim, NULL, NULL, NULL, *R.ptcl_vx, *R.ptcl_vy, *R.ptcl_vz, NULL, NULL,
+                         NULL))
+        fail("particle_updating_B");
+}
+
+/* reset.c:29-64: the host copies are zeroed with the device copies. */
+int reset(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_reset(g_sim))
+        return fail("reset");
+    long n = *R.no_ptcl_final;
+    memset(*R.ptcl_ax, 0, n * sizeof(double));
+    memset(*R.ptcl_ay, 0, n * sizeof(double));
+    memset(*R.ptcl_az, 0, n * sizeof(double));
+    struct node *h = *R.ptr_tree;
+    memset(h->ptr_d, 0, (size_t)qz_head_grid_points(g_sim) * sizeof(double));
+    return REF_SUCCESS;
+}
+
+/* ptcl_idx_to_box_idx.c:30-139.  The scalar form answers a host caller about
+ * one host-resident particle (the reference's tree bookkeeping calls it per
+ * particle), so it is evaluated in place with the reference's integer
+ * arithmetic; batches go through qz_ptcl_idx_to_box_idx on the device. */
+int ptcl_idx_to_box_idx(struct node *p, int i)
+{
+    if (!resolve())
+        return 0;
+    const int lv = p->lv;
+    const double X = (*R.ptcl_x)[i], Y = (*R.ptcl_y)[i], Z = (*R.ptcl_z)[i];
+    const double px = X * (1 << lv), py = Y * (1 << lv), pz = Z * (1 << lv);
+    const int fx = px < 0 ? -1 : (int)px, fy = py < 0 ? -1 : (int)py, fz = pz < 0 ? -1 : (int)pz;
+    int bx = fx - p->box_ts_x, by = fy - p->box_ts_y, bz = fz - p->box_ts_z;
+    if (p->pbc_crosses_sim_box_bdry)
+    {
+        /* periodic nodes that straddle or span the box (ptcl_idx_to_box_idx.c:69-131) */
+        const bool whole[3] = {p->pbc_crosses_whole_sim_box_x, p->pbc_crosses_whole_sim_box_y,
+                               p->pbc_crosses_whole_sim_box_z};
+        const bool cross[3] = {p->pbc_crosses_sim_box_bdry_x, p->pbc_crosses_sim_box_bdry_y,
+                               p->pbc_crosses_sim_box_bdry_z};
+        const int f[3] = {fx, fy, fz}, mx[3] = {p->box_max_x, p->box_max_y, p->box_max_z};
+        const double q[3] = {X, Y, Z};
+        int *b[3] = {&bx, &by, &bz};
+        for (int c = 0; c < 3; c++)
+        {
+            if (!whole[c])
+            {
+                if (cross[c] && f[c] > mx[c] + 1)
+                    *b[c] -= (1 << lv);
+            }
+            else if (q[c] < 0.)
+                *b[c] += (1 << lv);
+            else if (q[c] >= 1.)
+                *b[c] -= (1 << lv);
+        }
+    }
+    return bx + by * p->box_real_dim_x + bz * p->box_real_dim_x * p->box_real_dim_y;
+}
+
+/* poisson_error.c:290-347 for the head node (the only node of this build). */
+bool poisson_error(struct node *p, double *error, double error_total_pow2, int type)
+{
+    (void)error;
+    (void)error_total_pow2;
+    if (ensure())
+        return false;
+    if (p != *R.ptr_tree || type != 0)
+    {
+        printf("\nERROR (drop-in): poisson_error supports the head node (type 0) only\n");
+        return false;
+    }
+    int conv = 0;
+    if (qz_set_head_field(g_sim, QZ_FIELD_POT, p->ptr_pot) ||
+        qz_set_head_field(g_sim, QZ_FIELD_POT_OLD, p->ptr_pot_old) ||
+        qz_set_head_field(g_sim, QZ_FIELD_DENSITY, p->ptr_d) || qz_poisson_error(g_sim, &conv) ||
+        qz_get_head_field(g_sim, QZ_FIELD_POT_OLD, p->ptr_pot_old))
+    {
+        fail("poisson_error");
+        return false;
+    }
+    return conv != 0;
+}
+
+static int dense_order(void)
+{
+    const char *o = getenv("QZ_GS_ORDER");
+    return (o && !strcmp(o, "rb")) ? QZ_GS_REDBLACK : QZ_GS_LEX;
+}
+
+/* force_methods/multigrid.c:106-229 on caller arrays. */
+void multigrid(double *phi, const double *rho, int gridsize, int type_multigrid)
+{
+    if (!resolve())
+        return;
+    qz_config c;
+    fill_config(&c);
+    c.gs_order = dense_order();
+    c.precision = QZ_PREC_FP64;
+    if (*R.solver_pre > 1)
+    {
+        printf("\nERROR (drop-in): conjugate-gradient smoothing is not supported\n");
+        return;
+    }
+    if (qz_multigrid(&c, phi, rho, gridsize, type_multigrid))
+        fail("multigrid");
+}
+
+/* force_methods/gauss_saidel.c:29-55 */
+void gauss_saidel(double *phi, const double *rho, int gridsize, int iter_max)
+{
+    if (!resolve())
+        return;
+    if (qz_gauss_saidel(phi, rho, gridsize, iter_max, *R.w_sor_head, dense_order()))
+        fail("gauss_saidel");
+}
+
+/* force_methods/jacobi.c:29-82 */
+void jacobi(double *phi, const double *rho, int gridsize, int iter_max)
+{
+    if (!resolve())
+        return;
+    if (qz_jacobi(phi, rho, gridsize, iter_max, *R.w_sor_head))
+        fail("jacobi");
+}
+
+/* force_methods/conjugate_gradient.c:322-463: refinement-node solver, not in
+ * this build (head-only). */
+int conjugate_gradient(struct node *p)
+{
+    (void)p;
+    printf("\nERROR (drop-in): conjugate_gradient (refinement nodes) is not supported by this build\n");
+    return REF_FAILURE;
+}
+
+/* force_methods/conjugate_gradient_multigrid.c:29-176: not in this build. */
+void conjugate_gradient_multigrid(double *phi, const double *rho, int gridsize, int iters)
+{
+    (void)phi;
+    (void)rho;
+    (void)gridsize;
+    (void)iters;
+    printf("\nERROR (drop-in): conjugate-gradient smoothing is not supported by this build\n");
+}
+
+/* force_methods/multigrid2.c: never called by the reference; kept for linking. */
+void multigrid2(double *phi, double *rho, int type_multigrid)
+{
+    (void)phi;
+    (void)rho;
+    (void)type_multigrid;
+    printf("\nERROR (drop-in): multigrid2 is not supported by this build\n");
+}
+
+int qz_dropin_sync_from_host(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    return upload_all();
+}
+
+void *qz_dropin_context(void) { return g_sim; }

@@ -1,0 +1,193 @@
+// qz_internal.cuh -- device state and kernel declarations of libqzb200.
+//
+// Memory layout in HBM (one qz_sim):
+//   particles  SoA float64 x y z vx vy vz ax ay az m, length n (ID order)
+//   head grid  six float64 fields of D^3 points, D = 2^L + 3, index
+//              i + j*D + k*D*D (the reference's box grid, initialization.c:248-255);
+//              the multigrid finest level is the embedded (2^L+1)^3 solve grid
+//              at offset (1,1,1) -- no copy in/out per V-cycle.
+//   MG levels  coarse phi / rho of n_l^3 points, n_{l+1} = (n_l + 1) / 2, in
+//              float64 (and float32 for the mixed-precision form)
+//   deposit    sort keys / permutation (ping-pong), segment tables, per-cell
+//              CIC corner sums (8 float64 per occupied cell)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+
+#include "../../include/qz_b200.h"
+#include <utility>
+
+namespace qz {
+
+// Strided view of an n^3 multigrid level: point (i,j,k) at p[off + i + j*sy + k*sz].
+template <typename T>
+struct Grid {
+    T *p;
+    long off;
+    long sy;
+    long sz;
+    int n;
+};
+
+struct Level {
+    int n = 0;
+    double *phi = nullptr, *rho = nullptr;  // FP64 correction / right-hand side
+    float *phif = nullptr, *rhof = nullptr; // FP32 hierarchy (mixed precision)
+    double *scr = nullptr;                  // Jacobi ping-pong buffers (smoother 1)
+    float *scrf = nullptr;
+};
+
+// Device-side flag words (int).
+enum Flag {
+    F_RATIO_FAIL = 0, // ratio test |phi/phi_old - 1| > tol2 somewhere
+    F_CONVERGED = 1,  // result of the last convergence check
+    F_ERROR = 2,      // bitmask of bounds errors seen by kernels
+    F_NSEG = 3,       // number of occupied cells (deposit segments)
+    F_RESID_FAIL = 4, // method-1 pointwise residual failure
+    F_COUNT = 8
+};
+enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2 };
+
+struct Sort {
+    // Stable LSD radix sort of (uint32 key, int32 value) pairs.
+    unsigned *k0 = nullptr, *k1 = nullptr;
+    int *v0 = nullptr, *v1 = nullptr;
+    int *hist = nullptr; // 256 * tiles
+    long cap = 0;
+    long tiles_cap = 0;
+};
+
+} // namespace qz
+
+struct qz_sim {
+    qz_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    long n = 0, cap = 0;
+    double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    double *ax = nullptr, *ay = nullptr, *az = nullptr, *m = nullptr;
+
+    int L = 0;
+    long D = 0, gpts = 0;
+    double *pot = nullptr, *pot_old = nullptr, *d = nullptr, *gax = nullptr, *gay = nullptr,
+           *gaz = nullptr;
+    // mixed precision: FP64 residual of the fine grid stored as FP32 rhs, FP32 correction
+    float *rf = nullptr, *ef = nullptr;
+    std::vector<qz::Level> levels; // levels[0].n = 2^L + 1 (embedded), levels[l>0] owned
+    qz::Grid<double> fine_phi{}, fine_rho{}; // level-0 views (head solve grid)
+
+    // deposit scratch
+    qz::Sort sort;
+    int *seg_head = nullptr;  // n: 1 at first particle of a cell run
+    int *seg_id = nullptr;    // n: exclusive scan of seg_head
+    int *seg_start = nullptr; // n + 1
+    int *seg_cell = nullptr;  // n
+    int *cell_seg = nullptr;  // B^3 cells: segment of the cell or -1
+    double *cell_sums = nullptr; // 8 * n
+    int *scan_tmp = nullptr;
+    long scan_tmp_cap = 0;
+
+    double *red = nullptr; // reduction partials
+    int red_blocks = 0;
+    int *flags = nullptr;  // device flag words
+    int *h_flags = nullptr; // pinned mirror
+    double *h_red = nullptr; // pinned scalar readback
+    double *h_stage = nullptr; // pinned staging for host copies
+    size_t h_stage_bytes = 0;
+
+    qz_stats stats{};
+    bool forces_ready = false;
+
+    // per-kernel-category timing (qz_profile_*): begin/end events per launch
+    bool prof = false;
+    struct ProfRec {
+        int cat;
+        double bytes;
+        cudaEvent_t b, e;
+    };
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    long long prof_launches[QZ_PROF_CATEGORIES] = {};
+    double prof_ms[QZ_PROF_CATEGORIES] = {};
+    double prof_bytes[QZ_PROF_CATEGORIES] = {};
+};
+
+namespace qz {
+
+// ---- launch accounting and errors ------------------------------------------
+void set_error(const char *fmt, ...);
+bool check_cuda(cudaError_t e, const char *what);
+#define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
+
+cudaEvent_t prof_event(qz_sim *s);
+void prof_collect(qz_sim *s);
+
+// Launches kernel k on the library stream; counts it, and when profiling is
+// on brackets it with events and books `bytes` algorithmic bytes to `cat`.
+template <typename... KArgs, typename... Args>
+inline void launch(qz_sim *s, int cat, double bytes, void (*k)(KArgs...), dim3 g, dim3 b,
+                   Args &&...args)
+{
+    cudaEvent_t eb = nullptr, ee = nullptr;
+    if (s->prof)
+    {
+        eb = prof_event(s);
+        ee = prof_event(s);
+        cudaEventRecord(eb, s->stream);
+    }
+    k<<<g, b, 0, s->stream>>>(std::forward<Args>(args)...);
+    s->stats.kernel_launches++;
+    if (s->prof)
+    {
+        cudaEventRecord(ee, s->stream);
+        s->prof_pending.push_back({cat, bytes, eb, ee});
+    }
+}
+
+// ---- kernels-side entry points (host wrappers) ------------------------------
+int head_initial(qz_sim *s);
+int deposit_head(qz_sim *s);
+int grid_accel_head(qz_sim *s);
+int gather_head(qz_sim *s);
+int kick_drift(qz_sim *s, double dt);
+int kick(qz_sim *s, double dt);
+
+int potential_head(qz_sim *s);
+int poisson_error_head(qz_sim *s, int *converged);
+int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters);
+int vcycle(qz_sim *s, int level, int type);
+
+int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **vals_out);
+int scan_exclusive(qz_sim *s, const int *in, int *out, long n);
+
+// grid views
+inline Grid<double> head_view(qz_sim *s, double *field)
+{
+    Grid<double> g;
+    g.p = field;
+    g.off = 1 + s->D + s->D * s->D;
+    g.sy = s->D;
+    g.sz = s->D * s->D;
+    g.n = (1 << s->L) + 1;
+    return g;
+}
+template <typename T>
+inline Grid<T> dense_view(T *p, int n)
+{
+    Grid<T> g;
+    g.p = p;
+    g.off = 0;
+    g.sy = n;
+    g.sz = (long)n * n;
+    g.n = n;
+    return g;
+}
+
+inline int blocks_for(long n, int threads)
+{
+    long b = (n + threads - 1) / threads;
+    return (int)(b < 1 ? 1 : b);
+}
+
+} // namespace qz

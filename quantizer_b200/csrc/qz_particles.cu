@@ -1,0 +1,435 @@
+// qz_particles.cu -- particle-side kernels of the head-node step:
+//   CIC deposit      (grid_density.c:35-111)      sort + segmented reduce + gather
+//   CIC gather       (particle_acceleration.c:33-132)
+//   kick-drift       (particle_updating.c:39-207)
+//   kick             (particle_updating.c:2677-2688)
+//   box index        (ptcl_idx_to_box_idx.c:30-139)
+//   head boundary    (initial_potential_and_acceleration_head.c:297-334)
+//
+// Floating-point expressions keep the reference's operand order; the library
+// is built with -fmad=false, so products and sums round exactly as the
+// reference's x86-64 FP64 code (no contraction).  The deposit differs from the
+// reference only in the order in which particle contributions are summed at a
+// grid point (cell by cell instead of particle index order), which is
+// deterministic from run to run.
+#include "qz_internal.cuh"
+
+namespace qz {
+
+#define QZ_PI_D 3.14159265358979323846
+
+// ---- analytic head boundary ---------------------------------------------------
+__global__ void k_initial_head(int L, long D, double G, double M, double *__restrict__ pot,
+                               double *__restrict__ ax, double *__restrict__ ay,
+                               double *__restrict__ az)
+{
+    const int B = (1 << L) + 2; // box cells per side; points 0..B-1 are filled
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    long total = (long)B * B * B;
+    if (t >= total)
+        return;
+    int i = (int)(t % B), j = (int)((t / B) % B), k = (int)(t / ((long)B * B));
+    const double H = 1.0 / (1 << L);
+    double ai = (i - 1) * H - 0.5, aj = (j - 1) * H - 0.5, ak = (k - 1) * H - 0.5;
+    double dist = ai * ai + aj * aj + ak * ak;
+    dist = sqrt(dist);
+    if (dist == 0.0)
+        dist = 1.0 / (1 << L) * 1.0e-3;
+    long g = i + (long)j * D + (long)k * D * D;
+    double coeff = -G * M / (dist * dist * dist);
+    pot[g] = -G * M / dist;
+    ax[g] = coeff * ai;
+    ay[g] = coeff * aj;
+    az[g] = coeff * ak;
+}
+
+int head_initial(qz_sim *s)
+{
+    size_t bytes = (size_t)s->gpts * sizeof(double);
+    cudaMemsetAsync(s->pot, 0, bytes, s->stream);
+    cudaMemsetAsync(s->gax, 0, bytes, s->stream);
+    cudaMemsetAsync(s->gay, 0, bytes, s->stream);
+    cudaMemsetAsync(s->gaz, 0, bytes, s->stream);
+    long B = (1L << s->L) + 2;
+    launch(s, QZ_PROF_OTHER, 32.0 * B * B * B, k_initial_head, dim3(blocks_for(B * B * B, 256)), dim3(256), s->L, s->D, s->cfg.G, s->cfg.total_mass, s->pot, s->gax, s->gay, s->gaz);
+    return check_cuda(cudaGetLastError(), "initial head") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- deposit --------------------------------------------------------------------
+// Cell key of a particle in the head box: box-cell coordinates floor(x 2^L) + 1
+// (box_ts = -1), linear on B = 2^L + 2 cells per side.
+__device__ __forceinline__ int cell_coord(double x, int L, int *err)
+{
+    int f = (int)(x * (1 << L));
+    if (!(x >= 0.0) || f > (1 << L)) // outside [0, 1] or NaN: clamp and flag
+    {
+        *err |= E_PTCL_OUTSIDE;
+        f = x > 0.5 ? (1 << L) : 0;
+    }
+    return f + 1;
+}
+
+__global__ void k_head_keys(long n, int L, const double *__restrict__ x,
+                            const double *__restrict__ y, const double *__restrict__ z,
+                            unsigned *__restrict__ keys, int *__restrict__ vals,
+                            int *__restrict__ flags)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned B = (1u << L) + 2u;
+    int err = 0;
+    unsigned bx = cell_coord(x[i], L, &err), by = cell_coord(y[i], L, &err),
+             bz = cell_coord(z[i], L, &err);
+    keys[i] = bx + by * B + bz * B * B;
+    vals[i] = (int)i;
+    if (err)
+        atomicOr(&flags[F_ERROR], err);
+}
+
+__global__ void k_seg_heads(long n, const unsigned *__restrict__ k, int *__restrict__ head)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    head[i] = (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_seg_fill(long n, const unsigned *__restrict__ k, const int *__restrict__ head,
+                           const int *__restrict__ sid, int *__restrict__ seg_start,
+                           int *__restrict__ seg_cell, int *__restrict__ cell_seg,
+                           int *__restrict__ flags)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    if (head[i])
+    {
+        int sgm = sid[i];
+        seg_start[sgm] = (int)i;
+        seg_cell[sgm] = (int)k[i];
+        cell_seg[k[i]] = sgm;
+    }
+    if (i == n - 1)
+    {
+        int nseg = sid[i] + head[i];
+        seg_start[nseg] = (int)n;
+        flags[F_NSEG] = nseg;
+    }
+}
+
+// One warp per occupied cell: the 8 CIC corner sums of coeff * m * w over the
+// cell's particles (lane-strided partial sums, then a fixed xor-shuffle tree).
+__global__ void k_seg_reduce(int L, double coeff, const int *__restrict__ perm,
+                             const int *__restrict__ seg_start, const int *__restrict__ flags,
+                             const double *__restrict__ x, const double *__restrict__ y,
+                             const double *__restrict__ z, const double *__restrict__ m,
+                             double *__restrict__ cs)
+{
+    const int lane = threadIdx.x & 31;
+    const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    const int nseg = flags[F_NSEG];
+    const double scale = (double)(1 << L);
+    for (long sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const int b = seg_start[sg], e = seg_start[sg + 1];
+        double acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            acc[c] = 0.0;
+        for (int q = b + lane; q < e; q += 32)
+        {
+            const int i = perm[q];
+            double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
+            int fx = (int)px, fy = (int)py, fz = (int)pz;
+            double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+            double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+            double cm = coeff * m[i];
+            acc[0] += cm * (wx2 * wy2 * wz2);
+            acc[1] += cm * (wx1 * wy2 * wz2);
+            acc[2] += cm * (wx2 * wy1 * wz2);
+            acc[3] += cm * (wx1 * wy1 * wz2);
+            acc[4] += cm * (wx2 * wy2 * wz1);
+            acc[5] += cm * (wx1 * wy2 * wz1);
+            acc[6] += cm * (wx2 * wy1 * wz1);
+            acc[7] += cm * (wx1 * wy1 * wz1);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+        {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1)
+                v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc[c] = v;
+        }
+        if (lane < 8)
+        {
+            double v = acc[0];
+#pragma unroll
+            for (int c = 1; c < 8; c++)
+                if (lane == c)
+                    v = acc[c];
+            cs[sg * 8 + lane] = v;
+        }
+    }
+}
+
+// Each grid point sums the corner contributions of its (up to) 8 adjacent
+// occupied cells in a fixed order.
+__global__ void k_point_gather(int L, long D, const int *__restrict__ cell_seg,
+                               const double *__restrict__ cs, double *__restrict__ d)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= D * D * D)
+        return;
+    const long B = D - 1;
+    int gx = (int)(t % D), gy = (int)((t / D) % D), gz = (int)(t / (D * D));
+    double acc = 0.0;
+    for (int c = 0; c < 2; c++)
+    {
+        int cz = gz - 1 + c;
+        if (cz < 0 || cz >= B)
+            continue;
+        for (int b = 0; b < 2; b++)
+        {
+            int cy = gy - 1 + b;
+            if (cy < 0 || cy >= B)
+                continue;
+            for (int a = 0; a < 2; a++)
+            {
+                int cx = gx - 1 + a;
+                if (cx < 0 || cx >= B)
+                    continue;
+                int sg = cell_seg[cx + cy * B + (long)cz * B * B];
+                if (sg >= 0)
+                    acc += cs[(long)sg * 8 + (1 - a) + 2 * (1 - b) + 4 * (1 - c)];
+            }
+        }
+    }
+    d[t] = acc;
+}
+
+int deposit_head(qz_sim *s)
+{
+    const long n = s->n;
+    const int L = s->L;
+    const long B = (1L << L) + 2;
+    if (n == 0)
+        return cudaMemsetAsync(s->d, 0, s->gpts * sizeof(double), s->stream) == cudaSuccess
+                   ? QZ_SUCCESS
+                   : QZ_FAILURE;
+    launch(s, QZ_PROF_DEPOSIT, 32.0 * n, k_head_keys, dim3(blocks_for(n, 256)), dim3(256), n, L, s->x, s->y, s->z, s->sort.k0, s->sort.v0, s->flags);
+    int bits = 1;
+    while ((1L << bits) < B * B * B)
+        bits++;
+    unsigned *ks;
+    int *perm;
+    if (radix_sort_pairs(s, n, bits, &ks, &perm))
+        return QZ_FAILURE;
+    launch(s, QZ_PROF_DEPOSIT, 8.0 * n, k_seg_heads, dim3(blocks_for(n, 256)), dim3(256), n, ks, s->seg_head);
+    if (scan_exclusive(s, s->seg_head, s->seg_id, n))
+        return QZ_FAILURE;
+    cudaMemsetAsync(s->cell_seg, 0xFF, (size_t)(B * B * B) * sizeof(int), s->stream);
+    launch(s, QZ_PROF_DEPOSIT, 12.0 * n, k_seg_fill, dim3(blocks_for(n, 256)), dim3(256), n, ks, s->seg_head, s->seg_id, s->seg_start, s->seg_cell, s->cell_seg, s->flags);
+    const double H = 1.0 / (1 << L);
+    const double coeff = 4.0 * s->cfg.G * QZ_PI_D / (H * H * H);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    long want_warps = n; // upper bound on segments
+    long blocks = (want_warps * 32 + 255) / 256;
+    long max_blocks = (long)sms * 16;
+    if (blocks > max_blocks)
+        blocks = max_blocks;
+    launch(s, QZ_PROF_DEPOSIT, 36.0 * n, k_seg_reduce, dim3((int)blocks), dim3(256), L, coeff, perm, s->seg_start, s->flags, s->x, s->y, s->z, s->m, s->cell_sums);
+    launch(s, QZ_PROF_DEPOSIT, 12.0 * s->gpts, k_point_gather, dim3(blocks_for(s->gpts, 256)), dim3(256), L, s->D, s->cell_seg, s->cell_sums, s->d);
+    return check_cuda(cudaGetLastError(), "deposit") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- grid acceleration (3-point) ----------------------------------------------
+__global__ void k_grid_accel3(int L, long D, const double *__restrict__ pot,
+                              double *__restrict__ ax, double *__restrict__ ay,
+                              double *__restrict__ az)
+{
+    const int m = (1 << L) - 1; // interior points per axis: box coords 2..2^L
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)m * m * m)
+        return;
+    int i = 2 + (int)(t % m), j = 2 + (int)((t / m) % m), k = 2 + (int)(t / ((long)m * m));
+    const long D2 = D * D;
+    long g = i + j * D + k * D2;
+    const double H = 1.0 / (1 << L);
+    const double o2h = 1.0 / (2.0 * H);
+    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
+    ay[g] = o2h * (pot[g - D] - pot[g + D]);
+    az[g] = o2h * (pot[g - D2] - pot[g + D2]);
+}
+
+int grid_accel_head(qz_sim *s)
+{
+    long m = (1L << s->L) - 1;
+    if (m <= 0)
+        return QZ_SUCCESS;
+    launch(s, QZ_PROF_GRADIENT, 32.0 * m * m * m, k_grid_accel3, dim3(blocks_for(m * m * m, 256)), dim3(256), s->L, s->D, s->pot, s->gax, s->gay, s->gaz);
+    return check_cuda(cudaGetLastError(), "grid accel") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- CIC gather ---------------------------------------------------------------
+__global__ void k_gather_head(long n, int L, long D, const double *__restrict__ x,
+                              const double *__restrict__ y, const double *__restrict__ z,
+                              const double *__restrict__ gx, const double *__restrict__ gy,
+                              const double *__restrict__ gz, double *__restrict__ pax,
+                              double *__restrict__ pay, double *__restrict__ paz,
+                              int *__restrict__ flags)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double scale = (double)(1 << L);
+    double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
+    int fx = (int)px, fy = (int)py, fz = (int)pz;
+    if (!(px >= 0.0 && py >= 0.0 && pz >= 0.0) || fx > (1 << L) || fy > (1 << L) ||
+        fz > (1 << L))
+    {
+        atomicOr(&flags[F_ERROR], E_PTCL_OUTSIDE);
+        return;
+    }
+    double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+    double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+    double w[8];
+    w[0] = wx2 * wy2 * wz2;
+    w[1] = wx1 * wy2 * wz2;
+    w[2] = wx2 * wy1 * wz2;
+    w[3] = wx1 * wy1 * wz2;
+    w[4] = wx2 * wy2 * wz1;
+    w[5] = wx1 * wy2 * wz1;
+    w[6] = wx2 * wy1 * wz1;
+    w[7] = wx1 * wy1 * wz1;
+    const long D2 = D * D;
+    long g = (fx + 1) + (long)(fy + 1) * D + (long)(fz + 1) * D2;
+    double ax = pax[i], ay = pay[i], az = paz[i];
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int ii = 0; ii < 2; ii++)
+            {
+                int a = ii + 2 * jj + 4 * kk;
+                long q = g + ii + jj * D + kk * D2;
+                ax += gx[q] * w[a];
+                ay += gy[q] * w[a];
+                az += gz[q] * w[a];
+            }
+    pax[i] = ax;
+    pay[i] = ay;
+    paz[i] = az;
+}
+
+int gather_head(qz_sim *s)
+{
+    if (s->n == 0)
+        return QZ_SUCCESS;
+    launch(s, QZ_PROF_GATHER, 72.0 * s->n + 24.0 * s->gpts, k_gather_head, dim3(blocks_for(s->n, 256)), dim3(256), s->n, s->L, s->D, s->x, s->y, s->z, s->gax, s->gay, s->gaz, s->ax, s->ay, s->az, s->flags);
+    return check_cuda(cudaGetLastError(), "gather") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- leapfrog ---------------------------------------------------------------------
+__device__ __forceinline__ void boundary(int bdry, double &x, double &v, double &a)
+{
+    if (x < 0.0 || x >= 1.0)
+    {
+        if (bdry == 0)
+            x = x >= 1.0 ? x - 1.0 : 1.0 + x;
+        else
+        {
+            x = x >= 1.0 ? 2.0 - x : -x;
+            v *= -1.0;
+            a *= -1.0;
+        }
+    }
+}
+
+__global__ void k_kick_drift(long n, double dt, int bdry, double *__restrict__ x,
+                             double *__restrict__ y, double *__restrict__ z,
+                             double *__restrict__ vx, double *__restrict__ vy,
+                             double *__restrict__ vz, double *__restrict__ ax,
+                             double *__restrict__ ay, double *__restrict__ az)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double px = x[i], py = y[i], pz = z[i];
+    double qx = vx[i], qy = vy[i], qz = vz[i];
+    double gx = ax[i], gy = ay[i], gz = az[i];
+    qx += gx * dt * 0.5;
+    qy += gy * dt * 0.5;
+    qz += gz * dt * 0.5;
+    px += qx * dt;
+    py += qy * dt;
+    pz += qz * dt;
+    boundary(bdry, px, qx, gx);
+    boundary(bdry, py, qy, gy);
+    boundary(bdry, pz, qz, gz);
+    x[i] = px;
+    y[i] = py;
+    z[i] = pz;
+    vx[i] = qx;
+    vy[i] = qy;
+    vz[i] = qz;
+    ax[i] = gx;
+    ay[i] = gy;
+    az[i] = gz;
+}
+
+int kick_drift(qz_sim *s, double dt)
+{
+    if (s->n == 0)
+        return QZ_SUCCESS;
+    launch(s, QZ_PROF_LEAPFROG, 144.0 * s->n, k_kick_drift, dim3(blocks_for(s->n, 256)), dim3(256), s->n, dt, s->cfg.bdry, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az);
+    return check_cuda(cudaGetLastError(), "kick drift") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+__global__ void k_kick(long n, double dt, double *__restrict__ vx, double *__restrict__ vy,
+                       double *__restrict__ vz, const double *__restrict__ ax,
+                       const double *__restrict__ ay, const double *__restrict__ az)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    vx[i] += ax[i] * dt * 0.5;
+    vy[i] += ay[i] * dt * 0.5;
+    vz[i] += az[i] * dt * 0.5;
+}
+
+int kick(qz_sim *s, double dt)
+{
+    if (s->n == 0)
+        return QZ_SUCCESS;
+    launch(s, QZ_PROF_LEAPFROG, 72.0 * s->n, k_kick, dim3(blocks_for(s->n, 256)), dim3(256), s->n, dt, s->vx, s->vy, s->vz, s->ax, s->ay, s->az);
+    return check_cuda(cudaGetLastError(), "kick") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- particle -> box index ----------------------------------------------------------
+__global__ void k_box_idx(long n, int lv, int tsx, int tsy, int tsz, int dimx, int dimy,
+                          const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, int *__restrict__ out)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double scale = (double)(1 << lv);
+    double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
+    int fx = px < 0 ? -1 : (int)px;
+    int fy = py < 0 ? -1 : (int)py;
+    int fz = pz < 0 ? -1 : (int)pz;
+    out[i] = (fx - tsx) + (fy - tsy) * dimx + (fz - tsz) * dimx * dimy;
+}
+
+void launch_box_idx(cudaStream_t st, long n, int lv, int tsx, int tsy, int tsz, int dimx,
+                    int dimy, const double *x, const double *y, const double *z, int *out)
+{
+    k_box_idx<<<blocks_for(n, 256), 256, 0, st>>>(n, lv, tsx, tsy, tsz, dimx, dimy, x, y, z, out);
+}
+
+} // namespace qz

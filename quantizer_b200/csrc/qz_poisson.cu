@@ -1,0 +1,563 @@
+// qz_poisson.cu -- head-node Poisson solve (potential_head_node.c:32-179) by
+// multigrid cycles (force_methods/multigrid.c:106-229) on the embedded solve
+// grid of the head fields, with the convergence test of poisson_error.c:36-133.
+//
+// Kernels (FP64, and FP32 instances for the mixed-precision form):
+//   k_gs_rb          one colour of a red-black Gauss-Seidel sweep
+//   k_gs_lex_cta     lexicographic Gauss-Seidel in the reference's order, by
+//                    i+j+k wavefronts inside one CTA (parity mode)
+//   k_jacobi         weighted Jacobi ping-pong sweep (jacobi.c:29-82)
+//   k_resid_restrict residual at the even fine points only, injected into the
+//                    coarse right-hand side (multigrid.c:140-150 + 29-49: the
+//                    reference computes the residual everywhere but reads only
+//                    the injected points)
+//   k_prolong_add    trilinear prolongation written as a gather over the coarse
+//                    points in the reference's scatter order, fused with
+//                    phi += dphi (multigrid.c:51-104, 199-209)
+//   k_check_*        ratio test + residual norm, fixed-tree deterministic sums
+#include "qz_internal.cuh"
+
+namespace qz {
+
+#define QZ_PI_D 3.14159265358979323846
+
+template <typename T>
+__device__ __forceinline__ T gs_point(const T *__restrict__ rho, T *__restrict__ phi, long g,
+                                      long sy, long sz, T H2, T w)
+{
+    const T one_sixth = (T)(1.0 / 6.0);
+    T a = one_sixth * (-H2 * rho[g] + phi[g + 1] + phi[g - 1] + phi[g + sy] + phi[g - sy] +
+                       phi[g + sz] + phi[g - sz]);
+    return w * a + ((T)1.0 - w) * phi[g];
+}
+
+template <typename T>
+__global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
+{
+    const int m = phi.n - 2;
+    const int half = (m + 1) / 2;
+    int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y;
+    int k = 1 + blockIdx.z;
+    if (ti >= half)
+        return;
+    int i0 = (((1 + j + k) & 1) == color) ? 1 : 2;
+    int i = i0 + 2 * ti;
+    if (i > m)
+        return;
+    long gp = phi.off + i + j * phi.sy + k * phi.sz;
+    long gr = rho.off + i + j * rho.sy + k * rho.sz;
+    const T one_sixth = (T)(1.0 / 6.0);
+    T *p = phi.p;
+    T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
+                       p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
+    p[gp] = w * a + ((T)1.0 - w) * p[gp];
+}
+
+// Lexicographic sweeps (k slowest, i fastest) reproduced exactly: the update
+// of point (i,j,k) reads new values at i-1, j-1, k-1 and old values at i+1,
+// j+1, k+1, so all points with the same i+j+k are independent.
+template <typename T>
+__global__ void k_gs_lex_cta(Grid<T> phi, Grid<T> rho, int iters, T H2, T w)
+{
+    const int m = phi.n - 2;
+    const long pairs = (long)m * m;
+    const T one_sixth = (T)(1.0 / 6.0);
+    T *p = phi.p;
+    for (int it = 0; it < iters; it++)
+    {
+        for (int sidx = 3; sidx <= 3 * m; sidx++)
+        {
+            for (long q = threadIdx.x; q < pairs; q += blockDim.x)
+            {
+                int j = 1 + (int)(q % m), k = 1 + (int)(q / m);
+                int i = sidx - j - k;
+                if (i < 1 || i > m)
+                    continue;
+                long gp = phi.off + i + j * phi.sy + k * phi.sz;
+                long gr = rho.off + i + j * rho.sy + k * rho.sz;
+                T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
+                                   p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
+                p[gp] = w * a + ((T)1.0 - w) * p[gp];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_jacobi(Grid<T> oldp, Grid<T> newp, Grid<T> rho, T C, T w)
+{
+    const int m = oldp.n - 2;
+    int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y;
+    int k = 1 + blockIdx.z;
+    if (i > m)
+        return;
+    long go = oldp.off + i + j * oldp.sy + k * oldp.sz;
+    long gn = newp.off + i + j * newp.sy + k * newp.sz;
+    long gr = rho.off + i + j * rho.sy + k * rho.sz;
+    const T one_sixth = (T)(1.0 / 6.0);
+    const T *o = oldp.p;
+    T a = one_sixth * (C * rho.p[gr] + o[go + 1] + o[go - 1] + o[go + oldp.sy] + o[go - oldp.sy] +
+                       o[go + oldp.sz] + o[go - oldp.sz]);
+    newp.p[gn] = w * a + ((T)1.0 - w) * newp.p[gn];
+}
+
+template <typename T>
+__global__ void k_copy_grid(Grid<T> dst, Grid<T> src)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i >= src.n)
+        return;
+    dst.p[dst.off + i + j * dst.sy + k * dst.sz] = src.p[src.off + i + j * src.sy + k * src.sz];
+}
+
+// rho_c(l) = rho(2l) + ooh2 * (6 phi(2l) - sum of 6 neighbours) at the coarse
+// interior points; the coarse boundary stays zero.
+template <typename T>
+__global__ void k_resid_restrict(Grid<T> phi, Grid<T> rho, Grid<T> rc, T ooh2)
+{
+    const int mc = rc.n - 2;
+    int lx = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int ly = 1 + blockIdx.y;
+    int lz = 1 + blockIdx.z;
+    if (lx > mc)
+        return;
+    long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
+    long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
+    const T *p = phi.p;
+    T r = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
+                              p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
+    rc.p[rc.off + lx + ly * rc.sy + lz * rc.sz] = r;
+}
+
+// phi(fine interior) += sum over contributing interior coarse points, in the
+// coarse lexicographic order of the reference's scatter loop, of w * dphic.
+template <typename T>
+__global__ void k_prolong_add(Grid<T> phi, Grid<T> c)
+{
+    const int m = phi.n - 2;
+    const int mc = c.n - 2;
+    int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y;
+    int k = 1 + blockIdx.z;
+    if (i > m)
+        return;
+    int cx0, cx1, cy0, cy1, cz0, cz1;
+    T wx, wy, wz;
+    if (i & 1) { cx0 = (i - 1) >> 1; cx1 = cx0 + 1; wx = (T)0.5; } else { cx0 = cx1 = i >> 1; wx = (T)1; }
+    if (j & 1) { cy0 = (j - 1) >> 1; cy1 = cy0 + 1; wy = (T)0.5; } else { cy0 = cy1 = j >> 1; wy = (T)1; }
+    if (k & 1) { cz0 = (k - 1) >> 1; cz1 = cz0 + 1; wz = (T)0.5; } else { cz0 = cz1 = k >> 1; wz = (T)1; }
+    T acc;
+    if (!(i & 1) && !(j & 1) && !(k & 1))
+        acc = c.p[c.off + cx0 + cy0 * c.sy + cz0 * c.sz];
+    else
+    {
+        const T wgt = wx * wy * wz;
+        acc = (T)0;
+        for (int cz = cz0; cz <= cz1; cz++)
+        {
+            if (cz < 1 || cz > mc)
+                continue;
+            for (int cy = cy0; cy <= cy1; cy++)
+            {
+                if (cy < 1 || cy > mc)
+                    continue;
+                for (int cx = cx0; cx <= cx1; cx++)
+                {
+                    if (cx < 1 || cx > mc)
+                        continue;
+                    acc += wgt * c.p[c.off + cx + cy * c.sy + cz * c.sz];
+                }
+            }
+        }
+    }
+    phi.p[phi.off + i + j * phi.sy + k * phi.sz] += acc;
+}
+
+// ---- host-side multigrid -----------------------------------------------------
+template <typename T>
+static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scratch)
+{
+    const qz_config &c = s->cfg;
+    const int n = phi.n;
+    const int m = n - 2;
+    if (m <= 0 || iters <= 0)
+        return QZ_SUCCESS;
+    if (c.smoother == 0)
+    {
+        T H2 = (T)((1.0 / (n - 1)) * (1.0 / (n - 1)));
+        T w = (T)c.w_sor;
+        if (c.gs_order == QZ_GS_LEX)
+        {
+            launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m * iters, k_gs_lex_cta<T>, dim3(1), dim3(1024), phi, rho, iters, H2, w);
+        }
+        else
+        {
+            int half = (m + 1) / 2;
+            int tx = half < 128 ? ((half + 31) / 32) * 32 : 128;
+            dim3 grid((half + tx - 1) / tx, m, m);
+            for (int it = 0; it < iters; it++)
+                for (int color = 0; color < 2; color++)
+                {
+                    launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 1.5 * m * m * m, k_gs_rb<T>, dim3(grid), dim3(tx), phi, rho, color, H2, w);
+                }
+        }
+    }
+    else if (c.smoother == 1)
+    {
+        // jacobi.c:62-82: ping-pong through a copy; odd counts run one more sweep
+        T C = (T)(-(1.0 / (n - 1)) * (1.0 / (n - 1)));
+        T w = (T)c.w_sor;
+        int tx = m < 128 ? ((m + 31) / 32) * 32 : 128;
+        dim3 grid((m + tx - 1) / tx, m, m);
+        dim3 gfull((n + tx - 1) / tx, n, n);
+        launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 2.0 * n * n * n, k_copy_grid<T>, dim3(gfull), dim3(tx), scratch, phi);
+        int sweeps = iters % 2 == 0 ? iters : iters + 1;
+        Grid<T> a = iters % 2 == 0 ? phi : scratch;
+        Grid<T> b = iters % 2 == 0 ? scratch : phi;
+        for (int it = 0; it < sweeps; it++)
+        {
+            launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m, k_jacobi<T>, dim3(grid), dim3(tx), a, b, rho, C, w);
+            Grid<T> t = a;
+            a = b;
+            b = t;
+        }
+    }
+    else
+    {
+        set_error("smoother %d is not supported", c.smoother);
+        return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+template <typename T>
+struct LevelViews {
+    static Grid<T> phi(qz_sim *s, int l);
+    static Grid<T> rho(qz_sim *s, int l);
+    static Grid<T> scratch(qz_sim *s, int l);
+};
+
+// Level 0 of the FP64 hierarchy is the fine grid view of the context (the head
+// solve grid embedded in the head fields, or a dense array for the array-level
+// entry points); level 0 of the FP32 hierarchy is the fine correction /
+// residual pair ef / rf (dense n0^3).
+template <>
+Grid<double> LevelViews<double>::phi(qz_sim *s, int l)
+{
+    return l == 0 ? s->fine_phi : dense_view(s->levels[l].phi, s->levels[l].n);
+}
+template <>
+Grid<double> LevelViews<double>::rho(qz_sim *s, int l)
+{
+    return l == 0 ? s->fine_rho : dense_view(s->levels[l].rho, s->levels[l].n);
+}
+template <>
+Grid<double> LevelViews<double>::scratch(qz_sim *s, int l)
+{
+    return dense_view(s->levels[l].scr, s->levels[l].n);
+}
+template <>
+Grid<float> LevelViews<float>::phi(qz_sim *s, int l)
+{
+    return l == 0 ? dense_view(s->ef, s->levels[0].n) : dense_view(s->levels[l].phif, s->levels[l].n);
+}
+template <>
+Grid<float> LevelViews<float>::rho(qz_sim *s, int l)
+{
+    return l == 0 ? dense_view(s->rf, s->levels[0].n) : dense_view(s->levels[l].rhof, s->levels[l].n);
+}
+template <>
+Grid<float> LevelViews<float>::scratch(qz_sim *s, int l)
+{
+    return dense_view(s->levels[l].scrf, s->levels[l].n);
+}
+
+template <typename T>
+static int vcycle_t(qz_sim *s, int l, int type)
+{
+    const qz_config &c = s->cfg;
+    Grid<T> phi = LevelViews<T>::phi(s, l), rho = LevelViews<T>::rho(s, l);
+    const int n = phi.n;
+    const int nc = (n + 1) / 2;
+    Grid<T> scr{};
+    if (c.smoother == 1)
+        scr = LevelViews<T>::scratch(s, l);
+    if (smooth_t<T>(s, phi, rho, c.n_pre, scr))
+        return QZ_FAILURE;
+    if (nc < 4)
+    {
+        // multigrid.c:158-173: the coarse correction stays zero; the fine grid
+        // gets n_coarse more smoothing sweeps instead.
+        if (smooth_t<T>(s, phi, rho, c.n_coarse, scr))
+            return QZ_FAILURE;
+    }
+    else
+    {
+        if (l + 1 >= (int)s->levels.size())
+        {
+            set_error("multigrid hierarchy too shallow");
+            return QZ_FAILURE;
+        }
+        Grid<T> cphi = LevelViews<T>::phi(s, l + 1), crho = LevelViews<T>::rho(s, l + 1);
+        size_t cbytes = (size_t)nc * nc * nc * sizeof(T);
+        cudaMemsetAsync(cphi.p, 0, cbytes, s->stream);
+        int mc = nc - 2;
+        int tx = mc < 128 ? ((mc + 31) / 32) * 32 : 128;
+        dim3 g((mc + tx - 1) / tx, mc, mc);
+        T ooh2 = (T)(double)((n - 1) * (n - 1));
+        launch(s, QZ_PROF_RESTRICT, (double)sizeof(T) * 9.0 * mc * mc * mc, k_resid_restrict<T>, dim3(g), dim3(tx), phi, rho, crho, ooh2);
+        if (type == 0)
+        {
+            if (vcycle_t<T>(s, l + 1, 0))
+                return QZ_FAILURE;
+        }
+        else if (type == 1)
+        {
+            if (vcycle_t<T>(s, l + 1, 1) || vcycle_t<T>(s, l + 1, 0))
+                return QZ_FAILURE;
+        }
+        else
+        {
+            if (vcycle_t<T>(s, l + 1, 2) || vcycle_t<T>(s, l + 1, 2))
+                return QZ_FAILURE;
+        }
+        int m = n - 2;
+        int tf = m < 128 ? ((m + 31) / 32) * 32 : 128;
+        dim3 gf((m + tf - 1) / tf, m, m);
+        launch(s, QZ_PROF_PROLONG, (double)sizeof(T) * 2.125 * m * m * m, k_prolong_add<T>, dim3(gf), dim3(tf), phi, cphi);
+    }
+    if (smooth_t<T>(s, phi, rho, c.n_post, scr))
+        return QZ_FAILURE;
+    return check_cuda(cudaGetLastError(), "multigrid cycle") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int vcycle(qz_sim *s, int level, int type) { return vcycle_t<double>(s, level, type); }
+
+int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters)
+{
+    Grid<double> scr{};
+    if (s->cfg.smoother == 1)
+        scr = LevelViews<double>::scratch(s, 0);
+    return smooth_t<double>(s, phi, rho, iters, scr);
+}
+
+// ---- mixed precision: FP64 defect, FP32 cycles ---------------------------------
+// r32 = (float)(rho + ooh2 (6 phi - sum)) on the fine interior (FP64 arithmetic).
+__global__ void k_fine_residual_f32(Grid<double> phi, Grid<double> rho, float *__restrict__ rf,
+                                    double ooh2)
+{
+    const int n = phi.n, m = n - 2;
+    int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > m)
+        return;
+    long gp = phi.off + i + j * phi.sy + k * phi.sz;
+    long gr = rho.off + i + j * rho.sy + k * rho.sz;
+    const double *p = phi.p;
+    double r = rho.p[gr] + ooh2 * (6.0 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
+                                   p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
+    rf[i + (long)j * n + (long)k * n * n] = (float)r;
+}
+
+__global__ void k_add_correction(Grid<double> phi, const float *__restrict__ ef)
+{
+    const int n = phi.n, m = n - 2;
+    int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > m)
+        return;
+    phi.p[phi.off + i + j * phi.sy + k * phi.sz] += (double)ef[i + (long)j * n + (long)k * n * n];
+}
+
+static int mixed_iteration(qz_sim *s)
+{
+    Grid<double> phi = s->fine_phi, rho = s->fine_rho;
+    const int n = phi.n, m = n - 2;
+    int tx = m < 128 ? ((m + 31) / 32) * 32 : 128;
+    dim3 g((m + tx - 1) / tx, m, m);
+    double ooh2 = (double)((n - 1) * (n - 1));
+    launch(s, QZ_PROF_OTHER, 20.0 * m * m * m, k_fine_residual_f32, dim3(g), dim3(tx), phi, rho, s->rf, ooh2);
+    cudaMemsetAsync(s->ef, 0, (size_t)n * n * n * sizeof(float), s->stream);
+    int inner = s->cfg.inner_cycles > 0 ? s->cfg.inner_cycles : 1;
+    for (int q = 0; q < inner; q++)
+        if (vcycle_t<float>(s, 0, s->cfg.cycle))
+            return QZ_FAILURE;
+    launch(s, QZ_PROF_OTHER, 20.0 * m * m * m, k_add_correction, dim3(g), dim3(tx), phi, s->ef);
+    return check_cuda(cudaGetLastError(), "mixed iteration") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- convergence test (poisson_error.c:36-133) ------------------------------------
+constexpr int CK_THREADS = 256;
+
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0)
+    {
+        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+            r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_check_partial(int L, long D, const double *__restrict__ pot,
+                                const double *__restrict__ pot_old, const double *__restrict__ d,
+                                double tm, double tp, double oh2, double rm, double tol,
+                                int method, double *__restrict__ partial, int *__restrict__ flags)
+{
+    __shared__ double sh[32];
+    const int m = (1 << L) - 1;
+    const long total = (long)m * m * m;
+    const long D2 = D * D;
+    double acc = 0.0;
+    int ratio_fail = 0, resid_fail = 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x)
+    {
+        int i = 2 + (int)(t % m), j = 2 + (int)((t / m) % m), k = 2 + (int)(t / ((long)m * m));
+        long g = i + j * D + k * D2;
+        double a = pot[g] / pot_old[g];
+        if ((tm > a) || (tp < a))
+            ratio_fail = 1;
+        double diff = d[g] + oh2 * (6.0 * pot[g] - pot[g + 1] - pot[g - 1] - pot[g + D] -
+                                    pot[g - D] - pot[g + D2] - pot[g - D2]);
+        if (method == 1)
+        {
+            if (fabs(diff) / rm >= tol)
+                resid_fail = 1;
+        }
+        else
+            acc += diff * diff;
+    }
+    if (__syncthreads_or(ratio_fail) && threadIdx.x == 0)
+        flags[F_RATIO_FAIL] = 1;
+    if (__syncthreads_or(resid_fail) && threadIdx.x == 0)
+        flags[F_RESID_FAIL] = 1;
+    double b = block_sum(acc, sh);
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = b;
+}
+
+__global__ void k_check_final(int nblocks, long nintr, double rm, double tol, int method,
+                              const double *__restrict__ partial, int *__restrict__ flags,
+                              double *__restrict__ err_out)
+{
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        acc += partial[b];
+    double tot = block_sum(acc, sh);
+    if (threadIdx.x == 0)
+    {
+        int ok;
+        double err = 0.0;
+        if (method == 1)
+            ok = !flags[F_RESID_FAIL];
+        else
+        {
+            err = tot / nintr;
+            err = sqrt(err);
+            err = err / rm;
+            if (method == 2)
+                err = err / (cbrt((double)nintr) * cbrt((double)nintr));
+            ok = err < tol;
+        }
+        *err_out = err;
+        flags[F_CONVERGED] = (!flags[F_RATIO_FAIL]) && ok;
+    }
+}
+
+__global__ void k_copy_if_unconverged(long n, const double *__restrict__ src,
+                                      double *__restrict__ dst, const int *__restrict__ flags)
+{
+    if (flags[F_CONVERGED])
+        return;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+static int launch_check(qz_sim *s, double node_mass)
+{
+    const qz_config &c = s->cfg;
+    const int L = s->L;
+    const int nc = 1 << L;
+    const double H = 1.0 / (1 << L);
+    const double oh2 = 1.0 / (H * H);
+    const int size = nc * nc * nc;
+    const long nintr = (long)(nc - 1) * (nc - 1) * (nc - 1);
+    const double rm = 4.0 * c.G * QZ_PI_D * node_mass / (size * H * H * H);
+    cudaMemsetAsync(s->flags + F_RATIO_FAIL, 0, sizeof(int), s->stream);
+    cudaMemsetAsync(s->flags + F_RESID_FAIL, 0, sizeof(int), s->stream);
+    launch(s, QZ_PROF_CHECK, 24.0 * (double)nintr, k_check_partial, dim3(s->red_blocks), dim3(CK_THREADS), L, s->D, s->pot, s->pot_old, s->d, 1.0 - c.tol2, 1.0 + c.tol2, oh2, rm, c.tol, c.check_method, s->red, s->flags);
+    launch(s, QZ_PROF_CHECK, 8.0 * s->red_blocks, k_check_final, dim3(1), dim3(256), s->red_blocks, nintr, rm, c.tol, c.check_method, s->red, s->flags, s->red + s->red_blocks);
+    launch(s, QZ_PROF_CHECK, 16.0 * s->gpts, k_copy_if_unconverged, dim3(296), dim3(256), s->gpts, s->pot, s->pot_old, s->flags);
+    cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int), cudaMemcpyDeviceToHost,
+                    s->stream);
+    return check_cuda(cudaGetLastError(), "convergence check") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int poisson_error_head(qz_sim *s, int *converged)
+{
+    if (launch_check(s, s->cfg.total_mass))
+        return QZ_FAILURE;
+    if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
+        return QZ_FAILURE;
+    *converged = s->h_flags[F_CONVERGED] != 0;
+    return QZ_SUCCESS;
+}
+
+int potential_head(qz_sim *s)
+{
+    const qz_config &c = s->cfg;
+    cudaMemcpyAsync(s->pot_old, s->pot, s->gpts * sizeof(double), cudaMemcpyDeviceToDevice,
+                    s->stream);
+    int iter = 0;
+    bool check = false;
+    const int every = c.check_every > 0 ? c.check_every : 1;
+    while (iter < c.max_iter && !check)
+    {
+        int k = every - (iter % every);
+        if (k > c.max_iter - iter)
+            k = c.max_iter - iter;
+        for (int q = 0; q < k; q++)
+        {
+            int rc = c.precision == QZ_PREC_MIXED ? mixed_iteration(s) : vcycle(s, 0, c.cycle);
+            if (rc)
+                return QZ_FAILURE;
+            iter++;
+        }
+        if (iter % every == 0)
+        {
+            if (launch_check(s, c.total_mass))
+                return QZ_FAILURE;
+            if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
+                return QZ_FAILURE;
+            check = s->h_flags[F_CONVERGED] != 0;
+        }
+    }
+    s->stats.last_vcycles = iter;
+    s->stats.vcycles_total += iter;
+    s->stats.last_converged = check ? 1 : 0;
+    if (iter == c.max_iter)
+    {
+        set_error("the precision was not reached in the head node after %d multigrid cycles",
+                  iter);
+        return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+} // namespace qz

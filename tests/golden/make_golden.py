@@ -1,0 +1,111 @@
+"""Generate the golden fixtures of tests/golden/ from the compiled reference.
+
+QUANTIZER ships no tests or golden vectors, so every fixture here is produced
+by running the reference's own FP64 code, compiled unmodified from its
+sources (oracle/Makefile, target ``ref``):
+
+* ``head_L4_plummer1000.npz`` -- oracle/_ref/qz_ref_driver (the reference's
+  main-loop call order, fixed dt) on a 1000-particle Plummer sphere, head
+  16^3, 3 steps: head fields and particle state at steps 0 and 3, and the
+  head box index of every particle (ptcl_idx_to_box_idx).
+* ``head_L3_jacobi.npz`` -- the same with the Jacobi smoother (solver 1), head
+  8^3, 2 steps.
+* ``arrays.npz`` -- direct calls into oracle/_ref/libqzref.so of the
+  reference's gauss_saidel, jacobi (odd sweep count) and multigrid (V, F and W
+  cycles) on seeded random arrays.
+
+Run in a container that has the reference source tree:
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from quantizer_b200 import ics  # noqa: E402
+
+FIELDS = ("pot", "d", "gax", "gay", "gaz")
+PTCL = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+
+def run_case(name: str, ic: dict, steps: int, dt: float, **kw) -> None:
+    with tempfile.TemporaryDirectory() as td:
+        icp = os.path.join(td, "ic.bin")
+        ics.write_ic(icp, ic)
+        summary = O.run_reference(icp, td, steps=steps, dt=dt, dump=f"0,{steps}", **kw)
+        out = {f"ic_{k}": ic[k] for k in ics.FIELDS}
+        for s in (0, steps):
+            for f in FIELDS + PTCL:
+                out[f"s{s}_{f}"] = O.read_dump(td, s, f)
+            out[f"s{s}_bidx"] = O.read_dump(td, s, "bidx", np.int32)
+        out["meta"] = np.array([kw.get("lmin", 5), steps, dt, summary["n"]], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, summary)
+
+
+def arrays_case() -> None:
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libqzref.so"))
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)
+    try:
+        lib.global_variables()  # sets _Onesixth_, smoother choices, sweep counts
+    finally:
+        os.dup2(saved, 1)
+        os.close(devnull)
+    P = C.POINTER(C.c_double)
+    lib.gauss_saidel.argtypes = [P, P, C.c_int, C.c_int]
+    lib.jacobi.argtypes = [P, P, C.c_int, C.c_int]
+    lib.multigrid.argtypes = [P, P, C.c_int, C.c_int]
+    rng = np.random.default_rng(1234)
+    out = {}
+
+    def fresh(n):
+        # few significant bits, so the stored inputs compress well
+        phi = rng.integers(-1024, 1024, n ** 3).astype(np.float64) / 256.0
+        rho = rng.integers(-1024, 1024, n ** 3).astype(np.float64) / 4.0
+        return phi, rho
+
+    for n, iters in ((9, 2), (17, 3)):
+        phi, rho = fresh(n)
+        out[f"gs_n{n}_in_phi"], out[f"gs_n{n}_in_rho"] = phi.copy(), rho.copy()
+        lib.gauss_saidel(phi.ctypes.data_as(P), rho.ctypes.data_as(P), n, iters)
+        out[f"gs_n{n}_out"] = phi
+        out[f"gs_n{n}_iters"] = np.array([iters])
+    for n, iters in ((9, 3), (17, 2)):
+        phi, rho = fresh(n)
+        out[f"jac_n{n}_in_phi"], out[f"jac_n{n}_in_rho"] = phi.copy(), rho.copy()
+        lib.jacobi(phi.ctypes.data_as(P), rho.ctypes.data_as(P), n, iters)
+        out[f"jac_n{n}_out"] = phi
+        out[f"jac_n{n}_iters"] = np.array([iters])
+    for n, types in ((9, (0, 1, 2)), (17, (0, 1, 2)), (33, (0,))):
+        for t in types:
+            phi, rho = fresh(n)
+            out[f"mg_n{n}_t{t}_in_phi"], out[f"mg_n{n}_t{t}_in_rho"] = phi.copy(), rho.copy()
+            lib.multigrid(phi.ctypes.data_as(P), rho.ctypes.data_as(P), n, t)
+            out[f"mg_n{n}_t{t}_out"] = phi
+    np.savez_compressed(os.path.join(HERE, "arrays.npz"), **out)
+    print("wrote arrays.npz")
+
+
+def main() -> None:
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    ic = ics.plummer(1000, a=0.05, seed=11)
+    dt = 1e-3 * ics.crossing_time(0.05)
+    run_case("head_L4_plummer1000.npz", ic, steps=3, dt=dt, lmin=4)
+    run_case("head_L3_jacobi.npz", ic, steps=2, dt=dt, lmin=3, solver=1)
+    arrays_case()
+
+
+if __name__ == "__main__":
+    main()

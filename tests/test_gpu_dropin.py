@@ -1,0 +1,59 @@
+"""The drop-in link: the reference's own bookkeeping objects (initialization,
+tree construction/adaptation, globals) linked with libqz_dropin.so in place of
+its hot-path objects (oracle/_ref/qz_dropin_driver), run against the
+unmodified reference (oracle/_ref/qz_ref_driver) on the same inputs."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from quantizer_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def ic_file(tmp_path_factory):
+    d = tmp_path_factory.mktemp("dropin")
+    p = str(d / "ic.bin")
+    ics.write_ic(p, ics.plummer(4000, a=0.05, seed=21))
+    return p
+
+
+def _run(driver, ic_path, out, env=None, **kw):
+    os.makedirs(out, exist_ok=True)
+    old = dict(os.environ)
+    try:
+        if env:
+            os.environ.update(env)
+        return O.run_reference(ic_path, out, driver=driver, **kw)
+    finally:
+        os.environ.clear()
+        os.environ.update(old)
+
+
+@pytest.mark.parametrize("order,tol_pot,tol_pos", [("lex", 1e-12, 1e-13), ("rb", 1e-9, 1e-9)])
+def test_dropin_driver_matches_reference(ic_file, tmp_path, order, tol_pot, tol_pos):
+    for drv in (O.REF_DRIVER, O.DROPIN_DRIVER):
+        assert os.path.exists(drv), f"{drv} missing: run `make -C oracle ref dropin` where the reference is present"
+    kw = dict(lmin=5, steps=6, dt=7e-5, dump="0,6")
+    _run(O.REF_DRIVER, ic_file, str(tmp_path / "ref"), **kw)
+    _run(O.DROPIN_DRIVER, ic_file, str(tmp_path / "gpu"), env={"QZ_GS_ORDER": order}, **kw)
+    for s in (0, 6):
+        r = lambda f: O.read_dump(str(tmp_path / "ref"), s, f)
+        g = lambda f: O.read_dump(str(tmp_path / "gpu"), s, f)
+        assert _rel(g("d"), r("d")) < 1e-12
+        assert _rel(g("pot"), r("pot")) < tol_pot
+        for f in ("gax", "gay", "gaz"):
+            assert _rel(g(f), r(f)) < 100 * tol_pot
+        for f in ("x", "y", "z"):
+            assert np.abs(g(f) - r(f)).max() < tol_pos
+        for f in ("ax", "ay", "az"):
+            assert _rel(g(f), r(f)) < 100 * tol_pot
+        np.testing.assert_array_equal(O.read_dump(str(tmp_path / "gpu"), s, "bidx", np.int32),
+                                      O.read_dump(str(tmp_path / "ref"), s, "bidx", np.int32))
