@@ -114,10 +114,15 @@ __global__ void k_copy_grid(Grid<T> dst, Grid<T> src)
     dst.p[dst.off + i + j * dst.sy + k * dst.sz] = src.p[src.off + i + j * src.sy + k * src.sz];
 }
 
-// rho_c(l) = rho(2l) + ooh2 * (6 phi(2l) - sum of 6 neighbours) at the coarse
-// interior points; the coarse boundary stays zero.
+// rho_c(l) = scale * (rho(2l) + ooh2 * (6 phi(2l) - sum of 6 neighbours)) at
+// the coarse interior points; the coarse boundary stays zero.  scale is 1 in
+// the reference's lexicographic mode (plain injection, multigrid.c:29-49) and
+// 1/2 with red-black smoothing: after a red-black sweep the residual lives on
+// the red points only, and plain injection of it makes the cycle diverge
+// (measured growth x4 per cycle on a Plummer density), while half injection
+// converges at about 0.1 per cycle.
 template <typename T>
-__global__ void k_resid_restrict(Grid<T> phi, Grid<T> rho, Grid<T> rc, T ooh2)
+__global__ void k_resid_restrict(Grid<T> phi, Grid<T> rho, Grid<T> rc, T ooh2, T scale)
 {
     const int mc = rc.n - 2;
     int lx = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -130,7 +135,7 @@ __global__ void k_resid_restrict(Grid<T> phi, Grid<T> rho, Grid<T> rc, T ooh2)
     const T *p = phi.p;
     T r = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
                               p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
-    rc.p[rc.off + lx + ly * rc.sy + lz * rc.sz] = r;
+    rc.p[rc.off + lx + ly * rc.sy + lz * rc.sz] = scale * r;
 }
 
 // phi(fine interior) += sum over contributing interior coarse points, in the
@@ -309,7 +314,8 @@ static int vcycle_t(qz_sim *s, int l, int type)
         int tx = mc < 128 ? ((mc + 31) / 32) * 32 : 128;
         dim3 g((mc + tx - 1) / tx, mc, mc);
         T ooh2 = (T)(double)((n - 1) * (n - 1));
-        launch(s, QZ_PROF_RESTRICT, (double)sizeof(T) * 9.0 * mc * mc * mc, k_resid_restrict<T>, dim3(g), dim3(tx), phi, rho, crho, ooh2);
+        const T scale = (c.smoother == 0 && c.gs_order == QZ_GS_REDBLACK) ? (T)0.5 : (T)1.0;
+        launch(s, QZ_PROF_RESTRICT, (double)sizeof(T) * 9.0 * mc * mc * mc, k_resid_restrict<T>, dim3(g), dim3(tx), phi, rho, crho, ooh2, scale);
         if (type == 0)
         {
             if (vcycle_t<T>(s, l + 1, 0))

@@ -1,0 +1,93 @@
+"""Kernel micro-benchmarks of libqzb200 at chosen sizes (device time by CUDA
+events on the library stream; the per-launch profiler books algorithmic
+bytes per kernel category).
+
+    python -m quantizer_b200.kernel_bench smooth    --n 257 --iters 4
+    python -m quantizer_b200.kernel_bench multigrid --n 257 --cycles 2
+    python -m quantizer_b200.kernel_bench step      --particles 1000000 --lmin 7 --steps 3
+
+`smooth` and `multigrid` run the array-level routines (gauss_saidel /
+multigrid, red-black order) on seeded random grids of n^3 points, which is
+how the smoother is profiled at sizes whose fields exceed the 126 MB L2.
+`step` runs whole head-node leapfrog steps of a Plummer sphere (refinement
+off) -- a kernel-level measurement, not the workload of bench.py.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import core, ics
+
+
+def _smooth(args) -> dict:
+    n = args.n
+    rng = np.random.default_rng(0)
+    phi = rng.standard_normal(n ** 3)
+    rho = rng.standard_normal(n ** 3)
+    core.gauss_saidel(phi, rho, 1)  # warm-up (context, module load)
+    t0 = time.perf_counter()
+    core.gauss_saidel(phi, rho, args.iters)
+    t = time.perf_counter() - t0
+    return {"kernel": "smooth", "n": n, "iters": args.iters, "wall_s_incl_copies": t}
+
+
+def _multigrid(args) -> dict:
+    n = args.n
+    rng = np.random.default_rng(0)
+    phi = np.zeros(n ** 3)
+    rho = rng.standard_normal(n ** 3)
+    core.multigrid(phi, rho)
+    t0 = time.perf_counter()
+    for _ in range(args.cycles):
+        phi = core.multigrid(phi, rho)
+    t = time.perf_counter() - t0
+    return {"kernel": "multigrid", "n": n, "cycles": args.cycles, "wall_s_incl_copies": t}
+
+
+def _step(args) -> dict:
+    ic = ics.plummer(args.particles, a=args.a, seed=1)
+    dt = 1e-3 * ics.crossing_time(args.a)
+    with core.Simulation(ic, args.lmin, precision=args.precision) as sim:
+        sim.init_forces()
+        sim.step(dt, 1)
+        core.profile_reset(sim)
+        core.profile_enable(sim, True)
+        st0 = sim.stats()
+        t0 = time.perf_counter()
+        sim.step(dt, args.steps)
+        sim.synchronize()
+        t = time.perf_counter() - t0
+        st1 = sim.stats()
+        prof = core.profile_read(sim)
+    kern = {c: {"launches": v[0], "ms": round(v[1], 4),
+                "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else 0.0}
+            for c, v in prof.items() if v[0]}
+    return {"kernel": "step", "particles": args.particles, "lmin": args.lmin,
+            "steps": args.steps, "wall_ms_per_step": 1e3 * t / args.steps,
+            "vcycles_per_step": (st1.vcycles_total - st0.vcycles_total) / args.steps,
+            "launches_per_step": (st1.kernel_launches - st0.kernel_launches) / args.steps,
+            "kernels": kern}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=("smooth", "multigrid", "step"))
+    ap.add_argument("--n", type=int, default=257)
+    ap.add_argument("--iters", type=int, default=4)
+    ap.add_argument("--cycles", type=int, default=2)
+    ap.add_argument("--particles", type=int, default=1_000_000)
+    ap.add_argument("--lmin", type=int, default=7)
+    ap.add_argument("--a", type=float, default=0.02)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--precision", type=int, default=0)
+    args = ap.parse_args()
+    fn = {"smooth": _smooth, "multigrid": _multigrid, "step": _step}[args.what]
+    print(json.dumps(fn(args)))
+
+
+if __name__ == "__main__":
+    main()
