@@ -3,6 +3,7 @@
 // per-stage entry points in the reference's main-loop order, and array-level
 // wrappers of the force_methods routines.
 #include <stdarg.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -107,6 +108,13 @@ static bool build_levels(qz_sim *s, int n0)
             return false;
         if (mixed)
             cudaMemset(l.rhof, 0, pts * sizeof(float));
+        if (!dmalloc(&l.alt, pts, "mg alt"))
+            return false;
+        cudaMemset(l.alt, 0, pts * sizeof(double));
+        if (mixed && !dmalloc(&l.altf, pts, "mg alt32"))
+            return false;
+        if (mixed)
+            cudaMemset(l.altf, 0, pts * sizeof(float));
         s->levels.push_back(l);
         n = nc;
     }
@@ -121,10 +129,12 @@ static bool build_levels(qz_sim *s, int n0)
     if (mixed)
     {
         size_t pts = (size_t)n0 * n0 * n0;
-        if (!dmalloc(&s->rf, pts, "rf") || !dmalloc(&s->ef, pts, "ef"))
+        if (!dmalloc(&s->rf, pts, "rf") || !dmalloc(&s->ef, pts, "ef") ||
+            !dmalloc(&s->ef_alt, pts, "ef alt"))
             return false;
         cudaMemset(s->rf, 0, pts * sizeof(float));
         cudaMemset(s->ef, 0, pts * sizeof(float));
+        cudaMemset(s->ef_alt, 0, pts * sizeof(float));
     }
     return true;
 }
@@ -140,6 +150,8 @@ static void free_levels(qz_sim *s)
             dfree(l.rho);
             dfree(l.phif);
             dfree(l.rhof);
+            dfree(l.alt);
+            dfree(l.altf);
         }
         dfree(l.scr);
         dfree(l.scrf);
@@ -147,7 +159,10 @@ static void free_levels(qz_sim *s)
     s->levels.clear();
     dfree(s->rf);
     dfree(s->ef);
-    s->rf = s->ef = nullptr;
+    dfree(s->ef_alt);
+    dfree(s->fine_alt_buf);
+    s->rf = s->ef = s->ef_alt = nullptr;
+    s->fine_alt_buf = nullptr;
 }
 
 static bool ensure_stage(qz_sim *s, size_t bytes)
@@ -267,6 +282,8 @@ int qz_destroy(qz_sim *s)
     if (s->stream)
         cudaStreamSynchronize(s->stream);
     prof_collect(s);
+    if (s->check_exec)
+        cudaGraphExecDestroy(s->check_exec);
     for (cudaEvent_t e : s->ev_pool)
         cudaEventDestroy(e);
     s->ev_pool.clear();
@@ -325,6 +342,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     }
     qz_sim *s = new qz_sim();
     s->cfg = *cfg;
+    s->use_graphs = getenv("QZ_NO_GRAPHS") == nullptr;
     cudaGetDevice(&s->device);
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream"))
     {
@@ -364,7 +382,9 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         cudaMemset(s->d, 0, gb);
         s->fine_phi = head_view(s, s->pot);
         s->fine_rho = head_view(s, s->d);
-        ok = build_levels(s, (1 << s->L) + 1);
+        ok = build_levels(s, (1 << s->L) + 1) && dmalloc(&s->fine_alt_buf, s->gpts, "pot alt");
+        if (ok)
+            s->fine_alt = head_view(s, s->fine_alt_buf);
     }
     if (ok)
         ok = head_initial(s) == QZ_SUCCESS;
@@ -614,11 +634,12 @@ static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, 
     }
     s->fine_phi = dense_view(*dphi, gridsize);
     s->fine_rho = dense_view(*drho, gridsize);
-    if (!build_levels(s, gridsize))
+    if (!build_levels(s, gridsize) || !dmalloc(&s->fine_alt_buf, pts, "phi alt"))
     {
         qz_destroy(s);
         return nullptr;
     }
+    s->fine_alt = dense_view(s->fine_alt_buf, gridsize);
     return s;
 }
 
@@ -654,7 +675,11 @@ static int smooth_body(qz_sim *s, void *a)
 struct CycleArg {
     int type;
 };
-static int cycle_body(qz_sim *s, void *a) { return vcycle(s, 0, ((CycleArg *)a)->type); }
+static int cycle_body(qz_sim *s, void *a)
+{
+    sync_fine_alt(s);
+    return vcycle(s, 0, ((CycleArg *)a)->type);
+}
 
 int qz_gauss_saidel(double *phi, const double *rho, int gridsize, int iter_max, double w,
                     int gs_order)

@@ -36,6 +36,8 @@ struct Level {
     float *phif = nullptr, *rhof = nullptr; // FP32 hierarchy (mixed precision)
     double *scr = nullptr;                  // Jacobi ping-pong buffers (smoother 1)
     float *scrf = nullptr;
+    double *alt = nullptr;                  // red-black ping-pong partners (zero boundary)
+    float *altf = nullptr;
 };
 
 // Device-side flag words (int).
@@ -76,6 +78,9 @@ struct qz_sim {
     float *rf = nullptr, *ef = nullptr;
     std::vector<qz::Level> levels; // levels[0].n = 2^L + 1 (embedded), levels[l>0] owned
     qz::Grid<double> fine_phi{}, fine_rho{}; // level-0 views (head solve grid)
+    qz::Grid<double> fine_alt{};             // level-0 red-black ping-pong partner
+    double *fine_alt_buf = nullptr;
+    float *ef_alt = nullptr;
 
     // deposit scratch
     qz::Sort sort;
@@ -98,6 +103,11 @@ struct qz_sim {
 
     qz_stats stats{};
     bool forces_ready = false;
+
+    // CUDA graph of one convergence-check block of the head solve
+    bool use_graphs = true;
+    cudaGraphExec_t check_exec = nullptr;
+    long long check_graph_kernels = 0;
 
     // per-kernel-category timing (qz_profile_*): begin/end events per launch
     bool prof = false;
@@ -125,6 +135,26 @@ void prof_collect(qz_sim *s);
 
 // Launches kernel k on the library stream; counts it, and when profiling is
 // on brackets it with events and books `bytes` algorithmic bytes to `cat`.
+template <typename... KArgs, typename... Args>
+inline void launch_shm(qz_sim *s, int cat, double bytes, size_t shm, void (*k)(KArgs...), dim3 g,
+                       dim3 b, Args &&...args)
+{
+    cudaEvent_t eb = nullptr, ee = nullptr;
+    if (s->prof)
+    {
+        eb = prof_event(s);
+        ee = prof_event(s);
+        cudaEventRecord(eb, s->stream);
+    }
+    k<<<g, b, shm, s->stream>>>(std::forward<Args>(args)...);
+    s->stats.kernel_launches++;
+    if (s->prof)
+    {
+        cudaEventRecord(ee, s->stream);
+        s->prof_pending.push_back({cat, bytes, eb, ee});
+    }
+}
+
 template <typename... KArgs, typename... Args>
 inline void launch(qz_sim *s, int cat, double bytes, void (*k)(KArgs...), dim3 g, dim3 b,
                    Args &&...args)
@@ -156,6 +186,7 @@ int kick(qz_sim *s, double dt);
 int potential_head(qz_sim *s);
 int poisson_error_head(qz_sim *s, int *converged);
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters);
+void sync_fine_alt(qz_sim *s);
 int vcycle(qz_sim *s, int level, int type);
 
 int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **vals_out);

@@ -54,6 +54,84 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
     p[gp] = w * a + ((T)1.0 - w) * p[gp];
 }
 
+// One whole red-black sweep per launch, tiled in 3-D: a CTA stages its tile
+// of phi_in plus a 2-point halo in shared memory, updates the red points of
+// the tile and of a 1-point ring around it (the ring values are recomputed by
+// the neighbouring CTAs too, from the same inputs, so they agree bit for bit),
+// then the black points of the tile, and writes the tile to phi_out.  Reading
+// phi_in and writing phi_out (ping-pong) keeps CTAs from racing on halos.  The
+// arithmetic is that of k_gs_rb, so the result equals two k_gs_rb launches.
+constexpr int RBT_X = 32, RBT_Y = 8, RBT_Z = 8;
+constexpr int RBS_X = RBT_X + 4, RBS_Y = RBT_Y + 4, RBS_Z = RBT_Z + 4;
+
+template <typename T>
+__global__ void __launch_bounds__(RBT_X * RBT_Y) k_gs_rb_tile(Grid<T> pin, Grid<T> pout,
+                                                              Grid<T> rho, T H2, T w)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *S = reinterpret_cast<T *>(smem_raw);
+    const int m = pin.n - 2;
+    const int x0 = 1 + blockIdx.x * RBT_X, y0 = 1 + blockIdx.y * RBT_Y, z0 = 1 + blockIdx.z * RBT_Z;
+    const int tid = threadIdx.x + threadIdx.y * RBT_X;
+    const int nth = RBT_X * RBT_Y;
+    const int last = pin.n - 1;
+    // stage phi_in over the tile + 2-point halo (points outside the grid are never read)
+    for (int q = tid; q < RBS_X * RBS_Y * RBS_Z; q += nth)
+    {
+        int lx = q % RBS_X, ly = (q / RBS_X) % RBS_Y, lz = q / (RBS_X * RBS_Y);
+        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
+        T v = (T)0;
+        if (gx >= 0 && gx <= last && gy >= 0 && gy <= last && gz >= 0 && gz <= last)
+            v = pin.p[pin.off + gx + gy * pin.sy + (long)gz * pin.sz];
+        S[q] = v;
+    }
+    __syncthreads();
+    const T one_sixth = (T)(1.0 / 6.0);
+    const int SY = RBS_X, SZ = RBS_X * RBS_Y;
+    // red points (i+j+k even) of the tile and its 1-point ring
+    for (int q = tid; q < (RBT_X + 2) * (RBT_Y + 2) * (RBT_Z + 2); q += nth)
+    {
+        int lx = 1 + q % (RBT_X + 2), ly = 1 + (q / (RBT_X + 2)) % (RBT_Y + 2),
+            lz = 1 + q / ((RBT_X + 2) * (RBT_Y + 2));
+        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
+        if (gx < 1 || gx > m || gy < 1 || gy > m || gz < 1 || gz > m || ((gx + gy + gz) & 1))
+            continue;
+        int l = lx + ly * SY + lz * SZ;
+        T a = one_sixth * (-H2 * rho.p[rho.off + gx + gy * rho.sy + (long)gz * rho.sz] + S[l + 1] +
+                           S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] + S[l - SZ]);
+        S[l] = w * a + ((T)1.0 - w) * S[l];
+    }
+    __syncthreads();
+    // black points of the tile, then the tile is written out
+    for (int lz = 2; lz < RBT_Z + 2; lz++)
+    {
+        int lx = 2 + threadIdx.x, ly = 2 + threadIdx.y;
+        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
+        if (gx > m || gy > m || gz > m)
+            continue;
+        int l = lx + ly * SY + lz * SZ;
+        T v = S[l];
+        if ((gx + gy + gz) & 1)
+        {
+            T a = one_sixth * (-H2 * rho.p[rho.off + gx + gy * rho.sy + (long)gz * rho.sz] +
+                               S[l + 1] + S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] + S[l - SZ]);
+            v = w * a + ((T)1.0 - w) * v;
+        }
+        pout.p[pout.off + gx + gy * pout.sy + (long)gz * pout.sz] = v;
+    }
+}
+
+template <typename T>
+__global__ void k_copy_interior(Grid<T> dst, Grid<T> src)
+{
+    const int m = src.n - 2;
+    int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+    if (i > m)
+        return;
+    dst.p[dst.off + i + j * dst.sy + (long)k * dst.sz] = src.p[src.off + i + j * src.sy + (long)k * src.sz];
+}
+
 // Lexicographic sweeps (k slowest, i fastest) reproduced exactly: the update
 // of point (i,j,k) reads new values at i-1, j-1, k-1 and old values at i+1,
 // j+1, k+1, so all points with the same i+j+k are independent.
@@ -184,7 +262,8 @@ __global__ void k_prolong_add(Grid<T> phi, Grid<T> c)
 
 // ---- host-side multigrid -----------------------------------------------------
 template <typename T>
-static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scratch)
+static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scratch,
+                    Grid<T> alt)
 {
     const qz_config &c = s->cfg;
     const int n = phi.n;
@@ -198,6 +277,27 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
         if (c.gs_order == QZ_GS_LEX)
         {
             launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m * iters, k_gs_lex_cta<T>, dim3(1), dim3(1024), phi, rho, iters, H2, w);
+        }
+        else if (alt.p)
+        {
+            // fused sweeps, ping-pong phi <-> alt (alt has phi's boundary values)
+            dim3 grid((m + RBT_X - 1) / RBT_X, (m + RBT_Y - 1) / RBT_Y, (m + RBT_Z - 1) / RBT_Z);
+            size_t shm = sizeof(T) * RBS_X * RBS_Y * RBS_Z;
+            Grid<T> a = phi, b = alt;
+            for (int it = 0; it < iters; it++)
+            {
+                launch_shm(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m, shm,
+                           k_gs_rb_tile<T>, grid, dim3(RBT_X, RBT_Y), a, b, rho, H2, w);
+                Grid<T> t = a;
+                a = b;
+                b = t;
+            }
+            if (iters & 1)
+            {
+                int tx = m < 128 ? ((m + 31) / 32) * 32 : 128;
+                launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 2.0 * m * m * m, k_copy_interior<T>,
+                       dim3((m + tx - 1) / tx, m, m), dim3(tx), phi, alt);
+            }
         }
         else
         {
@@ -244,6 +344,7 @@ struct LevelViews {
     static Grid<T> phi(qz_sim *s, int l);
     static Grid<T> rho(qz_sim *s, int l);
     static Grid<T> scratch(qz_sim *s, int l);
+    static Grid<T> alt(qz_sim *s, int l);
 };
 
 // Level 0 of the FP64 hierarchy is the fine grid view of the context (the head
@@ -264,6 +365,16 @@ template <>
 Grid<double> LevelViews<double>::scratch(qz_sim *s, int l)
 {
     return dense_view(s->levels[l].scr, s->levels[l].n);
+}
+template <>
+Grid<double> LevelViews<double>::alt(qz_sim *s, int l)
+{
+    return l == 0 ? s->fine_alt : dense_view(s->levels[l].alt, s->levels[l].n);
+}
+template <>
+Grid<float> LevelViews<float>::alt(qz_sim *s, int l)
+{
+    return dense_view(l == 0 ? s->ef_alt : s->levels[l].altf, s->levels[l].n);
 }
 template <>
 Grid<float> LevelViews<float>::phi(qz_sim *s, int l)
@@ -288,16 +399,18 @@ static int vcycle_t(qz_sim *s, int l, int type)
     Grid<T> phi = LevelViews<T>::phi(s, l), rho = LevelViews<T>::rho(s, l);
     const int n = phi.n;
     const int nc = (n + 1) / 2;
-    Grid<T> scr{};
+    Grid<T> scr{}, alt{};
     if (c.smoother == 1)
         scr = LevelViews<T>::scratch(s, l);
-    if (smooth_t<T>(s, phi, rho, c.n_pre, scr))
+    if (c.smoother == 0 && c.gs_order == QZ_GS_REDBLACK)
+        alt = LevelViews<T>::alt(s, l);
+    if (smooth_t<T>(s, phi, rho, c.n_pre, scr, alt))
         return QZ_FAILURE;
     if (nc < 4)
     {
         // multigrid.c:158-173: the coarse correction stays zero; the fine grid
         // gets n_coarse more smoothing sweeps instead.
-        if (smooth_t<T>(s, phi, rho, c.n_coarse, scr))
+        if (smooth_t<T>(s, phi, rho, c.n_coarse, scr, alt))
             return QZ_FAILURE;
     }
     else
@@ -336,7 +449,7 @@ static int vcycle_t(qz_sim *s, int l, int type)
         dim3 gf((m + tf - 1) / tf, m, m);
         launch(s, QZ_PROF_PROLONG, (double)sizeof(T) * 2.125 * m * m * m, k_prolong_add<T>, dim3(gf), dim3(tf), phi, cphi);
     }
-    if (smooth_t<T>(s, phi, rho, c.n_post, scr))
+    if (smooth_t<T>(s, phi, rho, c.n_post, scr, alt))
         return QZ_FAILURE;
     return check_cuda(cudaGetLastError(), "multigrid cycle") ? QZ_SUCCESS : QZ_FAILURE;
 }
@@ -345,10 +458,27 @@ int vcycle(qz_sim *s, int level, int type) { return vcycle_t<double>(s, level, t
 
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters)
 {
-    Grid<double> scr{};
+    Grid<double> scr{}, alt{};
     if (s->cfg.smoother == 1)
         scr = LevelViews<double>::scratch(s, 0);
-    return smooth_t<double>(s, phi, rho, iters, scr);
+    if (s->cfg.smoother == 0 && s->cfg.gs_order == QZ_GS_REDBLACK)
+    {
+        sync_fine_alt(s);
+        alt = LevelViews<double>::alt(s, 0);
+    }
+    return smooth_t<double>(s, phi, rho, iters, scr, alt);
+}
+
+// The fine level's ping-pong partner must carry the fine grid's boundary
+// values (Dirichlet during a solve): refresh it from the fine grid.
+void sync_fine_alt(qz_sim *s)
+{
+    if (!s->fine_alt.p)
+        return;
+    const int n = s->fine_phi.n;
+    int tx = n < 128 ? ((n + 31) / 32) * 32 : 128;
+    launch(s, QZ_PROF_OTHER, 16.0 * n * n * n, k_copy_grid<double>, dim3((n + tx - 1) / tx, n, n),
+           dim3(tx), s->fine_alt, s->fine_phi);
 }
 
 // ---- mixed precision: FP64 defect, FP32 cycles ---------------------------------
@@ -515,6 +645,34 @@ static int launch_check(qz_sim *s, double node_mass)
     return check_cuda(cudaGetLastError(), "convergence check") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
+// Captures `every` solver iterations followed by the convergence test into a
+// CUDA graph (kernel parameters and buffers of a context never change).
+static int capture_check_block(qz_sim *s, int every)
+{
+    const long long before = s->stats.kernel_launches;
+    if (!check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal),
+                    "begin capture"))
+        return QZ_FAILURE;
+    int rc = QZ_SUCCESS;
+    for (int q = 0; q < every && rc == QZ_SUCCESS; q++)
+        rc = s->cfg.precision == QZ_PREC_MIXED ? mixed_iteration(s) : vcycle(s, 0, s->cfg.cycle);
+    if (rc == QZ_SUCCESS)
+        rc = launch_check(s, s->cfg.total_mass);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    s->check_graph_kernels = s->stats.kernel_launches - before;
+    s->stats.kernel_launches = before;
+    if (rc != QZ_SUCCESS || !check_cuda(e, "end capture"))
+    {
+        if (g)
+            cudaGraphDestroy(g);
+        return QZ_FAILURE;
+    }
+    e = cudaGraphInstantiate(&s->check_exec, g, 0);
+    cudaGraphDestroy(g);
+    return check_cuda(e, "graph instantiate") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 int poisson_error_head(qz_sim *s, int *converged)
 {
     if (launch_check(s, s->cfg.total_mass))
@@ -530,11 +688,27 @@ int potential_head(qz_sim *s)
     const qz_config &c = s->cfg;
     cudaMemcpyAsync(s->pot_old, s->pot, s->gpts * sizeof(double), cudaMemcpyDeviceToDevice,
                     s->stream);
+    sync_fine_alt(s);
     int iter = 0;
     bool check = false;
     const int every = c.check_every > 0 ? c.check_every : 1;
+    const bool graphs = s->use_graphs && !s->prof;
     while (iter < c.max_iter && !check)
     {
+        if (graphs && iter % every == 0 && c.max_iter - iter >= every)
+        {
+            // one graph launch = `every` cycles + the convergence test + flag read-back
+            if (!s->check_exec && capture_check_block(s, every))
+                return QZ_FAILURE;
+            if (!check_cuda(cudaGraphLaunch(s->check_exec, s->stream), "check-block graph"))
+                return QZ_FAILURE;
+            s->stats.kernel_launches += s->check_graph_kernels;
+            iter += every;
+            if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
+                return QZ_FAILURE;
+            check = s->h_flags[F_CONVERGED] != 0;
+            continue;
+        }
         int k = every - (iter % every);
         if (k > c.max_iter - iter)
             k = c.max_iter - iter;
