@@ -100,6 +100,12 @@ static void dump_nodes(const char *dir, int step)
             write_i32(dir, step, name, p->ptr_box, bcap);
             snprintf(name, sizeof name, "L%d_N%d_cells", lv, i);
             write_i32(dir, step, name, p->ptr_box_idx, p->cell_size);
+            snprintf(name, sizeof name, "L%d_N%d_cx", lv, i);
+            write_i32(dir, step, name, p->ptr_cell_idx_x, p->cell_size);
+            snprintf(name, sizeof name, "L%d_N%d_cy", lv, i);
+            write_i32(dir, step, name, p->ptr_cell_idx_y, p->cell_size);
+            snprintf(name, sizeof name, "L%d_N%d_cz", lv, i);
+            write_i32(dir, step, name, p->ptr_cell_idx_z, p->cell_size);
             snprintf(name, sizeof name, "L%d_N%d_pot", lv, i);
             write_f64(dir, step, name, p->ptr_pot, gcap);
             snprintf(name, sizeof name, "L%d_N%d_d", lv, i);

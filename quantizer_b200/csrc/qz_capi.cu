@@ -86,6 +86,7 @@ static void dfree(void *p)
 // (coarse size >= 4).
 static bool build_levels(qz_sim *s, int n0)
 {
+    init_kernel_attributes();
     const bool mixed = s->cfg.precision == QZ_PREC_MIXED;
     const bool jac = s->cfg.smoother == 1;
     s->levels.clear();
@@ -343,6 +344,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     qz_sim *s = new qz_sim();
     s->cfg = *cfg;
     s->use_graphs = getenv("QZ_NO_GRAPHS") == nullptr;
+    s->fused_rb = getenv("QZ_FUSED_RB") != nullptr;
     cudaGetDevice(&s->device);
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream"))
     {
@@ -623,6 +625,7 @@ static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, 
     }
     qz_sim *s = new qz_sim();
     s->cfg = *cfg;
+    s->fused_rb = getenv("QZ_FUSED_RB") != nullptr;
     cudaGetDevice(&s->device);
     size_t pts = (size_t)gridsize * gridsize * gridsize;
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream") ||

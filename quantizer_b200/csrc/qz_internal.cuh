@@ -106,6 +106,10 @@ struct qz_sim {
 
     // CUDA graph of one convergence-check block of the head solve
     bool use_graphs = true;
+    // one-launch tiled red-black sweep (k_gs_rb_tile) for levels of >= 64
+    // interior points per side; off by default (slower than two k_gs_rb
+    // launches on B200 at 257^3, see profiles/)
+    bool fused_rb = false;
     cudaGraphExec_t check_exec = nullptr;
     long long check_graph_kernels = 0;
 
@@ -187,6 +191,7 @@ int potential_head(qz_sim *s);
 int poisson_error_head(qz_sim *s, int *converged);
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters);
 void sync_fine_alt(qz_sim *s);
+void init_kernel_attributes();
 int vcycle(qz_sim *s, int level, int type);
 
 int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **vals_out);

@@ -15,6 +15,8 @@
 //                    points in the reference's scatter order, fused with
 //                    phi += dphi (multigrid.c:51-104, 199-209)
 //   k_check_*        ratio test + residual norm, fixed-tree deterministic sums
+#include <cuda_pipeline.h>
+
 #include "qz_internal.cuh"
 
 namespace qz {
@@ -55,70 +57,136 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
 }
 
 // One whole red-black sweep per launch, tiled in 3-D: a CTA stages its tile
-// of phi_in plus a 2-point halo in shared memory, updates the red points of
-// the tile and of a 1-point ring around it (the ring values are recomputed by
-// the neighbouring CTAs too, from the same inputs, so they agree bit for bit),
-// then the black points of the tile, and writes the tile to phi_out.  Reading
-// phi_in and writing phi_out (ping-pong) keeps CTAs from racing on halos.  The
-// arithmetic is that of k_gs_rb, so the result equals two k_gs_rb launches.
-constexpr int RBT_X = 32, RBT_Y = 8, RBT_Z = 8;
+// of phi_in plus a 2-point halo in shared memory (asynchronous copies), updates
+// the red points of the tile and of a 1-point ring around it (the ring values
+// are recomputed by the neighbouring CTAs too, from the same inputs, so they
+// agree bit for bit), then the black points of the tile, and writes the tile to
+// phi_out.  Reading phi_in and writing phi_out (ping-pong) keeps CTAs from
+// racing on halos.  Each thread owns x-adjacent pairs of points -- one red, one
+// black -- so every lane updates one point per row in each colour phase.  The
+// arithmetic is that of k_gs_rb: the result equals two k_gs_rb launches.
+constexpr int RBT_X = 64, RBT_Y = 8, RBT_Z = 8; // tile (points); 32 x 8 threads
 constexpr int RBS_X = RBT_X + 4, RBS_Y = RBT_Y + 4, RBS_Z = RBT_Z + 4;
+constexpr int RB_THREADS_X = 32, RB_THREADS_Y = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(RBT_X * RBT_Y) k_gs_rb_tile(Grid<T> pin, Grid<T> pout,
-                                                              Grid<T> rho, T H2, T w)
+__device__ __forceinline__ void rb_update(T *S, int l, T rho_v, T H2, T w)
+{
+    constexpr int SY = RBS_X, SZ = RBS_X * RBS_Y;
+    const T one_sixth = (T)(1.0 / 6.0);
+    T a = one_sixth * (-H2 * rho_v + S[l + 1] + S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] +
+                       S[l - SZ]);
+    S[l] = w * a + ((T)1.0 - w) * S[l];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RB_THREADS_X * RB_THREADS_Y)
+    k_gs_rb_tile(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w)
 {
     extern __shared__ unsigned char smem_raw[];
     T *S = reinterpret_cast<T *>(smem_raw);
+    constexpr int SY = RBS_X, SZ = RBS_X * RBS_Y;
     const int m = pin.n - 2;
-    const int x0 = 1 + blockIdx.x * RBT_X, y0 = 1 + blockIdx.y * RBT_Y, z0 = 1 + blockIdx.z * RBT_Z;
-    const int tid = threadIdx.x + threadIdx.y * RBT_X;
-    const int nth = RBT_X * RBT_Y;
     const int last = pin.n - 1;
-    // stage phi_in over the tile + 2-point halo (points outside the grid are never read)
-    for (int q = tid; q < RBS_X * RBS_Y * RBS_Z; q += nth)
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = 1 + blockIdx.x * RBT_X, y0 = 1 + blockIdx.y * RBT_Y, z0 = 1 + blockIdx.z * RBT_Z;
+    // stage: local x in 0..67 = global x0-2 .. x0+65; lanes take x = tx, 32+tx, 64+tx (tx<4)
+#pragma unroll
+    for (int lz = 0; lz < RBS_Z; lz++)
     {
-        int lx = q % RBS_X, ly = (q / RBS_X) % RBS_Y, lz = q / (RBS_X * RBS_Y);
-        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
-        T v = (T)0;
-        if (gx >= 0 && gx <= last && gy >= 0 && gy <= last && gz >= 0 && gz <= last)
-            v = pin.p[pin.off + gx + gy * pin.sy + (long)gz * pin.sz];
-        S[q] = v;
-    }
-    __syncthreads();
-    const T one_sixth = (T)(1.0 / 6.0);
-    const int SY = RBS_X, SZ = RBS_X * RBS_Y;
-    // red points (i+j+k even) of the tile and its 1-point ring
-    for (int q = tid; q < (RBT_X + 2) * (RBT_Y + 2) * (RBT_Z + 2); q += nth)
-    {
-        int lx = 1 + q % (RBT_X + 2), ly = 1 + (q / (RBT_X + 2)) % (RBT_Y + 2),
-            lz = 1 + q / ((RBT_X + 2) * (RBT_Y + 2));
-        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
-        if (gx < 1 || gx > m || gy < 1 || gy > m || gz < 1 || gz > m || ((gx + gy + gz) & 1))
+        const int gz = z0 - 2 + lz;
+        if (gz < 0 || gz > last)
             continue;
-        int l = lx + ly * SY + lz * SZ;
-        T a = one_sixth * (-H2 * rho.p[rho.off + gx + gy * rho.sy + (long)gz * rho.sz] + S[l + 1] +
-                           S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] + S[l - SZ]);
-        S[l] = w * a + ((T)1.0 - w) * S[l];
+#pragma unroll
+        for (int hy = 0; hy < 2; hy++)
+        {
+            const int ly = ty + RB_THREADS_Y * hy;
+            if (ly >= RBS_Y)
+                break;
+            const int gy = y0 - 2 + ly;
+            if (gy < 0 || gy > last)
+                continue;
+            const T *row = pin.p + pin.off + gy * pin.sy + (long)gz * pin.sz;
+#pragma unroll
+            for (int hx = 0; hx < 3; hx++)
+            {
+                const int lx = tx + 32 * hx;
+                const int gx = x0 - 2 + lx;
+                if (lx < RBS_X && gx >= 0 && gx <= last)
+                    __pipeline_memcpy_async(&S[lx + ly * SY + lz * SZ], row + gx, sizeof(T));
+            }
+        }
+    }
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    // red phase over the tile and its 1-point ring: local x pairs (1+2p, 2+2p),
+    // p = 0..32 (lane tx takes p = tx, and lane 0 also p = 32)
+#pragma unroll 2
+    for (int lz = 1; lz <= RBT_Z + 2; lz++)
+    {
+        const int gz = z0 - 2 + lz;
+        if (gz < 1 || gz > m)
+            continue;
+        for (int ly = 1 + ty; ly <= RBT_Y + 2; ly += RB_THREADS_Y)
+        {
+            const int gy = y0 - 2 + ly;
+            if (gy < 1 || gy > m)
+                continue;
+            const long rrow = rho.off + gy * rho.sy + (long)gz * rho.sz;
+#pragma unroll
+            for (int hp = 0; hp < 2; hp++)
+            {
+                const int pidx = tx + 32 * hp;
+                if (pidx > 32)
+                    break;
+                // the red member of the pair
+                int lx = 1 + 2 * pidx;
+                int gx = x0 - 2 + lx;
+                if ((gx + gy + gz) & 1)
+                {
+                    lx++;
+                    gx++;
+                }
+                if (gx >= 1 && gx <= m)
+                    rb_update(S, lx + ly * SY + lz * SZ, rho.p[rrow + gx], H2, w);
+            }
+        }
     }
     __syncthreads();
-    // black points of the tile, then the tile is written out
+    // black phase over the tile: local x pairs (2+2t, 3+2t), t = tx; write both
+    const int lxa = 2 + 2 * tx;
+    const int gxa = x0 + 2 * tx; // global x of the pair's first point
+    const int gy = y0 + ty;
+    if (gy > m || gxa > m)
+        return;
+    const bool second = gxa + 1 <= m;
+    const long rrow = rho.off + gy * rho.sy;
+    const long orow = pout.off + gy * pout.sy;
+    const int ly = 2 + ty;
+#pragma unroll 2
     for (int lz = 2; lz < RBT_Z + 2; lz++)
     {
-        int lx = 2 + threadIdx.x, ly = 2 + threadIdx.y;
-        int gx = x0 - 2 + lx, gy = y0 - 2 + ly, gz = z0 - 2 + lz;
-        if (gx > m || gy > m || gz > m)
-            continue;
-        int l = lx + ly * SY + lz * SZ;
-        T v = S[l];
-        if ((gx + gy + gz) & 1)
-        {
-            T a = one_sixth * (-H2 * rho.p[rho.off + gx + gy * rho.sy + (long)gz * rho.sz] +
-                               S[l + 1] + S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] + S[l - SZ]);
-            v = w * a + ((T)1.0 - w) * v;
-        }
-        pout.p[pout.off + gx + gy * pout.sy + (long)gz * pout.sz] = v;
+        const int gz = z0 - 2 + lz;
+        if (gz > m)
+            break;
+        const int l = lxa + ly * SY + lz * SZ;
+        const int black = ((gxa + gy + gz) & 1) ? 0 : 1; // offset of the black member
+        if (black == 0 || second)
+            rb_update(S, l + black, rho.p[rrow + (long)gz * rho.sz + gxa + black], H2, w);
+        pout.p[orow + (long)gz * pout.sz + gxa] = S[l];
+        if (second)
+            pout.p[orow + (long)gz * pout.sz + gxa + 1] = S[l + 1];
     }
+}
+
+// Opt the fused sweep in to more than 48 KB of dynamic shared memory.
+void init_kernel_attributes()
+{
+    cudaFuncSetAttribute(k_gs_rb_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double) * RBS_X * RBS_Y * RBS_Z));
+    cudaFuncSetAttribute(k_gs_rb_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(float) * RBS_X * RBS_Y * RBS_Z));
 }
 
 template <typename T>
@@ -278,7 +346,7 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
         {
             launch(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m * iters, k_gs_lex_cta<T>, dim3(1), dim3(1024), phi, rho, iters, H2, w);
         }
-        else if (alt.p)
+        else if (alt.p && m >= 64 && s->fused_rb)
         {
             // fused sweeps, ping-pong phi <-> alt (alt has phi's boundary values)
             dim3 grid((m + RBT_X - 1) / RBT_X, (m + RBT_Y - 1) / RBT_Y, (m + RBT_Z - 1) / RBT_Z);
@@ -287,7 +355,8 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
             for (int it = 0; it < iters; it++)
             {
                 launch_shm(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m, shm,
-                           k_gs_rb_tile<T>, grid, dim3(RBT_X, RBT_Y), a, b, rho, H2, w);
+                           k_gs_rb_tile<T>, grid, dim3(RB_THREADS_X, RB_THREADS_Y), a, b, rho,
+                           H2, w);
                 Grid<T> t = a;
                 a = b;
                 b = t;

@@ -54,14 +54,15 @@ def _step(args) -> dict:
     with core.Simulation(ic, args.lmin, precision=args.precision) as sim:
         sim.init_forces()
         sim.step(dt, 1)
-        core.profile_reset(sim)
-        core.profile_enable(sim, True)
         st0 = sim.stats()
         t0 = time.perf_counter()
-        sim.step(dt, args.steps)
+        sim.step(dt, args.steps)  # timed: CUDA graphs on, profiler off
         sim.synchronize()
         t = time.perf_counter() - t0
         st1 = sim.stats()
+        core.profile_reset(sim)  # separate profiled pass (per-launch events, no graphs)
+        core.profile_enable(sim, True)
+        sim.step(dt, args.steps)
         prof = core.profile_read(sim)
     kern = {c: {"launches": v[0], "ms": round(v[1], 4),
                 "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else 0.0}
