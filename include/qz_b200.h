@@ -74,6 +74,9 @@ typedef struct qz_config {
     int precision;      /* QZ_PREC_FP64 or QZ_PREC_MIXED */
     int inner_cycles;   /* mixed precision: FP32 V-cycles per FP64 correction */
     int force_stencil;  /* 0 = 3-point (only value supported) */
+    int ref_ptcl;       /* refine a cell holding >= ref_ptcl particles (ref_criterion_ptcl) */
+    int box_extra;      /* cells added to a child box on top of its smallest box
+                           (min_box_extra_size_per_side_real) */
 } qz_config;
 
 typedef struct qz_stats {
@@ -83,6 +86,9 @@ typedef struct qz_stats {
     long long kernel_launches; /* kernels this library launched since creation */
     long long steps;           /* completed qz_step steps */
     int error_flags;           /* device-side bounds / sanity flags seen (bit set) */
+    long long cg_iterations;   /* refinement-level conjugate-gradient iterations */
+    int levels;                /* refinement levels in the current tree (1 = head only) */
+    int nodes;                 /* nodes in the current tree, head included */
 } qz_stats;
 
 typedef struct qz_sim qz_sim;
@@ -98,7 +104,9 @@ typedef struct qz_sim qz_sim;
 #define QZ_PROF_GATHER 7     /* CIC force gather */
 #define QZ_PROF_LEAPFROG 8   /* kick-drift and kick */
 #define QZ_PROF_OTHER 9      /* boundary fill, copies, mixed-precision residual */
-#define QZ_PROF_CATEGORIES 10
+#define QZ_PROF_TREE 10      /* refinement tree: counts, flags, zones, children, lists */
+#define QZ_PROF_CG 11        /* refinement-node conjugate gradient */
+#define QZ_PROF_CATEGORIES 12
 
 /* Configuration with the reference defaults (global_variables.c:300-341). */
 QZ_API int qz_default_config(qz_config *cfg, int lmin);
@@ -137,6 +145,23 @@ QZ_API int qz_particle_updating_B(qz_sim *sim, double dt);
  * pot_old, then the residual test; pot_old <- pot when not converged.
  * *converged receives 1 or 0. */
 QZ_API int qz_poisson_error(qz_sim *sim, int *converged);
+
+/* tree_adaptation.c:8250-8590: rebuilds the refinement tree from the current
+ * positions with the construction rules of tree_construction.c (no-op when
+ * lmax == lmin). */
+QZ_API int qz_tree_adaptation(qz_sim *sim);
+
+/* Refinement-tree inspection (levels after the head exist when lmax > lmin).
+ * info receives 22 ints: lv, parent, box_ts[3], box_real_dim[3], box_min[3],
+ * box_max[3], cells, interior, boundary, sim-boundary grid points, particles,
+ * first child, children, touches the simulation boundary. */
+QZ_API int qz_amr_levels(qz_sim *sim);
+QZ_API int qz_amr_num_nodes(qz_sim *sim, int level);
+QZ_API int qz_amr_node_info(qz_sim *sim, int level, int node, int *info, double *mass);
+QZ_API int qz_amr_node_cells(qz_sim *sim, int level, int node, int *xyz);
+QZ_API int qz_amr_node_box(qz_sim *sim, int level, int node, int *out);
+QZ_API int qz_amr_node_list(qz_sim *sim, int level, int node, int which, int *out);
+QZ_API int qz_amr_node_field(qz_sim *sim, int level, int node, int which, double *out);
 
 /* Step 0 force computation (main.c:296-338) and whole leapfrog steps
  * (main.c:375-481 with a fixed dt). */

@@ -156,3 +156,32 @@ def run_reference(ic_path: str, out_dir: str, driver: str = REF_DRIVER, **kw) ->
 
 def read_dump(out_dir: str, step: int, name: str, dtype=np.float64) -> np.ndarray:
     return np.fromfile(os.path.join(out_dir, f"s{step}_{name}.bin"), dtype=dtype)
+
+
+def read_nodes(out_dir: str, step: int) -> list:
+    """Node summary written by the drivers for refinement runs: one dict per
+    node (tentacle level, index, geometry, list sizes, particles, mass, parent)."""
+    nodes = []
+    for line in open(os.path.join(out_dir, f"s{step}_nodes.txt")):
+        if line.startswith("#"):
+            continue
+        f = line.split()
+        v = [int(a) for a in f[:22]]
+        nodes.append({
+            "lv": v[0], "idx": v[1], "ID": v[2], "rd": tuple(v[3:6]), "ts": tuple(v[6:9]),
+            "bmin": tuple(v[9:12]), "bmax": tuple(v[12:15]), "ncells": v[15], "nintr": v[16],
+            "nbdry": v[17], "nsimb": v[18], "nptcl": v[19], "nptcl_outs": v[20],
+            "nchildren": v[21], "mass": float(f[22]), "parent_level": int(f[23]),
+            "parent": int(f[24]),
+        })
+    base = nodes[0]["lv"] if nodes else 0
+    for nd in nodes:
+        nd["level"] = nd["lv"] - base
+    return nodes
+
+
+def node_dump(out_dir: str, step: int, level: int, idx: int, what: str) -> np.ndarray:
+    """Per-node arrays: intr, bdry, simbdry, box, cells, cx, cy, cz (int32) or
+    pot, d, ax, ay, az (float64)."""
+    dt = np.int32 if what in ("intr", "bdry", "simbdry", "box", "cells", "cx", "cy", "cz") else np.float64
+    return read_dump(out_dir, step, f"L{level}_N{idx}_{what}", dt)

@@ -36,7 +36,8 @@ class Config(C.Structure):
         ("n_pre", C.c_int), ("n_post", C.c_int), ("n_coarse", C.c_int), ("w_sor", C.c_double),
         ("tol", C.c_double), ("tol2", C.c_double), ("check_every", C.c_int),
         ("max_iter", C.c_int), ("check_method", C.c_int), ("precision", C.c_int),
-        ("inner_cycles", C.c_int), ("force_stencil", C.c_int),
+        ("inner_cycles", C.c_int), ("force_stencil", C.c_int), ("ref_ptcl", C.c_int),
+        ("box_extra", C.c_int),
     ]
 
 
@@ -44,6 +45,7 @@ class Stats(C.Structure):
     _fields_ = [
         ("vcycles_total", C.c_longlong), ("last_vcycles", C.c_int), ("last_converged", C.c_int),
         ("kernel_launches", C.c_longlong), ("steps", C.c_longlong), ("error_flags", C.c_int),
+        ("cg_iterations", C.c_longlong), ("levels", C.c_int), ("nodes", C.c_int),
     ]
 
 
@@ -93,6 +95,15 @@ def load() -> C.CDLL:
         "qz_jacobi": ([_P, _P, C.c_int, C.c_int, C.c_double], C.c_int),
         "qz_multigrid": ([C.POINTER(Config), _P, _P, C.c_int, C.c_int], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
+        "qz_tree_adaptation": ([vp], C.c_int),
+        "qz_poisson_error": ([vp, _I], C.c_int),
+        "qz_amr_levels": ([vp], C.c_int),
+        "qz_amr_num_nodes": ([vp, C.c_int], C.c_int),
+        "qz_amr_node_info": ([vp, C.c_int, C.c_int, _I, _P], C.c_int),
+        "qz_amr_node_cells": ([vp, C.c_int, C.c_int, _I], C.c_int),
+        "qz_amr_node_box": ([vp, C.c_int, C.c_int, _I], C.c_int),
+        "qz_amr_node_list": ([vp, C.c_int, C.c_int, C.c_int, _I], C.c_int),
+        "qz_amr_node_field": ([vp, C.c_int, C.c_int, C.c_int, _P], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -209,6 +220,53 @@ class Simulation:
     def particle_updating_A(self, dt): _check(self.lib.qz_particle_updating_A(self.h, dt))
     def particle_updating_B(self, dt): _check(self.lib.qz_particle_updating_B(self.h, dt))
     def initial_potential_head(self): _check(self.lib.qz_initial_potential_head(self.h))
+
+    def tree_adaptation(self): _check(self.lib.qz_tree_adaptation(self.h))
+
+    # -- refinement tree -------------------------------------------------------------------
+    NODE_KEYS = ("lv", "parent", "ts", "rd", "bmin", "bmax", "ncells", "nintr", "nbdry",
+                 "nsimb", "nptcl", "zone_base", "nzones", "contact")
+
+    def levels(self) -> int:
+        return int(self.lib.qz_amr_levels(self.h))
+
+    def num_nodes(self, level: int) -> int:
+        return int(self.lib.qz_amr_num_nodes(self.h, level))
+
+    def node_info(self, level: int, node: int) -> dict:
+        info = np.zeros(22, dtype=np.int32)
+        mass = C.c_double()
+        _check(self.lib.qz_amr_node_info(self.h, level, node, _p(info), C.byref(mass)))
+        v = [int(a) for a in info]
+        return {"lv": v[0], "parent": v[1], "ts": tuple(v[2:5]), "rd": tuple(v[5:8]),
+                "bmin": tuple(v[8:11]), "bmax": tuple(v[11:14]), "ncells": v[14],
+                "nintr": v[15], "nbdry": v[16], "nsimb": v[17], "nptcl": v[18],
+                "zone_base": v[19], "nzones": v[20], "contact": v[21], "mass": mass.value}
+
+    def node_cells(self, level: int, node: int) -> np.ndarray:
+        n = self.node_info(level, node)["ncells"]
+        out = np.zeros(3 * n, dtype=np.int32)
+        _check(self.lib.qz_amr_node_cells(self.h, level, node, _p(out)))
+        return out.reshape(n, 3)
+
+    def node_box(self, level: int, node: int) -> np.ndarray:
+        rd = self.node_info(level, node)["rd"]
+        out = np.zeros(rd[0] * rd[1] * rd[2], dtype=np.int32)
+        _check(self.lib.qz_amr_node_box(self.h, level, node, _p(out)))
+        return out
+
+    def node_list(self, level: int, node: int, which: str) -> np.ndarray:
+        info = self.node_info(level, node)
+        k = {"intr": 0, "bdry": 1, "simb": 2}[which]
+        out = np.zeros(info[("nintr", "nbdry", "nsimb")[k]], dtype=np.int32)
+        _check(self.lib.qz_amr_node_list(self.h, level, node, k, _p(out)))
+        return out
+
+    def node_field(self, level: int, node: int, name: str) -> np.ndarray:
+        rd = self.node_info(level, node)["rd"]
+        out = np.zeros((rd[0] + 1) * (rd[1] + 1) * (rd[2] + 1))
+        _check(self.lib.qz_amr_node_field(self.h, level, node, FIELDS[name], _p(out)))
+        return out
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))

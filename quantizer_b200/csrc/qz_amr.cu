@@ -1,0 +1,1690 @@
+// qz_amr.cu -- the refinement tree and the per-level physics of refinement nodes.
+//
+// The tree is rebuilt on the device every step from the particle positions,
+// level by level from the head, with the reference's construction rules
+// (tree_construction.c:508-598, 685-926, 1032-2349):
+//   counts     particles per node cell
+//   flags      a cell holding >= ref_ptcl particles, and its 26 neighbours that
+//              belong to the same node, become "refine" (-1)
+//   zones      6-connected components of refine cells, numbered inside each node
+//              by the position of their first cell in the node's cell order
+//              (union-find that hooks the larger root under the smaller: every
+//              component ends rooted at its first cell, whatever the order in
+//              which the edges are processed)
+//   children   one node per zone: smallest box = twice the zone's bounding box,
+//              box padded by box_extra cells, cells = the 8 children of each
+//              zone cell in zone-cell order, box statuses -4 / -3 / -5
+//   grid       points classified interior / boundary / simulation boundary from
+//              the statuses of their 8 surrounding cells, listed in box order
+// The reference adapts the previous tree instead (tree_adaptation.c); on the
+// workloads checked the adapted tree equals the constructed one.  Zones smaller
+// than ref_ptcl particles (tree_construction.c:2350-2390) cannot occur with the
+// particle criterion: every zone holds a cell with >= ref_ptcl particles.
+//
+// Physics per refinement level (levels after the head, in order):
+//   deposit    grid_density.c:113-267 (weights in H units, 4 pi G / H^6)
+//   potential  potential_branches.c:93-332 (parent interpolation, analytic
+//              simulation boundary) and conjugate_gradient.c:322-463, with all
+//              nodes of a level in the same launches (per-node scalars, per-node
+//              convergence, fixed-order reductions)
+//   gradient   grid_acceleration.c:199-394 (analytic simulation boundary with the
+//              reference's y coordinate, boundary points from the parent's
+//              accelerations, 3-point interior)
+//   gather     particle_acceleration.c:134-355: every particle from the finest
+//              node whose cell holding it is not refined
+#include <algorithm>
+#include <climits>
+#include <string.h>
+
+#include "qz_internal.cuh"
+
+namespace qz {
+
+#define QZ_PI_D 3.14159265358979323846
+constexpr int AMR_MAX_LEVELS = 16;
+constexpr int CG_CHUNK = 2048;
+constexpr int CG_THREADS = 256;
+
+// ---- small device helpers --------------------------------------------------------------
+// Index of the last node whose offset (0: grid_off, 1: cls_off, 2: box_off) is <= v.
+__device__ __forceinline__ int find_node(const AmrNode *nodes, int nn, long v, int field)
+{
+    int lo = 0, hi = nn - 1;
+    while (lo < hi)
+    {
+        int mid = (lo + hi + 1) >> 1;
+        long off = field == 0 ? nodes[mid].grid_off : field == 1 ? nodes[mid].cls_off : nodes[mid].box_off;
+        if (off <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ long box_index(const AmrNode &N, int cx, int cy, int cz)
+{
+    return (long)(cx - N.ts[0]) + (long)(cy - N.ts[1]) * N.rd[0] +
+           (long)(cz - N.ts[2]) * N.rd[0] * N.rd[1];
+}
+
+__device__ __forceinline__ long grid_index(const AmrNode &N, int gx, int gy, int gz)
+{
+    // box grid coordinates (not level coordinates)
+    return N.grid_off + gx + (long)gy * (N.rd[0] + 1) + (long)gz * (N.rd[0] + 1) * (N.rd[1] + 1);
+}
+
+__device__ __forceinline__ void grid_coords(const AmrNode &N, long g, int *gx, int *gy, int *gz)
+{
+    long l = g - N.grid_off;
+    const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
+    *gz = (int)(l / sxy);
+    l -= (long)(*gz) * sxy;
+    *gy = (int)(l / sx);
+    *gx = (int)(l - (long)(*gy) * sx);
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0)
+    {
+        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+            r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;
+}
+
+// ---- tree: counts, flags, zones ------------------------------------------------------
+__global__ void k_fill_int(long n, int *a, int v)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = v;
+}
+
+__global__ void k_count(long n, const int *__restrict__ node_of, const AmrNode *__restrict__ nodes,
+                        const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, int *__restrict__ cnt, int *__restrict__ flags)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int nd = node_of[i];
+    if (nd < 0)
+        return;
+    const AmrNode N = nodes[nd];
+    const double sc = (double)(1 << N.lv);
+    int cx = (int)(x[i] * sc), cy = (int)(y[i] * sc), cz = (int)(z[i] * sc);
+    long b = box_index(N, cx, cy, cz);
+    if (b < 0 || b >= (long)N.rd[0] * N.rd[1] * N.rd[2])
+    {
+        atomicOr(&flags[F_ERROR], E_PTCL_OUTSIDE);
+        return;
+    }
+    atomicAdd(&cnt[N.box_off + b], 1);
+}
+
+__global__ void k_flag(int ncell, int ref_ptcl, const int *__restrict__ cell_box,
+                       const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
+                       const int *__restrict__ cnt, int *__restrict__ box)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell)
+        return;
+    long b = cell_box[c];
+    if (cnt[b] < ref_ptcl)
+        return;
+    const AmrNode N = nodes[cell_node[c]];
+    const long sy = N.rd[0], sz = (long)N.rd[0] * N.rd[1];
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++)
+            {
+                long nb = b + dx + dy * sy + dz * sz;
+                if (box[nb] == -3)
+                    box[nb] = -1; // every writer stores the same value
+            }
+}
+
+__global__ void k_cc_init(int ncell, const int *__restrict__ cell_box, const int *__restrict__ box,
+                          int *__restrict__ parent)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell)
+        return;
+    parent[c] = box[cell_box[c]] == -1 ? c : -1;
+}
+
+// Root of x; loads bypass L1 (parents change under concurrent hooking).
+__device__ __forceinline__ int cc_find(const int *parent, int x)
+{
+    int p = __ldcg(&parent[x]);
+    for (int guard = 0; p != x && guard < (1 << 20); guard++)
+    {
+        x = p;
+        p = __ldcg(&parent[x]);
+    }
+    return x;
+}
+
+__global__ void k_cc_hook(int ncell, const int *__restrict__ cell_box,
+                          const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
+                          const int *__restrict__ box, const int *__restrict__ pos_of_box,
+                          int *parent, int *__restrict__ flags)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell || parent[c] < 0)
+        return;
+    const AmrNode N = nodes[cell_node[c]];
+    const long b = cell_box[c];
+    const long off[6] = {1, -1, N.rd[0], -(long)N.rd[0], (long)N.rd[0] * N.rd[1],
+                         -(long)N.rd[0] * N.rd[1]};
+    for (int e = 0; e < 6; e++)
+    {
+        long nb = b + off[e];
+        if (box[nb] != -1)
+            continue;
+        int q = pos_of_box[nb];
+        if (q < 0)
+            continue;
+        int guard = 0;
+        for (; guard < (1 << 10); guard++)
+        {
+            int ra = cc_find(parent, c), rb = cc_find(parent, q);
+            if (ra == rb)
+                break;
+            if (ra < rb)
+            {
+                int t = ra;
+                ra = rb;
+                rb = t;
+            }
+            if (atomicCAS(&parent[ra], ra, rb) == ra)
+                break;
+        }
+        if (guard >= (1 << 10))
+            atomicOr(&flags[F_ERROR], 4);
+    }
+}
+
+__global__ void k_cc_roots(int ncell, const int *__restrict__ parent, int *__restrict__ is_root,
+                           int *__restrict__ flagged)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell)
+        return;
+    is_root[c] = parent[c] == c ? 1 : 0;
+    flagged[c] = parent[c] >= 0 ? 1 : 0;
+}
+
+__global__ void k_gather_at(int m, const int *__restrict__ src, const int *__restrict__ idx,
+                            int *__restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m)
+        out[i] = src[idx[i]];
+}
+
+__global__ void k_zone_box_init(int nz, int *zone_box, int *zone_cells)
+{
+    int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz)
+        return;
+    for (int q = 0; q < 3; q++)
+    {
+        zone_box[6 * z + q] = INT_MAX;
+        zone_box[6 * z + 3 + q] = INT_MIN;
+    }
+    zone_cells[z] = 0;
+}
+
+// Zone ids: zrank (exclusive scan of roots over the level's cells) is the
+// child index of each root in the next level; inside a node the zone id is
+// the rank minus the node's first rank.  Statuses of refine cells become zone
+// ids, and refine cells are written in cell order to (zone, cell) pairs.
+__global__ void k_cc_label(int ncell, const int *__restrict__ cell_box,
+                           const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
+                           const int *parent, const int *__restrict__ zrank,
+                           const int *__restrict__ slot, int *__restrict__ box,
+                           int *__restrict__ zone_box, int *__restrict__ zone_cells,
+                           const int *__restrict__ cell_xyz, unsigned *__restrict__ key,
+                           int *__restrict__ val)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell || parent[c] < 0)
+        return;
+    int r = cc_find(parent, c);
+    int zg = zrank[r];
+    const AmrNode N = nodes[cell_node[c]];
+    box[cell_box[c]] = zg - N.zone_base;
+    atomicMin(&zone_box[6 * zg + 0], cell_xyz[3 * c + 0]);
+    atomicMin(&zone_box[6 * zg + 1], cell_xyz[3 * c + 1]);
+    atomicMin(&zone_box[6 * zg + 2], cell_xyz[3 * c + 2]);
+    atomicMax(&zone_box[6 * zg + 3], cell_xyz[3 * c + 0]);
+    atomicMax(&zone_box[6 * zg + 4], cell_xyz[3 * c + 1]);
+    atomicMax(&zone_box[6 * zg + 5], cell_xyz[3 * c + 2]);
+    atomicAdd(&zone_cells[zg], 1);
+    key[slot[c]] = (unsigned)zg;
+    val[slot[c]] = c;
+}
+
+__global__ void k_set_zone_base(int nn, AmrNode *nodes, const int *__restrict__ zrank, int nz)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nn)
+        return;
+    int b = zrank[nodes[q].cell_off];
+    int e = q + 1 < nn ? zrank[nodes[q + 1].cell_off] : nz;
+    nodes[q].zone_base = b;
+    nodes[q].nzones = e - b;
+}
+
+// Children: the j-th cell of zone z (cell order) spawns child cells
+// 8 j + (ii + 2 jj + 4 kk) of child node z (tree_construction.c:1634-1671).
+__global__ void k_child_cells(int nzc, const unsigned *__restrict__ zkey,
+                              const int *__restrict__ zval, const int *__restrict__ zone_start,
+                              const int *__restrict__ pcell_xyz, const AmrNode *__restrict__ cn,
+                              int *__restrict__ cell_box, int *__restrict__ cell_xyz,
+                              int *__restrict__ cell_node)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nzc)
+        return;
+    int z = (int)zkey[q];
+    int pc = zval[q];
+    int j = q - zone_start[z];
+    const AmrNode N = cn[z];
+    int px = 2 * pcell_xyz[3 * pc], py = 2 * pcell_xyz[3 * pc + 1], pz = 2 * pcell_xyz[3 * pc + 2];
+    for (int sub = 0; sub < 8; sub++)
+    {
+        int ii = sub & 1, jj = (sub >> 1) & 1, kk = sub >> 2;
+        int c = N.cell_off + 8 * j + sub;
+        int cx = px + ii, cy = py + jj, cz = pz + kk;
+        cell_xyz[3 * c] = cx;
+        cell_xyz[3 * c + 1] = cy;
+        cell_xyz[3 * c + 2] = cz;
+        cell_box[c] = (int)(N.box_off + box_index(N, cx, cy, cz));
+        cell_node[c] = z;
+    }
+}
+
+__global__ void k_box_cells(int ncell, const int *__restrict__ cell_box, int *__restrict__ box,
+                            int *__restrict__ pos_of_box)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell)
+        return;
+    box[cell_box[c]] = -3;
+    pos_of_box[cell_box[c]] = c;
+}
+
+// Cells beyond the simulation box of a node that touches it (tree_construction.c:1745-1841).
+__global__ void k_box_simb(long total, int nn, const AmrNode *__restrict__ nodes,
+                           int *__restrict__ box)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total)
+        return;
+    const AmrNode N = nodes[find_node(nodes, nn, t, 2)];
+    if (!N.contact)
+        return;
+    long l = t - N.box_off;
+    int i = (int)(l % N.rd[0]), j = (int)((l / N.rd[0]) % N.rd[1]),
+        k = (int)(l / ((long)N.rd[0] * N.rd[1]));
+    const int top = 1 << N.lv;
+    const int g[3] = {i + N.ts[0], j + N.ts[1], k + N.ts[2]};
+    bool outside = false;
+    for (int a = 0; a < 3; a++)
+    {
+        if (N.bmin[a] == 0 && g[a] < 0)
+            outside = true;
+        if (N.bmax[a] == top - 1 && g[a] >= top)
+            outside = true;
+    }
+    if (outside)
+        box[t] = -5;
+}
+
+// Grid-point category from the 8 cells around the point (tree_construction.c:1935-2107):
+// 0 none, 1 interior, 2 boundary, 3 simulation boundary.
+__device__ __forceinline__ int classify_point(const int *box, long b, long sy, long sz, int gx,
+                                              int gy, int gz, int top, int contact)
+{
+    auto in = [&](long off) { return box[b + off] > -4; };
+    const bool c000 = in(0), c100 = in(-1), c010 = in(-sy), c110 = in(-1 - sy), c001 = in(-sz),
+               c101 = in(-1 - sz), c011 = in(-sy - sz), c111 = in(-1 - sy - sz);
+    bool bder = false;
+    if (c000)
+        bder = (!c100 && !c110 && !c101 && !c111) || (!c010 && !c110 && !c011 && !c111) ||
+               (!c001 && !c101 && !c011 && !c111);
+    else if (c100)
+        bder = (!c010 && !c001 && !c011) || (!c010 && !c110 && !c011 && !c111) ||
+               (!c001 && !c101 && !c011 && !c111);
+    else if (c010)
+        bder = (!c110 && !c101 && !c111) || (!c001 && !c101) || (!c001 && !c101 && !c011 && !c111);
+    else if (c110)
+        bder = (!c001 && !c011) || (!c001 && !c101) || (!c001 && !c101 && !c011 && !c111);
+    else if (c001 || c101 || c011 || c111)
+        bder = true;
+    else
+        return 0;
+    if (contact && bder && (gx == 0 || gx == top || gy == 0 || gy == top || gz == 0 || gz == top))
+        return 3;
+    return bder ? 2 : 1;
+}
+
+// Per node, the box grid points [bmin - ts, bmax - ts + 1]^3 in box order; fl
+// holds three flag arrays (interior | boundary | simulation boundary).
+__global__ void k_classify(long total, int nn, const AmrNode *__restrict__ nodes,
+                           const int *__restrict__ box, int *__restrict__ fl)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total)
+        return;
+    const AmrNode N = nodes[find_node(nodes, nn, t, 1)];
+    const int ex = N.bmax[0] - N.bmin[0] + 2, ey = N.bmax[1] - N.bmin[1] + 2;
+    long l = t - N.cls_off;
+    int ii = N.bmin[0] - N.ts[0] + (int)(l % ex);
+    int jj = N.bmin[1] - N.ts[1] + (int)((l / ex) % ey);
+    int kk = N.bmin[2] - N.ts[2] + (int)(l / ((long)ex * ey));
+    const long sy = N.rd[0], sz = (long)N.rd[0] * N.rd[1];
+    long b = N.box_off + ii + jj * sy + kk * sz;
+    int cat = classify_point(box, b, sy, sz, ii + N.ts[0], jj + N.ts[1], kk + N.ts[2], 1 << N.lv,
+                             N.contact);
+    fl[t] = cat == 1;
+    fl[total + t] = cat == 2;
+    fl[2 * total + t] = cat == 3;
+}
+
+__global__ void k_lists(long total, int nn, const AmrNode *__restrict__ nodes,
+                        const int *__restrict__ fl, const int *__restrict__ pos, int base1,
+                        int base2, int *__restrict__ intr, int *__restrict__ bdry,
+                        int *__restrict__ simb, int *__restrict__ intr_node,
+                        int *__restrict__ bdry_node, int *__restrict__ simb_node)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total)
+        return;
+    int cat = fl[t] ? 0 : fl[total + t] ? 1 : fl[2 * total + t] ? 2 : -1;
+    if (cat < 0)
+        return;
+    int nd = find_node(nodes, nn, t, 1);
+    const AmrNode N = nodes[nd];
+    const int ex = N.bmax[0] - N.bmin[0] + 2, ey = N.bmax[1] - N.bmin[1] + 2;
+    long l = t - N.cls_off;
+    int ii = N.bmin[0] - N.ts[0] + (int)(l % ex);
+    int jj = N.bmin[1] - N.ts[1] + (int)((l / ex) % ey);
+    int kk = N.bmin[2] - N.ts[2] + (int)(l / ((long)ex * ey));
+    int g = (int)grid_index(N, ii, jj, kk);
+    int p = pos[cat * total + t];
+    if (cat == 0)
+    {
+        intr[p] = g;
+        intr_node[p] = nd;
+    }
+    else if (cat == 1)
+    {
+        bdry[p - base1] = g;
+        bdry_node[p - base1] = nd;
+    }
+    else
+    {
+        simb[p - base2] = g;
+        simb_node[p - base2] = nd;
+    }
+}
+
+// Node of every particle one level down: the zone of its cell, if refined.
+__global__ void k_next_node(long n, const int *__restrict__ node_of, const AmrNode *__restrict__ nodes,
+                            const int *__restrict__ box, const double *__restrict__ x,
+                            const double *__restrict__ y, const double *__restrict__ z,
+                            int *__restrict__ next)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int nd = node_of[i];
+    int out = -1;
+    if (nd >= 0)
+    {
+        const AmrNode N = nodes[nd];
+        const double sc = (double)(1 << N.lv);
+        int cx = (int)(x[i] * sc), cy = (int)(y[i] * sc), cz = (int)(z[i] * sc);
+        int st = box[N.box_off + box_index(N, cx, cy, cz)];
+        if (st >= 0)
+            out = N.zone_base + st;
+    }
+    next[i] = out;
+}
+
+// ---- host helpers ---------------------------------------------------------------------
+static bool ensure_small(qz_sim *s, long need)
+{
+    if (need <= s->h_small_cap)
+        return true;
+    if (s->h_small)
+        cudaFreeHost(s->h_small);
+    s->h_small = nullptr;
+    s->h_small_cap = 0;
+    long nc = std::max(need, 4096L);
+    if (!check_cuda(cudaMallocHost((void **)&s->h_small, nc * sizeof(int)), "pinned small"))
+        return false;
+    s->h_small_cap = nc;
+    return true;
+}
+
+// Stream-ordered read-back of `count` ints (synchronises).
+static bool read_ints(qz_sim *s, const int *dsrc, long count, int *out)
+{
+    if (count <= 0)
+        return true;
+    if (!ensure_small(s, count))
+        return false;
+    if (!check_cuda(cudaMemcpyAsync(s->h_small, dsrc, count * sizeof(int), cudaMemcpyDeviceToHost,
+                                    s->stream),
+                    "read back") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "read back sync"))
+        return false;
+    memcpy(out, s->h_small, count * sizeof(int));
+    return true;
+}
+
+// Reads src[idx[q]] for the host index list idx (one launch, one read-back).
+static bool read_at(qz_sim *s, const int *dsrc, const std::vector<int> &idx, int *out)
+{
+    const int m = (int)idx.size();
+    if (m == 0)
+        return true;
+    if (!s->gather_idx.ensure(2L * m) || !ensure_small(s, m))
+    {
+        set_error("gather buffer");
+        return false;
+    }
+    memcpy(s->h_small, idx.data(), m * sizeof(int));
+    if (!check_cuda(cudaMemcpyAsync(s->gather_idx.p, s->h_small, m * sizeof(int),
+                                    cudaMemcpyHostToDevice, s->stream),
+                    "gather h2d"))
+        return false;
+    launch(s, QZ_PROF_TREE, 12.0 * m, k_gather_at, dim3(blocks_for(m, 256)), dim3(256), m, dsrc,
+           s->gather_idx.p, s->gather_idx.p + m);
+    return read_ints(s, s->gather_idx.p + m, m, out);
+}
+
+static bool upload_nodes(qz_sim *s, AmrLevel &L)
+{
+    if (!L.nodes.ensure(std::max(L.nnodes, 1)))
+    {
+        set_error("amr nodes");
+        return false;
+    }
+    return L.nnodes == 0 ||
+           check_cuda(cudaMemcpyAsync(L.nodes.p, L.h.data(), L.nnodes * sizeof(AmrNode),
+                                      cudaMemcpyHostToDevice, s->stream),
+                      "amr nodes h2d");
+}
+
+static void free_level(AmrLevel &L)
+{
+    DBuf<int> *ib[] = {&L.box, &L.cnt, &L.pos_of_box, &L.cell_seg, &L.cell_box, &L.cell_xyz,
+                       &L.cell_node, &L.intr, &L.bdry, &L.simb, &L.intr_node, &L.bdry_node,
+                       &L.simb_node, &L.nint};
+    for (auto *b : ib)
+        b->release();
+    DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
+                          &L.nscal, &L.chunk_part};
+    for (auto *b : db)
+        b->release();
+    L.nodes.release();
+    L.chunks.release();
+    L = AmrLevel();
+}
+
+void amr_free(qz_sim *s)
+{
+    for (auto &L : s->amr)
+        free_level(L);
+    s->amr.clear();
+    for (auto &b : s->node_of)
+        b.release();
+    s->node_of.clear();
+    s->amr_tmp.release();
+    s->amr_tmp2.release();
+    s->zone_box.release();
+    s->zone_cells.release();
+    s->gather_idx.release();
+    s->seg_mass.release();
+    if (s->h_small)
+        cudaFreeHost(s->h_small);
+    s->h_small = nullptr;
+    s->h_small_cap = 0;
+}
+
+// Level 0: the head node over the head fields and the (2^L+2)^3 head box.
+int amr_init(qz_sim *s)
+{
+    const int levels = s->cfg.lmax - s->cfg.lmin + 1;
+    if (levels > AMR_MAX_LEVELS)
+    {
+        set_error("at most %d refinement levels", AMR_MAX_LEVELS - 1);
+        return QZ_FAILURE;
+    }
+    s->amr.assign(levels, AmrLevel());
+    s->node_of.assign(levels, DBuf<int>());
+    for (int l = 0; l < levels; l++)
+        if (!s->node_of[l].ensure(s->cap))
+        {
+            set_error("node_of");
+            return QZ_FAILURE;
+        }
+    AmrLevel &H = s->amr[0];
+    const int L = s->L, nc = 1 << L, B = nc + 2;
+    AmrNode h{};
+    h.lv = L;
+    h.parent = -1;
+    for (int a = 0; a < 3; a++)
+    {
+        h.ts[a] = -1;
+        h.rd[a] = B;
+        h.bmin[a] = 0;
+        h.bmax[a] = nc - 1;
+    }
+    h.ncells = nc * nc * nc;
+    h.contact = 1;
+    h.mass = s->cfg.total_mass;
+    H.nnodes = 1;
+    H.h.assign(1, h);
+    H.box_total = (long)B * B * B;
+    H.grid_total = s->gpts;
+    H.cell_total = h.ncells;
+    H.pot = s->pot;
+    H.pot_old = s->pot_old;
+    H.d = s->d;
+    H.ax = s->gax;
+    H.ay = s->gay;
+    H.az = s->gaz;
+    if (!upload_nodes(s, H) || !H.box.ensure(H.box_total) || !H.cnt.ensure(H.box_total) ||
+        !H.pos_of_box.ensure(H.box_total) || !H.cell_box.ensure(H.cell_total) ||
+        !H.cell_xyz.ensure(3L * H.cell_total) || !H.cell_node.ensure(H.cell_total))
+    {
+        set_error("head tree buffers");
+        return QZ_FAILURE;
+    }
+    // head cells in the reference's order (initialization.c:126-142): i fastest
+    std::vector<int> cb(H.cell_total), cx(3L * H.cell_total), pb(H.box_total, -1);
+    for (int k = 0; k < nc; k++)
+        for (int j = 0; j < nc; j++)
+            for (int i = 0; i < nc; i++)
+            {
+                int c = i + j * nc + k * nc * nc;
+                int b = (i + 1) + (j + 1) * B + (k + 1) * B * B;
+                cb[c] = b;
+                cx[3 * c] = i;
+                cx[3 * c + 1] = j;
+                cx[3 * c + 2] = k;
+                pb[b] = c;
+            }
+    bool ok = check_cuda(cudaMemcpy(H.cell_box.p, cb.data(), cb.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice), "head cells") &&
+              check_cuda(cudaMemcpy(H.cell_xyz.p, cx.data(), cx.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice), "head cells") &&
+              check_cuda(cudaMemcpy(H.pos_of_box.p, pb.data(), pb.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice), "head pos") &&
+              check_cuda(cudaMemset(H.cell_node.p, 0, H.cell_total * sizeof(int)), "head cells") &&
+              check_cuda(cudaDeviceSynchronize(), "head tree init");
+    return ok ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+static bool ensure_sort(qz_sim *s, long need)
+{
+    Sort &S = s->sort;
+    if (need <= S.cap)
+        return true;
+    long tiles = radix_tiles(need);
+    void *ps[] = {S.k0, S.k1, S.v0, S.v1, S.hist};
+    for (void *p : ps)
+        if (p)
+            cudaFree(p);
+    S.k0 = S.k1 = nullptr;
+    S.v0 = S.v1 = S.hist = nullptr;
+    bool ok = check_cuda(cudaMalloc(&S.k0, need * sizeof(unsigned)), "sort") &&
+              check_cuda(cudaMalloc(&S.k1, need * sizeof(unsigned)), "sort") &&
+              check_cuda(cudaMalloc(&S.v0, need * sizeof(int)), "sort") &&
+              check_cuda(cudaMalloc(&S.v1, need * sizeof(int)), "sort") &&
+              check_cuda(cudaMalloc(&S.hist, 256L * tiles * sizeof(int)), "sort");
+    S.cap = ok ? need : 0;
+    S.tiles_cap = ok ? tiles : 0;
+    return ok;
+}
+
+// Rebuilds the tree below the head from the current positions.
+int amr_build(qz_sim *s)
+{
+    const long n = s->n;
+    const int levels = (int)s->amr.size();
+    AmrLevel &H = s->amr[0];
+    // head statuses (initialization.c:95-110): -5 on the ghost ring, -3 inside
+    launch(s, QZ_PROF_TREE, 4.0 * H.box_total, k_fill_int, dim3(blocks_for(H.box_total, 256)),
+           dim3(256), H.box_total, H.box.p, -5);
+    launch(s, QZ_PROF_TREE, 8.0 * H.cell_total, k_box_cells, dim3(blocks_for(H.cell_total, 256)),
+           dim3(256), H.cell_total, H.cell_box.p, H.box.p, H.pos_of_box.p);
+    cudaMemsetAsync(s->node_of[0].p, 0, (n > 0 ? n : 1) * sizeof(int), s->stream);
+    s->amr_nlev = 1;
+    for (int l = 1; l < levels; l++)
+        s->amr[l].nnodes = 0;
+    for (int l = 0; l + 1 < levels; l++)
+    {
+        AmrLevel &P = s->amr[l];
+        if (P.nnodes == 0)
+            break;
+        cudaMemsetAsync(P.cnt.p, 0, P.box_total * sizeof(int), s->stream);
+        if (n > 0)
+            launch(s, QZ_PROF_TREE, 28.0 * n, k_count, dim3(blocks_for(n, 256)), dim3(256), n,
+                   s->node_of[l].p, P.nodes.p, s->x, s->y, s->z, P.cnt.p, s->flags);
+        const int nc = P.cell_total;
+        launch(s, QZ_PROF_TREE, 12.0 * nc, k_flag, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               s->cfg.ref_ptcl, P.cell_box.p, P.cell_node.p, P.nodes.p, P.cnt.p, P.box.p);
+        // union-find over the refine cells: parent | is_root | zone rank | flagged | slot
+        if (!s->amr_tmp.ensure(5L * nc + 8))
+        {
+            set_error("amr scratch");
+            return QZ_FAILURE;
+        }
+        int *parent = s->amr_tmp.p, *isroot = parent + nc, *zrank = isroot + nc,
+            *flagged = zrank + nc, *slot = flagged + nc;
+        launch(s, QZ_PROF_TREE, 8.0 * nc, k_cc_init, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               P.cell_box.p, P.box.p, parent);
+        launch(s, QZ_PROF_TREE, 32.0 * nc, k_cc_hook, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               P.cell_box.p, P.cell_node.p, P.nodes.p, P.box.p, P.pos_of_box.p, parent,
+               s->flags);
+        launch(s, QZ_PROF_TREE, 12.0 * nc, k_cc_roots, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               parent, isroot, flagged);
+        if (scan_exclusive(s, isroot, zrank, nc) || scan_exclusive(s, flagged, slot, nc))
+            return QZ_FAILURE;
+        // zones = last rank + last root flag; refine cells = last slot + last flag
+        int t[4];
+        if (!read_at(s, parent, {2 * nc + nc - 1, nc + nc - 1, 4 * nc + nc - 1, 3 * nc + nc - 1}, t))
+            return QZ_FAILURE;
+        const int nz = t[0] + t[1], nzc = t[2] + t[3];
+        if (nz == 0)
+        {
+            for (auto &nd : P.h)
+                nd.zone_base = nd.nzones = 0;
+            upload_nodes(s, P);
+            break;
+        }
+        if (!s->zone_box.ensure(6L * nz) || !s->zone_cells.ensure(nz) || !ensure_sort(s, nzc))
+        {
+            set_error("zone buffers");
+            return QZ_FAILURE;
+        }
+        launch(s, QZ_PROF_TREE, 4.0 * P.nnodes, k_set_zone_base, dim3(blocks_for(P.nnodes, 128)),
+               dim3(128), P.nnodes, P.nodes.p, zrank, nz);
+        launch(s, QZ_PROF_TREE, 28.0 * nz, k_zone_box_init, dim3(blocks_for(nz, 256)), dim3(256),
+               nz, s->zone_box.p, s->zone_cells.p);
+        launch(s, QZ_PROF_TREE, 48.0 * nc, k_cc_label, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               P.cell_box.p, P.cell_node.p, P.nodes.p, parent, zrank, slot, P.box.p,
+               s->zone_box.p, s->zone_cells.p, P.cell_xyz.p, s->sort.k0, s->sort.v0);
+        // zone cells in (zone, cell position) order: a stable sort on the zone id
+        int zbits = 1;
+        while ((1L << zbits) < nz)
+            zbits++;
+        unsigned *zk;
+        int *zv;
+        if (radix_sort_pairs(s, nzc, zbits, &zk, &zv))
+            return QZ_FAILURE;
+        std::vector<int> zbox(6L * nz), zcells(nz);
+        std::vector<AmrNode> pnodes(P.nnodes);
+        if (!read_ints(s, s->zone_box.p, 6L * nz, zbox.data()) ||
+            !read_ints(s, s->zone_cells.p, nz, zcells.data()) ||
+            !check_cuda(cudaMemcpyAsync(pnodes.data(), P.nodes.p, P.nnodes * sizeof(AmrNode),
+                                        cudaMemcpyDeviceToHost, s->stream), "nodes d2h") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "nodes d2h sync"))
+            return QZ_FAILURE;
+        for (int q = 0; q < P.nnodes; q++)
+        {
+            P.h[q].zone_base = pnodes[q].zone_base;
+            P.h[q].nzones = pnodes[q].nzones;
+        }
+        // ---- child level geometry (host) ---------------------------------------------
+        AmrLevel &C = s->amr[l + 1];
+        C.nnodes = nz;
+        C.h.assign(nz, AmrNode());
+        long box_total = 0, grid_total = 0, cls_total = 0;
+        int cell_total = 0;
+        const int clv = P.h[0].lv + 1;
+        const int top = 1 << clv;
+        std::vector<int> zstart(nz);
+        for (int q = 0; q < P.nnodes; q++)
+            for (int zz = 0; zz < P.h[q].nzones; zz++)
+            {
+                const int z = P.h[q].zone_base + zz;
+                AmrNode &N = C.h[z];
+                N.lv = clv;
+                N.parent = q;
+                for (int a = 0; a < 3; a++)
+                {
+                    N.bmin[a] = 2 * zbox[6 * z + a];
+                    N.bmax[a] = 2 * zbox[6 * z + 3 + a] + 1;
+                    const int dim = N.bmax[a] - N.bmin[a] + 1;
+                    N.rd[a] = dim + s->cfg.box_extra;
+                    N.ts[a] = N.bmin[a] - (N.rd[a] - dim) / 2;
+                    if (N.bmin[a] == 0 || N.bmax[a] == top - 1)
+                        N.contact = 1;
+                }
+                N.box_off = box_total;
+                box_total += (long)N.rd[0] * N.rd[1] * N.rd[2];
+                N.grid_off = grid_total;
+                grid_total += (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
+                zstart[z] = cell_total / 8;
+                N.cell_off = cell_total;
+                N.ncells = 8 * zcells[z];
+                cell_total += N.ncells;
+                N.cls_off = cls_total;
+                cls_total += (long)(N.bmax[0] - N.bmin[0] + 2) * (N.bmax[1] - N.bmin[1] + 2) *
+                             (N.bmax[2] - N.bmin[2] + 2);
+            }
+        C.box_total = box_total;
+        C.grid_total = grid_total;
+        C.cell_total = cell_total;
+        C.cls_total = cls_total;
+        if (!C.box.ensure(box_total) || !C.cnt.ensure(box_total) ||
+            !C.pos_of_box.ensure(box_total) || !C.cell_box.ensure(cell_total) ||
+            !C.cell_xyz.ensure(3L * cell_total) || !C.cell_node.ensure(cell_total) ||
+            !s->amr_tmp2.ensure(std::max((long)nz, 6L * cls_total + 8)))
+        {
+            set_error("child level buffers");
+            return QZ_FAILURE;
+        }
+        if (!upload_nodes(s, C))
+            return QZ_FAILURE;
+        int *dzstart = s->amr_tmp2.p;
+        if (!ensure_small(s, nz))
+            return QZ_FAILURE;
+        memcpy(s->h_small, zstart.data(), nz * sizeof(int));
+        if (!check_cuda(cudaMemcpyAsync(dzstart, s->h_small, nz * sizeof(int),
+                                        cudaMemcpyHostToDevice, s->stream),
+                        "zone start") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "zone start sync"))
+            return QZ_FAILURE;
+        launch(s, QZ_PROF_TREE, 40.0 * nzc, k_child_cells, dim3(blocks_for(nzc, 256)), dim3(256),
+               nzc, zk, zv, dzstart, P.cell_xyz.p, C.nodes.p, C.cell_box.p, C.cell_xyz.p,
+               C.cell_node.p);
+        launch(s, QZ_PROF_TREE, 4.0 * box_total, k_fill_int, dim3(blocks_for(box_total, 256)),
+               dim3(256), box_total, C.box.p, -4);
+        launch(s, QZ_PROF_TREE, 4.0 * box_total, k_fill_int, dim3(blocks_for(box_total, 256)),
+               dim3(256), box_total, C.pos_of_box.p, -1);
+        launch(s, QZ_PROF_TREE, 8.0 * cell_total, k_box_cells, dim3(blocks_for(cell_total, 256)),
+               dim3(256), cell_total, C.cell_box.p, C.box.p, C.pos_of_box.p);
+        launch(s, QZ_PROF_TREE, 4.0 * box_total, k_box_simb, dim3(blocks_for(box_total, 256)),
+               dim3(256), box_total, C.nnodes, C.nodes.p, C.box.p);
+        // grid-point lists
+        int *fl = s->amr_tmp2.p, *pos = fl + 3 * cls_total;
+        launch(s, QZ_PROF_TREE, 32.0 * cls_total, k_classify, dim3(blocks_for(cls_total, 256)),
+               dim3(256), cls_total, C.nnodes, C.nodes.p, C.box.p, fl);
+        if (scan_exclusive(s, fl, pos, 3 * cls_total))
+            return QZ_FAILURE;
+        // scan values at every node's range start in each category, and the totals
+        std::vector<int> idx;
+        for (int cat = 0; cat < 3; cat++)
+            for (int q = 0; q < nz; q++)
+                idx.push_back((int)(cat * cls_total + C.h[q].cls_off));
+        idx.push_back((int)(3 * cls_total - 1));
+        std::vector<int> sv(idx.size()), lastf(1);
+        if (!read_at(s, pos, idx, sv.data()) || !read_at(s, fl, {(int)(3 * cls_total - 1)}, lastf.data()))
+            return QZ_FAILURE;
+        const int total_all = sv.back() + lastf[0];
+        auto start = [&](int cat, int q) {
+            if (q < nz)
+                return sv[cat * nz + q];
+            return cat < 2 ? sv[(cat + 1) * nz] : total_all;
+        };
+        C.intr_total = start(0, nz) - start(0, 0);
+        C.bdry_total = start(1, nz) - start(1, 0);
+        C.simb_total = start(2, nz) - start(2, 0);
+        for (int q = 0; q < nz; q++)
+        {
+            AmrNode &N = C.h[q];
+            N.intr_off = start(0, q) - start(0, 0);
+            N.nintr = start(0, q + 1) - start(0, q);
+            N.bdry_off = start(1, q) - start(1, 0);
+            N.nbdry = start(1, q + 1) - start(1, q);
+            N.simb_off = start(2, q) - start(2, 0);
+            N.nsimb = start(2, q + 1) - start(2, q);
+            N.zone_base = N.nzones = 0;
+        }
+        if (!C.intr.ensure(C.intr_total) || !C.intr_node.ensure(C.intr_total) ||
+            !C.bdry.ensure(C.bdry_total) || !C.bdry_node.ensure(C.bdry_total) ||
+            !C.simb.ensure(C.simb_total) || !C.simb_node.ensure(C.simb_total))
+        {
+            set_error("grid lists");
+            return QZ_FAILURE;
+        }
+        launch(s, QZ_PROF_TREE, 24.0 * cls_total, k_lists, dim3(blocks_for(cls_total, 256)),
+               dim3(256), cls_total, C.nnodes, C.nodes.p, fl, pos, start(1, 0), start(2, 0),
+               C.intr.p, C.bdry.p, C.simb.p, C.intr_node.p, C.bdry_node.p, C.simb_node.p);
+        if (!upload_nodes(s, C))
+            return QZ_FAILURE;
+        if (n > 0)
+            launch(s, QZ_PROF_TREE, 36.0 * n, k_next_node, dim3(blocks_for(n, 256)), dim3(256), n,
+                   s->node_of[l].p, P.nodes.p, P.box.p, s->x, s->y, s->z, s->node_of[l + 1].p);
+        s->amr_nlev = l + 2;
+        if (!check_cuda(cudaGetLastError(), "amr build"))
+            return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+
+// ---- deposit on refinement levels ------------------------------------------------------
+__global__ void k_lvl_keys(long n, const int *__restrict__ node_of, const AmrNode *__restrict__ nodes,
+                           const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, const int *__restrict__ slot,
+                           unsigned *__restrict__ keys, int *__restrict__ vals)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int nd = node_of[i];
+    if (nd < 0)
+        return;
+    const AmrNode N = nodes[nd];
+    const double sc = (double)(1 << N.lv);
+    int cx = (int)(x[i] * sc), cy = (int)(y[i] * sc), cz = (int)(z[i] * sc);
+    keys[slot[i]] = (unsigned)(N.box_off + box_index(N, cx, cy, cz));
+    vals[slot[i]] = (int)i;
+}
+
+__global__ void k_in_level(long n, const int *__restrict__ node_of, int *__restrict__ flag)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        flag[i] = node_of[i] >= 0 ? 1 : 0;
+}
+
+// One warp per occupied cell: CIC corner sums with the branch weights
+// (grid_density.c:166-245): w1 = x - H floor(x / H), w2 = H - w1, times
+// 4 pi G m / H^6; plus the cell's mass.
+__global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ perm,
+                                 const int *__restrict__ seg_start, const int *__restrict__ flags,
+                                 const double *__restrict__ x, const double *__restrict__ y,
+                                 const double *__restrict__ z, const double *__restrict__ m,
+                                 double *__restrict__ cs, double *__restrict__ smass)
+{
+    const int lane = threadIdx.x & 31;
+    const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    const int nseg = flags[F_NSEG];
+    const double H = 1.0 / (1 << lv);
+    const double ooh = (double)(1 << lv);
+    for (long sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const int b = seg_start[sg], e = seg_start[sg + 1];
+        double acc[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++)
+            acc[c] = 0.0;
+        for (int q = b + lane; q < e; q += 32)
+        {
+            const int i = perm[q];
+            int fx = (int)(x[i] * ooh), fy = (int)(y[i] * ooh), fz = (int)(z[i] * ooh);
+            double wx1 = x[i] - H * fx, wy1 = y[i] - H * fy, wz1 = z[i] - H * fz;
+            double wx2 = H - wx1, wy2 = H - wy1, wz2 = H - wz1;
+            double cm = coeff * m[i];
+            acc[0] += cm * (wx2 * wy2 * wz2);
+            acc[1] += cm * (wx1 * wy2 * wz2);
+            acc[2] += cm * (wx2 * wy1 * wz2);
+            acc[3] += cm * (wx1 * wy1 * wz2);
+            acc[4] += cm * (wx2 * wy2 * wz1);
+            acc[5] += cm * (wx1 * wy2 * wz1);
+            acc[6] += cm * (wx2 * wy1 * wz1);
+            acc[7] += cm * (wx1 * wy1 * wz1);
+            acc[8] += m[i];
+        }
+#pragma unroll
+        for (int c = 0; c < 9; c++)
+        {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1)
+                v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc[c] = v;
+        }
+        if (lane < 8)
+        {
+            double v = acc[0];
+#pragma unroll
+            for (int c = 1; c < 8; c++)
+                if (lane == c)
+                    v = acc[c];
+            cs[sg * 8 + lane] = v;
+        }
+        if (lane == 0)
+            smass[sg] = acc[8];
+    }
+}
+
+__global__ void k_lvl_point_gather(long total, int nn, const AmrNode *__restrict__ nodes,
+                                   const int *__restrict__ cell_seg, const double *__restrict__ cs,
+                                   double *__restrict__ d)
+{
+    long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total)
+        return;
+    const AmrNode N = nodes[find_node(nodes, nn, g, 0)];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    double acc = 0.0;
+    for (int c = 0; c < 2; c++)
+    {
+        int cz = gz - 1 + c;
+        if (cz < 0 || cz >= N.rd[2])
+            continue;
+        for (int b = 0; b < 2; b++)
+        {
+            int cy = gy - 1 + b;
+            if (cy < 0 || cy >= N.rd[1])
+                continue;
+            for (int a = 0; a < 2; a++)
+            {
+                int cx = gx - 1 + a;
+                if (cx < 0 || cx >= N.rd[0])
+                    continue;
+                int sg = cell_seg[N.box_off + cx + (long)cy * N.rd[0] + (long)cz * N.rd[0] * N.rd[1]];
+                if (sg >= 0)
+                    acc += cs[(long)sg * 8 + (1 - a) + 2 * (1 - b) + 4 * (1 - c)];
+            }
+        }
+    }
+    d[g] = acc;
+}
+
+// Node masses and particle counts from the cell segments (segments of a node
+// are contiguous in key order): one block per node, fixed-order sums.
+__global__ void k_node_mass(int nn, AmrNode *nodes, const int *__restrict__ seg_cell,
+                            const int *__restrict__ seg_start, const double *__restrict__ smass,
+                            const int *__restrict__ flags)
+{
+    __shared__ double sh[32];
+    __shared__ int lo_hi[2];
+    const int nd = blockIdx.x;
+    if (nd >= nn)
+        return;
+    const int nseg = flags[F_NSEG];
+    if (threadIdx.x < 2)
+    {
+        long key = threadIdx.x == 0 ? nodes[nd].box_off
+                                    : nodes[nd].box_off + (long)nodes[nd].rd[0] * nodes[nd].rd[1] * nodes[nd].rd[2];
+        int lo = 0, hi = nseg; // first segment with cell >= key
+        while (lo < hi)
+        {
+            int mid = (lo + hi) >> 1;
+            if ((long)seg_cell[mid] < key)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        lo_hi[threadIdx.x] = lo;
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int q = lo_hi[0] + threadIdx.x; q < lo_hi[1]; q += blockDim.x)
+        acc += smass[q];
+    double tot = block_sum_d(acc, sh);
+    if (threadIdx.x == 0)
+    {
+        nodes[nd].mass = tot;
+        nodes[nd].nptcl = lo_hi[1] > lo_hi[0] ? seg_start[lo_hi[1]] - seg_start[lo_hi[0]] : 0;
+    }
+}
+
+int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
+                     unsigned **ks_out, int **perm_out); // qz_particles.cu
+
+int amr_deposit(qz_sim *s)
+{
+    const long n = s->n;
+    for (int l = 1; l < s->amr_nlev; l++)
+    {
+        AmrLevel &L = s->amr[l];
+        if (L.nnodes == 0)
+            break;
+        if (!L.gd.ensure(L.grid_total) || !L.cell_seg.ensure(L.box_total) ||
+            !s->amr_tmp.ensure(2 * n + 2) || !ensure_sort(s, n))
+        {
+            set_error("level deposit buffers");
+            return QZ_FAILURE;
+        }
+        L.d = L.gd.p;
+        int *flag = s->amr_tmp.p, *slot = flag + n;
+        launch(s, QZ_PROF_DEPOSIT, 8.0 * n, k_in_level, dim3(blocks_for(n, 256)), dim3(256), n,
+               s->node_of[l].p, flag);
+        if (scan_exclusive(s, flag, slot, n))
+            return QZ_FAILURE;
+        int t[2];
+        if (!read_at(s, s->amr_tmp.p, {(int)(2 * n - 1), (int)(n - 1)}, t))
+            return QZ_FAILURE;
+        const long m = t[0] + t[1];
+        launch(s, QZ_PROF_DEPOSIT, 44.0 * n, k_lvl_keys, dim3(blocks_for(n, 256)), dim3(256), n,
+               s->node_of[l].p, L.nodes.p, s->x, s->y, s->z, slot, s->sort.k0, s->sort.v0);
+        int bits = 1;
+        while ((1L << bits) < L.box_total)
+            bits++;
+        unsigned *ks;
+        int *perm;
+        if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm))
+            return QZ_FAILURE;
+        if (!s->seg_mass.ensure(m + 1))
+        {
+            set_error("segment mass");
+            return QZ_FAILURE;
+        }
+        const double H = 1.0 / (1 << L.h[0].lv);
+        const double coeff = 4.0 * s->cfg.G * QZ_PI_D / (H * H * H * H * H * H);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+        long blocks = std::min((m * 32 + 255) / 256 + 1, (long)sms * 16);
+        launch(s, QZ_PROF_DEPOSIT, 40.0 * m, k_lvl_seg_reduce, dim3((int)blocks), dim3(256),
+               L.h[0].lv, coeff, perm, s->seg_start, s->flags, s->x, s->y, s->z, s->m,
+               s->cell_sums, s->seg_mass.p);
+        launch(s, QZ_PROF_DEPOSIT, 12.0 * L.grid_total, k_lvl_point_gather,
+               dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, L.nnodes, L.nodes.p,
+               L.cell_seg.p, s->cell_sums, L.d);
+        launch(s, QZ_PROF_DEPOSIT, 16.0 * m, k_node_mass, dim3(L.nnodes), dim3(256), L.nnodes,
+               L.nodes.p, s->seg_cell, s->seg_start, s->seg_mass.p, s->flags);
+        std::vector<AmrNode> tmp(L.nnodes);
+        if (!check_cuda(cudaMemcpyAsync(tmp.data(), L.nodes.p, L.nnodes * sizeof(AmrNode),
+                                        cudaMemcpyDeviceToHost, s->stream), "nodes d2h") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "nodes d2h sync"))
+            return QZ_FAILURE;
+        for (int q = 0; q < L.nnodes; q++)
+        {
+            L.h[q].mass = tmp[q].mass;
+            L.h[q].nptcl = tmp[q].nptcl;
+        }
+        if (!check_cuda(cudaGetLastError(), "level deposit"))
+            return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+// ---- potential on refinement levels -----------------------------------------------------
+// Parent-interpolated start (potential_branches.c:204-331): 0.125 times the sum
+// of the 8 parent values at (c >> 1, (c + 1) >> 1) per axis, in the reference's
+// order; `field` selects potential or acceleration arrays of the parent.
+__device__ __forceinline__ double from_parent(const AmrNode &P, const double *__restrict__ pf,
+                                              int cx, int cy, int cz)
+{
+    const int x1 = (cx >> 1) - P.ts[0], x2 = ((cx + 1) >> 1) - P.ts[0];
+    const int y1 = (cy >> 1) - P.ts[1], y2 = ((cy + 1) >> 1) - P.ts[1];
+    const int z1 = (cz >> 1) - P.ts[2], z2 = ((cz + 1) >> 1) - P.ts[2];
+    const long sx = P.rd[0] + 1, sxy = sx * (P.rd[1] + 1);
+    const long o = P.grid_off;
+    return 0.125 * (pf[o + x1 + y1 * sx + z1 * sxy] + pf[o + x2 + y1 * sx + z1 * sxy] +
+                    pf[o + x1 + y2 * sx + z1 * sxy] + pf[o + x2 + y2 * sx + z1 * sxy] +
+                    pf[o + x1 + y1 * sx + z2 * sxy] + pf[o + x2 + y1 * sx + z2 * sxy] +
+                    pf[o + x1 + y2 * sx + z2 * sxy] + pf[o + x2 + y2 * sx + z2 * sxy]);
+}
+
+__global__ void k_pot_init(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                           const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
+                           const double *__restrict__ ppot, double *__restrict__ pot)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    pot[g] = from_parent(pnodes[N.parent], ppot, gx + N.ts[0], gy + N.ts[1], gz + N.ts[2]);
+}
+
+// potential_branches.c:93-151: -G M / |r - 0.5|, with a coordinate on the box's
+// faces (0 or 2^lv) taken as 0.
+__global__ void k_pot_simb(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                           const AmrNode *__restrict__ nodes, double coeff, double *__restrict__ pot)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const int top = 1 << N.lv;
+    const double H = 1.0 / (1 << N.lv);
+    const int cx = gx + N.ts[0], cy = gy + N.ts[1], cz = gz + N.ts[2];
+    double ai = (cx == 0 || cx == top) ? 0.0 : cx * H;
+    double aj = (cy == 0 || cy == top) ? 0.0 : cy * H;
+    double ak = (cz == 0 || cz == top) ? 0.0 : cz * H;
+    double dist = (ai - 0.5) * (ai - 0.5) + (aj - 0.5) * (aj - 0.5) + (ak - 0.5) * (ak - 0.5);
+    dist = sqrt(dist);
+    pot[g] = coeff / dist;
+}
+
+__global__ void k_copy_d(long n, const double *__restrict__ a, double *__restrict__ b)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        b[i] = a[i];
+}
+
+// per-node scalar slots in nscal (6 per node) and nint (6 per node)
+enum { S_RSOLD = 0, S_RSNEW = 1, S_ALPHA = 2, S_BETA = 3, S_DOT = 4, S_RM = 5 };
+enum { I_CONV = 0, I_RFAIL = 1, I_CB = 2, I_CE = 3, I_CHECKED = 4 };
+
+// Conjugate gradient on the interior points of every node of a level
+// (conjugate_gradient.c:322-463).  Chunk kernels work on [begin, end) of the
+// interior list of one node and write one partial sum per chunk; node kernels
+// add a node's partials in chunk order.
+__global__ void k_cg_init(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
+                          const AmrNode *__restrict__ nodes, const double *__restrict__ d,
+                          const double *__restrict__ pot, double *__restrict__ r,
+                          double *__restrict__ p, double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const AmrChunk C = ch[blockIdx.x];
+    const AmrNode N = nodes[C.node];
+    const double H = 1.0 / (1 << N.lv);
+    const double oh2 = 1.0 / (H * H);
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    double acc = 0.0;
+    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+    {
+        const long g = intr[e];
+        double rv = d[g] + oh2 * (6.0 * pot[g] - pot[g + 1] - pot[g - 1] - pot[g + sy] -
+                                  pot[g - sy] - pot[g + sz] - pot[g - sz]);
+        r[g] = rv;
+        p[g] = rv;
+        acc += rv * rv;
+    }
+    double t = block_sum_d(acc, sh);
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = t;
+}
+
+__global__ void k_cg_Ap(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
+                        const AmrNode *__restrict__ nodes, const int *__restrict__ nint,
+                        const double *__restrict__ p, double *__restrict__ Ap,
+                        double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const AmrChunk C = ch[blockIdx.x];
+    if (nint[6 * C.node + I_CONV])
+        return;
+    const AmrNode N = nodes[C.node];
+    const double H = 1.0 / (1 << N.lv);
+    const double oh2 = 1.0 / (H * H);
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    double acc = 0.0;
+    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+    {
+        const long g = intr[e];
+        double a = -oh2 * (6.0 * p[g] - p[g + 1] - p[g - 1] - p[g + sy] - p[g - sy] - p[g + sz] -
+                           p[g - sz]);
+        Ap[g] = a;
+        acc += p[g] * a;
+    }
+    double t = block_sum_d(acc, sh);
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = t;
+}
+
+__global__ void k_cg_update(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
+                            const int *__restrict__ nint, const double *__restrict__ nscal,
+                            const double *__restrict__ p, const double *__restrict__ Ap,
+                            double *__restrict__ pot, double *__restrict__ r,
+                            double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const AmrChunk C = ch[blockIdx.x];
+    if (nint[6 * C.node + I_CONV])
+        return;
+    const double alpha = nscal[6 * C.node + S_ALPHA];
+    double acc = 0.0;
+    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+    {
+        const long g = intr[e];
+        pot[g] += alpha * p[g];
+        double rv = r[g] - alpha * Ap[g];
+        r[g] = rv;
+        acc += rv * rv;
+    }
+    double t = block_sum_d(acc, sh);
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = t;
+}
+
+__global__ void k_cg_p(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
+                       const int *__restrict__ nint, const double *__restrict__ nscal,
+                       const double *__restrict__ r, double *__restrict__ p)
+{
+    const AmrChunk C = ch[blockIdx.x];
+    if (nint[6 * C.node + I_CONV])
+        return;
+    const double beta = nscal[6 * C.node + S_BETA];
+    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+    {
+        const long g = intr[e];
+        p[g] = r[g] + beta * p[g];
+    }
+}
+
+// Ratio test of poisson_error.c:36-81 on a chunk of interior points.
+__global__ void k_cg_ratio(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
+                           int *__restrict__ nint, const double *__restrict__ pot,
+                           const double *__restrict__ pot_old, double tm, double tp)
+{
+    const AmrChunk C = ch[blockIdx.x];
+    if (nint[6 * C.node + I_CONV])
+        return;
+    int fail = 0;
+    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+    {
+        const long g = intr[e];
+        double a = pot[g] / pot_old[g];
+        if ((tm > a) || (tp < a))
+            fail = 1;
+    }
+    if (__syncthreads_or(fail) && threadIdx.x == 0)
+        nint[6 * C.node + I_RFAIL] = 1;
+}
+
+// Node stages: 0 rsold from the init partials; 1 alpha = rsold / (p . Ap);
+// 2 rsnew and beta; 3 convergence (poisson_error.c:236-254); 4 rsold = rsnew.
+__global__ void k_cg_node(int nn, int stage, const AmrNode *__restrict__ nodes,
+                          const double *__restrict__ part, double *__restrict__ nscal,
+                          int *__restrict__ nint, double tol, double G, int *__restrict__ flags)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nn)
+        return;
+    int *I = nint + 6 * q;
+    double *S = nscal + 6 * q;
+    if (stage != 0 && I[I_CONV])
+        return;
+    double sum = 0.0;
+    if (stage <= 2)
+        for (int c = I[I_CB]; c < I[I_CE]; c++)
+            sum += part[c];
+    if (stage == 0)
+    {
+        S[S_RSOLD] = sum;
+        I[I_CONV] = 0;
+        I[I_RFAIL] = 0;
+        const AmrNode N = nodes[q];
+        const double H = 1.0 / (1 << N.lv);
+        S[S_RM] = 4.0 * G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+    }
+    else if (stage == 1)
+    {
+        S[S_DOT] = sum;
+        S[S_ALPHA] = S[S_RSOLD] / sum;
+    }
+    else if (stage == 2)
+    {
+        S[S_RSNEW] = sum;
+        S[S_BETA] = sum / S[S_RSOLD];
+    }
+    else if (stage == 3)
+    {
+        const AmrNode N = nodes[q];
+        bool ok = !I[I_RFAIL];
+        if (ok)
+        {
+            double t = tol * S[S_RM];
+            double aux_tol = N.nintr * t * t;
+            ok = S[S_RSNEW] < aux_tol;
+        }
+        I[I_CHECKED] = ok ? 0 : 1; // 1: copy pot to pot_old
+        I[I_RFAIL] = 0;
+        if (ok)
+        {
+            I[I_CONV] = 1;
+            atomicAdd(&flags[F_AMR_CONV], 1);
+        }
+    }
+    else
+        S[S_RSOLD] = S[S_RSNEW];
+}
+
+// pot_old <- pot on the whole grid of every node whose check failed.
+__global__ void k_cg_copy_old(long total, int nn, const AmrNode *__restrict__ nodes,
+                              int *__restrict__ nint, const double *__restrict__ pot,
+                              double *__restrict__ pot_old)
+{
+    long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total)
+        return;
+    int nd = find_node(nodes, nn, g, 0);
+    if (nint[6 * nd + I_CHECKED])
+        pot_old[g] = pot[g];
+}
+
+static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
+{
+    const qz_config &c = s->cfg;
+    const int nn = L.nnodes;
+    // chunks over each node's interior list
+    L.hchunks.clear();
+    std::vector<int> hint(6L * nn, 0);
+    for (int q = 0; q < nn; q++)
+    {
+        hint[6 * q + I_CB] = (int)L.hchunks.size();
+        const AmrNode &N = L.h[q];
+        for (int b = N.intr_off; b < N.intr_off + N.nintr; b += CG_CHUNK)
+            L.hchunks.push_back({q, b, std::min(b + CG_CHUNK, N.intr_off + N.nintr)});
+        hint[6 * q + I_CE] = (int)L.hchunks.size();
+    }
+    L.nchunks = (int)L.hchunks.size();
+    if (L.nchunks == 0)
+        return QZ_SUCCESS;
+    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(L.nchunks) ||
+        !L.nscal.ensure(6L * nn) || !L.nint.ensure(6L * nn) || !L.r.ensure(L.grid_total) ||
+        !L.p.ensure(L.grid_total) || !L.Ap.ensure(L.grid_total))
+    {
+        set_error("cg buffers");
+        return QZ_FAILURE;
+    }
+    if (!check_cuda(cudaMemcpyAsync(L.chunks.p, L.hchunks.data(), L.nchunks * sizeof(AmrChunk),
+                                    cudaMemcpyHostToDevice, s->stream), "chunks") ||
+        !check_cuda(cudaMemcpyAsync(L.nint.p, hint.data(), 6L * nn * sizeof(int),
+                                    cudaMemcpyHostToDevice, s->stream), "cg ints") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "cg set-up"))
+        return QZ_FAILURE;
+    cudaMemsetAsync(L.p.p, 0, L.grid_total * sizeof(double), s->stream);
+    const dim3 gc(L.nchunks), bc(CG_THREADS), gn(blocks_for(nn, 128)), bn(128);
+    const double intr_bytes = (double)L.intr_total;
+    launch(s, QZ_PROF_CG, 40.0 * intr_bytes, k_cg_init, gc, bc, L.chunks.p, L.intr.p, L.nodes.p,
+           L.d, L.pot, L.r.p, L.p.p, L.chunk_part.p);
+    launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 0, L.nodes.p, L.chunk_part.p,
+           L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+    // iteration cap of the reference per node: min(node grid size, max_iter);
+    // nodes iterate in lockstep, so the level runs to the largest cap
+    long cap_it = 0;
+    for (auto &N : L.h)
+        cap_it = std::max(cap_it, std::min((long)c.max_iter,
+                                           (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1)));
+    const int every = c.check_every > 0 ? c.check_every : 1;
+    int converged = 0;
+    long it = 0;
+    cudaMemsetAsync(s->flags + F_AMR_CONV, 0, sizeof(int), s->stream);
+    while (it < cap_it && converged < nn)
+    {
+        for (int q = 0; q < every && it < cap_it; q++)
+        {
+            it++;
+            launch(s, QZ_PROF_CG, 24.0 * intr_bytes, k_cg_Ap, gc, bc, L.chunks.p, L.intr.p,
+                   L.nodes.p, L.nint.p, L.p.p, L.Ap.p, L.chunk_part.p);
+            launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 1, L.nodes.p,
+                   L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+            launch(s, QZ_PROF_CG, 48.0 * intr_bytes, k_cg_update, gc, bc, L.chunks.p, L.intr.p,
+                   L.nint.p, L.nscal.p, L.p.p, L.Ap.p, L.pot, L.r.p, L.chunk_part.p);
+            launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 2, L.nodes.p,
+                   L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+            if (it % every == 0)
+            {
+                launch(s, QZ_PROF_CG, 20.0 * intr_bytes, k_cg_ratio, gc, bc, L.chunks.p, L.intr.p,
+                       L.nint.p, L.pot, L.pot_old, 1.0 - c.tol2, 1.0 + c.tol2);
+                launch(s, QZ_PROF_CG, 8.0 * nn, k_cg_node, gn, bn, nn, 3, L.nodes.p,
+                       L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+                launch(s, QZ_PROF_CG, 16.0 * L.grid_total, k_cg_copy_old,
+                       dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, nn,
+                       L.nodes.p, L.nint.p, L.pot, L.pot_old);
+            }
+            launch(s, QZ_PROF_CG, 24.0 * intr_bytes, k_cg_p, gc, bc, L.chunks.p, L.intr.p,
+                   L.nint.p, L.nscal.p, L.r.p, L.p.p);
+            launch(s, QZ_PROF_CG, 8.0 * nn, k_cg_node, gn, bn, nn, 4, L.nodes.p, L.chunk_part.p,
+                   L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+        }
+        int cv;
+        if (!read_ints(s, s->flags + F_AMR_CONV, 1, &cv))
+            return QZ_FAILURE;
+        converged = cv;
+    }
+    s->stats.cg_iterations += it;
+    if (converged < nn)
+    {
+        set_error("the precision was not reached in refinement level %d after %ld conjugate "
+                  "gradient iterations", level_index, it);
+        return QZ_FAILURE;
+    }
+    return check_cuda(cudaGetLastError(), "cg") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+int amr_potential(qz_sim *s)
+{
+    const double coeff = -s->cfg.G * s->cfg.total_mass;
+    for (int l = 1; l < s->amr_nlev; l++)
+    {
+        AmrLevel &L = s->amr[l];
+        AmrLevel &P = s->amr[l - 1];
+        if (L.nnodes == 0)
+            break;
+        if (!L.gpot.ensure(L.grid_total) || !L.gpot_old.ensure(L.grid_total))
+        {
+            set_error("level potential buffers");
+            return QZ_FAILURE;
+        }
+        L.pot = L.gpot.p;
+        L.pot_old = L.gpot_old.p;
+        cudaMemsetAsync(L.pot, 0, L.grid_total * sizeof(double), s->stream);
+        if (L.simb_total > 0)
+            launch(s, QZ_PROF_OTHER, 16.0 * L.simb_total, k_pot_simb,
+                   dim3(blocks_for(L.simb_total, 256)), dim3(256), L.simb_total, L.simb.p,
+                   L.simb_node.p, L.nodes.p, coeff, L.pot);
+        if (L.bdry_total > 0)
+            launch(s, QZ_PROF_OTHER, 80.0 * L.bdry_total, k_pot_init,
+                   dim3(blocks_for(L.bdry_total, 256)), dim3(256), L.bdry_total, L.bdry.p,
+                   L.bdry_node.p, L.nodes.p, P.nodes.p, P.pot, L.pot);
+        if (L.intr_total > 0)
+            launch(s, QZ_PROF_OTHER, 80.0 * L.intr_total, k_pot_init,
+                   dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
+                   L.intr_node.p, L.nodes.p, P.nodes.p, P.pot, L.pot);
+        launch(s, QZ_PROF_OTHER, 16.0 * L.grid_total, k_copy_d, dim3(blocks_for(L.grid_total, 256)),
+               dim3(256), L.grid_total, L.pot, L.pot_old);
+        if (cg_level(s, L, l))
+            return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+// ---- gradient on refinement levels -------------------------------------------------------
+// grid_acceleration.c:199-268, with the y coordinate not scaled by H (as there).
+__global__ void k_acc_simb(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                           const AmrNode *__restrict__ nodes, double coeff1,
+                           double *__restrict__ ax, double *__restrict__ ay,
+                           double *__restrict__ az)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const int top = 1 << N.lv;
+    const double H = 1.0 / (1 << N.lv);
+    const int cx = gx + N.ts[0], cy = gy + N.ts[1], cz = gz + N.ts[2];
+    double ai = (cx == 0 || cx == top) ? 0.0 : cx * H;
+    double aj = (cy == 0 || cy == top) ? 0.0 : (double)cy;
+    double ak = (cz == 0 || cz == top) ? 0.0 : cz * H;
+    double dist = (ai - 0.5) * (ai - 0.5) + (aj - 0.5) * (aj - 0.5) + (ak - 0.5) * (ak - 0.5);
+    dist = sqrt(dist);
+    double c2 = coeff1 / (dist * dist * dist);
+    ax[g] = c2 * (ai - 0.5);
+    ay[g] = c2 * (aj - 0.5);
+    az[g] = c2 * (ak - 0.5);
+}
+
+__global__ void k_acc_bdry(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                           const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
+                           const double *__restrict__ pax, const double *__restrict__ pay,
+                           const double *__restrict__ paz, double *__restrict__ ax,
+                           double *__restrict__ ay, double *__restrict__ az)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const AmrNode P = pnodes[N.parent];
+    const int cx = gx + N.ts[0], cy = gy + N.ts[1], cz = gz + N.ts[2];
+    ax[g] = from_parent(P, pax, cx, cy, cz);
+    ay[g] = from_parent(P, pay, cx, cy, cz);
+    az[g] = from_parent(P, paz, cx, cy, cz);
+}
+
+__global__ void k_acc_intr(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                           const AmrNode *__restrict__ nodes, const double *__restrict__ pot,
+                           double *__restrict__ ax, double *__restrict__ ay,
+                           double *__restrict__ az)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    const double H = 1.0 / (1 << N.lv);
+    const double o2h = 1.0 / (2.0 * H);
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
+    ay[g] = o2h * (pot[g - sy] - pot[g + sy]);
+    az[g] = o2h * (pot[g - sz] - pot[g + sz]);
+}
+
+int amr_grid_accel(qz_sim *s)
+{
+    const double coeff1 = -s->cfg.G * s->cfg.total_mass;
+    for (int l = 1; l < s->amr_nlev; l++)
+    {
+        AmrLevel &L = s->amr[l];
+        AmrLevel &P = s->amr[l - 1];
+        if (L.nnodes == 0)
+            break;
+        if (!L.gax.ensure(L.grid_total) || !L.gay.ensure(L.grid_total) ||
+            !L.gaz.ensure(L.grid_total))
+        {
+            set_error("level acceleration buffers");
+            return QZ_FAILURE;
+        }
+        L.ax = L.gax.p;
+        L.ay = L.gay.p;
+        L.az = L.gaz.p;
+        for (double *f : {L.ax, L.ay, L.az})
+            cudaMemsetAsync(f, 0, L.grid_total * sizeof(double), s->stream);
+        if (L.simb_total > 0)
+            launch(s, QZ_PROF_GRADIENT, 32.0 * L.simb_total, k_acc_simb,
+                   dim3(blocks_for(L.simb_total, 256)), dim3(256), L.simb_total, L.simb.p,
+                   L.simb_node.p, L.nodes.p, coeff1, L.ax, L.ay, L.az);
+        if (L.bdry_total > 0)
+            launch(s, QZ_PROF_GRADIENT, 224.0 * L.bdry_total, k_acc_bdry,
+                   dim3(blocks_for(L.bdry_total, 256)), dim3(256), L.bdry_total, L.bdry.p,
+                   L.bdry_node.p, L.nodes.p, P.nodes.p, P.ax, P.ay, P.az, L.ax, L.ay, L.az);
+        if (L.intr_total > 0)
+            launch(s, QZ_PROF_GRADIENT, 32.0 * L.intr_total, k_acc_intr,
+                   dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
+                   L.intr_node.p, L.nodes.p, L.pot, L.ax, L.ay, L.az);
+    }
+    return check_cuda(cudaGetLastError(), "level gradient") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// ---- gather from the finest node -----------------------------------------------------------
+struct LevelRefs {
+    const AmrNode *nodes[AMR_MAX_LEVELS];
+    const int *node_of[AMR_MAX_LEVELS];
+    const double *ax[AMR_MAX_LEVELS], *ay[AMR_MAX_LEVELS], *az[AMR_MAX_LEVELS];
+    int nlev;
+};
+
+__global__ void k_amr_gather(long n, LevelRefs R, const double *__restrict__ x,
+                             const double *__restrict__ y, const double *__restrict__ z,
+                             double *__restrict__ pax, double *__restrict__ pay,
+                             double *__restrict__ paz, int *__restrict__ flags)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int l = R.nlev - 1;
+    int nd = -1;
+    for (; l > 0; l--)
+    {
+        nd = R.node_of[l][i];
+        if (nd >= 0)
+            break;
+    }
+    if (l == 0)
+        nd = 0;
+    const AmrNode N = R.nodes[l][nd];
+    const double sc = (double)(1 << N.lv);
+    double px = x[i] * sc, py = y[i] * sc, pz = z[i] * sc;
+    int fx = (int)px, fy = (int)py, fz = (int)pz;
+    long b = box_index(N, fx, fy, fz);
+    if (!(px >= 0.0 && py >= 0.0 && pz >= 0.0) || b < 0 || b >= (long)N.rd[0] * N.rd[1] * N.rd[2])
+    {
+        atomicOr(&flags[F_ERROR], E_PTCL_OUTSIDE);
+        return;
+    }
+    double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+    double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+    double w[8];
+    w[0] = wx2 * wy2 * wz2;
+    w[1] = wx1 * wy2 * wz2;
+    w[2] = wx2 * wy1 * wz2;
+    w[3] = wx1 * wy1 * wz2;
+    w[4] = wx2 * wy2 * wz1;
+    w[5] = wx1 * wy2 * wz1;
+    w[6] = wx2 * wy1 * wz1;
+    w[7] = wx1 * wy1 * wz1;
+    const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
+    const long g = grid_index(N, fx - N.ts[0], fy - N.ts[1], fz - N.ts[2]);
+    const double *gx = R.ax[l], *gy = R.ay[l], *gz = R.az[l];
+    double ax = pax[i], ay = pay[i], az = paz[i];
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int ii = 0; ii < 2; ii++)
+            {
+                int a = ii + 2 * jj + 4 * kk;
+                long q = g + ii + jj * sx + kk * sxy;
+                ax += gx[q] * w[a];
+                ay += gy[q] * w[a];
+                az += gz[q] * w[a];
+            }
+    pax[i] = ax;
+    pay[i] = ay;
+    paz[i] = az;
+}
+
+int amr_gather(qz_sim *s)
+{
+    if (s->n == 0)
+        return QZ_SUCCESS;
+    LevelRefs R{};
+    R.nlev = s->amr_nlev;
+    for (int l = 0; l < s->amr_nlev; l++)
+    {
+        R.nodes[l] = s->amr[l].nodes.p;
+        R.node_of[l] = s->node_of[l].p;
+        R.ax[l] = s->amr[l].ax;
+        R.ay[l] = s->amr[l].ay;
+        R.az[l] = s->amr[l].az;
+    }
+    launch(s, QZ_PROF_GATHER, 72.0 * s->n + 8.0 * s->n * s->amr_nlev, k_amr_gather,
+           dim3(blocks_for(s->n, 256)), dim3(256), s->n, R, s->x, s->y, s->z, s->ax, s->ay, s->az,
+           s->flags);
+    return check_cuda(cudaGetLastError(), "amr gather") ? QZ_SUCCESS : QZ_FAILURE;
+}
+} // namespace qz

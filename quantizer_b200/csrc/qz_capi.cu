@@ -273,6 +273,8 @@ int qz_default_config(qz_config *c, int lmin)
     c->precision = QZ_PREC_FP64;
     c->inner_cycles = 1;
     c->force_stencil = 0;
+    c->ref_ptcl = 4;   /* global_variables.c:289 */
+    c->box_extra = 10; /* 2 * min_box_extra_size_per_side_user, global_variables.c:294-295 */
     return QZ_SUCCESS;
 }
 
@@ -295,6 +297,7 @@ int qz_destroy(qz_sim *s)
     for (void *p : ptrs)
         dfree(p);
     free_levels(s);
+    amr_free(s);
     if (s->h_flags)
         cudaFreeHost(s->h_flags);
     if (s->h_stage)
@@ -318,9 +321,16 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         set_error("qz_create: lmin=%d outside the supported range 2..9", cfg->lmin);
         return QZ_FAILURE;
     }
-    if (cfg->lmax != cfg->lmin)
+    if (cfg->lmax < cfg->lmin || cfg->lmax - cfg->lmin > 12 || cfg->lmax > 20)
     {
-        set_error("qz_create: this context runs the head-only path (lmax == lmin)");
+        set_error("qz_create: lmax=%d outside lmin..min(lmin+12, 20)", cfg->lmax);
+        return QZ_FAILURE;
+    }
+    if (cfg->lmax > cfg->lmin && (cfg->bdry != 1 || cfg->ref_ptcl < 1 || cfg->box_extra < 2 ||
+                                  (cfg->box_extra & 1)))
+    {
+        set_error("qz_create: refinement needs reflexive boundaries, ref_ptcl >= 1 and an even "
+                  "box_extra >= 2");
         return QZ_FAILURE;
     }
     if (cfg->bdry != 0 && cfg->bdry != 1)
@@ -390,6 +400,8 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     }
     if (ok)
         ok = head_initial(s) == QZ_SUCCESS;
+    if (ok && cfg->lmax > cfg->lmin)
+        ok = amr_init(s) == QZ_SUCCESS;
     if (ok)
         ok = check_cuda(cudaStreamSynchronize(s->stream), "create sync") &&
              check_cuda(cudaDeviceSynchronize(), "create device sync");
@@ -505,9 +517,28 @@ int qz_reset(qz_sim *s)
     return ok ? QZ_SUCCESS : QZ_FAILURE;
 }
 
-int qz_grid_density(qz_sim *s) { return s ? deposit_head(s) : QZ_FAILURE; }
+static bool amr_on(const qz_sim *s) { return s->cfg.lmax > s->cfg.lmin; }
 
-int qz_potential(qz_sim *s) { return s ? potential_head(s) : QZ_FAILURE; }
+int qz_tree_adaptation(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_build(s) : QZ_SUCCESS;
+}
+
+int qz_grid_density(qz_sim *s)
+{
+    if (!s || deposit_head(s))
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_deposit(s) : QZ_SUCCESS;
+}
+
+int qz_potential(qz_sim *s)
+{
+    if (!s || potential_head(s))
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_potential(s) : QZ_SUCCESS;
+}
 
 int qz_poisson_error(qz_sim *s, int *converged)
 {
@@ -516,9 +547,19 @@ int qz_poisson_error(qz_sim *s, int *converged)
     return poisson_error_head(s, converged);
 }
 
-int qz_grid_acceleration(qz_sim *s) { return s ? grid_accel_head(s) : QZ_FAILURE; }
+int qz_grid_acceleration(qz_sim *s)
+{
+    if (!s || grid_accel_head(s))
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_grid_accel(s) : QZ_SUCCESS;
+}
 
-int qz_particle_acceleration(qz_sim *s) { return s ? gather_head(s) : QZ_FAILURE; }
+int qz_particle_acceleration(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_gather(s) : gather_head(s);
+}
 
 int qz_particle_updating_A(qz_sim *s, double dt) { return s ? kick_drift(s, dt) : QZ_FAILURE; }
 
@@ -528,8 +569,8 @@ int qz_init_forces(qz_sim *s)
 {
     if (!s)
         return QZ_FAILURE;
-    if (qz_reset(s) || deposit_head(s) || potential_head(s) || grid_accel_head(s) ||
-        gather_head(s) || check_flags(s))
+    if (qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) || qz_potential(s) ||
+        qz_grid_acceleration(s) || qz_particle_acceleration(s) || check_flags(s))
         return QZ_FAILURE;
     s->forces_ready = true;
     return QZ_SUCCESS;
@@ -543,8 +584,9 @@ int qz_step(qz_sim *s, double dt, int nsteps)
         return QZ_FAILURE;
     for (int q = 0; q < nsteps; q++)
     {
-        if (kick_drift(s, dt) || qz_reset(s) || deposit_head(s) || potential_head(s) ||
-            grid_accel_head(s) || gather_head(s) || kick(s, dt))
+        if (kick_drift(s, dt) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
+            qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) ||
+            kick(s, dt))
             return QZ_FAILURE;
         s->stats.steps++;
     }
@@ -563,7 +605,115 @@ int qz_get_stats(qz_sim *s, qz_stats *out)
     if (!s || !out)
         return QZ_FAILURE;
     *out = s->stats;
+    out->levels = amr_on(s) ? s->amr_nlev : 1;
+    out->nodes = 1;
+    if (amr_on(s))
+        for (int l = 1; l < s->amr_nlev; l++)
+            out->nodes += s->amr[l].nnodes;
     return QZ_SUCCESS;
+}
+
+// ---- refinement tree inspection ---------------------------------------------------------
+static const AmrNode *tree_node(qz_sim *s, int level, int node)
+{
+    if (!s || !amr_on(s) || level < 0 || level >= s->amr_nlev || node < 0 ||
+        node >= s->amr[level].nnodes)
+    {
+        set_error("no node %d at level %d", node, level);
+        return nullptr;
+    }
+    return &s->amr[level].h[node];
+}
+
+int qz_amr_levels(qz_sim *s) { return !s ? 0 : amr_on(s) ? s->amr_nlev : 1; }
+
+int qz_amr_num_nodes(qz_sim *s, int level)
+{
+    if (!s || !amr_on(s) || level < 0 || level >= s->amr_nlev)
+        return level == 0 && s ? 1 : 0;
+    return s->amr[level].nnodes;
+}
+
+int qz_amr_node_info(qz_sim *s, int level, int node, int *info, double *mass)
+{
+    const AmrNode *N = tree_node(s, level, node);
+    if (!N || !info)
+        return QZ_FAILURE;
+    int v[22] = {N->lv, N->parent, N->ts[0], N->ts[1], N->ts[2], N->rd[0], N->rd[1], N->rd[2],
+                 N->bmin[0], N->bmin[1], N->bmin[2], N->bmax[0], N->bmax[1], N->bmax[2],
+                 N->ncells, N->nintr, N->nbdry, N->nsimb, N->nptcl, N->zone_base, N->nzones,
+                 N->contact};
+    memcpy(info, v, sizeof v);
+    if (mass)
+        *mass = N->mass;
+    return QZ_SUCCESS;
+}
+
+static bool d2h_int(qz_sim *s, int *dst, const int *src, long count)
+{
+    return count <= 0 ||
+           (check_cuda(cudaMemcpyAsync(dst, src, count * sizeof(int), cudaMemcpyDeviceToHost,
+                                       s->stream), "tree d2h") &&
+            check_cuda(cudaStreamSynchronize(s->stream), "tree d2h sync"));
+}
+
+int qz_amr_node_cells(qz_sim *s, int level, int node, int *xyz)
+{
+    const AmrNode *N = tree_node(s, level, node);
+    if (!N || !xyz)
+        return QZ_FAILURE;
+    return d2h_int(s, xyz, s->amr[level].cell_xyz.p + 3L * N->cell_off, 3L * N->ncells)
+               ? QZ_SUCCESS
+               : QZ_FAILURE;
+}
+
+int qz_amr_node_box(qz_sim *s, int level, int node, int *out)
+{
+    const AmrNode *N = tree_node(s, level, node);
+    if (!N || !out)
+        return QZ_FAILURE;
+    return d2h_int(s, out, s->amr[level].box.p + N->box_off, (long)N->rd[0] * N->rd[1] * N->rd[2])
+               ? QZ_SUCCESS
+               : QZ_FAILURE;
+}
+
+// which: 0 interior, 1 boundary, 2 simulation boundary; node-local grid indices.
+int qz_amr_node_list(qz_sim *s, int level, int node, int which, int *out)
+{
+    const AmrNode *N = tree_node(s, level, node);
+    if (!N || !out || level == 0 || which < 0 || which > 2)
+        return QZ_FAILURE;
+    AmrLevel &L = s->amr[level];
+    const int *src = which == 0 ? L.intr.p + N->intr_off : which == 1 ? L.bdry.p + N->bdry_off
+                                                                       : L.simb.p + N->simb_off;
+    const int cnt = which == 0 ? N->nintr : which == 1 ? N->nbdry : N->nsimb;
+    if (!d2h_int(s, out, src, cnt))
+        return QZ_FAILURE;
+    for (int i = 0; i < cnt; i++)
+        out[i] -= (int)N->grid_off;
+    return QZ_SUCCESS;
+}
+
+int qz_amr_node_field(qz_sim *s, int level, int node, int which, double *out)
+{
+    const AmrNode *N = tree_node(s, level, node);
+    if (!N || !out)
+        return QZ_FAILURE;
+    AmrLevel &L = s->amr[level];
+    const double *f = which == QZ_FIELD_POT ? L.pot : which == QZ_FIELD_POT_OLD ? L.pot_old
+                    : which == QZ_FIELD_DENSITY ? L.d : which == QZ_FIELD_AX ? L.ax
+                    : which == QZ_FIELD_AY ? L.ay : which == QZ_FIELD_AZ ? L.az : nullptr;
+    if (!f)
+    {
+        set_error("field %d not available at level %d", which, level);
+        return QZ_FAILURE;
+    }
+    const long cnt = (long)(N->rd[0] + 1) * (N->rd[1] + 1) * (N->rd[2] + 1);
+    return check_cuda(cudaMemcpyAsync(out, f + N->grid_off, cnt * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s->stream), "field d2h") &&
+                   check_cuda(cudaStreamSynchronize(s->stream), "field d2h sync")
+               ? QZ_SUCCESS
+               : QZ_FAILURE;
 }
 
 void *qz_stream(qz_sim *s) { return s ? (void *)s->stream : nullptr; }

@@ -47,6 +47,7 @@ enum Flag {
     F_ERROR = 2,      // bitmask of bounds errors seen by kernels
     F_NSEG = 3,       // number of occupied cells (deposit segments)
     F_RESID_FAIL = 4, // method-1 pointwise residual failure
+    F_AMR_CONV = 5,   // refinement nodes converged in the current level solve
     F_COUNT = 8
 };
 enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2 };
@@ -58,6 +59,95 @@ struct Sort {
     int *hist = nullptr; // 256 * tiles
     long cap = 0;
     long tiles_cap = 0;
+};
+
+// One node of the refinement tree (host and device copies are identical PODs).
+// Box coordinates are cell indices at the node's level minus ts; the node's
+// grid fields have (rd + 1)^3 points, linear index i + j*(rd_x+1) + k*(rd_x+1)*(rd_y+1)
+// (initialize_node.h:63-216, tree_construction.c:1032-2349).
+struct AmrNode {
+    int lv;          // absolute level
+    int parent;      // index in the parent level's node array (-1: head)
+    int ts[3];       // box_ts
+    int rd[3];       // box_real_dim
+    int bmin[3];     // smallest box, level coordinates
+    int bmax[3];
+    long box_off;    // first cell of the node box in the level's box pool
+    long grid_off;   // first point of the node grid in the level's grid pools
+    int cell_off, ncells;                 // node cells in the level's cell pool
+    int intr_off, nintr, bdry_off, nbdry, simb_off, nsimb; // grid-point lists
+    long cls_off;    // first point of the node's classification range
+    int zone_base;   // first child (index in the next level)
+    int nzones;
+    int nptcl;       // particles in the node (no_ptcl_full_node)
+    int contact;     // touches the simulation boundary (sim_bdry_contact)
+    double mass;     // node_mass
+};
+
+struct AmrChunk {
+    int node, begin, end; // [begin, end) of the level's interior list, one node
+};
+
+// Grow-only device buffer.
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    long cap = 0;
+    bool ensure(long need)
+    {
+        if (need < 1)
+            need = 1;
+        if (p && need <= cap)
+            return true;
+        long nc = need > cap * 3 / 2 + 1024 ? need : cap * 3 / 2 + 1024;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc((void **)&p, nc * sizeof(T)) != cudaSuccess)
+        {
+            p = nullptr;
+            return false;
+        }
+        cap = nc;
+        return true;
+    }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Device pools of one refinement level.  Level 0 is the head: its grid pools
+// alias the head fields and its box is the (2^L + 2)^3 head box.
+struct AmrLevel {
+    int nnodes = 0;
+    std::vector<AmrNode> h;
+    DBuf<AmrNode> nodes;
+    long box_total = 0, grid_total = 0, cls_total = 0;
+    int cell_total = 0, intr_total = 0, bdry_total = 0, simb_total = 0;
+    DBuf<int> box;        // cell status (-5 outside sim, -4 not in node, -3 in node,
+                          // -1 refine, >= 0 zone id)
+    DBuf<int> cnt;        // particles per box cell
+    DBuf<int> pos_of_box; // level cell position of a box cell, -1 if none
+    DBuf<int> cell_seg;   // deposit segment of a box cell, -1 if none
+    DBuf<int> cell_box;   // per cell: level box-pool index
+    DBuf<int> cell_xyz;   // per cell: level coordinates (x, y, z)
+    DBuf<int> cell_node;  // per cell: node index
+    DBuf<int> intr, bdry, simb, intr_node, bdry_node, simb_node; // level grid-pool indices
+    double *pot = nullptr, *pot_old = nullptr, *d = nullptr, *ax = nullptr, *ay = nullptr,
+           *az = nullptr; // head aliases on level 0
+    DBuf<double> gpot, gpot_old, gd, gax, gay, gaz, r, p, Ap;
+    // conjugate gradient per node: rsold, rsnew, alpha, beta, dot, mass
+    DBuf<double> nscal;
+    DBuf<int> nint; // per node: conv, ratio_fail, chunk_begin, chunk_end, active, nptcl
+    DBuf<AmrChunk> chunks;
+    DBuf<double> chunk_part;
+    int nchunks = 0;
+    std::vector<AmrChunk> hchunks;
 };
 
 } // namespace qz
@@ -103,6 +193,18 @@ struct qz_sim {
 
     qz_stats stats{};
     bool forces_ready = false;
+
+    // refinement tree (lmax > lmin): levels[0] = head, rebuilt every step
+    std::vector<qz::AmrLevel> amr;
+    int amr_nlev = 1;                  // levels in use this step
+    std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
+    qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)
+    qz::DBuf<int> zone_box;            // per zone: min x,y,z, max x,y,z
+    qz::DBuf<int> zone_cells;          // per zone: cells
+    qz::DBuf<int> gather_idx;          // small gathers of scan values
+    qz::DBuf<double> seg_mass;         // per deposit segment: mass
+    int *h_small = nullptr;            // pinned read-back buffer
+    long h_small_cap = 0;
 
     // CUDA graph of one convergence-check block of the head solve
     bool use_graphs = true;
@@ -188,6 +290,13 @@ int kick_drift(qz_sim *s, double dt);
 int kick(qz_sim *s, double dt);
 
 int potential_head(qz_sim *s);
+int amr_init(qz_sim *s);
+void amr_free(qz_sim *s);
+int amr_build(qz_sim *s);
+int amr_deposit(qz_sim *s);
+int amr_potential(qz_sim *s);
+int amr_grid_accel(qz_sim *s);
+int amr_gather(qz_sim *s);
 int poisson_error_head(qz_sim *s, int *converged);
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters);
 void sync_fine_alt(qz_sim *s);
@@ -195,6 +304,7 @@ void init_kernel_attributes();
 int vcycle(qz_sim *s, int level, int type);
 
 int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **vals_out);
+long radix_tiles(long n);
 int scan_exclusive(qz_sim *s, const int *in, int *out, long n);
 
 // grid views

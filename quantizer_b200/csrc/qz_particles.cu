@@ -210,6 +210,33 @@ __global__ void k_point_gather(int L, long D, const int *__restrict__ cell_seg,
     d[t] = acc;
 }
 
+// Sorts the m (cell key, particle) pairs staged in s->sort.k0 / v0 and builds
+// the cell segments: seg_start / seg_cell of every occupied cell, cell_seg
+// (ncells_box entries, -1 for empty cells) and flags[F_NSEG].
+int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
+                     unsigned **ks_out, int **perm_out)
+{
+    unsigned *ks;
+    int *perm;
+    if (radix_sort_pairs(s, m, bits, &ks, &perm))
+        return QZ_FAILURE;
+    cudaMemsetAsync(cell_seg, 0xFF, (size_t)ncells_box * sizeof(int), s->stream);
+    if (m > 0)
+    {
+        launch(s, QZ_PROF_DEPOSIT, 8.0 * m, k_seg_heads, dim3(blocks_for(m, 256)), dim3(256), m,
+               ks, s->seg_head);
+        if (scan_exclusive(s, s->seg_head, s->seg_id, m))
+            return QZ_FAILURE;
+        launch(s, QZ_PROF_DEPOSIT, 12.0 * m, k_seg_fill, dim3(blocks_for(m, 256)), dim3(256), m,
+               ks, s->seg_head, s->seg_id, s->seg_start, s->seg_cell, cell_seg, s->flags);
+    }
+    else
+        cudaMemsetAsync(s->flags + F_NSEG, 0, sizeof(int), s->stream);
+    *ks_out = ks;
+    *perm_out = perm;
+    return QZ_SUCCESS;
+}
+
 int deposit_head(qz_sim *s)
 {
     const long n = s->n;
@@ -225,13 +252,8 @@ int deposit_head(qz_sim *s)
         bits++;
     unsigned *ks;
     int *perm;
-    if (radix_sort_pairs(s, n, bits, &ks, &perm))
+    if (deposit_segments(s, n, bits, s->cell_seg, B * B * B, &ks, &perm))
         return QZ_FAILURE;
-    launch(s, QZ_PROF_DEPOSIT, 8.0 * n, k_seg_heads, dim3(blocks_for(n, 256)), dim3(256), n, ks, s->seg_head);
-    if (scan_exclusive(s, s->seg_head, s->seg_id, n))
-        return QZ_FAILURE;
-    cudaMemsetAsync(s->cell_seg, 0xFF, (size_t)(B * B * B) * sizeof(int), s->stream);
-    launch(s, QZ_PROF_DEPOSIT, 12.0 * n, k_seg_fill, dim3(blocks_for(n, 256)), dim3(256), n, ks, s->seg_head, s->seg_id, s->seg_start, s->seg_cell, s->cell_seg, s->flags);
     const double H = 1.0 / (1 << L);
     const double coeff = 4.0 * s->cfg.G * QZ_PI_D / (H * H * H);
     int sms = 148;
