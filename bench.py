@@ -4,8 +4,14 @@
                     [--workload NAME]
 
 A step is one leapfrog step of QUANTIZER's main loop (main.c:375-481 with a
-fixed dt): kick-drift, reset, CIC deposit, head Poisson solve to the
-reference's thresholds, gradient, CIC gather, kick.  Metric: particle-steps/s.
+fixed dt): kick-drift, reset, refinement-tree rebuild, CIC deposit on every
+level, Poisson solves to the reference's thresholds (head multigrid, then the
+refinement levels by conjugate gradient), gradients, CIC gather from each
+particle's finest node, kick.  Metric: particle-steps/s.  The default workload
+is the 1M-particle Plummer sphere on a 128^3 head with 3 refinement levels; the
+value is the mixed-precision form (FP32 head smoothing inside FP64 defect
+correction), with the plain FP64 drop-in and the force error between the two
+reported in "plain_fp64".
 
 * value  -- whole-job throughput with the state resident in HBM; the device
   time of exactly K steps (CUDA events on the library stream), L2 flushed
@@ -23,9 +29,9 @@ reference's thresholds, gradient, CIC gather, kick.  Metric: particle-steps/s.
 --impl reference times the reference's CPU implementation of the same workload
 with all host threads (OpenMP), on rank 0 only.
 
-Multi-GPU (torchrun): the head-only path has no exchange step, so each rank
-runs an independent replica (different seed); value = all ranks' particle
-steps / max-over-ranks device time ("scaling": "weak").
+Multi-GPU (torchrun): the step has no exchange between independent
+simulations, so each rank runs its own replica (different seed); value = all
+ranks' particle steps / max-over-ranks device time ("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -43,10 +49,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # Plummer N=10,000, a=0.05, head 32^3, FP64, dt = 1e-3 t_cr, 100 steps
-    "plummer10k_head32": dict(n=10000, a=0.05, lmin=5, steps=100, precision=0),
+    # Plummer N=10,000, a=0.05, head 32^3, no refinement, FP64, dt = 1e-3 t_cr
+    "plummer10k_head32": dict(n=10000, a=0.05, lmin=5, levels=0, ref_ptcl=4, steps=100,
+                              precision=0, cpu_steps=100, ref_steps=100),
+    # Plummer N=1,048,576, a=0.02, head 128^3, refinement up to 3 levels above the head,
+    # a cell refines when it holds more than 8 particles; FP32 smoothing inside FP64
+    # defect correction for the head solve, reported beside the plain FP64 drop-in
+    "plummer1m_head128_amr3": dict(n=1048576, a=0.02, lmin=7, levels=3, ref_ptcl=9, steps=100,
+                                   precision=1, cpu_steps=3, ref_steps=10),
 }
-DEFAULT_WORKLOAD = "plummer10k_head32"
+DEFAULT_WORKLOAD = "plummer1m_head128_amr3"
 METRIC = "particle-steps/s"
 
 
@@ -130,12 +142,16 @@ def run_reference_cpu(wl: dict, steps: int, threads: int, seed: int) -> dict:
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "ic.bin")
         ics.write_ic(p, ic)
-        r = O.run_reference(p, td, lmin=wl["lmin"], steps=steps, dt=dt, threads=threads)
+        r = O.run_reference(p, td, lmin=wl["lmin"], lmax=wl["lmin"] + wl["levels"],
+                            ref_ptcl=wl["ref_ptcl"], steps=steps, dt=dt, threads=threads)
     return {"kind": "reference", "value": wl["n"] * steps / r["loop_s"], "seconds": r["loop_s"],
             "steps": steps}
 
 
 def run_port_cpu(wl: dict, steps: int, seed: int) -> dict:
+    if wl["levels"]:
+        raise RuntimeError("the CPU restatement covers the head-only path; refinement needs "
+                           "the compiled reference (oracle/_ref)")
     import numpy as np
     from oracle import oracle as O
     from quantizer_b200 import ics
@@ -166,23 +182,27 @@ def main() -> int:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     config = {"workload": args.workload, "particles": wl["n"], "head_grid": 2 ** wl["lmin"],
-              "lmax_minus_lmin": 0, "dt": "1e-3 crossing time", "precision":
-              "fp64" if wl["precision"] == 0 else "fp32-in-fp64", "residual_tol": 1e-10,
-              "l2": "flushed between timed steps (256 MiB write)", "replicas": world}
+              "lmax_minus_lmin": wl["levels"], "refine_above_particles": wl["ref_ptcl"] - 1,
+              "dt": "1e-3 crossing time", "precision":
+              "fp64" if wl["precision"] == 0 else "fp32 head smoothing in fp64 defect correction",
+              "residual_tol": 1e-10, "l2": "flushed between timed steps (256 MiB write)",
+              "replicas": world}
 
     if args.impl == "reference":
         if rank != 0:
             return 0
         threads = os.cpu_count() or 1
-        r = run_reference_cpu(wl, K, threads, seed=1)
+        Kr = min(K, wl["ref_steps"])
+        r = run_reference_cpu(wl, Kr, threads, seed=1)
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
-                "n_gpus": args.gpus, "steps": K, "warmup": 0,
-                "ms_per_step": 1e3 * r["seconds"] / K, "higher_is_better": True,
+                "n_gpus": args.gpus, "steps": Kr, "warmup": 0,
+                "ms_per_step": 1e3 * r["seconds"] / Kr, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config,
                 "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": threads,
                                  "kind": r.get("kind", "reference"),
-                                 "sample": f"{K} steps of the workload (whole step loop)"},
+                                 "sample": f"{Kr} steps of the workload after its step-0 "
+                                           "forces (whole step loop, OpenMP threads)"},
                 "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -206,24 +226,29 @@ def main() -> int:
 
     ic = ics.plummer(wl["n"], a=wl["a"], seed=1 + rank)
     dt = 1e-3 * ics.crossing_time(wl["a"])
-    sim = core.Simulation(ic, wl["lmin"], precision=wl["precision"])
+    simcfg = dict(lmax=wl["lmin"] + wl["levels"], ref_ptcl=wl["ref_ptcl"])
+    sim = core.Simulation(ic, wl["lmin"], precision=wl["precision"], **simcfg)
     ext = torch.cuda.ExternalStream(sim.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     sim.init_forces()
     for _ in range(W):
         sim.step(dt, 1)
 
-    def timed_steps(fn, k):
+    def timed_steps_on(sm, fn, k):
+        st = torch.cuda.ExternalStream(sm.stream, device=dev)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(k)]
         for i in range(k):
-            with torch.cuda.stream(ext):
+            with torch.cuda.stream(st):
                 flush.add_(1.0)
-                evs[i][0].record(ext)
+                evs[i][0].record(st)
             fn()
-            evs[i][1].record(ext)
+            evs[i][1].record(st)
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs)
+
+    def timed_steps(fn, k):
+        return timed_steps_on(sim, fn, k)
 
     # ---- device-resident timed region -------------------------------------------------
     st0 = sim.stats()
@@ -234,6 +259,7 @@ def main() -> int:
     st1 = sim.stats()
     launches = int(st1.kernel_launches - st0.kernel_launches)
     vcycles = int(st1.vcycles_total - st0.vcycles_total)
+    cgit = int(st1.cg_iterations - st0.cg_iterations)
     t = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -257,12 +283,13 @@ def main() -> int:
     e2e_value = world * wl["n"] * Ke / (float(t.item()) / 1e3)
 
     # ---- profiled pass: per-kernel-category device time --------------------------------
-    Kp = min(K, 20)
+    Kp = min(K, 5)
     core.profile_reset(sim)
     core.profile_enable(sim, True)
     sim.set_particles({**p, "m": ic["m"]})
     sim.set_accelerations(p["ax"], p["ay"], p["az"])
     sim.step(dt, Kp)
+    sim.synchronize()
     prof = core.profile_read(sim)
     core.profile_enable(sim, False)
     dom = max(prof, key=lambda c: prof[c][1])
@@ -285,12 +312,46 @@ def main() -> int:
                    "GBps": round((v[2] / (v[1] / 1e3)) / 1e9, 1) if v[1] > 0 else 0.0}
                for c, v in prof.items() if v[0]}
 
+    # the plain FP64 drop-in on the same workload, and the force error of the
+    # mixed-precision form against it after the same steps from the same state
+    plain = None
+    if wl["precision"] != 0:
+        st_pos = sim.particles()
+        ref_sim = core.Simulation(ic, wl["lmin"], precision=0, **simcfg)
+        ref_sim.init_forces()
+        for _ in range(W):
+            ref_sim.step(dt, 1)
+        barrier()
+        ms_plain = timed_steps_on(ref_sim, lambda: ref_sim.step(dt, 1), K)
+        t = torch.tensor([ms_plain], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        plain_value = world * wl["n"] * K / (float(t.item()) / 1e3)
+        # force error: both forms from one state, one step
+        state = {**st_pos, "m": ic["m"]}
+        errs = []
+        outs = []
+        for sm in (sim, ref_sim):
+            sm.set_particles(state)
+            sm.set_accelerations(state["ax"], state["ay"], state["az"])
+            sm.step(dt, 1)
+            outs.append(sm.particles())
+        a_m = np.sqrt(sum(outs[0][k] ** 2 for k in ("ax", "ay", "az")))
+        a_p = np.sqrt(sum(outs[1][k] ** 2 for k in ("ax", "ay", "az")))
+        diff = np.sqrt(sum((outs[0][k] - outs[1][k]) ** 2 for k in ("ax", "ay", "az")))
+        errs = diff / np.maximum(a_p, 1e-300)
+        plain = {"value": plain_value, "ms_per_step": float(t.item()) / K,
+                 "max_rel_force_err_mixed_vs_fp64": float(errs.max()),
+                 "median_rel_force_err_mixed_vs_fp64": float(np.median(errs))}
+        ref_sim.close()
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            r = run_reference_cpu(wl, wl["steps"], 1, seed=1)
+            r = run_reference_cpu(wl, wl["cpu_steps"], 1, seed=1)
             cpu = {"value": r["value"], "unit": METRIC, "cores": 1, "kind": r.get("kind", "reference"),
-                   "sample": f"{r['steps']} steps of the same workload, reference default 1 thread"}
+                   "sample": f"{r['steps']} steps of the same workload after its step-0 forces, "
+                             "reference default 1 thread"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -304,7 +365,9 @@ def main() -> int:
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 80 * n,
                         "d2h_bytes_per_step": 72 * n},
                 "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
-                "vcycles_per_step": vcycles / K, "clocks": clk.summary(), "kernels": kernels}
+                "vcycles_per_step": vcycles / K, "cg_iterations_per_step": cgit / K,
+                "tree": {"levels": st1.levels, "nodes": st1.nodes},
+                "plain_fp64": plain, "clocks": clk.summary(), "kernels": kernels}
         print(json.dumps(line), flush=True)
     sim.close()
     if world > 1:

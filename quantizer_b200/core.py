@@ -332,7 +332,7 @@ def ptcl_idx_to_box_idx(lv: int, box_ts: tuple, box_real_dim: tuple, x, y, z) ->
 
 # -- per-launch profiler ---------------------------------------------------------------
 PROF_CATEGORIES = ("smooth", "restrict", "prolong", "check", "deposit", "sort", "gradient",
-                   "gather", "leapfrog", "other")
+                   "gather", "leapfrog", "other", "tree", "cg")
 
 
 def _prof_sig(lib):

@@ -34,15 +34,18 @@
 //              node whose cell holding it is not refined
 #include <algorithm>
 #include <climits>
+#include <cooperative_groups.h>
 #include <string.h>
 
 #include "qz_internal.cuh"
+
+namespace cgrp = cooperative_groups;
 
 namespace qz {
 
 #define QZ_PI_D 3.14159265358979323846
 constexpr int AMR_MAX_LEVELS = 16;
-constexpr int CG_CHUNK = 2048;
+constexpr int CG_CHUNK = 512;
 constexpr int CG_THREADS = 256;
 
 // ---- small device helpers --------------------------------------------------------------
@@ -1369,26 +1372,252 @@ __global__ void k_cg_copy_old(long total, int nn, const AmrNode *__restrict__ no
         pot_old[g] = pot[g];
 }
 
+// The whole conjugate-gradient solve of one level in one cooperative launch
+// (conjugate_gradient.c:322-463 for every node of the level at once).  Per
+// iteration, with a grid-wide barrier after each phase:
+//   A   Ap = -(1/H^2) L p on each chunk, partial p.Ap per chunk
+//   R1  per node (one warp): alpha = rsold / sum of the node's p.Ap partials
+//   B   pot += alpha p, r -= alpha Ap, partial r.r per chunk; on check
+//       iterations the ratio test (poisson_error.c:36-81) on the updated pot
+//   R2  per node: rsnew, beta = rsnew / rsold; on check iterations the residual
+//       test (poisson_error.c:236-254): converged nodes stop (the reference
+//       returns before updating p), failed ones refresh pot_old; rsold = rsnew
+//   C   p = r + beta p on active nodes; pot_old <- pot on the grids of nodes
+//       whose check failed
+// Node sums add the chunk partials in a fixed lane / shuffle order, so the
+// result does not depend on scheduling.  Every block runs the same loop and
+// reaches every barrier; the loop ends when all nodes converged or at the
+// iteration cap.
+struct CgArgs {
+    const AmrChunk *chunks;
+    int nchunks;
+    const int *intr;
+    const AmrNode *nodes;
+    int nn;
+    const int *node_chunk; // per node: first chunk, end chunk
+    const double *d;
+    double *pot, *pot_old, *r, *p, *Ap;
+    double *part1, *part2; // per chunk
+    double *ns;            // per node: rsold, alpha, beta
+    int *conv;             // per node: converged (0/1)
+    int *rfail;            // per node: ratio test failed at this check
+    int *refresh;          // per node: pot_old refresh at this check
+    long grid_total;
+    double tol, tol2, G;
+    int every;
+    long cap_it;
+    int *status; // [0] iterations run, [1] all converged
+};
+
+// Sum of node q's chunk partials by one warp: lane-strided partial sums, then
+// a fixed xor-shuffle tree (the same order on every call).
+__device__ __forceinline__ double warp_node_sum(const double *part, const int *node_chunk, int q,
+                                                int lane)
+{
+    double s = 0.0;
+    for (int c = node_chunk[2 * q] + lane; c < node_chunk[2 * q + 1]; c += 32)
+        s += part[c];
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+__global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
+{
+    cgrp::grid_group grid = cgrp::this_grid();
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    // initial residual, p = r
+    for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+    {
+        const AmrChunk C = A.chunks[c];
+        const AmrNode N = A.nodes[C.node];
+        const double H = 1.0 / (1 << N.lv);
+        const double oh2 = 1.0 / (H * H);
+        const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+        double acc = 0.0;
+        for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+        {
+            const long g = A.intr[e];
+            const double *pt = A.pot;
+            double rv = A.d[g] + oh2 * (6.0 * pt[g] - pt[g + 1] - pt[g - 1] - pt[g + sy] -
+                                        pt[g - sy] - pt[g + sz] - pt[g - sz]);
+            A.r[g] = rv;
+            A.p[g] = rv;
+            acc += rv * rv;
+        }
+        double t = block_sum_d(acc, sh);
+        if (threadIdx.x == 0)
+            A.part2[c] = t;
+    }
+    grid.sync();
+    for (long q = gwarp; q < A.nn; q += nwarps)
+    {
+        double rs = warp_node_sum(A.part2, A.node_chunk, (int)q, lane);
+        if (lane == 0)
+        {
+            A.ns[3 * q] = rs;
+            A.conv[q] = 0;
+            A.rfail[q] = 0;
+            A.refresh[q] = 0;
+        }
+    }
+    grid.sync();
+    long it = 0;
+    bool all_done = false;
+    const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
+    while (it < A.cap_it && !all_done)
+    {
+        it++;
+        const bool check = (it % A.every) == 0;
+        // A: Ap and p.Ap
+        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+        {
+            const AmrChunk C = A.chunks[c];
+            if (A.conv[C.node])
+                continue;
+            const AmrNode N = A.nodes[C.node];
+            const double H = 1.0 / (1 << N.lv);
+            const double oh2 = 1.0 / (H * H);
+            const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+            double acc = 0.0;
+            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+            {
+                const long g = A.intr[e];
+                const double *pp = A.p;
+                double a = -oh2 * (6.0 * pp[g] - pp[g + 1] - pp[g - 1] - pp[g + sy] - pp[g - sy] -
+                                   pp[g + sz] - pp[g - sz]);
+                A.Ap[g] = a;
+                acc += pp[g] * a;
+            }
+            double t = block_sum_d(acc, sh);
+            if (threadIdx.x == 0)
+                A.part1[c] = t;
+        }
+        grid.sync();
+        // R1: alpha
+        for (long q = gwarp; q < A.nn; q += nwarps)
+        {
+            if (A.conv[q])
+                continue;
+            double dot = warp_node_sum(A.part1, A.node_chunk, (int)q, lane);
+            if (lane == 0)
+                A.ns[3 * q + 1] = A.ns[3 * q] / dot;
+        }
+        grid.sync();
+        // B: pot, r, r.r, ratio test
+        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+        {
+            const AmrChunk C = A.chunks[c];
+            if (A.conv[C.node])
+                continue;
+            const double alpha = A.ns[3 * C.node + 1];
+            double acc = 0.0;
+            int fail = 0;
+            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+            {
+                const long g = A.intr[e];
+                double pv = A.pot[g] + alpha * A.p[g];
+                A.pot[g] = pv;
+                double rv = A.r[g] - alpha * A.Ap[g];
+                A.r[g] = rv;
+                acc += rv * rv;
+                if (check)
+                {
+                    double ratio = pv / A.pot_old[g];
+                    if ((tm > ratio) || (tp < ratio))
+                        fail = 1;
+                }
+            }
+            double t = block_sum_d(acc, sh);
+            if (threadIdx.x == 0)
+                A.part2[c] = t;
+            if (check && __syncthreads_or(fail) && threadIdx.x == 0)
+                atomicOr(&A.rfail[C.node], 1);
+        }
+        grid.sync();
+        // R2: rsnew, beta, convergence
+        for (long q = gwarp; q < A.nn; q += nwarps)
+        {
+            if (A.conv[q])
+                continue;
+            double rsnew = warp_node_sum(A.part2, A.node_chunk, (int)q, lane);
+            if (lane == 0)
+            {
+                A.ns[3 * q + 2] = rsnew / A.ns[3 * q];
+                A.ns[3 * q] = rsnew;
+                A.refresh[q] = 0;
+                if (check)
+                {
+                    const AmrNode N = A.nodes[q];
+                    const double H = 1.0 / (1 << N.lv);
+                    const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+                    const double tt = A.tol * rm;
+                    if (!A.rfail[q] && rsnew < N.nintr * tt * tt)
+                        A.conv[q] = 1;
+                    else
+                        A.refresh[q] = 1;
+                    A.rfail[q] = 0;
+                }
+            }
+        }
+        grid.sync();
+        // C: p update, pot_old refresh
+        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+        {
+            const AmrChunk C = A.chunks[c];
+            if (A.conv[C.node])
+                continue;
+            const double beta = A.ns[3 * C.node + 2];
+            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+            {
+                const long g = A.intr[e];
+                A.p[g] = A.r[g] + beta * A.p[g];
+            }
+        }
+        if (check)
+        {
+            for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < A.grid_total;
+                 g += (long)gridDim.x * blockDim.x)
+                if (A.refresh[find_node(A.nodes, A.nn, g, 0)])
+                    A.pot_old[g] = A.pot[g];
+            int pending = 0;
+            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
+                pending |= !A.conv[q];
+            all_done = !__syncthreads_or(pending);
+        }
+        grid.sync();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        A.status[0] = (int)it;
+        A.status[1] = all_done ? 1 : 0;
+    }
+}
+
 static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
     // chunks over each node's interior list
     L.hchunks.clear();
-    std::vector<int> hint(6L * nn, 0);
+    std::vector<int> node_chunk(2L * nn, 0);
     for (int q = 0; q < nn; q++)
     {
-        hint[6 * q + I_CB] = (int)L.hchunks.size();
+        node_chunk[2 * q] = (int)L.hchunks.size();
         const AmrNode &N = L.h[q];
         for (int b = N.intr_off; b < N.intr_off + N.nintr; b += CG_CHUNK)
             L.hchunks.push_back({q, b, std::min(b + CG_CHUNK, N.intr_off + N.nintr)});
-        hint[6 * q + I_CE] = (int)L.hchunks.size();
+        node_chunk[2 * q + 1] = (int)L.hchunks.size();
     }
     L.nchunks = (int)L.hchunks.size();
     if (L.nchunks == 0)
         return QZ_SUCCESS;
-    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(L.nchunks) ||
-        !L.nscal.ensure(6L * nn) || !L.nint.ensure(6L * nn) || !L.r.ensure(L.grid_total) ||
+    // nint: node_chunk (2 nn) | conv (nn) | rfail (nn) | refresh (nn) | status (2)
+    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(2L * L.nchunks) ||
+        !L.nscal.ensure(3L * nn) || !L.nint.ensure(5L * nn + 2) || !L.r.ensure(L.grid_total) ||
         !L.p.ensure(L.grid_total) || !L.Ap.ensure(L.grid_total))
     {
         set_error("cg buffers");
@@ -1396,65 +1625,80 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     }
     if (!check_cuda(cudaMemcpyAsync(L.chunks.p, L.hchunks.data(), L.nchunks * sizeof(AmrChunk),
                                     cudaMemcpyHostToDevice, s->stream), "chunks") ||
-        !check_cuda(cudaMemcpyAsync(L.nint.p, hint.data(), 6L * nn * sizeof(int),
-                                    cudaMemcpyHostToDevice, s->stream), "cg ints") ||
-        !check_cuda(cudaStreamSynchronize(s->stream), "cg set-up"))
+        !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), 2L * nn * sizeof(int),
+                                    cudaMemcpyHostToDevice, s->stream), "cg ints"))
         return QZ_FAILURE;
     cudaMemsetAsync(L.p.p, 0, L.grid_total * sizeof(double), s->stream);
-    const dim3 gc(L.nchunks), bc(CG_THREADS), gn(blocks_for(nn, 128)), bn(128);
-    const double intr_bytes = (double)L.intr_total;
-    launch(s, QZ_PROF_CG, 40.0 * intr_bytes, k_cg_init, gc, bc, L.chunks.p, L.intr.p, L.nodes.p,
-           L.d, L.pot, L.r.p, L.p.p, L.chunk_part.p);
-    launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 0, L.nodes.p, L.chunk_part.p,
-           L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
+    cudaMemsetAsync(L.nint.p + 2 * nn, 0, (3L * nn + 2) * sizeof(int), s->stream);
     // iteration cap of the reference per node: min(node grid size, max_iter);
     // nodes iterate in lockstep, so the level runs to the largest cap
     long cap_it = 0;
     for (auto &N : L.h)
         cap_it = std::max(cap_it, std::min((long)c.max_iter,
                                            (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1)));
-    const int every = c.check_every > 0 ? c.check_every : 1;
-    int converged = 0;
-    long it = 0;
-    cudaMemsetAsync(s->flags + F_AMR_CONV, 0, sizeof(int), s->stream);
-    while (it < cap_it && converged < nn)
+    CgArgs A;
+    A.chunks = L.chunks.p;
+    A.nchunks = L.nchunks;
+    A.intr = L.intr.p;
+    A.nodes = L.nodes.p;
+    A.nn = nn;
+    A.node_chunk = L.nint.p;
+    A.d = L.d;
+    A.pot = L.pot;
+    A.pot_old = L.pot_old;
+    A.r = L.r.p;
+    A.p = L.p.p;
+    A.Ap = L.Ap.p;
+    A.part1 = L.chunk_part.p;
+    A.part2 = L.chunk_part.p + L.nchunks;
+    A.ns = L.nscal.p;
+    A.conv = L.nint.p + 2 * nn;
+    A.rfail = L.nint.p + 3 * nn;
+    A.refresh = L.nint.p + 4 * nn;
+    A.status = L.nint.p + 5 * nn;
+    A.grid_total = L.grid_total;
+    A.tol = c.tol;
+    A.tol2 = c.tol2;
+    A.G = c.G;
+    A.every = c.check_every > 0 ? c.check_every : 1;
+    A.cap_it = cap_it;
+    int per_sm = 0, sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    if (!check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent,
+                                                                  CG_THREADS, 0), "occupancy"))
+        return QZ_FAILURE;
+    int blocks = std::max(1, std::min(per_sm * sms, L.nchunks));
+    void *args[] = {&A};
+    cudaEvent_t eb = nullptr, ee = nullptr;
+    if (s->prof)
     {
-        for (int q = 0; q < every && it < cap_it; q++)
-        {
-            it++;
-            launch(s, QZ_PROF_CG, 24.0 * intr_bytes, k_cg_Ap, gc, bc, L.chunks.p, L.intr.p,
-                   L.nodes.p, L.nint.p, L.p.p, L.Ap.p, L.chunk_part.p);
-            launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 1, L.nodes.p,
-                   L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
-            launch(s, QZ_PROF_CG, 48.0 * intr_bytes, k_cg_update, gc, bc, L.chunks.p, L.intr.p,
-                   L.nint.p, L.nscal.p, L.p.p, L.Ap.p, L.pot, L.r.p, L.chunk_part.p);
-            launch(s, QZ_PROF_CG, 8.0 * L.nchunks, k_cg_node, gn, bn, nn, 2, L.nodes.p,
-                   L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
-            if (it % every == 0)
-            {
-                launch(s, QZ_PROF_CG, 20.0 * intr_bytes, k_cg_ratio, gc, bc, L.chunks.p, L.intr.p,
-                       L.nint.p, L.pot, L.pot_old, 1.0 - c.tol2, 1.0 + c.tol2);
-                launch(s, QZ_PROF_CG, 8.0 * nn, k_cg_node, gn, bn, nn, 3, L.nodes.p,
-                       L.chunk_part.p, L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
-                launch(s, QZ_PROF_CG, 16.0 * L.grid_total, k_cg_copy_old,
-                       dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, nn,
-                       L.nodes.p, L.nint.p, L.pot, L.pot_old);
-            }
-            launch(s, QZ_PROF_CG, 24.0 * intr_bytes, k_cg_p, gc, bc, L.chunks.p, L.intr.p,
-                   L.nint.p, L.nscal.p, L.r.p, L.p.p);
-            launch(s, QZ_PROF_CG, 8.0 * nn, k_cg_node, gn, bn, nn, 4, L.nodes.p, L.chunk_part.p,
-                   L.nscal.p, L.nint.p, c.tol, c.G, s->flags);
-        }
-        int cv;
-        if (!read_ints(s, s->flags + F_AMR_CONV, 1, &cv))
-            return QZ_FAILURE;
-        converged = cv;
+        eb = prof_event(s);
+        ee = prof_event(s);
+        cudaEventRecord(eb, s->stream);
     }
-    s->stats.cg_iterations += it;
-    if (converged < nn)
+    if (!check_cuda(cudaLaunchCooperativeKernel((void *)k_cg_persistent, dim3(blocks),
+                                                dim3(CG_THREADS), args, 0, s->stream),
+                    "cooperative cg"))
+        return QZ_FAILURE;
+    s->stats.kernel_launches++;
+    if (s->prof)
     {
-        set_error("the precision was not reached in refinement level %d after %ld conjugate "
-                  "gradient iterations", level_index, it);
+        cudaEventRecord(ee, s->stream);
+        s->prof_pending.push_back({QZ_PROF_CG, 0.0, eb, ee});
+    }
+    int st[2];
+    if (!read_ints(s, A.status, 2, st))
+        return QZ_FAILURE;
+    s->stats.cg_iterations += st[0];
+    if (s->prof)
+    {
+        // bytes of the launch: per iteration Ap 16, update 48, p 24 B per interior point
+        s->prof_pending.back().bytes = 88.0 * L.intr_total * st[0];
+    }
+    if (!st[1])
+    {
+        set_error("the precision was not reached in refinement level %d after %d conjugate "
+                  "gradient iterations", level_index, st[0]);
         return QZ_FAILURE;
     }
     return check_cuda(cudaGetLastError(), "cg") ? QZ_SUCCESS : QZ_FAILURE;

@@ -51,7 +51,8 @@ def _multigrid(args) -> dict:
 def _step(args) -> dict:
     ic = ics.plummer(args.particles, a=args.a, seed=1)
     dt = 1e-3 * ics.crossing_time(args.a)
-    with core.Simulation(ic, args.lmin, precision=args.precision) as sim:
+    with core.Simulation(ic, args.lmin, lmax=args.lmin + args.levels, ref_ptcl=args.ref_ptcl,
+                         precision=args.precision) as sim:
         sim.init_forces()
         sim.step(dt, 1)
         st0 = sim.stats()
@@ -64,10 +65,13 @@ def _step(args) -> dict:
         core.profile_enable(sim, True)
         sim.step(dt, args.steps)
         prof = core.profile_read(sim)
+        st2 = sim.stats()
     kern = {c: {"launches": v[0], "ms": round(v[1], 4),
                 "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else 0.0}
             for c, v in prof.items() if v[0]}
     return {"kernel": "step", "particles": args.particles, "lmin": args.lmin,
+            "levels": st2.levels, "nodes": st2.nodes,
+            "cg_iterations_per_step": (st1.cg_iterations - st0.cg_iterations) / args.steps,
             "steps": args.steps, "wall_ms_per_step": 1e3 * t / args.steps,
             "vcycles_per_step": (st1.vcycles_total - st0.vcycles_total) / args.steps,
             "launches_per_step": (st1.kernel_launches - st0.kernel_launches) / args.steps,
@@ -85,6 +89,8 @@ def main() -> None:
     ap.add_argument("--a", type=float, default=0.02)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--levels", type=int, default=0, help="refinement levels above the head")
+    ap.add_argument("--ref-ptcl", type=int, default=9)
     args = ap.parse_args()
     fn = {"smooth": _smooth, "multigrid": _multigrid, "step": _step}[args.what]
     print(json.dumps(fn(args)))
