@@ -360,7 +360,9 @@ def main() -> int:
         n = wl["n"]
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if wl["precision"] == 0 else "f64 (f32 head smoothing)",
+                "data": "synthetic",
                 "config": config,
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 80 * n,
                         "d2h_bytes_per_step": 72 * n},
