@@ -333,9 +333,11 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
                   "box_extra >= 2");
         return QZ_FAILURE;
     }
-    if (cfg->bdry != 0 && cfg->bdry != 1)
+    if (cfg->bdry != 1)
     {
-        set_error("qz_create: bdry=%d not supported (0 periodic, 1 reflexive)", cfg->bdry);
+        // the periodic head boundary of initial_potential_and_acceleration_head.c:66-296
+        // and outflow particle removal are not built
+        set_error("qz_create: bdry=%d not supported (1 reflexive only)", cfg->bdry);
         return QZ_FAILURE;
     }
     if (cfg->force_stencil != 0 || cfg->smoother < 0 || cfg->smoother > 1 || cfg->cycle < 0 ||
