@@ -193,6 +193,28 @@ QZ_API int qz_jacobi(double *phi, const double *rho, int gridsize, int iter_max,
 QZ_API int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, int gridsize,
                  int type_multigrid);
 
+/* Weighted Jacobi smoothing (the sweeps of jacobi above) on DEVICE arrays the
+ * caller owns, that allocates no device memory: no cudaMalloc, no cudaFree, no
+ * allocating library routine.  No counterpart in the reference, whose jacobi
+ * mallocs its ping-pong copy on every call.  It is for callers that cannot
+ * allocate: code that runs inside a host framework whose caching allocator or
+ * memory pool already owns the device memory budget (a raw cudaMalloc there can
+ * fail or fragment the pool), and loops that must not allocate once running,
+ * because cudaMalloc and cudaFree synchronise the whole device and stall every
+ * other stream.  The ping-pong copy lives in a fixed device array inside the
+ * library, of QZ_NOALLOC_MAX_GRID^3 doubles (2.2 MB), which every GPU that
+ * loads the library holds until the process exits; gridsize above
+ * QZ_NOALLOC_MAX_GRID is rejected with an error.  phi (in/out) and rho are
+ * gridsize^3 float64 device arrays; stream is a cudaStream_t (NULL for the
+ * default stream); the call only enqueues work on it.  The first call on a
+ * device looks up the array's device address once (make that first call before
+ * any stream capture).  All calls share the array, which keeps the last call's
+ * contents (each call starts by copying phi into it); calls that overlap on
+ * the GPU race on it, so serialise them. */
+#define QZ_NOALLOC_MAX_GRID 65
+QZ_API int qz_jacobi_noalloc(double *phi, const double *rho, int gridsize, int iter_max,
+                             double w, void *stream);
+
 /* Batched ptcl_idx_to_box_idx for one non-periodic node geometry. */
 QZ_API int qz_ptcl_idx_to_box_idx(int lv, int box_ts_x, int box_ts_y, int box_ts_z,
                            int box_real_dim_x, int box_real_dim_y, long n, const double *x,
