@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <climits>
 #include <cooperative_groups.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "qz_internal.cuh"
@@ -543,7 +544,7 @@ static void free_level(AmrLevel &L)
     for (auto *b : ib)
         b->release();
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
-                          &L.nscal, &L.chunk_part};
+                          &L.chunk_part};
     for (auto *b : db)
         b->release();
     L.nodes.release();
@@ -1180,214 +1181,26 @@ __global__ void k_copy_d(long n, const double *__restrict__ a, double *__restric
         b[i] = a[i];
 }
 
-// per-node scalar slots in nscal (6 per node) and nint (6 per node)
-enum { S_RSOLD = 0, S_RSNEW = 1, S_ALPHA = 2, S_BETA = 3, S_DOT = 4, S_RM = 5 };
-enum { I_CONV = 0, I_RFAIL = 1, I_CB = 2, I_CE = 3, I_CHECKED = 4 };
-
-// Conjugate gradient on the interior points of every node of a level
-// (conjugate_gradient.c:322-463).  Chunk kernels work on [begin, end) of the
-// interior list of one node and write one partial sum per chunk; node kernels
-// add a node's partials in chunk order.
-__global__ void k_cg_init(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
-                          const AmrNode *__restrict__ nodes, const double *__restrict__ d,
-                          const double *__restrict__ pot, double *__restrict__ r,
-                          double *__restrict__ p, double *__restrict__ part)
-{
-    __shared__ double sh[32];
-    const AmrChunk C = ch[blockIdx.x];
-    const AmrNode N = nodes[C.node];
-    const double H = 1.0 / (1 << N.lv);
-    const double oh2 = 1.0 / (H * H);
-    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
-    double acc = 0.0;
-    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-    {
-        const long g = intr[e];
-        double rv = d[g] + oh2 * (6.0 * pot[g] - pot[g + 1] - pot[g - 1] - pot[g + sy] -
-                                  pot[g - sy] - pot[g + sz] - pot[g - sz]);
-        r[g] = rv;
-        p[g] = rv;
-        acc += rv * rv;
-    }
-    double t = block_sum_d(acc, sh);
-    if (threadIdx.x == 0)
-        part[blockIdx.x] = t;
-}
-
-__global__ void k_cg_Ap(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
-                        const AmrNode *__restrict__ nodes, const int *__restrict__ nint,
-                        const double *__restrict__ p, double *__restrict__ Ap,
-                        double *__restrict__ part)
-{
-    __shared__ double sh[32];
-    const AmrChunk C = ch[blockIdx.x];
-    if (nint[6 * C.node + I_CONV])
-        return;
-    const AmrNode N = nodes[C.node];
-    const double H = 1.0 / (1 << N.lv);
-    const double oh2 = 1.0 / (H * H);
-    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
-    double acc = 0.0;
-    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-    {
-        const long g = intr[e];
-        double a = -oh2 * (6.0 * p[g] - p[g + 1] - p[g - 1] - p[g + sy] - p[g - sy] - p[g + sz] -
-                           p[g - sz]);
-        Ap[g] = a;
-        acc += p[g] * a;
-    }
-    double t = block_sum_d(acc, sh);
-    if (threadIdx.x == 0)
-        part[blockIdx.x] = t;
-}
-
-__global__ void k_cg_update(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
-                            const int *__restrict__ nint, const double *__restrict__ nscal,
-                            const double *__restrict__ p, const double *__restrict__ Ap,
-                            double *__restrict__ pot, double *__restrict__ r,
-                            double *__restrict__ part)
-{
-    __shared__ double sh[32];
-    const AmrChunk C = ch[blockIdx.x];
-    if (nint[6 * C.node + I_CONV])
-        return;
-    const double alpha = nscal[6 * C.node + S_ALPHA];
-    double acc = 0.0;
-    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-    {
-        const long g = intr[e];
-        pot[g] += alpha * p[g];
-        double rv = r[g] - alpha * Ap[g];
-        r[g] = rv;
-        acc += rv * rv;
-    }
-    double t = block_sum_d(acc, sh);
-    if (threadIdx.x == 0)
-        part[blockIdx.x] = t;
-}
-
-__global__ void k_cg_p(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
-                       const int *__restrict__ nint, const double *__restrict__ nscal,
-                       const double *__restrict__ r, double *__restrict__ p)
-{
-    const AmrChunk C = ch[blockIdx.x];
-    if (nint[6 * C.node + I_CONV])
-        return;
-    const double beta = nscal[6 * C.node + S_BETA];
-    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-    {
-        const long g = intr[e];
-        p[g] = r[g] + beta * p[g];
-    }
-}
-
-// Ratio test of poisson_error.c:36-81 on a chunk of interior points.
-__global__ void k_cg_ratio(const AmrChunk *__restrict__ ch, const int *__restrict__ intr,
-                           int *__restrict__ nint, const double *__restrict__ pot,
-                           const double *__restrict__ pot_old, double tm, double tp)
-{
-    const AmrChunk C = ch[blockIdx.x];
-    if (nint[6 * C.node + I_CONV])
-        return;
-    int fail = 0;
-    for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-    {
-        const long g = intr[e];
-        double a = pot[g] / pot_old[g];
-        if ((tm > a) || (tp < a))
-            fail = 1;
-    }
-    if (__syncthreads_or(fail) && threadIdx.x == 0)
-        nint[6 * C.node + I_RFAIL] = 1;
-}
-
-// Node stages: 0 rsold from the init partials; 1 alpha = rsold / (p . Ap);
-// 2 rsnew and beta; 3 convergence (poisson_error.c:236-254); 4 rsold = rsnew.
-__global__ void k_cg_node(int nn, int stage, const AmrNode *__restrict__ nodes,
-                          const double *__restrict__ part, double *__restrict__ nscal,
-                          int *__restrict__ nint, double tol, double G, int *__restrict__ flags)
-{
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nn)
-        return;
-    int *I = nint + 6 * q;
-    double *S = nscal + 6 * q;
-    if (stage != 0 && I[I_CONV])
-        return;
-    double sum = 0.0;
-    if (stage <= 2)
-        for (int c = I[I_CB]; c < I[I_CE]; c++)
-            sum += part[c];
-    if (stage == 0)
-    {
-        S[S_RSOLD] = sum;
-        I[I_CONV] = 0;
-        I[I_RFAIL] = 0;
-        const AmrNode N = nodes[q];
-        const double H = 1.0 / (1 << N.lv);
-        S[S_RM] = 4.0 * G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
-    }
-    else if (stage == 1)
-    {
-        S[S_DOT] = sum;
-        S[S_ALPHA] = S[S_RSOLD] / sum;
-    }
-    else if (stage == 2)
-    {
-        S[S_RSNEW] = sum;
-        S[S_BETA] = sum / S[S_RSOLD];
-    }
-    else if (stage == 3)
-    {
-        const AmrNode N = nodes[q];
-        bool ok = !I[I_RFAIL];
-        if (ok)
-        {
-            double t = tol * S[S_RM];
-            double aux_tol = N.nintr * t * t;
-            ok = S[S_RSNEW] < aux_tol;
-        }
-        I[I_CHECKED] = ok ? 0 : 1; // 1: copy pot to pot_old
-        I[I_RFAIL] = 0;
-        if (ok)
-        {
-            I[I_CONV] = 1;
-            atomicAdd(&flags[F_AMR_CONV], 1);
-        }
-    }
-    else
-        S[S_RSOLD] = S[S_RSNEW];
-}
-
-// pot_old <- pot on the whole grid of every node whose check failed.
-__global__ void k_cg_copy_old(long total, int nn, const AmrNode *__restrict__ nodes,
-                              int *__restrict__ nint, const double *__restrict__ pot,
-                              double *__restrict__ pot_old)
-{
-    long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total)
-        return;
-    int nd = find_node(nodes, nn, g, 0);
-    if (nint[6 * nd + I_CHECKED])
-        pot_old[g] = pot[g];
-}
-
 // The whole conjugate-gradient solve of one level in one cooperative launch
-// (conjugate_gradient.c:322-463 for every node of the level at once).  Per
-// iteration, with a grid-wide barrier after each phase:
-//   A   Ap = -(1/H^2) L p on each chunk, partial p.Ap per chunk
-//   R1  per node (one warp): alpha = rsold / sum of the node's p.Ap partials
-//   B   pot += alpha p, r -= alpha Ap, partial r.r per chunk; on check
-//       iterations the ratio test (poisson_error.c:36-81) on the updated pot
-//   R2  per node: rsnew, beta = rsnew / rsold; on check iterations the residual
-//       test (poisson_error.c:236-254): converged nodes stop (the reference
-//       returns before updating p), failed ones refresh pot_old; rsold = rsnew
-//   C   p = r + beta p on active nodes; pot_old <- pot on the grids of nodes
-//       whose check failed
-// Node sums add the chunk partials in a fixed lane / shuffle order, so the
-// result does not depend on scheduling.  Every block runs the same loop and
-// reaches every barrier; the loop ends when all nodes converged or at the
-// iteration cap.
+// (conjugate_gradient.c:322-463 for every node of the level at once), two
+// phases and two grid-wide barriers per iteration k:
+//   P  (decision for the check at k-1, then) p_{k-1} = r_{k-1} + beta p_{k-2}
+//      with beta = rs_{k-1} / rs_{k-2}, computed by every stencil on the fly for
+//      its seven points (the owner stores it), Ap = -(1/H^2) L p_{k-1} and the
+//      chunk's partial of p.Ap
+//   U  alpha = rs_{k-1} / (p.Ap); pot += alpha p, r -= alpha Ap with Ap
+//      recomputed from the stored p (the same expression, so the same value);
+//      the chunk's partial of r.r; on check iterations the ratio test
+//      (poisson_error.c:36-81) on the updated pot
+// The residual test of a check iteration (poisson_error.c:236-254) is taken at
+// the start of the next P phase: converged nodes stop there (the reference
+// returns before updating p); the others copy pot to pot_old on their interior
+// points, the only points the ratio test reads.  Node scalars are not stored:
+// each block adds the node's chunk partials itself in a fixed order, so every
+// block obtains the same value.  p and the r.r
+// partials are double-buffered by iteration parity; r and both p buffers are
+// zero off the interior points.  Every block runs the same loop and reaches
+// every barrier; it ends when every node converged or after the iteration cap.
 struct CgArgs {
     const AmrChunk *chunks;
     int nchunks;
@@ -1396,40 +1209,68 @@ struct CgArgs {
     int nn;
     const int *node_chunk; // per node: first chunk, end chunk
     const double *d;
-    double *pot, *pot_old, *r, *p, *Ap;
-    double *part1, *part2; // per chunk
-    double *ns;            // per node: rsold, alpha, beta
-    int *conv;             // per node: converged (0/1)
-    int *rfail;            // per node: ratio test failed at this check
-    int *refresh;          // per node: pot_old refresh at this check
-    long grid_total;
+    double *pot, *pot_old, *r;
+    double *pbuf[2];  // p_j in pbuf[j & 1]
+    double *pap;      // per chunk: partial p.Ap
+    double *rr[2];    // per chunk: partial r_j.r_j in rr[j & 1]
+    int *conv;        // per node: converged (0/1)
+    int *rfail[2];    // per node: ratio test failed at check j, in rfail[j & 1]
     double tol, tol2, G;
     int every;
     long cap_it;
     int *status; // [0] iterations run, [1] all converged
 };
 
-// Sum of node q's chunk partials by one warp: lane-strided partial sums, then
-// a fixed xor-shuffle tree (the same order on every call).
-__device__ __forceinline__ double warp_node_sum(const double *part, const int *node_chunk, int q,
-                                                int lane)
+// Sums of node q's chunk partials in two arrays (b may be null), computed by the
+// whole block and returned to every thread: thread t adds chunks t, t + blockDim,
+// ... in order, then a fixed xor-shuffle tree per warp and the warp totals in
+// warp order.  Every block of the launch has the same size, so every block
+// obtains the same two values.
+__device__ __forceinline__ double2 node_sums(const double *a, const double *b,
+                                             const int *node_chunk, int q, double2 *sh2)
 {
-    double s = 0.0;
-    for (int c = node_chunk[2 * q] + lane; c < node_chunk[2 * q + 1]; c += 32)
-        s += part[c];
+    double sa = 0.0, sb = 0.0;
+    for (int c = node_chunk[2 * q] + threadIdx.x; c < node_chunk[2 * q + 1]; c += blockDim.x)
+    {
+        sa += __ldcg(&a[c]);
+        if (b)
+            sb += __ldcg(&b[c]);
+    }
     for (int o = 16; o > 0; o >>= 1)
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
+    {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+        sh2[threadIdx.x >> 5] = make_double2(sa, sb);
+    __syncthreads();
+    double2 t = make_double2(0.0, 0.0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+    {
+        t.x += sh2[w].x;
+        t.y += sh2[w].y;
+    }
+    __syncthreads(); // sh2 is rewritten by the next call
+    return t;
+}
+
+__device__ __forceinline__ double lap7(const double *v, long g, long sy, long sz, double oh2)
+{
+    return -oh2 * (6.0 * v[g] - v[g + 1] - v[g - 1] - v[g + sy] - v[g - sy] - v[g + sz] -
+                   v[g - sz]);
 }
 
 __global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
 {
     cgrp::grid_group grid = cgrp::this_grid();
     __shared__ double sh[32];
-    const int lane = threadIdx.x & 31;
-    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-    // initial residual, p = r
+    __shared__ double2 sh2[CG_THREADS / 32];
+    // nodes without interior points have nothing to solve
+    if (blockIdx.x == 0)
+        for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
+            if (A.node_chunk[2 * q] == A.node_chunk[2 * q + 1])
+                A.conv[q] = 1;
+    // r_0 = d - (-(1/H^2) L pot), partial rs_0
     for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
     {
         const AmrChunk C = A.chunks[c];
@@ -1445,40 +1286,70 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
             double rv = A.d[g] + oh2 * (6.0 * pt[g] - pt[g + 1] - pt[g - 1] - pt[g + sy] -
                                         pt[g - sy] - pt[g + sz] - pt[g - sz]);
             A.r[g] = rv;
-            A.p[g] = rv;
             acc += rv * rv;
         }
         double t = block_sum_d(acc, sh);
         if (threadIdx.x == 0)
-            A.part2[c] = t;
+            A.rr[0][c] = t;
     }
     grid.sync();
-    for (long q = gwarp; q < A.nn; q += nwarps)
-    {
-        double rs = warp_node_sum(A.part2, A.node_chunk, (int)q, lane);
-        if (lane == 0)
-        {
-            A.ns[3 * q] = rs;
-            A.conv[q] = 0;
-            A.rfail[q] = 0;
-            A.refresh[q] = 0;
-        }
-    }
-    grid.sync();
-    long it = 0;
-    bool all_done = false;
     const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
-    while (it < A.cap_it && !all_done)
+    long k = 1;
+    bool all_done = false;
+    for (;; k++)
     {
-        it++;
-        const bool check = (it % A.every) == 0;
-        // A: Ap and p.Ap
+        const bool decide = k > 1 && (k - 1) % A.every == 0;
+        const bool work = k <= A.cap_it;
+        // ---- P phase ----
+        if (decide && blockIdx.x == 0)
+        {
+            // the ratio-test flags of the next check start clear
+            int *next = A.rfail[((k - 1) / A.every + 1) & 1];
+            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
+                next[q] = 0;
+        }
+        const double *pold = A.pbuf[k & 1];
+        double *pnew = A.pbuf[(k - 1) & 1];
+        int cached = -1; // node of the block's last sums in this phase
+        double2 sums = make_double2(0.0, 0.0);
         for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
         {
             const AmrChunk C = A.chunks[c];
-            if (A.conv[C.node])
+            const int q = C.node;
+            // another block may mark q converged during this phase: one read per
+            // block keeps the branch uniform (the sums below synchronise the block)
+            if (__syncthreads_or(threadIdx.x == 0 && __ldcg(&A.conv[q])))
                 continue;
-            const AmrNode N = A.nodes[C.node];
+            const AmrNode N = A.nodes[q];
+            if (q != cached)
+            {
+                // rs_{k-1} and rs_{k-2}
+                sums = node_sums(A.rr[(k - 1) & 1], k == 1 ? nullptr : A.rr[k & 1],
+                                 A.node_chunk, q, sh2);
+                cached = q;
+            }
+            const double rs1 = sums.x;
+            if (decide)
+            {
+                const double H = 1.0 / (1 << N.lv);
+                const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+                const double tt = A.tol * rm;
+                const int rf = __ldcg(&A.rfail[((k - 1) / A.every) & 1][q]);
+                if (!rf && rs1 < N.nintr * tt * tt)
+                {
+                    if (threadIdx.x == 0)
+                        A.conv[q] = 1;
+                    continue;
+                }
+                for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+                {
+                    const long g = A.intr[e];
+                    A.pot_old[g] = A.pot[g];
+                }
+            }
+            if (!work)
+                continue;
+            const double beta = k == 1 ? 0.0 : rs1 / sums.y;
             const double H = 1.0 / (1 << N.lv);
             const double oh2 = 1.0 / (H * H);
             const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
@@ -1486,42 +1357,59 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
             for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
             {
                 const long g = A.intr[e];
-                const double *pp = A.p;
-                double a = -oh2 * (6.0 * pp[g] - pp[g + 1] - pp[g - 1] - pp[g + sy] - pp[g - sy] -
-                                   pp[g + sz] - pp[g - sz]);
-                A.Ap[g] = a;
-                acc += pp[g] * a;
+                const double *r = A.r;
+                const double p0 = r[g] + beta * pold[g];
+                const double a =
+                    -oh2 * (6.0 * p0 - (r[g + 1] + beta * pold[g + 1]) -
+                            (r[g - 1] + beta * pold[g - 1]) - (r[g + sy] + beta * pold[g + sy]) -
+                            (r[g - sy] + beta * pold[g - sy]) -
+                            (r[g + sz] + beta * pold[g + sz]) - (r[g - sz] + beta * pold[g - sz]));
+                pnew[g] = p0;
+                acc += p0 * a;
             }
             double t = block_sum_d(acc, sh);
             if (threadIdx.x == 0)
-                A.part1[c] = t;
+                A.pap[c] = t;
         }
         grid.sync();
-        // R1: alpha
-        for (long q = gwarp; q < A.nn; q += nwarps)
+        // ---- U phase ----
         {
-            if (A.conv[q])
-                continue;
-            double dot = warp_node_sum(A.part1, A.node_chunk, (int)q, lane);
-            if (lane == 0)
-                A.ns[3 * q + 1] = A.ns[3 * q] / dot;
+            int pending = 0;
+            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
+                pending |= !__ldcg(&A.conv[q]);
+            all_done = !__syncthreads_or(pending);
         }
-        grid.sync();
-        // B: pot, r, r.r, ratio test
+        if (all_done || !work)
+            break;
+        const bool check = k % A.every == 0;
+        int *rfail = A.rfail[(k / A.every) & 1];
+        cached = -1;
         for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
         {
             const AmrChunk C = A.chunks[c];
-            if (A.conv[C.node])
+            const int q = C.node;
+            if (__ldcg(&A.conv[q]))
                 continue;
-            const double alpha = A.ns[3 * C.node + 1];
+            const AmrNode N = A.nodes[q];
+            if (q != cached)
+            {
+                // rs_{k-1} and p.Ap
+                sums = node_sums(A.rr[(k - 1) & 1], A.pap, A.node_chunk, q, sh2);
+                cached = q;
+            }
+            const double alpha = sums.x / sums.y;
+            const double H = 1.0 / (1 << N.lv);
+            const double oh2 = 1.0 / (H * H);
+            const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
             double acc = 0.0;
             int fail = 0;
             for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
             {
                 const long g = A.intr[e];
-                double pv = A.pot[g] + alpha * A.p[g];
+                const double a = lap7(pnew, g, sy, sz, oh2);
+                double pv = A.pot[g] + alpha * pnew[g];
                 A.pot[g] = pv;
-                double rv = A.r[g] - alpha * A.Ap[g];
+                double rv = A.r[g] - alpha * a;
                 A.r[g] = rv;
                 acc += rv * rv;
                 if (check)
@@ -1532,67 +1420,19 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
                 }
             }
             double t = block_sum_d(acc, sh);
+            fail = __syncthreads_or(fail);
             if (threadIdx.x == 0)
-                A.part2[c] = t;
-            if (check && __syncthreads_or(fail) && threadIdx.x == 0)
-                atomicOr(&A.rfail[C.node], 1);
-        }
-        grid.sync();
-        // R2: rsnew, beta, convergence
-        for (long q = gwarp; q < A.nn; q += nwarps)
-        {
-            if (A.conv[q])
-                continue;
-            double rsnew = warp_node_sum(A.part2, A.node_chunk, (int)q, lane);
-            if (lane == 0)
             {
-                A.ns[3 * q + 2] = rsnew / A.ns[3 * q];
-                A.ns[3 * q] = rsnew;
-                A.refresh[q] = 0;
-                if (check)
-                {
-                    const AmrNode N = A.nodes[q];
-                    const double H = 1.0 / (1 << N.lv);
-                    const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
-                    const double tt = A.tol * rm;
-                    if (!A.rfail[q] && rsnew < N.nintr * tt * tt)
-                        A.conv[q] = 1;
-                    else
-                        A.refresh[q] = 1;
-                    A.rfail[q] = 0;
-                }
+                A.rr[k & 1][c] = t;
+                if (check && fail)
+                    atomicOr(&rfail[q], 1);
             }
-        }
-        grid.sync();
-        // C: p update, pot_old refresh
-        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
-        {
-            const AmrChunk C = A.chunks[c];
-            if (A.conv[C.node])
-                continue;
-            const double beta = A.ns[3 * C.node + 2];
-            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-            {
-                const long g = A.intr[e];
-                A.p[g] = A.r[g] + beta * A.p[g];
-            }
-        }
-        if (check)
-        {
-            for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < A.grid_total;
-                 g += (long)gridDim.x * blockDim.x)
-                if (A.refresh[find_node(A.nodes, A.nn, g, 0)])
-                    A.pot_old[g] = A.pot[g];
-            int pending = 0;
-            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
-                pending |= !A.conv[q];
-            all_done = !__syncthreads_or(pending);
         }
         grid.sync();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
-        A.status[0] = (int)it;
+        A.status[0] = (int)(k - 1);
         A.status[1] = all_done ? 1 : 0;
     }
 }
@@ -1615,9 +1455,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     L.nchunks = (int)L.hchunks.size();
     if (L.nchunks == 0)
         return QZ_SUCCESS;
-    // nint: node_chunk (2 nn) | conv (nn) | rfail (nn) | refresh (nn) | status (2)
-    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(2L * L.nchunks) ||
-        !L.nscal.ensure(3L * nn) || !L.nint.ensure(5L * nn + 2) || !L.r.ensure(L.grid_total) ||
+    // nint: node_chunk (2 nn) | conv (nn) | rfail[0] (nn) | rfail[1] (nn) | status (2)
+    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(3L * L.nchunks) ||
+        !L.nint.ensure(5L * nn + 2) || !L.r.ensure(L.grid_total) ||
         !L.p.ensure(L.grid_total) || !L.Ap.ensure(L.grid_total))
     {
         set_error("cg buffers");
@@ -1628,7 +1468,10 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
         !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), 2L * nn * sizeof(int),
                                     cudaMemcpyHostToDevice, s->stream), "cg ints"))
         return QZ_FAILURE;
+    // r and both p buffers are zero off the interior points
+    cudaMemsetAsync(L.r.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.p.p, 0, L.grid_total * sizeof(double), s->stream);
+    cudaMemsetAsync(L.Ap.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.nint.p + 2 * nn, 0, (3L * nn + 2) * sizeof(int), s->stream);
     // iteration cap of the reference per node: min(node grid size, max_iter);
     // nodes iterate in lockstep, so the level runs to the largest cap
@@ -1647,16 +1490,15 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.pot = L.pot;
     A.pot_old = L.pot_old;
     A.r = L.r.p;
-    A.p = L.p.p;
-    A.Ap = L.Ap.p;
-    A.part1 = L.chunk_part.p;
-    A.part2 = L.chunk_part.p + L.nchunks;
-    A.ns = L.nscal.p;
+    A.pbuf[0] = L.p.p;
+    A.pbuf[1] = L.Ap.p;
+    A.pap = L.chunk_part.p;
+    A.rr[0] = L.chunk_part.p + L.nchunks;
+    A.rr[1] = L.chunk_part.p + 2L * L.nchunks;
     A.conv = L.nint.p + 2 * nn;
-    A.rfail = L.nint.p + 3 * nn;
-    A.refresh = L.nint.p + 4 * nn;
+    A.rfail[0] = L.nint.p + 3 * nn;
+    A.rfail[1] = L.nint.p + 4 * nn;
     A.status = L.nint.p + 5 * nn;
-    A.grid_total = L.grid_total;
     A.tol = c.tol;
     A.tol2 = c.tol2;
     A.G = c.G;
@@ -1667,6 +1509,13 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     if (!check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent,
                                                                   CG_THREADS, 0), "occupancy"))
         return QZ_FAILURE;
+    // blocks per SM: more hide memory latency, fewer make the grid barriers cheaper
+    static const int cg_bps = [] {
+        const char *e = getenv("QZ_CG_BLOCKS_PER_SM");
+        return e ? atoi(e) : 0;
+    }();
+    if (cg_bps > 0)
+        per_sm = std::min(per_sm, cg_bps);
     int blocks = std::max(1, std::min(per_sm * sms, L.nchunks));
     void *args[] = {&A};
     cudaEvent_t eb = nullptr, ee = nullptr;
@@ -1692,8 +1541,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     s->stats.cg_iterations += st[0];
     if (s->prof)
     {
-        // bytes of the launch: per iteration Ap 16, update 48, p 24 B per interior point
-        s->prof_pending.back().bytes = 88.0 * L.intr_total * st[0];
+        // bytes of the launch per iteration and interior point: P phase reads r and
+        // p_{k-2} and writes p_{k-1} (24 B), U phase reads p, pot, r and writes pot, r (40 B)
+        s->prof_pending.back().bytes = 64.0 * L.intr_total * st[0];
     }
     if (!st[1])
     {

@@ -140,12 +140,11 @@ struct AmrLevel {
     DBuf<int> intr, bdry, simb, intr_node, bdry_node, simb_node; // level grid-pool indices
     double *pot = nullptr, *pot_old = nullptr, *d = nullptr, *ax = nullptr, *ay = nullptr,
            *az = nullptr; // head aliases on level 0
+    // conjugate gradient: residual r and the two p buffers (p and Ap, by iteration parity)
     DBuf<double> gpot, gpot_old, gd, gax, gay, gaz, r, p, Ap;
-    // conjugate gradient per node: rsold, rsnew, alpha, beta, dot, mass
-    DBuf<double> nscal;
-    DBuf<int> nint; // per node: conv, ratio_fail, chunk_begin, chunk_end, active, nptcl
+    DBuf<int> nint; // node chunk ranges, converged flags, ratio-test flags, status
     DBuf<AmrChunk> chunks;
-    DBuf<double> chunk_part;
+    DBuf<double> chunk_part; // per chunk: p.Ap partial and two r.r partials
     int nchunks = 0;
     std::vector<AmrChunk> hchunks;
 };
