@@ -34,7 +34,9 @@
 //              node whose cell holding it is not refined
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <cooperative_groups.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -46,8 +48,8 @@ namespace qz {
 
 #define QZ_PI_D 3.14159265358979323846
 constexpr int AMR_MAX_LEVELS = 16;
-constexpr int CG_CHUNK = 512;
-constexpr int CG_THREADS = 256;
+// largest block of the conjugate gradient kernel (two blocks per SM at 64 registers)
+constexpr int CG_MAX_THREADS = 512;
 
 // ---- small device helpers --------------------------------------------------------------
 // Index of the last node whose offset (0: grid_off, 1: cls_off, 2: box_off) is <= v.
@@ -479,7 +481,8 @@ static bool ensure_small(qz_sim *s, long need)
         cudaFreeHost(s->h_small);
     s->h_small = nullptr;
     s->h_small_cap = 0;
-    long nc = std::max(need, 4096L);
+    // freeing pinned memory waits for the device: grow rarely
+    long nc = std::max(2 * need, 1L << 20);
     if (!check_cuda(cudaMallocHost((void **)&s->h_small, nc * sizeof(int)), "pinned small"))
         return false;
     s->h_small_cap = nc;
@@ -508,7 +511,7 @@ static bool read_at(qz_sim *s, const int *dsrc, const std::vector<int> &idx, int
     const int m = (int)idx.size();
     if (m == 0)
         return true;
-    if (!s->gather_idx.ensure(2L * m) || !ensure_small(s, m))
+    if (!s->gather_idx.ensure(s->mem, 2L * m) || !ensure_small(s, m))
     {
         set_error("gather buffer");
         return false;
@@ -525,7 +528,7 @@ static bool read_at(qz_sim *s, const int *dsrc, const std::vector<int> &idx, int
 
 static bool upload_nodes(qz_sim *s, AmrLevel &L)
 {
-    if (!L.nodes.ensure(std::max(L.nnodes, 1)))
+    if (!L.nodes.ensure(s->mem, std::max(L.nnodes, 1)))
     {
         set_error("amr nodes");
         return false;
@@ -536,36 +539,36 @@ static bool upload_nodes(qz_sim *s, AmrLevel &L)
                       "amr nodes h2d");
 }
 
-static void free_level(AmrLevel &L)
+static void free_level(const MemCtx &m, AmrLevel &L)
 {
     DBuf<int> *ib[] = {&L.box, &L.cnt, &L.pos_of_box, &L.cell_seg, &L.cell_box, &L.cell_xyz,
                        &L.cell_node, &L.intr, &L.bdry, &L.simb, &L.intr_node, &L.bdry_node,
                        &L.simb_node, &L.nint};
     for (auto *b : ib)
-        b->release();
+        b->release(m);
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
                           &L.chunk_part};
     for (auto *b : db)
-        b->release();
-    L.nodes.release();
-    L.chunks.release();
+        b->release(m);
+    L.nodes.release(m);
+    L.chunks.release(m);
     L = AmrLevel();
 }
 
 void amr_free(qz_sim *s)
 {
     for (auto &L : s->amr)
-        free_level(L);
+        free_level(s->mem, L);
     s->amr.clear();
     for (auto &b : s->node_of)
-        b.release();
+        b.release(s->mem);
     s->node_of.clear();
-    s->amr_tmp.release();
-    s->amr_tmp2.release();
-    s->zone_box.release();
-    s->zone_cells.release();
-    s->gather_idx.release();
-    s->seg_mass.release();
+    s->amr_tmp.release(s->mem);
+    s->amr_tmp2.release(s->mem);
+    s->zone_box.release(s->mem);
+    s->zone_cells.release(s->mem);
+    s->gather_idx.release(s->mem);
+    s->seg_mass.release(s->mem);
     if (s->h_small)
         cudaFreeHost(s->h_small);
     s->h_small = nullptr;
@@ -584,7 +587,7 @@ int amr_init(qz_sim *s)
     s->amr.assign(levels, AmrLevel());
     s->node_of.assign(levels, DBuf<int>());
     for (int l = 0; l < levels; l++)
-        if (!s->node_of[l].ensure(s->cap))
+        if (!s->node_of[l].ensure(s->mem, s->cap))
         {
             set_error("node_of");
             return QZ_FAILURE;
@@ -615,9 +618,9 @@ int amr_init(qz_sim *s)
     H.ax = s->gax;
     H.ay = s->gay;
     H.az = s->gaz;
-    if (!upload_nodes(s, H) || !H.box.ensure(H.box_total) || !H.cnt.ensure(H.box_total) ||
-        !H.pos_of_box.ensure(H.box_total) || !H.cell_box.ensure(H.cell_total) ||
-        !H.cell_xyz.ensure(3L * H.cell_total) || !H.cell_node.ensure(H.cell_total))
+    if (!upload_nodes(s, H) || !H.box.ensure(s->mem, H.box_total) || !H.cnt.ensure(s->mem, H.box_total) ||
+        !H.pos_of_box.ensure(s->mem, H.box_total) || !H.cell_box.ensure(s->mem, H.cell_total) ||
+        !H.cell_xyz.ensure(s->mem, 3L * H.cell_total) || !H.cell_node.ensure(s->mem, H.cell_total))
     {
         set_error("head tree buffers");
         return QZ_FAILURE;
@@ -697,7 +700,7 @@ int amr_build(qz_sim *s)
         launch(s, QZ_PROF_TREE, 12.0 * nc, k_flag, dim3(blocks_for(nc, 256)), dim3(256), nc,
                s->cfg.ref_ptcl, P.cell_box.p, P.cell_node.p, P.nodes.p, P.cnt.p, P.box.p);
         // union-find over the refine cells: parent | is_root | zone rank | flagged | slot
-        if (!s->amr_tmp.ensure(5L * nc + 8))
+        if (!s->amr_tmp.ensure(s->mem, 5L * nc + 8))
         {
             set_error("amr scratch");
             return QZ_FAILURE;
@@ -725,7 +728,7 @@ int amr_build(qz_sim *s)
             upload_nodes(s, P);
             break;
         }
-        if (!s->zone_box.ensure(6L * nz) || !s->zone_cells.ensure(nz) || !ensure_sort(s, nzc))
+        if (!s->zone_box.ensure(s->mem, 6L * nz) || !s->zone_cells.ensure(s->mem, nz) || !ensure_sort(s, nzc))
         {
             set_error("zone buffers");
             return QZ_FAILURE;
@@ -800,10 +803,10 @@ int amr_build(qz_sim *s)
         C.grid_total = grid_total;
         C.cell_total = cell_total;
         C.cls_total = cls_total;
-        if (!C.box.ensure(box_total) || !C.cnt.ensure(box_total) ||
-            !C.pos_of_box.ensure(box_total) || !C.cell_box.ensure(cell_total) ||
-            !C.cell_xyz.ensure(3L * cell_total) || !C.cell_node.ensure(cell_total) ||
-            !s->amr_tmp2.ensure(std::max((long)nz, 6L * cls_total + 8)))
+        if (!C.box.ensure(s->mem, box_total) || !C.cnt.ensure(s->mem, box_total) ||
+            !C.pos_of_box.ensure(s->mem, box_total) || !C.cell_box.ensure(s->mem, cell_total) ||
+            !C.cell_xyz.ensure(s->mem, 3L * cell_total) || !C.cell_node.ensure(s->mem, cell_total) ||
+            !s->amr_tmp2.ensure(s->mem, std::max((long)nz, 6L * cls_total + 8)))
         {
             set_error("child level buffers");
             return QZ_FAILURE;
@@ -865,9 +868,9 @@ int amr_build(qz_sim *s)
             N.nsimb = start(2, q + 1) - start(2, q);
             N.zone_base = N.nzones = 0;
         }
-        if (!C.intr.ensure(C.intr_total) || !C.intr_node.ensure(C.intr_total) ||
-            !C.bdry.ensure(C.bdry_total) || !C.bdry_node.ensure(C.bdry_total) ||
-            !C.simb.ensure(C.simb_total) || !C.simb_node.ensure(C.simb_total))
+        if (!C.intr.ensure(s->mem, C.intr_total) || !C.intr_node.ensure(s->mem, C.intr_total) ||
+            !C.bdry.ensure(s->mem, C.bdry_total) || !C.bdry_node.ensure(s->mem, C.bdry_total) ||
+            !C.simb.ensure(s->mem, C.simb_total) || !C.simb_node.ensure(s->mem, C.simb_total))
         {
             set_error("grid lists");
             return QZ_FAILURE;
@@ -1060,8 +1063,8 @@ int amr_deposit(qz_sim *s)
         AmrLevel &L = s->amr[l];
         if (L.nnodes == 0)
             break;
-        if (!L.gd.ensure(L.grid_total) || !L.cell_seg.ensure(L.box_total) ||
-            !s->amr_tmp.ensure(2 * n + 2) || !ensure_sort(s, n))
+        if (!L.gd.ensure(s->mem, L.grid_total) || !L.cell_seg.ensure(s->mem, L.box_total) ||
+            !s->amr_tmp.ensure(s->mem, 2 * n + 2) || !ensure_sort(s, n))
         {
             set_error("level deposit buffers");
             return QZ_FAILURE;
@@ -1085,7 +1088,7 @@ int amr_deposit(qz_sim *s)
         int *perm;
         if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm))
             return QZ_FAILURE;
-        if (!s->seg_mass.ensure(m + 1))
+        if (!s->seg_mass.ensure(s->mem, m + 1))
         {
             set_error("segment mass");
             return QZ_FAILURE;
@@ -1181,9 +1184,9 @@ __global__ void k_copy_d(long n, const double *__restrict__ a, double *__restric
         b[i] = a[i];
 }
 
-// The whole conjugate-gradient solve of one level in one cooperative launch
-// (conjugate_gradient.c:322-463 for every node of the level at once), two
-// phases and two grid-wide barriers per iteration k:
+// The conjugate-gradient solves of all nodes of one level in one launch
+// (conjugate_gradient.c:322-463 for every node at once).  Iteration k of a node
+// has two phases:
 //   P  (decision for the check at k-1, then) p_{k-1} = r_{k-1} + beta p_{k-2}
 //      with beta = rs_{k-1} / rs_{k-2}, computed by every stencil on the fly for
 //      its seven points (the owner stores it), Ap = -(1/H^2) L p_{k-1} and the
@@ -1195,296 +1198,481 @@ __global__ void k_copy_d(long n, const double *__restrict__ a, double *__restric
 // The residual test of a check iteration (poisson_error.c:236-254) is taken at
 // the start of the next P phase: converged nodes stop there (the reference
 // returns before updating p); the others copy pot to pot_old on their interior
-// points, the only points the ratio test reads.  Node scalars are not stored:
-// each block adds the node's chunk partials itself in a fixed order, so every
-// block obtains the same value.  p and the r.r
-// partials are double-buffered by iteration parity; r and both p buffers are
-// zero off the interior points.  Every block runs the same loop and reaches
-// every barrier; it ends when every node converged or after the iteration cap.
+// points, the only points the ratio test reads.  A node stops without
+// converging after min(node grid points, max_iter) iterations, as there.
+//
+// Nodes are independent problems and there is no grid-wide barrier.  A chunk's
+// partial is published with a release store into a slot that holds an all-ones
+// word (a NaN payload that arithmetic never produces) until then; a block that
+// needs the node's sum polls the node's slots with acquire loads until none
+// holds the marker, which also makes the node's data of the previous phase
+// visible.  Every block adds the same partials in the same fixed order, so all
+// blocks of a node obtain the same sums and take the same decisions.  A slot is
+// reset to the marker by its owner once the owner has seen every block of the
+// node publish a later partial (so all of them have read it), before the owner
+// publishes its own next partial.  p and the partials are double-buffered by
+// iteration parity; r and both p buffers are zero off the interior points.
+// Block b owns chunks b, b + gridDim, ... (its slots); their node constants and
+// (up to ncache slots) grid indices sit in shared memory for the whole solve.
+// All blocks are resident (cooperative launch); every wait gives up after a
+// bounded number of polls and reports it in status[1].
 struct CgArgs {
     const AmrChunk *chunks;
     int nchunks;
+    int chunk;  // interior points per chunk
+    int ncache; // slots per block whose grid indices are kept in shared memory
     const int *intr;
     const AmrNode *nodes;
-    int nn;
     const int *node_chunk; // per node: first chunk, end chunk
     const double *d;
     double *pot, *pot_old, *r;
-    double *pbuf[2];  // p_j in pbuf[j & 1]
-    double *pap;      // per chunk: partial p.Ap
-    double *rr[2];    // per chunk: partial r_j.r_j in rr[j & 1]
-    int *conv;        // per node: converged (0/1)
-    int *rfail[2];    // per node: ratio test failed at check j, in rfail[j & 1]
+    double *pbuf[2]; // p_j in pbuf[j & 1]
+    double *pap[2];  // per chunk: partial p.Ap of iteration k in pap[k & 1]
+    double *rr[2];   // per chunk: partial r_j.r_j in rr[j & 1]
+    int *rfail[2];   // per node: ratio test failed at check j, in rfail[j & 1]
+    int *status;     // [0] most iterations of a node, [1] a wait gave up, [2] unconverged nodes
+    int *iters;      // per node: iterations run
     double tol, tol2, G;
     int every;
-    long cap_it;
-    int *status; // [0] iterations run, [1] all converged
+    int max_iter;
 };
 
-// Sums of node q's chunk partials in two arrays (b may be null), computed by the
-// whole block and returned to every thread: thread t adds chunks t, t + blockDim,
-// ... in order, then a fixed xor-shuffle tree per warp and the warp totals in
-// warp order.  Every block of the launch has the same size, so every block
-// obtains the same two values.
-__device__ __forceinline__ double2 node_sums(const double *a, const double *b,
-                                             const int *node_chunk, int q, double2 *sh2)
+constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
+constexpr int CG_POLL_LIMIT = 1 << 21;
+
+__device__ __forceinline__ double cg_ld_acquire(const double *p)
 {
-    double sa = 0.0, sb = 0.0;
-    for (int c = node_chunk[2 * q] + threadIdx.x; c < node_chunk[2 * q + 1]; c += blockDim.x)
-    {
-        sa += __ldcg(&a[c]);
-        if (b)
-            sb += __ldcg(&b[c]);
-    }
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ void cg_st_release(double *p, double v)
+{
+    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p),
+                 "l"((unsigned long long)__double_as_longlong(v))
+                 : "memory");
+}
+
+// Seven stencil operands of point g in the order of the Laplacian:
+// g, g+1, g-1, g+sy, g-sy, g+sz, g-sz.
+__device__ __forceinline__ void cg_load7(const double *v, int g, int sy, int sz, double o[7])
+{
+    o[0] = v[g];
+    o[1] = v[g + 1];
+    o[2] = v[g - 1];
+    o[3] = v[g + sy];
+    o[4] = v[g - sy];
+    o[5] = v[g + sz];
+    o[6] = v[g - sz];
+}
+
+// A block's view of one of its chunks (shared memory).
+struct CgSlot {
+    double oh2;     // 1 / H^2
+    double thr;     // residual threshold nintr * (tol * rm)^2 (poisson_error.c:236-254)
+    double rs_prev; // rs_{k-2} of the node
+    double rs_cur;  // rs_{k-1} of the node
+    int c, q, cb, ce; // chunk, node, node's chunk range
+    int begin, n;     // interior list range of the chunk
+    int sy, sz;       // grid strides of the node
+    int cap;          // iteration cap of the node
+    int done;         // node finished
+};
+
+// Block-wide sums of (a, b) and bitwise OR of f, returned to every thread.  Warp
+// order and shuffle order are fixed, so every block of the launch (all of the
+// same size) obtains the same values from the same inputs.
+__device__ __forceinline__ double2 cg_reduce(double a, double b, int &f, double2 *sh2, int *shf)
+{
     for (int o = 16; o > 0; o >>= 1)
     {
-        sa += __shfl_xor_sync(0xffffffffu, sa, o);
-        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
     }
+    f = (int)__reduce_or_sync(0xffffffffu, (unsigned)f);
     if ((threadIdx.x & 31) == 0)
-        sh2[threadIdx.x >> 5] = make_double2(sa, sb);
+    {
+        sh2[threadIdx.x >> 5] = make_double2(a, b);
+        shf[threadIdx.x >> 5] = f;
+    }
     __syncthreads();
     double2 t = make_double2(0.0, 0.0);
+    int any = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++)
     {
         t.x += sh2[w].x;
         t.y += sh2[w].y;
+        any |= shf[w];
     }
-    __syncthreads(); // sh2 is rewritten by the next call
+    __syncthreads(); // the slots are rewritten by the next call
+    f = any;
     return t;
 }
 
-__device__ __forceinline__ double lap7(const double *v, long g, long sy, long sz, double oh2)
+// Sum of the published partials of chunks [cb, ce), waiting for each; thread t
+// takes chunks cb + t, cb + t + blockDim, ...  *gave_up is set in every thread
+// if a wait hit the poll limit.
+__device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce, int *gave_up,
+                                              double2 *sh2, int *shf)
 {
-    return -oh2 * (6.0 * v[g] - v[g + 1] - v[g - 1] - v[g + sy] - v[g - sy] - v[g + sz] -
-                   v[g - sz]);
+    double s = 0.0;
+    int bad = 0;
+    for (int c = cb + (int)threadIdx.x; c < ce; c += (int)blockDim.x)
+    {
+        double v = cg_ld_acquire(&part[c]);
+        int polls = 0;
+        while (__double_as_longlong(v) == CG_EMPTY)
+        {
+            if (++polls > CG_POLL_LIMIT)
+            {
+                bad = 1;
+                v = 0.0;
+                break;
+            }
+            v = cg_ld_acquire(&part[c]);
+        }
+        s += v;
+    }
+    int f = bad;
+    const double2 t = cg_reduce(s, 0.0, f, sh2, shf);
+    *gave_up = f;
+    return t.x;
 }
 
-__global__ void __launch_bounds__(CG_THREADS) k_cg_persistent(CgArgs A)
+__global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
 {
-    cgrp::grid_group grid = cgrp::this_grid();
     __shared__ double sh[32];
-    __shared__ double2 sh2[CG_THREADS / 32];
-    // nodes without interior points have nothing to solve
-    if (blockIdx.x == 0)
-        for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
-            if (A.node_chunk[2 * q] == A.node_chunk[2 * q + 1])
-                A.conv[q] = 1;
-    // r_0 = d - (-(1/H^2) L pot), partial rs_0
-    for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+    __shared__ double2 sh2[CG_MAX_THREADS / 32];
+    __shared__ int shf[CG_MAX_THREADS / 32];
+    const int NT = blockDim.x;
+    extern __shared__ __align__(16) unsigned char cg_dyn[];
+    const double empty = __longlong_as_double(CG_EMPTY);
+    // the host launches at most nchunks blocks: every block has at least one slot
+    const int nslot = (A.nchunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    CgSlot *slot = reinterpret_cast<CgSlot *>(cg_dyn);
+    int *gidx = reinterpret_cast<int *>(slot + nslot);
+    for (int s = threadIdx.x; s < nslot; s += NT)
     {
+        const int c = blockIdx.x + s * gridDim.x;
         const AmrChunk C = A.chunks[c];
         const AmrNode N = A.nodes[C.node];
+        CgSlot x;
+        x.c = c;
+        x.q = C.node;
+        x.cb = A.node_chunk[2 * C.node];
+        x.ce = A.node_chunk[2 * C.node + 1];
+        x.begin = C.begin;
+        x.n = C.end - C.begin;
+        x.sy = N.rd[0] + 1;
+        x.sz = x.sy * (N.rd[1] + 1);
         const double H = 1.0 / (1 << N.lv);
-        const double oh2 = 1.0 / (H * H);
-        const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+        x.oh2 = 1.0 / (H * H);
+        const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+        const double tt = A.tol * rm;
+        x.thr = N.nintr * tt * tt;
+        const long size = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
+        x.cap = (int)(size < A.max_iter ? size : A.max_iter);
+        x.rs_prev = x.rs_cur = 0.0;
+        x.done = 0;
+        slot[s] = x;
+    }
+    const int ncache = min(nslot, A.ncache);
+    for (int s = 0; s < ncache; s++)
+    {
+        const AmrChunk C = A.chunks[blockIdx.x + s * gridDim.x];
+        for (int e = threadIdx.x; e < C.end - C.begin; e += NT)
+            gidx[s * A.chunk + e] = A.intr[C.begin + e];
+    }
+    __syncthreads();
+    // grid index of entry e of slot s
+    auto gi = [&](int s, int e) -> int {
+        return s < ncache ? gidx[s * A.chunk + e] : A.intr[slot[s].begin + e];
+    };
+    // r_0 = d - (-(1/H^2) L pot), partial rs_0
+    for (int s = 0; s < nslot; s++)
+    {
+        const CgSlot &x = slot[s];
         double acc = 0.0;
-        for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+        for (int e = threadIdx.x; e < x.n; e += NT)
         {
-            const long g = A.intr[e];
+            const int g = gi(s, e);
             const double *pt = A.pot;
-            double rv = A.d[g] + oh2 * (6.0 * pt[g] - pt[g + 1] - pt[g - 1] - pt[g + sy] -
-                                        pt[g - sy] - pt[g + sz] - pt[g - sz]);
+            const double rv = A.d[g] + x.oh2 * (6.0 * pt[g] - pt[g + 1] - pt[g - 1] - pt[g + x.sy] -
+                                                pt[g - x.sy] - pt[g + x.sz] - pt[g - x.sz]);
             A.r[g] = rv;
             acc += rv * rv;
         }
-        double t = block_sum_d(acc, sh);
+        const double t = block_sum_d(acc, sh);
         if (threadIdx.x == 0)
-            A.rr[0][c] = t;
+            cg_st_release(&A.rr[0][x.c], t);
     }
-    grid.sync();
-    const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
-    long k = 1;
-    bool all_done = false;
-    for (;; k++)
+    int gave_up = 0;
+    for (long k = 1;; k++)
     {
-        const bool decide = k > 1 && (k - 1) % A.every == 0;
-        const bool work = k <= A.cap_it;
         // ---- P phase ----
-        if (decide && blockIdx.x == 0)
-        {
-            // the ratio-test flags of the next check start clear
-            int *next = A.rfail[((k - 1) / A.every + 1) & 1];
-            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
-                next[q] = 0;
-        }
+        const bool decide = k > 1 && (k - 1) % A.every == 0;
         const double *pold = A.pbuf[k & 1];
         double *pnew = A.pbuf[(k - 1) & 1];
-        int cached = -1; // node of the block's last sums in this phase
-        double2 sums = make_double2(0.0, 0.0);
-        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
+        int live = 0, cq = -1;
+        double rs1 = 0.0;
+        for (int s = 0; s < nslot && !gave_up; s++)
         {
-            const AmrChunk C = A.chunks[c];
-            const int q = C.node;
-            // another block may mark q converged during this phase: one read per
-            // block keeps the branch uniform (the sums below synchronise the block)
-            if (__syncthreads_or(threadIdx.x == 0 && __ldcg(&A.conv[q])))
+            CgSlot &x = slot[s];
+            if (x.done)
                 continue;
-            const AmrNode N = A.nodes[q];
-            if (q != cached)
+            if (x.q != cq)
             {
-                // rs_{k-1} and rs_{k-2}
-                sums = node_sums(A.rr[(k - 1) & 1], k == 1 ? nullptr : A.rr[k & 1],
-                                 A.node_chunk, q, sh2);
-                cached = q;
+                // rs_{k-1}; also makes the node's r of iteration k-1 visible
+                rs1 = cg_node_sum(A.rr[(k - 1) & 1], x.cb, x.ce, &gave_up, sh2, shf);
+                cq = x.q;
+                if (gave_up)
+                    break;
             }
-            const double rs1 = sums.x;
+            // every block of the node has read the p.Ap partials of iteration k-1
+            if (threadIdx.x == 0 && k > 1)
+                A.pap[(k - 1) & 1][x.c] = empty;
             if (decide)
             {
-                const double H = 1.0 / (1 << N.lv);
-                const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
-                const double tt = A.tol * rm;
-                const int rf = __ldcg(&A.rfail[((k - 1) / A.every) & 1][q]);
-                if (!rf && rs1 < N.nintr * tt * tt)
+                const int rf = __syncthreads_or(
+                    threadIdx.x == 0 && __ldcg(&A.rfail[((k - 1) / A.every) & 1][x.q]));
+                if (!rf && rs1 < x.thr)
                 {
                     if (threadIdx.x == 0)
-                        A.conv[q] = 1;
+                    {
+                        x.done = 1;
+                        if (x.c == x.cb) // once per node
+                        {
+                            A.iters[x.q] = (int)(k - 1);
+                            atomicMax(&A.status[0], (int)(k - 1));
+                            atomicSub(&A.status[2], 1);
+                        }
+                    }
                     continue;
                 }
-                for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+                for (int e = threadIdx.x; e < x.n; e += NT)
                 {
-                    const long g = A.intr[e];
+                    const int g = gi(s, e);
                     A.pot_old[g] = A.pot[g];
                 }
+                // the ratio-test flags of the next check start clear
+                if (threadIdx.x == 0 && x.c == x.cb)
+                    A.rfail[((k - 1) / A.every + 1) & 1][x.q] = 0;
             }
-            if (!work)
-                continue;
-            const double beta = k == 1 ? 0.0 : rs1 / sums.y;
-            const double H = 1.0 / (1 << N.lv);
-            const double oh2 = 1.0 / (H * H);
-            const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
-            double acc = 0.0;
-            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
+            if (k > x.cap)
             {
-                const long g = A.intr[e];
-                const double *r = A.r;
-                const double p0 = r[g] + beta * pold[g];
-                const double a =
-                    -oh2 * (6.0 * p0 - (r[g + 1] + beta * pold[g + 1]) -
-                            (r[g - 1] + beta * pold[g - 1]) - (r[g + sy] + beta * pold[g + sy]) -
-                            (r[g - sy] + beta * pold[g - sy]) -
-                            (r[g + sz] + beta * pold[g + sz]) - (r[g - sz] + beta * pold[g - sz]));
-                pnew[g] = p0;
-                acc += p0 * a;
-            }
-            double t = block_sum_d(acc, sh);
-            if (threadIdx.x == 0)
-                A.pap[c] = t;
-        }
-        grid.sync();
-        // ---- U phase ----
-        {
-            int pending = 0;
-            for (int q = threadIdx.x; q < A.nn; q += blockDim.x)
-                pending |= !__ldcg(&A.conv[q]);
-            all_done = !__syncthreads_or(pending);
-        }
-        if (all_done || !work)
-            break;
-        const bool check = k % A.every == 0;
-        int *rfail = A.rfail[(k / A.every) & 1];
-        cached = -1;
-        for (int c = blockIdx.x; c < A.nchunks; c += gridDim.x)
-        {
-            const AmrChunk C = A.chunks[c];
-            const int q = C.node;
-            if (__ldcg(&A.conv[q]))
-                continue;
-            const AmrNode N = A.nodes[q];
-            if (q != cached)
-            {
-                // rs_{k-1} and p.Ap
-                sums = node_sums(A.rr[(k - 1) & 1], A.pap, A.node_chunk, q, sh2);
-                cached = q;
-            }
-            const double alpha = sums.x / sums.y;
-            const double H = 1.0 / (1 << N.lv);
-            const double oh2 = 1.0 / (H * H);
-            const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
-            double acc = 0.0;
-            int fail = 0;
-            for (int e = C.begin + threadIdx.x; e < C.end; e += blockDim.x)
-            {
-                const long g = A.intr[e];
-                const double a = lap7(pnew, g, sy, sz, oh2);
-                double pv = A.pot[g] + alpha * pnew[g];
-                A.pot[g] = pv;
-                double rv = A.r[g] - alpha * a;
-                A.r[g] = rv;
-                acc += rv * rv;
-                if (check)
+                // the node used its iterations without converging
+                if (threadIdx.x == 0)
                 {
-                    double ratio = pv / A.pot_old[g];
-                    if ((tm > ratio) || (tp < ratio))
-                        fail = 1;
+                    x.done = 1;
+                    if (x.c == x.cb)
+                    {
+                        A.iters[x.q] = (int)(k - 1);
+                        atomicMax(&A.status[0], (int)(k - 1));
+                    }
+                }
+                continue;
+            }
+            live = 1;
+            const double beta = k == 1 ? 0.0 : rs1 / x.rs_prev;
+            const double oh2 = x.oh2;
+            const int sy = x.sy, sz = x.sz;
+            double acc = 0.0;
+            // a thread's two points of a chunk together, so their loads overlap
+            for (int e0 = threadIdx.x; e0 < x.n; e0 += 2 * NT)
+            {
+                const int e1 = e0 + NT;
+                const bool has1 = e1 < x.n;
+                const int ga = gi(s, e0), gb = has1 ? gi(s, e1) : ga;
+                const double *r = A.r;
+                double ra[7], pa[7], rb[7], pb[7];
+                cg_load7(r, ga, sy, sz, ra);
+                cg_load7(pold, ga, sy, sz, pa);
+                cg_load7(r, gb, sy, sz, rb);
+                cg_load7(pold, gb, sy, sz, pb);
+                const double p0a = ra[0] + beta * pa[0];
+                const double aa = -oh2 * (6.0 * p0a - (ra[1] + beta * pa[1]) - (ra[2] + beta * pa[2]) -
+                                          (ra[3] + beta * pa[3]) - (ra[4] + beta * pa[4]) -
+                                          (ra[5] + beta * pa[5]) - (ra[6] + beta * pa[6]));
+                pnew[ga] = p0a;
+                acc += p0a * aa;
+                if (has1)
+                {
+                    const double p0b = rb[0] + beta * pb[0];
+                    const double ab =
+                        -oh2 * (6.0 * p0b - (rb[1] + beta * pb[1]) - (rb[2] + beta * pb[2]) -
+                                (rb[3] + beta * pb[3]) - (rb[4] + beta * pb[4]) -
+                                (rb[5] + beta * pb[5]) - (rb[6] + beta * pb[6]));
+                    pnew[gb] = p0b;
+                    acc += p0b * ab;
                 }
             }
-            double t = block_sum_d(acc, sh);
+            const double t = block_sum_d(acc, sh);
+            if (threadIdx.x == 0)
+            {
+                x.rs_prev = rs1;
+                x.rs_cur = rs1;
+                cg_st_release(&A.pap[k & 1][x.c], t);
+            }
+        }
+        __syncthreads(); // slot flags written by thread 0 above
+        if (gave_up || !live)
+            break;
+        // ---- U phase ----
+        const bool check = k % A.every == 0;
+        const double *pn = pnew;
+        const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
+        cq = -1;
+        double pap = 0.0;
+        for (int s = 0; s < nslot; s++)
+        {
+            CgSlot &x = slot[s];
+            if (x.done)
+                continue;
+            if (x.q != cq)
+            {
+                // p.Ap; also makes the node's p of iteration k visible
+                pap = cg_node_sum(A.pap[k & 1], x.cb, x.ce, &gave_up, sh2, shf);
+                cq = x.q;
+                if (gave_up)
+                    break;
+            }
+            // every block of the node has read the r.r partials of iteration k-1
+            if (threadIdx.x == 0)
+                A.rr[(k - 1) & 1][x.c] = empty;
+            const double alpha = x.rs_cur / pap;
+            const double oh2 = x.oh2;
+            const int sy = x.sy, sz = x.sz;
+            double acc = 0.0;
+            int fail = 0;
+            // a thread's two points of a chunk together, so their loads overlap
+            for (int e0 = threadIdx.x; e0 < x.n; e0 += 2 * NT)
+            {
+                const int e1 = e0 + NT;
+                const bool has1 = e1 < x.n;
+                const int ga = gi(s, e0), gb = has1 ? gi(s, e1) : ga;
+                double va[7], vb[7];
+                cg_load7(pn, ga, sy, sz, va);
+                cg_load7(pn, gb, sy, sz, vb);
+                const double pota = A.pot[ga], potb = A.pot[gb];
+                const double rva = A.r[ga], rvb = A.r[gb];
+                const double olda = check ? A.pot_old[ga] : 1.0;
+                const double oldb = check ? A.pot_old[gb] : 1.0;
+                {
+                    const double a =
+                        -oh2 * (6.0 * va[0] - va[1] - va[2] - va[3] - va[4] - va[5] - va[6]);
+                    const double pv = pota + alpha * va[0];
+                    A.pot[ga] = pv;
+                    const double rv = rva - alpha * a;
+                    A.r[ga] = rv;
+                    acc += rv * rv;
+                    if (check)
+                    {
+                        const double ratio = pv / olda;
+                        if ((tm > ratio) || (tp < ratio))
+                            fail = 1;
+                    }
+                }
+                if (has1)
+                {
+                    const double a =
+                        -oh2 * (6.0 * vb[0] - vb[1] - vb[2] - vb[3] - vb[4] - vb[5] - vb[6]);
+                    const double pv = potb + alpha * vb[0];
+                    A.pot[gb] = pv;
+                    const double rv = rvb - alpha * a;
+                    A.r[gb] = rv;
+                    acc += rv * rv;
+                    if (check)
+                    {
+                        const double ratio = pv / oldb;
+                        if ((tm > ratio) || (tp < ratio))
+                            fail = 1;
+                    }
+                }
+            }
+            const double t = block_sum_d(acc, sh);
             fail = __syncthreads_or(fail);
             if (threadIdx.x == 0)
             {
-                A.rr[k & 1][c] = t;
                 if (check && fail)
-                    atomicOr(&rfail[q], 1);
+                    atomicOr(&A.rfail[(k / A.every) & 1][x.q], 1);
+                cg_st_release(&A.rr[k & 1][x.c], t);
             }
         }
-        grid.sync();
+        __syncthreads();
+        if (gave_up)
+            break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-    {
-        A.status[0] = (int)(k - 1);
-        A.status[1] = all_done ? 1 : 0;
-    }
+    if (gave_up && threadIdx.x == 0)
+        atomicOr(&A.status[1], 1);
 }
 
 static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
-    // chunks over each node's interior list
+    // Chunks of 1024 interior points (never across nodes), two points a thread of
+    // a 512-thread block.  Levels of up to two chunks per resident block-slot
+    // give every block one chunk; larger levels give blocks several.
+    constexpr int kCgSmem = 40 * 1024; // slot records and cached grid indices
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    static int per_sm = 0;
+    static std::once_flag occ_once;
+    std::call_once(occ_once, [] {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cg_nodes,
+                                                      CG_MAX_THREADS, kCgSmem);
+    });
+    if (per_sm < 1)
+    {
+        set_error("conjugate gradient kernel cannot be resident");
+        return QZ_FAILURE;
+    }
+    const long max_blocks = (long)per_sm * sms;
+    const int nt = CG_MAX_THREADS;
+    const int chunk = 2 * nt;
     L.hchunks.clear();
     std::vector<int> node_chunk(2L * nn, 0);
     for (int q = 0; q < nn; q++)
     {
         node_chunk[2 * q] = (int)L.hchunks.size();
         const AmrNode &N = L.h[q];
-        for (int b = N.intr_off; b < N.intr_off + N.nintr; b += CG_CHUNK)
-            L.hchunks.push_back({q, b, std::min(b + CG_CHUNK, N.intr_off + N.nintr)});
+        for (int b = N.intr_off; b < N.intr_off + N.nintr; b += chunk)
+            L.hchunks.push_back({q, b, std::min(b + chunk, N.intr_off + N.nintr)});
         node_chunk[2 * q + 1] = (int)L.hchunks.size();
     }
     L.nchunks = (int)L.hchunks.size();
     if (L.nchunks == 0)
         return QZ_SUCCESS;
-    // nint: node_chunk (2 nn) | conv (nn) | rfail[0] (nn) | rfail[1] (nn) | status (2)
-    if (!L.chunks.ensure(L.nchunks) || !L.chunk_part.ensure(3L * L.nchunks) ||
-        !L.nint.ensure(5L * nn + 2) || !L.r.ensure(L.grid_total) ||
-        !L.p.ensure(L.grid_total) || !L.Ap.ensure(L.grid_total))
+    // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
+    if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, 4L * L.nchunks) ||
+        !L.nint.ensure(s->mem, 5L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
+        !L.p.ensure(s->mem, L.grid_total) || !L.Ap.ensure(s->mem, L.grid_total))
     {
         set_error("cg buffers");
         return QZ_FAILURE;
     }
+    // status[2]: nodes with interior points, all unconverged at the start
+    int active = 0;
+    for (int q = 0; q < nn; q++)
+        active += node_chunk[2 * q + 1] > node_chunk[2 * q];
+    node_chunk.resize(5L * nn + 3, 0);
+    node_chunk[4L * nn + 2] = active;
     if (!check_cuda(cudaMemcpyAsync(L.chunks.p, L.hchunks.data(), L.nchunks * sizeof(AmrChunk),
                                     cudaMemcpyHostToDevice, s->stream), "chunks") ||
-        !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), 2L * nn * sizeof(int),
+        !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), (5L * nn + 3) * sizeof(int),
                                     cudaMemcpyHostToDevice, s->stream), "cg ints"))
         return QZ_FAILURE;
-    // r and both p buffers are zero off the interior points
+    // r and both p buffers are zero off the interior points; partials start unpublished
     cudaMemsetAsync(L.r.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.p.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.Ap.p, 0, L.grid_total * sizeof(double), s->stream);
-    cudaMemsetAsync(L.nint.p + 2 * nn, 0, (3L * nn + 2) * sizeof(int), s->stream);
-    // iteration cap of the reference per node: min(node grid size, max_iter);
-    // nodes iterate in lockstep, so the level runs to the largest cap
-    long cap_it = 0;
-    for (auto &N : L.h)
-        cap_it = std::max(cap_it, std::min((long)c.max_iter,
-                                           (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1)));
+    cudaMemsetAsync(L.chunk_part.p, 0xff, 4L * L.nchunks * sizeof(double), s->stream);
     CgArgs A;
     A.chunks = L.chunks.p;
     A.nchunks = L.nchunks;
     A.intr = L.intr.p;
     A.nodes = L.nodes.p;
-    A.nn = nn;
     A.node_chunk = L.nint.p;
     A.d = L.d;
     A.pot = L.pot;
@@ -1492,31 +1680,29 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.r = L.r.p;
     A.pbuf[0] = L.p.p;
     A.pbuf[1] = L.Ap.p;
-    A.pap = L.chunk_part.p;
-    A.rr[0] = L.chunk_part.p + L.nchunks;
-    A.rr[1] = L.chunk_part.p + 2L * L.nchunks;
-    A.conv = L.nint.p + 2 * nn;
-    A.rfail[0] = L.nint.p + 3 * nn;
-    A.rfail[1] = L.nint.p + 4 * nn;
-    A.status = L.nint.p + 5 * nn;
+    A.pap[0] = L.chunk_part.p;
+    A.pap[1] = L.chunk_part.p + L.nchunks;
+    A.rr[0] = L.chunk_part.p + 2L * L.nchunks;
+    A.rr[1] = L.chunk_part.p + 3L * L.nchunks;
+    A.rfail[0] = L.nint.p + 2 * nn;
+    A.rfail[1] = L.nint.p + 3 * nn;
+    A.status = L.nint.p + 4 * nn;
+    A.iters = L.nint.p + 4 * nn + 3;
     A.tol = c.tol;
     A.tol2 = c.tol2;
     A.G = c.G;
     A.every = c.check_every > 0 ? c.check_every : 1;
-    A.cap_it = cap_it;
-    int per_sm = 0, sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    if (!check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_persistent,
-                                                                  CG_THREADS, 0), "occupancy"))
+    A.max_iter = c.max_iter;
+    const int blocks = (int)std::min(max_blocks, (long)L.nchunks);
+    const int nslot = (L.nchunks + blocks - 1) / blocks;
+    A.chunk = chunk;
+    A.ncache = std::max(0, (int)((kCgSmem - nslot * (long)sizeof(CgSlot)) / (chunk * 4L)));
+    const size_t smem = nslot * sizeof(CgSlot) + (size_t)std::min(nslot, A.ncache) * chunk * 4;
+    if (smem > (size_t)kCgSmem)
+    {
+        set_error("conjugate gradient: %d chunks per block exceed the shared memory budget", nslot);
         return QZ_FAILURE;
-    // blocks per SM: more hide memory latency, fewer make the grid barriers cheaper
-    static const int cg_bps = [] {
-        const char *e = getenv("QZ_CG_BLOCKS_PER_SM");
-        return e ? atoi(e) : 0;
-    }();
-    if (cg_bps > 0)
-        per_sm = std::min(per_sm, cg_bps);
-    int blocks = std::max(1, std::min(per_sm * sms, L.nchunks));
+    }
     void *args[] = {&A};
     cudaEvent_t eb = nullptr, ee = nullptr;
     if (s->prof)
@@ -1525,8 +1711,8 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
         ee = prof_event(s);
         cudaEventRecord(eb, s->stream);
     }
-    if (!check_cuda(cudaLaunchCooperativeKernel((void *)k_cg_persistent, dim3(blocks),
-                                                dim3(CG_THREADS), args, 0, s->stream),
+    if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_cg_nodes, dim3(blocks), dim3(nt),
+                                                args, smem, s->stream),
                     "cooperative cg"))
         return QZ_FAILURE;
     s->stats.kernel_launches++;
@@ -1535,17 +1721,26 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
         cudaEventRecord(ee, s->stream);
         s->prof_pending.push_back({QZ_PROF_CG, 0.0, eb, ee});
     }
-    int st[2];
-    if (!read_ints(s, A.status, 2, st))
+    std::vector<int> st(3 + nn);
+    if (!read_ints(s, A.status, 3 + nn, st.data()))
         return QZ_FAILURE;
     s->stats.cg_iterations += st[0];
     if (s->prof)
     {
-        // bytes of the launch per iteration and interior point: P phase reads r and
-        // p_{k-2} and writes p_{k-1} (24 B), U phase reads p, pot, r and writes pot, r (40 B)
-        s->prof_pending.back().bytes = 64.0 * L.intr_total * st[0];
+        // bytes per iteration and interior point: the P phase reads r and p_{k-2} and
+        // writes p_{k-1} (24 B), the U phase reads p, pot, r and writes pot, r (40 B)
+        double pts_it = 0.0;
+        for (int q = 0; q < nn; q++)
+            pts_it += (double)L.h[q].nintr * st[3 + q];
+        s->prof_pending.back().bytes = 64.0 * pts_it;
     }
-    if (!st[1])
+    if (st[1])
+    {
+        set_error("conjugate gradient in refinement level %d: a wait for partial sums gave up",
+                  level_index);
+        return QZ_FAILURE;
+    }
+    if (st[2] != 0)
     {
         set_error("the precision was not reached in refinement level %d after %d conjugate "
                   "gradient iterations", level_index, st[0]);
@@ -1563,7 +1758,7 @@ int amr_potential(qz_sim *s)
         AmrLevel &P = s->amr[l - 1];
         if (L.nnodes == 0)
             break;
-        if (!L.gpot.ensure(L.grid_total) || !L.gpot_old.ensure(L.grid_total))
+        if (!L.gpot.ensure(s->mem, L.grid_total) || !L.gpot_old.ensure(s->mem, L.grid_total))
         {
             set_error("level potential buffers");
             return QZ_FAILURE;
@@ -1666,8 +1861,8 @@ int amr_grid_accel(qz_sim *s)
         AmrLevel &P = s->amr[l - 1];
         if (L.nnodes == 0)
             break;
-        if (!L.gax.ensure(L.grid_total) || !L.gay.ensure(L.grid_total) ||
-            !L.gaz.ensure(L.grid_total))
+        if (!L.gax.ensure(s->mem, L.grid_total) || !L.gay.ensure(s->mem, L.grid_total) ||
+            !L.gaz.ensure(s->mem, L.grid_total))
         {
             set_error("level acceleration buffers");
             return QZ_FAILURE;

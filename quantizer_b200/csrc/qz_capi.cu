@@ -278,6 +278,25 @@ int qz_default_config(qz_config *c, int lmin)
     return QZ_SUCCESS;
 }
 
+// The simulation's stream-ordered pool: freed memory stays in the pool, so buffers
+// that grow with the refinement tree never wait for the device.
+static bool make_pool(qz_sim *s)
+{
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    if (!check_cuda(cudaMemPoolCreate(&s->mem.pool, &props), "memory pool"))
+    {
+        s->mem.pool = nullptr;
+        return false;
+    }
+    unsigned long long keep = ~0ULL;
+    s->mem.stream = s->stream;
+    return check_cuda(cudaMemPoolSetAttribute(s->mem.pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                      "memory pool threshold");
+}
+
 int qz_destroy(qz_sim *s)
 {
     if (!s)
@@ -298,6 +317,10 @@ int qz_destroy(qz_sim *s)
         dfree(p);
     free_levels(s);
     amr_free(s);
+    if (s->stream)
+        cudaStreamSynchronize(s->stream); // the pool frees are stream-ordered
+    if (s->mem.pool)
+        cudaMemPoolDestroy(s->mem.pool);
     if (s->h_flags)
         cudaFreeHost(s->h_flags);
     if (s->h_stage)
@@ -361,6 +384,11 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream"))
     {
         delete s;
+        return QZ_FAILURE;
+    }
+    if (!make_pool(s))
+    {
+        qz_destroy(s);
         return QZ_FAILURE;
     }
     s->cap = n_capacity;
@@ -781,7 +809,7 @@ static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, 
     cudaGetDevice(&s->device);
     size_t pts = (size_t)gridsize * gridsize * gridsize;
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream") ||
-        !dmalloc(dphi, pts, "phi") || !dmalloc(drho, pts, "rho") ||
+        !make_pool(s) || !dmalloc(dphi, pts, "phi") || !dmalloc(drho, pts, "rho") ||
         !check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned"))
     {
         qz_destroy(s);

@@ -88,23 +88,43 @@ struct AmrChunk {
     int node, begin, end; // [begin, end) of the level's interior list, one node
 };
 
-// Grow-only device buffer.
+// Stream-ordered allocation context of a simulation: a private memory pool that
+// keeps freed memory (release threshold at its maximum) and the stream the
+// simulation's work runs on, so that growing a buffer never synchronises the device.
+struct MemCtx {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+template <typename T> bool pool_alloc(const MemCtx &m, T **p, long count)
+{
+    *p = nullptr;
+    return cudaMallocFromPoolAsync((void **)p, (size_t)count * sizeof(T), m.pool, m.stream) ==
+           cudaSuccess;
+}
+
+inline void pool_free(const MemCtx &m, void *p)
+{
+    if (p)
+        cudaFreeAsync(p, m.stream);
+}
+
+// Grow-only device buffer (1.5x growth, stream-ordered).
 template <typename T>
 struct DBuf {
     T *p = nullptr;
     long cap = 0;
-    bool ensure(long need)
+    bool ensure(const MemCtx &m, long need)
     {
         if (need < 1)
             need = 1;
         if (p && need <= cap)
             return true;
         long nc = need > cap * 3 / 2 + 1024 ? need : cap * 3 / 2 + 1024;
-        if (p)
-            cudaFree(p);
+        pool_free(m, p);
         p = nullptr;
         cap = 0;
-        if (cudaMalloc((void **)&p, nc * sizeof(T)) != cudaSuccess)
+        if (!pool_alloc(m, &p, nc))
         {
             p = nullptr;
             return false;
@@ -112,10 +132,9 @@ struct DBuf {
         cap = nc;
         return true;
     }
-    void release()
+    void release(const MemCtx &m)
     {
-        if (p)
-            cudaFree(p);
+        pool_free(m, p);
         p = nullptr;
         cap = 0;
     }
@@ -146,6 +165,7 @@ struct AmrLevel {
     DBuf<AmrChunk> chunks;
     DBuf<double> chunk_part; // per chunk: p.Ap partial and two r.r partials
     int nchunks = 0;
+    int h_active = 0; // host copy of the unconverged-node count at the start of a solve
     std::vector<AmrChunk> hchunks;
 };
 
@@ -155,6 +175,7 @@ struct qz_sim {
     qz_config cfg;
     int device = 0;
     cudaStream_t stream = nullptr;
+    qz::MemCtx mem; // stream-ordered pool for buffers that grow during a run
     long n = 0, cap = 0;
     double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *m = nullptr;
