@@ -161,65 +161,109 @@ __global__ void k_flag(int ncell, int ref_ptcl, const int *__restrict__ cell_box
             }
 }
 
-__global__ void k_cc_init(int ncell, const int *__restrict__ cell_box, const int *__restrict__ box,
+// Union-find over the refine cells (status -1) of a level, joined through face
+// neighbours inside a node's box.  Every parent pointer refers to a smaller cell
+// position or to the cell itself, so the root of a component is its first cell
+// and zones come out numbered in the order of their first cell, as the
+// reference numbers them.  The start points every cell at its smallest refine
+// face neighbour, which leaves short trees for the hooking pass.
+__global__ void k_cc_init(int ncell, const int *__restrict__ cell_box,
+                          const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
+                          const int *__restrict__ box, const int *__restrict__ pos_of_box,
                           int *__restrict__ parent)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell)
         return;
-    parent[c] = box[cell_box[c]] == -1 ? c : -1;
+    const long b = cell_box[c];
+    if (box[b] != -1)
+    {
+        parent[c] = -1;
+        return;
+    }
+    const AmrNode N = nodes[cell_node[c]];
+    const long sy = N.rd[0], sz = (long)N.rd[0] * N.rd[1];
+    const long off[6] = {1, -1, sy, -sy, sz, -sz};
+    int m = c;
+    for (int e = 0; e < 6; e++)
+    {
+        const long nb = b + off[e];
+        if (box[nb] != -1)
+            continue;
+        const int q = pos_of_box[nb];
+        if (q >= 0 && q < m)
+            m = q;
+    }
+    parent[c] = m;
 }
 
-// Root of x; loads bypass L1 (parents change under concurrent hooking).
-__device__ __forceinline__ int cc_find(const int *parent, int x)
+// Root of x, pointing every visited cell at its grandparent on the way (path
+// splitting).  Loads bypass L1: parents change under concurrent hooking.  Only
+// non-roots are rewritten, always to an ancestor, so the races are benign.
+__device__ __forceinline__ int cc_find(int *parent, int x)
 {
     int p = __ldcg(&parent[x]);
     for (int guard = 0; p != x && guard < (1 << 20); guard++)
     {
+        const int gp = __ldcg(&parent[p]);
+        if (gp != p)
+            __stcg(&parent[x], gp);
         x = p;
-        p = __ldcg(&parent[x]);
+        p = gp;
     }
     return x;
 }
 
+// Joins each refine cell with its +x, +y and +z refine neighbours (every face
+// once): the larger root is hooked under the smaller one by compare-and-swap.
 __global__ void k_cc_hook(int ncell, const int *__restrict__ cell_box,
                           const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
                           const int *__restrict__ box, const int *__restrict__ pos_of_box,
                           int *parent, int *__restrict__ flags)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell || parent[c] < 0)
+    if (c >= ncell || __ldcg(&parent[c]) < 0)
         return;
     const AmrNode N = nodes[cell_node[c]];
     const long b = cell_box[c];
-    const long off[6] = {1, -1, N.rd[0], -(long)N.rd[0], (long)N.rd[0] * N.rd[1],
-                         -(long)N.rd[0] * N.rd[1]};
-    for (int e = 0; e < 6; e++)
+    const long off[3] = {1, N.rd[0], (long)N.rd[0] * N.rd[1]};
+    for (int e = 0; e < 3; e++)
     {
-        long nb = b + off[e];
+        const long nb = b + off[e];
         if (box[nb] != -1)
             continue;
-        int q = pos_of_box[nb];
+        const int q = pos_of_box[nb];
         if (q < 0)
             continue;
+        int ra = cc_find(parent, c), rb = cc_find(parent, q);
         int guard = 0;
-        for (; guard < (1 << 10); guard++)
+        for (; guard < (1 << 10) && ra != rb; guard++)
         {
-            int ra = cc_find(parent, c), rb = cc_find(parent, q);
-            if (ra == rb)
-                break;
             if (ra < rb)
             {
-                int t = ra;
+                const int t = ra;
                 ra = rb;
                 rb = t;
             }
-            if (atomicCAS(&parent[ra], ra, rb) == ra)
+            const int old = atomicCAS(&parent[ra], ra, rb);
+            if (old == ra)
                 break;
+            ra = cc_find(parent, old);
+            rb = cc_find(parent, rb);
         }
         if (guard >= (1 << 10))
             atomicOr(&flags[F_ERROR], 4);
     }
+}
+
+// Every refine cell points at its root.
+__global__ void k_cc_compress(int ncell, int *parent)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell || __ldcg(&parent[c]) < 0)
+        return;
+    const int r = cc_find(parent, c);
+    __stcg(&parent[c], r);
 }
 
 __global__ void k_cc_roots(int ncell, const int *__restrict__ parent, int *__restrict__ is_root,
@@ -259,26 +303,38 @@ __global__ void k_zone_box_init(int nz, int *zone_box, int *zone_cells)
 // ids, and refine cells are written in cell order to (zone, cell) pairs.
 __global__ void k_cc_label(int ncell, const int *__restrict__ cell_box,
                            const int *__restrict__ cell_node, const AmrNode *__restrict__ nodes,
-                           const int *parent, const int *__restrict__ zrank,
+                           const int *__restrict__ parent, const int *__restrict__ zrank,
                            const int *__restrict__ slot, int *__restrict__ box,
                            int *__restrict__ zone_box, int *__restrict__ zone_cells,
                            const int *__restrict__ cell_xyz, unsigned *__restrict__ key,
                            int *__restrict__ val)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell || parent[c] < 0)
+    if (c >= ncell)
         return;
-    int r = cc_find(parent, c);
-    int zg = zrank[r];
+    const int r = parent[c]; // the root (parents are compressed)
+    const int zg = r >= 0 ? zrank[r] : -1;
+    // lanes of one zone add their bounds and count once (a zone spans many cells)
+    const unsigned grp = __match_any_sync(__activemask(), zg);
+    if (r < 0)
+        return;
+    const int x = cell_xyz[3 * c + 0], y = cell_xyz[3 * c + 1], z = cell_xyz[3 * c + 2];
+    const int x0 = __reduce_min_sync(grp, x), y0 = __reduce_min_sync(grp, y),
+              z0 = __reduce_min_sync(grp, z);
+    const int x1 = __reduce_max_sync(grp, x), y1 = __reduce_max_sync(grp, y),
+              z1 = __reduce_max_sync(grp, z);
+    if ((int)(threadIdx.x & 31) == __ffs(grp) - 1)
+    {
+        atomicMin(&zone_box[6 * zg + 0], x0);
+        atomicMin(&zone_box[6 * zg + 1], y0);
+        atomicMin(&zone_box[6 * zg + 2], z0);
+        atomicMax(&zone_box[6 * zg + 3], x1);
+        atomicMax(&zone_box[6 * zg + 4], y1);
+        atomicMax(&zone_box[6 * zg + 5], z1);
+        atomicAdd(&zone_cells[zg], __popc(grp));
+    }
     const AmrNode N = nodes[cell_node[c]];
     box[cell_box[c]] = zg - N.zone_base;
-    atomicMin(&zone_box[6 * zg + 0], cell_xyz[3 * c + 0]);
-    atomicMin(&zone_box[6 * zg + 1], cell_xyz[3 * c + 1]);
-    atomicMin(&zone_box[6 * zg + 2], cell_xyz[3 * c + 2]);
-    atomicMax(&zone_box[6 * zg + 3], cell_xyz[3 * c + 0]);
-    atomicMax(&zone_box[6 * zg + 4], cell_xyz[3 * c + 1]);
-    atomicMax(&zone_box[6 * zg + 5], cell_xyz[3 * c + 2]);
-    atomicAdd(&zone_cells[zg], 1);
     key[slot[c]] = (unsigned)zg;
     val[slot[c]] = c;
 }
@@ -543,11 +599,11 @@ static void free_level(const MemCtx &m, AmrLevel &L)
 {
     DBuf<int> *ib[] = {&L.box, &L.cnt, &L.pos_of_box, &L.cell_seg, &L.cell_box, &L.cell_xyz,
                        &L.cell_node, &L.intr, &L.bdry, &L.simb, &L.intr_node, &L.bdry_node,
-                       &L.simb_node, &L.nint};
+                       &L.simb_node, &L.nint, &L.mass_range};
     for (auto *b : ib)
         b->release(m);
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
-                          &L.chunk_part};
+                          &L.chunk_part, &L.mass_part};
     for (auto *b : db)
         b->release(m);
     L.nodes.release(m);
@@ -707,11 +763,13 @@ int amr_build(qz_sim *s)
         }
         int *parent = s->amr_tmp.p, *isroot = parent + nc, *zrank = isroot + nc,
             *flagged = zrank + nc, *slot = flagged + nc;
-        launch(s, QZ_PROF_TREE, 8.0 * nc, k_cc_init, dim3(blocks_for(nc, 256)), dim3(256), nc,
-               P.cell_box.p, P.box.p, parent);
+        launch(s, QZ_PROF_TREE, 36.0 * nc, k_cc_init, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               P.cell_box.p, P.cell_node.p, P.nodes.p, P.box.p, P.pos_of_box.p, parent);
         launch(s, QZ_PROF_TREE, 32.0 * nc, k_cc_hook, dim3(blocks_for(nc, 256)), dim3(256), nc,
                P.cell_box.p, P.cell_node.p, P.nodes.p, P.box.p, P.pos_of_box.p, parent,
                s->flags);
+        launch(s, QZ_PROF_TREE, 8.0 * nc, k_cc_compress, dim3(blocks_for(nc, 256)), dim3(256), nc,
+               parent);
         launch(s, QZ_PROF_TREE, 12.0 * nc, k_cc_roots, dim3(blocks_for(nc, 256)), dim3(256), nc,
                parent, isroot, flagged);
         if (scan_exclusive(s, isroot, zrank, nc) || scan_exclusive(s, flagged, slot, nc))
@@ -1014,42 +1072,71 @@ __global__ void k_lvl_point_gather(long total, int nn, const AmrNode *__restrict
 }
 
 // Node masses and particle counts from the cell segments (segments of a node
-// are contiguous in key order): one block per node, fixed-order sums.
-__global__ void k_node_mass(int nn, AmrNode *nodes, const int *__restrict__ seg_cell,
-                            const int *__restrict__ seg_start, const double *__restrict__ smass,
-                            const int *__restrict__ flags)
+// are contiguous in key order).  Pass 1: block (node, j) adds the j-th of
+// NM_PARTS equal slices of the node's segments; pass 2 adds the slices in order,
+// so the sum does not depend on scheduling.
+constexpr int NM_PARTS = 32;
+
+__device__ __forceinline__ int seg_lower_bound(const int *seg_cell, int nseg, long key)
+{
+    int lo = 0, hi = nseg; // first segment with cell >= key
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if ((long)seg_cell[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_node_mass_parts(int nn, const AmrNode *__restrict__ nodes,
+                                  const int *__restrict__ seg_cell,
+                                  const double *__restrict__ smass, const int *__restrict__ flags,
+                                  double *__restrict__ part, int *__restrict__ range)
 {
     __shared__ double sh[32];
     __shared__ int lo_hi[2];
-    const int nd = blockIdx.x;
-    if (nd >= nn)
-        return;
+    const int nd = blockIdx.x, j = blockIdx.y;
     const int nseg = flags[F_NSEG];
     if (threadIdx.x < 2)
     {
-        long key = threadIdx.x == 0 ? nodes[nd].box_off
-                                    : nodes[nd].box_off + (long)nodes[nd].rd[0] * nodes[nd].rd[1] * nodes[nd].rd[2];
-        int lo = 0, hi = nseg; // first segment with cell >= key
-        while (lo < hi)
-        {
-            int mid = (lo + hi) >> 1;
-            if ((long)seg_cell[mid] < key)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        lo_hi[threadIdx.x] = lo;
+        const AmrNode N = nodes[nd];
+        const long key = N.box_off + (threadIdx.x == 0 ? 0L : (long)N.rd[0] * N.rd[1] * N.rd[2]);
+        lo_hi[threadIdx.x] = seg_lower_bound(seg_cell, nseg, key);
     }
     __syncthreads();
+    const int lo = lo_hi[0], hi = lo_hi[1];
+    const int len = (hi - lo + NM_PARTS - 1) / NM_PARTS;
+    const int b = lo + j * len, e = min(hi, b + len);
     double acc = 0.0;
-    for (int q = lo_hi[0] + threadIdx.x; q < lo_hi[1]; q += blockDim.x)
+    for (int q = b + threadIdx.x; q < e; q += blockDim.x)
         acc += smass[q];
-    double tot = block_sum_d(acc, sh);
+    const double tot = block_sum_d(acc, sh);
     if (threadIdx.x == 0)
     {
-        nodes[nd].mass = tot;
-        nodes[nd].nptcl = lo_hi[1] > lo_hi[0] ? seg_start[lo_hi[1]] - seg_start[lo_hi[0]] : 0;
+        part[nd * NM_PARTS + j] = tot;
+        if (j == 0)
+        {
+            range[2 * nd] = lo;
+            range[2 * nd + 1] = hi;
+        }
     }
+}
+
+__global__ void k_node_mass(int nn, AmrNode *nodes, const int *__restrict__ seg_start,
+                            const double *__restrict__ part, const int *__restrict__ range)
+{
+    const int nd = blockIdx.x * blockDim.x + threadIdx.x;
+    if (nd >= nn)
+        return;
+    double tot = 0.0;
+    for (int j = 0; j < NM_PARTS; j++)
+        tot += part[nd * NM_PARTS + j];
+    const int lo = range[2 * nd], hi = range[2 * nd + 1];
+    nodes[nd].mass = tot;
+    nodes[nd].nptcl = hi > lo ? seg_start[hi] - seg_start[lo] : 0;
 }
 
 int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
@@ -1104,8 +1191,18 @@ int amr_deposit(qz_sim *s)
         launch(s, QZ_PROF_DEPOSIT, 12.0 * L.grid_total, k_lvl_point_gather,
                dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, L.nnodes, L.nodes.p,
                L.cell_seg.p, s->cell_sums, L.d);
-        launch(s, QZ_PROF_DEPOSIT, 16.0 * m, k_node_mass, dim3(L.nnodes), dim3(256), L.nnodes,
-               L.nodes.p, s->seg_cell, s->seg_start, s->seg_mass.p, s->flags);
+        if (!L.mass_part.ensure(s->mem, (long)NM_PARTS * L.nnodes) ||
+            !L.mass_range.ensure(s->mem, 2L * L.nnodes))
+        {
+            set_error("node mass buffers");
+            return QZ_FAILURE;
+        }
+        launch(s, QZ_PROF_DEPOSIT, 12.0 * m, k_node_mass_parts, dim3(L.nnodes, NM_PARTS), dim3(256),
+               L.nnodes, L.nodes.p, s->seg_cell, s->seg_mass.p, s->flags, L.mass_part.p,
+               L.mass_range.p);
+        launch(s, QZ_PROF_DEPOSIT, 8.0 * NM_PARTS * L.nnodes, k_node_mass,
+               dim3(blocks_for(L.nnodes, 128)), dim3(128), L.nnodes, L.nodes.p, s->seg_start,
+               L.mass_part.p, L.mass_range.p);
         std::vector<AmrNode> tmp(L.nnodes);
         if (!check_cuda(cudaMemcpyAsync(tmp.data(), L.nodes.p, L.nnodes * sizeof(AmrNode),
                                         cudaMemcpyDeviceToHost, s->stream), "nodes d2h") ||

@@ -312,11 +312,13 @@ int qz_destroy(qz_sim *s)
     void *ptrs[] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m,
                     s->pot, s->pot_old, s->d, s->gax, s->gay, s->gaz, s->sort.k0, s->sort.k1,
                     s->sort.v0, s->sort.v1, s->sort.hist, s->seg_head, s->seg_id, s->seg_start,
-                    s->seg_cell, s->cell_seg, s->cell_sums, s->scan_tmp, s->red, s->flags};
+                    s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags};
     for (void *p : ptrs)
         dfree(p);
     free_levels(s);
     amr_free(s);
+    if (s->mem.pool)
+        pool_free(s->mem, s->scan_tmp);
     if (s->stream)
         cudaStreamSynchronize(s->stream); // the pool frees are stream-ordered
     if (s->mem.pool)

@@ -163,7 +163,9 @@ struct AmrLevel {
     DBuf<double> gpot, gpot_old, gd, gax, gay, gaz, r, p, Ap;
     DBuf<int> nint; // node chunk ranges, converged flags, ratio-test flags, status
     DBuf<AmrChunk> chunks;
-    DBuf<double> chunk_part; // per chunk: p.Ap partial and two r.r partials
+    DBuf<double> chunk_part; // per chunk: two p.Ap and two r.r partials
+    DBuf<double> mass_part;  // node mass slices (32 a node)
+    DBuf<int> mass_range;    // per node: segment range
     int nchunks = 0;
     int h_active = 0; // host copy of the unconverged-node count at the start of a solve
     std::vector<AmrChunk> hchunks;

@@ -178,8 +178,8 @@ __global__ void k_scan_single(int *__restrict__ a, long m)
     }
 }
 
-__global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, long n,
-                             const int *__restrict__ tile_offsets)
+// in and out may be the same array (each block reads its tile before writing it)
+__global__ void k_scan_apply(const int *in, int *out, long n, const int *__restrict__ tile_offsets)
 {
     __shared__ int sh[32];
     long base = (long)blockIdx.x * SC_TILE + (long)threadIdx.x * SC_ITEMS;
@@ -207,12 +207,16 @@ int scan_exclusive(qz_sim *s, const int *in, int *out, long n)
     long tiles = (n + SC_TILE - 1) / SC_TILE;
     if (s->scan_tmp_cap < tiles)
     {
-        if (s->scan_tmp)
-            cudaFree(s->scan_tmp);
+        pool_free(s->mem, s->scan_tmp);
         s->scan_tmp = nullptr;
-        if (!check_cuda(cudaMalloc(&s->scan_tmp, tiles * sizeof(int)), "scan scratch"))
+        s->scan_tmp_cap = 0;
+        const long cap = tiles + tiles / 2 + 64;
+        if (!pool_alloc(s->mem, &s->scan_tmp, cap))
+        {
+            set_error("scan scratch: out of device memory");
             return QZ_FAILURE;
-        s->scan_tmp_cap = tiles;
+        }
+        s->scan_tmp_cap = cap;
     }
     launch(s, QZ_PROF_SORT, 4.0 * n, k_scan_tiles, dim3((int)tiles), dim3(SC_THREADS), in, n, s->scan_tmp);
     launch(s, QZ_PROF_SORT, 8.0 * 256 * tiles, k_scan_single, dim3(1), dim3(SC_THREADS), s->scan_tmp, tiles);
@@ -237,7 +241,12 @@ int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **val
     for (int shift = 0; shift < bits; shift += 8)
     {
         launch(s, QZ_PROF_SORT, 4.0 * n, k_rs_upsweep, dim3(tiles), dim3(RS_WARPS * 32), ki, n, shift, tiles, S.hist);
-        launch(s, QZ_PROF_SORT, 8.0 * 256 * tiles, k_scan_single, dim3(1), dim3(SC_THREADS), S.hist, (long)RS_RADIX * tiles);
+        // digit-major counts of all tiles: exclusive scan in place (one block when small)
+        const long hm = (long)RS_RADIX * tiles;
+        if (hm <= 4L * SC_TILE)
+            launch(s, QZ_PROF_SORT, 8.0 * hm, k_scan_single, dim3(1), dim3(SC_THREADS), S.hist, hm);
+        else if (scan_exclusive(s, S.hist, S.hist, hm))
+            return QZ_FAILURE;
         launch(s, QZ_PROF_SORT, 16.0 * n, k_rs_downsweep, dim3(tiles), dim3(RS_WARPS * 32), ki, vi, ko, vo, n, shift, tiles, S.hist);
         unsigned *tk = ki;
         ki = ko;
