@@ -603,7 +603,7 @@ static void free_level(const MemCtx &m, AmrLevel &L)
     for (auto *b : ib)
         b->release(m);
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
-                          &L.chunk_part, &L.mass_part};
+                          &L.apv, &L.chunk_part, &L.mass_part};
     for (auto *b : db)
         b->release(m);
     L.nodes.release(m);
@@ -1324,6 +1324,7 @@ struct CgArgs {
     const double *d;
     double *pot, *pot_old, *r;
     double *pbuf[2]; // p_j in pbuf[j & 1]
+    double *apv;     // Ap of the current iteration at the interior points
     double *pap[2];  // per chunk: partial p.Ap of iteration k in pap[k & 1]
     double *rr[2];   // per chunk: partial r_j.r_j in rr[j & 1]
     int *rfail[2];   // per node: ratio test failed at check j, in rfail[j & 1]
@@ -1342,6 +1343,20 @@ __device__ __forceinline__ double cg_ld_acquire(const double *p)
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ double cg_ld_relaxed(const double *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ void cg_st_relaxed(double *p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p),
+                 "l"((unsigned long long)__double_as_longlong(v))
+                 : "memory");
 }
 
 __device__ __forceinline__ void cg_st_release(double *p, double v)
@@ -1408,8 +1423,10 @@ __device__ __forceinline__ double2 cg_reduce(double a, double b, int &f, double2
 }
 
 // Sum of the published partials of chunks [cb, ce), waiting for each; thread t
-// takes chunks cb + t, cb + t + blockDim, ...  *gave_up is set in every thread
-// if a wait hit the poll limit.
+// takes chunks cb + t, cb + t + blockDim, ...  ACQ: acquire loads (the partials
+// also publish data), else relaxed.  *gave_up is set in every thread if a wait
+// hit the poll limit.
+template <bool ACQ>
 __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce, int *gave_up,
                                               double2 *sh2, int *shf)
 {
@@ -1417,7 +1434,7 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
     int bad = 0;
     for (int c = cb + (int)threadIdx.x; c < ce; c += (int)blockDim.x)
     {
-        double v = cg_ld_acquire(&part[c]);
+        double v = ACQ ? cg_ld_acquire(&part[c]) : cg_ld_relaxed(&part[c]);
         int polls = 0;
         while (__double_as_longlong(v) == CG_EMPTY)
         {
@@ -1427,7 +1444,7 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
                 v = 0.0;
                 break;
             }
-            v = cg_ld_acquire(&part[c]);
+            v = ACQ ? cg_ld_acquire(&part[c]) : cg_ld_relaxed(&part[c]);
         }
         s += v;
     }
@@ -1437,7 +1454,7 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
     return t.x;
 }
 
-__global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
+__global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
 {
     __shared__ double sh[32];
     __shared__ double2 sh2[CG_MAX_THREADS / 32];
@@ -1521,7 +1538,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
             if (x.q != cq)
             {
                 // rs_{k-1}; also makes the node's r of iteration k-1 visible
-                rs1 = cg_node_sum(A.rr[(k - 1) & 1], x.cb, x.ce, &gave_up, sh2, shf);
+                rs1 = cg_node_sum<true>(A.rr[(k - 1) & 1], x.cb, x.ce, &gave_up, sh2, shf);
                 cq = x.q;
                 if (gave_up)
                     break;
@@ -1592,6 +1609,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
                                           (ra[3] + beta * pa[3]) - (ra[4] + beta * pa[4]) -
                                           (ra[5] + beta * pa[5]) - (ra[6] + beta * pa[6]));
                 pnew[ga] = p0a;
+                A.apv[ga] = aa;
                 acc += p0a * aa;
                 if (has1)
                 {
@@ -1601,6 +1619,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
                                 (rb[3] + beta * pb[3]) - (rb[4] + beta * pb[4]) -
                                 (rb[5] + beta * pb[5]) - (rb[6] + beta * pb[6]));
                     pnew[gb] = p0b;
+                    A.apv[gb] = ab;
                     acc += p0b * ab;
                 }
             }
@@ -1609,13 +1628,16 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
             {
                 x.rs_prev = rs1;
                 x.rs_cur = rs1;
-                cg_st_release(&A.pap[k & 1][x.c], t);
+                // the U phase reads no other block's data of this phase: no fence
+                cg_st_relaxed(&A.pap[k & 1][x.c], t);
             }
         }
         __syncthreads(); // slot flags written by thread 0 above
         if (gave_up || !live)
             break;
         // ---- U phase ----
+        // Only this thread's own points are read (p_{k-1} and Ap stored by the P
+        // phase, pot, r): their loads are issued before the wait for p.Ap.
         const bool check = k % A.every == 0;
         const double *pn = pnew;
         const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
@@ -1626,10 +1648,32 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
             CgSlot &x = slot[s];
             if (x.done)
                 continue;
+            const int e0 = threadIdx.x, e1 = threadIdx.x + NT;
+            const bool h0 = e0 < x.n, h1 = e1 < x.n;
+            const int ga = h0 ? gi(s, e0) : 0, gb = h1 ? gi(s, e1) : 0;
+            double apa = 0.0, apb = 0.0, pva = 0.0, pvb = 0.0, pota = 0.0, potb = 0.0,
+                   rva = 0.0, rvb = 0.0, olda = 1.0, oldb = 1.0;
+            if (h0)
+            {
+                apa = A.apv[ga];
+                pva = pn[ga];
+                pota = A.pot[ga];
+                rva = A.r[ga];
+                if (check)
+                    olda = A.pot_old[ga];
+            }
+            if (h1)
+            {
+                apb = A.apv[gb];
+                pvb = pn[gb];
+                potb = A.pot[gb];
+                rvb = A.r[gb];
+                if (check)
+                    oldb = A.pot_old[gb];
+            }
             if (x.q != cq)
             {
-                // p.Ap; also makes the node's p of iteration k visible
-                pap = cg_node_sum(A.pap[k & 1], x.cb, x.ce, &gave_up, sh2, shf);
+                pap = cg_node_sum<false>(A.pap[k & 1], x.cb, x.ce, &gave_up, sh2, shf);
                 cq = x.q;
                 if (gave_up)
                     break;
@@ -1638,53 +1682,34 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
             if (threadIdx.x == 0)
                 A.rr[(k - 1) & 1][x.c] = empty;
             const double alpha = x.rs_cur / pap;
-            const double oh2 = x.oh2;
-            const int sy = x.sy, sz = x.sz;
             double acc = 0.0;
             int fail = 0;
-            // a thread's two points of a chunk together, so their loads overlap
-            for (int e0 = threadIdx.x; e0 < x.n; e0 += 2 * NT)
+            if (h0)
             {
-                const int e1 = e0 + NT;
-                const bool has1 = e1 < x.n;
-                const int ga = gi(s, e0), gb = has1 ? gi(s, e1) : ga;
-                double va[7], vb[7];
-                cg_load7(pn, ga, sy, sz, va);
-                cg_load7(pn, gb, sy, sz, vb);
-                const double pota = A.pot[ga], potb = A.pot[gb];
-                const double rva = A.r[ga], rvb = A.r[gb];
-                const double olda = check ? A.pot_old[ga] : 1.0;
-                const double oldb = check ? A.pot_old[gb] : 1.0;
+                const double pv = pota + alpha * pva;
+                A.pot[ga] = pv;
+                const double rv = rva - alpha * apa;
+                A.r[ga] = rv;
+                acc += rv * rv;
+                if (check)
                 {
-                    const double a =
-                        -oh2 * (6.0 * va[0] - va[1] - va[2] - va[3] - va[4] - va[5] - va[6]);
-                    const double pv = pota + alpha * va[0];
-                    A.pot[ga] = pv;
-                    const double rv = rva - alpha * a;
-                    A.r[ga] = rv;
-                    acc += rv * rv;
-                    if (check)
-                    {
-                        const double ratio = pv / olda;
-                        if ((tm > ratio) || (tp < ratio))
-                            fail = 1;
-                    }
+                    const double ratio = pv / olda;
+                    if ((tm > ratio) || (tp < ratio))
+                        fail = 1;
                 }
-                if (has1)
+            }
+            if (h1)
+            {
+                const double pv = potb + alpha * pvb;
+                A.pot[gb] = pv;
+                const double rv = rvb - alpha * apb;
+                A.r[gb] = rv;
+                acc += rv * rv;
+                if (check)
                 {
-                    const double a =
-                        -oh2 * (6.0 * vb[0] - vb[1] - vb[2] - vb[3] - vb[4] - vb[5] - vb[6]);
-                    const double pv = potb + alpha * vb[0];
-                    A.pot[gb] = pv;
-                    const double rv = rvb - alpha * a;
-                    A.r[gb] = rv;
-                    acc += rv * rv;
-                    if (check)
-                    {
-                        const double ratio = pv / oldb;
-                        if ((tm > ratio) || (tp < ratio))
-                            fail = 1;
-                    }
+                    const double ratio = pv / oldb;
+                    if ((tm > ratio) || (tp < ratio))
+                        fail = 1;
                 }
             }
             const double t = block_sum_d(acc, sh);
@@ -1693,6 +1718,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS) k_cg_nodes(CgArgs A)
             {
                 if (check && fail)
                     atomicOr(&A.rfail[(k / A.every) & 1][x.q], 1);
+                // publishes this block's r and p of the iteration with the partial
                 cg_st_release(&A.rr[k & 1][x.c], t);
             }
         }
@@ -1744,7 +1770,8 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
     if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, 4L * L.nchunks) ||
         !L.nint.ensure(s->mem, 5L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
-        !L.p.ensure(s->mem, L.grid_total) || !L.Ap.ensure(s->mem, L.grid_total))
+        !L.p.ensure(s->mem, L.grid_total) || !L.Ap.ensure(s->mem, L.grid_total) ||
+        !L.apv.ensure(s->mem, L.grid_total))
     {
         set_error("cg buffers");
         return QZ_FAILURE;
@@ -1777,6 +1804,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.r = L.r.p;
     A.pbuf[0] = L.p.p;
     A.pbuf[1] = L.Ap.p;
+    A.apv = L.apv.p;
     A.pap[0] = L.chunk_part.p;
     A.pap[1] = L.chunk_part.p + L.nchunks;
     A.rr[0] = L.chunk_part.p + 2L * L.nchunks;

@@ -15,7 +15,9 @@
 //                    points in the reference's scatter order, fused with
 //                    phi += dphi (multigrid.c:51-104, 199-209)
 //   k_check_*        ratio test + residual norm, fixed-tree deterministic sums
+#include <cooperative_groups.h>
 #include <cuda_pipeline.h>
+#include <mutex>
 
 #include "qz_internal.cuh"
 
@@ -525,6 +527,329 @@ static int vcycle_t(qz_sim *s, int l, int type)
 
 int vcycle(qz_sim *s, int level, int type) { return vcycle_t<double>(s, level, type); }
 
+// ---- persistent V-cycles ----------------------------------------------------------
+// The red-black V-cycle (multigrid.c:106-229 with the smoother, restriction and
+// prolongation above) as one cooperative launch that runs several cycles.  A
+// cycle is a fixed sequence of dependent phases on grids that fit in L2, so one
+// launch per phase costs more than the work; here the levels larger than
+// MG_SMALL_N points a side run their phases on the whole grid separated by grid
+// barriers, and the smaller levels run inside block 0 with block barriers while
+// the other blocks wait at the next grid barrier.  Every point update uses the
+// arithmetic of the kernels above, and the order of updates within a phase does
+// not matter (one colour of a red-black sweep, restriction and prolongation read
+// only what earlier phases wrote), so the result equals the launch-per-phase
+// path bit for bit.  In the mixed-precision form a launch also holds the FP64
+// fine residual and the FP64 correction of each iteration.
+namespace cgm = cooperative_groups;
+
+constexpr int MG_MAXLEV = 12;
+constexpr int MG_SMALL_N = 17;
+constexpr int MG_THREADS = 512;
+
+template <typename T> struct MgArgs {
+    Grid<T> phi[MG_MAXLEV], rho[MG_MAXLEV];
+    int nlev;   // levels; the last one is smoothed instead of corrected
+    int nsmall; // first level of at most MG_SMALL_N points a side
+    int n_pre, n_post, n_coarse;
+    T w, scale;
+    int iters; // cycles (mixed: defect-correction iterations) in this launch
+    int mixed;
+    Grid<double> fphi, frho; // FP64 fine grid (mixed form): phi[0] / rho[0] are ef / rf
+};
+
+template <typename T>
+__device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rho, int color,
+                                           T H2, T w, unsigned tid, unsigned nthr)
+{
+    const int m = phi.n - 2;
+    const unsigned half = (unsigned)(m + 1) / 2;
+    const unsigned total = half * (unsigned)m * (unsigned)m;
+    const T one_sixth = (T)(1.0 / 6.0);
+    for (unsigned t = tid; t < total; t += nthr)
+    {
+        const unsigned ti = t % half, r = t / half;
+        const int j = 1 + (int)(r % (unsigned)m), k = 1 + (int)(r / (unsigned)m);
+        const int i = ((((1 + j + k) & 1) == color) ? 1 : 2) + 2 * (int)ti;
+        if (i > m)
+            continue;
+        const long gp = phi.off + i + j * phi.sy + k * phi.sz;
+        const long gr = rho.off + i + j * rho.sy + k * rho.sz;
+        T *p = phi.p;
+        T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
+                           p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
+        p[gp] = w * a + ((T)1.0 - w) * p[gp];
+    }
+}
+
+// rho_c = scale * residual at the injected points; phi_c = 0 everywhere.
+template <typename T>
+__device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &rho,
+                                            const Grid<T> &cphi, const Grid<T> &crho, T ooh2,
+                                            T scale, unsigned tid, unsigned nthr)
+{
+    const unsigned nc = (unsigned)cphi.n, nc3 = nc * nc * nc;
+    for (unsigned t = tid; t < nc3; t += nthr)
+    {
+        const int i = (int)(t % nc), j = (int)((t / nc) % nc), k = (int)(t / (nc * nc));
+        cphi.p[cphi.off + i + j * cphi.sy + k * cphi.sz] = (T)0;
+    }
+    const unsigned mc = nc - 2, mc3 = mc * mc * mc;
+    for (unsigned t = tid; t < mc3; t += nthr)
+    {
+        const int lx = 1 + (int)(t % mc), ly = 1 + (int)((t / mc) % mc), lz = 1 + (int)(t / (mc * mc));
+        const long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
+        const long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
+        const T *p = phi.p;
+        T rv = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
+                                   p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
+        crho.p[crho.off + lx + ly * crho.sy + lz * crho.sz] = scale * rv;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void mg_prolong(const Grid<T> &phi, const Grid<T> &c, unsigned tid,
+                                           unsigned nthr)
+{
+    const int m = phi.n - 2, mc = c.n - 2;
+    const unsigned um = (unsigned)m, total = um * um * um;
+    for (unsigned t = tid; t < total; t += nthr)
+    {
+        const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+        int cx0, cx1, cy0, cy1, cz0, cz1;
+        T wx, wy, wz;
+        if (i & 1) { cx0 = (i - 1) >> 1; cx1 = cx0 + 1; wx = (T)0.5; } else { cx0 = cx1 = i >> 1; wx = (T)1; }
+        if (j & 1) { cy0 = (j - 1) >> 1; cy1 = cy0 + 1; wy = (T)0.5; } else { cy0 = cy1 = j >> 1; wy = (T)1; }
+        if (k & 1) { cz0 = (k - 1) >> 1; cz1 = cz0 + 1; wz = (T)0.5; } else { cz0 = cz1 = k >> 1; wz = (T)1; }
+        T acc;
+        if (!(i & 1) && !(j & 1) && !(k & 1))
+            acc = c.p[c.off + cx0 + cy0 * c.sy + cz0 * c.sz];
+        else
+        {
+            const T wgt = wx * wy * wz;
+            acc = (T)0;
+            for (int cz = cz0; cz <= cz1; cz++)
+            {
+                if (cz < 1 || cz > mc)
+                    continue;
+                for (int cy = cy0; cy <= cy1; cy++)
+                {
+                    if (cy < 1 || cy > mc)
+                        continue;
+                    for (int cx = cx0; cx <= cx1; cx++)
+                    {
+                        if (cx < 1 || cx > mc)
+                            continue;
+                        acc += wgt * c.p[c.off + cx + cy * c.sy + cz * c.sz];
+                    }
+                }
+            }
+        }
+        phi.p[phi.off + i + j * phi.sy + k * phi.sz] += acc;
+    }
+}
+
+template <typename T> __device__ __forceinline__ T mg_h2(int n)
+{
+    return (T)((1.0 / (n - 1)) * (1.0 / (n - 1)));
+}
+
+// Smoothing sweeps of level l; sync() separates the colours.
+template <typename T, typename Sync>
+__device__ __forceinline__ void mg_smooth(const MgArgs<T> &A, int l, int sweeps, unsigned tid,
+                                          unsigned nthr, Sync sync)
+{
+    const T H2 = mg_h2<T>(A.phi[l].n);
+    for (int it = 0; it < sweeps; it++)
+        for (int color = 0; color < 2; color++)
+        {
+            mg_rb_half(A.phi[l], A.rho[l], color, H2, A.w, tid, nthr);
+            sync();
+        }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(MgArgs<T> A)
+{
+    cgm::grid_group grid = cgm::this_grid();
+    const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+    auto gsync = [&]() { grid.sync(); };
+    auto bsync = [&]() { __syncthreads(); };
+    for (int it = 0; it < A.iters; it++)
+    {
+        if (A.mixed)
+        {
+            // rf = (float)(rho + ooh2 (6 phi - sum)) on the fine interior (FP64), ef = 0
+            const Grid<double> &P = A.fphi, &R = A.frho;
+            const int n = P.n, m = n - 2;
+            const double ooh2 = (double)((n - 1) * (n - 1));
+            const unsigned um = (unsigned)m, tot = um * um * um, n3 = (unsigned)n * n * n;
+            float *rf = (float *)A.rho[0].p, *ef = (float *)A.phi[0].p;
+            for (unsigned t = gtid; t < n3; t += gn)
+                ef[t] = 0.0f;
+            for (unsigned t = gtid; t < tot; t += gn)
+            {
+                const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+                const long gp = P.off + i + j * P.sy + k * P.sz;
+                const long gr = R.off + i + j * R.sy + k * R.sz;
+                const double *p = P.p;
+                const double r = R.p[gr] + ooh2 * (6.0 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + P.sy] -
+                                                   p[gp - P.sy] - p[gp + P.sz] - p[gp - P.sz]);
+                rf[i + (long)j * n + (long)k * n * n] = (float)r;
+            }
+            grid.sync();
+        }
+        // levels above the small ones: grid-wide phases
+        for (int l = 0; l < A.nsmall; l++)
+        {
+            mg_smooth(A, l, A.n_pre, gtid, gn, gsync);
+            const int n = A.phi[l].n;
+            mg_restrict(A.phi[l], A.rho[l], A.phi[l + 1], A.rho[l + 1], (T)(double)((n - 1) * (n - 1)),
+                        A.scale, gtid, gn);
+            grid.sync();
+        }
+        // the small levels: a whole sub-cycle inside block 0
+        if (blockIdx.x == 0)
+        {
+            const unsigned bt = threadIdx.x, bn = blockDim.x;
+            for (int l = A.nsmall; l < A.nlev; l++)
+            {
+                mg_smooth(A, l, A.n_pre, bt, bn, bsync);
+                if (l == A.nlev - 1)
+                    mg_smooth(A, l, A.n_coarse, bt, bn, bsync);
+                else
+                {
+                    const int n = A.phi[l].n;
+                    mg_restrict(A.phi[l], A.rho[l], A.phi[l + 1], A.rho[l + 1],
+                                (T)(double)((n - 1) * (n - 1)), A.scale, bt, bn);
+                    __syncthreads();
+                }
+            }
+            for (int l = A.nlev - 1; l >= A.nsmall; l--)
+            {
+                if (l < A.nlev - 1)
+                {
+                    mg_prolong(A.phi[l], A.phi[l + 1], bt, bn);
+                    __syncthreads();
+                }
+                mg_smooth(A, l, A.n_post, bt, bn, bsync);
+            }
+        }
+        grid.sync();
+        for (int l = A.nsmall - 1; l >= 0; l--)
+        {
+            mg_prolong(A.phi[l], A.phi[l + 1], gtid, gn);
+            grid.sync();
+            mg_smooth(A, l, A.n_post, gtid, gn, gsync);
+        }
+        if (A.mixed)
+        {
+            const Grid<double> &P = A.fphi;
+            const int n = P.n, m = n - 2;
+            const unsigned um = (unsigned)m, tot = um * um * um;
+            const float *ef = (const float *)A.phi[0].p;
+            for (unsigned t = gtid; t < tot; t += gn)
+            {
+                const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+                P.p[P.off + i + j * P.sy + k * P.sz] += (double)ef[i + (long)j * n + (long)k * n * n];
+            }
+            grid.sync();
+        }
+    }
+}
+
+// True when the head solve runs as persistent launches (red-black Gauss-Seidel
+// V-cycles, no tiled sweeps); QZ_MG_LAUNCHES=1 selects one launch per phase.
+bool mg_persistent(const qz_sim *s)
+{
+    static const bool off = getenv("QZ_MG_LAUNCHES") != nullptr;
+    const qz_config &c = s->cfg;
+    return !off && c.smoother == 0 && c.gs_order == QZ_GS_REDBLACK && c.cycle == 0 &&
+           !s->fused_rb && (int)s->levels.size() <= MG_MAXLEV;
+}
+
+template <typename T> static int mg_launch(qz_sim *s, int iters)
+{
+    const qz_config &c = s->cfg;
+    MgArgs<T> A;
+    memset(&A, 0, sizeof A);
+    A.nlev = (int)s->levels.size();
+    A.nsmall = A.nlev - 1;
+    for (int l = 0; l < A.nlev; l++)
+    {
+        A.phi[l] = LevelViews<T>::phi(s, l);
+        A.rho[l] = LevelViews<T>::rho(s, l);
+        if (A.phi[l].n <= MG_SMALL_N && l < A.nsmall)
+            A.nsmall = l;
+    }
+    A.n_pre = c.n_pre;
+    A.n_post = c.n_post;
+    A.n_coarse = c.n_coarse;
+    A.w = (T)c.w_sor;
+    A.scale = (T)0.5; // red-black: half injection (see k_resid_restrict)
+    A.iters = iters;
+    A.mixed = std::is_same<T, float>::value ? 1 : 0;
+    A.fphi = s->fine_phi;
+    A.frho = s->fine_rho;
+    static int per_sm[2] = {0, 0};
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_mg_cycles<double>, MG_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_mg_cycles<float>, MG_THREADS, 0);
+    });
+    const int ps = per_sm[std::is_same<T, float>::value ? 1 : 0];
+    if (ps < 1)
+    {
+        set_error("multigrid kernel cannot be resident");
+        return QZ_FAILURE;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const int blocks = std::min(ps, 2) * sms;
+    // algorithmic bytes of one cycle, as the launch-per-phase path counts them
+    double bytes = 0.0;
+    for (int l = 0; l < A.nlev; l++)
+    {
+        const double m = A.phi[l].n - 2;
+        const int sweeps = c.n_pre + c.n_post + (l == A.nlev - 1 ? c.n_coarse : 0);
+        bytes += sizeof(T) * 3.0 * m * m * m * sweeps;
+        if (l < A.nlev - 1)
+        {
+            const double mc = A.phi[l + 1].n - 2;
+            bytes += sizeof(T) * 9.0 * mc * mc * mc + sizeof(T) * 2.125 * m * m * m;
+        }
+    }
+    if (A.mixed)
+    {
+        const double m = s->fine_phi.n - 2;
+        bytes += 40.0 * m * m * m;
+    }
+    void *args[] = {&A};
+    cudaEvent_t eb = nullptr, ee = nullptr;
+    if (s->prof)
+    {
+        eb = prof_event(s);
+        ee = prof_event(s);
+        cudaEventRecord(eb, s->stream);
+    }
+    if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_mg_cycles<T>, dim3(blocks),
+                                                dim3(MG_THREADS), args, 0, s->stream),
+                    "multigrid cycles"))
+        return QZ_FAILURE;
+    s->stats.kernel_launches++;
+    if (s->prof)
+    {
+        cudaEventRecord(ee, s->stream);
+        s->prof_pending.push_back({QZ_PROF_SMOOTH, bytes * iters, eb, ee});
+    }
+    return QZ_SUCCESS;
+}
+
+int mg_cycles(qz_sim *s, int iters)
+{
+    return s->cfg.precision == QZ_PREC_MIXED ? mg_launch<float>(s, iters)
+                                               : mg_launch<double>(s, iters);
+}
+
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters)
 {
     Grid<double> scr{}, alt{};
@@ -762,6 +1087,27 @@ int potential_head(qz_sim *s)
     bool check = false;
     const int every = c.check_every > 0 ? c.check_every : 1;
     const bool graphs = s->use_graphs && !s->prof;
+    if (mg_persistent(s))
+    {
+        // one cooperative launch per check block, then the convergence test
+        while (iter < c.max_iter && !check)
+        {
+            int k = every - (iter % every);
+            if (k > c.max_iter - iter)
+                k = c.max_iter - iter;
+            if (mg_cycles(s, k))
+                return QZ_FAILURE;
+            iter += k;
+            if (iter % every == 0)
+            {
+                if (launch_check(s, c.total_mass))
+                    return QZ_FAILURE;
+                if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
+                    return QZ_FAILURE;
+                check = s->h_flags[F_CONVERGED] != 0;
+            }
+        }
+    }
     while (iter < c.max_iter && !check)
     {
         if (graphs && iter % every == 0 && c.max_iter - iter >= every)
