@@ -73,7 +73,8 @@ typedef struct qz_config {
     int check_method;   /* check_poisson_error_method 0/1/2 */
     int precision;      /* QZ_PREC_FP64 or QZ_PREC_MIXED */
     int inner_cycles;   /* mixed precision: FP32 V-cycles per FP64 correction */
-    int force_stencil;  /* 0 = 3-point (only value supported) */
+    int force_stencil;  /* 0 = 3-point, 1 = 5-point where the cells exist
+                           (force_stencil, grid_acceleration.c:694-738) */
     int ref_ptcl;       /* refine a cell holding >= ref_ptcl particles (ref_criterion_ptcl) */
     int box_extra;      /* cells added to a child box on top of its smallest box
                            (min_box_extra_size_per_side_real) */

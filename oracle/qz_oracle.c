@@ -382,14 +382,27 @@ void qzo_grid_accel_head(const qzo_params *p, const double *pot, double *ax, dou
     long D = nc + 3, D2 = D * D;
     double H = 1.0 / (1 << p->L);
     double o2h = 1.0 / (2.0 * H);
+    /* grid_acceleration.c:78-197 (force_stencil 1): 5-point along an axis whose
+     * cells at -2 and +1 are inside the simulation, i.e. box coordinates
+     * 3..2^L-1 (the head box ring of status -5 is the only missing cell) */
+    double o12h = 1.0 / (12.0 * H), t3h = 2.0 / (3.0 * H);
     for (long k = 2; k <= nc; k++)
         for (long j = 2; j <= nc; j++)
             for (long i = 2; i <= nc; i++)
             {
                 long g = i + j * D + k * D2;
-                ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
-                ay[g] = o2h * (pot[g - D] - pot[g + D]);
-                az[g] = o2h * (pot[g - D2] - pot[g + D2]);
+                if (p->force_stencil == 1 && i >= 3 && i <= nc - 1)
+                    ax[g] = (pot[g - 1] - pot[g + 1]) * t3h - (pot[g - 2] - pot[g + 2]) * o12h;
+                else
+                    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
+                if (p->force_stencil == 1 && j >= 3 && j <= nc - 1)
+                    ay[g] = (pot[g - D] - pot[g + D]) * t3h - (pot[g - 2 * D] - pot[g + 2 * D]) * o12h;
+                else
+                    ay[g] = o2h * (pot[g - D] - pot[g + D]);
+                if (p->force_stencil == 1 && k >= 3 && k <= nc - 1)
+                    az[g] = (pot[g - D2] - pot[g + D2]) * t3h - (pot[g - 2 * D2] - pot[g + 2 * D2]) * o12h;
+                else
+                    az[g] = o2h * (pot[g - D2] - pot[g + D2]);
             }
 }
 

@@ -15,7 +15,9 @@
  *
  * Usage: qz_ref_driver IC.bin OUTDIR key=value ...
  *   keys: lmin, lmax, steps, dt, dump (comma list of steps, -1 = none),
- *         ref_ptcl, G, threads, solver (0 GS,1 Jacobi,2 CG), bdry
+ *         ref_ptcl, G, threads, solver (0 GS,1 Jacobi,2 CG), bdry, cg_head,
+ *         stencil (force_stencil), branch_cg_cells (nodes of more cells use
+ *         conjugate gradient, the others red-black SOR)
  * IC.bin: int64 N, then x[N] y[N] z[N] vx[N] vy[N] vz[N] m[N] (float64).
  * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles),
  *        OUTDIR/s<step>_nodes.txt (AMR node summary when lmax > lmin).
@@ -183,6 +185,8 @@ int main(int argc, char **argv)
     const char *out = argv[2];
     int L = 5, LMAX = -1, steps = 1, ref_ptcl = 9, threads = 1, solver = 0, bdry = 1;
     int cg_head = 0;
+    int stencil = 0;        /* force_stencil */
+    int branch_cg_cells = -1; /* branches_maximal_node_number_to_activate_conjugate_gradient */
     double dt = 1e-4, G = 1.0;
     const char *dump = NULL;
     for (int a = 3; a < argc; a++)
@@ -205,6 +209,8 @@ int main(int argc, char **argv)
         else if (!strcmp(key, "solver")) solver = atoi(v);
         else if (!strcmp(key, "bdry")) bdry = atoi(v);
         else if (!strcmp(key, "cg_head")) cg_head = atoi(v);
+        else if (!strcmp(key, "stencil")) stencil = atoi(v);
+        else if (!strcmp(key, "branch_cg_cells")) branch_cg_cells = atoi(v);
         else die("unknown key");
     }
     if (LMAX < 0)
@@ -235,6 +241,9 @@ int main(int argc, char **argv)
     bdry_cond_type = bdry;
     solverPreS = solverPostS = solverfinddphic = solver;
     head_pot_method = cg_head;
+    force_stencil = stencil;
+    if (branch_cg_cells >= 0)
+        branches_maximal_node_number_to_activate_conjugate_gradient = branch_cg_cells;
     NUMBER_OF_THEADS = threads;
     omp_set_num_threads(threads);
     bder_os_sim = 1 > n_exp ? 1 : n_exp;

@@ -1959,8 +1959,14 @@ __global__ void k_acc_bdry(int nlist, const int *__restrict__ list, const int *_
     az[g] = from_parent(P, paz, cx, cy, cz);
 }
 
-__global__ void k_acc_intr(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
-                           const AmrNode *__restrict__ nodes, const double *__restrict__ pot,
+// Interior points.  stencil 0: 3-point (grid_acceleration.c:384-393).  stencil
+// 1 (grid_acceleration.c:533-692): along x the 5-point difference where the node
+// cells at -2 and +1 exist (status > -4); along y and z the reference keeps the
+// 3-point difference without periodic boundaries (its 5-point test there never
+// sets the flag that selects the 5-point formula, :606-613, :636-643).
+__global__ void k_acc_intr(int nlist, int stencil, const int *__restrict__ list,
+                           const int *__restrict__ lnode, const AmrNode *__restrict__ nodes,
+                           const int *__restrict__ box, const double *__restrict__ pot,
                            double *__restrict__ ax, double *__restrict__ ay,
                            double *__restrict__ az)
 {
@@ -1972,7 +1978,22 @@ __global__ void k_acc_intr(int nlist, const int *__restrict__ list, const int *_
     const double H = 1.0 / (1 << N.lv);
     const double o2h = 1.0 / (2.0 * H);
     const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
-    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
+    bool five = false;
+    if (stencil == 1)
+    {
+        int gx, gy, gz;
+        grid_coords(N, g, &gx, &gy, &gz);
+        const long b = N.box_off + gx + (long)gy * N.rd[0] + (long)gz * N.rd[0] * N.rd[1];
+        five = box[b - 2] > -4 && box[b + 1] > -4;
+    }
+    if (five)
+    {
+        const double o12h = 1.0 / (12.0 * H);
+        const double t3h = 2.0 / (3.0 * H);
+        ax[g] = (pot[g - 1] - pot[g + 1]) * t3h - (pot[g - 2] - pot[g + 2]) * o12h;
+    }
+    else
+        ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
     ay[g] = o2h * (pot[g - sy] - pot[g + sy]);
     az[g] = o2h * (pot[g - sz] - pot[g + sz]);
 }
@@ -2006,9 +2027,10 @@ int amr_grid_accel(qz_sim *s)
                    dim3(blocks_for(L.bdry_total, 256)), dim3(256), L.bdry_total, L.bdry.p,
                    L.bdry_node.p, L.nodes.p, P.nodes.p, P.ax, P.ay, P.az, L.ax, L.ay, L.az);
         if (L.intr_total > 0)
-            launch(s, QZ_PROF_GRADIENT, 32.0 * L.intr_total, k_acc_intr,
-                   dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
-                   L.intr_node.p, L.nodes.p, L.pot, L.ax, L.ay, L.az);
+            launch(s, QZ_PROF_GRADIENT, (s->cfg.force_stencil ? 48.0 : 32.0) * L.intr_total,
+                   k_acc_intr, dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total,
+                   s->cfg.force_stencil, L.intr.p, L.intr_node.p, L.nodes.p, L.box.p, L.pot,
+                   L.ax, L.ay, L.az);
     }
     return check_cuda(cudaGetLastError(), "level gradient") ? QZ_SUCCESS : QZ_FAILURE;
 }

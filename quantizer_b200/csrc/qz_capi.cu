@@ -365,7 +365,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         set_error("qz_create: bdry=%d not supported (1 reflexive only)", cfg->bdry);
         return QZ_FAILURE;
     }
-    if (cfg->force_stencil != 0 || cfg->smoother < 0 || cfg->smoother > 1 || cfg->cycle < 0 ||
+    if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 1 || cfg->cycle < 0 ||
         cfg->cycle > 2 || n_capacity > (1L << 30))
     {
         set_error("qz_create: unsupported configuration");

@@ -269,9 +269,13 @@ int deposit_head(qz_sim *s)
 }
 
 // ---- grid acceleration (3-point) ----------------------------------------------
-__global__ void k_grid_accel3(int L, long D, const double *__restrict__ pot,
-                              double *__restrict__ ax, double *__restrict__ ay,
-                              double *__restrict__ az)
+// a = -grad phi on the head interior.  stencil 0: 3-point
+// (grid_acceleration.c:36-76).  stencil 1 (grid_acceleration.c:78-197): the
+// 5-point difference along an axis whose cells at -2 and +1 are inside the
+// simulation (head box coordinates 3..2^L-1), else the 3-point one.
+__global__ void k_grid_accel_head(int L, long D, int stencil, const double *__restrict__ pot,
+                                  double *__restrict__ ax, double *__restrict__ ay,
+                                  double *__restrict__ az)
 {
     const int m = (1 << L) - 1; // interior points per axis: box coords 2..2^L
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -282,9 +286,25 @@ __global__ void k_grid_accel3(int L, long D, const double *__restrict__ pot,
     long g = i + j * D + k * D2;
     const double H = 1.0 / (1 << L);
     const double o2h = 1.0 / (2.0 * H);
-    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
-    ay[g] = o2h * (pot[g - D] - pot[g + D]);
-    az[g] = o2h * (pot[g - D2] - pot[g + D2]);
+    if (stencil == 0)
+    {
+        ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
+        ay[g] = o2h * (pot[g - D] - pot[g + D]);
+        az[g] = o2h * (pot[g - D2] - pot[g + D2]);
+        return;
+    }
+    const double o12h = 1.0 / (12.0 * H);
+    const double t3h = 2.0 / (3.0 * H);
+    const int hi = (1 << L) - 1;
+    ax[g] = (i >= 3 && i <= hi)
+                ? (pot[g - 1] - pot[g + 1]) * t3h - (pot[g - 2] - pot[g + 2]) * o12h
+                : o2h * (pot[g - 1] - pot[g + 1]);
+    ay[g] = (j >= 3 && j <= hi)
+                ? (pot[g - D] - pot[g + D]) * t3h - (pot[g - 2 * D] - pot[g + 2 * D]) * o12h
+                : o2h * (pot[g - D] - pot[g + D]);
+    az[g] = (k >= 3 && k <= hi)
+                ? (pot[g - D2] - pot[g + D2]) * t3h - (pot[g - 2 * D2] - pot[g + 2 * D2]) * o12h
+                : o2h * (pot[g - D2] - pot[g + D2]);
 }
 
 int grid_accel_head(qz_sim *s)
@@ -292,7 +312,9 @@ int grid_accel_head(qz_sim *s)
     long m = (1L << s->L) - 1;
     if (m <= 0)
         return QZ_SUCCESS;
-    launch(s, QZ_PROF_GRADIENT, 32.0 * m * m * m, k_grid_accel3, dim3(blocks_for(m * m * m, 256)), dim3(256), s->L, s->D, s->pot, s->gax, s->gay, s->gaz);
+    const double bytes = (s->cfg.force_stencil ? 56.0 : 32.0) * m * m * m;
+    launch(s, QZ_PROF_GRADIENT, bytes, k_grid_accel_head, dim3(blocks_for(m * m * m, 256)), dim3(256),
+           s->L, s->D, s->cfg.force_stencil, s->pot, s->gax, s->gay, s->gaz);
     return check_cuda(cudaGetLastError(), "grid accel") ? QZ_SUCCESS : QZ_FAILURE;
 }
 

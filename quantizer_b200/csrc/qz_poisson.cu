@@ -545,6 +545,7 @@ namespace cgm = cooperative_groups;
 constexpr int MG_MAXLEV = 12;
 constexpr int MG_SMALL_N = 17;
 constexpr int MG_THREADS = 512;
+constexpr size_t MG_SMEM_MAX = 100 * 1024; // two resident blocks a SM
 
 template <typename T> struct MgArgs {
     Grid<T> phi[MG_MAXLEV], rho[MG_MAXLEV];
@@ -555,8 +556,11 @@ template <typename T> struct MgArgs {
     int iters; // cycles (mixed: defect-correction iterations) in this launch
     int mixed;
     Grid<double> fphi, frho; // FP64 fine grid (mixed form): phi[0] / rho[0] are ef / rf
+    int smem;                // the small levels live in block 0's shared memory
+    int soff[MG_MAXLEV];     // their offsets there (phi, then rho), in elements
 };
 
+// One colour of a red-black sweep over work items t = tid, tid + nthr, ...
 template <typename T>
 __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rho, int color,
                                            T H2, T w, unsigned tid, unsigned nthr)
@@ -565,6 +569,7 @@ __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rh
     const unsigned half = (unsigned)(m + 1) / 2;
     const unsigned total = half * (unsigned)m * (unsigned)m;
     const T one_sixth = (T)(1.0 / 6.0);
+#pragma unroll 4
     for (unsigned t = tid; t < total; t += nthr)
     {
         const unsigned ti = t % half, r = t / half;
@@ -655,22 +660,54 @@ template <typename T> __device__ __forceinline__ T mg_h2(int n)
 
 // Smoothing sweeps of level l; sync() separates the colours.
 template <typename T, typename Sync>
-__device__ __forceinline__ void mg_smooth(const MgArgs<T> &A, int l, int sweeps, unsigned tid,
-                                          unsigned nthr, Sync sync)
+__device__ __forceinline__ void mg_smooth_g(const Grid<T> &phi, const Grid<T> &rho, T w,
+                                            int sweeps, unsigned tid, unsigned nthr, Sync sync)
 {
-    const T H2 = mg_h2<T>(A.phi[l].n);
+    const T H2 = mg_h2<T>(phi.n);
     for (int it = 0; it < sweeps; it++)
         for (int color = 0; color < 2; color++)
         {
-            mg_rb_half(A.phi[l], A.rho[l], color, H2, A.w, tid, nthr);
+            mg_rb_half(phi, rho, color, H2, w, tid, nthr);
             sync();
         }
 }
 
+template <typename T, typename Sync>
+__device__ __forceinline__ void mg_smooth(const MgArgs<T> &A, int l, int sweeps, unsigned tid,
+                                          unsigned nthr, Sync sync)
+{
+    mg_smooth_g(A.phi[l], A.rho[l], A.w, sweeps, tid, nthr, sync);
+}
+
+template <typename T> __device__ __forceinline__ Grid<T> mg_dense(T *p, int n)
+{
+    Grid<T> g;
+    g.p = p;
+    g.off = 0;
+    g.sy = n;
+    g.sz = (long)n * n;
+    g.n = n;
+    return g;
+}
+
+// Copies all points of grid a into grid b (same size), block-wide.
 template <typename T>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(MgArgs<T> A)
+__device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsigned tid,
+                                        unsigned nthr)
+{
+    const unsigned n = (unsigned)a.n, n3 = n * n * n;
+    for (unsigned t = tid; t < n3; t += nthr)
+    {
+        const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / (n * n));
+        b.p[b.off + i + j * b.sy + k * b.sz] = a.p[a.off + i + j * a.sy + k * a.sz];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant__ MgArgs<T> A)
 {
     cgm::grid_group grid = cgm::this_grid();
+    extern __shared__ __align__(16) unsigned char mg_dyn[];
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
     auto gsync = [&]() { grid.sync(); };
     auto bsync = [&]() { __syncthreads(); };
@@ -707,20 +744,36 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(MgArgs<T> A)
                         A.scale, gtid, gn);
             grid.sync();
         }
-        // the small levels: a whole sub-cycle inside block 0
+        // the small levels: a whole sub-cycle inside block 0, in its shared memory
+        // when they fit (the first small level is copied in and its correction out)
         if (blockIdx.x == 0)
         {
             const unsigned bt = threadIdx.x, bn = blockDim.x;
+            T *sm = reinterpret_cast<T *>(mg_dyn);
+            auto P = [&](int l) {
+                return A.smem ? mg_dense(sm + A.soff[l], A.phi[l].n) : A.phi[l];
+            };
+            auto R = [&](int l) {
+                return A.smem ? mg_dense(sm + A.soff[l] + A.phi[l].n * A.phi[l].n * A.phi[l].n,
+                                         A.phi[l].n)
+                              : A.rho[l];
+            };
+            if (A.smem)
+            {
+                mg_copy(A.phi[A.nsmall], P(A.nsmall), bt, bn);
+                mg_copy(A.rho[A.nsmall], R(A.nsmall), bt, bn);
+                __syncthreads();
+            }
             for (int l = A.nsmall; l < A.nlev; l++)
             {
-                mg_smooth(A, l, A.n_pre, bt, bn, bsync);
+                mg_smooth_g(P(l), R(l), A.w, A.n_pre, bt, bn, bsync);
                 if (l == A.nlev - 1)
-                    mg_smooth(A, l, A.n_coarse, bt, bn, bsync);
+                    mg_smooth_g(P(l), R(l), A.w, A.n_coarse, bt, bn, bsync);
                 else
                 {
                     const int n = A.phi[l].n;
-                    mg_restrict(A.phi[l], A.rho[l], A.phi[l + 1], A.rho[l + 1],
-                                (T)(double)((n - 1) * (n - 1)), A.scale, bt, bn);
+                    mg_restrict(P(l), R(l), P(l + 1), R(l + 1), (T)(double)((n - 1) * (n - 1)),
+                                A.scale, bt, bn);
                     __syncthreads();
                 }
             }
@@ -728,11 +781,13 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(MgArgs<T> A)
             {
                 if (l < A.nlev - 1)
                 {
-                    mg_prolong(A.phi[l], A.phi[l + 1], bt, bn);
+                    mg_prolong(P(l), P(l + 1), bt, bn);
                     __syncthreads();
                 }
-                mg_smooth(A, l, A.n_post, bt, bn, bsync);
+                mg_smooth_g(P(l), R(l), A.w, A.n_post, bt, bn, bsync);
             }
+            if (A.smem)
+                mg_copy(P(A.nsmall), A.phi[A.nsmall], bt, bn);
         }
         grid.sync();
         for (int l = A.nsmall - 1; l >= 0; l--)
@@ -790,11 +845,29 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     A.mixed = std::is_same<T, float>::value ? 1 : 0;
     A.fphi = s->fine_phi;
     A.frho = s->fine_rho;
+    // shared memory for the small levels (phi and rho of each)
+    long elems = 0;
+    for (int l = A.nsmall; l < A.nlev; l++)
+    {
+        A.soff[l] = (int)elems;
+        const long n = A.phi[l].n;
+        elems += 2 * n * n * n;
+    }
+    size_t smem = elems * sizeof(T);
+    A.smem = smem <= MG_SMEM_MAX ? 1 : 0;
+    if (!A.smem)
+        smem = 0;
     static int per_sm[2] = {0, 0};
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_mg_cycles<double>, MG_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_mg_cycles<float>, MG_THREADS, 0);
+        cudaFuncSetAttribute((const void *)k_mg_cycles<double>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_MAX);
+        cudaFuncSetAttribute((const void *)k_mg_cycles<float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_MAX);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_mg_cycles<double>, MG_THREADS,
+                                                      MG_SMEM_MAX);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_mg_cycles<float>, MG_THREADS,
+                                                      MG_SMEM_MAX);
     });
     const int ps = per_sm[std::is_same<T, float>::value ? 1 : 0];
     if (ps < 1)
@@ -832,7 +905,7 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
         cudaEventRecord(eb, s->stream);
     }
     if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_mg_cycles<T>, dim3(blocks),
-                                                dim3(MG_THREADS), args, 0, s->stream),
+                                                dim3(MG_THREADS), args, smem, s->stream),
                     "multigrid cycles"))
         return QZ_FAILURE;
     s->stats.kernel_launches++;

@@ -36,3 +36,8 @@ def jacobi_golden():
 @pytest.fixture(scope="session")
 def arrays_golden():
     return golden("arrays.npz")
+
+
+@pytest.fixture(scope="session")
+def stencil5_golden():
+    return golden("head_L4_stencil5.npz")

@@ -10,12 +10,14 @@ sources (oracle/Makefile, target ``ref``):
   head box index of every particle (ptcl_idx_to_box_idx).
 * ``head_L3_jacobi.npz`` -- the same with the Jacobi smoother (solver 1), head
   8^3, 2 steps.
+* ``head_L4_stencil5.npz`` -- the head_L4 case with the 5-point force stencil
+  (force_stencil = 1).
 * ``arrays.npz`` -- direct calls into oracle/_ref/libqzref.so of the
   reference's gauss_saidel, jacobi (odd sweep count) and multigrid (V, F and W
   cycles) on seeded random arrays.
 
 Run in a container that has the reference source tree:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture-name ...]   (default: all)
 """
 from __future__ import annotations
 
@@ -100,11 +102,19 @@ def arrays_case() -> None:
 
 def main() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    want = set(sys.argv[1:])
     ic = ics.plummer(1000, a=0.05, seed=11)
     dt = 1e-3 * ics.crossing_time(0.05)
-    run_case("head_L4_plummer1000.npz", ic, steps=3, dt=dt, lmin=4)
-    run_case("head_L3_jacobi.npz", ic, steps=2, dt=dt, lmin=3, solver=1)
-    arrays_case()
+    cases = [
+        ("head_L4_plummer1000.npz", dict(steps=3, lmin=4)),
+        ("head_L3_jacobi.npz", dict(steps=2, lmin=3, solver=1)),
+        ("head_L4_stencil5.npz", dict(steps=3, lmin=4, stencil=1)),
+    ]
+    for name, kw in cases:
+        if not want or name in want:
+            run_case(name, ic, dt=dt, **kw)
+    if not want or "arrays.npz" in want:
+        arrays_case()
 
 
 if __name__ == "__main__":

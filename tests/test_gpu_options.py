@@ -1,0 +1,75 @@
+"""GPU parity of the reference's optional solver and stencil settings against
+the compiled reference (oracle/_ref/qz_ref_driver) and its fixtures.
+
+* force_stencil 1 (grid_acceleration.c:78-197, 396-692): head-only run in the
+  lexicographic Gauss-Seidel mode (the reference's arithmetic order) against
+  the fixture, tolerances of the 3-point pipeline test; a refinement run
+  against the driver at step 0 and after 3 steps, tolerances of the
+  refinement tests (node accelerations 1e-6 of the node's max, particle
+  accelerations 1e-6, positions 1e-10 box units).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from quantizer_b200 import core, ics
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _ic(g):
+    return {k: g["ic_" + k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+
+
+def test_five_point_stencil_head(stencil5_golden):
+    g = stencil5_golden
+    steps, dt = int(g["meta"][1]), float(g["meta"][2])
+    with core.Simulation(_ic(g), 4, gs_order=core.QZ_GS_LEX, force_stencil=1) as sim:
+        sim.init_forces()
+        p0 = sim.particles()
+        g0 = {k: sim.field(k) for k in ("ax", "ay", "az")}
+        sim.step(dt, steps)
+        p = sim.particles()
+    for k in ("ax", "ay", "az"):
+        assert _rel(g0[k], g[f"s0_g{k}"]) < 1e-11, k
+        assert _rel(p0[k], g[f"s0_{k}"]) < 1e-11, k
+        assert _rel(p[k], g[f"s{steps}_{k}"]) < 1e-11, k
+    for k in ("x", "y", "z"):
+        assert np.abs(p[k] - g[f"s{steps}_{k}"]).max() < 1e-13
+
+
+def test_five_point_stencil_refinement(tmp_path):
+    n, a, lmin, lmax, rp, seed = 20000, 0.05, 5, 8, 9, 3
+    ic = ics.plummer(n, a=a, seed=seed)
+    dt = 1e-3 * ics.crossing_time(a)
+    steps = 3
+    icp = os.path.join(str(tmp_path), "ic.bin")
+    ics.write_ic(icp, ic)
+    O.run_reference(icp, str(tmp_path), steps=steps, dt=dt, dump=f"0,{steps}", lmin=lmin,
+                    lmax=lmax, ref_ptcl=rp, stencil=1)
+    ref = O.read_nodes(str(tmp_path), 0)
+    with core.Simulation(ic, lmin, lmax=lmax, ref_ptcl=rp, force_stencil=1) as sim:
+        sim.init_forces()
+        p0 = sim.particles()
+        for nd in ref:
+            L, i = nd["level"], nd["idx"]
+            if L == 0:
+                continue
+            pts = sim.node_list(L, i, "intr")
+            for f in ("ax", "ay", "az"):
+                mine = sim.node_field(L, i, f)[pts]
+                theirs = O.node_dump(str(tmp_path), 0, L, i, f)[pts]
+                assert _rel(mine, theirs) < 1e-6, (L, i, f)
+        sim.step(dt, steps)
+        p = sim.particles()
+    for k in ("ax", "ay", "az"):
+        assert _rel(p0[k], O.read_dump(str(tmp_path), 0, k)) < 1e-6
+        assert _rel(p[k], O.read_dump(str(tmp_path), steps, k)) < 1e-6
+    for k in ("x", "y", "z"):
+        assert np.abs(p[k] - O.read_dump(str(tmp_path), steps, k)).max() < 1e-10

@@ -43,6 +43,11 @@ def test_head_pipeline_jacobi_bit_exact(jacobi_golden):
     _assert_exact(jacobi_golden, steps, s0, s1)
 
 
+def test_head_pipeline_five_point_stencil_bit_exact(stencil5_golden):
+    steps, s0, s1 = _run(stencil5_golden, 4, force_stencil=1)
+    _assert_exact(stencil5_golden, steps, s0, s1)
+
+
 def test_box_index_bit_exact(head_golden):
     lib = O.load()
     L = 4
