@@ -62,7 +62,8 @@ typedef struct qz_config {
     double G;           /* gravitational constant (_G_) */
     double total_mass;  /* GL_total_mass_initial: analytic boundary and mean density */
     int bdry;           /* 0 periodic, 1 reflexive (bdry_cond_type) */
-    int smoother;       /* 0 Gauss-Seidel, 1 Jacobi (solverPreS/PostS/finddphic) */
+    int smoother;       /* 0 Gauss-Seidel, 1 Jacobi, 2 conjugate gradient
+                           (solverPreS/PostS/finddphic) */
     int gs_order;       /* QZ_GS_REDBLACK or QZ_GS_LEX */
     int cycle;          /* 0 V, 1 F, 2 W (multigrid_cycle) */
     int n_pre, n_post, n_coarse; /* _NiterPreS_, _NiterPostS_, _Niterfinddphic_ */
@@ -78,6 +79,14 @@ typedef struct qz_config {
     int ref_ptcl;       /* refine a cell holding >= ref_ptcl particles (ref_criterion_ptcl) */
     int box_extra;      /* cells added to a child box on top of its smallest box
                            (min_box_extra_size_per_side_real) */
+    /* refinement levels: a node of more than branch_cg_cells cells is solved by
+     * conjugate gradient, the others by red-black SOR of branch_sor_sweeps
+     * sweeps per check iteration with weight w_sor_branch
+     * (branches_maximal_node_number_to_activate_conjugate_gradient,
+     * _Iter_branches_solver_, _w_SOR_; potential_branches.c:460-512) */
+    int branch_cg_cells;
+    int branch_sor_sweeps;
+    double w_sor_branch;
 } qz_config;
 
 typedef struct qz_stats {
@@ -191,6 +200,10 @@ QZ_API int qz_profile_read(qz_sim *sim, int category, long long *launches, doubl
 QZ_API int qz_gauss_saidel(double *phi, const double *rho, int gridsize, int iter_max, double w,
                     int gs_order);
 QZ_API int qz_jacobi(double *phi, const double *rho, int gridsize, int iter_max, double w);
+/* conjugate_gradient_multigrid (force_methods/conjugate_gradient_multigrid.c:29-176):
+ * iters conjugate-gradient iterations as a smoother, early exit below a
+ * residual ratio of 1e-16; FP64 sums in block order (tolerance parity). */
+QZ_API int qz_conjugate_gradient_multigrid(double *phi, const double *rho, int gridsize, int iters);
 QZ_API int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, int gridsize,
                  int type_multigrid);
 

@@ -61,6 +61,7 @@ def load():
         lib.qzo_deposit_head.argtypes = [C.POINTER(Params), C.c_long, _P, _P, _P, _P, _P]
         lib.qzo_gauss_saidel.argtypes = [_P, _P, C.c_int, C.c_int, C.c_double]
         lib.qzo_jacobi.argtypes = [_P, _P, C.c_int, C.c_int, C.c_double]
+        lib.qzo_cg_smooth.argtypes = [_P, _P, C.c_int, C.c_int]
         lib.qzo_multigrid.argtypes = [C.POINTER(Params), _P, _P, C.c_int, C.c_int]
         lib.qzo_poisson_check_head.argtypes = [C.POINTER(Params), _P, _P, _P, C.c_double]
         lib.qzo_potential_head.argtypes = [C.POINTER(Params), _P, _P, _P, C.c_double]

@@ -170,13 +170,99 @@ void qzo_jacobi(double *phi, const double *rho, int n, int iters, double w)
     free(cp);
 }
 
+/* conjugate_gradient_multigrid.c:29-176: r = rho + (6 phi - sum)/H^2 on the
+ * interior, p = r, then up to min(iters, interior points) CG iterations with
+ * lexicographic sums, leaving when rs_new / rs_old < 1e-16. */
+void qzo_cg_smooth(double *phi, const double *rho, int n, int iters)
+{
+    double H = 1.0 / (n - 1);
+    double oh2 = 1.0 / (H * H);
+    long n2 = (long)n * n, n3 = n2 * n;
+    double *r = calloc(n3, sizeof(double)), *p = malloc(n3 * sizeof(double)),
+           *ap = malloc(n3 * sizeof(double));
+    for (long k = 1; k < n - 1; k++)
+        for (long j = 1; j < n - 1; j++)
+            for (long i = 1; i < n - 1; i++)
+            {
+                long g = i + j * n + k * n2;
+                r[g] = rho[g] + oh2 * (6.0 * phi[g] - phi[g + 1] - phi[g - 1] - phi[g + n] -
+                                       phi[g - n] - phi[g + n2] - phi[g - n2]);
+            }
+    memcpy(p, r, n3 * sizeof(double));
+    double rsold = 0.0;
+    for (long k = 1; k < n - 1; k++)
+        for (long j = 1; j < n - 1; j++)
+            for (long i = 1; i < n - 1; i++)
+            {
+                long g = i + j * n + k * n2;
+                rsold += r[g] * r[g];
+            }
+    long m3 = (long)(n - 2) * (n - 2) * (n - 2);
+    long cycle = iters < m3 ? iters : m3;
+    for (long it = 0; it < cycle; it++)
+    {
+        double dot = 0.0, rsnew = 0.0;
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    ap[g] = -oh2 * (6.0 * p[g] - p[g + 1] - p[g - 1] - p[g + n] - p[g - n] -
+                                    p[g + n2] - p[g - n2]);
+                }
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    dot += p[g] * ap[g];
+                }
+        double alpha = rsold / dot;
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    phi[g] += alpha * p[g];
+                }
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    r[g] -= alpha * ap[g];
+                }
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    rsnew += r[g] * r[g];
+                }
+        if (rsnew / rsold < 1.0e-16)
+            break;
+        for (long k = 1; k < n - 1; k++)
+            for (long j = 1; j < n - 1; j++)
+                for (long i = 1; i < n - 1; i++)
+                {
+                    long g = i + j * n + k * n2;
+                    p[g] = r[g] + rsnew / rsold * p[g];
+                }
+        rsold = rsnew;
+    }
+    free(r);
+    free(p);
+    free(ap);
+}
+
 static void smooth(const qzo_params *p, double *phi, const double *rho, int n, int iters)
 {
     if (p->solver == 0)
         qzo_gauss_saidel(phi, rho, n, iters, p->w_sor);
     else if (p->solver == 1)
         qzo_jacobi(phi, rho, n, iters, p->w_sor);
-    /* solver 2 (CG smoother) is not restated */
+    else if (p->solver == 2)
+        qzo_cg_smooth(phi, rho, n, iters);
 }
 
 /* force_methods/multigrid.c:106-229: one V/F/W cycle. */

@@ -50,6 +50,8 @@ void qzo_deposit_head(const qzo_params *p, long n, const double *x, const double
 void qzo_gauss_saidel(double *phi, const double *rho, int gridsize, int iters, double w);
 /* force_methods/jacobi.c:29-82 */
 void qzo_jacobi(double *phi, const double *rho, int gridsize, int iters, double w);
+/* conjugate_gradient_multigrid.c:29-176 */
+void qzo_cg_smooth(double *phi, const double *rho, int gridsize, int iters);
 /* force_methods/multigrid.c:106-229 */
 void qzo_multigrid(const qzo_params *p, double *phi, const double *rho, int gridsize, int type);
 /* poisson_error.c:36-133 for the head node; returns 1 when converged. */

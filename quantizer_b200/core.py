@@ -37,7 +37,8 @@ class Config(C.Structure):
         ("tol", C.c_double), ("tol2", C.c_double), ("check_every", C.c_int),
         ("max_iter", C.c_int), ("check_method", C.c_int), ("precision", C.c_int),
         ("inner_cycles", C.c_int), ("force_stencil", C.c_int), ("ref_ptcl", C.c_int),
-        ("box_extra", C.c_int),
+        ("box_extra", C.c_int), ("branch_cg_cells", C.c_int), ("branch_sor_sweeps", C.c_int),
+        ("w_sor_branch", C.c_double),
     ]
 
 
@@ -94,6 +95,7 @@ def load() -> C.CDLL:
         "qz_gauss_saidel": ([_P, _P, C.c_int, C.c_int, C.c_double, C.c_int], C.c_int),
         "qz_jacobi": ([_P, _P, C.c_int, C.c_int, C.c_double], C.c_int),
         "qz_multigrid": ([C.POINTER(Config), _P, _P, C.c_int, C.c_int], C.c_int),
+        "qz_conjugate_gradient_multigrid": ([_P, _P, C.c_int, C.c_int], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -310,6 +312,15 @@ def jacobi(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0) -> np.n
     out = _f64(phi).copy()
     r = _f64(rho)
     _check(load().qz_jacobi(_p(out), _p(r), n, iters, w))
+    return out
+
+
+def conjugate_gradient_multigrid(phi: np.ndarray, rho: np.ndarray, iters: int) -> np.ndarray:
+    """conjugate_gradient_multigrid.c:29-176 on a gridsize^3 array (returns a copy)."""
+    n = round(phi.size ** (1 / 3))
+    out = _f64(phi).copy()
+    r = _f64(rho)
+    _check(load().qz_conjugate_gradient_multigrid(_p(out), _p(r), n, iters))
     return out
 
 

@@ -599,7 +599,7 @@ static void free_level(const MemCtx &m, AmrLevel &L)
 {
     DBuf<int> *ib[] = {&L.box, &L.cnt, &L.pos_of_box, &L.cell_seg, &L.cell_box, &L.cell_xyz,
                        &L.cell_node, &L.intr, &L.bdry, &L.simb, &L.intr_node, &L.bdry_node,
-                       &L.simb_node, &L.nint, &L.mass_range};
+                       &L.simb_node, &L.nint, &L.mass_range, &L.sor};
     for (auto *b : ib)
         b->release(m);
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
@@ -1730,6 +1730,162 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
         atomicOr(&A.status[1], 1);
 }
 
+// Red-black SOR on the nodes of a level with at most branch_cg_cells cells
+// (potential_branches.c:35-91, 334-399, 471-512), one block per node: an
+// iteration is `sweeps` red-black sweeps over the node's interior list (red:
+// even sum of the level coordinates), every `every` iterations the test of
+// poisson_error.c:290-347 (the ratio test, then the residual by
+// check_method 0/1/2); a failed test copies pot to pot_old over the node grid.
+// Reaching max_iter is a failure, as there.  The reference evaluates 1/6 in
+// long double (1.0L / 6.0L) before rounding the update to double; here 1/6 is a
+// double, so updates agree to rounding.
+struct SorArgs {
+    const int *sor_nodes; // node index of each block
+    const AmrNode *nodes;
+    const int *intr;
+    const double *d;
+    double *pot, *pot_old;
+    int sweeps, every, max_iter, method;
+    double w, tol, tol2, G;
+    int *iters; // per block: iterations run; negative if not converged
+};
+
+__device__ __forceinline__ bool sor_red(const AmrNode &N, long g)
+{
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    return (((gx + N.ts[0]) + (gy + N.ts[1]) + (gz + N.ts[2])) & 1) == 0;
+}
+
+__global__ void __launch_bounds__(256) k_sor_nodes(SorArgs A)
+{
+    __shared__ double sh[32];
+    const int q = A.sor_nodes[blockIdx.x];
+    const AmrNode N = A.nodes[q];
+    const double H = 1.0 / (1 << N.lv);
+    const double H2 = H * H, oh2 = 1.0 / (H * H);
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    const long ngrid = sz * (N.rd[2] + 1);
+    const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+    const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
+    const double one_sixth = 1.0 / 6.0;
+    const int *list = A.intr + N.intr_off;
+    double *pot = A.pot;
+    int iter = 0;
+    bool check = false;
+    while (iter < A.max_iter && !check)
+    {
+        iter++;
+        for (int sw = 0; sw < A.sweeps; sw++)
+            for (int color = 0; color < 2; color++)
+            {
+                for (int e = threadIdx.x; e < N.nintr; e += blockDim.x)
+                {
+                    const long g = list[e];
+                    if (sor_red(N, g) != (color == 0))
+                        continue;
+                    double aux = one_sixth * (-H2 * A.d[g] + pot[g + 1] + pot[g - 1] + pot[g + sy] +
+                                              pot[g - sy] + pot[g + sz] + pot[g - sz]);
+                    pot[g] = A.w * aux + (1.0 - A.w) * pot[g];
+                }
+                __syncthreads();
+            }
+        if (iter % A.every == 0)
+        {
+            int ratio_fail = 0, resid_fail = 0;
+            double acc = 0.0;
+            for (int e = threadIdx.x; e < N.nintr; e += blockDim.x)
+            {
+                const long g = list[e];
+                const double a = pot[g] / A.pot_old[g];
+                if ((tm > a) || (tp < a))
+                    ratio_fail = 1;
+                const double diff = A.d[g] + oh2 * (6.0 * pot[g] - pot[g + 1] - pot[g - 1] -
+                                                    pot[g + sy] - pot[g - sy] - pot[g + sz] -
+                                                    pot[g - sz]);
+                if (A.method == 1)
+                {
+                    if (fabs(diff) / rm >= A.tol)
+                        resid_fail = 1;
+                }
+                else
+                    acc += diff * diff;
+            }
+            ratio_fail = __syncthreads_or(ratio_fail);
+            resid_fail = __syncthreads_or(resid_fail);
+            const double tot = block_sum_d(acc, sh);
+            int ok = 0;
+            if (threadIdx.x == 0)
+            {
+                if (A.method == 1)
+                    ok = !resid_fail;
+                else
+                {
+                    double err = sqrt(tot / N.nintr) / rm;
+                    if (A.method == 2)
+                        err = err / (cbrt((double)N.nintr) * cbrt((double)N.nintr));
+                    ok = err < A.tol;
+                }
+                ok = ok && !ratio_fail;
+            }
+            check = __syncthreads_or(ok) != 0;
+            if (!check)
+            {
+                for (long t = threadIdx.x; t < ngrid; t += blockDim.x)
+                    A.pot_old[N.grid_off + t] = pot[N.grid_off + t];
+                __syncthreads();
+            }
+        }
+    }
+    if (threadIdx.x == 0)
+        A.iters[blockIdx.x] = (check && iter < A.max_iter) ? iter : -iter;
+}
+
+static int sor_level(qz_sim *s, AmrLevel &L, int level_index, const std::vector<int> &sor_nodes)
+{
+    const qz_config &c = s->cfg;
+    const int ns = (int)sor_nodes.size();
+    if (!L.sor.ensure(s->mem, 2L * ns))
+    {
+        set_error("sor buffers");
+        return QZ_FAILURE;
+    }
+    if (!check_cuda(cudaMemcpyAsync(L.sor.p, sor_nodes.data(), ns * sizeof(int),
+                                    cudaMemcpyHostToDevice, s->stream), "sor nodes"))
+        return QZ_FAILURE;
+    SorArgs A;
+    A.sor_nodes = L.sor.p;
+    A.nodes = L.nodes.p;
+    A.intr = L.intr.p;
+    A.d = L.d;
+    A.pot = L.pot;
+    A.pot_old = L.pot_old;
+    A.sweeps = c.branch_sor_sweeps > 0 ? c.branch_sor_sweeps : 1;
+    A.every = c.check_every > 0 ? c.check_every : 1;
+    A.max_iter = c.max_iter;
+    A.method = c.check_method;
+    A.w = c.w_sor_branch;
+    A.tol = c.tol;
+    A.tol2 = c.tol2;
+    A.G = c.G;
+    A.iters = L.sor.p + ns;
+    double pts = 0.0;
+    for (int q : sor_nodes)
+        pts += L.h[q].nintr;
+    launch(s, QZ_PROF_CG, 24.0 * pts * A.sweeps, k_sor_nodes, dim3(ns), dim3(256), A);
+    std::vector<int> it(ns);
+    if (!read_ints(s, A.iters, ns, it.data()))
+        return QZ_FAILURE;
+    for (int k = 0; k < ns; k++)
+        if (it[k] < 0)
+        {
+            set_error("the precision was not reached in a refinement-level node (level %d) after "
+                      "%d SOR iterations", level_index, -it[k]);
+            return QZ_FAILURE;
+        }
+    return check_cuda(cudaGetLastError(), "sor") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
 {
     const qz_config &c = s->cfg;
@@ -1756,15 +1912,21 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     const int chunk = 2 * nt;
     L.hchunks.clear();
     std::vector<int> node_chunk(2L * nn, 0);
+    std::vector<int> sor_nodes; // nodes of at most branch_cg_cells cells: red-black SOR
     for (int q = 0; q < nn; q++)
     {
         node_chunk[2 * q] = (int)L.hchunks.size();
         const AmrNode &N = L.h[q];
-        for (int b = N.intr_off; b < N.intr_off + N.nintr; b += chunk)
-            L.hchunks.push_back({q, b, std::min(b + chunk, N.intr_off + N.nintr)});
+        if (N.ncells > c.branch_cg_cells)
+            for (int b = N.intr_off; b < N.intr_off + N.nintr; b += chunk)
+                L.hchunks.push_back({q, b, std::min(b + chunk, N.intr_off + N.nintr)});
+        else if (N.nintr > 0)
+            sor_nodes.push_back(q);
         node_chunk[2 * q + 1] = (int)L.hchunks.size();
     }
     L.nchunks = (int)L.hchunks.size();
+    if (!sor_nodes.empty() && sor_level(s, L, level_index, sor_nodes))
+        return QZ_FAILURE;
     if (L.nchunks == 0)
         return QZ_SUCCESS;
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)

@@ -119,6 +119,9 @@ static bool build_levels(qz_sim *s, int n0)
         s->levels.push_back(l);
         n = nc;
     }
+    const bool cgs = s->cfg.smoother == 2;
+    if (cgs && !s->cg_part && !dmalloc(&s->cg_part, 2 * QZ_CG_PART_MAX, "cg partials"))
+        return false;
     for (auto &l : s->levels)
     {
         size_t pts = (size_t)l.n * l.n * l.n;
@@ -126,6 +129,25 @@ static bool build_levels(qz_sim *s, int n0)
             return false;
         if (jac && mixed && !dmalloc(&l.scrf, pts, "jacobi scratch32"))
             return false;
+        if (cgs)
+        {
+            // r and p stay zero on the boundary (conjugate_gradient_multigrid.c:37-39)
+            if (!dmalloc(&l.cgr, pts, "cg r") || !dmalloc(&l.cgp, pts, "cg p") ||
+                !dmalloc(&l.cga, pts, "cg Ap"))
+                return false;
+            cudaMemset(l.cgr, 0, pts * sizeof(double));
+            cudaMemset(l.cgp, 0, pts * sizeof(double));
+            cudaMemset(l.cga, 0, pts * sizeof(double));
+            if (mixed)
+            {
+                if (!dmalloc(&l.cgrf, pts, "cg r32") || !dmalloc(&l.cgpf, pts, "cg p32") ||
+                    !dmalloc(&l.cgaf, pts, "cg Ap32"))
+                    return false;
+                cudaMemset(l.cgrf, 0, pts * sizeof(float));
+                cudaMemset(l.cgpf, 0, pts * sizeof(float));
+                cudaMemset(l.cgaf, 0, pts * sizeof(float));
+            }
+        }
     }
     if (mixed)
     {
@@ -156,8 +178,13 @@ static void free_levels(qz_sim *s)
         }
         dfree(l.scr);
         dfree(l.scrf);
+        void *cg[] = {l.cgr, l.cgp, l.cga, l.cgrf, l.cgpf, l.cgaf};
+        for (void *q : cg)
+            dfree(q);
     }
     s->levels.clear();
+    dfree(s->cg_part);
+    s->cg_part = nullptr;
     dfree(s->rf);
     dfree(s->ef);
     dfree(s->ef_alt);
@@ -275,6 +302,9 @@ int qz_default_config(qz_config *c, int lmin)
     c->force_stencil = 0;
     c->ref_ptcl = 4;   /* global_variables.c:289 */
     c->box_extra = 10; /* 2 * min_box_extra_size_per_side_user, global_variables.c:294-295 */
+    c->branch_cg_cells = 0;    /* global_variables.c:334 */
+    c->branch_sor_sweeps = 10; /* global_variables.c:328 */
+    c->w_sor_branch = 1.0;     /* global_variables.c:329 */
     return QZ_SUCCESS;
 }
 
@@ -365,7 +395,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         set_error("qz_create: bdry=%d not supported (1 reflexive only)", cfg->bdry);
         return QZ_FAILURE;
     }
-    if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 1 || cfg->cycle < 0 ||
+    if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 2 || cfg->cycle < 0 ||
         cfg->cycle > 2 || n_capacity > (1L << 30))
     {
         set_error("qz_create: unsupported configuration");
@@ -885,6 +915,15 @@ int qz_jacobi(double *phi, const double *rho, int gridsize, int iter_max, double
     c.smoother = 1;
     c.w_sor = w;
     SmoothArg a{iter_max};
+    return run_dense(&c, phi, rho, gridsize, smooth_body, &a);
+}
+
+int qz_conjugate_gradient_multigrid(double *phi, const double *rho, int gridsize, int iters)
+{
+    qz_config c;
+    qz_default_config(&c, 2);
+    c.smoother = 2;
+    SmoothArg a{iters};
     return run_dense(&c, phi, rho, gridsize, smooth_body, &a);
 }
 

@@ -41,6 +41,8 @@ static struct {
     struct node **ptr_tree;
     int *niter_pre, *niter_post, *niter_coarse, *solver_pre, *solver_post, *solver_coarse;
     int *cycle, *check_every, *max_iter, *check_method, *head_pot_method, *force_stencil;
+    int *branch_cg_cells, *branch_sweeps;
+    double *w_sor_branch;
     double *w_sor_head, *tol, *tol2;
     int resolved;
 } R;
@@ -95,6 +97,9 @@ static int resolve(void)
     R.check_method = need("check_poisson_error_method", &ok);
     R.head_pot_method = need("head_pot_method", &ok);
     R.force_stencil = need("force_stencil", &ok);
+    R.branch_cg_cells = need("branches_maximal_node_number_to_activate_conjugate_gradient", &ok);
+    R.branch_sweeps = need("_Iter_branches_solver_", &ok);
+    R.w_sor_branch = need("_w_SOR_", &ok);
     R.w_sor_head = need("_w_SOR_HEAD_", &ok);
     R.tol = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_", &ok);
     R.tol2 = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_2", &ok);
@@ -121,6 +126,9 @@ static void fill_config(qz_config *c)
     c->max_iter = *R.max_iter;
     c->check_method = *R.check_method;
     c->force_stencil = *R.force_stencil;
+    c->branch_cg_cells = *R.branch_cg_cells;
+    c->branch_sor_sweeps = *R.branch_sweeps;
+    c->w_sor_branch = *R.w_sor_branch;
     const char *o = getenv("QZ_GS_ORDER");
     c->gs_order = (o && !strcmp(o, "lex")) ? QZ_GS_LEX : QZ_GS_REDBLACK;
     const char *p = getenv("QZ_PRECISION");
@@ -170,10 +178,10 @@ static int ensure(void)
         return REF_FAILURE;
     }
     if (*R.head_pot_method != 0 || *R.solver_pre != *R.solver_post ||
-        *R.solver_pre != *R.solver_coarse || *R.solver_pre > 1)
+        *R.solver_pre != *R.solver_coarse || *R.solver_pre > 2)
     {
         printf("\nERROR (drop-in): head solver configuration not supported "
-               "(multigrid with Gauss-Seidel or Jacobi smoothing only)\n");
+               "(multigrid with one smoother for all stages only)\n");
         g_failed = 1;
         return REF_FAILURE;
     }
@@ -384,11 +392,6 @@ void multigrid(double *phi, const double *rho, int gridsize, int type_multigrid)
     fill_config(&c);
     c.gs_order = dense_order();
     c.precision = QZ_PREC_FP64;
-    if (*R.solver_pre > 1)
-    {
-        printf("\nERROR (drop-in): conjugate-gradient smoothing is not supported\n");
-        return;
-    }
     if (qz_multigrid(&c, phi, rho, gridsize, type_multigrid))
         fail("multigrid");
 }
@@ -420,14 +423,11 @@ int conjugate_gradient(struct node *p)
     return REF_FAILURE;
 }
 
-/* force_methods/conjugate_gradient_multigrid.c:29-176: not in this build. */
+/* force_methods/conjugate_gradient_multigrid.c:29-176 */
 void conjugate_gradient_multigrid(double *phi, const double *rho, int gridsize, int iters)
 {
-    (void)phi;
-    (void)rho;
-    (void)gridsize;
-    (void)iters;
-    printf("\nERROR (drop-in): conjugate-gradient smoothing is not supported by this build\n");
+    if (qz_conjugate_gradient_multigrid(phi, rho, gridsize, iters))
+        fail("conjugate_gradient_multigrid");
 }
 
 /* force_methods/multigrid2.c: never called by the reference; kept for linking. */

@@ -38,6 +38,8 @@ struct Level {
     float *scrf = nullptr;
     double *alt = nullptr;                  // red-black ping-pong partners (zero boundary)
     float *altf = nullptr;
+    double *cgr = nullptr, *cgp = nullptr, *cga = nullptr; // CG smoothing r, p, Ap (smoother 2)
+    float *cgrf = nullptr, *cgpf = nullptr, *cgaf = nullptr;
 };
 
 // Device-side flag words (int).
@@ -167,6 +169,7 @@ struct AmrLevel {
     DBuf<double> chunk_part; // per chunk: two p.Ap and two r.r partials
     DBuf<double> mass_part;  // node mass slices (32 a node)
     DBuf<int> mass_range;    // per node: segment range
+    DBuf<int> sor;           // red-black SOR nodes of the level and their iteration counts
     int nchunks = 0;
     int h_active = 0; // host copy of the unconverged-node count at the start of a solve
     std::vector<AmrChunk> hchunks;
@@ -174,11 +177,14 @@ struct AmrLevel {
 
 } // namespace qz
 
+#define QZ_CG_PART_MAX 1024
+
 struct qz_sim {
     qz_config cfg;
     int device = 0;
     cudaStream_t stream = nullptr;
     qz::MemCtx mem; // stream-ordered pool for buffers that grow during a run
+    double *cg_part = nullptr; // conjugate-gradient smoothing: 2 x QZ_CG_PART_MAX partial sums
     long n = 0, cap = 0;
     double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *m = nullptr;

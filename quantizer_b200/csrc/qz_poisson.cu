@@ -330,10 +330,133 @@ __global__ void k_prolong_add(Grid<T> phi, Grid<T> c)
     phi.p[phi.off + i + j * phi.sy + k * phi.sz] += acc;
 }
 
+// ---- conjugate gradient as the smoother (smoother 2) ----------------------------
+// conjugate_gradient_multigrid.c:29-176 on one level: r = rho + (1/H^2)(6 phi - sum),
+// p = r, then up to min(iters, interior points) iterations of plain CG, leaving
+// early when rs_new / rs_old < 1e-16.  One cooperative launch per call; each
+// block adds its points' contributions in a fixed order, and after a grid
+// barrier every block adds the block partials in block order, so all blocks hold
+// the same sums (FP64) and take the same early exit.
+namespace cgs = cooperative_groups;
+
+template <typename T> struct CgsArgs {
+    Grid<T> phi, rho;
+    T *r, *p, *ap; // dense n^3, zero on the boundary
+    double *part;  // 2 * gridDim partial sums
+    int iters;
+};
+
+__device__ __forceinline__ double cgs_block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+        t += sh[w];
+    __syncthreads();
+    return t;
+}
+
+// Sum of the gridDim partials at part, in block order (every block, every thread).
+__device__ __forceinline__ double cgs_grid_sum(const double *part, double *sh)
+{
+    double v = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+        v += __ldcg(&part[b]);
+    return cgs_block_sum(v, sh);
+}
+
+template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs<T> A)
+{
+    cgs::grid_group grid = cgs::this_grid();
+    __shared__ double sh[32];
+    const int n = A.phi.n, m = n - 2;
+    const unsigned um = (unsigned)m, total = um * um * um;
+    const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+    const long n2 = (long)n * n;
+    const T H = (T)1.0 / (T)(n - 1);
+    const T oh2 = (T)1.0 / (H * H);
+    const Grid<T> &P = A.phi, &R = A.rho;
+    double *part0 = A.part, *part1 = A.part + gridDim.x;
+    double acc = 0.0;
+    for (unsigned t = gtid; t < total; t += gn)
+    {
+        const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+        const long gp = P.off + i + j * P.sy + k * P.sz;
+        const long l = i + j * (long)n + k * n2;
+        const T *ph = P.p;
+        const T rv = R.p[R.off + i + j * R.sy + k * R.sz] +
+                     oh2 * ((T)6.0 * ph[gp] - ph[gp + 1] - ph[gp - 1] - ph[gp + P.sy] -
+                            ph[gp - P.sy] - ph[gp + P.sz] - ph[gp - P.sz]);
+        A.r[l] = rv;
+        A.p[l] = rv;
+        acc += (double)rv * (double)rv;
+    }
+    double b = cgs_block_sum(acc, sh);
+    if (threadIdx.x == 0)
+        part0[blockIdx.x] = b;
+    grid.sync();
+    double rsold = cgs_grid_sum(part0, sh);
+    const long cap = (long)m * m * m;
+    const long cycle = A.iters < cap ? A.iters : cap;
+    for (long it = 0; it < cycle; it++)
+    {
+        acc = 0.0;
+        for (unsigned t = gtid; t < total; t += gn)
+        {
+            const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+            const long l = i + j * (long)n + k * n2;
+            const T *pp = A.p;
+            const T a = -oh2 * ((T)6.0 * pp[l] - pp[l + 1] - pp[l - 1] - pp[l + n] - pp[l - n] -
+                                pp[l + n2] - pp[l - n2]);
+            A.ap[l] = a;
+            acc += (double)pp[l] * (double)a;
+        }
+        b = cgs_block_sum(acc, sh);
+        if (threadIdx.x == 0)
+            part1[blockIdx.x] = b;
+        grid.sync();
+        const T alpha = (T)(rsold / cgs_grid_sum(part1, sh));
+        acc = 0.0;
+        for (unsigned t = gtid; t < total; t += gn)
+        {
+            const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+            const long l = i + j * (long)n + k * n2;
+            P.p[P.off + i + j * P.sy + k * P.sz] += alpha * A.p[l];
+            const T rv = A.r[l] - alpha * A.ap[l];
+            A.r[l] = rv;
+            acc += (double)rv * (double)rv;
+        }
+        b = cgs_block_sum(acc, sh);
+        if (threadIdx.x == 0)
+            part0[blockIdx.x] = b;
+        grid.sync();
+        const double rsnew = cgs_grid_sum(part0, sh);
+        if (rsnew / rsold < 1.0e-16)
+            break;
+        const T beta = (T)(rsnew / rsold);
+        for (unsigned t = gtid; t < total; t += gn)
+        {
+            const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+            const long l = i + j * (long)n + k * n2;
+            A.p[l] = A.r[l] + beta * A.p[l];
+        }
+        rsold = rsnew;
+        grid.sync();
+    }
+}
+
 // ---- host-side multigrid -----------------------------------------------------
+template <typename T> struct CgsScratch {
+    T *r = nullptr, *p = nullptr, *ap = nullptr;
+};
+
 template <typename T>
 static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scratch,
-                    Grid<T> alt)
+                    Grid<T> alt, CgsScratch<T> cgs_scratch = CgsScratch<T>())
 {
     const qz_config &c = s->cfg;
     const int n = phi.n;
@@ -402,6 +525,59 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
             b = t;
         }
     }
+    else if (c.smoother == 2)
+    {
+        if (!cgs_scratch.r || !s->cg_part)
+        {
+            set_error("conjugate-gradient smoothing buffers missing");
+            return QZ_FAILURE;
+        }
+        CgsArgs<T> A;
+        A.phi = phi;
+        A.rho = rho;
+        A.r = cgs_scratch.r;
+        A.p = cgs_scratch.p;
+        A.ap = cgs_scratch.ap;
+        A.part = s->cg_part;
+        A.iters = iters;
+        static int per_sm[2] = {0, 0};
+        static std::once_flag once;
+        std::call_once(once, [] {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_cg_smooth<double>, 256, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_cg_smooth<float>, 256, 0);
+        });
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+        const int ps = per_sm[sizeof(T) == 4 ? 1 : 0];
+        const long want = ((long)m * m * m + 255) / 256;
+        const int blocks = (int)std::max(1L, std::min(want, (long)std::min(ps, 2) * sms));
+        if (ps < 1 || blocks > QZ_CG_PART_MAX)
+        {
+            set_error("conjugate-gradient smoothing kernel cannot be resident");
+            return QZ_FAILURE;
+        }
+        void *args[] = {&A};
+        cudaEvent_t eb = nullptr, ee = nullptr;
+        if (s->prof)
+        {
+            eb = prof_event(s);
+            ee = prof_event(s);
+            cudaEventRecord(eb, s->stream);
+        }
+        if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_cg_smooth<T>, dim3(blocks),
+                                                    dim3(256), args, 0, s->stream),
+                        "conjugate-gradient smoothing"))
+            return QZ_FAILURE;
+        s->stats.kernel_launches++;
+        if (s->prof)
+        {
+            cudaEventRecord(ee, s->stream);
+            // the residual pass (24 B a point) and 88 B a point per iteration, FP64 units
+            s->prof_pending.push_back({QZ_PROF_SMOOTH,
+                                       (double)sizeof(T) * (24.0 + 88.0 * iters) * m * m * m / 8.0,
+                                       eb, ee});
+        }
+    }
     else
     {
         set_error("smoother %d is not supported", c.smoother);
@@ -416,7 +592,19 @@ struct LevelViews {
     static Grid<T> rho(qz_sim *s, int l);
     static Grid<T> scratch(qz_sim *s, int l);
     static Grid<T> alt(qz_sim *s, int l);
+    static CgsScratch<T> cgs(qz_sim *s, int l);
 };
+
+template <> CgsScratch<double> LevelViews<double>::cgs(qz_sim *s, int l)
+{
+    const Level &v = s->levels[l];
+    return CgsScratch<double>{v.cgr, v.cgp, v.cga};
+}
+template <> CgsScratch<float> LevelViews<float>::cgs(qz_sim *s, int l)
+{
+    const Level &v = s->levels[l];
+    return CgsScratch<float>{v.cgrf, v.cgpf, v.cgaf};
+}
 
 // Level 0 of the FP64 hierarchy is the fine grid view of the context (the head
 // solve grid embedded in the head fields, or a dense array for the array-level
@@ -475,13 +663,14 @@ static int vcycle_t(qz_sim *s, int l, int type)
         scr = LevelViews<T>::scratch(s, l);
     if (c.smoother == 0 && c.gs_order == QZ_GS_REDBLACK)
         alt = LevelViews<T>::alt(s, l);
-    if (smooth_t<T>(s, phi, rho, c.n_pre, scr, alt))
+    const CgsScratch<T> cgw = LevelViews<T>::cgs(s, l);
+    if (smooth_t<T>(s, phi, rho, c.n_pre, scr, alt, cgw))
         return QZ_FAILURE;
     if (nc < 4)
     {
         // multigrid.c:158-173: the coarse correction stays zero; the fine grid
         // gets n_coarse more smoothing sweeps instead.
-        if (smooth_t<T>(s, phi, rho, c.n_coarse, scr, alt))
+        if (smooth_t<T>(s, phi, rho, c.n_coarse, scr, alt, cgw))
             return QZ_FAILURE;
     }
     else
@@ -520,7 +709,7 @@ static int vcycle_t(qz_sim *s, int l, int type)
         dim3 gf((m + tf - 1) / tf, m, m);
         launch(s, QZ_PROF_PROLONG, (double)sizeof(T) * 2.125 * m * m * m, k_prolong_add<T>, dim3(gf), dim3(tf), phi, cphi);
     }
-    if (smooth_t<T>(s, phi, rho, c.n_post, scr, alt))
+    if (smooth_t<T>(s, phi, rho, c.n_post, scr, alt, cgw))
         return QZ_FAILURE;
     return check_cuda(cudaGetLastError(), "multigrid cycle") ? QZ_SUCCESS : QZ_FAILURE;
 }
@@ -933,7 +1122,7 @@ int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters)
         sync_fine_alt(s);
         alt = LevelViews<double>::alt(s, 0);
     }
-    return smooth_t<double>(s, phi, rho, iters, scr, alt);
+    return smooth_t<double>(s, phi, rho, iters, scr, alt, LevelViews<double>::cgs(s, 0));
 }
 
 // The fine level's ping-pong partner must carry the fine grid's boundary

@@ -41,3 +41,8 @@ def arrays_golden():
 @pytest.fixture(scope="session")
 def stencil5_golden():
     return golden("head_L4_stencil5.npz")
+
+
+@pytest.fixture(scope="session")
+def cgsmooth_golden():
+    return golden("head_L4_cgsmooth.npz")

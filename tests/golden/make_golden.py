@@ -12,9 +12,11 @@ sources (oracle/Makefile, target ``ref``):
   8^3, 2 steps.
 * ``head_L4_stencil5.npz`` -- the head_L4 case with the 5-point force stencil
   (force_stencil = 1).
+* ``head_L4_cgsmooth.npz`` -- the head_L4 case, 2 steps, with conjugate
+  gradient as the multigrid smoother (solver 2).
 * ``arrays.npz`` -- direct calls into oracle/_ref/libqzref.so of the
-  reference's gauss_saidel, jacobi (odd sweep count) and multigrid (V, F and W
-  cycles) on seeded random arrays.
+  reference's gauss_saidel, jacobi (odd sweep count), conjugate_gradient_multigrid
+  and multigrid (V, F and W cycles) on seeded random arrays.
 
 Run in a container that has the reference source tree:
     python tests/golden/make_golden.py [fixture-name ...]   (default: all)
@@ -90,6 +92,13 @@ def arrays_case() -> None:
         lib.jacobi(phi.ctypes.data_as(P), rho.ctypes.data_as(P), n, iters)
         out[f"jac_n{n}_out"] = phi
         out[f"jac_n{n}_iters"] = np.array([iters])
+    lib.conjugate_gradient_multigrid.argtypes = [P, P, C.c_int, C.c_int]
+    for n, iters in ((9, 4), (17, 6)):
+        phi, rho = fresh(n)
+        out[f"cgs_n{n}_in_phi"], out[f"cgs_n{n}_in_rho"] = phi.copy(), rho.copy()
+        lib.conjugate_gradient_multigrid(phi.ctypes.data_as(P), rho.ctypes.data_as(P), n, iters)
+        out[f"cgs_n{n}_out"] = phi
+        out[f"cgs_n{n}_iters"] = np.array([iters])
     for n, types in ((9, (0, 1, 2)), (17, (0, 1, 2)), (33, (0,))):
         for t in types:
             phi, rho = fresh(n)
@@ -109,6 +118,7 @@ def main() -> None:
         ("head_L4_plummer1000.npz", dict(steps=3, lmin=4)),
         ("head_L3_jacobi.npz", dict(steps=2, lmin=3, solver=1)),
         ("head_L4_stencil5.npz", dict(steps=3, lmin=4, stencil=1)),
+        ("head_L4_cgsmooth.npz", dict(steps=2, lmin=4, solver=2)),
     ]
     for name, kw in cases:
         if not want or name in want:

@@ -37,11 +37,22 @@ def _run(driver, ic_path, out, env=None, **kw):
         os.environ.update(old)
 
 
-@pytest.mark.parametrize("order,tol_pot,tol_pos", [("lex", 1e-12, 1e-13), ("rb", 1e-9, 1e-9)])
-def test_dropin_driver_matches_reference(ic_file, tmp_path, order, tol_pot, tol_pos):
+# (Gauss-Seidel order, extra driver settings, potential / position tolerances); the
+# conjugate-gradient smoother (solver 2) and the 5-point stencil are the
+# reference's own settings, read by the drop-in from its globals
+CASES = [
+    ("lex", {}, 1e-12, 1e-13),
+    ("rb", {}, 1e-9, 1e-9),
+    ("rb", {"solver": 2}, 1e-9, 1e-9),
+    ("lex", {"stencil": 1}, 1e-12, 1e-13),
+]
+
+
+@pytest.mark.parametrize("order,extra,tol_pot,tol_pos", CASES)
+def test_dropin_driver_matches_reference(ic_file, tmp_path, order, extra, tol_pot, tol_pos):
     for drv in (O.REF_DRIVER, O.DROPIN_DRIVER):
         assert os.path.exists(drv), f"{drv} missing: run `make -C oracle ref dropin` where the reference is present"
-    kw = dict(lmin=5, steps=6, dt=7e-5, dump="0,6")
+    kw = dict(lmin=5, steps=6, dt=7e-5, dump="0,6", **extra)
     _run(O.REF_DRIVER, ic_file, str(tmp_path / "ref"), **kw)
     _run(O.DROPIN_DRIVER, ic_file, str(tmp_path / "gpu"), env={"QZ_GS_ORDER": order}, **kw)
     for s in (0, 6):

@@ -48,6 +48,20 @@ def test_head_pipeline_five_point_stencil_bit_exact(stencil5_golden):
     _assert_exact(stencil5_golden, steps, s0, s1)
 
 
+def test_head_pipeline_cg_smoothing_bit_exact(cgsmooth_golden):
+    steps, s0, s1 = _run(cgsmooth_golden, 4, solver=2)
+    _assert_exact(cgsmooth_golden, steps, s0, s1)
+
+
+def test_cg_smoother_bit_exact(arrays_golden):
+    g = arrays_golden
+    lib = O.load()
+    for n in (9, 17):
+        phi, rho = g[f"cgs_n{n}_in_phi"].copy(), g[f"cgs_n{n}_in_rho"].copy()
+        lib.qzo_cg_smooth(O.ptr(phi), O.ptr(rho), n, int(g[f"cgs_n{n}_iters"][0]))
+        np.testing.assert_array_equal(phi, g[f"cgs_n{n}_out"])
+
+
 def test_box_index_bit_exact(head_golden):
     lib = O.load()
     L = 4
