@@ -87,6 +87,11 @@ typedef struct qz_config {
     int branch_cg_cells;
     int branch_sor_sweeps;
     double w_sor_branch;
+    /* time step (timestep.c:589-700): _CFL_, _MAX_dt_, time_step_method
+     * (0 velocity only, 1 velocity and acceleration) */
+    double cfl;
+    double max_dt;
+    int time_step_method;
 } qz_config;
 
 typedef struct qz_stats {
@@ -99,6 +104,8 @@ typedef struct qz_stats {
     long long cg_iterations;   /* refinement-level conjugate-gradient iterations */
     int levels;                /* refinement levels in the current tree (1 = head only) */
     int nodes;                 /* nodes in the current tree, head included */
+    double last_dt;            /* step size of the last qz_step step */
+    double sim_time;           /* sum of the qz_step step sizes */
 } qz_stats;
 
 typedef struct qz_sim qz_sim;
@@ -174,9 +181,15 @@ QZ_API int qz_amr_node_list(qz_sim *sim, int level, int node, int which, int *ou
 QZ_API int qz_amr_node_field(qz_sim *sim, int level, int node, int which, double *out);
 
 /* Step 0 force computation (main.c:296-338) and whole leapfrog steps
- * (main.c:375-481 with a fixed dt). */
+ * (main.c:375-481).  dt > 0: that fixed step; dt <= 0: each step takes the
+ * CFL step of qz_timestep from the current state, as main.c:375 does. */
 QZ_API int qz_init_forces(qz_sim *sim);
 QZ_API int qz_step(qz_sim *sim, double dt, int nsteps);
+
+/* timestep (timestep.c:589-700, headers/timestep.h): the CFL time step of the
+ * current velocities and accelerations, each particle with the cell size of its
+ * finest node; reduced on the device (exact, order-independent min / max). */
+QZ_API int qz_timestep(qz_sim *sim, double *dt);
 
 /* Synchronise the library stream and report statistics. */
 QZ_API int qz_synchronize(qz_sim *sim);

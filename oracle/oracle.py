@@ -62,6 +62,8 @@ def load():
         lib.qzo_gauss_saidel.argtypes = [_P, _P, C.c_int, C.c_int, C.c_double]
         lib.qzo_jacobi.argtypes = [_P, _P, C.c_int, C.c_int, C.c_double]
         lib.qzo_cg_smooth.argtypes = [_P, _P, C.c_int, C.c_int]
+        lib.qzo_timestep_head.restype = C.c_double
+        lib.qzo_timestep_head.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_long] + [_P] * 6
         lib.qzo_multigrid.argtypes = [C.POINTER(Params), _P, _P, C.c_int, C.c_int]
         lib.qzo_poisson_check_head.argtypes = [C.POINTER(Params), _P, _P, _P, C.c_double]
         lib.qzo_potential_head.argtypes = [C.POINTER(Params), _P, _P, _P, C.c_double]

@@ -655,3 +655,61 @@ void qzo_sim_free(qzo_sim *s)
         free(a[q]);
     memset(s, 0, sizeof *s);
 }
+
+/* timestep.c:35-157 (head only): method 0 from the largest velocity
+ * component, method 1 per particle and axis from velocity and acceleration. */
+static double qzo_ts_axis(double v, double a, double H, double cfl, double dt)
+{
+    if (fabs(a) < 1.0e-16)
+    {
+        if (fabs(v) > 1.0e-16)
+        {
+            double aux = cfl * H / fabs(v);
+            dt = dt < aux ? dt : aux;
+        }
+    }
+    else
+    {
+        double c = v * v + 2.0 * fabs(a) * H * cfl;
+        double aux;
+        if (1 - v * v / c > 1.0e-8)
+            aux = (-fabs(v) + sqrt(c)) / fabs(a);
+        else
+        {
+            double eps = fabs(a * H * cfl / (v * v));
+            aux = fabs(v / a) * (eps - eps * eps * 0.5);
+        }
+        dt = dt < aux ? dt : aux;
+    }
+    return dt;
+}
+
+double qzo_timestep_head(int L, int method, double cfl, double max_dt, long n, const double *vx,
+                         const double *vy, const double *vz, const double *ax, const double *ay,
+                         const double *az)
+{
+    double H = 1.0 / (1 << L);
+    if (method == 1)
+    {
+        double dt = max_dt;
+        for (long i = 0; i < n; i++)
+        {
+            dt = qzo_ts_axis(vx[i], ax[i], H, cfl, dt);
+            dt = qzo_ts_axis(vy[i], ay[i], H, cfl, dt);
+            dt = qzo_ts_axis(vz[i], az[i], H, cfl, dt);
+        }
+        return dt;
+    }
+    double vmax = 0.0;
+    for (long i = 0; i < n; i++)
+    {
+        if (vmax < fabs(vx[i]))
+            vmax = fabs(vx[i]);
+        if (vmax < fabs(vy[i]))
+            vmax = fabs(vy[i]);
+        if (vmax < fabs(vz[i]))
+            vmax = fabs(vz[i]);
+    }
+    double d = vmax < (cfl * H / max_dt) ? max_dt : (cfl * H / vmax);
+    return max_dt > d ? d : max_dt;
+}

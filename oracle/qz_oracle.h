@@ -50,6 +50,10 @@ void qzo_deposit_head(const qzo_params *p, long n, const double *x, const double
 void qzo_gauss_saidel(double *phi, const double *rho, int gridsize, int iters, double w);
 /* force_methods/jacobi.c:29-82 */
 void qzo_jacobi(double *phi, const double *rho, int gridsize, int iters, double w);
+/* timestep.c:35-157, 589-700 (head only) */
+double qzo_timestep_head(int L, int method, double cfl, double max_dt, long n, const double *vx,
+                         const double *vy, const double *vz, const double *ax, const double *ay,
+                         const double *az);
 /* conjugate_gradient_multigrid.c:29-176 */
 void qzo_cg_smooth(double *phi, const double *rho, int gridsize, int iters);
 /* force_methods/multigrid.c:106-229 */

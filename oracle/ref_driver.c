@@ -17,9 +17,11 @@
  *   keys: lmin, lmax, steps, dt, dump (comma list of steps, -1 = none),
  *         ref_ptcl, G, threads, solver (0 GS,1 Jacobi,2 CG), bdry, cg_head,
  *         stencil (force_stencil), branch_cg_cells (nodes of more cells use
- *         conjugate gradient, the others red-black SOR)
+ *         conjugate gradient, the others red-black SOR), tsm (time_step_method),
+ *         cfl (_CFL_), max_dt (_MAX_dt_)
  * IC.bin: int64 N, then x[N] y[N] z[N] vx[N] vy[N] vz[N] m[N] (float64).
- * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles),
+ * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles, and
+ *        dtcfl: the reference's timestep() of that state),
  *        OUTDIR/s<step>_nodes.txt (AMR node summary when lmax > lmin).
  * The last stdout line is a JSON summary with the step-loop wall time.
  */
@@ -150,6 +152,11 @@ static void dump_step(const char *dir, int step, int amr)
     free(bidx);
     if (amr)
         dump_nodes(dir, step);
+    /* the CFL step the main loop would take next (main.c:375, timestep.c:589-700) */
+    double dtc = 0.0;
+    if (timestep(&dtc) == _FAILURE_)
+        fprintf(stderr, "ref_driver: timestep failed\n");
+    write_f64(dir, step, "dtcfl", &dtc, 1);
 }
 
 static int in_list(const char *list, int step)
@@ -186,6 +193,9 @@ int main(int argc, char **argv)
     int L = 5, LMAX = -1, steps = 1, ref_ptcl = 9, threads = 1, solver = 0, bdry = 1;
     int cg_head = 0;
     int stencil = 0;        /* force_stencil */
+    int tsm = -1;           /* time_step_method */
+    double cfl = -1.0;      /* _CFL_ */
+    double max_dt = -1.0;   /* _MAX_dt_ */
     int branch_cg_cells = -1; /* branches_maximal_node_number_to_activate_conjugate_gradient */
     double dt = 1e-4, G = 1.0;
     const char *dump = NULL;
@@ -210,6 +220,9 @@ int main(int argc, char **argv)
         else if (!strcmp(key, "bdry")) bdry = atoi(v);
         else if (!strcmp(key, "cg_head")) cg_head = atoi(v);
         else if (!strcmp(key, "stencil")) stencil = atoi(v);
+        else if (!strcmp(key, "tsm")) tsm = atoi(v);
+        else if (!strcmp(key, "cfl")) cfl = atof(v);
+        else if (!strcmp(key, "max_dt")) max_dt = atof(v);
         else if (!strcmp(key, "branch_cg_cells")) branch_cg_cells = atoi(v);
         else die("unknown key");
     }
@@ -242,6 +255,12 @@ int main(int argc, char **argv)
     solverPreS = solverPostS = solverfinddphic = solver;
     head_pot_method = cg_head;
     force_stencil = stencil;
+    if (tsm >= 0)
+        time_step_method = tsm;
+    if (cfl > 0.0)
+        _CFL_ = cfl;
+    if (max_dt > 0.0)
+        _MAX_dt_ = max_dt;
     if (branch_cg_cells >= 0)
         branches_maximal_node_number_to_activate_conjugate_gradient = branch_cg_cells;
     NUMBER_OF_THEADS = threads;
@@ -314,8 +333,10 @@ int main(int argc, char **argv)
     for (int lv = 0; lv <= GL_tentacles_level_max; lv++)
         nodes += GL_tentacles_size[lv];
     printf("\n{\"n\": %d, \"steps\": %d, \"init_s\": %.6f, \"loop_s\": %.6f, "
-           "\"ptcl_steps_per_s\": %.6e, \"levels\": %d, \"nodes\": %d, \"threads\": %d}\n",
+           "\"ptcl_steps_per_s\": %.6e, \"levels\": %d, \"nodes\": %d, \"threads\": %d, "
+           "\"max_dt\": %.17e, \"cfl\": %.17e, \"time_step_method\": %d}\n",
            N, steps, t_init, t_loop, steps > 0 ? (double)N * steps / t_loop : 0.0,
-           GL_tentacles_level_max, nodes, threads);
+           GL_tentacles_level_max, nodes, threads, (double)_MAX_dt_, (double)_CFL_,
+           time_step_method);
     return 0;
 }

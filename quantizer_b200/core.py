@@ -38,7 +38,8 @@ class Config(C.Structure):
         ("max_iter", C.c_int), ("check_method", C.c_int), ("precision", C.c_int),
         ("inner_cycles", C.c_int), ("force_stencil", C.c_int), ("ref_ptcl", C.c_int),
         ("box_extra", C.c_int), ("branch_cg_cells", C.c_int), ("branch_sor_sweeps", C.c_int),
-        ("w_sor_branch", C.c_double),
+        ("w_sor_branch", C.c_double), ("cfl", C.c_double), ("max_dt", C.c_double),
+        ("time_step_method", C.c_int),
     ]
 
 
@@ -47,6 +48,7 @@ class Stats(C.Structure):
         ("vcycles_total", C.c_longlong), ("last_vcycles", C.c_int), ("last_converged", C.c_int),
         ("kernel_launches", C.c_longlong), ("steps", C.c_longlong), ("error_flags", C.c_int),
         ("cg_iterations", C.c_longlong), ("levels", C.c_int), ("nodes", C.c_int),
+        ("last_dt", C.c_double), ("sim_time", C.c_double),
     ]
 
 
@@ -96,6 +98,7 @@ def load() -> C.CDLL:
         "qz_jacobi": ([_P, _P, C.c_int, C.c_int, C.c_double], C.c_int),
         "qz_multigrid": ([C.POINTER(Config), _P, _P, C.c_int, C.c_int], C.c_int),
         "qz_conjugate_gradient_multigrid": ([_P, _P, C.c_int, C.c_int], C.c_int),
+        "qz_timestep": ([vp, _P], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -269,6 +272,12 @@ class Simulation:
         out = np.zeros((rd[0] + 1) * (rd[1] + 1) * (rd[2] + 1))
         _check(self.lib.qz_amr_node_field(self.h, level, node, FIELDS[name], _p(out)))
         return out
+
+    def timestep(self) -> float:
+        """CFL step of the current state (timestep.c:589-700)."""
+        dt = C.c_double()
+        _check(self.lib.qz_timestep(self.h, C.byref(dt)))
+        return dt.value
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))

@@ -305,6 +305,9 @@ int qz_default_config(qz_config *c, int lmin)
     c->branch_cg_cells = 0;    /* global_variables.c:334 */
     c->branch_sor_sweeps = 10; /* global_variables.c:328 */
     c->w_sor_branch = 1.0;     /* global_variables.c:329 */
+    c->cfl = 0.5;              /* _CFL_, global_variables.c:291 */
+    c->max_dt = 1.0e30;        /* _MAX_dt_ (0.005 Maxdt in the reference's units): no cap */
+    c->time_step_method = 1;   /* global_variables.c:342 */
     return QZ_SUCCESS;
 }
 
@@ -342,7 +345,7 @@ int qz_destroy(qz_sim *s)
     void *ptrs[] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m,
                     s->pot, s->pot_old, s->d, s->gax, s->gay, s->gaz, s->sort.k0, s->sort.k1,
                     s->sort.v0, s->sort.v1, s->sort.hist, s->seg_head, s->seg_id, s->seg_start,
-                    s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags};
+                    s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags, s->d_ts};
     for (void *p : ptrs)
         dfree(p);
     free_levels(s);
@@ -355,6 +358,8 @@ int qz_destroy(qz_sim *s)
         cudaMemPoolDestroy(s->mem.pool);
     if (s->h_flags)
         cudaFreeHost(s->h_flags);
+    if (s->h_ts)
+        cudaFreeHost(s->h_ts);
     if (s->h_stage)
         cudaFreeHost(s->h_stage);
     if (s->stream)
@@ -446,6 +451,9 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     s->red_blocks = 296;
     ok = ok && dmalloc(&s->red, s->red_blocks + 8, "red") && dmalloc(&s->flags, F_COUNT, "flags");
     ok = ok && check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned");
+    ok = ok && check_cuda(cudaMallocHost((void **)&s->h_ts, 34 * sizeof(unsigned long long)),
+                          "pinned time step") &&
+         dmalloc(&s->d_ts, 17, "time step");
     s->sort.cap = cap;
     s->sort.tiles_cap = tiles;
     if (ok)
@@ -646,11 +654,16 @@ int qz_step(qz_sim *s, double dt, int nsteps)
         return QZ_FAILURE;
     for (int q = 0; q < nsteps; q++)
     {
-        if (kick_drift(s, dt) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
+        double h = dt;
+        if (dt <= 0.0 && timestep_cfl(s, &h))
+            return QZ_FAILURE;
+        if (kick_drift(s, h) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
             qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) ||
-            kick(s, dt))
+            kick(s, h))
             return QZ_FAILURE;
         s->stats.steps++;
+        s->stats.last_dt = h;
+        s->stats.sim_time += h;
     }
     return check_flags(s);
 }

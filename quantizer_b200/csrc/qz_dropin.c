@@ -42,7 +42,8 @@ static struct {
     int *niter_pre, *niter_post, *niter_coarse, *solver_pre, *solver_post, *solver_coarse;
     int *cycle, *check_every, *max_iter, *check_method, *head_pot_method, *force_stencil;
     int *branch_cg_cells, *branch_sweeps;
-    double *w_sor_branch;
+    double *w_sor_branch, *cfl, *max_dt;
+    int *time_step_method;
     double *w_sor_head, *tol, *tol2;
     int resolved;
 } R;
@@ -100,6 +101,9 @@ static int resolve(void)
     R.branch_cg_cells = need("branches_maximal_node_number_to_activate_conjugate_gradient", &ok);
     R.branch_sweeps = need("_Iter_branches_solver_", &ok);
     R.w_sor_branch = need("_w_SOR_", &ok);
+    R.cfl = need("_CFL_", &ok);
+    R.max_dt = need("_MAX_dt_", &ok);
+    R.time_step_method = need("time_step_method", &ok);
     R.w_sor_head = need("_w_SOR_HEAD_", &ok);
     R.tol = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_", &ok);
     R.tol2 = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_2", &ok);
@@ -129,6 +133,9 @@ static void fill_config(qz_config *c)
     c->branch_cg_cells = *R.branch_cg_cells;
     c->branch_sor_sweeps = *R.branch_sweeps;
     c->w_sor_branch = *R.w_sor_branch;
+    c->cfl = *R.cfl;
+    c->max_dt = *R.max_dt;
+    c->time_step_method = *R.time_step_method;
     const char *o = getenv("QZ_GS_ORDER");
     c->gs_order = (o && !strcmp(o, "lex")) ? QZ_GS_LEX : QZ_GS_REDBLACK;
     const char *p = getenv("QZ_PRECISION");
@@ -260,6 +267,16 @@ int grid_acceleration(void)
     if (head_field_back(QZ_FIELD_AX, h->ptr_ax) || head_field_back(QZ_FIELD_AY, h->ptr_ay) ||
         head_field_back(QZ_FIELD_AZ, h->ptr_az))
         return REF_FAILURE;
+    return REF_SUCCESS;
+}
+
+/* timestep.c:589-700: the CFL step of the current state, reduced on the device */
+int timestep(double *ptr_dt)
+{
+    if (ensure())
+        return REF_FAILURE;
+    if (qz_timestep(g_sim, ptr_dt))
+        return fail("timestep");
     return REF_SUCCESS;
 }
 

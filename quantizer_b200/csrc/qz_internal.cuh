@@ -216,6 +216,8 @@ struct qz_sim {
     int red_blocks = 0;
     int *flags = nullptr;  // device flag words
     int *h_flags = nullptr; // pinned mirror
+    unsigned long long *d_ts = nullptr; // time-step reduction words (17)
+    unsigned long long *h_ts = nullptr; // pinned: 17 words out, 17 back
     double *h_red = nullptr; // pinned scalar readback
     double *h_stage = nullptr; // pinned staging for host copies
     size_t h_stage_bytes = 0;
@@ -262,6 +264,7 @@ namespace qz {
 
 // ---- launch accounting and errors ------------------------------------------
 void set_error(const char *fmt, ...);
+int timestep_cfl(qz_sim *s, double *dt_out); // qz_observe.cu
 bool check_cuda(cudaError_t e, const char *what);
 #define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
 

@@ -46,3 +46,8 @@ def stencil5_golden():
 @pytest.fixture(scope="session")
 def cgsmooth_golden():
     return golden("head_L4_cgsmooth.npz")
+
+
+@pytest.fixture(scope="session")
+def timestep_golden():
+    return golden("timestep_head_L4.npz")

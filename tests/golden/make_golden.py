@@ -14,6 +14,9 @@ sources (oracle/Makefile, target ``ref``):
   (force_stencil = 1).
 * ``head_L4_cgsmooth.npz`` -- the head_L4 case, 2 steps, with conjugate
   gradient as the multigrid smoother (solver 2).
+* ``timestep_head_L4.npz`` -- the reference's timestep() (methods 0 and 1) on the
+  states of the head_L4 case at steps 0 and 3 (_MAX_dt_ set to 1 so that the CFL
+  condition decides), with its _MAX_dt_ and _CFL_.
 * ``arrays.npz`` -- direct calls into oracle/_ref/libqzref.so of the
   reference's gauss_saidel, jacobi (odd sweep count), conjugate_gradient_multigrid
   and multigrid (V, F and W cycles) on seeded random arrays.
@@ -55,6 +58,23 @@ def run_case(name: str, ic: dict, steps: int, dt: float, **kw) -> None:
         out["meta"] = np.array([kw.get("lmin", 5), steps, dt, summary["n"]], dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, name), **out)
     print("wrote", name, summary)
+
+
+def timestep_case(ic: dict, dt: float) -> None:
+    """The reference's timestep() (both methods) on the states of the head_L4 case."""
+    out = {}
+    for tsm in (0, 1):
+        with tempfile.TemporaryDirectory() as td:
+            icp = os.path.join(td, "ic.bin")
+            ics.write_ic(icp, ic)
+            summary = O.run_reference(icp, td, steps=3, dt=dt, dump="0,3", lmin=4, tsm=tsm,
+                                      max_dt=1.0)
+            for s in (0, 3):
+                out[f"m{tsm}_s{s}_dt"] = O.read_dump(td, s, "dtcfl")
+            out["max_dt"] = np.array([summary["max_dt"]])
+            out["cfl"] = np.array([summary["cfl"]])
+    np.savez_compressed(os.path.join(HERE, "timestep_head_L4.npz"), **out)
+    print("wrote timestep_head_L4.npz", {k: v.tolist() for k, v in out.items()})
 
 
 def arrays_case() -> None:
@@ -123,6 +143,8 @@ def main() -> None:
     for name, kw in cases:
         if not want or name in want:
             run_case(name, ic, dt=dt, **kw)
+    if not want or "timestep_head_L4.npz" in want:
+        timestep_case(ic, dt)
     if not want or "arrays.npz" in want:
         arrays_case()
 

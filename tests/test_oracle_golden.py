@@ -62,6 +62,17 @@ def test_cg_smoother_bit_exact(arrays_golden):
         np.testing.assert_array_equal(phi, g[f"cgs_n{n}_out"])
 
 
+def test_timestep_head_bit_exact(head_golden, timestep_golden):
+    lib = O.load()
+    g, t = head_golden, timestep_golden
+    for m in (0, 1):
+        for s in (0, 3):
+            arr = [np.ascontiguousarray(g[f"s{s}_{k}"]) for k in ("vx", "vy", "vz", "ax", "ay", "az")]
+            dt = lib.qzo_timestep_head(4, m, float(t["cfl"][0]), float(t["max_dt"][0]),
+                                       arr[0].size, *[O.ptr(a) for a in arr])
+            assert dt == float(t[f"m{m}_s{s}_dt"][0]), (m, s, dt)
+
+
 def test_box_index_bit_exact(head_golden):
     lib = O.load()
     L = 4
