@@ -191,6 +191,15 @@ QZ_API int qz_step(qz_sim *sim, double dt, int nsteps);
  * finest node; reduced on the device (exact, order-independent min / max). */
 QZ_API int qz_timestep(qz_sim *sim, double *dt);
 
+/* observables (observables.c:661-696): out[0] kinetic, out[1] potential,
+ * out[2] total energy, out[3..5] momentum.  potential_type 0: exact sum over
+ * particle pairs (O(N^2), potential_energy_exact :77-112); 1: from the
+ * potential grid at each particle's finest node (:590-618).  units: NULL for
+ * code units, else {_conversion_velocity_, _conversion_time_,
+ * _conversion_dist_, GL_cm_vx, GL_cm_vy, GL_cm_vz}.  FP64 sums in fixed
+ * order (reproducible; equal to the reference's to rounding). */
+QZ_API int qz_observables(qz_sim *sim, int potential_type, const double *units, double *out);
+
 /* Synchronise the library stream and report statistics. */
 QZ_API int qz_synchronize(qz_sim *sim);
 QZ_API int qz_get_stats(qz_sim *sim, qz_stats *out);

@@ -65,6 +65,9 @@ QZ_DROPIN_API void gauss_saidel(double *phi, const double *rho, int gridsize, in
 QZ_DROPIN_API void jacobi(double *phi, const double *rho, int gridsize, int iter_max);
 /* headers/conjugate_gradient.h:33 */
 QZ_DROPIN_API int conjugate_gradient(struct node *ptr_node);
+/* headers/observables.h:32 */
+QZ_DROPIN_API int observables(void);
+
 /* headers/timestep.h: int timestep(vtype *ptr_dt) */
 QZ_DROPIN_API int timestep(double *ptr_dt);
 

@@ -18,7 +18,8 @@
  *         ref_ptcl, G, threads, solver (0 GS,1 Jacobi,2 CG), bdry, cg_head,
  *         stencil (force_stencil), branch_cg_cells (nodes of more cells use
  *         conjugate gradient, the others red-black SOR), tsm (time_step_method),
- *         cfl (_CFL_), max_dt (_MAX_dt_)
+ *         cfl (_CFL_), max_dt (_MAX_dt_), obs (1: dump observables of both
+ *         potential-energy forms as obs0 / obs1: energies[3], momentum[3])
  * IC.bin: int64 N, then x[N] y[N] z[N] vx[N] vy[N] vz[N] m[N] (float64).
  * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles, and
  *        dtcfl: the reference's timestep() of that state),
@@ -125,6 +126,8 @@ static void dump_nodes(const char *dir, int step)
     fclose(f);
 }
 
+static int g_obs = 0; /* dump observables at each dumped step */
+
 static void dump_step(const char *dir, int step, int amr)
 {
     struct node *h = GL_ptr_tree;
@@ -152,6 +155,25 @@ static void dump_step(const char *dir, int step, int amr)
     free(bidx);
     if (amr)
         dump_nodes(dir, step);
+    /* energies and momentum (observables.c:661-696), both potential-energy forms */
+    if (g_obs)
+    {
+        int saved = potential_energy_type;
+        for (int t = 0; t < 2; t++)
+        {
+            potential_energy_type = t;
+            double o[6] = {0, 0, 0, 0, 0, 0};
+            if (observables() == _FAILURE_)
+                fprintf(stderr, "ref_driver: observables failed\n");
+            for (int k = 0; k < 3; k++)
+            {
+                o[k] = GL_energies[k];
+                o[3 + k] = GL_momentum[k];
+            }
+            write_f64(dir, step, t == 0 ? "obs0" : "obs1", o, 6);
+        }
+        potential_energy_type = saved;
+    }
     /* the CFL step the main loop would take next (main.c:375, timestep.c:589-700) */
     double dtc = 0.0;
     if (timestep(&dtc) == _FAILURE_)
@@ -223,6 +245,7 @@ int main(int argc, char **argv)
         else if (!strcmp(key, "tsm")) tsm = atoi(v);
         else if (!strcmp(key, "cfl")) cfl = atof(v);
         else if (!strcmp(key, "max_dt")) max_dt = atof(v);
+        else if (!strcmp(key, "obs")) g_obs = atoi(v);
         else if (!strcmp(key, "branch_cg_cells")) branch_cg_cells = atoi(v);
         else die("unknown key");
     }
@@ -334,9 +357,12 @@ int main(int argc, char **argv)
         nodes += GL_tentacles_size[lv];
     printf("\n{\"n\": %d, \"steps\": %d, \"init_s\": %.6f, \"loop_s\": %.6f, "
            "\"ptcl_steps_per_s\": %.6e, \"levels\": %d, \"nodes\": %d, \"threads\": %d, "
-           "\"max_dt\": %.17e, \"cfl\": %.17e, \"time_step_method\": %d}\n",
+           "\"max_dt\": %.17e, \"cfl\": %.17e, \"time_step_method\": %d, "
+           "\"conversion_velocity\": %.17e, \"conversion_time\": %.17e, "
+           "\"conversion_dist\": %.17e}\n",
            N, steps, t_init, t_loop, steps > 0 ? (double)N * steps / t_loop : 0.0,
            GL_tentacles_level_max, nodes, threads, (double)_MAX_dt_, (double)_CFL_,
-           time_step_method);
+           time_step_method, (double)_conversion_velocity_, (double)_conversion_time_,
+           (double)_conversion_dist_);
     return 0;
 }

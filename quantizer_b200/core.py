@@ -99,6 +99,7 @@ def load() -> C.CDLL:
         "qz_multigrid": ([C.POINTER(Config), _P, _P, C.c_int, C.c_int], C.c_int),
         "qz_conjugate_gradient_multigrid": ([_P, _P, C.c_int, C.c_int], C.c_int),
         "qz_timestep": ([vp, _P], C.c_int),
+        "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -278,6 +279,14 @@ class Simulation:
         dt = C.c_double()
         _check(self.lib.qz_timestep(self.h, C.byref(dt)))
         return dt.value
+
+    def observables(self, potential_type: int = 0, units=None) -> dict:
+        """Energies and momentum (observables.c:661-696); units as qz_observables."""
+        out = np.zeros(6)
+        u = None if units is None else _p(np.ascontiguousarray(units, dtype=np.float64))
+        _check(self.lib.qz_observables(self.h, potential_type, u, _p(out)))
+        return {"kinetic": out[0], "potential": out[1], "total": out[2],
+                "momentum": out[3:6].copy()}
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))

@@ -2266,6 +2266,72 @@ __global__ void k_amr_gather(long n, LevelRefs R, const double *__restrict__ x,
     paz[i] = az;
 }
 
+// observables.c:205-424: m times the potential interpolated (CIC) at the
+// particle from its finest node; per-block partial sums (fixed order).
+__global__ void k_amr_pot_energy(long n, LevelRefs R, const double *__restrict__ x,
+                                 const double *__restrict__ y, const double *__restrict__ z,
+                                 const double *__restrict__ m, double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (i < n)
+    {
+        int l = R.nlev - 1;
+        int nd = -1;
+        for (; l > 0; l--)
+        {
+            nd = R.node_of[l][i];
+            if (nd >= 0)
+                break;
+        }
+        if (l == 0)
+            nd = 0;
+        const AmrNode N = R.nodes[l][nd];
+        const double sc = (double)(1 << N.lv);
+        const double px = x[i] * sc, py = y[i] * sc, pz = z[i] * sc;
+        const int fx = (int)px, fy = (int)py, fz = (int)pz;
+        const double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+        const double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+        double w[8];
+        w[0] = wx2 * wy2 * wz2;
+        w[1] = wx1 * wy2 * wz2;
+        w[2] = wx2 * wy1 * wz2;
+        w[3] = wx1 * wy1 * wz2;
+        w[4] = wx2 * wy2 * wz1;
+        w[5] = wx1 * wy2 * wz1;
+        w[6] = wx2 * wy1 * wz1;
+        w[7] = wx1 * wy1 * wz1;
+        const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
+        const long g = grid_index(N, fx - N.ts[0], fy - N.ts[1], fz - N.ts[2]);
+        const double *pot = R.ax[l];
+        double a = 0.0;
+        for (int kk = 0; kk < 2; kk++)
+            for (int jj = 0; jj < 2; jj++)
+                for (int ii = 0; ii < 2; ii++)
+                    a += pot[g + ii + jj * sx + kk * sxy] * w[ii + 2 * jj + 4 * kk];
+        e = m[i] * a;
+    }
+    const double t = block_sum_d(e, sh);
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = t;
+}
+
+int amr_pot_energy_partials(qz_sim *s, double *part)
+{
+    LevelRefs R{};
+    R.nlev = s->amr_nlev;
+    for (int l = 0; l < s->amr_nlev; l++)
+    {
+        R.nodes[l] = s->amr[l].nodes.p;
+        R.node_of[l] = s->node_of[l].p;
+        R.ax[l] = s->amr[l].pot;
+    }
+    launch(s, QZ_PROF_OTHER, 96.0 * s->n, k_amr_pot_energy, dim3(blocks_for(s->n, 256)),
+           dim3(256), s->n, R, s->x, s->y, s->z, s->m, part);
+    return check_cuda(cudaGetLastError(), "potential energy") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 int amr_gather(qz_sim *s)
 {
     if (s->n == 0)

@@ -43,6 +43,9 @@ static struct {
     int *cycle, *check_every, *max_iter, *check_method, *head_pot_method, *force_stencil;
     int *branch_cg_cells, *branch_sweeps;
     double *w_sor_branch, *cfl, *max_dt;
+    double *conv_velocity, *conv_time, *conv_dist, *cm_vx, *cm_vy, *cm_vz;
+    double **energies, **momentum;
+    int *pe_type;
     int *time_step_method;
     double *w_sor_head, *tol, *tol2;
     int resolved;
@@ -104,6 +107,15 @@ static int resolve(void)
     R.cfl = need("_CFL_", &ok);
     R.max_dt = need("_MAX_dt_", &ok);
     R.time_step_method = need("time_step_method", &ok);
+    R.conv_velocity = need("_conversion_velocity_", &ok);
+    R.conv_time = need("_conversion_time_", &ok);
+    R.conv_dist = need("_conversion_dist_", &ok);
+    R.cm_vx = need("GL_cm_vx", &ok);
+    R.cm_vy = need("GL_cm_vy", &ok);
+    R.cm_vz = need("GL_cm_vz", &ok);
+    R.energies = need("GL_energies", &ok);
+    R.momentum = need("GL_momentum", &ok);
+    R.pe_type = need("potential_energy_type", &ok);
     R.w_sor_head = need("_w_SOR_HEAD_", &ok);
     R.tol = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_", &ok);
     R.tol2 = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_2", &ok);
@@ -277,6 +289,29 @@ int timestep(double *ptr_dt)
         return REF_FAILURE;
     if (qz_timestep(g_sim, ptr_dt))
         return fail("timestep");
+    return REF_SUCCESS;
+}
+
+/* observables.c:661-696: energies into GL_energies, momentum into GL_momentum */
+int observables(void)
+{
+    if (ensure())
+        return REF_FAILURE;
+    const double units[6] = {*R.conv_velocity, *R.conv_time, *R.conv_dist,
+                             *R.cm_vx, *R.cm_vy, *R.cm_vz};
+    double out[6];
+    if (*R.pe_type != 0 && *R.pe_type != 1)
+    {
+        printf("Error, the potential_energy_type value is different of 0 or 1\n");
+        return REF_FAILURE;
+    }
+    if (qz_observables(g_sim, *R.pe_type, units, out))
+        return fail("observables");
+    for (int k = 0; k < 3; k++)
+    {
+        (*R.energies)[k] = out[k];
+        (*R.momentum)[k] = out[3 + k];
+    }
     return REF_SUCCESS;
 }
 
