@@ -261,7 +261,10 @@ static int check_flags(qz_sim *s)
     if (e)
     {
         cudaMemsetAsync(s->flags + F_ERROR, 0, sizeof(int), s->stream);
-        set_error("device bounds check failed (flags 0x%x): a particle left the unit box", e);
+        if (e & E_BARRIER)
+            set_error("a grid barrier wait in a cooperative kernel gave up (flags 0x%x)", e);
+        else
+            set_error("device bounds check failed (flags 0x%x): a particle left the unit box", e);
         return QZ_FAILURE;
     }
     return QZ_SUCCESS;
@@ -345,7 +348,8 @@ int qz_destroy(qz_sim *s)
     void *ptrs[] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->m,
                     s->pot, s->pot_old, s->d, s->gax, s->gay, s->gaz, s->sort.k0, s->sort.k1,
                     s->sort.v0, s->sort.v1, s->sort.hist, s->seg_head, s->seg_id, s->seg_start,
-                    s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags, s->d_ts};
+                    s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags, s->d_ts,
+                    s->gbar};
     for (void *p : ptrs)
         dfree(p);
     free_levels(s);
@@ -451,6 +455,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     s->red_blocks = 296;
     ok = ok && dmalloc(&s->red, s->red_blocks + 8, "red") && dmalloc(&s->flags, F_COUNT, "flags");
     ok = ok && check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned");
+    ok = ok && dmalloc(&s->gbar, 4, "grid barrier");
     ok = ok && check_cuda(cudaMallocHost((void **)&s->h_ts, 34 * sizeof(unsigned long long)),
                           "pinned time step") &&
          dmalloc(&s->d_ts, 17, "time step");
@@ -854,12 +859,14 @@ static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, 
     cudaGetDevice(&s->device);
     size_t pts = (size_t)gridsize * gridsize * gridsize;
     if (!check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream") ||
-        !make_pool(s) || !dmalloc(dphi, pts, "phi") || !dmalloc(drho, pts, "rho") ||
+        !make_pool(s) || !dmalloc(&s->gbar, 4, "grid barrier") ||
+        !dmalloc(&s->flags, F_COUNT, "flags") || !dmalloc(dphi, pts, "phi") || !dmalloc(drho, pts, "rho") ||
         !check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned"))
     {
         qz_destroy(s);
         return nullptr;
     }
+    cudaMemset(s->flags, 0, F_COUNT * sizeof(int));
     s->fine_phi = dense_view(*dphi, gridsize);
     s->fine_rho = dense_view(*drho, gridsize);
     if (!build_levels(s, gridsize) || !dmalloc(&s->fine_alt_buf, pts, "phi alt"))
@@ -887,6 +894,8 @@ static int run_dense(const qz_config *cfg, double *phi, const double *rho, int g
     int rc = (h2d(s, dphi, phi, pts) && h2d(s, drho, rho, pts)) ? body(s, arg) : QZ_FAILURE;
     if (rc == QZ_SUCCESS && !d2h(s, phi, dphi, pts))
         rc = QZ_FAILURE;
+    if (rc == QZ_SUCCESS)
+        rc = check_flags(s);
     dfree(dphi);
     dfree(drho);
     qz_destroy(s);

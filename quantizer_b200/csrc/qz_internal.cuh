@@ -52,7 +52,70 @@ enum Flag {
     F_AMR_CONV = 5,   // refinement nodes converged in the current level solve
     F_COUNT = 8
 };
-enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2 };
+enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2, E_BARRIER = 8 };
+
+// Grid-wide barrier of a cooperative launch with bounded waits.  word[0]
+// counts arrivals, word[1] is the generation, word[2] is set once a wait of
+// this launch gave up; word[0] and word[2] must be zero at launch.  The last
+// block to arrive resets the count and advances the generation after a fence;
+// the others poll the generation with acquire loads.  A wait that hits the
+// poll limit sets word[2] and E_BARRIER in flags[F_ERROR]; from then on every
+// barrier of the launch returns false at once, so the kernel finishes.
+constexpr int GBAR_POLL_LIMIT = 1 << 21;
+
+struct GridBar {
+    unsigned *word;
+    int *flags;
+};
+
+__device__ __forceinline__ unsigned gbar_ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool gbar_sync(const GridBar &B, int *sh_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int ok = gbar_ld_acquire(&B.word[2]) == 0;
+        if (ok)
+        {
+            const unsigned gen = gbar_ld_acquire(&B.word[1]);
+            __threadfence(); // this block's writes before its arrival
+            const unsigned prev = atomicAdd(&B.word[0], 1u);
+            if (prev == gridDim.x - 1)
+            {
+                atomicExch(&B.word[0], 0u);
+                __threadfence();
+                atomicAdd(&B.word[1], 1u);
+            }
+            else
+            {
+                int polls = 0;
+                while (gbar_ld_acquire(&B.word[1]) == gen)
+                {
+                    if (++polls > GBAR_POLL_LIMIT || gbar_ld_acquire(&B.word[2]) != 0)
+                    {
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        if (!ok)
+        {
+            atomicExch(&B.word[2], 1u);
+            atomicOr(&B.flags[F_ERROR], E_BARRIER);
+        }
+        __threadfence();
+        *sh_ok = ok;
+    }
+    __syncthreads();
+    return *sh_ok != 0;
+}
 
 struct Sort {
     // Stable LSD radix sort of (uint32 key, int32 value) pairs.
@@ -185,6 +248,7 @@ struct qz_sim {
     cudaStream_t stream = nullptr;
     qz::MemCtx mem; // stream-ordered pool for buffers that grow during a run
     double *cg_part = nullptr; // conjugate-gradient smoothing: 2 x QZ_CG_PART_MAX partial sums
+    unsigned *gbar = nullptr;  // grid barrier words of the cooperative launches (4)
     long n = 0, cap = 0;
     double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *m = nullptr;

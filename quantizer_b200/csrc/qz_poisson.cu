@@ -337,13 +337,13 @@ __global__ void k_prolong_add(Grid<T> phi, Grid<T> c)
 // block adds its points' contributions in a fixed order, and after a grid
 // barrier every block adds the block partials in block order, so all blocks hold
 // the same sums (FP64) and take the same early exit.
-namespace cgs = cooperative_groups;
 
 template <typename T> struct CgsArgs {
     Grid<T> phi, rho;
     T *r, *p, *ap; // dense n^3, zero on the boundary
     double *part;  // 2 * gridDim partial sums
     int iters;
+    GridBar bar;
 };
 
 __device__ __forceinline__ double cgs_block_sum(double v, double *sh)
@@ -371,8 +371,8 @@ __device__ __forceinline__ double cgs_grid_sum(const double *part, double *sh)
 
 template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs<T> A)
 {
-    cgs::grid_group grid = cgs::this_grid();
     __shared__ double sh[32];
+    __shared__ int sh_ok;
     const int n = A.phi.n, m = n - 2;
     const unsigned um = (unsigned)m, total = um * um * um;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
@@ -398,7 +398,7 @@ template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs
     double b = cgs_block_sum(acc, sh);
     if (threadIdx.x == 0)
         part0[blockIdx.x] = b;
-    grid.sync();
+    gbar_sync(A.bar, &sh_ok);
     double rsold = cgs_grid_sum(part0, sh);
     const long cap = (long)m * m * m;
     const long cycle = A.iters < cap ? A.iters : cap;
@@ -418,7 +418,7 @@ template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs
         b = cgs_block_sum(acc, sh);
         if (threadIdx.x == 0)
             part1[blockIdx.x] = b;
-        grid.sync();
+        gbar_sync(A.bar, &sh_ok);
         const T alpha = (T)(rsold / cgs_grid_sum(part1, sh));
         acc = 0.0;
         for (unsigned t = gtid; t < total; t += gn)
@@ -433,7 +433,7 @@ template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs
         b = cgs_block_sum(acc, sh);
         if (threadIdx.x == 0)
             part0[blockIdx.x] = b;
-        grid.sync();
+        gbar_sync(A.bar, &sh_ok);
         const double rsnew = cgs_grid_sum(part0, sh);
         if (rsnew / rsold < 1.0e-16)
             break;
@@ -445,7 +445,7 @@ template <typename T> __global__ void __launch_bounds__(256) k_cg_smooth(CgsArgs
             A.p[l] = A.r[l] + beta * A.p[l];
         }
         rsold = rsnew;
-        grid.sync();
+        gbar_sync(A.bar, &sh_ok);
     }
 }
 
@@ -540,6 +540,8 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
         A.ap = cgs_scratch.ap;
         A.part = s->cg_part;
         A.iters = iters;
+        A.bar = GridBar{s->gbar, s->flags};
+        cudaMemsetAsync(s->gbar, 0, 4 * sizeof(unsigned), s->stream);
         static int per_sm[2] = {0, 0};
         static std::once_flag once;
         std::call_once(once, [] {
@@ -729,7 +731,6 @@ int vcycle(qz_sim *s, int level, int type) { return vcycle_t<double>(s, level, t
 // only what earlier phases wrote), so the result equals the launch-per-phase
 // path bit for bit.  In the mixed-precision form a launch also holds the FP64
 // fine residual and the FP64 correction of each iteration.
-namespace cgm = cooperative_groups;
 
 constexpr int MG_MAXLEV = 12;
 constexpr int MG_SMALL_N = 17;
@@ -747,6 +748,7 @@ template <typename T> struct MgArgs {
     Grid<double> fphi, frho; // FP64 fine grid (mixed form): phi[0] / rho[0] are ef / rf
     int smem;                // the small levels live in block 0's shared memory
     int soff[MG_MAXLEV];     // their offsets there (phi, then rho), in elements
+    GridBar bar;
 };
 
 // One colour of a red-black sweep over work items t = tid, tid + nthr, ...
@@ -895,10 +897,10 @@ __device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsi
 template <typename T>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant__ MgArgs<T> A)
 {
-    cgm::grid_group grid = cgm::this_grid();
     extern __shared__ __align__(16) unsigned char mg_dyn[];
+    __shared__ int sh_ok;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
-    auto gsync = [&]() { grid.sync(); };
+    auto gsync = [&]() { gbar_sync(A.bar, &sh_ok); };
     auto bsync = [&]() { __syncthreads(); };
     for (int it = 0; it < A.iters; it++)
     {
@@ -922,7 +924,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
                                                    p[gp - P.sy] - p[gp + P.sz] - p[gp - P.sz]);
                 rf[i + (long)j * n + (long)k * n * n] = (float)r;
             }
-            grid.sync();
+            gsync();
         }
         // levels above the small ones: grid-wide phases
         for (int l = 0; l < A.nsmall; l++)
@@ -931,7 +933,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             const int n = A.phi[l].n;
             mg_restrict(A.phi[l], A.rho[l], A.phi[l + 1], A.rho[l + 1], (T)(double)((n - 1) * (n - 1)),
                         A.scale, gtid, gn);
-            grid.sync();
+            gsync();
         }
         // the small levels: a whole sub-cycle inside block 0, in its shared memory
         // when they fit (the first small level is copied in and its correction out)
@@ -978,11 +980,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             if (A.smem)
                 mg_copy(P(A.nsmall), A.phi[A.nsmall], bt, bn);
         }
-        grid.sync();
+        gsync();
         for (int l = A.nsmall - 1; l >= 0; l--)
         {
             mg_prolong(A.phi[l], A.phi[l + 1], gtid, gn);
-            grid.sync();
+            gsync();
             mg_smooth(A, l, A.n_post, gtid, gn, gsync);
         }
         if (A.mixed)
@@ -996,7 +998,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
                 const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
                 P.p[P.off + i + j * P.sy + k * P.sz] += (double)ef[i + (long)j * n + (long)k * n * n];
             }
-            grid.sync();
+            gsync();
         }
     }
 }
@@ -1034,6 +1036,8 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     A.mixed = std::is_same<T, float>::value ? 1 : 0;
     A.fphi = s->fine_phi;
     A.frho = s->fine_rho;
+    A.bar = GridBar{s->gbar, s->flags};
+    cudaMemsetAsync(s->gbar, 0, 4 * sizeof(unsigned), s->stream);
     // shared memory for the small levels (phi and rho of each)
     long elems = 0;
     for (int l = A.nsmall; l < A.nlev; l++)
@@ -1367,6 +1371,11 @@ int potential_head(qz_sim *s)
                 if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
                     return QZ_FAILURE;
                 check = s->h_flags[F_CONVERGED] != 0;
+                if (s->h_flags[F_ERROR] & E_BARRIER)
+                {
+                    set_error("multigrid cycles: a grid barrier wait gave up");
+                    return QZ_FAILURE;
+                }
             }
         }
     }
