@@ -100,6 +100,7 @@ def load() -> C.CDLL:
         "qz_conjugate_gradient_multigrid": ([_P, _P, C.c_int, C.c_int], C.c_int),
         "qz_timestep": ([vp, _P], C.c_int),
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
+        "qz_ensemble_step": ([C.POINTER(vp), C.c_int, C.c_double, C.c_int, C.c_int], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -316,6 +317,12 @@ class Simulation:
 
 
 # -- array-level routines ---------------------------------------------------------------
+def ensemble_step(sims: list, dt: float, nsteps: int = 1, threads: int = 8) -> None:
+    """Steps independent Simulations concurrently (qz_ensemble_step)."""
+    arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
+    _check(load().qz_ensemble_step(arr, len(sims), dt, nsteps, threads))
+
+
 def gauss_saidel(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0,
                  order: int = QZ_GS_REDBLACK) -> np.ndarray:
     n = round(phi.size ** (1 / 3))

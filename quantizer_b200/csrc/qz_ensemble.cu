@@ -1,0 +1,82 @@
+// qz_ensemble.cu -- the batching form: many independent simulations (for
+// example an ensemble of initial conditions) stepped together on one GPU.
+//
+// One simulation's step is a chain of short kernels and a few host
+// synchronisations (tree sizes, convergence checks); on its own it leaves most
+// of the GPU idle.  Every qz_sim owns its stream and memory pool, so the
+// simulations of an ensemble are stepped concurrently by a pool of host
+// threads: each thread takes the next simulation (atomic counter) and runs its
+// steps, and the chains of different simulations overlap on the GPU.  Every
+// simulation computes exactly what it computes alone (its kernels and their
+// order are unchanged), so results do not depend on the number of threads.
+#include <atomic>
+#include <mutex>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "qz_internal.cuh"
+
+using namespace qz;
+
+extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, double dt, int nsteps,
+                                       int nthreads)
+{
+    if (!sims || nsims < 0 || nsteps < 0)
+    {
+        set_error("qz_ensemble_step: bad arguments");
+        return QZ_FAILURE;
+    }
+    for (int k = 0; k < nsims; k++)
+        if (!sims[k])
+        {
+            set_error("qz_ensemble_step: simulation %d is null", k);
+            return QZ_FAILURE;
+        }
+    if (nthreads < 1)
+        nthreads = 1;
+    if (nthreads > nsims)
+        nthreads = nsims > 0 ? nsims : 1;
+    std::atomic<int> next{0};
+    std::atomic<int> failed{-1};
+    std::mutex mu;
+    std::string first_error;
+    auto worker = [&]() {
+        for (;;)
+        {
+            const int k = next.fetch_add(1);
+            if (k >= nsims || failed.load() >= 0)
+                return;
+            qz_sim *s = sims[k];
+            int rc = cudaSetDevice(s->device) == cudaSuccess ? QZ_SUCCESS : QZ_FAILURE;
+            if (rc == QZ_SUCCESS)
+                rc = qz_step(s, dt, nsteps);
+            if (rc == QZ_SUCCESS)
+                rc = qz_synchronize(s);
+            if (rc != QZ_SUCCESS)
+            {
+                int none = -1;
+                if (failed.compare_exchange_strong(none, k))
+                {
+                    std::lock_guard<std::mutex> lock(mu);
+                    first_error = qz_last_error();
+                }
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; t++)
+        pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool)
+        th.join();
+    if (failed.load() >= 0)
+    {
+        set_error("qz_ensemble_step: simulation %d: %s", failed.load(), first_error.c_str());
+        return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
