@@ -7,7 +7,11 @@ A step is one leapfrog step of QUANTIZER's main loop (main.c:375-481 with a
 fixed dt): kick-drift, reset, refinement-tree rebuild, CIC deposit on every
 level, Poisson solves to the reference's thresholds (head multigrid, then the
 refinement levels by conjugate gradient), gradients, CIC gather from each
-particle's finest node, kick.  Metric: particle-steps/s.  The default workload
+particle's finest node, kick.  Metric: particle-steps/s.  Other workloads
+(--workload): the 4.2M-particle Hernquist merger on a 256^3 head with four
+refinement levels, and the 512-member batching form (ensemble512: value is
+the members stepped concurrently, beside the same members stepped one after
+another).  The default workload
 is the 1M-particle Plummer sphere on a 128^3 head with 3 refinement levels in
 FP64 (the reference's arithmetic); the mixed-precision form (FP32 head
 smoothing inside FP64 defect correction) is timed on the same workload and
@@ -58,7 +62,37 @@ WORKLOADS = {
     "plummer1m_head128_amr3": dict(n=1048576, a=0.02, lmin=7, levels=3, ref_ptcl=9, steps=100,
                                    precision=0, variant=1, cpu_steps=3, ref_steps=10),
 }
+WORKLOADS.update({
+    # two Hernquist spheres of N = 2,097,152 each (a = 0.03, truncated at r <= 0.14,
+    # centres 0.35 / 0.65 on x, approaching at half the mutual escape speed), head
+    # 256^3, refinement up to 4 levels above the head, FP64
+    "merger4m_head256_amr4": dict(ic="merger", n=2 * 2097152, a=0.03, lmin=8, levels=4,
+                                  ref_ptcl=9, steps=20, precision=0, cpu_steps=1,
+                                  ref_steps=1),
+    # batching form: 512 Plummer members, N log-uniform in [2048, 65536], a uniform in
+    # [0.02, 0.08], head 32^3 below N = 16384 else 64^3, two refinement levels, each
+    # member with dt = 1e-3 of its own crossing time; stepped concurrently
+    "ensemble512": dict(ic="ensemble", members=512, n=0, a=0.0, lmin=5, levels=2, ref_ptcl=9,
+                        steps=10, precision=0, cpu_steps=2, ref_steps=2, threads=16),
+})
 DEFAULT_WORKLOAD = "plummer1m_head128_amr3"
+
+
+def make_ic(wl: dict, seed: int) -> dict:
+    from quantizer_b200 import ics
+    if wl.get("ic") == "merger":
+        return ics.merger(wl["n"] // 2, a=wl["a"], seed=seed)
+    return ics.plummer(wl["n"], a=wl["a"], seed=seed)
+
+
+def ensemble_members(wl: dict, seed: int = 0) -> list:
+    """(n, a, lmin) of each ensemble member (seeded)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    m = wl["members"]
+    ns = np.exp(rng.uniform(np.log(2048.0), np.log(65536.0), m)).astype(int)
+    As = rng.uniform(0.02, 0.08, m)
+    return [(int(n), float(a), 5 if n < 16384 else 6) for n, a in zip(ns, As)]
 METRIC = "particle-steps/s"
 
 
@@ -137,7 +171,7 @@ def run_reference_cpu(wl: dict, steps: int, threads: int, seed: int) -> dict:
     from quantizer_b200 import ics
     if not os.path.exists(O.REF_DRIVER):
         return {"kind": "port"} | run_port_cpu(wl, steps, seed)
-    ic = ics.plummer(wl["n"], a=wl["a"], seed=seed)
+    ic = make_ic(wl, seed)
     dt = 1e-3 * ics.crossing_time(wl["a"])
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "ic.bin")
@@ -165,6 +199,120 @@ def run_port_cpu(wl: dict, steps: int, seed: int) -> dict:
     return {"value": wl["n"] * steps / t, "seconds": t, "steps": steps}
 
 
+def run_ensemble(args, wl: dict, K: int, W: int) -> int:
+    """The batching form: all members stepped together (qz_ensemble_step) against the
+    same members stepped one after another (one host thread, the single-instance
+    path).  Time = device makespan over the members' streams (CUDA events)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    members = ensemble_members(wl, seed=rank)
+    total = sum(n for n, _, _ in members)
+    config = {"workload": args.workload, "members": len(members), "particles": total,
+              "particles_per_member": "log-uniform in [2048, 65536]", "head_grid": "32 or 64",
+              "lmax_minus_lmin": wl["levels"], "refine_above_particles": wl["ref_ptcl"] - 1,
+              "dt": "1e-3 crossing time of each member", "precision": "fp64",
+              "threads": wl["threads"], "replicas": world,
+              "l2": "aggregate member state above L2, members interleave (no flush)"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = ensemble_reference(wl, members, min(K, wl["ref_steps"]), os.cpu_count() or 1)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": 0,
+                "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+                "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"],
+                                 "kind": "reference", "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    import torch
+    import torch.distributed as dist
+    from quantizer_b200 import core, ics
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sims, dts = [], []
+    for k, (n, a, lmin) in enumerate(members):
+        s = core.Simulation(ics.plummer(n, a=a, seed=1000 * rank + k), lmin,
+                            lmax=lmin + wl["levels"], ref_ptcl=wl["ref_ptcl"])
+        s.init_forces()
+        sims.append(s)
+        dts.append(1e-3 * ics.crossing_time(a))
+    streams = [torch.cuda.ExternalStream(s.stream, device=dev) for s in sims]
+
+    def makespan(fn) -> float:
+        starts, ends = [], []
+        for st in streams:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            starts.append(e)
+        fn()
+        for st in streams:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            ends.append(e)
+        torch.cuda.synchronize()
+        return max(starts[0].elapsed_time(e) for e in ends)
+
+    core.ensemble_step(sims, dts, W, threads=wl["threads"])
+    st0 = [s.stats() for s in sims]
+    with ClockSampler(local) as clk:
+        ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=wl["threads"]))
+    launches = sum(s.stats().kernel_launches - a.kernel_launches for s, a in zip(sims, st0))
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * total * K / (ms_max / 1e3)
+    Kl = min(K, 2)
+    ms_loop = makespan(lambda: core.ensemble_step(sims, dts, Kl, threads=1))
+    loop_value = total * Kl / (ms_loop / 1e3)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        r = ensemble_reference(wl, members[:4], wl["cpu_steps"], 1)
+        cpu = {"value": r["value"], "unit": METRIC, "cores": 1, "kind": "reference",
+               "sample": r["sample"]}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config, "e2e": None,
+                "single_instance_loop": {"value": loop_value, "steps": Kl,
+                                         "speedup_of_batching": value / world / loop_value},
+                "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    for s in sims:
+        s.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def ensemble_reference(wl: dict, members: list, steps: int, threads: int) -> dict:
+    """The reference on ensemble members one after another (host)."""
+    from oracle import oracle as O
+    from quantizer_b200 import ics
+    parts, secs = 0, 0.0
+    for k, (n, a, lmin) in enumerate(members):
+        ic = ics.plummer(n, a=a, seed=k)
+        with tempfile.TemporaryDirectory() as td:
+            p = os.path.join(td, "ic.bin")
+            ics.write_ic(p, ic)
+            r = O.run_reference(p, td, lmin=lmin, lmax=lmin + wl["levels"], ref_ptcl=wl["ref_ptcl"],
+                                steps=steps, dt=1e-3 * ics.crossing_time(a), threads=threads)
+        parts += n * steps
+        secs += r["loop_s"]
+    return {"value": parts / secs, "steps": steps, "cores": threads, "seconds": secs,
+            "sample": f"{len(members)} members x {steps} steps after their step-0 forces, "
+                      f"one after another, {threads} thread(s)"}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,6 +325,8 @@ def main() -> int:
     wl = WORKLOADS[args.workload]
     K = args.steps if args.steps is not None else wl["steps"]
     W = max(3, args.warmup)
+    if wl.get("ic") == "ensemble":
+        return run_ensemble(args, wl, K, W)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -224,7 +374,7 @@ def main() -> int:
             dist.barrier()
         torch.cuda.synchronize()
 
-    ic = ics.plummer(wl["n"], a=wl["a"], seed=1 + rank)
+    ic = make_ic(wl, 1 + rank)
     dt = 1e-3 * ics.crossing_time(wl["a"])
     simcfg = dict(lmax=wl["lmin"] + wl["levels"], ref_ptcl=wl["ref_ptcl"])
     sim = core.Simulation(ic, wl["lmin"], precision=wl["precision"], **simcfg)

@@ -92,6 +92,9 @@ typedef struct qz_config {
     double cfl;
     double max_dt;
     int time_step_method;
+    /* head solve: 0 multigrid cycles, 1 conjugate gradient (head_pot_method,
+     * potential_head_node.c:112-176) */
+    int head_pot_method;
 } qz_config;
 
 typedef struct qz_stats {
@@ -191,12 +194,13 @@ QZ_API int qz_step(qz_sim *sim, double dt, int nsteps);
  * finest node; reduced on the device (exact, order-independent min / max). */
 QZ_API int qz_timestep(qz_sim *sim, double *dt);
 
-/* Batching form: nsteps steps of each of nsims independent simulations (same
- * dt semantics as qz_step), stepped concurrently by nthreads host threads on
- * the simulations' own streams.  Each simulation's results equal those of
- * qz_step on it alone.  Returns the first failure (with its index in
- * qz_last_error). */
-QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, double dt, int nsteps, int nthreads);
+/* Batching form: nsteps steps of each of nsims independent simulations,
+ * member k with step dt[k] (qz_step's meaning; dt NULL: CFL steps for all),
+ * stepped concurrently by nthreads host threads on the simulations' own
+ * streams.  Each simulation's results equal those of qz_step on it alone.
+ * Returns the first failure (with its index in qz_last_error). */
+QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *dt, int nsteps,
+                            int nthreads);
 
 /* observables (observables.c:661-696): out[0] kinetic, out[1] potential,
  * out[2] total energy, out[3..5] momentum.  potential_type 0: exact sum over

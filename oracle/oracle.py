@@ -28,7 +28,7 @@ class Params(C.Structure):
         ("solver", C.c_int), ("cycle", C.c_int), ("n_pre", C.c_int), ("n_post", C.c_int),
         ("n_coarse", C.c_int), ("w_sor", C.c_double), ("tol", C.c_double), ("tol2", C.c_double),
         ("check_every", C.c_int), ("max_iter", C.c_int), ("check_method", C.c_int),
-        ("force_stencil", C.c_int),
+        ("force_stencil", C.c_int), ("head_pot_method", C.c_int),
     ]
 
 

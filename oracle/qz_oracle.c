@@ -39,6 +39,7 @@ void qzo_default_params(qzo_params *p, int L)
     p->max_iter = 5000;
     p->check_method = 0;
     p->force_stencil = 0;
+    p->head_pot_method = 0;
 }
 
 long qzo_grid_points(int L)
@@ -419,12 +420,124 @@ int qzo_poisson_check_head(const qzo_params *p, double *pot, double *pot_old, co
     return check;
 }
 
+/* conjugate_gradient.c:322-463 on the head (interior points of box
+ * coordinates 2..2^L, lexicographic, sums in that order): r = d + lap(pot)
+ * sign convention of the reference, p = r; each iteration Ap, alpha =
+ * rsold / (p.Ap), pot += alpha p, r -= alpha Ap, rsnew = r.r; every
+ * check_every iterations poisson_error type 1 (poisson_error.c:290-347:
+ * the pot/pot_old ratio test, then conj_grad_error poisson_error.c:235-282;
+ * pot_old <- pot when it fails); then p = r + rsnew/rsold p.  The cycle
+ * cap is min(grid points, max_iter). */
+int qzo_cg_head(const qzo_params *p, double *pot, double *pot_old, const double *d,
+                double node_mass)
+{
+    int nc = 1 << p->L;
+    long D = nc + 3, D2 = D * D, cap = D2 * D;
+    long nintr = (long)(nc - 1) * (nc - 1) * (nc - 1);
+    double H = 1.0 / (1 << p->L);
+    double oh2 = 1.0 / (H * H);
+    long *ix = (long *)malloc(nintr * sizeof(long));
+    long q = 0;
+    for (long k = 2; k <= nc; k++)
+        for (long j = 2; j <= nc; j++)
+            for (long i = 2; i <= nc; i++)
+                ix[q++] = i + j * D + k * D2;
+    double *r = (double *)calloc(cap, sizeof(double));
+    double *pv = (double *)calloc(cap, sizeof(double));
+    double *Ap = (double *)calloc(cap, sizeof(double));
+    double rsold = 0.0, rsnew = 0.0;
+    for (long t = 0; t < nintr; t++)
+    {
+        long g = ix[t];
+        r[g] = d[g] + oh2 * (6.0 * pot[g] - pot[g + 1] - pot[g - 1] - pot[g + D] - pot[g - D] -
+                             pot[g + D2] - pot[g - D2]);
+        pv[g] = r[g];
+        rsold += r[g] * r[g];
+    }
+    double rm = 4.0 * p->G * QZ_PI * node_mass / ((double)(nc * nc * nc) * H * H * H);
+    long cycle = cap < p->max_iter ? cap : p->max_iter;
+    int done = 0;
+    long it;
+    for (it = 0; it < cycle && !done; it++)
+    {
+        double pap = 0.0;
+        for (long t = 0; t < nintr; t++)
+        {
+            long g = ix[t];
+            Ap[g] = -oh2 * (6.0 * pv[g] - pv[g + 1] - pv[g - 1] - pv[g + D] - pv[g - D] -
+                            pv[g + D2] - pv[g - D2]);
+            pap += pv[g] * Ap[g];
+        }
+        double alpha = rsold / pap;
+        rsnew = 0.0;
+        for (long t = 0; t < nintr; t++)
+        {
+            long g = ix[t];
+            pot[g] += alpha * pv[g];
+            r[g] -= alpha * Ap[g];
+            rsnew += r[g] * r[g];
+        }
+        if ((it + 1) % p->check_every == 0)
+        {
+            int check = 1;
+            double tm = 1.0 - p->tol2, tp = 1.0 + p->tol2;
+            for (long t = 0; t < nintr; t++)
+            {
+                double a = pot[ix[t]] / pot_old[ix[t]];
+                if ((tm > a) || (tp < a))
+                {
+                    check = 0;
+                    break;
+                }
+            }
+            if (check)
+            {
+                if (p->check_method == 0)
+                    check = rsnew < nintr * (p->tol * rm) * (p->tol * rm);
+                else if (p->check_method == 1)
+                {
+                    for (long t = 0; t < nintr && check; t++)
+                        if (fabs(r[ix[t]]) / rm >= p->tol)
+                            check = 0;
+                }
+                else
+                    check = rsnew < nintr * (p->tol * rm) * (p->tol * rm) *
+                                        (cbrt((double)nintr) * cbrt((double)nintr));
+            }
+            if (check)
+            {
+                done = 1;
+                break;
+            }
+            memcpy(pot_old, pot, cap * sizeof(double));
+        }
+        for (long t = 0; t < nintr; t++)
+        {
+            long g = ix[t];
+            pv[g] = r[g] + rsnew / rsold * pv[g];
+        }
+        rsold = rsnew;
+    }
+    free(ix);
+    free(r);
+    free(pv);
+    free(Ap);
+    return done ? (int)(it + 1) : -(int)it;
+}
+
 /* potential_head_node.c:32-179: V-cycles on the solve grid (box points
  * 1..2^L+1 copied to an aux array and back), checked every check_every
- * cycles; returns the number of cycles, or -cycles when max_iter was hit. */
+ * cycles; returns the number of cycles, or -cycles when max_iter was hit.
+ * With head_pot_method 1 the node conjugate gradient instead
+ * (potential_head_node.c:157-171). */
 int qzo_potential_head(const qzo_params *p, double *pot, double *pot_old, double *d,
                        double node_mass)
 {
+    if (p->head_pot_method == 1)
+    {
+        memcpy(pot_old, pot, qzo_grid_points(p->L) * sizeof(double));
+        return qzo_cg_head(p, pot, pot_old, d, node_mass);
+    }
     int nc = 1 << p->L;
     long D = nc + 3, D2 = D * D, cap = D2 * D;
     int n = nc + 1;

@@ -36,6 +36,7 @@ typedef struct {
     int max_iter;        /* _MAX_NUMBER_OF_ITERATIONS_IN_POISSON_EQUATION_ */
     int check_method;    /* check_poisson_error_method 0/1/2 */
     int force_stencil;   /* 0 = 3-point, 1 = 5-point */
+    int head_pot_method; /* 0 multigrid cycles, 1 node conjugate gradient */
 } qzo_params;
 
 void qzo_default_params(qzo_params *p, int L);
@@ -61,7 +62,12 @@ void qzo_multigrid(const qzo_params *p, double *phi, const double *rho, int grid
 /* poisson_error.c:36-133 for the head node; returns 1 when converged. */
 int qzo_poisson_check_head(const qzo_params *p, double *pot, double *pot_old, const double *d,
                            double node_mass);
-/* potential_head_node.c:32-179; returns V-cycles used (negative on failure). */
+/* conjugate_gradient.c:322-463 on the head node with poisson_error.c:235-347
+ * (type 1); returns iterations used (negative on failure). */
+int qzo_cg_head(const qzo_params *p, double *pot, double *pot_old, const double *d,
+                double node_mass);
+/* potential_head_node.c:32-179; returns V-cycles (or conjugate gradient
+ * iterations) used, negative on failure. */
 int qzo_potential_head(const qzo_params *p, double *pot, double *pot_old, double *d,
                        double node_mass);
 /* grid_acceleration.c:36-76 (3-point) */

@@ -19,7 +19,8 @@
  *         stencil (force_stencil), branch_cg_cells (nodes of more cells use
  *         conjugate gradient, the others red-black SOR), tsm (time_step_method),
  *         cfl (_CFL_), max_dt (_MAX_dt_), obs (1: dump observables of both
- *         potential-energy forms as obs0 / obs1: energies[3], momentum[3])
+ *         potential-energy forms as obs0 / obs1: energies[3], momentum[3]),
+ *         check (check_poisson_error_method 0/1/2)
  * IC.bin: int64 N, then x[N] y[N] z[N] vx[N] vy[N] vz[N] m[N] (float64).
  * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles, and
  *        dtcfl: the reference's timestep() of that state),
@@ -219,6 +220,7 @@ int main(int argc, char **argv)
     double cfl = -1.0;      /* _CFL_ */
     double max_dt = -1.0;   /* _MAX_dt_ */
     int branch_cg_cells = -1; /* branches_maximal_node_number_to_activate_conjugate_gradient */
+    int check = -1;           /* check_poisson_error_method */
     double dt = 1e-4, G = 1.0;
     const char *dump = NULL;
     for (int a = 3; a < argc; a++)
@@ -247,6 +249,7 @@ int main(int argc, char **argv)
         else if (!strcmp(key, "max_dt")) max_dt = atof(v);
         else if (!strcmp(key, "obs")) g_obs = atoi(v);
         else if (!strcmp(key, "branch_cg_cells")) branch_cg_cells = atoi(v);
+        else if (!strcmp(key, "check")) check = atoi(v);
         else die("unknown key");
     }
     if (LMAX < 0)
@@ -286,6 +289,8 @@ int main(int argc, char **argv)
         _MAX_dt_ = max_dt;
     if (branch_cg_cells >= 0)
         branches_maximal_node_number_to_activate_conjugate_gradient = branch_cg_cells;
+    if (check >= 0)
+        check_poisson_error_method = check;
     NUMBER_OF_THEADS = threads;
     omp_set_num_threads(threads);
     bder_os_sim = 1 > n_exp ? 1 : n_exp;

@@ -39,7 +39,7 @@ class Config(C.Structure):
         ("inner_cycles", C.c_int), ("force_stencil", C.c_int), ("ref_ptcl", C.c_int),
         ("box_extra", C.c_int), ("branch_cg_cells", C.c_int), ("branch_sor_sweeps", C.c_int),
         ("w_sor_branch", C.c_double), ("cfl", C.c_double), ("max_dt", C.c_double),
-        ("time_step_method", C.c_int),
+        ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
     ]
 
 
@@ -100,7 +100,7 @@ def load() -> C.CDLL:
         "qz_conjugate_gradient_multigrid": ([_P, _P, C.c_int, C.c_int], C.c_int),
         "qz_timestep": ([vp, _P], C.c_int),
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
-        "qz_ensemble_step": ([C.POINTER(vp), C.c_int, C.c_double, C.c_int, C.c_int], C.c_int),
+        "qz_ensemble_step": ([C.POINTER(vp), C.c_int, _P, C.c_int, C.c_int], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -317,10 +317,15 @@ class Simulation:
 
 
 # -- array-level routines ---------------------------------------------------------------
-def ensemble_step(sims: list, dt: float, nsteps: int = 1, threads: int = 8) -> None:
-    """Steps independent Simulations concurrently (qz_ensemble_step)."""
+def ensemble_step(sims: list, dt, nsteps: int = 1, threads: int = 8) -> None:
+    """Steps independent Simulations concurrently (qz_ensemble_step); dt is one
+    step for all, one per member, or None for CFL steps."""
     arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
-    _check(load().qz_ensemble_step(arr, len(sims), dt, nsteps, threads))
+    if dt is None:
+        d = None
+    else:
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(sims),)))
+    _check(load().qz_ensemble_step(arr, len(sims), None if d is None else _p(d), nsteps, threads))
 
 
 def gauss_saidel(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0,

@@ -615,6 +615,7 @@ void amr_free(qz_sim *s)
 {
     for (auto &L : s->amr)
         free_level(s->mem, L);
+    free_level(s->mem, s->head_cg);
     s->amr.clear();
     for (auto &b : s->node_of)
         b.release(s->mem);
@@ -1327,12 +1328,13 @@ struct CgArgs {
     double *apv;     // Ap of the current iteration at the interior points
     double *pap[2];  // per chunk: partial p.Ap of iteration k in pap[k & 1]
     double *rr[2];   // per chunk: partial r_j.r_j in rr[j & 1]
-    int *rfail[2];   // per node: ratio test failed at check j, in rfail[j & 1]
+    int *rfail[2];   // per node: ratio (or, check_method 1, residual) test failed at check j, in rfail[j & 1]
     int *status;     // [0] most iterations of a node, [1] a wait gave up, [2] unconverged nodes
     int *iters;      // per node: iterations run
     double tol, tol2, G;
     int every;
     int max_iter;
+    int method; // check_method 0/1/2 of conj_grad_error (poisson_error.c:235-282)
 };
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
@@ -1382,7 +1384,9 @@ __device__ __forceinline__ void cg_load7(const double *v, int g, int sy, int sz,
 // A block's view of one of its chunks (shared memory).
 struct CgSlot {
     double oh2;     // 1 / H^2
-    double thr;     // residual threshold nintr * (tol * rm)^2 (poisson_error.c:236-254)
+    double thr;     // residual threshold of r.r: nintr (tol rm)^2, times cbrt(nintr)^2 for
+                    // check_method 2 (poisson_error.c:236-282)
+    double rm;      // 4 pi G rhomean of the node
     double rs_prev; // rs_{k-2} of the node
     double rs_cur;  // rs_{k-1} of the node
     int c, q, cb, ce; // chunk, node, node's chunk range
@@ -1484,7 +1488,10 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
         x.oh2 = 1.0 / (H * H);
         const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
         const double tt = A.tol * rm;
+        x.rm = rm;
         x.thr = N.nintr * tt * tt;
+        if (A.method == 2)
+            x.thr = x.thr * (cbrt((double)N.nintr) * cbrt((double)N.nintr));
         const long size = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
         x.cap = (int)(size < A.max_iter ? size : A.max_iter);
         x.rs_prev = x.rs_cur = 0.0;
@@ -1550,7 +1557,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             {
                 const int rf = __syncthreads_or(
                     threadIdx.x == 0 && __ldcg(&A.rfail[((k - 1) / A.every) & 1][x.q]));
-                if (!rf && rs1 < x.thr)
+                if (!rf && (A.method == 1 || rs1 < x.thr))
                 {
                     if (threadIdx.x == 0)
                     {
@@ -1639,6 +1646,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
         // Only this thread's own points are read (p_{k-1} and Ap stored by the P
         // phase, pot, r): their loads are issued before the wait for p.Ap.
         const bool check = k % A.every == 0;
+        const bool res1 = A.method == 1; // per-point residual test joins the ratio test
         const double *pn = pnew;
         const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
         cq = -1;
@@ -1694,7 +1702,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
                 if (check)
                 {
                     const double ratio = pv / olda;
-                    if ((tm > ratio) || (tp < ratio))
+                    if ((tm > ratio) || (tp < ratio) || (res1 && fabs(rv) / x.rm >= A.tol))
                         fail = 1;
                 }
             }
@@ -1708,7 +1716,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
                 if (check)
                 {
                     const double ratio = pv / oldb;
-                    if ((tm > ratio) || (tp < ratio))
+                    if ((tm > ratio) || (tp < ratio) || (res1 && fabs(rv) / x.rm >= A.tol))
                         fail = 1;
                 }
             }
@@ -1886,7 +1894,7 @@ static int sor_level(qz_sim *s, AmrLevel &L, int level_index, const std::vector<
     return check_cuda(cudaGetLastError(), "sor") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
-static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
+static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = true)
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
@@ -1917,7 +1925,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     {
         node_chunk[2 * q] = (int)L.hchunks.size();
         const AmrNode &N = L.h[q];
-        if (N.ncells > c.branch_cg_cells)
+        if (!allow_sor || N.ncells > c.branch_cg_cells)
             for (int b = N.intr_off; b < N.intr_off + N.nintr; b += chunk)
                 L.hchunks.push_back({q, b, std::min(b + chunk, N.intr_off + N.nintr)});
         else if (N.nintr > 0)
@@ -1980,6 +1988,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.G = c.G;
     A.every = c.check_every > 0 ? c.check_every : 1;
     A.max_iter = c.max_iter;
+    A.method = c.check_method;
     const int blocks = (int)std::min(max_blocks, (long)L.nchunks);
     const int nslot = (L.nchunks + blocks - 1) / blocks;
     A.chunk = chunk;
@@ -2071,6 +2080,65 @@ int amr_potential(qz_sim *s)
             return QZ_FAILURE;
     }
     return QZ_SUCCESS;
+}
+
+// ---- head solved by conjugate gradient (head_pot_method 1) ----------------------------------
+// potential_head_node.c:157-171: the head node's potential by the node conjugate
+// gradient (conjugate_gradient.c:322-463) instead of multigrid cycles.  The head
+// becomes a one-node level: grid (2^L+3)^3 with box_ts -1, interior list all
+// points of box coordinates 2..2^L in lexicographic order, mass the total mass,
+// 2^(3L) cells.
+__global__ void k_head_intr(int L, long D, int *__restrict__ out)
+{
+    const long m = (1L << L) - 1;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m * m * m)
+        return;
+    const long i = 2 + t % m, j = 2 + (t / m) % m, k = 2 + t / (m * m);
+    out[t] = (int)(i + j * D + k * D * D);
+}
+
+int head_cg_solve(qz_sim *s)
+{
+    AmrLevel &L = s->head_cg;
+    const int Lv = s->cfg.lmin;
+    const long m = (1L << Lv) - 1;
+    if (L.nnodes == 0)
+    {
+        AmrNode N{};
+        N.lv = Lv;
+        N.parent = -1;
+        for (int q = 0; q < 3; q++)
+        {
+            N.ts[q] = -1;
+            N.rd[q] = (1 << Lv) + 2;
+            N.bmin[q] = 0;
+            N.bmax[q] = (1 << Lv) - 1;
+        }
+        N.ncells = 1 << (3 * Lv);
+        N.intr_off = 0;
+        N.nintr = (int)(m * m * m);
+        N.contact = 1;
+        L.nnodes = 1;
+        L.h.assign(1, N);
+        L.intr_total = N.nintr;
+        L.grid_total = s->gpts;
+        if (!L.intr.ensure(s->mem, L.intr_total))
+        {
+            set_error("head conjugate gradient buffers");
+            return QZ_FAILURE;
+        }
+        launch(s, QZ_PROF_OTHER, 4.0 * L.intr_total, k_head_intr,
+               dim3(blocks_for(L.intr_total, 256)), dim3(256), Lv, s->D, L.intr.p);
+    }
+    L.h[0].mass = s->cfg.total_mass;
+    L.h[0].nptcl = (int)s->n;
+    if (!upload_nodes(s, L))
+        return QZ_FAILURE;
+    L.d = s->d;
+    L.pot = s->pot;
+    L.pot_old = s->pot_old;
+    return cg_level(s, L, 0, false);
 }
 
 // ---- gradient on refinement levels -------------------------------------------------------

@@ -7,6 +7,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+#include <vector>
+
 #include "qz_internal.cuh"
 
 namespace qz {
@@ -311,26 +314,39 @@ int qz_default_config(qz_config *c, int lmin)
     c->cfl = 0.5;              /* _CFL_, global_variables.c:291 */
     c->max_dt = 1.0e30;        /* _MAX_dt_ (0.005 Maxdt in the reference's units): no cap */
     c->time_step_method = 1;   /* global_variables.c:342 */
+    c->head_pot_method = 0;    /* global_variables.c (multigrid) */
     return QZ_SUCCESS;
 }
 
-// The simulation's stream-ordered pool: freed memory stays in the pool, so buffers
-// that grow with the refinement tree never wait for the device.
+// Stream-ordered pool of a device, shared by all simulations on it (created once,
+// kept until the process exits): freed memory stays in the pool, so buffers that
+// grow with the refinement tree never wait for the device.  One pool per
+// simulation would not scale to ensembles of hundreds of simulations.
 static bool make_pool(qz_sim *s)
 {
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = s->device;
-    if (!check_cuda(cudaMemPoolCreate(&s->mem.pool, &props), "memory pool"))
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)pools.size() <= s->device)
+        pools.resize(s->device + 1, nullptr);
+    if (!pools[s->device])
     {
-        s->mem.pool = nullptr;
-        return false;
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = s->device;
+        cudaMemPool_t p = nullptr;
+        if (!check_cuda(cudaMemPoolCreate(&p, &props), "memory pool"))
+            return false;
+        unsigned long long keep = ~0ULL;
+        if (!check_cuda(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep),
+                        "memory pool threshold"))
+            return false;
+        pools[s->device] = p;
     }
-    unsigned long long keep = ~0ULL;
+    s->mem.pool = pools[s->device];
     s->mem.stream = s->stream;
-    return check_cuda(cudaMemPoolSetAttribute(s->mem.pool, cudaMemPoolAttrReleaseThreshold, &keep),
-                      "memory pool threshold");
+    return true;
 }
 
 int qz_destroy(qz_sim *s)
@@ -359,7 +375,7 @@ int qz_destroy(qz_sim *s)
     if (s->stream)
         cudaStreamSynchronize(s->stream); // the pool frees are stream-ordered
     if (s->mem.pool)
-        cudaMemPoolDestroy(s->mem.pool);
+        cudaMemPoolTrimTo(s->mem.pool, 0); // unused memory back to the device
     if (s->h_flags)
         cudaFreeHost(s->h_flags);
     if (s->h_ts)
@@ -405,7 +421,8 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         return QZ_FAILURE;
     }
     if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 2 || cfg->cycle < 0 ||
-        cfg->cycle > 2 || n_capacity > (1L << 30))
+        cfg->cycle > 2 || cfg->head_pot_method < 0 || cfg->head_pot_method > 1 ||
+        n_capacity > (1L << 30))
     {
         set_error("qz_create: unsupported configuration");
         return QZ_FAILURE;

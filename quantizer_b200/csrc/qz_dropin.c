@@ -148,6 +148,7 @@ static void fill_config(qz_config *c)
     c->cfl = *R.cfl;
     c->max_dt = *R.max_dt;
     c->time_step_method = *R.time_step_method;
+    c->head_pot_method = *R.head_pot_method;
     const char *o = getenv("QZ_GS_ORDER");
     c->gs_order = (o && !strcmp(o, "lex")) ? QZ_GS_LEX : QZ_GS_REDBLACK;
     const char *p = getenv("QZ_PRECISION");
@@ -196,11 +197,11 @@ static int ensure(void)
         g_failed = 1;
         return REF_FAILURE;
     }
-    if (*R.head_pot_method != 0 || *R.solver_pre != *R.solver_post ||
+    if (*R.head_pot_method < 0 || *R.head_pot_method > 1 || *R.solver_pre != *R.solver_post ||
         *R.solver_pre != *R.solver_coarse || *R.solver_pre > 2)
     {
         printf("\nERROR (drop-in): head solver configuration not supported "
-               "(multigrid with one smoother for all stages only)\n");
+               "(multigrid with one smoother for all stages, or conjugate gradient)\n");
         g_failed = 1;
         return REF_FAILURE;
     }

@@ -21,7 +21,7 @@
 
 using namespace qz;
 
-extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, double dt, int nsteps,
+extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *dt, int nsteps,
                                        int nthreads)
 {
     if (!sims || nsims < 0 || nsteps < 0)
@@ -52,7 +52,7 @@ extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, double dt, int 
             qz_sim *s = sims[k];
             int rc = cudaSetDevice(s->device) == cudaSuccess ? QZ_SUCCESS : QZ_FAILURE;
             if (rc == QZ_SUCCESS)
-                rc = qz_step(s, dt, nsteps);
+                rc = qz_step(s, dt ? dt[k] : 0.0, nsteps);
             if (rc == QZ_SUCCESS)
                 rc = qz_synchronize(s);
             if (rc != QZ_SUCCESS)

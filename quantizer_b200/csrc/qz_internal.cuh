@@ -153,9 +153,10 @@ struct AmrChunk {
     int node, begin, end; // [begin, end) of the level's interior list, one node
 };
 
-// Stream-ordered allocation context of a simulation: a private memory pool that
-// keeps freed memory (release threshold at its maximum) and the stream the
-// simulation's work runs on, so that growing a buffer never synchronises the device.
+// Stream-ordered allocation context of a simulation: the device's memory pool
+// (shared by the simulations on the device; it keeps freed memory, release
+// threshold at its maximum) and the stream the simulation's work runs on, so
+// that growing a buffer never synchronises the device.
 struct MemCtx {
     cudaMemPool_t pool = nullptr;
     cudaStream_t stream = nullptr;
@@ -291,6 +292,7 @@ struct qz_sim {
 
     // refinement tree (lmax > lmin): levels[0] = head, rebuilt every step
     std::vector<qz::AmrLevel> amr;
+    qz::AmrLevel head_cg; // the head as a one-node level (head_pot_method 1)
     int amr_nlev = 1;                  // levels in use this step
     std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
     qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)
@@ -329,6 +331,7 @@ namespace qz {
 // ---- launch accounting and errors ------------------------------------------
 void set_error(const char *fmt, ...);
 int timestep_cfl(qz_sim *s, double *dt_out); // qz_observe.cu
+int head_cg_solve(qz_sim *s);                 // qz_amr.cu
 bool check_cuda(cudaError_t e, const char *what);
 #define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
 

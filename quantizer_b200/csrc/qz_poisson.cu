@@ -1354,6 +1354,8 @@ int potential_head(qz_sim *s)
     const qz_config &c = s->cfg;
     cudaMemcpyAsync(s->pot_old, s->pot, s->gpts * sizeof(double), cudaMemcpyDeviceToDevice,
                     s->stream);
+    if (c.head_pot_method == 1)
+        return head_cg_solve(s);
     sync_fine_alt(s);
     int iter = 0;
     bool check = false;

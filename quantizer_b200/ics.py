@@ -118,6 +118,20 @@ def hernquist(n: int, a: float = 0.03, M: float = 1.0, G: float = 1.0,
     }
 
 
+def merger(n_each: int, a: float = 0.03, M: float = 1.0, G: float = 1.0, seed: int = 0,
+           rmax: float = 0.14, sep: float = 0.3) -> dict:
+    """Two Hernquist spheres of mass M each, centred at 0.5 -/+ sep/2 on x and
+    approaching along x at half the mutual escape speed sqrt(2 G (2M) / sep)
+    (each moving at a quarter of it), truncated at rmax (per-particle mass
+    renormalised to M per sphere)."""
+    v = 0.25 * math.sqrt(2.0 * G * 2.0 * M / sep)
+    left = hernquist(n_each, a=a, M=M, G=G, seed=2 * seed, rmax=rmax,
+                     center=(0.5 - sep / 2, 0.5, 0.5), bulk_v=(v, 0.0, 0.0))
+    right = hernquist(n_each, a=a, M=M, G=G, seed=2 * seed + 1, rmax=rmax,
+                      center=(0.5 + sep / 2, 0.5, 0.5), bulk_v=(-v, 0.0, 0.0))
+    return {k: np.concatenate([left[k], right[k]]) for k in left}
+
+
 def crossing_time(a: float, M: float = 1.0, G: float = 1.0) -> float:
     rv = 16.0 * a / (3.0 * math.pi)
     return 2.0 * math.sqrt(2.0) * math.sqrt(rv ** 3 / (G * M))

@@ -49,5 +49,10 @@ def cgsmooth_golden():
 
 
 @pytest.fixture(scope="session")
+def cghead_golden():
+    return golden("head_L4_cghead.npz")
+
+
+@pytest.fixture(scope="session")
 def timestep_golden():
     return golden("timestep_head_L4.npz")

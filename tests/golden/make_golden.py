@@ -14,6 +14,8 @@ sources (oracle/Makefile, target ``ref``):
   (force_stencil = 1).
 * ``head_L4_cgsmooth.npz`` -- the head_L4 case, 2 steps, with conjugate
   gradient as the multigrid smoother (solver 2).
+* ``head_L4_cghead.npz`` -- the head_L4 case with the head solved by the node
+  conjugate gradient (head_pot_method = 1) instead of multigrid cycles.
 * ``timestep_head_L4.npz`` -- the reference's timestep() (methods 0 and 1) on the
   states of the head_L4 case at steps 0 and 3 (_MAX_dt_ set to 1 so that the CFL
   condition decides), with its _MAX_dt_ and _CFL_.
@@ -139,6 +141,7 @@ def main() -> None:
         ("head_L3_jacobi.npz", dict(steps=2, lmin=3, solver=1)),
         ("head_L4_stencil5.npz", dict(steps=3, lmin=4, stencil=1)),
         ("head_L4_cgsmooth.npz", dict(steps=2, lmin=4, solver=2)),
+        ("head_L4_cghead.npz", dict(steps=3, lmin=4, cg_head=1)),
     ]
     for name, kw in cases:
         if not want or name in want:

@@ -45,6 +45,7 @@ CASES = [
     ("rb", {}, 1e-9, 1e-9),
     ("rb", {"solver": 2}, 1e-9, 1e-9),
     ("lex", {"stencil": 1}, 1e-12, 1e-13),
+    ("rb", {"cg_head": 1}, 1e-9, 1e-9),
 ]
 
 

@@ -12,6 +12,11 @@ the compiled reference (oracle/_ref/qz_ref_driver) and its fixtures.
   point by point, the GPU in fixed block order, so the iterates agree to
   rounding: arrays 1e-10 of the max, head pipeline potential 1e-9,
   accelerations 1e-8, positions 1e-10 box units.
+* the head solved by the node conjugate gradient (head_pot_method 1,
+  potential_head_node.c:157-171, conjugate_gradient.c:322-463): head run
+  against the fixture with the cg-smoothing tolerances (the dot products are
+  added in a different order); a refinement run against the driver with the
+  same setting, tolerances of the refinement tests.
 * red-black SOR for refinement nodes of at most branch_cg_cells cells
   (potential_branches.c:460-512; here 6000 cells, so the level-1 node takes SOR
   and the larger ones CG): refinement run against the driver with the same
@@ -108,6 +113,74 @@ def test_cg_smoothing_head_pipeline(cgsmooth_golden):
         assert _rel(p[k], g[f"s{steps}_{k}"]) < 1e-8, k
     for k in ("x", "y", "z"):
         assert np.abs(p[k] - g[f"s{steps}_{k}"]).max() < 1e-10
+
+
+def test_cg_head_pipeline(cghead_golden):
+    g = cghead_golden
+    steps, dt = int(g["meta"][1]), float(g["meta"][2])
+    with core.Simulation(_ic(g), 4, head_pot_method=1) as sim:
+        sim.init_forces()
+        pot0 = sim.field("pot")
+        p0 = sim.particles()
+        sim.step(dt, steps)
+        p = sim.particles()
+        pot = sim.field("pot")
+    assert _rel(pot0, g["s0_pot"]) < 1e-9
+    assert _rel(pot, g[f"s{steps}_pot"]) < 1e-9
+    for k in ("ax", "ay", "az"):
+        assert _rel(p0[k], g[f"s0_{k}"]) < 1e-8, k
+        assert _rel(p[k], g[f"s{steps}_{k}"]) < 1e-8, k
+    for k in ("x", "y", "z"):
+        assert np.abs(p[k] - g[f"s{steps}_{k}"]).max() < 1e-10
+
+
+def test_cg_head_refinement(tmp_path):
+    n, a, lmin, lmax, rp, seed = 20000, 0.05, 5, 8, 9, 3
+    ic = ics.plummer(n, a=a, seed=seed)
+    dt = 1e-3 * ics.crossing_time(a)
+    steps = 3
+    icp = os.path.join(str(tmp_path), "ic.bin")
+    ics.write_ic(icp, ic)
+    O.run_reference(icp, str(tmp_path), steps=steps, dt=dt, dump=f"0,{steps}", lmin=lmin,
+                    lmax=lmax, ref_ptcl=rp, cg_head=1)
+    with core.Simulation(ic, lmin, lmax=lmax, ref_ptcl=rp, head_pot_method=1) as sim:
+        sim.init_forces()
+        pot0 = sim.field("pot")
+        p0 = sim.particles()
+        sim.step(dt, steps)
+        p = sim.particles()
+    assert _rel(pot0, O.read_dump(str(tmp_path), 0, "pot")) < 1e-9
+    for k in ("ax", "ay", "az"):
+        assert _rel(p0[k], O.read_dump(str(tmp_path), 0, k)) < 1e-6
+        assert _rel(p[k], O.read_dump(str(tmp_path), steps, k)) < 1e-6
+    for k in ("x", "y", "z"):
+        assert np.abs(p[k] - O.read_dump(str(tmp_path), steps, k)).max() < 1e-10
+
+
+@pytest.mark.parametrize("check", [1, 2])
+def test_cg_check_methods_refinement(tmp_path, check):
+    """conj_grad_error (poisson_error.c:235-282) with check_method 1 (every
+    interior residual below tol * 4 pi G rhomean) and 2 (the r.r threshold
+    times cbrt(nintr)^2), head and refinement nodes by conjugate gradient."""
+    n, a, lmin, lmax, rp, seed = 20000, 0.05, 5, 8, 9, 3
+    ic = ics.plummer(n, a=a, seed=seed)
+    dt = 1e-3 * ics.crossing_time(a)
+    steps = 2
+    icp = os.path.join(str(tmp_path), "ic.bin")
+    ics.write_ic(icp, ic)
+    O.run_reference(icp, str(tmp_path), steps=steps, dt=dt, dump=f"0,{steps}", lmin=lmin,
+                    lmax=lmax, ref_ptcl=rp, cg_head=1, check=check)
+    with core.Simulation(ic, lmin, lmax=lmax, ref_ptcl=rp, head_pot_method=1,
+                         check_method=check) as sim:
+        sim.init_forces()
+        pot0 = sim.field("pot")
+        sim.step(dt, steps)
+        p = sim.particles()
+    assert _rel(pot0, O.read_dump(str(tmp_path), 0, "pot")) < 1e-9
+    for k in ("ax", "ay", "az"):
+        assert _rel(p[k], O.read_dump(str(tmp_path), steps, k)) < 1e-6
+    for k in ("x", "y", "z"):
+        assert np.abs(p[k] - O.read_dump(str(tmp_path), steps, k)).max() < 1e-10
 
 
 def test_sor_for_small_refinement_nodes(tmp_path):

@@ -53,6 +53,11 @@ def test_head_pipeline_cg_smoothing_bit_exact(cgsmooth_golden):
     _assert_exact(cgsmooth_golden, steps, s0, s1)
 
 
+def test_head_pipeline_cg_head_bit_exact(cghead_golden):
+    steps, s0, s1 = _run(cghead_golden, 4, head_pot_method=1)
+    _assert_exact(cghead_golden, steps, s0, s1)
+
+
 def test_cg_smoother_bit_exact(arrays_golden):
     g = arrays_golden
     lib = O.load()
