@@ -74,6 +74,14 @@ WORKLOADS.update({
     # member with dt = 1e-3 of its own crossing time; stepped concurrently
     "ensemble512": dict(ic="ensemble", members=512, n=0, a=0.0, lmin=5, levels=2, ref_ptcl=9,
                         steps=10, precision=0, cpu_steps=2, ref_steps=2, threads=16),
+    # differentiation form: Plummer N = 262,144, a = 0.04, head 128^3 with the tree fixed
+    # to the head node, FP64, 200 steps; loss = mean squared distance of the final
+    # positions to targets from a forward run of ICs perturbed by N(0, 1e-3^2);
+    # gradients with respect to x0, v0, m with a checkpoint every 20 steps, checked
+    # against central differences on 64 random coordinates
+    "adjoint262k_head128": dict(ic="adjoint", n=262144, a=0.04, lmin=7, levels=0, ref_ptcl=9,
+                                steps=200, precision=0, cpu_steps=2, ref_steps=2, every=20,
+                                fd_coords=64, tol=1e-11),
 })
 DEFAULT_WORKLOAD = "plummer1m_head128_amr3"
 
@@ -294,6 +302,151 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     return 0
 
 
+def run_adjoint(args, wl: dict, K: int, W: int) -> int:
+    """Differentiation form: a plain forward of K steps against the gradient of the
+    final-position loss (forward with checkpoints + reverse sweep), both device
+    time (CUDA events); the gradient is checked against central differences of the
+    forward on random coordinates (positions and velocities eps = 1e-6 box units,
+    masses eps = 1e-3 m_p)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": args.workload, "particles": wl["n"], "head_grid": 2 ** wl["lmin"],
+              "tree": "head node only (fixed)", "dt": "1e-3 crossing time", "precision": "fp64",
+              "residual_tol": wl["tol"], "adjoint_tol": wl["tol"],
+              "checkpoint_every": wl["every"], "loss": "mean_p |x_T - x*_T|^2",
+              "targets": "forward run of ICs perturbed by N(0, 1e-3^2) in x, y, z",
+              "replicas": world}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        r = run_reference_cpu(wl, min(K, wl["ref_steps"]), threads, seed=1)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": 0,
+                "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config, "note": "the reference has no adjoint: its forward only",
+                "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": threads,
+                                 "kind": "reference", "sample": f"{r['steps']} forward steps"},
+                "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from quantizer_b200 import core, ics
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, L = wl["n"], wl["lmin"]
+    cfg = dict(tol=wl["tol"], tol2=wl["tol"], adjoint_tol=wl["tol"])
+    ic = ics.plummer(n, a=wl["a"], seed=1 + rank)
+    dt = 1e-3 * ics.crossing_time(wl["a"])
+    rng = np.random.default_rng(100 + rank)
+    pert = {k: v.copy() for k, v in ic.items()}
+    for k in ("x", "y", "z"):
+        pert[k] = pert[k] + rng.normal(0.0, 1e-3, n)
+
+    def forward(c, steps):
+        with core.Simulation(c, L, **cfg) as sm:
+            sm.init_forces()
+            sm.step(dt, steps)
+            return sm.particles()
+
+    pt = forward(pert, K)
+    tgt = {k: pt[k] for k in ("x", "y", "z")}
+
+    def loss_of(c):
+        p = forward(c, K)
+        d = sum((p[k] - tgt[k]) ** 2 for k in ("x", "y", "z"))
+        return float(d.sum() / n)
+
+    # plain forward timing (warm-up runs first, then W+1 timed repetitions; the median)
+    sim = core.Simulation(ic, L, **cfg)
+    ext = torch.cuda.ExternalStream(sim.stream, device=dev)
+    fwd_ms = []
+    for rep_i in range(W + 1):
+        sim.set_particles(ic)
+        sim.init_forces()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        sim.step(dt, K)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        if rep_i > 0 or W == 0:
+            fwd_ms.append(e0.elapsed_time(e1))
+    forward_ms = statistics.median(fwd_ms)
+    # gradient (after one untimed warm-up call)
+    runs = []
+    st0 = sim.stats()
+    with ClockSampler(local) as clk:
+        for rep_i in range(2):
+            sim.set_particles(ic)
+            sim.init_forces()
+            g = sim.adjoint_final_loss(K, dt, tgt, checkpoint_every=wl["every"])
+            runs.append(g["stats"])
+    st1 = sim.stats()
+    sa = runs[-1]
+    adj_ms = sa["forward_ms"] + sa["reverse_ms"]
+    t = torch.tensor([adj_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    adj_ms_max = float(t.item())
+    free, total_mem = torch.cuda.mem_get_info(dev)
+    # finite differences on random coordinates
+    kinds = [("x", "gx", 1e-6)] * 12 + [("y", "gy", 1e-6)] * 6 + [("z", "gz", 1e-6)] * 6 + \
+            [("vx", "gvx", 1e-6)] * 8 + [("vy", "gvy", 1e-6)] * 8 + [("vz", "gvz", 1e-6)] * 8 + \
+            [("m", "gm", None)] * 16
+    kinds = kinds[:wl["fd_coords"]]
+    picks = rng.choice(n, len(kinds), replace=False)
+    errs, rels = [], []
+    for (field, key, eps), p in zip(kinds, picks):
+        h = eps if eps is not None else 1e-3 * ic["m"][p]
+        cp, cm = {k: v.copy() for k, v in ic.items()}, {k: v.copy() for k, v in ic.items()}
+        cp[field][p] += h
+        cm[field][p] -= h
+        fd = (loss_of(cp) - loss_of(cm)) / (2 * h)
+        scale = float(np.abs(g[key]).max())
+        errs.append(abs(fd - g[key][p]) / scale)
+        rels.append(abs(fd - g[key][p]) / max(abs(fd), 1e-300))
+    sim.close()
+    value = world * n * K / (adj_ms_max / 1e3)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": adj_ms_max / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config, "e2e": None,
+                "adjoint": {"forward_ms": forward_ms, "gradient_ms": adj_ms,
+                            "gradient_over_forward": adj_ms / forward_ms,
+                            "reverse_over_forward": sa["reverse_ms"] / forward_ms,
+                            "checkpointed_forward_ms": sa["forward_ms"],
+                            "reverse_ms": sa["reverse_ms"],
+                            "adjoint_cycles_per_step": sa["adjoint_cycles"] / K,
+                            "recomputed_steps": sa["recomputed_steps"],
+                            "checkpoints": sa["checkpoints"],
+                            "pool_peak_bytes": sa["pool_peak_bytes"],
+                            "stored_state_bytes": sa["stored_bytes"],
+                            "device_bytes_in_use_after": total_mem - free,
+                            "loss": runs[-1]["loss"]},
+                "finite_differences": {"coords": len(kinds),
+                                       "max_err_over_gradient_max": float(max(errs)),
+                                       "median_err_over_gradient_max": float(np.median(errs)),
+                                       "median_rel_err": float(np.median(rels)),
+                                       "max_rel_err": float(max(rels)),
+                                       "eps": "1e-6 (x, v), 1e-3 m_p (m)"},
+                "gpu_launches": int(st1.kernel_launches - st0.kernel_launches) // 2,
+                "clocks": clk.summary(), "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def ensemble_reference(wl: dict, members: list, steps: int, threads: int) -> dict:
     """The reference on ensemble members one after another (host)."""
     from oracle import oracle as O
@@ -327,6 +480,8 @@ def main() -> int:
     W = max(3, args.warmup)
     if wl.get("ic") == "ensemble":
         return run_ensemble(args, wl, K, W)
+    if wl.get("ic") == "adjoint":
+        return run_adjoint(args, wl, K, W)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -95,6 +95,9 @@ typedef struct qz_config {
     /* head solve: 0 multigrid cycles, 1 conjugate gradient (head_pot_method,
      * potential_head_node.c:112-176) */
     int head_pot_method;
+    /* adjoint Poisson solves (qz_force_vjp, qz_adjoint_final_loss): multigrid
+     * cycles until |r| <= adjoint_tol |rhs| (2-norms over the head interior) */
+    double adjoint_tol;
 } qz_config;
 
 typedef struct qz_stats {
@@ -109,7 +112,20 @@ typedef struct qz_stats {
     int nodes;                 /* nodes in the current tree, head included */
     double last_dt;            /* step size of the last qz_step step */
     double sim_time;           /* sum of the qz_step step sizes */
+    long long adjoint_cycles;  /* multigrid cycles of the adjoint solves */
 } qz_stats;
+
+/* Result of qz_adjoint_final_loss. */
+typedef struct qz_adjoint_stats {
+    double loss;               /* (1/N) sum_p |x_T,p - x*_p|^2 */
+    double forward_ms;         /* forward pass with checkpoints (device time) */
+    double reverse_ms;         /* recomputation and reverse sweep (device time) */
+    long long adjoint_cycles;  /* multigrid cycles of the adjoint Poisson solves */
+    long long recomputed_steps;/* forward steps run again from checkpoints */
+    int checkpoints;           /* stored checkpoints */
+    double pool_peak_bytes;    /* high-water mark of the device memory pool during the call */
+    double stored_bytes;       /* checkpoints + a segment's states + the final state */
+} qz_adjoint_stats;
 
 typedef struct qz_sim qz_sim;
 
@@ -201,6 +217,33 @@ QZ_API int qz_timestep(qz_sim *sim, double *dt);
  * Returns the first failure (with its index in qz_last_error). */
 QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *dt, int nsteps,
                             int nthreads);
+
+/* Differentiation form (no reference counterpart: QUANTIZER has no adjoint).
+ * Head-only FP64 runs (lmax == lmin, 3-point stencil, reflexive walls,
+ * multigrid head solve).  The force F(x, m) = gather(-grad Lap^-1 deposit(x, m))
+ * of grid_density.c:35-111, potential_head_node.c:99-179,
+ * grid_acceleration.c:36-76 and particle_acceleration.c:33-132 is
+ * differentiated with the Poisson solve taken as exact (its adjoint is a
+ * second solve with zero boundary, to adjoint_tol) and the shell boundary
+ * linear in total_mass (which is taken as the sum of the masses).
+ *
+ * qz_force_vjp: for host a-bar (n each) at the current state (forces computed),
+ * writes gx..gz = (dF/dx)^T abar and gm = (dF/dm)^T abar (host, n each).
+ *
+ * qz_adjoint_final_loss: from the current state (x0, v0, a0 = F(x0)), runs
+ * nsteps fixed-dt steps (particle_updating.c:39-207, 2677-2688) with a
+ * checkpoint every checkpoint_every steps (<= 0: one segment), then the
+ * reverse sweep, recomputing each earlier segment from its checkpoint.
+ * Writes the gradients of L = (1/N) sum_p |x_T,p - x*_p|^2 (targets tx..tz)
+ * with respect to the initial positions, velocities and masses (host, n each)
+ * and, when st is not NULL, the loss and timings.  The simulation is left at
+ * the final state, as after qz_step(sim, dt, nsteps). */
+QZ_API int qz_force_vjp(qz_sim *sim, const double *abx, const double *aby, const double *abz,
+                        double *gx, double *gy, double *gz, double *gm);
+QZ_API int qz_adjoint_final_loss(qz_sim *sim, int nsteps, double dt, int checkpoint_every,
+                                 const double *tx, const double *ty, const double *tz,
+                                 double *gx, double *gy, double *gz, double *gvx, double *gvy,
+                                 double *gvz, double *gm, qz_adjoint_stats *st);
 
 /* observables (observables.c:661-696): out[0] kinetic, out[1] potential,
  * out[2] total energy, out[3..5] momentum.  potential_type 0: exact sum over

@@ -40,6 +40,7 @@ class Config(C.Structure):
         ("box_extra", C.c_int), ("branch_cg_cells", C.c_int), ("branch_sor_sweeps", C.c_int),
         ("w_sor_branch", C.c_double), ("cfl", C.c_double), ("max_dt", C.c_double),
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
+        ("adjoint_tol", C.c_double),
     ]
 
 
@@ -49,6 +50,16 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_longlong), ("steps", C.c_longlong), ("error_flags", C.c_int),
         ("cg_iterations", C.c_longlong), ("levels", C.c_int), ("nodes", C.c_int),
         ("last_dt", C.c_double), ("sim_time", C.c_double),
+        ("adjoint_cycles", C.c_longlong),
+    ]
+
+
+class AdjointStats(C.Structure):
+    _fields_ = [
+        ("loss", C.c_double), ("forward_ms", C.c_double), ("reverse_ms", C.c_double),
+        ("adjoint_cycles", C.c_longlong), ("recomputed_steps", C.c_longlong),
+        ("checkpoints", C.c_int), ("pool_peak_bytes", C.c_double),
+        ("stored_bytes", C.c_double),
     ]
 
 
@@ -101,6 +112,9 @@ def load() -> C.CDLL:
         "qz_timestep": ([vp, _P], C.c_int),
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
         "qz_ensemble_step": ([C.POINTER(vp), C.c_int, _P, C.c_int, C.c_int], C.c_int),
+        "qz_force_vjp": ([vp] + [_P] * 7, C.c_int),
+        "qz_adjoint_final_loss": ([vp, C.c_int, C.c_double, C.c_int] + [_P] * 10 +
+                                  [C.POINTER(AdjointStats)], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
         "qz_tree_adaptation": ([vp], C.c_int),
         "qz_poisson_error": ([vp, _I], C.c_int),
@@ -291,6 +305,34 @@ class Simulation:
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))
+
+    def force_vjp(self, abx, aby, abz) -> dict:
+        """(dF/dx)^T abar and (dF/dm)^T abar of the head force at the current
+        state (qz_force_vjp); keys gx, gy, gz, gm."""
+        a = [_f64(v) for v in (abx, aby, abz)]
+        n = self.n
+        out = {k: np.empty(n) for k in ("gx", "gy", "gz", "gm")}
+        _check(self.lib.qz_force_vjp(self.h, *[_p(v) for v in a],
+                                     *[_p(out[k]) for k in ("gx", "gy", "gz", "gm")]))
+        return out
+
+    def adjoint_final_loss(self, nsteps: int, dt: float, targets: dict,
+                           checkpoint_every: int = 0) -> dict:
+        """Gradients of L = mean_p |x_T,p - x*_p|^2 after nsteps fixed-dt steps
+        with respect to the current x, v, m (qz_adjoint_final_loss); the
+        simulation is left at step nsteps.  Keys gx..gz, gvx..gvz, gm, loss,
+        stats (AdjointStats as a dict)."""
+        t = [_f64(targets[k]) for k in ("x", "y", "z")]
+        n = self.n
+        keys = ("gx", "gy", "gz", "gvx", "gvy", "gvz", "gm")
+        out = {k: np.empty(n) for k in keys}
+        st = AdjointStats()
+        _check(self.lib.qz_adjoint_final_loss(self.h, nsteps, dt, checkpoint_every,
+                                              *[_p(v) for v in t],
+                                              *[_p(out[k]) for k in keys], C.byref(st)))
+        out["loss"] = st.loss
+        out["stats"] = {f: getattr(st, f) for f, _ in AdjointStats._fields_}
+        return out
 
     def step(self, dt: float, nsteps: int = 1) -> None:
         _check(self.lib.qz_step(self.h, dt, nsteps))

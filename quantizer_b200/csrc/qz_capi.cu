@@ -252,7 +252,7 @@ static bool d2h(qz_sim *s, double *dst, const double *src, long count)
     return true;
 }
 
-static int check_flags(qz_sim *s)
+int check_flags(qz_sim *s)
 {
     if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
                                     cudaMemcpyDeviceToHost, s->stream),
@@ -315,6 +315,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->max_dt = 1.0e30;        /* _MAX_dt_ (0.005 Maxdt in the reference's units): no cap */
     c->time_step_method = 1;   /* global_variables.c:342 */
     c->head_pot_method = 0;    /* global_variables.c (multigrid) */
+    c->adjoint_tol = 1e-10;
     return QZ_SUCCESS;
 }
 
@@ -370,6 +371,7 @@ int qz_destroy(qz_sim *s)
         dfree(p);
     free_levels(s);
     amr_free(s);
+    adjoint_free(s);
     if (s->mem.pool)
         pool_free(s->mem, s->scan_tmp);
     if (s->stream)
@@ -668,6 +670,25 @@ int qz_init_forces(qz_sim *s)
     return QZ_SUCCESS;
 }
 
+} // extern "C"
+
+namespace qz {
+// main.c:375-481 with a given dt: kick-drift, reset, tree, deposit, potential,
+// gradient, gather, kick.
+int step_core(qz_sim *s, double h)
+{
+    if (kick_drift(s, h) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
+        qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, h))
+        return QZ_FAILURE;
+    s->stats.steps++;
+    s->stats.last_dt = h;
+    s->stats.sim_time += h;
+    return QZ_SUCCESS;
+}
+} // namespace qz
+
+extern "C" {
+
 int qz_step(qz_sim *s, double dt, int nsteps)
 {
     if (!s)
@@ -679,13 +700,8 @@ int qz_step(qz_sim *s, double dt, int nsteps)
         double h = dt;
         if (dt <= 0.0 && timestep_cfl(s, &h))
             return QZ_FAILURE;
-        if (kick_drift(s, h) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
-            qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) ||
-            kick(s, h))
+        if (step_core(s, h))
             return QZ_FAILURE;
-        s->stats.steps++;
-        s->stats.last_dt = h;
-        s->stats.sim_time += h;
     }
     return check_flags(s);
 }

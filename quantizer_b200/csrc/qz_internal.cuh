@@ -243,6 +243,10 @@ struct AmrLevel {
 
 #define QZ_CG_PART_MAX 1024
 
+namespace qz {
+struct Adjoint; // qz_adjoint.cu
+}
+
 struct qz_sim {
     qz_config cfg;
     int device = 0;
@@ -293,6 +297,7 @@ struct qz_sim {
     // refinement tree (lmax > lmin): levels[0] = head, rebuilt every step
     std::vector<qz::AmrLevel> amr;
     qz::AmrLevel head_cg; // the head as a one-node level (head_pot_method 1)
+    qz::Adjoint *adj = nullptr; // adjoint buffers (qz_force_vjp, qz_adjoint_final_loss)
     int amr_nlev = 1;                  // levels in use this step
     std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
     qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)
@@ -332,6 +337,11 @@ namespace qz {
 void set_error(const char *fmt, ...);
 int timestep_cfl(qz_sim *s, double *dt_out); // qz_observe.cu
 int head_cg_solve(qz_sim *s);                 // qz_amr.cu
+int solve_zero_bc(qz_sim *s, double *lam, double *f, double rtol, double *scratch,
+                  double *host, int *cycles);  // qz_poisson.cu
+int check_flags(qz_sim *s);                   // qz_capi.cu
+int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
+void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
 bool check_cuda(cudaError_t e, const char *what);
 #define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
 
@@ -384,6 +394,8 @@ inline void launch(qz_sim *s, int cat, double bytes, void (*k)(KArgs...), dim3 g
 int head_initial(qz_sim *s);
 int deposit_head(qz_sim *s);
 int grid_accel_head(qz_sim *s);
+int grid_accel_head_from(qz_sim *s, const double *pot);
+int head_segments(qz_sim *s, const double *x, const double *y, const double *z, int **perm_out);
 int gather_head(qz_sim *s);
 int kick_drift(qz_sim *s, double dt);
 int kick(qz_sim *s, double dt);

@@ -237,22 +237,32 @@ int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box
     return QZ_SUCCESS;
 }
 
-int deposit_head(qz_sim *s)
+// Head cell keys of the particles at (x, y, z), sorted, and their cell
+// segments (seg_start, cell_seg, flags[F_NSEG]); *perm_out: particle of each
+// sorted position.
+int head_segments(qz_sim *s, const double *x, const double *y, const double *z, int **perm_out)
 {
     const long n = s->n;
     const int L = s->L;
     const long B = (1L << L) + 2;
-    if (n == 0)
-        return cudaMemsetAsync(s->d, 0, s->gpts * sizeof(double), s->stream) == cudaSuccess
-                   ? QZ_SUCCESS
-                   : QZ_FAILURE;
-    launch(s, QZ_PROF_DEPOSIT, 32.0 * n, k_head_keys, dim3(blocks_for(n, 256)), dim3(256), n, L, s->x, s->y, s->z, s->sort.k0, s->sort.v0, s->flags);
+    launch(s, QZ_PROF_DEPOSIT, 32.0 * n, k_head_keys, dim3(blocks_for(n, 256)), dim3(256), n, L, x, y, z, s->sort.k0, s->sort.v0, s->flags);
     int bits = 1;
     while ((1L << bits) < B * B * B)
         bits++;
     unsigned *ks;
+    return deposit_segments(s, n, bits, s->cell_seg, B * B * B, &ks, perm_out);
+}
+
+int deposit_head(qz_sim *s)
+{
+    const long n = s->n;
+    const int L = s->L;
+    if (n == 0)
+        return cudaMemsetAsync(s->d, 0, s->gpts * sizeof(double), s->stream) == cudaSuccess
+                   ? QZ_SUCCESS
+                   : QZ_FAILURE;
     int *perm;
-    if (deposit_segments(s, n, bits, s->cell_seg, B * B * B, &ks, &perm))
+    if (head_segments(s, s->x, s->y, s->z, &perm))
         return QZ_FAILURE;
     const double H = 1.0 / (1 << L);
     const double coeff = 4.0 * s->cfg.G * QZ_PI_D / (H * H * H);
@@ -307,16 +317,18 @@ __global__ void k_grid_accel_head(int L, long D, int stencil, const double *__re
                 : o2h * (pot[g - D2] - pot[g + D2]);
 }
 
-int grid_accel_head(qz_sim *s)
+int grid_accel_head_from(qz_sim *s, const double *pot)
 {
     long m = (1L << s->L) - 1;
     if (m <= 0)
         return QZ_SUCCESS;
     const double bytes = (s->cfg.force_stencil ? 56.0 : 32.0) * m * m * m;
     launch(s, QZ_PROF_GRADIENT, bytes, k_grid_accel_head, dim3(blocks_for(m * m * m, 256)), dim3(256),
-           s->L, s->D, s->cfg.force_stencil, s->pot, s->gax, s->gay, s->gaz);
+           s->L, s->D, s->cfg.force_stencil, pot, s->gax, s->gay, s->gaz);
     return check_cuda(cudaGetLastError(), "grid accel") ? QZ_SUCCESS : QZ_FAILURE;
 }
+
+int grid_accel_head(qz_sim *s) { return grid_accel_head_from(s, s->pot); }
 
 // ---- CIC gather ---------------------------------------------------------------
 __global__ void k_gather_head(long n, int L, long D, const double *__restrict__ x,

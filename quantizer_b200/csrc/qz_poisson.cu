@@ -1311,6 +1311,140 @@ static int launch_check(qz_sim *s, double node_mass)
     return check_cuda(cudaGetLastError(), "convergence check") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
+// ---- Poisson solve with zero Dirichlet boundary (adjoint of the head solve) ----------
+// Partial sums, per block, of r^2 and f^2 over the head interior, r = f + (6 lam -
+// sum of the 6 neighbours) / H^2 (the residual convention of the head solve).
+__global__ void k_resid_norm_partial(int L, long D, const double *__restrict__ lam,
+                                     const double *__restrict__ f, double oh2,
+                                     double *__restrict__ partial)
+{
+    __shared__ double sh[32];
+    const int m = (1 << L) - 1;
+    const long total = (long)m * m * m;
+    const long D2 = D * D;
+    double rr = 0.0, ff = 0.0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long)gridDim.x * blockDim.x)
+    {
+        const long i = 2 + t % m, j = 2 + (t / m) % m, k = 2 + t / ((long)m * m);
+        const long g = i + j * D + k * D2;
+        const double r = f[g] + oh2 * (6.0 * lam[g] - lam[g + 1] - lam[g - 1] - lam[g + D] -
+                                       lam[g - D] - lam[g + D2] - lam[g - D2]);
+        rr += r * r;
+        ff += f[g] * f[g];
+    }
+    const double a = block_sum(rr, sh);
+    const double b = block_sum(ff, sh);
+    if (threadIdx.x == 0)
+    {
+        partial[2 * blockIdx.x] = a;
+        partial[2 * blockIdx.x + 1] = b;
+    }
+}
+
+__global__ void k_resid_norm_final(int nb, const double *__restrict__ partial,
+                                   double *__restrict__ out)
+{
+    __shared__ double sh[32];
+    double a = 0.0, b = 0.0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x)
+    {
+        a += partial[2 * q];
+        b += partial[2 * q + 1];
+    }
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0)
+    {
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+// |r|^2 and |f|^2 of lam against f into host[0..1] (pinned), synchronising.
+static int resid_norms(qz_sim *s, const double *lam, const double *f, double *scratch,
+                       double *host)
+{
+    const double H = 1.0 / (1 << s->L);
+    const long m = (1L << s->L) - 1;
+    launch(s, QZ_PROF_CHECK, 16.0 * m * m * m, k_resid_norm_partial, dim3(s->red_blocks),
+           dim3(CK_THREADS), s->L, s->D, lam, f, 1.0 / (H * H), scratch);
+    launch(s, QZ_PROF_CHECK, 16.0 * s->red_blocks, k_resid_norm_final, dim3(1), dim3(256),
+           s->red_blocks, scratch, scratch + 2 * s->red_blocks);
+    if (!check_cuda(cudaMemcpyAsync(host, scratch + 2 * s->red_blocks, 2 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s->stream),
+                    "residual norm") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "residual norm sync"))
+        return QZ_FAILURE;
+    return QZ_SUCCESS;
+}
+
+// Solves Lap_h lam = f on the head interior with lam = 0 on the solve grid's
+// boundary, by FP64 multigrid cycles of the configured kind (the operator of
+// the head solve is symmetric, so this is also its adjoint), from the initial
+// guess in lam, until |r| <= rtol |f| (checked every 2 cycles).  scratch holds
+// 2 * red_blocks + 2 doubles; host 2 pinned doubles.  *cycles: cycles run.
+int solve_zero_bc(qz_sim *s, double *lam, double *f, double rtol, double *scratch,
+                  double *host, int *cycles)
+{
+    const qz_config &c = s->cfg;
+    *cycles = 0;
+    if (resid_norms(s, lam, f, scratch, host))
+        return QZ_FAILURE;
+    if (host[1] == 0.0)
+    {
+        cudaMemsetAsync(lam, 0, s->gpts * sizeof(double), s->stream);
+        return QZ_SUCCESS;
+    }
+    const double goal = rtol * rtol * host[1];
+    if (host[0] <= goal)
+        return QZ_SUCCESS;
+    const Grid<double> keep_phi = s->fine_phi, keep_rho = s->fine_rho;
+    s->fine_phi = head_view(s, lam);
+    s->fine_rho = head_view(s, f);
+    sync_fine_alt(s);
+    int rc = QZ_SUCCESS;
+    bool done = false;
+    while (!done && *cycles < c.max_iter)
+    {
+        const int k = std::min(2, c.max_iter - *cycles);
+        if (mg_persistent(s))
+            rc = mg_launch<double>(s, k);
+        else
+            for (int q = 0; q < k && !rc; q++)
+                rc = vcycle(s, 0, c.cycle);
+        if (rc)
+            break;
+        *cycles += k;
+        if ((rc = resid_norms(s, lam, f, scratch, host)))
+            break;
+        if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
+                                        cudaMemcpyDeviceToHost, s->stream), "flags") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "flags sync"))
+        {
+            rc = QZ_FAILURE;
+            break;
+        }
+        if (s->h_flags[F_ERROR] & E_BARRIER)
+        {
+            set_error("adjoint multigrid cycles: a grid barrier wait gave up");
+            rc = QZ_FAILURE;
+            break;
+        }
+        done = host[0] <= goal;
+    }
+    s->fine_phi = keep_phi;
+    s->fine_rho = keep_rho;
+    sync_fine_alt(s);
+    if (!rc && !done)
+    {
+        set_error("adjoint Poisson solve: |r|/|f| = %.3e after %d cycles (goal %.3e)",
+                  sqrt(host[0] / host[1]), *cycles, rtol);
+        rc = QZ_FAILURE;
+    }
+    return rc;
+}
+
 // Captures `every` solver iterations followed by the convergence test into a
 // CUDA graph (kernel parameters and buffers of a context never change).
 static int capture_check_block(qz_sim *s, int every)
