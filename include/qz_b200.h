@@ -245,6 +245,21 @@ QZ_API int qz_adjoint_final_loss(qz_sim *sim, int nsteps, double dt, int checkpo
                                  double *gx, double *gy, double *gz, double *gvx, double *gvy,
                                  double *gvz, double *gm, qz_adjoint_stats *st);
 
+/* Snapshot file of output_snapshots.c:141-239 from the device-resident state:
+ * m[N], x, y, z, vx, vy, vz in user units ((x - 0.5) / conversion_dist + cm_x
+ * + cm_vx * real_time; vx / conversion_velocity + cm_vx), then, when
+ * observables_type is 0 or 1, energies[3] and momentum[3] of qz_observables
+ * with that potential type, then real_time = actual_time / conversion_time
+ * (float64, native byte order).  units: {conversion_dist, conversion_velocity,
+ * conversion_time, cm_x, cm_y, cm_z, cm_vx, cm_vy, cm_vz}, NULL for 1, 1, 1
+ * and zeros; observables_type -1: none.  async != 0: the copy to the host and
+ * the file write run behind the simulation's stream (the state may be stepped
+ * at once); qz_snapshot_wait joins the write and reports its result (so does
+ * the next qz_write_snapshot and qz_destroy). */
+QZ_API int qz_write_snapshot(qz_sim *sim, const char *path, double actual_time,
+                             const double *units, int observables_type, int async);
+QZ_API int qz_snapshot_wait(qz_sim *sim);
+
 /* observables (observables.c:661-696): out[0] kinetic, out[1] potential,
  * out[2] total energy, out[3..5] momentum.  potential_type 0: exact sum over
  * particle pairs (O(N^2), potential_energy_exact :77-112); 1: from the

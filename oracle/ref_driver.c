@@ -20,7 +20,11 @@
  *         conjugate gradient, the others red-black SOR), tsm (time_step_method),
  *         cfl (_CFL_), max_dt (_MAX_dt_), obs (1: dump observables of both
  *         potential-energy forms as obs0 / obs1: energies[3], momentum[3]),
- *         check (check_poisson_error_method 0/1/2)
+ *         check (check_poisson_error_method 0/1/2), snap (after the last step:
+ *         1 output_snapshots(snap_time, 0) into OUTDIR/run/../output, 2 the same
+ *         after observables() with compute_observables_FLAG set and
+ *         potential_energy_type snap_pe), snap_time,
+ *         cm (GL_cm_x,y,z,vx,vy,vz as a comma list)
  * IC.bin: int64 N, then x[N] y[N] z[N] vx[N] vy[N] vz[N] m[N] (float64).
  * Dumps: OUTDIR/s<step>_<field>.bin raw float64 (head grid and particles, and
  *        dtcfl: the reference's timestep() of that state),
@@ -29,7 +33,9 @@
  */
 #include "main.h"
 #include <stdint.h>
+#include <sys/stat.h>
 #include <time.h>
+#include <unistd.h>
 
 static void die(const char *msg)
 {
@@ -221,6 +227,10 @@ int main(int argc, char **argv)
     double max_dt = -1.0;   /* _MAX_dt_ */
     int branch_cg_cells = -1; /* branches_maximal_node_number_to_activate_conjugate_gradient */
     int check = -1;           /* check_poisson_error_method */
+    int snap = 0;             /* write a snapshot after the last step */
+    double snap_time = 0.0;
+    int snap_pe = -1;         /* potential_energy_type of the snapshot's observables */
+    double cm[6] = {0, 0, 0, 0, 0, 0};
     double dt = 1e-4, G = 1.0;
     const char *dump = NULL;
     for (int a = 3; a < argc; a++)
@@ -250,6 +260,19 @@ int main(int argc, char **argv)
         else if (!strcmp(key, "obs")) g_obs = atoi(v);
         else if (!strcmp(key, "branch_cg_cells")) branch_cg_cells = atoi(v);
         else if (!strcmp(key, "check")) check = atoi(v);
+        else if (!strcmp(key, "snap")) snap = atoi(v);
+        else if (!strcmp(key, "snap_time")) snap_time = atof(v);
+        else if (!strcmp(key, "snap_pe")) snap_pe = atoi(v);
+        else if (!strcmp(key, "cm"))
+        {
+            const char *p = v;
+            for (int q = 0; q < 6; q++)
+            {
+                char *end;
+                cm[q] = strtod(p, &end);
+                p = *end == ',' ? end + 1 : end;
+            }
+        }
         else die("unknown key");
     }
     if (LMAX < 0)
@@ -316,6 +339,12 @@ int main(int argc, char **argv)
     for (int i = 0; i < N; i++)
         GL_total_mass_initial += GL_ptcl_mass[i];
     GL_cm_x = GL_cm_y = GL_cm_z = GL_cm_vx = GL_cm_vy = GL_cm_vz = 0.0;
+    GL_cm_x = cm[0];
+    GL_cm_y = cm[1];
+    GL_cm_z = cm[2];
+    GL_cm_vx = cm[3];
+    GL_cm_vy = cm[4];
+    GL_cm_vz = cm[5];
 
     if (initialization() == _FAILURE_)
         die("initialization failed");
@@ -356,6 +385,29 @@ int main(int argc, char **argv)
         t_loop += now_s() - ts;
         if (in_list(dump, s))
             dump_step(out, s, amr);
+    }
+    if (snap)
+    {
+        /* output_snapshots writes under ../output relative to the working directory */
+        char here[4096], run[4200];
+        if (!getcwd(here, sizeof here))
+            die("getcwd");
+        snprintf(run, sizeof run, "%s/run", out);
+        mkdir(run, 0777);
+        if (chdir(run))
+            die("chdir");
+        if (snap == 2)
+        {
+            compute_observables_FLAG = true;
+            if (snap_pe >= 0)
+                potential_energy_type = snap_pe;
+            if (observables() == _FAILURE_)
+                die("observables failed");
+        }
+        if (output_snapshots(snap_time, 0) == _FAILURE_)
+            die("output_snapshots failed");
+        if (chdir(here))
+            die("chdir back");
     }
     int nodes = 0;
     for (int lv = 0; lv <= GL_tentacles_level_max; lv++)

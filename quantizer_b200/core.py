@@ -113,6 +113,8 @@ def load() -> C.CDLL:
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
         "qz_ensemble_step": ([C.POINTER(vp), C.c_int, _P, C.c_int, C.c_int], C.c_int),
         "qz_force_vjp": ([vp] + [_P] * 7, C.c_int),
+        "qz_write_snapshot": ([vp, C.c_char_p, C.c_double, _P, C.c_int, C.c_int], C.c_int),
+        "qz_snapshot_wait": ([vp], C.c_int),
         "qz_adjoint_final_loss": ([vp, C.c_int, C.c_double, C.c_int] + [_P] * 10 +
                                   [C.POINTER(AdjointStats)], C.c_int),
         "qz_ptcl_idx_to_box_idx": ([C.c_int] * 6 + [C.c_long, _P, _P, _P, _I], C.c_int),
@@ -305,6 +307,18 @@ class Simulation:
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))
+
+    def write_snapshot(self, path: str, actual_time: float, units=None,
+                       observables_type: int = -1, wait: bool = True) -> None:
+        """Snapshot file in the layout of output_snapshots.c:141-239
+        (qz_write_snapshot); units as there, observables_type -1 for none."""
+        self._snap_units = None if units is None else np.ascontiguousarray(units, dtype=np.float64)
+        u = None if self._snap_units is None else _p(self._snap_units)
+        _check(self.lib.qz_write_snapshot(self.h, path.encode(), actual_time, u,
+                                          observables_type, 0 if wait else 1))
+
+    def snapshot_wait(self) -> None:
+        _check(self.lib.qz_snapshot_wait(self.h))
 
     def force_vjp(self, abx, aby, abz) -> dict:
         """(dF/dx)^T abar and (dF/dm)^T abar of the head force at the current

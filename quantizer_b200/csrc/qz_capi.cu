@@ -357,6 +357,7 @@ int qz_destroy(qz_sim *s)
     if (s->stream)
         cudaStreamSynchronize(s->stream);
     prof_collect(s);
+    snapshot_free(s);
     if (s->check_exec)
         cudaGraphExecDestroy(s->check_exec);
     for (cudaEvent_t e : s->ev_pool)

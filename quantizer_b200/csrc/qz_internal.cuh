@@ -244,7 +244,8 @@ struct AmrLevel {
 #define QZ_CG_PART_MAX 1024
 
 namespace qz {
-struct Adjoint; // qz_adjoint.cu
+struct Adjoint;  // qz_adjoint.cu
+struct Snapshot; // qz_snapshot.cu
 }
 
 struct qz_sim {
@@ -298,6 +299,7 @@ struct qz_sim {
     std::vector<qz::AmrLevel> amr;
     qz::AmrLevel head_cg; // the head as a one-node level (head_pot_method 1)
     qz::Adjoint *adj = nullptr; // adjoint buffers (qz_force_vjp, qz_adjoint_final_loss)
+    qz::Snapshot *snap = nullptr; // snapshot staging and writer thread (qz_write_snapshot)
     int amr_nlev = 1;                  // levels in use this step
     std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
     qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)
@@ -342,6 +344,7 @@ int solve_zero_bc(qz_sim *s, double *lam, double *f, double rtol, double *scratc
 int check_flags(qz_sim *s);                   // qz_capi.cu
 int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
 void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
+void snapshot_free(qz_sim *s);                // qz_snapshot.cu
 bool check_cuda(cudaError_t e, const char *what);
 #define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
 
