@@ -172,6 +172,10 @@ QZ_API int qz_initial_potential_head(qz_sim *sim); /* initial_potential_and_acce
 QZ_API int qz_reset(qz_sim *sim);
 QZ_API int qz_grid_density(qz_sim *sim);
 QZ_API int qz_potential(qz_sim *sim);
+/* potential.c:29-51 in its two halves: potential_head_node.c:99-179 and
+ * potential_branches.c:401-532 (no-op without refinement) */
+QZ_API int qz_potential_head_node(qz_sim *sim);
+QZ_API int qz_potential_branches(qz_sim *sim);
 QZ_API int qz_grid_acceleration(qz_sim *sim);
 QZ_API int qz_particle_acceleration(qz_sim *sim);
 QZ_API int qz_particle_updating_A(qz_sim *sim, double dt);

@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libqzoracle.so")
 REF_DRIVER = os.path.join(HERE, "_ref", "qz_ref_driver")
 DROPIN_DRIVER = os.path.join(HERE, "_ref", "qz_dropin_driver")
+DROPIN_AMR_DRIVER = os.path.join(HERE, "_ref", "qz_dropin_amr_driver")
 
 _P = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)

@@ -95,6 +95,8 @@ def load() -> C.CDLL:
         "qz_reset": ([vp], C.c_int),
         "qz_grid_density": ([vp], C.c_int),
         "qz_potential": ([vp], C.c_int),
+        "qz_potential_head_node": ([vp], C.c_int),
+        "qz_potential_branches": ([vp], C.c_int),
         "qz_grid_acceleration": ([vp], C.c_int),
         "qz_particle_acceleration": ([vp], C.c_int),
         "qz_particle_updating_A": ([vp, C.c_double], C.c_int),

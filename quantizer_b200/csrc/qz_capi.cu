@@ -635,6 +635,15 @@ int qz_potential(qz_sim *s)
     return amr_on(s) ? amr_potential(s) : QZ_SUCCESS;
 }
 
+int qz_potential_head_node(qz_sim *s) { return s ? potential_head(s) : QZ_FAILURE; }
+
+int qz_potential_branches(qz_sim *s)
+{
+    if (!s)
+        return QZ_FAILURE;
+    return amr_on(s) ? amr_potential(s) : QZ_SUCCESS;
+}
+
 int qz_poisson_error(qz_sim *s, int *converged)
 {
     if (!s || !converged)

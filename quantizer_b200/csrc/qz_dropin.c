@@ -10,9 +10,20 @@
  * to the host globals before returning (write-through), so host code that
  * reads them (timestep, observables, snapshots) always sees current values.
  *
- * Scope of this build: the head-only path (lmax == lmin) with reflexive or
- * periodic boundaries, Gauss-Seidel or Jacobi smoothing, the 3-point force
- * stencil.  Other configurations are rejected with the reference's error
+ * Refinement runs (lmax > lmin): the tree bookkeeping stays in the reference's
+ * C -- tree_adaptation and the particle moves between cell lists of
+ * particle_updating.c:634-1381, so the host program links the reference's
+ * particle_updating.o -- and the host particle arrays are authoritative for
+ * x and v: grid_density, timestep and observables upload them first.  The
+ * density, potentials, grid and particle accelerations are computed on the
+ * device on its own copy of the tree (built from the same rules,
+ * tree_construction.c; its refined cells equal the reference's adapted tree);
+ * particle accelerations and the head node's fields are written back,
+ * refinement nodes' grid fields are not.
+ *
+ * Supported: reflexive boundaries, one smoother for all multigrid stages or
+ * the head conjugate gradient, the particle refinement criterion with n_exp
+ * = 1.  Other configurations are rejected with the reference's error
  * convention (message + _FAILURE_).
  *
  * Environment: QZ_GS_ORDER=lex selects the reference's lexicographic
@@ -48,11 +59,14 @@ static struct {
     int *pe_type;
     int *time_step_method;
     double *w_sor_head, *tol, *tol2;
+    int *ref_ptcl, *n_exp, *box_extra;
+    double *ref_mass;
     int resolved;
 } R;
 
 static qz_sim *g_sim = NULL;
 static int g_failed = 0;
+static int g_amr = 0; /* refinement run: host x, v authoritative */
 
 static void *need(const char *name, int *ok)
 {
@@ -119,6 +133,10 @@ static int resolve(void)
     R.w_sor_head = need("_w_SOR_HEAD_", &ok);
     R.tol = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_", &ok);
     R.tol2 = need("_ERROR_THRESHOLD_IN_THE_POISSON_EQUATION_2", &ok);
+    R.ref_ptcl = need("ref_criterion_ptcl", &ok);
+    R.ref_mass = need("ref_criterion_mass", &ok);
+    R.n_exp = need("n_exp", &ok);
+    R.box_extra = need("min_box_extra_size_per_side_real", &ok);
     R.resolved = ok;
     return ok;
 }
@@ -149,6 +167,8 @@ static void fill_config(qz_config *c)
     c->max_dt = *R.max_dt;
     c->time_step_method = *R.time_step_method;
     c->head_pot_method = *R.head_pot_method;
+    c->ref_ptcl = *R.ref_ptcl;
+    c->box_extra = *R.box_extra;
     const char *o = getenv("QZ_GS_ORDER");
     c->gs_order = (o && !strcmp(o, "lex")) ? QZ_GS_LEX : QZ_GS_REDBLACK;
     const char *p = getenv("QZ_PRECISION");
@@ -191,9 +211,11 @@ static int ensure(void)
         g_failed = 1;
         return REF_FAILURE;
     }
-    if (*R.lmin != *R.lmax)
+    g_amr = *R.lmax > *R.lmin;
+    if (g_amr && (*R.n_exp != 1 || *R.ref_mass < 1.0e99 || *R.bdry_cond_type != 1))
     {
-        printf("\nERROR (drop-in): lmax > lmin (refinement) is not supported by this build\n");
+        printf("\nERROR (drop-in): refinement runs need n_exp = 1, the particle criterion "
+               "only (ref_criterion_mass off) and reflexive boundaries\n");
         g_failed = 1;
         return REF_FAILURE;
     }
@@ -215,6 +237,19 @@ static int ensure(void)
     return upload_all();
 }
 
+/* Refinement runs: x, v (and m) from the host arrays, which the reference's
+ * particle_updating moved; with_accel also the accelerations. */
+static int sync_host_particles(int with_accel)
+{
+    if (!g_amr)
+        return REF_SUCCESS;
+    if (qz_set_particles(g_sim, *R.no_ptcl_final, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx,
+                         *R.ptcl_vy, *R.ptcl_vz, *R.ptcl_mass) ||
+        (with_accel && qz_set_particle_accel(g_sim, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az)))
+        return fail("upload of the host particles");
+    return REF_SUCCESS;
+}
+
 static int head_field_back(int which, double *dst)
 {
     if (qz_get_head_field(g_sim, which, dst))
@@ -225,9 +260,9 @@ static int head_field_back(int which, double *dst)
 /* grid_density.c:269-306 */
 void grid_density(void)
 {
-    if (ensure())
+    if (ensure() || sync_host_particles(0))
         return;
-    if (qz_grid_density(g_sim))
+    if ((g_amr && qz_tree_adaptation(g_sim)) || qz_grid_density(g_sim))
     {
         fail("grid_density");
         return;
@@ -240,7 +275,7 @@ int potential_head_node(void)
 {
     if (ensure())
         return REF_FAILURE;
-    if (qz_potential(g_sim))
+    if (qz_potential_head_node(g_sim))
     {
         printf("\n\n Error running potential_head_node() function \n\n ");
         return fail("potential_head_node");
@@ -251,11 +286,14 @@ int potential_head_node(void)
     return REF_SUCCESS;
 }
 
-/* potential_branches.c:401-532: nothing to solve without refinement. */
+/* potential_branches.c:401-532: the refinement levels' solves (none without
+ * refinement). */
 int potential_branches(void)
 {
     if (ensure())
         return REF_FAILURE;
+    if (qz_potential_branches(g_sim))
+        return fail("potential_branches");
     return REF_SUCCESS;
 }
 
@@ -286,7 +324,7 @@ int grid_acceleration(void)
 /* timestep.c:589-700: the CFL step of the current state, reduced on the device */
 int timestep(double *ptr_dt)
 {
-    if (ensure())
+    if (ensure() || sync_host_particles(1))
         return REF_FAILURE;
     if (qz_timestep(g_sim, ptr_dt))
         return fail("timestep");
@@ -296,7 +334,7 @@ int timestep(double *ptr_dt)
 /* observables.c:661-696: energies into GL_energies, momentum into GL_momentum */
 int observables(void)
 {
-    if (ensure())
+    if (ensure() || sync_host_particles(1))
         return REF_FAILURE;
     const double units[6] = {*R.conv_velocity, *R.conv_time, *R.conv_dist,
                              *R.cm_vx, *R.cm_vy, *R.cm_vz};
@@ -328,11 +366,23 @@ int particle_acceleration(void)
     return REF_SUCCESS;
 }
 
+/* Refinement runs move particles between the host tree's cell lists in the
+ * reference's particle_updating.c, which the host program links instead. */
+static int amr_update_refused(void)
+{
+    printf("\nERROR (drop-in): refinement runs keep the reference's particle_updating.o "
+           "(cell-list bookkeeping of particle_updating.c:634-1381) in the link\n");
+    g_failed = 1;
+    return REF_FAILURE;
+}
+
 /* particle_updating.c:2584-2675 */
 int particle_updating_A(double dt)
 {
     if (ensure())
         return REF_FAILURE;
+    if (g_amr)
+        return amr_update_refused();
     if (qz_particle_updating_A(g_sim, dt) ||
         qz_get_particles(g_sim, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
                          *R.ptcl_vz, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az))
@@ -345,6 +395,11 @@ void particle_updating_B(double dt)
 {
     if (ensure())
         return;
+    if (g_amr)
+    {
+        amr_update_refused();
+        return;
+    }
     if (qz_particle_updating_B(g_sim, dt) ||
         qz_get_particles(g_sim, NULL, NULL, NULL, *R.ptcl_vx, *R.ptcl_vy, *R.ptcl_vz, NULL, NULL,
                          NULL))

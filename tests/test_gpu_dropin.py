@@ -1,7 +1,13 @@
 """The drop-in link: the reference's own bookkeeping objects (initialization,
 tree construction/adaptation, globals) linked with libqz_dropin.so in place of
 its hot-path objects (oracle/_ref/qz_dropin_driver), run against the
-unmodified reference (oracle/_ref/qz_ref_driver) on the same inputs."""
+unmodified reference (oracle/_ref/qz_ref_driver) on the same inputs.
+
+Refinement runs (oracle/_ref/qz_dropin_amr_driver, which also keeps the
+reference's particle_updating.o for the cell-list moves): positions after 4
+steps within 1e-10 box units, particle accelerations within 1e-6 of the
+largest, head potential within 1e-9, box indices equal, and the reference's
+own adapted tree (node count and particles per node) as in the plain run."""
 import os
 
 import numpy as np
@@ -69,3 +75,29 @@ def test_dropin_driver_matches_reference(ic_file, tmp_path, order, extra, tol_po
             assert _rel(g(f), r(f)) < 100 * tol_pot
         np.testing.assert_array_equal(O.read_dump(str(tmp_path / "gpu"), s, "bidx", np.int32),
                                       O.read_dump(str(tmp_path / "ref"), s, "bidx", np.int32))
+
+
+def test_dropin_refinement_run_matches_reference(tmp_path):
+    drv = O.DROPIN_AMR_DRIVER
+    assert os.path.exists(drv), f"{drv} missing: run `make -C oracle ref dropin`"
+    p = str(tmp_path / "ic.bin")
+    ics.write_ic(p, ics.plummer(20000, a=0.05, seed=3))
+    steps = 4
+    kw = dict(lmin=5, lmax=8, ref_ptcl=9, steps=steps,
+              dt=1e-3 * ics.crossing_time(0.05), dump=f"0,{steps}")
+    rr = _run(O.REF_DRIVER, p, str(tmp_path / "ref"), **kw)
+    rg = _run(drv, p, str(tmp_path / "gpu"), **kw)
+    assert rr["levels"] == rg["levels"] == 3 and rr["nodes"] == rg["nodes"]
+    for s in (0, steps):
+        r = lambda f: O.read_dump(str(tmp_path / "ref"), s, f)
+        g = lambda f: O.read_dump(str(tmp_path / "gpu"), s, f)
+        assert _rel(g("pot"), r("pot")) < 1e-9
+        for f in ("x", "y", "z"):
+            assert np.abs(g(f) - r(f)).max() < 1e-10, (s, f)
+        for f in ("ax", "ay", "az"):
+            assert _rel(g(f), r(f)) < 1e-6, (s, f)
+        np.testing.assert_array_equal(O.read_dump(str(tmp_path / "gpu"), s, "bidx", np.int32),
+                                      O.read_dump(str(tmp_path / "ref"), s, "bidx", np.int32))
+        nr = O.read_nodes(str(tmp_path / "ref"), s)
+        ng = O.read_nodes(str(tmp_path / "gpu"), s)
+        assert [(n["lv"], n["nptcl"]) for n in nr] == [(n["lv"], n["nptcl"]) for n in ng]
