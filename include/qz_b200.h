@@ -175,6 +175,13 @@ QZ_API int qz_potential(qz_sim *sim);
 /* potential.c:29-51 in its two halves: potential_head_node.c:99-179 and
  * potential_branches.c:401-532 (no-op without refinement) */
 QZ_API int qz_potential_head_node(qz_sim *sim);
+/* Outflow boundaries (bdry 2, particle_updating.c:123-196): the removals of
+ * the last qz_particle_updating_A / step, in the reference's visiting order --
+ * slots[r] lost its particle and received the one of sources[r] (when the slot
+ * is below the new count).  slots / sources may be NULL to read the count. */
+QZ_API int qz_outflow_removed(qz_sim *sim, long *count, int *slots, int *sources);
+/* The head node's mass (node_mass): total_mass less outflow removals. */
+QZ_API double qz_head_mass(const qz_sim *sim);
 QZ_API int qz_potential_branches(qz_sim *sim);
 QZ_API int qz_grid_acceleration(qz_sim *sim);
 QZ_API int qz_particle_acceleration(qz_sim *sim);

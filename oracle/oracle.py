@@ -37,7 +37,7 @@ class Sim(C.Structure):
     _fields_ = [("p", Params), ("n", C.c_long)] + [
         (k, _P) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m",
                           "pot", "pot_old", "d", "gax", "gay", "gaz")
-    ] + [("vcycles_total", C.c_long), ("last_vcycles", C.c_int)]
+    ] + [("vcycles_total", C.c_long), ("last_vcycles", C.c_int), ("head_mass", C.c_double)]
 
 
 _lib = None
@@ -121,7 +121,7 @@ class OracleSim:
             raise RuntimeError("oracle step failed")
 
     def particles(self) -> dict:
-        n = self.n
+        n = int(self.s.n)
         return {k: np.ctypeslib.as_array(getattr(self.s, k), shape=(n,)).copy()
                 for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
 

@@ -51,6 +51,9 @@ long qzo_grid_points(int L)
 /* initial_potential_and_acceleration_head.c:297-334: analytic point-mass
  * potential and acceleration about (0.5, 0.5, 0.5) at every box point
  * 0 .. 2^L+1 per axis (the last grid layer stays zero, as after calloc). */
+static void qzo_initial_head_periodic(const qzo_params *p, double *pot, double *ax, double *ay,
+                                      double *az);
+
 void qzo_initial_head(const qzo_params *p, double *pot, double *ax, double *ay, double *az)
 {
     int nc = 1 << p->L;
@@ -62,6 +65,11 @@ void qzo_initial_head(const qzo_params *p, double *pot, double *ax, double *ay, 
     memset(ax, 0, cap * sizeof(double));
     memset(ay, 0, cap * sizeof(double));
     memset(az, 0, cap * sizeof(double));
+    if (p->bdry == 0)
+    {
+        qzo_initial_head_periodic(p, pot, ax, ay, az);
+        return;
+    }
     for (int k = 0; k < bside; k++)
     {
         double ak = (k - 1) * H - 0.5;
@@ -84,6 +92,133 @@ void qzo_initial_head(const qzo_params *p, double *pot, double *ax, double *ay, 
             }
         }
     }
+}
+
+/* initial_potential_and_acceleration_head.c:78-296 (periodic boundaries): only
+ * points with a box coordinate equal to 1 (coordinates 1 .. 2^L, k outer, i
+ * inner) are written, with -G M / d, d the smallest distance from the centre
+ * over the point and its images on the far faces (coordinate gl = 2^L + 1);
+ * the point's acceleration -G M (a_i, a_j, a_k) / d^3 is copied to the images.
+ * The image lists keep the reference's indices as written, including the ones
+ * whose x coordinate is 1 where the point's own i would be expected
+ * (:125-126, :178, :203, :225), so those far-face points are written from other
+ * points and some stay zero. */
+static void qzo_initial_head_periodic(const qzo_params *p, double *pot, double *ax, double *ay,
+                                      double *az)
+{
+    const int nc = 1 << p->L;
+    const long gs = nc + 3, gs2 = gs * gs;
+    const int gl = nc + 1;
+    const double H = 1.0 / nc;
+    const double a0 = (gl - 1) * H - 0.5;
+#define QZO_G(I, J, K) ((long)(I) + (long)(J) * gs + (long)(K) * gs2)
+    for (int k = 1; k < gl; k++)
+    {
+        const double ak = (k - 1) * H - 0.5;
+        for (int j = 1; j < gl; j++)
+        {
+            const double aj = (j - 1) * H - 0.5;
+            for (int i = 1; i < gl; i++)
+            {
+                const double ai = (i - 1) * H - 0.5;
+                long idx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                double dist = 0.0, d0, d1, d2, d3;
+                int cnt = 0;
+                if (i == 1)
+                {
+                    idx[0] = QZO_G(i, j, k);
+                    idx[1] = QZO_G(gl, j, k);
+                    d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                    d1 = sqrt(a0 * a0 + aj * aj + ak * ak);
+                    dist = d0 < d1 ? d0 : d1;
+                    cnt++;
+                }
+                if (j == 1)
+                {
+                    if (cnt == 0)
+                    {
+                        idx[0] = QZO_G(i, j, k);
+                        idx[1] = QZO_G(1, gl, k);
+                        d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                        d1 = sqrt(ai * ai + a0 * a0 + ak * ak);
+                        dist = d0 < d1 ? d0 : d1;
+                    }
+                    else
+                    {
+                        idx[2] = QZO_G(1, gl, k);
+                        idx[3] = QZO_G(gl, gl, k);
+                        d2 = sqrt(ai * ai + a0 * a0 + ak * ak);
+                        d3 = sqrt(a0 * a0 + a0 * a0 + ak * ak);
+                        dist = dist < d2 ? dist : d2;
+                        dist = dist < d3 ? dist : d3;
+                    }
+                    cnt++;
+                }
+                if (k == 1)
+                {
+                    if (cnt == 0)
+                    {
+                        idx[0] = QZO_G(i, j, k);
+                        idx[1] = QZO_G(1, j, gl);
+                        d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                        d1 = sqrt(ai * ai + aj * aj + a0 * a0);
+                        dist = d0 < d1 ? d0 : d1;
+                    }
+                    else if (cnt == 1)
+                    {
+                        if (i == 1)
+                        {
+                            idx[2] = QZO_G(1, j, gl);
+                            idx[3] = QZO_G(gl, j, gl);
+                            d2 = sqrt(ai * ai + aj * aj + a0 * a0);
+                            d3 = sqrt(a0 * a0 + aj * aj + a0 * a0);
+                        }
+                        else
+                        {
+                            idx[2] = QZO_G(1, j, gl);
+                            idx[3] = QZO_G(i, gl, gl);
+                            d2 = sqrt(ai * ai + aj * aj + a0 * a0);
+                            d3 = sqrt(ai * ai + a0 * a0 + a0 * a0);
+                        }
+                        dist = dist < d2 ? dist : d2;
+                        dist = dist < d3 ? dist : d3;
+                    }
+                    else
+                    {
+                        idx[4] = QZO_G(1, j, gl);
+                        idx[5] = QZO_G(gl, j, gl);
+                        idx[6] = QZO_G(1, gl, gl);
+                        idx[7] = QZO_G(gl, gl, gl);
+                        const double e4 = sqrt(ai * ai + aj * aj + a0 * a0);
+                        const double e5 = sqrt(a0 * a0 + aj * aj + a0 * a0);
+                        const double e6 = sqrt(ai * ai + a0 * a0 + a0 * a0);
+                        const double e7 = sqrt(a0 * a0 + a0 * a0 + a0 * a0);
+                        dist = dist < e4 ? dist : e4;
+                        dist = dist < e5 ? dist : e5;
+                        dist = dist < e6 ? dist : e6;
+                        dist = dist < e7 ? dist : e7;
+                    }
+                    cnt++;
+                }
+                if (cnt == 0)
+                    continue;
+                const double c = -p->G * p->total_mass / dist;
+                for (int l = 0; l < (1 << cnt); l++)
+                    pot[idx[l]] = c;
+                const double c3 = -p->G * p->total_mass / (dist * dist * dist);
+                ax[idx[0]] = c3 * ai;
+                ay[idx[0]] = c3 * aj;
+                az[idx[0]] = c3 * ak;
+                for (int l = 1; l < (1 << cnt); l++)
+                {
+                    ax[idx[l]] = ax[idx[0]];
+                    ay[idx[l]] = ay[idx[0]];
+                    az[idx[l]] = az[idx[0]];
+                }
+            }
+        }
+    }
+#undef QZO_G
 }
 
 /* grid_density.c:35-111 (head): CIC scatter of 4 pi G m / H^3 onto the 8
@@ -590,18 +725,29 @@ void qzo_grid_accel_head(const qzo_params *p, const double *pot, double *ax, dou
             for (long i = 2; i <= nc; i++)
             {
                 long g = i + j * D + k * D2;
-                if (p->force_stencil == 1 && i >= 3 && i <= nc - 1)
-                    ax[g] = (pot[g - 1] - pot[g + 1]) * t3h - (pot[g - 2] - pot[g + 2]) * o12h;
-                else
-                    ax[g] = o2h * (pot[g - 1] - pot[g + 1]);
-                if (p->force_stencil == 1 && j >= 3 && j <= nc - 1)
-                    ay[g] = (pot[g - D] - pot[g + D]) * t3h - (pot[g - 2 * D] - pot[g + 2 * D]) * o12h;
-                else
-                    ay[g] = o2h * (pot[g - D] - pot[g + D]);
-                if (p->force_stencil == 1 && k >= 3 && k <= nc - 1)
-                    az[g] = (pot[g - D2] - pot[g + D2]) * t3h - (pot[g - 2 * D2] - pot[g + 2 * D2]) * o12h;
-                else
-                    az[g] = o2h * (pot[g - D2] - pot[g + D2]);
+                /* periodic (grid_acceleration.c:139-145, 159-165, 179-185): at box
+                 * coordinate 2 the -2 neighbour is taken 2^L further, at 2^L the
+                 * +2 neighbour 2^L back */
+                const long sx[3] = {1, D, D2};
+                const long c[3] = {i, j, k};
+                double *out[3] = {ax, ay, az};
+                for (int q = 0; q < 3; q++)
+                {
+                    const long s = sx[q];
+                    if (p->force_stencil == 1 && c[q] >= 3 && c[q] <= nc - 1)
+                        out[q][g] = (pot[g - s] - pot[g + s]) * t3h - (pot[g - 2 * s] - pot[g + 2 * s]) * o12h;
+                    else if (p->force_stencil == 1 && p->bdry == 0)
+                    {
+                        long n7 = g + 2 * s, n8 = g - 2 * s;
+                        if (c[q] == 2)
+                            n8 += (long)nc * s;
+                        else
+                            n7 -= (long)nc * s;
+                        out[q][g] = (pot[g - s] - pot[g + s]) * t3h - (pot[n8] - pot[n7]) * o12h;
+                    }
+                    else
+                        out[q][g] = o2h * (pot[g - s] - pot[g + s]);
+                }
             }
 }
 
@@ -666,11 +812,43 @@ int qzo_update_A_head(const qzo_params *p, long n, double dt, double *x, double 
                     A[c][i] *= -1.0;
                 }
                 else
-                    return 1; /* outflow removal is not restated */
+                    return 1; /* outflow: qzo_update_A_outflow */
             }
         }
     }
     return 0;
+}
+
+/* particle_updating.c:123-196 (outflow, head only): particles in index order;
+ * one that leaves [0, 1) on any axis is removed -- the head's mass drops by
+ * the mass at its slot, the count drops by one and the last particle's x, v
+ * and a move into the slot (the mass array is not moved), and the loop goes
+ * on with the next index, so the moved particle is not advanced in this step.
+ * Returns the new count (0: none left, an error there). */
+long qzo_update_A_outflow(long n, double dt, double *x, double *y, double *z, double *vx,
+                          double *vy, double *vz, double *ax, double *ay, double *az,
+                          const double *m, double *node_mass)
+{
+    double *F[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    for (long i = 0; i < n; i++)
+    {
+        vx[i] += ax[i] * dt * 0.5;
+        vy[i] += ay[i] * dt * 0.5;
+        vz[i] += az[i] * dt * 0.5;
+        x[i] += vx[i] * dt;
+        y[i] += vy[i] * dt;
+        z[i] += vz[i] * dt;
+        if (x[i] < 0.0 || x[i] >= 1.0 || y[i] < 0.0 || y[i] >= 1.0 || z[i] < 0.0 || z[i] >= 1.0)
+        {
+            *node_mass -= m[i];
+            n--;
+            for (int q = 0; q < 9; q++)
+                F[q][i] = F[q][n];
+            if (n == 0)
+                return 0;
+        }
+    }
+    return n;
 }
 
 /* particle_updating.c:2677-2688 */
@@ -727,7 +905,8 @@ int qzo_sim_init(qzo_sim *s, const qzo_params *p, long n, const double *x, const
     qzo_initial_head(&s->p, s->pot, s->gax, s->gay, s->gaz);
     /* step 0: main.c:296-338 */
     qzo_deposit_head(&s->p, n, s->x, s->y, s->z, s->m, s->d);
-    int it = qzo_potential_head(&s->p, s->pot, s->pot_old, s->d, s->p.total_mass);
+    s->head_mass = s->p.total_mass; /* initialization.c:190 */
+    int it = qzo_potential_head(&s->p, s->pot, s->pot_old, s->d, s->head_mass);
     s->last_vcycles = it;
     if (it < 0)
         return 1;
@@ -741,7 +920,14 @@ int qzo_sim_init(qzo_sim *s, const qzo_params *p, long n, const double *x, const
 int qzo_sim_step(qzo_sim *s, double dt)
 {
     long n = s->n;
-    if (qzo_update_A_head(&s->p, n, dt, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az))
+    if (s->p.bdry == 2)
+    {
+        n = s->n = qzo_update_A_outflow(n, dt, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay,
+                                        s->az, s->m, &s->head_mass);
+        if (n == 0)
+            return 1;
+    }
+    else if (qzo_update_A_head(&s->p, n, dt, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az))
         return 1;
     long cap = qzo_grid_points(s->p.L);
     memset(s->ax, 0, n * sizeof(double));
@@ -749,7 +935,7 @@ int qzo_sim_step(qzo_sim *s, double dt)
     memset(s->az, 0, n * sizeof(double));
     memset(s->d, 0, cap * sizeof(double));
     qzo_deposit_head(&s->p, n, s->x, s->y, s->z, s->m, s->d);
-    int it = qzo_potential_head(&s->p, s->pot, s->pot_old, s->d, s->p.total_mass);
+    int it = qzo_potential_head(&s->p, s->pot, s->pot_old, s->d, s->head_mass);
     s->last_vcycles = it;
     if (it < 0)
         return 1;

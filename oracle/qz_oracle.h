@@ -79,6 +79,10 @@ void qzo_gather_head(const qzo_params *p, long n, const double *x, const double 
 /* particle_updating.c:39-207 (bdry 0/1; outflow not restated) */
 int qzo_update_A_head(const qzo_params *p, long n, double dt, double *x, double *y, double *z,
                       double *vx, double *vy, double *vz, double *ax, double *ay, double *az);
+/* particle_updating.c:123-196 (outflow, head only); returns the new count */
+long qzo_update_A_outflow(long n, double dt, double *x, double *y, double *z, double *vx,
+                          double *vy, double *vz, double *ax, double *ay, double *az,
+                          const double *m, double *node_mass);
 /* particle_updating.c:2677-2688 */
 void qzo_update_B_head(long n, double dt, double *vx, double *vy, double *vz,
                        const double *ax, const double *ay, const double *az);
@@ -97,6 +101,7 @@ typedef struct {
     double *pot, *pot_old, *d, *gax, *gay, *gaz;
     long vcycles_total;
     int last_vcycles;
+    double head_mass; /* the head's node_mass (falls with outflow removals) */
 } qzo_sim;
 
 int qzo_sim_init(qzo_sim *s, const qzo_params *p, long n, const double *x, const double *y,

@@ -96,6 +96,8 @@ def load() -> C.CDLL:
         "qz_grid_density": ([vp], C.c_int),
         "qz_potential": ([vp], C.c_int),
         "qz_potential_head_node": ([vp], C.c_int),
+        "qz_outflow_removed": ([vp, C.POINTER(C.c_long), _I, _I], C.c_int),
+        "qz_head_mass": ([vp], C.c_double),
         "qz_potential_branches": ([vp], C.c_int),
         "qz_grid_acceleration": ([vp], C.c_int),
         "qz_particle_acceleration": ([vp], C.c_int),
@@ -309,6 +311,18 @@ class Simulation:
 
     def init_forces(self) -> None:
         _check(self.lib.qz_init_forces(self.h))
+
+    def outflow_removed(self):
+        """(count, slots, sources) of the last step's outflow removals."""
+        cnt = C.c_long()
+        _check(self.lib.qz_outflow_removed(self.h, C.byref(cnt), None, None))
+        slots = np.zeros(max(cnt.value, 1), dtype=np.int32)
+        srcs = np.zeros(max(cnt.value, 1), dtype=np.int32)
+        _check(self.lib.qz_outflow_removed(self.h, C.byref(cnt), _p(slots), _p(srcs)))
+        return cnt.value, slots[:cnt.value], srcs[:cnt.value]
+
+    def head_mass(self) -> float:
+        return float(self.lib.qz_head_mass(self.h))
 
     def write_snapshot(self, path: str, actual_time: float, units=None,
                        observables_type: int = -1, wait: bool = True) -> None:

@@ -2131,7 +2131,7 @@ int head_cg_solve(qz_sim *s)
         launch(s, QZ_PROF_OTHER, 4.0 * L.intr_total, k_head_intr,
                dim3(blocks_for(L.intr_total, 256)), dim3(256), Lv, s->D, L.intr.p);
     }
-    L.h[0].mass = s->cfg.total_mass;
+    L.h[0].mass = s->head_mass;
     L.h[0].nptcl = (int)s->n;
     if (!upload_nodes(s, L))
         return QZ_FAILURE;

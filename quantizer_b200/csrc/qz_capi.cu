@@ -373,6 +373,8 @@ int qz_destroy(qz_sim *s)
     free_levels(s);
     amr_free(s);
     adjoint_free(s);
+    s->ofl_state.release(s->mem);
+    s->ofl_int.release(s->mem);
     if (s->mem.pool)
         pool_free(s->mem, s->scan_tmp);
     if (s->stream)
@@ -381,6 +383,8 @@ int qz_destroy(qz_sim *s)
         cudaMemPoolTrimTo(s->mem.pool, 0); // unused memory back to the device
     if (s->h_flags)
         cudaFreeHost(s->h_flags);
+    if (s->h_ofl)
+        cudaFreeHost(s->h_ofl);
     if (s->h_ts)
         cudaFreeHost(s->h_ts);
     if (s->h_stage)
@@ -416,11 +420,13 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
                   "box_extra >= 2");
         return QZ_FAILURE;
     }
-    if (cfg->bdry != 1)
+    if (cfg->bdry < 0 || cfg->bdry > 2 || (cfg->bdry != 1 && cfg->lmax > cfg->lmin))
     {
-        // the periodic head boundary of initial_potential_and_acceleration_head.c:66-296
-        // and outflow particle removal are not built
-        set_error("qz_create: bdry=%d not supported (1 reflexive only)", cfg->bdry);
+        // periodic and outflow boundaries are built for head-only runs; the
+        // refinement tree follows the reflexive rules (no periodic ghost cells,
+        // no removal inside refinement nodes)
+        set_error("qz_create: bdry=%d not supported%s", cfg->bdry,
+                  cfg->lmax > cfg->lmin ? " with refinement (reflexive only)" : "");
         return QZ_FAILURE;
     }
     if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 2 || cfg->cycle < 0 ||
@@ -453,6 +459,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
         return QZ_FAILURE;
     }
     s->cap = n_capacity;
+    s->head_mass = cfg->total_mass; // initialization.c:190
     s->L = cfg->lmin;
     s->D = (1L << s->L) + 3;
     s->gpts = s->D * s->D * s->D;
@@ -521,6 +528,8 @@ int qz_set_particles(qz_sim *s, long n, const double *x, const double *y, const 
         return QZ_FAILURE;
     }
     s->n = n;
+    s->head_mass = s->cfg.total_mass;
+    s->ofl_removed = 0;
     bool ok = h2d(s, s->x, x, n) && h2d(s, s->y, y, n) && h2d(s, s->z, z, n) &&
               h2d(s, s->vx, vx, n) && h2d(s, s->vy, vy, n) && h2d(s, s->vz, vz, n) &&
               h2d(s, s->m, m, n);
@@ -634,6 +643,28 @@ int qz_potential(qz_sim *s)
         return QZ_FAILURE;
     return amr_on(s) ? amr_potential(s) : QZ_SUCCESS;
 }
+
+int qz_outflow_removed(qz_sim *s, long *count, int *slots, int *sources)
+{
+    if (!s || !count)
+        return QZ_FAILURE;
+    *count = s->ofl_removed;
+    if (s->ofl_removed == 0 || (!slots && !sources))
+        return QZ_SUCCESS;
+    const long n0 = s->ofl_layout_n;
+    const int *base = s->ofl_int.p;
+    bool ok = true;
+    if (slots)
+        ok = ok && check_cuda(cudaMemcpyAsync(slots, base + 2 * n0, s->ofl_removed * sizeof(int),
+                                              cudaMemcpyDeviceToHost, s->stream), "removed");
+    if (sources)
+        ok = ok && check_cuda(cudaMemcpyAsync(sources, base + 3 * n0, s->ofl_removed * sizeof(int),
+                                              cudaMemcpyDeviceToHost, s->stream), "removed");
+    return ok && check_cuda(cudaStreamSynchronize(s->stream), "removed sync") ? QZ_SUCCESS
+                                                                               : QZ_FAILURE;
+}
+
+double qz_head_mass(const qz_sim *s) { return s ? s->head_mass : 0.0; }
 
 int qz_potential_head_node(qz_sim *s) { return s ? potential_head(s) : QZ_FAILURE; }
 

@@ -61,6 +61,8 @@ static struct {
     double *w_sor_head, *tol, *tol2;
     int *ref_ptcl, *n_exp, *box_extra;
     double *ref_mass;
+    int **ptcl_id;
+    double *total_mass_final;
     int resolved;
 } R;
 
@@ -137,6 +139,8 @@ static int resolve(void)
     R.ref_mass = need("ref_criterion_mass", &ok);
     R.n_exp = need("n_exp", &ok);
     R.box_extra = need("min_box_extra_size_per_side_real", &ok);
+    R.ptcl_id = need("GL_ptcl_ID", &ok);
+    R.total_mass_final = need("GL_total_mass_final", &ok);
     R.resolved = ok;
     return ok;
 }
@@ -376,6 +380,43 @@ static int amr_update_refused(void)
     return REF_FAILURE;
 }
 
+/* Outflow removals of the last update, applied to the host's bookkeeping in
+ * the reference's order (particle_updating.c:164-176): total and head masses,
+ * counts, and the IDs, which move with the particles (the masses do not). */
+static int apply_removals(void)
+{
+    long cnt = 0;
+    if (qz_outflow_removed(g_sim, &cnt, NULL, NULL))
+        return fail("outflow removals");
+    if (cnt == 0)
+        return REF_SUCCESS;
+    int *slots = (int *)malloc(cnt * sizeof(int)), *srcs = (int *)malloc(cnt * sizeof(int));
+    if (!slots || !srcs || qz_outflow_removed(g_sim, &cnt, slots, srcs))
+    {
+        free(slots);
+        free(srcs);
+        return fail("outflow removals");
+    }
+    struct node *h = *R.ptr_tree;
+    for (long r = 0; r < cnt; r++)
+    {
+        const double m = (*R.ptcl_mass)[slots[r]];
+        *R.total_mass_final -= m;
+        (*R.no_ptcl_final)--;
+        h->node_mass -= m;
+        h->no_ptcl_full_node--;
+        (*R.ptcl_id)[slots[r]] = (*R.ptcl_id)[srcs[r]];
+    }
+    free(slots);
+    free(srcs);
+    if (*R.no_ptcl_final == 0)
+    {
+        printf("Error, There are no particles in the simulation\n");
+        return REF_FAILURE;
+    }
+    return REF_SUCCESS;
+}
+
 /* particle_updating.c:2584-2675 */
 int particle_updating_A(double dt)
 {
@@ -383,7 +424,7 @@ int particle_updating_A(double dt)
         return REF_FAILURE;
     if (g_amr)
         return amr_update_refused();
-    if (qz_particle_updating_A(g_sim, dt) ||
+    if (qz_particle_updating_A(g_sim, dt) || apply_removals() ||
         qz_get_particles(g_sim, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
                          *R.ptcl_vz, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az))
         return fail("particle_updating_A");

@@ -300,6 +300,16 @@ struct qz_sim {
     qz::AmrLevel head_cg; // the head as a one-node level (head_pot_method 1)
     qz::Adjoint *adj = nullptr; // adjoint buffers (qz_force_vjp, qz_adjoint_final_loss)
     qz::Snapshot *snap = nullptr; // snapshot staging and writer thread (qz_write_snapshot)
+    // the head node's mass (node_mass): the configured total mass, lowered by
+    // outflow removals; the convergence tests of the head solve use it
+    double head_mass = 0.0;
+    // outflow boundaries: advanced state (9 n), flags / scan / removal lists, the
+    // last step's removals (count on the host, lists on the device)
+    qz::DBuf<double> ofl_state;
+    qz::DBuf<int> ofl_int;
+    double *h_ofl = nullptr; // pinned: bound, count, head mass
+    long ofl_removed = 0;
+    long ofl_layout_n = 0; // particle count the lists of the last step were laid out for
     int amr_nlev = 1;                  // levels in use this step
     std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
     qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)

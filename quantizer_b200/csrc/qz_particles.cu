@@ -43,6 +43,130 @@ __global__ void k_initial_head(int L, long D, double G, double M, double *__rest
     az[g] = coeff * ak;
 }
 
+// Periodic boundaries (initial_potential_and_acceleration_head.c:78-296): only
+// points with a box coordinate equal to 1 (coordinates 1 .. 2^L, k outer, i
+// inner) are written, with -G M / d, d the smallest distance from the centre
+// over the point and its images on the far faces (coordinate gl = 2^L + 1); the
+// point's acceleration -G M (a_i, a_j, a_k) / d^3 is copied to its images.  The
+// image indices are the reference's as written (:125-126, :178, :203, :225 use
+// x coordinate 1 where the point's own i would be expected), so later points
+// overwrite some far-face values and others stay zero.  Writes of a k-plane
+// land in that plane (k = 1 also in plane gl), so one thread per plane keeps
+// the reference's write order.
+__device__ __forceinline__ long pgi(long i, long j, long k, long D) { return i + j * D + k * D * D; }
+
+__global__ void k_initial_head_periodic(int L, long D, double G, double M,
+                                        double *__restrict__ pot, double *__restrict__ ax,
+                                        double *__restrict__ ay, double *__restrict__ az)
+{
+    const int nc = 1 << L, gl = nc + 1;
+    const int k = 1 + (int)((long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= gl)
+        return;
+    const double H = 1.0 / nc;
+    const double a0 = (gl - 1) * H - 0.5;
+    const double ak = (k - 1) * H - 0.5;
+    for (int j = 1; j < gl; j++)
+    {
+        const double aj = (j - 1) * H - 0.5;
+        for (int i = 1; i < gl; i++)
+        {
+            if (i != 1 && j != 1 && k != 1)
+                continue;
+            const double ai = (i - 1) * H - 0.5;
+            long idx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double dist = 0.0;
+            int cnt = 0;
+            if (i == 1)
+            {
+                idx[0] = pgi(i, j, k, D);
+                idx[1] = pgi(gl, j, k, D);
+                const double d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                const double d1 = sqrt(a0 * a0 + aj * aj + ak * ak);
+                dist = d0 < d1 ? d0 : d1;
+                cnt++;
+            }
+            if (j == 1)
+            {
+                if (cnt == 0)
+                {
+                    idx[0] = pgi(i, j, k, D);
+                    idx[1] = pgi(1, gl, k, D);
+                    const double d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                    const double d1 = sqrt(ai * ai + a0 * a0 + ak * ak);
+                    dist = d0 < d1 ? d0 : d1;
+                }
+                else
+                {
+                    idx[2] = pgi(1, gl, k, D);
+                    idx[3] = pgi(gl, gl, k, D);
+                    const double d2 = sqrt(ai * ai + a0 * a0 + ak * ak);
+                    const double d3 = sqrt(a0 * a0 + a0 * a0 + ak * ak);
+                    dist = dist < d2 ? dist : d2;
+                    dist = dist < d3 ? dist : d3;
+                }
+                cnt++;
+            }
+            if (k == 1)
+            {
+                if (cnt == 0)
+                {
+                    idx[0] = pgi(i, j, k, D);
+                    idx[1] = pgi(1, j, gl, D);
+                    const double d0 = sqrt(ai * ai + aj * aj + ak * ak);
+                    const double d1 = sqrt(ai * ai + aj * aj + a0 * a0);
+                    dist = d0 < d1 ? d0 : d1;
+                }
+                else if (cnt == 1)
+                {
+                    double d2, d3;
+                    idx[2] = pgi(1, j, gl, D);
+                    d2 = sqrt(ai * ai + aj * aj + a0 * a0);
+                    if (i == 1)
+                    {
+                        idx[3] = pgi(gl, j, gl, D);
+                        d3 = sqrt(a0 * a0 + aj * aj + a0 * a0);
+                    }
+                    else
+                    {
+                        idx[3] = pgi(i, gl, gl, D);
+                        d3 = sqrt(ai * ai + a0 * a0 + a0 * a0);
+                    }
+                    dist = dist < d2 ? dist : d2;
+                    dist = dist < d3 ? dist : d3;
+                }
+                else
+                {
+                    idx[4] = pgi(1, j, gl, D);
+                    idx[5] = pgi(gl, j, gl, D);
+                    idx[6] = pgi(1, gl, gl, D);
+                    idx[7] = pgi(gl, gl, gl, D);
+                    const double e4 = sqrt(ai * ai + aj * aj + a0 * a0);
+                    const double e5 = sqrt(a0 * a0 + aj * aj + a0 * a0);
+                    const double e6 = sqrt(ai * ai + a0 * a0 + a0 * a0);
+                    const double e7 = sqrt(a0 * a0 + a0 * a0 + a0 * a0);
+                    dist = dist < e4 ? dist : e4;
+                    dist = dist < e5 ? dist : e5;
+                    dist = dist < e6 ? dist : e6;
+                    dist = dist < e7 ? dist : e7;
+                }
+                cnt++;
+            }
+            const double c = -G * M / dist;
+            for (int l = 0; l < (1 << cnt); l++)
+                pot[idx[l]] = c;
+            const double c3 = -G * M / (dist * dist * dist);
+            const double vx = c3 * ai, vy = c3 * aj, vz = c3 * ak;
+            for (int l = 0; l < (1 << cnt); l++)
+            {
+                ax[idx[l]] = vx;
+                ay[idx[l]] = vy;
+                az[idx[l]] = vz;
+            }
+        }
+    }
+}
+
 int head_initial(qz_sim *s)
 {
     size_t bytes = (size_t)s->gpts * sizeof(double);
@@ -50,6 +174,14 @@ int head_initial(qz_sim *s)
     cudaMemsetAsync(s->gax, 0, bytes, s->stream);
     cudaMemsetAsync(s->gay, 0, bytes, s->stream);
     cudaMemsetAsync(s->gaz, 0, bytes, s->stream);
+    if (s->cfg.bdry == 0)
+    {
+        const int nc = 1 << s->L;
+        launch(s, QZ_PROF_OTHER, 96.0 * 3 * nc * nc, k_initial_head_periodic,
+               dim3(blocks_for(nc, 128)), dim3(128), s->L, s->D, s->cfg.G, s->cfg.total_mass,
+               s->pot, s->gax, s->gay, s->gaz);
+        return check_cuda(cudaGetLastError(), "initial head") ? QZ_SUCCESS : QZ_FAILURE;
+    }
     long B = (1L << s->L) + 2;
     launch(s, QZ_PROF_OTHER, 32.0 * B * B * B, k_initial_head, dim3(blocks_for(B * B * B, 256)), dim3(256), s->L, s->D, s->cfg.G, s->cfg.total_mass, s->pot, s->gax, s->gay, s->gaz);
     return check_cuda(cudaGetLastError(), "initial head") ? QZ_SUCCESS : QZ_FAILURE;
@@ -283,9 +415,24 @@ int deposit_head(qz_sim *s)
 // (grid_acceleration.c:36-76).  stencil 1 (grid_acceleration.c:78-197): the
 // 5-point difference along an axis whose cells at -2 and +1 are inside the
 // simulation (head box coordinates 3..2^L-1), else the 3-point one.
-__global__ void k_grid_accel_head(int L, long D, int stencil, const double *__restrict__ pot,
-                                  double *__restrict__ ax, double *__restrict__ ay,
-                                  double *__restrict__ az)
+// Periodic boundaries with stencil 1 (grid_acceleration.c:139-145, 159-165,
+// 179-185): where the 5-point condition fails (box coordinate 2 or 2^L) the
+// 5-point difference still applies, the -2 neighbour taken 2^L further at
+// coordinate 2 and the +2 neighbour 2^L back at coordinate 2^L.
+__device__ __forceinline__ double grad5_periodic(const double *__restrict__ pot, long g, long st,
+                                                 int c, int nc, double t3h, double o12h)
+{
+    long n7 = g + 2 * st, n8 = g - 2 * st;
+    if (c == 2)
+        n8 += (long)nc * st;
+    else
+        n7 -= (long)nc * st;
+    return (pot[g - st] - pot[g + st]) * t3h - (pot[n8] - pot[n7]) * o12h;
+}
+
+__global__ void k_grid_accel_head(int L, long D, int stencil, int periodic,
+                                  const double *__restrict__ pot, double *__restrict__ ax,
+                                  double *__restrict__ ay, double *__restrict__ az)
 {
     const int m = (1 << L) - 1; // interior points per axis: box coords 2..2^L
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -306,15 +453,19 @@ __global__ void k_grid_accel_head(int L, long D, int stencil, const double *__re
     const double o12h = 1.0 / (12.0 * H);
     const double t3h = 2.0 / (3.0 * H);
     const int hi = (1 << L) - 1;
+    const int nc = 1 << L;
     ax[g] = (i >= 3 && i <= hi)
                 ? (pot[g - 1] - pot[g + 1]) * t3h - (pot[g - 2] - pot[g + 2]) * o12h
-                : o2h * (pot[g - 1] - pot[g + 1]);
+            : periodic ? grad5_periodic(pot, g, 1, i, nc, t3h, o12h)
+                       : o2h * (pot[g - 1] - pot[g + 1]);
     ay[g] = (j >= 3 && j <= hi)
                 ? (pot[g - D] - pot[g + D]) * t3h - (pot[g - 2 * D] - pot[g + 2 * D]) * o12h
-                : o2h * (pot[g - D] - pot[g + D]);
+            : periodic ? grad5_periodic(pot, g, D, j, nc, t3h, o12h)
+                       : o2h * (pot[g - D] - pot[g + D]);
     az[g] = (k >= 3 && k <= hi)
                 ? (pot[g - D2] - pot[g + D2]) * t3h - (pot[g - 2 * D2] - pot[g + 2 * D2]) * o12h
-                : o2h * (pot[g - D2] - pot[g + D2]);
+            : periodic ? grad5_periodic(pot, g, D2, k, nc, t3h, o12h)
+                       : o2h * (pot[g - D2] - pot[g + D2]);
 }
 
 int grid_accel_head_from(qz_sim *s, const double *pot)
@@ -324,7 +475,8 @@ int grid_accel_head_from(qz_sim *s, const double *pot)
         return QZ_SUCCESS;
     const double bytes = (s->cfg.force_stencil ? 56.0 : 32.0) * m * m * m;
     launch(s, QZ_PROF_GRADIENT, bytes, k_grid_accel_head, dim3(blocks_for(m * m * m, 256)), dim3(256),
-           s->L, s->D, s->cfg.force_stencil, pot, s->gax, s->gay, s->gaz);
+           s->L, s->D, s->cfg.force_stencil, s->cfg.bdry == 0 ? 1 : 0, pot, s->gax, s->gay,
+           s->gaz);
     return check_cuda(cudaGetLastError(), "grid accel") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
@@ -438,10 +590,170 @@ __global__ void k_kick_drift(long n, double dt, int bdry, double *__restrict__ x
     az[i] = gz;
 }
 
+// ---- outflow boundaries (particle_updating.c:123-196) ------------------------------
+// The reference advances particles in index order; one that leaves [0, 1) on any
+// axis is removed: the head's mass drops by the mass at its slot, the count by
+// one, the last particle's x, v, a move into the slot (masses stay in their
+// slots) and the loop continues with the next index, so the moved particle is
+// not advanced in this step.  In parallel: every particle is advanced into a
+// copy and flagged; with E(i) the flagged particles before i, index i is
+// visited while i + E(i) < n, the first k indices; the E(k) visited flagged
+// slots each receive the un-advanced state of index n - 1 - E(i); the count
+// becomes n - E(k).
+__global__ void k_outflow_advance(long n, double dt, const double *__restrict__ x,
+                                  const double *__restrict__ y, const double *__restrict__ z,
+                                  const double *__restrict__ vx, const double *__restrict__ vy,
+                                  const double *__restrict__ vz, const double *__restrict__ ax,
+                                  const double *__restrict__ ay, const double *__restrict__ az,
+                                  double *__restrict__ st, int *__restrict__ flag)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double qx = vx[i], qy = vy[i], qz = vz[i];
+    qx += ax[i] * dt * 0.5;
+    qy += ay[i] * dt * 0.5;
+    qz += az[i] * dt * 0.5;
+    double px = x[i], py = y[i], pz = z[i];
+    px += qx * dt;
+    py += qy * dt;
+    pz += qz * dt;
+    st[i] = px;
+    st[n + i] = py;
+    st[2 * n + i] = pz;
+    st[3 * n + i] = qx;
+    st[4 * n + i] = qy;
+    st[5 * n + i] = qz;
+    flag[i] = (px < 0.0 || px >= 1.0 || py < 0.0 || py >= 1.0 || pz < 0.0 || pz >= 1.0) ? 1 : 0;
+}
+
+// bound[0] = k (first i with i + E(i) >= n), bound[1] = E(k); E(n) = total.
+__global__ void k_outflow_bound(long n, const int *__restrict__ flag, const int *__restrict__ E,
+                                int *__restrict__ bound)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n)
+        return;
+    auto e_at = [&](long q) { return q < n ? (long)E[q] : (long)E[n - 1] + flag[n - 1]; };
+    const bool here = i + e_at(i) >= n;
+    const bool before = i > 0 && (i - 1) + e_at(i - 1) >= n;
+    if (here && !before)
+    {
+        bound[0] = (int)i;
+        bound[1] = (int)e_at(i);
+    }
+}
+
+__global__ void k_outflow_apply(long n, const double *__restrict__ st, const int *__restrict__ flag,
+                                const int *__restrict__ E, const int *__restrict__ bound,
+                                double *__restrict__ x, double *__restrict__ y,
+                                double *__restrict__ z, double *__restrict__ vx,
+                                double *__restrict__ vy, double *__restrict__ vz,
+                                double *__restrict__ ax, double *__restrict__ ay,
+                                double *__restrict__ az, int *__restrict__ slots,
+                                int *__restrict__ srcs)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long k = bound[0], nf = n - bound[1];
+    if (i >= k)
+        return;
+    double *F[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    if (!flag[i])
+    {
+        // visited and kept: its advanced state (i < k <= n - E(k) + ... is a kept slot)
+        for (int q = 0; q < 6; q++)
+            F[q][i] = st[q * n + i];
+        return;
+    }
+    const long r = E[i], src = n - 1 - r;
+    slots[r] = (int)i;
+    srcs[r] = (int)src;
+    if (i < nf) // a slot beyond the new count only drops its particle
+        for (int q = 0; q < 9; q++)
+            F[q][i] = F[q][src];
+}
+
+// the head's mass minus the removed slots' masses, in visiting order
+__global__ void k_outflow_mass(int removed, const int *__restrict__ slots,
+                               const double *__restrict__ m, const double *__restrict__ mass_in,
+                               double *__restrict__ out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0)
+        return;
+    double hm = mass_in[0];
+    for (int r = 0; r < removed; r++)
+        hm -= m[slots[r]];
+    out[0] = hm;
+}
+
+static int outflow_step(qz_sim *s, double dt)
+{
+    const long n = s->n;
+    if (!s->ofl_state.ensure(s->mem, 9 * n) || !s->ofl_int.ensure(s->mem, 4 * n + 8))
+    {
+        set_error("outflow buffers");
+        return QZ_FAILURE;
+    }
+    if (!s->h_ofl && !check_cuda(cudaMallocHost((void **)&s->h_ofl, 4 * sizeof(double)),
+                                 "outflow pinned"))
+        return QZ_FAILURE;
+    int *flag = s->ofl_int.p, *E = flag + n, *slots = flag + 2 * n, *srcs = flag + 3 * n,
+        *bound = flag + 4 * n;
+    double *dmass = s->red + s->red_blocks + 4; // two scratch words after the partials
+    launch(s, QZ_PROF_LEAPFROG, 148.0 * n, k_outflow_advance, dim3(blocks_for(n, 256)), dim3(256),
+           n, dt, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az, s->ofl_state.p, flag);
+    if (scan_exclusive(s, flag, E, n))
+        return QZ_FAILURE;
+    launch(s, QZ_PROF_LEAPFROG, 8.0 * n, k_outflow_bound, dim3(blocks_for(n + 1, 256)), dim3(256),
+           n, flag, E, bound);
+    launch(s, QZ_PROF_LEAPFROG, 104.0 * n, k_outflow_apply, dim3(blocks_for(n, 256)), dim3(256), n,
+           s->ofl_state.p, flag, E, bound, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay,
+           s->az, slots, srcs);
+    if (!check_cuda(cudaMemcpyAsync(s->h_ofl, bound, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                    s->stream), "outflow bound") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "outflow sync"))
+        return QZ_FAILURE;
+    int hb[2];
+    memcpy(hb, s->h_ofl, sizeof hb);
+    const long removed = hb[1];
+    s->ofl_removed = removed;
+    s->ofl_layout_n = n;
+    if (removed > 0)
+    {
+        s->h_ofl[2] = s->head_mass;
+        if (!check_cuda(cudaMemcpyAsync(dmass, &s->h_ofl[2], sizeof(double),
+                                        cudaMemcpyHostToDevice, s->stream), "outflow mass"))
+            return QZ_FAILURE;
+        launch(s, QZ_PROF_LEAPFROG, 8.0 * removed, k_outflow_mass, dim3(1), dim3(32), (int)removed,
+               slots, s->m, dmass, dmass + 1);
+        if (!check_cuda(cudaMemcpyAsync(&s->h_ofl[3], dmass + 1, sizeof(double),
+                                        cudaMemcpyDeviceToHost, s->stream), "outflow mass") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "outflow sync"))
+            return QZ_FAILURE;
+        s->head_mass = s->h_ofl[3];
+        s->n = n - removed;
+        // the captured check block holds the old mass in its thresholds
+        if (s->check_exec)
+        {
+            cudaGraphExecDestroy(s->check_exec);
+            s->check_exec = nullptr;
+        }
+    }
+    if (s->n == 0)
+    {
+        set_error("there are no particles in the simulation (all left through the outflow "
+                  "boundaries)");
+        return QZ_FAILURE;
+    }
+    return check_cuda(cudaGetLastError(), "outflow") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 int kick_drift(qz_sim *s, double dt)
 {
     if (s->n == 0)
         return QZ_SUCCESS;
+    if (s->cfg.bdry == 2)
+        return outflow_step(s, dt);
     launch(s, QZ_PROF_LEAPFROG, 144.0 * s->n, k_kick_drift, dim3(blocks_for(s->n, 256)), dim3(256), s->n, dt, s->cfg.bdry, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az);
     return check_cuda(cudaGetLastError(), "kick drift") ? QZ_SUCCESS : QZ_FAILURE;
 }

@@ -1457,7 +1457,7 @@ static int capture_check_block(qz_sim *s, int every)
     for (int q = 0; q < every && rc == QZ_SUCCESS; q++)
         rc = s->cfg.precision == QZ_PREC_MIXED ? mixed_iteration(s) : vcycle(s, 0, s->cfg.cycle);
     if (rc == QZ_SUCCESS)
-        rc = launch_check(s, s->cfg.total_mass);
+        rc = launch_check(s, s->head_mass);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     s->check_graph_kernels = s->stats.kernel_launches - before;
@@ -1475,7 +1475,7 @@ static int capture_check_block(qz_sim *s, int every)
 
 int poisson_error_head(qz_sim *s, int *converged)
 {
-    if (launch_check(s, s->cfg.total_mass))
+    if (launch_check(s, s->head_mass))
         return QZ_FAILURE;
     if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
         return QZ_FAILURE;
@@ -1508,7 +1508,7 @@ int potential_head(qz_sim *s)
             iter += k;
             if (iter % every == 0)
             {
-                if (launch_check(s, c.total_mass))
+                if (launch_check(s, s->head_mass))
                     return QZ_FAILURE;
                 if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
                     return QZ_FAILURE;
@@ -1549,7 +1549,7 @@ int potential_head(qz_sim *s)
         }
         if (iter % every == 0)
         {
-            if (launch_check(s, c.total_mass))
+            if (launch_check(s, s->head_mass))
                 return QZ_FAILURE;
             if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
                 return QZ_FAILURE;

@@ -54,5 +54,20 @@ def cghead_golden():
 
 
 @pytest.fixture(scope="session")
+def periodic_golden():
+    return golden("head_L4_periodic.npz")
+
+
+@pytest.fixture(scope="session")
+def periodic5_golden():
+    return golden("head_L4_periodic5.npz")
+
+
+@pytest.fixture(scope="session")
+def outflow_golden():
+    return golden("head_L4_outflow.npz")
+
+
+@pytest.fixture(scope="session")
 def timestep_golden():
     return golden("timestep_head_L4.npz")

@@ -16,6 +16,13 @@ sources (oracle/Makefile, target ``ref``):
   gradient as the multigrid smoother (solver 2).
 * ``head_L4_cghead.npz`` -- the head_L4 case with the head solved by the node
   conjugate gradient (head_pot_method = 1) instead of multigrid cycles.
+* ``head_L4_periodic.npz`` / ``head_L4_periodic5.npz`` -- periodic boundaries
+  (bdry_cond_type = 0; 3- and 5-point stencils) on the 1000-particle sphere
+  with 48 extra particles placed 1e-6 inside the faces and moving outwards, so
+  that they wrap in the first step; 3 steps.
+* ``head_L4_outflow.npz`` -- outflow boundaries (bdry_cond_type = 2) on the same
+  set: the particles that leave are removed (particle count and arrays after 3
+  steps, in the reference's order).
 * ``timestep_head_L4.npz`` -- the reference's timestep() (methods 0 and 1) on the
   states of the head_L4 case at steps 0 and 3 (_MAX_dt_ set to 1 so that the CFL
   condition decides), with its _MAX_dt_ and _CFL_.
@@ -60,6 +67,26 @@ def run_case(name: str, ic: dict, steps: int, dt: float, **kw) -> None:
         out["meta"] = np.array([kw.get("lmin", 5), steps, dt, summary["n"]], dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, name), **out)
     print("wrote", name, summary)
+
+
+def edge_ic(ic: dict) -> dict:
+    """The sphere plus 48 particles 1e-6 inside the six faces (8 per face),
+    moving outwards at speed 2 (box units per unit time)."""
+    rng = np.random.default_rng(5)
+    extra = {k: [] for k in ics.FIELDS}
+    for axis in range(3):
+        for side in (0, 1):
+            for _ in range(8):
+                pos = rng.uniform(0.2, 0.8, 3)
+                vel = rng.normal(0.0, 0.1, 3)
+                pos[axis] = 1e-6 if side == 0 else 1.0 - 1e-6
+                vel[axis] = -2.0 if side == 0 else 2.0
+                for q, k in enumerate(("x", "y", "z")):
+                    extra[k].append(pos[q])
+                for q, k in enumerate(("vx", "vy", "vz")):
+                    extra[k].append(vel[q])
+                extra["m"].append(ic["m"][0])
+    return {k: np.concatenate([ic[k], np.array(extra[k])]) for k in ics.FIELDS}
 
 
 def timestep_case(ic: dict, dt: float) -> None:
@@ -146,6 +173,12 @@ def main() -> None:
     for name, kw in cases:
         if not want or name in want:
             run_case(name, ic, dt=dt, **kw)
+    eic = edge_ic(ic)
+    for name, kw in (("head_L4_periodic.npz", dict(steps=3, lmin=4, bdry=0)),
+                     ("head_L4_periodic5.npz", dict(steps=3, lmin=4, bdry=0, stencil=1)),
+                     ("head_L4_outflow.npz", dict(steps=3, lmin=4, bdry=2))):
+        if not want or name in want:
+            run_case(name, eic, dt=dt, **kw)
     if not want or "timestep_head_L4.npz" in want:
         timestep_case(ic, dt)
     if not want or "arrays.npz" in want:

@@ -108,3 +108,20 @@ def test_array_kernels_bit_exact(arrays_golden):
         rho = g[key.replace("_out", "_in_rho")].copy()
         lib.qzo_multigrid(C.byref(p), O.ptr(phi), O.ptr(rho), n, t)
         np.testing.assert_array_equal(phi, g[key], err_msg=key)
+
+
+def test_head_pipeline_periodic_bit_exact(periodic_golden):
+    steps, s0, s1 = _run(periodic_golden, 4, bdry=0)
+    _assert_exact(periodic_golden, steps, s0, s1)
+
+
+def test_head_pipeline_periodic_five_point_bit_exact(periodic5_golden):
+    steps, s0, s1 = _run(periodic5_golden, 4, bdry=0, force_stencil=1)
+    _assert_exact(periodic5_golden, steps, s0, s1)
+
+
+def test_head_pipeline_outflow_bit_exact(outflow_golden):
+    g = outflow_golden
+    steps, s0, s1 = _run(g, 4, bdry=2)
+    assert s1[1]["x"].size == g[f"s{steps}_x"].size < s0[1]["x"].size
+    _assert_exact(g, steps, s0, s1)
