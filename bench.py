@@ -474,6 +474,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cg-variant", type=int, default=None,
+                    help="refinement conjugate gradient: 0 two reductions per iteration "
+                         "(the reference's order), 1 one reduction")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     K = args.steps if args.steps is not None else wl["steps"]
@@ -532,6 +535,9 @@ def main() -> int:
     ic = make_ic(wl, 1 + rank)
     dt = 1e-3 * ics.crossing_time(wl["a"])
     simcfg = dict(lmax=wl["lmin"] + wl["levels"], ref_ptcl=wl["ref_ptcl"])
+    if args.cg_variant is not None:
+        simcfg["cg_variant"] = args.cg_variant
+        config["cg_variant"] = args.cg_variant
     sim = core.Simulation(ic, wl["lmin"], precision=wl["precision"], **simcfg)
     ext = torch.cuda.ExternalStream(sim.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)

@@ -98,6 +98,10 @@ typedef struct qz_config {
     /* adjoint Poisson solves (qz_force_vjp, qz_adjoint_final_loss): multigrid
      * cycles until |r| <= adjoint_tol |rhs| (2-norms over the head interior) */
     double adjoint_tol;
+    /* refinement-node conjugate gradient: 0 the reference's two reductions per
+     * iteration, 1 one reduction per iteration (Chronopoulos-Gear arrangement:
+     * the same iterates in exact arithmetic, half the waits) */
+    int cg_variant;
 } qz_config;
 
 typedef struct qz_stats {

@@ -40,7 +40,7 @@ class Config(C.Structure):
         ("box_extra", C.c_int), ("branch_cg_cells", C.c_int), ("branch_sor_sweeps", C.c_int),
         ("w_sor_branch", C.c_double), ("cfl", C.c_double), ("max_dt", C.c_double),
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
-        ("adjoint_tol", C.c_double),
+        ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
     ]
 
 

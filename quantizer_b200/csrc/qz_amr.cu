@@ -603,7 +603,7 @@ static void free_level(const MemCtx &m, AmrLevel &L)
     for (auto *b : ib)
         b->release(m);
     DBuf<double> *db[] = {&L.gpot, &L.gpot_old, &L.gd, &L.gax, &L.gay, &L.gaz, &L.r, &L.p, &L.Ap,
-                          &L.apv, &L.chunk_part, &L.mass_part};
+                          &L.apv, &L.cg1, &L.chunk_part, &L.mass_part};
     for (auto *b : db)
         b->release(m);
     L.nodes.release(m);
@@ -1338,6 +1338,10 @@ struct CgArgs {
 };
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
+// Partial-sum slots are 128 bytes apart (one L2 line each): every block of a
+// node polls every slot of the node, so slots sharing lines would serialise the
+// polls and the publications of many chunks on a few lines.
+constexpr int CG_PS = 16;
 constexpr int CG_POLL_LIMIT = 1 << 21;
 
 __device__ __forceinline__ double cg_ld_acquire(const double *p)
@@ -1438,7 +1442,8 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
     int bad = 0;
     for (int c = cb + (int)threadIdx.x; c < ce; c += (int)blockDim.x)
     {
-        double v = ACQ ? cg_ld_acquire(&part[c]) : cg_ld_relaxed(&part[c]);
+        double v = ACQ ? cg_ld_acquire(&part[(long)c * CG_PS])
+                       : cg_ld_relaxed(&part[(long)c * CG_PS]);
         int polls = 0;
         while (__double_as_longlong(v) == CG_EMPTY)
         {
@@ -1448,7 +1453,8 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
                 v = 0.0;
                 break;
             }
-            v = ACQ ? cg_ld_acquire(&part[c]) : cg_ld_relaxed(&part[c]);
+            v = ACQ ? cg_ld_acquire(&part[(long)c * CG_PS])
+                    : cg_ld_relaxed(&part[(long)c * CG_PS]);
         }
         s += v;
     }
@@ -1526,7 +1532,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
         }
         const double t = block_sum_d(acc, sh);
         if (threadIdx.x == 0)
-            cg_st_release(&A.rr[0][x.c], t);
+            cg_st_release(&A.rr[0][x.c * CG_PS], t);
     }
     int gave_up = 0;
     for (long k = 1;; k++)
@@ -1552,7 +1558,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             }
             // every block of the node has read the p.Ap partials of iteration k-1
             if (threadIdx.x == 0 && k > 1)
-                A.pap[(k - 1) & 1][x.c] = empty;
+                A.pap[(k - 1) & 1][x.c * CG_PS] = empty;
             if (decide)
             {
                 const int rf = __syncthreads_or(
@@ -1636,7 +1642,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
                 x.rs_prev = rs1;
                 x.rs_cur = rs1;
                 // the U phase reads no other block's data of this phase: no fence
-                cg_st_relaxed(&A.pap[k & 1][x.c], t);
+                cg_st_relaxed(&A.pap[k & 1][x.c * CG_PS], t);
             }
         }
         __syncthreads(); // slot flags written by thread 0 above
@@ -1688,7 +1694,7 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             }
             // every block of the node has read the r.r partials of iteration k-1
             if (threadIdx.x == 0)
-                A.rr[(k - 1) & 1][x.c] = empty;
+                A.rr[(k - 1) & 1][x.c * CG_PS] = empty;
             const double alpha = x.rs_cur / pap;
             double acc = 0.0;
             int fail = 0;
@@ -1727,11 +1733,358 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
                 if (check && fail)
                     atomicOr(&A.rfail[(k / A.every) & 1][x.q], 1);
                 // publishes this block's r and p of the iteration with the partial
-                cg_st_release(&A.rr[k & 1][x.c], t);
+                cg_st_release(&A.rr[k & 1][x.c * CG_PS], t);
             }
         }
         __syncthreads();
         if (gave_up)
+            break;
+    }
+    if (gave_up && threadIdx.x == 0)
+        atomicOr(&A.status[1], 1);
+}
+
+// ---- single-reduction conjugate gradient (cg_variant 1) ------------------------------
+// The same iterates as the reference's conjugate_gradient (conjugate_gradient.c:
+// 322-463) in exact arithmetic, in Chronopoulos and Gear's arrangement (1989):
+// with w = A r and s = A p carried along, both dot products of an iteration,
+// gamma = r.r and delta = w.r, come from one reduction:
+//
+//   beta_j  = gamma_j / gamma_{j-1}                      (beta_0 = 0)
+//   alpha_j = gamma_j / (delta_j - beta_j gamma_j / alpha_{j-1})  (alpha_0 = gamma_0 / delta_0)
+//   p_j = r_j + beta_j p_{j-1};  s_j = w_j + beta_j s_{j-1}
+//   pot += alpha_j p_j;  r_{j+1} = r_j - alpha_j s_j;  w_{j+1} = A r_{j+1}
+//
+// so an iteration waits once for its node's partial sums instead of twice.
+// w_{j+1} at a point needs r_{j+1} at its six neighbours; each thread recomputes
+// those from the neighbours' r_j, w_j, s_{j-1} (the same expression, so the same
+// bits as the neighbour's own thread), so no neighbour waits are needed.  r, w,
+// s and p are double-buffered by iteration parity (a block overwrites a buffer
+// only after every block of the node has published the iteration that read
+// it); all four are zero off the interior points.  The partial sums are
+// triple-buffered (iteration j in slot j mod 3): with one publication per
+// iteration, the owner clears the slot of iteration j + 1 at the start of
+// iteration j, after every block has read it (it held iteration j - 2), and a
+// block reaches the wait on that slot only after seeing the owner's iteration j
+// publication, which follows the clearing.  The convergence test of the reference after update j-1
+// (gamma_j, and the ratio test of the new pot) is taken at the start of
+// iteration j, before p_j, where the reference returns.  Rounding differs from
+// the two-reduction order, so the iterates agree with the reference's to
+// rounding, not bit for bit.
+struct Cg1Args {
+    const AmrChunk *chunks;
+    int nchunks;
+    int chunk;
+    int ncache;
+    const int *intr;
+    const AmrNode *nodes;
+    const int *node_chunk;
+    const double *d;
+    double *pot, *pot_old;
+    double *rb[2], *wb[2], *sb[2], *pb[2]; // r_j in rb[j & 1], ...
+    double *pg[3], *pd[3];                 // per chunk: partial gamma, delta of j in [j % 3]
+    int *rfail[2];
+    int *status;
+    int *iters;
+    double tol, tol2, G;
+    int every;
+    int max_iter;
+    int method;
+};
+
+struct Cg1Slot {
+    double oh2, thr, rm;
+    double g_prev, a_prev; // gamma_{j-1}, alpha_{j-1} of the node
+    int c, q, cb, ce;
+    int begin, n;
+    int sy, sz;
+    int cap;
+    int done;
+};
+
+// r_{j+1} at point g from its r_j, w_j, s_{j-1} (zero off the interior)
+__device__ __forceinline__ double cg1_rnext(const double *__restrict__ r,
+                                            const double *__restrict__ w,
+                                            const double *__restrict__ s, int g, double alpha,
+                                            double beta)
+{
+    const double sv = w[g] + beta * s[g];
+    return r[g] - alpha * sv;
+}
+
+// One point of an iteration, computed without stores: p_j, s_j, the new pot,
+// r_{j+1} and w_{j+1} = A r_{j+1}.
+struct Cg1Point {
+    double p, s, x, r, w;
+};
+
+__device__ __forceinline__ Cg1Point cg1_point(const double *r, const double *w, const double *so,
+                                              const double *po, const double *pot, int g, int sy,
+                                              int sz, double alpha, double beta, double oh2)
+{
+    Cg1Point o;
+    const double rg = r[g], wg = w[g];
+    o.p = rg + beta * po[g];
+    o.s = wg + beta * so[g];
+    o.x = pot[g] + alpha * o.p;
+    o.r = rg - alpha * o.s;
+    const double r1 = cg1_rnext(r, w, so, g + 1, alpha, beta);
+    const double r2 = cg1_rnext(r, w, so, g - 1, alpha, beta);
+    const double r3 = cg1_rnext(r, w, so, g + sy, alpha, beta);
+    const double r4 = cg1_rnext(r, w, so, g - sy, alpha, beta);
+    const double r5 = cg1_rnext(r, w, so, g + sz, alpha, beta);
+    const double r6 = cg1_rnext(r, w, so, g - sz, alpha, beta);
+    o.w = -oh2 * (6.0 * o.r - r1 - r2 - r3 - r4 - r5 - r6);
+    return o;
+}
+
+// Node sums of two published partials.  Both slots of a chunk are polled with
+// relaxed loads in the same round trip; once both hold values, a gpu-scope
+// fence makes the pair an acquire (the publisher's release of the gamma slot
+// orders its data and its delta slot before it).
+__device__ __forceinline__ double2 cg1_node_sum(const double *ga, const double *da, int cb, int ce,
+                                                int *gave_up, double2 *sh2, int *shf)
+{
+    double sg = 0.0, sd = 0.0;
+    int bad = 0, any = 0;
+    for (int c = cb + (int)threadIdx.x; c < ce; c += (int)blockDim.x)
+    {
+        const long o = (long)c * CG_PS;
+        double v = cg_ld_relaxed(&ga[o]), u = cg_ld_relaxed(&da[o]);
+        int polls = 0;
+        while (__double_as_longlong(v) == CG_EMPTY || __double_as_longlong(u) == CG_EMPTY)
+        {
+            if (++polls > CG_POLL_LIMIT)
+            {
+                bad = 1;
+                v = u = 0.0;
+                break;
+            }
+            v = cg_ld_relaxed(&ga[o]);
+            u = cg_ld_relaxed(&da[o]);
+        }
+        sg += v;
+        sd += u;
+        any = 1;
+    }
+    if (any)
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    int f = bad;
+    const double2 t = cg_reduce(sg, sd, f, sh2, shf);
+    *gave_up = f;
+    return t;
+}
+
+__global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg1_nodes(Cg1Args A)
+{
+    __shared__ double2 sh2[CG_MAX_THREADS / 32];
+    __shared__ int shf[CG_MAX_THREADS / 32];
+    const int NT = blockDim.x;
+    extern __shared__ __align__(16) unsigned char cg_dyn[];
+    const double empty = __longlong_as_double(CG_EMPTY);
+    const int nslot = (A.nchunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    Cg1Slot *slot = reinterpret_cast<Cg1Slot *>(cg_dyn);
+    int *gidx = reinterpret_cast<int *>(cg_dyn + nslot * sizeof(Cg1Slot));
+    for (int s = threadIdx.x; s < nslot; s += NT)
+    {
+        const int c = blockIdx.x + s * gridDim.x;
+        const AmrChunk C = A.chunks[c];
+        const AmrNode N = A.nodes[C.node];
+        Cg1Slot x;
+        x.c = c;
+        x.q = C.node;
+        x.cb = A.node_chunk[2 * C.node];
+        x.ce = A.node_chunk[2 * C.node + 1];
+        x.begin = C.begin;
+        x.n = C.end - C.begin;
+        x.sy = N.rd[0] + 1;
+        x.sz = x.sy * (N.rd[1] + 1);
+        const double H = 1.0 / (1 << N.lv);
+        x.oh2 = 1.0 / (H * H);
+        const double rm = 4.0 * A.G * QZ_PI_D * N.mass / (N.ncells * H * H * H);
+        const double tt = A.tol * rm;
+        x.rm = rm;
+        x.thr = N.nintr * tt * tt;
+        if (A.method == 2)
+            x.thr = x.thr * (cbrt((double)N.nintr) * cbrt((double)N.nintr));
+        const long size = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
+        x.cap = (int)(size < A.max_iter ? size : A.max_iter);
+        x.g_prev = x.a_prev = 0.0;
+        x.done = 0;
+        slot[s] = x;
+    }
+    const int ncache = min(nslot, A.ncache);
+    for (int s = 0; s < ncache; s++)
+    {
+        const AmrChunk C = A.chunks[blockIdx.x + s * gridDim.x];
+        for (int e = threadIdx.x; e < C.end - C.begin; e += NT)
+            gidx[s * A.chunk + e] = A.intr[C.begin + e];
+    }
+    __syncthreads();
+    auto gi = [&](int s, int e) -> int {
+        return s < ncache ? gidx[s * A.chunk + e] : A.intr[slot[s].begin + e];
+    };
+    int gave_up = 0;
+    // ---- r_0 = d - A pot; partial gamma_0 into slot 2 (iteration -1) ----
+    for (int s = 0; s < nslot; s++)
+    {
+        const Cg1Slot &x = slot[s];
+        double acc = 0.0;
+        for (int e = threadIdx.x; e < x.n; e += NT)
+        {
+            const int g = gi(s, e);
+            const double *pt = A.pot;
+            const double rv = A.d[g] + x.oh2 * (6.0 * pt[g] - pt[g + 1] - pt[g - 1] - pt[g + x.sy] -
+                                                pt[g - x.sy] - pt[g + x.sz] - pt[g - x.sz]);
+            A.rb[0][g] = rv;
+            acc += rv * rv;
+        }
+        int f = 0;
+        const double t = cg_reduce(acc, 0.0, f, sh2, shf).x;
+        if (threadIdx.x == 0)
+            cg_st_release(&A.pg[2][x.c * CG_PS], t);
+    }
+    // ---- w_0 = A r_0 once the node's r_0 is visible; partial delta_0 into slot 2 ----
+    {
+        int cq = -1;
+        for (int s = 0; s < nslot && !gave_up; s++)
+        {
+            const Cg1Slot &x = slot[s];
+            if (x.q != cq)
+            {
+                cg_node_sum<true>(A.pg[2], x.cb, x.ce, &gave_up, sh2, shf);
+                cq = x.q;
+                if (gave_up)
+                    break;
+            }
+            const double *r = A.rb[0];
+            double acc = 0.0;
+            for (int e = threadIdx.x; e < x.n; e += NT)
+            {
+                const int g = gi(s, e);
+                const double wv = -x.oh2 * (6.0 * r[g] - r[g + 1] - r[g - 1] - r[g + x.sy] -
+                                            r[g - x.sy] - r[g + x.sz] - r[g - x.sz]);
+                A.wb[0][g] = wv;
+                acc += wv * r[g];
+            }
+            int f = 0;
+            const double t = cg_reduce(acc, 0.0, f, sh2, shf).x;
+            if (threadIdx.x == 0)
+                cg_st_release(&A.pd[2][x.c * CG_PS], t); // also publishes w_0
+        }
+        __syncthreads();
+    }
+    for (long j = 0; !gave_up; j++)
+    {
+        // data buffers by parity; partial slots: this iteration's, the previous one's
+        // (gamma_j, delta_j) and the next one's (cleared here)
+        const int cur = (int)(j & 1), prv = cur ^ 1;
+        const int scur = (int)(j % 3), sprv = (int)((j + 2) % 3), snxt = (int)((j + 1) % 3);
+        const bool decide = j > 0 && j % A.every == 0;
+        int live = 0, cq = -1;
+        double2 gd = make_double2(0.0, 0.0);
+        const bool check_next = (j + 1) % A.every == 0;
+        const double tm = 1.0 - A.tol2, tp = 1.0 + A.tol2;
+        for (int s = 0; s < nslot && !gave_up; s++)
+        {
+            Cg1Slot &x = slot[s];
+            if (x.done)
+                continue;
+            if (x.q != cq)
+            {
+                gd = cg1_node_sum(A.pg[sprv], A.pd[sprv], x.cb, x.ce, &gave_up, sh2, shf);
+                cq = x.q;
+                if (gave_up)
+                    break;
+            }
+            // every block of the node has read the partials of iteration j - 2: the
+            // owner clears that slot, which iteration j + 1 publishes into
+            if (threadIdx.x == 0)
+            {
+                cg_st_relaxed(&A.pd[snxt][x.c * CG_PS], empty);
+                cg_st_relaxed(&A.pg[snxt][x.c * CG_PS], empty);
+            }
+            const double gamma = gd.x, delta = gd.y;
+            if (decide)
+            {
+                const int rf = __syncthreads_or(
+                    threadIdx.x == 0 && __ldcg(&A.rfail[(j / A.every) & 1][x.q]));
+                if (!rf && (A.method == 1 || gamma < x.thr))
+                {
+                    if (threadIdx.x == 0)
+                    {
+                        x.done = 1;
+                        if (x.c == x.cb)
+                        {
+                            A.iters[x.q] = (int)j;
+                            atomicMax(&A.status[0], (int)j);
+                            atomicSub(&A.status[2], 1);
+                        }
+                    }
+                    continue;
+                }
+                for (int e = threadIdx.x; e < x.n; e += NT)
+                {
+                    const int g = gi(s, e);
+                    A.pot_old[g] = A.pot[g];
+                }
+                if (threadIdx.x == 0 && x.c == x.cb)
+                    A.rfail[(j / A.every + 1) & 1][x.q] = 0;
+            }
+            if (j >= x.cap)
+            {
+                if (threadIdx.x == 0)
+                {
+                    x.done = 1;
+                    if (x.c == x.cb)
+                    {
+                        A.iters[x.q] = (int)j;
+                        atomicMax(&A.status[0], (int)j);
+                    }
+                }
+                continue;
+            }
+            live = 1;
+            const double beta = j == 0 ? 0.0 : gamma / x.g_prev;
+            const double alpha = j == 0 ? gamma / delta : gamma / (delta - beta * gamma / x.a_prev);
+            const double *r = A.rb[cur], *w = A.wb[cur], *so = A.sb[prv], *po = A.pb[prv];
+            double *rn = A.rb[prv], *wn = A.wb[prv], *sn = A.sb[cur], *pn = A.pb[cur];
+            const double oh2 = x.oh2;
+            const int sy = x.sy, sz = x.sz;
+            double ag = 0.0, ad = 0.0;
+            int fail = 0;
+            for (int e = threadIdx.x; e < x.n; e += NT)
+            {
+                const int g = gi(s, e);
+                const Cg1Point a = cg1_point(r, w, so, po, A.pot, g, sy, sz, alpha, beta, oh2);
+                pn[g] = a.p;
+                sn[g] = a.s;
+                A.pot[g] = a.x;
+                rn[g] = a.r;
+                wn[g] = a.w;
+                ag += a.r * a.r;
+                ad += a.w * a.r;
+                if (check_next)
+                {
+                    const double ratio = a.x / A.pot_old[g];
+                    if ((tm > ratio) || (tp < ratio) || (A.method == 1 && fabs(a.r) / x.rm >= A.tol))
+                        fail = 1;
+                }
+            }
+            const double2 t = cg_reduce(ag, ad, fail, sh2, shf);
+            if (threadIdx.x == 0)
+            {
+                x.g_prev = gamma;
+                x.a_prev = alpha;
+                if (check_next && fail)
+                    atomicOr(&A.rfail[((j + 1) / A.every) & 1][x.q], 1);
+                cg_st_relaxed(&A.pd[scur][x.c * CG_PS], t.y);
+                // publishes this block's r, w, s, p, pot of the iteration with gamma
+                cg_st_release(&A.pg[scur][x.c * CG_PS], t.x);
+            }
+        }
+        __syncthreads();
+        if (gave_up || !live)
             break;
     }
     if (gave_up && threadIdx.x == 0)
@@ -1904,12 +2257,15 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     constexpr int kCgSmem = 40 * 1024; // slot records and cached grid indices
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    static int per_sm = 0;
+    static int occ[2] = {0, 0};
     static std::once_flag occ_once;
     std::call_once(occ_once, [] {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cg_nodes,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], (const void *)k_cg_nodes,
+                                                      CG_MAX_THREADS, kCgSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], (const void *)k_cg1_nodes,
                                                       CG_MAX_THREADS, kCgSmem);
     });
+    const int per_sm = occ[c.cg_variant == 1 ? 1 : 0];
     if (per_sm < 1)
     {
         set_error("conjugate gradient kernel cannot be resident");
@@ -1938,10 +2294,13 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     if (L.nchunks == 0)
         return QZ_SUCCESS;
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
-    if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, 4L * L.nchunks) ||
+    const bool one = c.cg_variant == 1;
+    const long nparts = (one ? 3L : 4L) * L.nchunks * CG_PS;
+    if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, nparts) ||
         !L.nint.ensure(s->mem, 5L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
         !L.p.ensure(s->mem, L.grid_total) || !L.Ap.ensure(s->mem, L.grid_total) ||
-        !L.apv.ensure(s->mem, L.grid_total))
+        !L.apv.ensure(s->mem, L.grid_total) ||
+        (one && !L.cg1.ensure(s->mem, 4 * L.grid_total)))
     {
         set_error("cg buffers");
         return QZ_FAILURE;
@@ -1961,7 +2320,12 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     cudaMemsetAsync(L.r.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.p.p, 0, L.grid_total * sizeof(double), s->stream);
     cudaMemsetAsync(L.Ap.p, 0, L.grid_total * sizeof(double), s->stream);
-    cudaMemsetAsync(L.chunk_part.p, 0xff, 4L * L.nchunks * sizeof(double), s->stream);
+    if (one)
+    {
+        cudaMemsetAsync(L.apv.p, 0, L.grid_total * sizeof(double), s->stream);
+        cudaMemsetAsync(L.cg1.p, 0, 4 * L.grid_total * sizeof(double), s->stream);
+    }
+    cudaMemsetAsync(L.chunk_part.p, 0xff, nparts * sizeof(double), s->stream);
     CgArgs A;
     A.chunks = L.chunks.p;
     A.nchunks = L.nchunks;
@@ -1976,9 +2340,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     A.pbuf[1] = L.Ap.p;
     A.apv = L.apv.p;
     A.pap[0] = L.chunk_part.p;
-    A.pap[1] = L.chunk_part.p + L.nchunks;
-    A.rr[0] = L.chunk_part.p + 2L * L.nchunks;
-    A.rr[1] = L.chunk_part.p + 3L * L.nchunks;
+    A.pap[1] = L.chunk_part.p + (long)L.nchunks * CG_PS;
+    A.rr[0] = L.chunk_part.p + 2L * L.nchunks * CG_PS;
+    A.rr[1] = L.chunk_part.p + 3L * L.nchunks * CG_PS;
     A.rfail[0] = L.nint.p + 2 * nn;
     A.rfail[1] = L.nint.p + 3 * nn;
     A.status = L.nint.p + 4 * nn;
@@ -1992,14 +2356,50 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     const int blocks = (int)std::min(max_blocks, (long)L.nchunks);
     const int nslot = (L.nchunks + blocks - 1) / blocks;
     A.chunk = chunk;
-    A.ncache = std::max(0, (int)((kCgSmem - nslot * (long)sizeof(CgSlot)) / (chunk * 4L)));
-    const size_t smem = nslot * sizeof(CgSlot) + (size_t)std::min(nslot, A.ncache) * chunk * 4;
+    const long slot_bytes = one ? (long)sizeof(Cg1Slot) : (long)sizeof(CgSlot);
+    A.ncache = std::max(0, (int)((kCgSmem - nslot * slot_bytes) / (chunk * 4L)));
+    const size_t smem = nslot * slot_bytes + (size_t)std::min(nslot, A.ncache) * chunk * 4;
     if (smem > (size_t)kCgSmem)
     {
         set_error("conjugate gradient: %d chunks per block exceed the shared memory budget", nslot);
         return QZ_FAILURE;
     }
-    void *args[] = {&A};
+    Cg1Args B;
+    B.chunks = A.chunks;
+    B.nchunks = A.nchunks;
+    B.chunk = A.chunk;
+    B.ncache = A.ncache;
+    B.intr = A.intr;
+    B.nodes = A.nodes;
+    B.node_chunk = A.node_chunk;
+    B.d = A.d;
+    B.pot = A.pot;
+    B.pot_old = A.pot_old;
+    B.rb[0] = L.r.p;
+    B.rb[1] = L.p.p;
+    B.wb[0] = L.Ap.p;
+    B.wb[1] = L.apv.p;
+    B.sb[0] = one ? L.cg1.p : nullptr;
+    B.sb[1] = one ? L.cg1.p + L.grid_total : nullptr;
+    B.pb[0] = one ? L.cg1.p + 2 * L.grid_total : nullptr;
+    B.pb[1] = one ? L.cg1.p + 3 * L.grid_total : nullptr;
+    for (int q = 0; q < 3; q++)
+    {
+        // gamma and delta of a chunk share its slot's line
+        B.pg[q] = L.chunk_part.p + (long)q * L.nchunks * CG_PS;
+        B.pd[q] = B.pg[q] + 1;
+    }
+    B.rfail[0] = A.rfail[0];
+    B.rfail[1] = A.rfail[1];
+    B.status = A.status;
+    B.iters = A.iters;
+    B.tol = A.tol;
+    B.tol2 = A.tol2;
+    B.G = A.G;
+    B.every = A.every;
+    B.max_iter = A.max_iter;
+    B.method = A.method;
+    void *args[] = {one ? (void *)&B : (void *)&A};
     cudaEvent_t eb = nullptr, ee = nullptr;
     if (s->prof)
     {
@@ -2007,8 +2407,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         ee = prof_event(s);
         cudaEventRecord(eb, s->stream);
     }
-    if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_cg_nodes, dim3(blocks), dim3(nt),
-                                                args, smem, s->stream),
+    if (!check_cuda(cudaLaunchCooperativeKernel(one ? (const void *)k_cg1_nodes
+                                                    : (const void *)k_cg_nodes,
+                                                dim3(blocks), dim3(nt), args, smem, s->stream),
                     "cooperative cg"))
         return QZ_FAILURE;
     s->stats.kernel_launches++;
@@ -2024,11 +2425,12 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     if (s->prof)
     {
         // bytes per iteration and interior point: the P phase reads r and p_{k-2} and
-        // writes p_{k-1} (24 B), the U phase reads p, pot, r and writes pot, r (40 B)
+        // writes p_{k-1} (24 B), the U phase reads p, pot, r and writes pot, r (40 B);
+        // the single-reduction form reads r, w, s, p, pot and writes the five (80 B)
         double pts_it = 0.0;
         for (int q = 0; q < nn; q++)
             pts_it += (double)L.h[q].nintr * st[3 + q];
-        s->prof_pending.back().bytes = 64.0 * pts_it;
+        s->prof_pending.back().bytes = (one ? 80.0 : 64.0) * pts_it;
     }
     if (st[1])
     {

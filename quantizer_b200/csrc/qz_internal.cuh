@@ -228,6 +228,7 @@ struct AmrLevel {
     // conjugate gradient: residual r and the two p buffers (p and Ap, by iteration parity)
     DBuf<double> gpot, gpot_old, gd, gax, gay, gaz, r, p, Ap;
     DBuf<double> apv; // conjugate gradient: Ap at the interior points
+    DBuf<double> cg1; // single-reduction conjugate gradient: s and p, two parities each
     DBuf<int> nint; // node chunk ranges, converged flags, ratio-test flags, status
     DBuf<AmrChunk> chunks;
     DBuf<double> chunk_part; // per chunk: two p.Ap and two r.r partials
