@@ -269,9 +269,14 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
         return max(starts[0].elapsed_time(e) for e in ends)
 
     core.ensemble_step(sims, dts, W, threads=wl["threads"])
+    # autotuner: host threads x multigrid points per thread, one trial step each,
+    # states put back (untimed)
+    threads, ppt, tune_ms = core.ensemble_autotune(sims, dts)
+    config["threads"] = threads
+    config["mg_points_per_thread"] = ppt
     st0 = [s.stats() for s in sims]
     with ClockSampler(local) as clk:
-        ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=wl["threads"]))
+        ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=threads))
     launches = sum(s.stats().kernel_launches - a.kernel_launches for s, a in zip(sims, st0))
     t = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
@@ -293,6 +298,9 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
                 "config": config, "e2e": None,
                 "single_instance_loop": {"value": loop_value, "steps": Kl,
                                          "speedup_of_batching": value / world / loop_value},
+                "autotune": {"threads": threads, "mg_points_per_thread": ppt,
+                             "best_trial_ms": tune_ms,
+                             "grid": "threads {4, 8, 16, 32, 64} x points per thread {2, 4, 8}"},
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     for s in sims:

@@ -102,6 +102,10 @@ typedef struct qz_config {
      * iteration, 1 one reduction per iteration (Chronopoulos-Gear arrangement:
      * the same iterates in exact arithmetic, half the waits) */
     int cg_variant;
+    /* persistent multigrid cycles: finest-level points of one colour per thread,
+     * which sets the launch's block count (at most two blocks per SM); results
+     * do not depend on it (qz_ensemble_autotune picks it for ensembles) */
+    int mg_points_per_thread;
 } qz_config;
 
 typedef struct qz_stats {
@@ -232,6 +236,18 @@ QZ_API int qz_timestep(qz_sim *sim, double *dt);
  * Returns the first failure (with its index in qz_last_error). */
 QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *dt, int nsteps,
                             int nthreads);
+
+/* Autotuner of the batching form: times one ensemble step (host wall time to
+ * completion) for every pair of host thread count (thread_opts) and multigrid
+ * points per thread (ppt_opts), restoring every simulation's state (particles,
+ * accelerations, head potential, statistics) after each trial; sets every
+ * simulation's mg_points_per_thread to the best pair's and writes the best
+ * thread count, points per thread and step time.  The simulations are left as
+ * they were (their results do not depend on the choice). */
+QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const double *dt,
+                                const int *thread_opts, int nthread_opts, const int *ppt_opts,
+                                int nppt_opts, int *best_threads, int *best_ppt,
+                                double *best_ms);
 
 /* Differentiation form (no reference counterpart: QUANTIZER has no adjoint).
  * Head-only FP64 runs (lmax == lmin, 3-point stencil, reflexive walls,

@@ -317,6 +317,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->head_pot_method = 0;    /* global_variables.c (multigrid) */
     c->adjoint_tol = 1e-10;
     c->cg_variant = 0;
+    c->mg_points_per_thread = 4;
     return QZ_SUCCESS;
 }
 
@@ -728,6 +729,42 @@ int step_core(qz_sim *s, double h)
     s->stats.sim_time += h;
     return QZ_SUCCESS;
 }
+bool state_save(qz_sim *s, SavedState &st)
+{
+    const long n = s->n;
+    if (!st.buf.ensure(s->mem, 9 * n + s->gpts))
+        return false;
+    const double *src[9] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    for (int q = 0; q < 9; q++)
+        if (!check_cuda(cudaMemcpyAsync(st.buf.p + q * n, src[q], n * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, s->stream), "state save"))
+            return false;
+    st.n = n;
+    st.head_mass = s->head_mass;
+    st.forces_ready = s->forces_ready;
+    st.stats = s->stats;
+    return check_cuda(cudaMemcpyAsync(st.buf.p + 9 * n, s->pot, s->gpts * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s->stream), "state save");
+}
+
+bool state_restore(qz_sim *s, const SavedState &st)
+{
+    const long n = st.n;
+    double *dst[9] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    for (int q = 0; q < 9; q++)
+        if (!check_cuda(cudaMemcpyAsync(dst[q], st.buf.p + q * n, n * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, s->stream), "state restore"))
+            return false;
+    s->n = n;
+    s->head_mass = st.head_mass;
+    s->forces_ready = st.forces_ready;
+    s->stats = st.stats;
+    return check_cuda(cudaMemcpyAsync(s->pot, st.buf.p + 9 * n, s->gpts * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s->stream), "state restore");
+}
+
+void state_free(qz_sim *s, SavedState &st) { st.buf.release(s->mem); }
+
 } // namespace qz
 
 extern "C" {

@@ -3,13 +3,14 @@
 //
 // One simulation's step is a chain of short kernels and a few host
 // synchronisations (tree sizes, convergence checks); on its own it leaves most
-// of the GPU idle.  Every qz_sim owns its stream and memory pool, so the
-// simulations of an ensemble are stepped concurrently by a pool of host
-// threads: each thread takes the next simulation (atomic counter) and runs its
+// of the GPU idle.  Every qz_sim owns its stream (device memory comes from the
+// device's shared stream-ordered pool), so the simulations of an ensemble are
+// stepped concurrently by a pool of host threads: each thread takes the next simulation (atomic counter) and runs its
 // steps, and the chains of different simulations overlap on the GPU.  Every
 // simulation computes exactly what it computes alone (its kernels and their
 // order are unchanged), so results do not depend on the number of threads.
 #include <atomic>
+#include <chrono>
 #include <mutex>
 #include <stdio.h>
 #include <string.h>
@@ -78,5 +79,68 @@ extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *d
         set_error("qz_ensemble_step: simulation %d: %s", failed.load(), first_error.c_str());
         return QZ_FAILURE;
     }
+    return QZ_SUCCESS;
+}
+
+extern "C" QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const double *dt,
+                                           const int *thread_opts, int nthread_opts,
+                                           const int *ppt_opts, int nppt_opts, int *best_threads,
+                                           int *best_ppt, double *best_ms)
+{
+    if (!sims || nsims < 1 || !thread_opts || nthread_opts < 1 || !ppt_opts || nppt_opts < 1)
+    {
+        set_error("qz_ensemble_autotune: bad arguments");
+        return QZ_FAILURE;
+    }
+    std::vector<SavedState> saved(nsims);
+    auto restore_all = [&]() {
+        for (int k = 0; k < nsims; k++)
+            if (!state_restore(sims[k], saved[k]) || qz_synchronize(sims[k]))
+                return false;
+        return true;
+    };
+    int rc = QZ_SUCCESS;
+    for (int k = 0; k < nsims && rc == QZ_SUCCESS; k++)
+    {
+        if (!sims[k] || (!sims[k]->forces_ready && qz_init_forces(sims[k])) ||
+            !state_save(sims[k], saved[k]) || qz_synchronize(sims[k]))
+            rc = QZ_FAILURE;
+    }
+    int bt = thread_opts[0], bp = ppt_opts[0];
+    double bms = 1e300;
+    for (int a = 0; a < nppt_opts && rc == QZ_SUCCESS; a++)
+    {
+        for (int k = 0; k < nsims; k++)
+            sims[k]->cfg.mg_points_per_thread = ppt_opts[a];
+        for (int b = 0; b < nthread_opts && rc == QZ_SUCCESS; b++)
+        {
+            const auto t0 = std::chrono::steady_clock::now();
+            rc = qz_ensemble_step(sims, nsims, dt, 1, thread_opts[b]);
+            const double ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                    .count();
+            if (rc == QZ_SUCCESS && ms < bms)
+            {
+                bms = ms;
+                bt = thread_opts[b];
+                bp = ppt_opts[a];
+            }
+            if (rc == QZ_SUCCESS && !restore_all())
+                rc = QZ_FAILURE;
+        }
+    }
+    for (int k = 0; k < nsims; k++)
+    {
+        sims[k]->cfg.mg_points_per_thread = bp;
+        state_free(sims[k], saved[k]);
+    }
+    if (rc != QZ_SUCCESS)
+        return QZ_FAILURE;
+    if (best_threads)
+        *best_threads = bt;
+    if (best_ppt)
+        *best_ppt = bp;
+    if (best_ms)
+        *best_ms = bms;
     return QZ_SUCCESS;
 }

@@ -356,6 +356,19 @@ int check_flags(qz_sim *s);                   // qz_capi.cu
 int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
 void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
 void snapshot_free(qz_sim *s);                // qz_snapshot.cu
+// A copy of the state a step reads (particles, accelerations, head potential)
+// and of the statistics, to run trial steps and put the simulation back
+// (qz_capi.cu).
+struct SavedState {
+    DBuf<double> buf;
+    long n = 0;
+    double head_mass = 0.0;
+    bool forces_ready = false;
+    qz_stats stats{};
+};
+bool state_save(qz_sim *s, SavedState &st);
+bool state_restore(qz_sim *s, const SavedState &st);
+void state_free(qz_sim *s, SavedState &st);
 bool check_cuda(cudaError_t e, const char *what);
 #define QZ_LAUNCHED(sim) ((sim)->stats.kernel_launches++)
 

@@ -1070,13 +1070,14 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    // about four points of one colour of the finest level per thread, at most two
-    // blocks per SM: small heads take few SMs, so independent simulations can
-    // run their cycles side by side
+    // mg_points_per_thread points of one colour of the finest level per thread
+    // (4 by default), at most two blocks per SM: small heads take few SMs, so
+    // independent simulations can run their cycles side by side
     const long m0 = A.phi[0].n - 2;
     const long work = (m0 + 1) / 2 * m0 * m0;
+    const long ppt = c.mg_points_per_thread > 0 ? c.mg_points_per_thread : 4;
     const int blocks = (int)std::max(1L, std::min((long)std::min(ps, 2) * sms,
-                                                  (work + 4L * MG_THREADS - 1) / (4L * MG_THREADS)));
+                                                  (work + ppt * MG_THREADS - 1) / (ppt * MG_THREADS)));
     // algorithmic bytes of one cycle, as the launch-per-phase path counts them
     double bytes = 0.0;
     for (int l = 0; l < A.nlev; l++)
