@@ -239,10 +239,8 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
         return 0
     import torch
     import torch.distributed as dist
-    from quantizer_b200 import core, ics
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from quantizer_b200 import core, ics, replicas
+    replicas.init("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     sims, dts = [], []
@@ -278,10 +276,8 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     with ClockSampler(local) as clk:
         ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=threads))
     launches = sum(s.stats().kernel_launches - a.kernel_launches for s, a in zip(sims, st0))
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    t_max = replicas.max_over_ranks(ms, dev)
+    ms_max = t_max
     value = world * total * K / (ms_max / 1e3)
     Kl = min(K, 2)
     ms_loop = makespan(lambda: core.ensemble_step(sims, dts, Kl, threads=1))
@@ -305,8 +301,7 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
         print(json.dumps(line), flush=True)
     for s in sims:
         s.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
@@ -344,15 +339,13 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     import numpy as np
     import torch
     import torch.distributed as dist
-    from quantizer_b200 import core, ics
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from quantizer_b200 import core, ics, replicas
+    replicas.init("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n, L = wl["n"], wl["lmin"]
     cfg = dict(tol=wl["tol"], tol2=wl["tol"], adjoint_tol=wl["tol"])
-    ic = ics.plummer(n, a=wl["a"], seed=1 + rank)
+    ic = ics.plummer(n, a=wl["a"], seed=replicas.seed_for(rank))
     dt = 1e-3 * ics.crossing_time(wl["a"])
     rng = np.random.default_rng(100 + rank)
     pert = {k: v.copy() for k, v in ic.items()}
@@ -401,10 +394,8 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     st1 = sim.stats()
     sa = runs[-1]
     adj_ms = sa["forward_ms"] + sa["reverse_ms"]
-    t = torch.tensor([adj_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    adj_ms_max = float(t.item())
+    t_max = replicas.max_over_ranks(adj_ms, dev)
+    adj_ms_max = t_max
     free, total_mem = torch.cuda.mem_get_info(dev)
     # finite differences on random coordinates
     kinds = [("x", "gx", 1e-6)] * 12 + [("y", "gy", 1e-6)] * 6 + [("z", "gz", 1e-6)] * 6 + \
@@ -450,8 +441,7 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
                 "gpu_launches": int(st1.kernel_launches - st0.kernel_launches) // 2,
                 "clocks": clk.summary(), "cpu_baseline": None}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
@@ -527,11 +517,9 @@ def main() -> int:
     import numpy as np
     import torch
     import torch.distributed as dist
-    from quantizer_b200 import core, ics
+    from quantizer_b200 import core, ics, replicas
 
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    replicas.init("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
@@ -540,7 +528,7 @@ def main() -> int:
             dist.barrier()
         torch.cuda.synchronize()
 
-    ic = make_ic(wl, 1 + rank)
+    ic = make_ic(wl, replicas.seed_for(rank))
     dt = 1e-3 * ics.crossing_time(wl["a"])
     simcfg = dict(lmax=wl["lmin"] + wl["levels"], ref_ptcl=wl["ref_ptcl"])
     if args.cg_variant is not None:
@@ -579,10 +567,8 @@ def main() -> int:
     launches = int(st1.kernel_launches - st0.kernel_launches)
     vcycles = int(st1.vcycles_total - st0.vcycles_total)
     cgit = int(st1.cg_iterations - st0.cg_iterations)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    t_max = replicas.max_over_ranks(ms, dev)
+    ms_max = t_max
     value = world * wl["n"] * K / (ms_max / 1e3)
 
     # ---- end to end through the C ABI with host buffers --------------------------------
@@ -596,10 +582,8 @@ def main() -> int:
     barrier()
     ms_e2e = timed_steps(lambda: sim.step_host(host, dt), Ke)
     barrier()
-    t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * wl["n"] * Ke / (float(t.item()) / 1e3)
+    t_max = replicas.max_over_ranks(ms_e2e, dev)
+    e2e_value = world * wl["n"] * Ke / (t_max / 1e3)
 
     # ---- profiled pass: per-kernel-category device time --------------------------------
     Kp = min(K, 5)
@@ -642,10 +626,8 @@ def main() -> int:
             ref_sim.step(dt, 1)
         barrier()
         ms_plain = timed_steps_on(ref_sim, lambda: ref_sim.step(dt, 1), K)
-        t = torch.tensor([ms_plain], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        plain_value = world * wl["n"] * K / (float(t.item()) / 1e3)
+        t_max = replicas.max_over_ranks(ms_plain, dev)
+        plain_value = world * wl["n"] * K / (t_max / 1e3)
         # force error: both forms from one state, one step
         state = {**st_pos, "m": ic["m"]}
         errs = []
@@ -662,7 +644,7 @@ def main() -> int:
         errs = diff / np.maximum(a_p, 1e-300)
         plain = {"precision": "fp64" if wl["variant"] == 0 else
                  "fp32 head smoothing in fp64 defect correction",
-                 "value": plain_value, "ms_per_step": float(t.item()) / K,
+                 "value": plain_value, "ms_per_step": t_max / K,
                  "max_rel_force_err_mixed_vs_fp64": float(errs.max()),
                  "median_rel_force_err_mixed_vs_fp64": float(np.median(errs))}
         ref_sim.close()
@@ -694,8 +676,7 @@ def main() -> int:
                 "variant": plain, "clocks": clk.summary(), "kernels": kernels}
         print(json.dumps(line), flush=True)
     sim.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
