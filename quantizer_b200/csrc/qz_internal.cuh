@@ -55,12 +55,16 @@ enum Flag {
 enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2, E_BARRIER = 8 };
 
 // Grid-wide barrier of a cooperative launch with bounded waits.  word[0]
-// counts arrivals, word[1] is the generation, word[2] is set once a wait of
-// this launch gave up; word[0] and word[2] must be zero at launch.  The last
-// block to arrive resets the count and advances the generation after a fence;
-// the others poll the generation with acquire loads.  A wait that hits the
-// poll limit sets word[2] and E_BARRIER in flags[F_ERROR]; from then on every
-// barrier of the launch returns false at once, so the kernel finishes.
+// counts arrivals, word[2] is the generation and word[3] is set once a wait of
+// this launch gave up (words 2 and 3 are read together by one 64-bit acquire
+// load); all four words are zero at launch.  A block arrives with one
+// acquire-release atomic add (which also releases the block's writes, ordered
+// before it by the block barrier); the last one resets the count and advances
+// the generation with a release; the others poll the generation with acquire
+// loads.  Two dependent L2 round trips on the critical path: the arrival and
+// the poll that sees the new generation.  A wait that hits the poll limit sets
+// word[3] and E_BARRIER in flags[F_ERROR]; from then on every barrier of the
+// launch returns false at once, so the kernel finishes.
 constexpr int GBAR_POLL_LIMIT = 1 << 21;
 
 struct GridBar {
@@ -75,29 +79,43 @@ __device__ __forceinline__ unsigned gbar_ld_acquire(const unsigned *p)
     return v;
 }
 
+__device__ __forceinline__ unsigned long long gbar_ld_acquire64(const unsigned *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool gbar_sync(const GridBar &B, int *sh_ok)
 {
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        int ok = gbar_ld_acquire(&B.word[2]) == 0;
+        unsigned long long gw = gbar_ld_acquire64(&B.word[2]); // generation | gave-up << 32
+        const unsigned gen = (unsigned)gw;
+        int ok = (gw >> 32) == 0;
         if (ok)
         {
-            const unsigned gen = gbar_ld_acquire(&B.word[1]);
-            __threadfence(); // this block's writes before its arrival
-            const unsigned prev = atomicAdd(&B.word[0], 1u);
+            unsigned prev;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                         : "=r"(prev)
+                         : "l"(&B.word[0])
+                         : "memory");
             if (prev == gridDim.x - 1)
             {
-                atomicExch(&B.word[0], 0u);
-                __threadfence();
-                atomicAdd(&B.word[1], 1u);
+                asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&B.word[0]) : "memory");
+                asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&B.word[2])
+                             : "memory");
             }
             else
             {
                 int polls = 0;
-                while (gbar_ld_acquire(&B.word[1]) == gen)
+                for (;;)
                 {
-                    if (++polls > GBAR_POLL_LIMIT || gbar_ld_acquire(&B.word[2]) != 0)
+                    gw = gbar_ld_acquire64(&B.word[2]);
+                    if ((unsigned)gw != gen)
+                        break;
+                    if ((gw >> 32) != 0 || ++polls > GBAR_POLL_LIMIT)
                     {
                         ok = 0;
                         break;
@@ -107,10 +125,9 @@ __device__ __forceinline__ bool gbar_sync(const GridBar &B, int *sh_ok)
         }
         if (!ok)
         {
-            atomicExch(&B.word[2], 1u);
+            atomicExch(&B.word[3], 1u);
             atomicOr(&B.flags[F_ERROR], E_BARRIER);
         }
-        __threadfence();
         *sh_ok = ok;
     }
     __syncthreads();
