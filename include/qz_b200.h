@@ -106,6 +106,11 @@ typedef struct qz_config {
      * which sets the launch's block count (at most two blocks per SM); results
      * do not depend on it (qz_ensemble_autotune picks it for ensembles) */
     int mg_points_per_thread;
+    /* refinement tree frozen after its first construction (the differentiation
+     * form's fixed tree): later steps keep the nodes and only reassign the
+     * particles to them (each level's node of a particle from its parent's box
+     * status, as the construction does) instead of rebuilding the tree */
+    int freeze_tree;
 } qz_config;
 
 typedef struct qz_stats {

@@ -45,7 +45,8 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, "libqzb200.so")
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
-    deps = srcs + [os.path.join(CSRC, "qz_internal.cuh"), os.path.join(ROOT, "include", "qz_b200.h")]
+    deps = srcs + [os.path.join(CSRC, "qz_internal.cuh"), os.path.join(CSRC, "qz_amr_dev.cuh"),
+                   os.path.join(ROOT, "include", "qz_b200.h")]
     if not force and not _newer(out, deps):
         return out
     objs = []

@@ -41,7 +41,7 @@ class Config(C.Structure):
         ("w_sor_branch", C.c_double), ("cfl", C.c_double), ("max_dt", C.c_double),
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
         ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
-        ("mg_points_per_thread", C.c_int),
+        ("mg_points_per_thread", C.c_int), ("freeze_tree", C.c_int),
     ]
 
 

@@ -33,7 +33,7 @@
 // the forward is deterministic) before its reverse sweep.  The adjoint
 // deposit is a sort by head cell and a warp-segmented reduction like the
 // forward deposit (no float atomics); every reduction has a fixed order.
-#include "qz_internal.cuh"
+#include "qz_amr_dev.cuh"
 
 namespace qz {
 
@@ -52,6 +52,15 @@ struct Adjoint {
     DBuf<double> red;                // reduction partials and results
     double *host = nullptr;          // 8 pinned doubles
     long seg_recs = 0, ck_recs = 0;
+    // refinement levels (index = level): a-bar deposits (3 x grid), children's
+    // phi-bar contributions, phi-bar, lam (kept: the next solve's start on a frozen
+    // tree), scratch, interior masks, node thresholds
+    std::vector<DBuf<double>> lA, lphic, lphib, llam, lscr, lthr;
+    std::vector<DBuf<int>> lmask;
+    DBuf<int> finest;   // per particle: its finest level
+    DBuf<double> abh;   // a-bar of the particles whose finest node is the head (3n)
+    DBuf<double> phic0; // children's phi-bar contributions on the head grid
+    DBuf<double> nrm;   // per node sums
 };
 
 void adjoint_free(qz_sim *s)
@@ -60,9 +69,16 @@ void adjoint_free(qz_sim *s)
     if (!A)
         return;
     DBuf<double> *b[] = {&A->xb, &A->vb, &A->mb, &A->ac, &A->ab, &A->Ab, &A->phib, &A->lam,
-                         &A->cs, &A->ck, &A->seg, &A->fin, &A->tgt, &A->red};
+                         &A->cs, &A->ck, &A->seg, &A->fin, &A->tgt, &A->red, &A->abh,
+                         &A->phic0, &A->nrm};
     for (auto *q : b)
         q->release(s->mem);
+    for (auto *v : {&A->lA, &A->lphic, &A->lphib, &A->llam, &A->lscr, &A->lthr})
+        for (auto &q : *v)
+            q.release(s->mem);
+    for (auto &q : A->lmask)
+        q.release(s->mem);
+    A->finest.release(s->mem);
     if (A->host)
         cudaFreeHost(A->host);
     delete A;
@@ -262,7 +278,8 @@ __global__ void k_adj_shell(int L, long D, double o2h, double oh2, const double 
                             const double *__restrict__ lam, const double *__restrict__ Abx,
                             const double *__restrict__ Aby, const double *__restrict__ Abz,
                             const double *__restrict__ gx, const double *__restrict__ gy,
-                            const double *__restrict__ gz, double *__restrict__ partial)
+                            const double *__restrict__ gz, const double *__restrict__ phic,
+                            double *__restrict__ partial)
 {
     __shared__ double sh[32];
     const int n = (1 << L) + 1, hi = 1 << L;
@@ -278,7 +295,8 @@ __global__ void k_adj_shell(int L, long D, double o2h, double oh2, const double 
         const long g = i + j * D + k * D2;
         const double nb = lam[g + 1] + lam[g - 1] + lam[g + D] + lam[g - D] + lam[g + D2] +
                           lam[g - D2];
-        const double pb = adj_negdiv(i, j, k, D, hi, o2h, Abx, Aby, Abz) - oh2 * nb;
+        const double pb = adj_negdiv(i, j, k, D, hi, o2h, Abx, Aby, Abz) - oh2 * nb +
+                          (phic ? phic[g] : 0.0);
         acc += pot[g] * pb + (Abx[g] * gx[g] + Aby[g] * gy[g] + Abz[g] * gz[g]);
     }
     acc = adj_block_sum(acc, sh);
@@ -409,15 +427,381 @@ __global__ void k_adj_add_scalar(long n, const double *__restrict__ v, double *_
         out[i] += v[0];
 }
 
+// ---- refinement levels (frozen tree) ------------------------------------------------------
+// The level forward (grid_density.c:113-267, potential_branches.c:93-331,
+// grid_acceleration.c:199-394, particle_acceleration.c:134-355) is linear in the
+// node densities and in the parents' fields:
+//   d_l   = sum_p (4 pi G / H^6) m_p W_l(x_p)   particles of level l's nodes
+//   phi_l = A_l^-1 (d_l - B phi_b / H^2),  phi_b = P(phi_{l-1}) at node boundary
+//           points, shell(M) at simulation-boundary points
+//   a_l   = -grad phi_l (interior), P(a_{l-1}) (boundary), shell accel(M) (sim boundary)
+//   F_p   = sum_g w_g(x_p) a_{l*}[g]          l* the particle's finest level
+// with P the 8-point parent average of from_parent.  The pull-back runs from the
+// finest level down: the gather's transpose deposits a-bar on each particle's
+// finest level; on each level the gradient's transpose (-div over the interior
+// points), children's contributions, the node solves with zero boundary, and the
+// transposes of P (to the parent's a-bar and phi-bar: accumulated with atomic
+// adds, the only sums here whose order is not fixed), the shell (to the total
+// mass) and the deposit (to x and m).
+
+struct NodeOfPtrs {
+    const int *p[AMR_MAX_LEVELS];
+};
+
+// finest level holding each particle (0: the head)
+__global__ void k_adj_finest(long n, int nlev, NodeOfPtrs no, int *__restrict__ fin)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int l = nlev - 1;
+    for (; l > 0; l--)
+        if (no.p[l][i] >= 0)
+            break;
+    fin[i] = l;
+}
+
+__global__ void k_adj_mask_ab(long n, const int *__restrict__ fin, const double *__restrict__ ab,
+                              double *__restrict__ abh)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const bool h = fin[i] == 0;
+    abh[i] = h ? ab[i] : 0.0;
+    abh[n + i] = h ? ab[n + i] : 0.0;
+    abh[2 * n + i] = h ? ab[2 * n + i] : 0.0;
+}
+
+__global__ void k_adj_flag_level(long n, const int *__restrict__ fin, int l, int *__restrict__ flag)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        flag[i] = fin[i] == l ? 1 : 0;
+}
+
+// cell keys (level box pool) of the particles whose finest level is l
+__global__ void k_adj_lvl_keys(long n, int l, const int *__restrict__ fin,
+                               const int *__restrict__ node_of, const AmrNode *__restrict__ nodes,
+                               const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const int *__restrict__ slot,
+                               unsigned *__restrict__ keys, int *__restrict__ vals)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || fin[i] != l)
+        return;
+    const AmrNode N = nodes[node_of[i]];
+    const double sc = (double)(1 << N.lv);
+    const int cx = (int)(x[i] * sc), cy = (int)(y[i] * sc), cz = (int)(z[i] * sc);
+    keys[slot[i]] = (unsigned)(N.box_off + box_index(N, cx, cy, cz));
+    vals[slot[i]] = (int)i;
+}
+
+// grid points of level l: the 8 corner sums of their adjacent occupied cells, three
+// components (cs: segment * 24 + component * 8 + corner)
+__global__ void k_adj_lvl_point_gather3(long total, int nn, const AmrNode *__restrict__ nodes,
+                                        const int *__restrict__ cell_seg,
+                                        const double *__restrict__ cs, double *__restrict__ A0,
+                                        double *__restrict__ A1, double *__restrict__ A2)
+{
+    long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total)
+        return;
+    const AmrNode N = nodes[find_node(nodes, nn, g, 0)];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int c = 0; c < 2; c++)
+    {
+        const int cz = gz - 1 + c;
+        if (cz < 0 || cz >= N.rd[2])
+            continue;
+        for (int b = 0; b < 2; b++)
+        {
+            const int cy = gy - 1 + b;
+            if (cy < 0 || cy >= N.rd[1])
+                continue;
+            for (int a = 0; a < 2; a++)
+            {
+                const int cx = gx - 1 + a;
+                if (cx < 0 || cx >= N.rd[0])
+                    continue;
+                const int sg =
+                    cell_seg[N.box_off + cx + (long)cy * N.rd[0] + (long)cz * N.rd[0] * N.rd[1]];
+                if (sg >= 0)
+                {
+                    const int corner = (1 - a) + 2 * (1 - b) + 4 * (1 - c);
+                    a0 += cs[(long)sg * 24 + corner];
+                    a1 += cs[(long)sg * 24 + 8 + corner];
+                    a2 += cs[(long)sg * 24 + 16 + corner];
+                }
+            }
+        }
+    }
+    A0[g] = a0;
+    A1[g] = a1;
+    A2[g] = a2;
+}
+
+// the gather's weight derivatives for particles whose finest level is a refinement
+// level: xbar += sum_g grad w_g (abar . a_l[g])
+__global__ void k_adj_gather_w(long n, LevelRefs R, const int *__restrict__ fin,
+                               const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const double *__restrict__ ab,
+                               double *__restrict__ xb)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int l = fin[i];
+    if (l == 0)
+        return;
+    const AmrNode N = R.nodes[l][R.node_of[l][i]];
+    const double sc = (double)(1 << N.lv);
+    const double px = x[i] * sc, py = y[i] * sc, pz = z[i] * sc;
+    const int fx = (int)px, fy = (int)py, fz = (int)pz;
+    double wx[2], wy[2], wz[2];
+    wx[1] = px - fx;
+    wy[1] = py - fy;
+    wz[1] = pz - fz;
+    wx[0] = 1.0 - wx[1];
+    wy[0] = 1.0 - wy[1];
+    wz[0] = 1.0 - wz[1];
+    const double sgn[2] = {-sc, sc};
+    const double a0 = ab[i], a1 = ab[n + i], a2 = ab[2 * n + i];
+    const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
+    const long g0 = grid_index(N, fx - N.ts[0], fy - N.ts[1], fz - N.ts[2]);
+    const double *gx = R.ax[l], *gy = R.ay[l], *gz = R.az[l];
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int ii = 0; ii < 2; ii++)
+            {
+                const long q = g0 + ii + jj * sx + kk * sxy;
+                const double sv = a0 * gx[q] + a1 * gy[q] + a2 * gz[q];
+                dx += sgn[ii] * wy[jj] * wz[kk] * sv;
+                dy += wx[ii] * sgn[jj] * wz[kk] * sv;
+                dz += wx[ii] * wy[jj] * sgn[kk] * sv;
+            }
+    xb[i] += dx;
+    xb[n + i] += dy;
+    xb[2 * n + i] += dz;
+}
+
+__global__ void k_adj_set_mask(int nlist, const int *__restrict__ list, int *__restrict__ mask)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nlist)
+        mask[list[e]] = 1;
+}
+
+// phi-bar at every grid point of level l: -div of a-bar over the interior points
+// where the gradient is taken (neighbours inside the node grid), plus the
+// children's contributions
+__global__ void k_adj_lvl_negdiv(long total, int nn, const AmrNode *__restrict__ nodes,
+                                 const int *__restrict__ mask, const double *__restrict__ A0,
+                                 const double *__restrict__ A1, const double *__restrict__ A2,
+                                 const double *__restrict__ phic, double *__restrict__ out)
+{
+    long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total)
+        return;
+    const AmrNode N = nodes[find_node(nodes, nn, g, 0)];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const double o2h = 1.0 / (2.0 * (1.0 / (1 << N.lv)));
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    double v = 0.0;
+    if (gx + 1 <= N.rd[0] && mask[g + 1])
+        v += A0[g + 1];
+    if (gx - 1 >= 0 && mask[g - 1])
+        v -= A0[g - 1];
+    if (gy + 1 <= N.rd[1] && mask[g + sy])
+        v += A1[g + sy];
+    if (gy - 1 >= 0 && mask[g - sy])
+        v -= A1[g - sy];
+    if (gz + 1 <= N.rd[2] && mask[g + sz])
+        v += A2[g + sz];
+    if (gz - 1 >= 0 && mask[g - sz])
+        v -= A2[g - sz];
+    out[g] = v * o2h + phic[g];
+}
+
+// per node: sum of rhs^2 over its interior list (one block a node, fixed order)
+__global__ void k_adj_node_norm(const AmrNode *__restrict__ nodes, const int *__restrict__ intr,
+                                const double *__restrict__ rhs, double *__restrict__ out)
+{
+    __shared__ double sh[32];
+    const AmrNode N = nodes[blockIdx.x];
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < N.nintr; e += blockDim.x)
+    {
+        const double v = rhs[intr[N.intr_off + e]];
+        acc += v * v;
+    }
+    acc = adj_block_sum(acc, sh);
+    if (threadIdx.x == 0)
+        out[blockIdx.x] = acc;
+}
+
+// phi-bar of a boundary point after the solve: its own minus the solve's
+// coupling (1/H^2) sum of lam at the six neighbours (lam is zero off the interior)
+__device__ __forceinline__ double adj_phit(const AmrNode &N, long g, const double *phib,
+                                           const double *lam)
+{
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const double H = 1.0 / (1 << N.lv);
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    double nb = 0.0;
+    if (gx + 1 <= N.rd[0])
+        nb += lam[g + 1];
+    if (gx - 1 >= 0)
+        nb += lam[g - 1];
+    if (gy + 1 <= N.rd[1])
+        nb += lam[g + sy];
+    if (gy - 1 >= 0)
+        nb += lam[g - sy];
+    if (gz + 1 <= N.rd[2])
+        nb += lam[g + sz];
+    if (gz - 1 >= 0)
+        nb += lam[g - sz];
+    return phib[g] - nb / (H * H);
+}
+
+// transposes of the parent averages at the node boundary points: 0.125 of the
+// point's phi-bar (after the solve) and a-bar to each of its 8 parent points
+__global__ void k_adj_bdry_T(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                             const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
+                             const double *__restrict__ phib, const double *__restrict__ lam,
+                             const double *__restrict__ A0, const double *__restrict__ A1,
+                             const double *__restrict__ A2, double *__restrict__ pA0,
+                             double *__restrict__ pA1, double *__restrict__ pA2,
+                             double *__restrict__ pphic)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nlist)
+        return;
+    const long g = list[e];
+    const AmrNode N = nodes[lnode[e]];
+    const AmrNode P = pnodes[N.parent];
+    int gx, gy, gz;
+    grid_coords(N, g, &gx, &gy, &gz);
+    const int cx = gx + N.ts[0], cy = gy + N.ts[1], cz = gz + N.ts[2];
+    const double ft = 0.125 * adj_phit(N, g, phib, lam);
+    const double a0 = 0.125 * A0[g], a1 = 0.125 * A1[g], a2 = 0.125 * A2[g];
+    const int xs[2] = {(cx >> 1) - P.ts[0], ((cx + 1) >> 1) - P.ts[0]};
+    const int ys[2] = {(cy >> 1) - P.ts[1], ((cy + 1) >> 1) - P.ts[1]};
+    const int zs[2] = {(cz >> 1) - P.ts[2], ((cz + 1) >> 1) - P.ts[2]};
+    const long sx = P.rd[0] + 1, sxy = sx * (P.rd[1] + 1);
+    for (int kk = 0; kk < 2; kk++)
+        for (int jj = 0; jj < 2; jj++)
+            for (int ii = 0; ii < 2; ii++)
+            {
+                const long q = P.grid_off + xs[ii] + ys[jj] * sx + zs[kk] * sxy;
+                atomicAdd(&pphic[q], ft);
+                atomicAdd(&pA0[q], a0);
+                atomicAdd(&pA1[q], a1);
+                atomicAdd(&pA2[q], a2);
+            }
+}
+
+// simulation-boundary points (analytic, linear in M): per block partial sums of
+// phi-bar (after the solve) times phi plus a-bar . a
+__global__ void k_adj_simb_T(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                             const AmrNode *__restrict__ nodes, const double *__restrict__ phib,
+                             const double *__restrict__ lam, const double *__restrict__ pot,
+                             const double *__restrict__ A0, const double *__restrict__ A1,
+                             const double *__restrict__ A2, const double *__restrict__ a0,
+                             const double *__restrict__ a1, const double *__restrict__ a2,
+                             double *__restrict__ partial)
+{
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nlist; e += gridDim.x * blockDim.x)
+    {
+        const long g = list[e];
+        const AmrNode N = nodes[lnode[e]];
+        acc += adj_phit(N, g, phib, lam) * pot[g] + (A0[g] * a0[g] + A1[g] * a1[g] + A2[g] * a2[g]);
+    }
+    acc = adj_block_sum(acc, sh);
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = acc;
+}
+
+// the level deposit's transpose for every particle of level l's nodes (branch
+// weights w1 = x - H floor(x / H), w2 = H - w1, times 4 pi G m / H^6)
+__global__ void k_adj_lvl_depT(long n, double coeff, const int *__restrict__ node_of,
+                               const AmrNode *__restrict__ nodes, const double *__restrict__ x,
+                               const double *__restrict__ y, const double *__restrict__ z,
+                               const double *__restrict__ m, const double *__restrict__ lam,
+                               double *__restrict__ xb, double *__restrict__ mb)
+{
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int nd = node_of[i];
+    if (nd < 0)
+        return;
+    const AmrNode N = nodes[nd];
+    const double H = 1.0 / (1 << N.lv), ooh = (double)(1 << N.lv);
+    const int fx = (int)(x[i] * ooh), fy = (int)(y[i] * ooh), fz = (int)(z[i] * ooh);
+    double wx[2], wy[2], wz[2];
+    wx[1] = x[i] - H * fx;
+    wy[1] = y[i] - H * fy;
+    wz[1] = z[i] - H * fz;
+    wx[0] = H - wx[1];
+    wy[0] = H - wy[1];
+    wz[0] = H - wz[1];
+    const double sgn[2] = {-1.0, 1.0};
+    const double cm = coeff * m[i];
+    const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
+    const long g0 = grid_index(N, fx - N.ts[0], fy - N.ts[1], fz - N.ts[2]);
+    double dx = 0.0, dy = 0.0, dz = 0.0, dm = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int ii = 0; ii < 2; ii++)
+            {
+                const double lq = lam[g0 + ii + jj * sx + kk * sxy];
+                dx += sgn[ii] * wy[jj] * wz[kk] * lq;
+                dy += wx[ii] * sgn[jj] * wz[kk] * lq;
+                dz += wx[ii] * wy[jj] * sgn[kk] * lq;
+                dm += wx[ii] * wy[jj] * wz[kk] * lq;
+            }
+    xb[i] += cm * dx;
+    xb[n + i] += cm * dy;
+    xb[2 * n + i] += cm * dz;
+    mb[i] += coeff * dm;
+}
+
+// the head's phi-bar at its interior points gains the children's contributions
+__global__ void k_adj_add_interior(int L, long D, const double *__restrict__ phic,
+                                   double *__restrict__ phib)
+{
+    const int m = (1 << L) - 1;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)m * m * m)
+        return;
+    const long i = 2 + t % m, j = 2 + (t / m) % m, k = 2 + t / ((long)m * m);
+    const long g = i + j * D + k * D * D;
+    phib[g] += phic[g];
+}
+
 // ---- host side ----------------------------------------------------------------------------
 static int adj_check(qz_sim *s)
 {
     const qz_config &c = s->cfg;
-    if (c.lmax != c.lmin || c.force_stencil != 0 || c.bdry != 1 || c.precision != QZ_PREC_FP64 ||
-        c.head_pot_method != 0)
+    if ((c.lmax != c.lmin && !c.freeze_tree) || c.force_stencil != 0 || c.bdry != 1 ||
+        c.precision != QZ_PREC_FP64 || c.head_pot_method != 0)
     {
-        set_error("adjoint: head-only FP64 runs with the 3-point stencil, reflexive walls and "
-                  "the multigrid head solve only");
+        set_error("adjoint: FP64 runs with the 3-point stencil, reflexive walls and the "
+                  "multigrid head solve, head-only or with a frozen refinement tree only");
         return QZ_FAILURE;
     }
     if (c.total_mass <= 0.0)
@@ -428,8 +812,18 @@ static int adj_check(qz_sim *s)
     return QZ_SUCCESS;
 }
 
-// record layout of a stored state: x y z vx vy vz ax ay az (n each), then pot (gpts)
-static long rec_len(const qz_sim *s) { return 9 * s->n + s->gpts; }
+static bool amr_adj(const qz_sim *s);
+
+// record layout of a stored state: x y z vx vy vz ax ay az (n each), the head
+// potential (gpts), then on a frozen refinement tree every level's potential
+static long rec_len(const qz_sim *s)
+{
+    long r = 9 * s->n + s->gpts;
+    if (amr_adj(s))
+        for (int l = 1; l < s->amr_nlev; l++)
+            r += s->amr[l].grid_total;
+    return r;
+}
 
 static bool copy_d2d(qz_sim *s, double *dst, const double *src, long count)
 {
@@ -445,7 +839,19 @@ static bool save_state(qz_sim *s, double *rec)
     for (int q = 0; q < 9; q++)
         if (!copy_d2d(s, rec + q * n, src[q], n))
             return false;
-    return copy_d2d(s, rec + 9 * n, s->pot, s->gpts);
+    if (!copy_d2d(s, rec + 9 * n, s->pot, s->gpts))
+        return false;
+    if (amr_adj(s))
+    {
+        long o = 9 * n + s->gpts;
+        for (int l = 1; l < s->amr_nlev; l++)
+        {
+            if (!copy_d2d(s, rec + o, s->amr[l].pot, s->amr[l].grid_total))
+                return false;
+            o += s->amr[l].grid_total;
+        }
+    }
+    return true;
 }
 
 static bool load_state(qz_sim *s, const double *rec)
@@ -455,7 +861,31 @@ static bool load_state(qz_sim *s, const double *rec)
     for (int q = 0; q < 9; q++)
         if (!copy_d2d(s, dst[q], rec + q * n, n))
             return false;
-    return copy_d2d(s, s->pot, rec + 9 * n, s->gpts);
+    if (!copy_d2d(s, s->pot, rec + 9 * n, s->gpts))
+        return false;
+    if (amr_adj(s))
+    {
+        long o = 9 * n + s->gpts;
+        for (int l = 1; l < s->amr_nlev; l++)
+        {
+            if (!copy_d2d(s, s->amr[l].pot, rec + o, s->amr[l].grid_total))
+                return false;
+            o += s->amr[l].grid_total;
+        }
+    }
+    return true;
+}
+
+// A stored state made current for a pull-back: particles and potentials loaded,
+// particles reassigned to the frozen tree, grid accelerations recomputed.
+static int prepare_state(qz_sim *s, const double *rec)
+{
+    if (!load_state(s, rec))
+        return QZ_FAILURE;
+    if (!amr_adj(s))
+        return QZ_SUCCESS;
+    return (amr_reassign(s) || grid_accel_head(s) || amr_grid_accel(s)) ? QZ_FAILURE
+                                                                         : QZ_SUCCESS;
 }
 
 static int adj_alloc(qz_sim *s, long ck_recs, long seg_recs)
@@ -492,9 +922,103 @@ static int adj_alloc(qz_sim *s, long ck_recs, long seg_recs)
 // mbar += the total-mass term of this pull-back is accumulated in red[2*RB + 8].
 static double *mbar_acc(qz_sim *s) { return s->adj->red.p + 2L * ADJ_RED_BLOCKS + 8; }
 
+static bool amr_adj(const qz_sim *s) { return s->cfg.lmax > s->cfg.lmin && s->amr_nlev > 1; }
+
+// Per-level adjoint buffers for the current tree.
+static int adj_alloc_levels(qz_sim *s)
+{
+    Adjoint &A = *s->adj;
+    const int nl = s->amr_nlev;
+    auto grow = [&](auto &v) {
+        if ((int)v.size() < nl)
+            v.resize(nl);
+    };
+    grow(A.lA);
+    grow(A.lphic);
+    grow(A.lphib);
+    grow(A.llam);
+    grow(A.lscr);
+    grow(A.lthr);
+    grow(A.lmask);
+    const long n = s->n > 0 ? s->n : 1;
+    if (!A.finest.ensure(s->mem, n) || !A.abh.ensure(s->mem, 3 * n) ||
+        !A.phic0.ensure(s->mem, s->gpts))
+        return QZ_FAILURE;
+    long nnmax = 1;
+    for (int l = 1; l < nl; l++)
+    {
+        const AmrLevel &L = s->amr[l];
+        const long gt = L.grid_total > 0 ? L.grid_total : 1;
+        const bool fresh = A.llam[l].p == nullptr || A.llam[l].cap < gt;
+        if (!A.lA[l].ensure(s->mem, 3 * gt) || !A.lphic[l].ensure(s->mem, gt) ||
+            !A.lphib[l].ensure(s->mem, gt) || !A.llam[l].ensure(s->mem, gt) ||
+            !A.lscr[l].ensure(s->mem, gt) || !A.lmask[l].ensure(s->mem, gt) ||
+            !A.lthr[l].ensure(s->mem, L.nnodes > 0 ? L.nnodes : 1))
+            return QZ_FAILURE;
+        if (fresh)
+            cudaMemsetAsync(A.llam[l].p, 0, A.llam[l].cap * sizeof(double), s->stream);
+        nnmax = std::max(nnmax, (long)L.nnodes);
+    }
+    return A.nrm.ensure(s->mem, nnmax) ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// a-bar deposited on the grid of level l >= 1 from the particles whose finest
+// level is l (sort by level cell, segmented sums, point sums: fixed order)
+static int adj_level_deposit(qz_sim *s, int l, const double *x, const double *y, const double *z,
+                             const double *ab)
+{
+    Adjoint &A = *s->adj;
+    AmrLevel &L = s->amr[l];
+    const long n = s->n;
+    double *A0 = A.lA[l].p, *A1 = A0 + L.grid_total, *A2 = A1 + L.grid_total;
+    if (!s->amr_tmp.ensure(s->mem, 2 * n + 2) || !L.cell_seg.ensure(s->mem, L.box_total))
+        return QZ_FAILURE;
+    int *flag = s->amr_tmp.p, *slot = flag + n;
+    launch(s, QZ_PROF_DEPOSIT, 8.0 * n, k_adj_flag_level, dim3(blocks_for(n, 256)), dim3(256), n,
+           A.finest.p, l, flag);
+    if (scan_exclusive(s, flag, slot, n))
+        return QZ_FAILURE;
+    int t[2];
+    if (!check_cuda(cudaMemcpyAsync(A.host, slot + n - 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                    s->stream), "adjoint level count") ||
+        !check_cuda(cudaMemcpyAsync((char *)A.host + sizeof(int), flag + n - 1, sizeof(int),
+                                    cudaMemcpyDeviceToHost, s->stream), "adjoint level count") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "adjoint level count"))
+        return QZ_FAILURE;
+    memcpy(t, A.host, sizeof t);
+    const long m = (long)t[0] + t[1];
+    if (m == 0)
+    {
+        cudaMemsetAsync(A0, 0, 3 * L.grid_total * sizeof(double), s->stream);
+        return QZ_SUCCESS;
+    }
+    launch(s, QZ_PROF_DEPOSIT, 44.0 * n, k_adj_lvl_keys, dim3(blocks_for(n, 256)), dim3(256), n, l,
+           A.finest.p, s->node_of[l].p, L.nodes.p, x, y, z, slot, s->sort.k0, s->sort.v0);
+    int bits = 1;
+    while ((1L << bits) < L.box_total)
+        bits++;
+    unsigned *ks;
+    int *perm;
+    if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm))
+        return QZ_FAILURE;
+    if (!A.cs.ensure(s->mem, 24 * m + 24))
+        return QZ_FAILURE;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const long blocks = std::min((m * 32 + 255) / 256, (long)sms * 16);
+    launch(s, QZ_PROF_DEPOSIT, 56.0 * m, k_adj_seg_reduce, dim3((int)blocks), dim3(256),
+           L.h[0].lv, perm, s->seg_start, s->flags, x, y, z, ab, ab + n, ab + 2 * n, A.cs.p);
+    launch(s, QZ_PROF_DEPOSIT, 24.0 * L.grid_total, k_adj_lvl_point_gather3,
+           dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, L.nnodes, L.nodes.p,
+           L.cell_seg.p, A.cs.p, A0, A1, A2);
+    return check_cuda(cudaGetLastError(), "adjoint level deposit") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 // Vector-Jacobian product of the force at the positions (x, y, z) with
 // potential pot, for the accelerations' adjoint ab (3n): adds into xb (3n), mb
-// (n) and the total-mass accumulator.  lam is the solve's initial guess.
+// (n) and the total-mass accumulator.  lam is the solve's initial guess.  With
+// refinement levels (a frozen tree), the levels' potentials, accelerations and
+// particle assignments must be those of this state.
 static int force_vjp(qz_sim *s, const double *x, const double *y, const double *z,
                      const double *pot, const double *ab, int *cycles)
 {
@@ -508,7 +1032,26 @@ static int force_vjp(qz_sim *s, const double *x, const double *y, const double *
     *cycles = 0;
     if (n == 0)
         return QZ_SUCCESS;
-    // grid accelerations of this state (interior; the shell values stay)
+    const bool amr = amr_adj(s);
+    const int nl = amr ? s->amr_nlev : 1;
+    const double *abh = ab;
+    if (amr)
+    {
+        if (adj_alloc_levels(s))
+        {
+            set_error("adjoint level buffers: out of device memory");
+            return QZ_FAILURE;
+        }
+        NodeOfPtrs no{};
+        for (int l = 0; l < nl; l++)
+            no.p[l] = s->node_of[l].p;
+        launch(s, QZ_PROF_GATHER, 8.0 * n * nl, k_adj_finest, dim3(blocks_for(n, 256)), dim3(256),
+               n, nl, no, A.finest.p);
+        launch(s, QZ_PROF_GATHER, 56.0 * n, k_adj_mask_ab, dim3(blocks_for(n, 256)), dim3(256), n,
+               A.finest.p, ab, A.abh.p);
+        abh = A.abh.p;
+    }
+    // head grid accelerations of this state (interior; the shell values stay)
     if (grid_accel_head_from(s, pot))
         return QZ_FAILURE;
     int *perm;
@@ -517,24 +1060,133 @@ static int force_vjp(qz_sim *s, const double *x, const double *y, const double *
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     const long blocks = std::min((n * 32 + 255) / 256, (long)sms * 16);
+    if (!A.cs.ensure(s->mem, 24 * n + 24))
+        return QZ_FAILURE;
     launch(s, QZ_PROF_DEPOSIT, 56.0 * n, k_adj_seg_reduce, dim3((int)blocks), dim3(256), L, perm,
-           s->seg_start, s->flags, x, y, z, ab, ab + n, ab + 2 * n, A.cs.p);
+           s->seg_start, s->flags, x, y, z, abh, abh + n, abh + 2 * n, A.cs.p);
     double *Abx = A.Ab.p, *Aby = A.Ab.p + s->gpts, *Abz = A.Ab.p + 2 * s->gpts;
     launch(s, QZ_PROF_DEPOSIT, 24.0 * s->gpts, k_adj_point_gather, dim3(blocks_for(s->gpts, 256)),
            dim3(256), D, s->cell_seg, A.cs.p, Abx, Aby, Abz);
+    if (amr)
+    {
+        // the finest-level gathers' transposes, then the levels from the finest down
+        for (int l = 1; l < nl; l++)
+            if (adj_level_deposit(s, l, x, y, z, ab))
+                return QZ_FAILURE;
+        LevelRefs R{};
+        R.nlev = nl;
+        for (int l = 0; l < nl; l++)
+        {
+            R.nodes[l] = s->amr[l].nodes.p;
+            R.node_of[l] = s->node_of[l].p;
+            R.ax[l] = l == 0 ? s->gax : s->amr[l].ax;
+            R.ay[l] = l == 0 ? s->gay : s->amr[l].ay;
+            R.az[l] = l == 0 ? s->gaz : s->amr[l].az;
+        }
+        launch(s, QZ_PROF_GATHER, 112.0 * n, k_adj_gather_w, dim3(blocks_for(n, 256)), dim3(256), n,
+               R, A.finest.p, x, y, z, ab, A.xb.p);
+        cudaMemsetAsync(A.phic0.p, 0, s->gpts * sizeof(double), s->stream);
+        for (int l = 1; l < nl; l++)
+            cudaMemsetAsync(A.lphic[l].p, 0, s->amr[l].grid_total * sizeof(double), s->stream);
+        for (int l = nl - 1; l >= 1; l--)
+        {
+            AmrLevel &Lv = s->amr[l];
+            AmrLevel &P = s->amr[l - 1];
+            const long gt = Lv.grid_total;
+            double *A0 = A.lA[l].p, *A1 = A0 + gt, *A2 = A1 + gt;
+            double *pA0, *pA1, *pA2, *pphic;
+            if (l == 1)
+            {
+                pA0 = Abx;
+                pA1 = Aby;
+                pA2 = Abz;
+                pphic = A.phic0.p;
+            }
+            else
+            {
+                const long pg = P.grid_total;
+                pA0 = A.lA[l - 1].p;
+                pA1 = pA0 + pg;
+                pA2 = pA1 + pg;
+                pphic = A.lphic[l - 1].p;
+            }
+            cudaMemsetAsync(A.lmask[l].p, 0, gt * sizeof(int), s->stream);
+            if (Lv.intr_total > 0)
+                launch(s, QZ_PROF_OTHER, 8.0 * Lv.intr_total, k_adj_set_mask,
+                       dim3(blocks_for(Lv.intr_total, 256)), dim3(256), Lv.intr_total, Lv.intr.p,
+                       A.lmask[l].p);
+            launch(s, QZ_PROF_GRADIENT, 60.0 * gt, k_adj_lvl_negdiv, dim3(blocks_for(gt, 256)),
+                   dim3(256), gt, Lv.nnodes, Lv.nodes.p, A.lmask[l].p, A0, A1, A2, A.lphic[l].p,
+                   A.lphib[l].p);
+            // node thresholds from the rhs norms; nodes with a zero rhs keep lam = 0
+            launch(s, QZ_PROF_OTHER, 8.0 * Lv.intr_total, k_adj_node_norm, dim3(Lv.nnodes),
+                   dim3(256), Lv.nodes.p, Lv.intr.p, A.lphib[l].p, A.nrm.p);
+            std::vector<double> nrm(Lv.nnodes);
+            if (!check_cuda(cudaMemcpyAsync(nrm.data(), A.nrm.p, Lv.nnodes * sizeof(double),
+                                            cudaMemcpyDeviceToHost, s->stream), "node norms") ||
+                !check_cuda(cudaStreamSynchronize(s->stream), "node norms"))
+                return QZ_FAILURE;
+            std::vector<char> skip(Lv.nnodes, 0);
+            std::vector<double> thr(Lv.nnodes, 0.0);
+            const double rt = s->cfg.adjoint_tol;
+            for (int q = 0; q < Lv.nnodes; q++)
+            {
+                skip[q] = nrm[q] == 0.0 || Lv.h[q].nintr == 0;
+                thr[q] = rt * rt * nrm[q];
+                if (skip[q])
+                {
+                    const AmrNode &N = Lv.h[q];
+                    const long pts = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
+                    cudaMemsetAsync(A.llam[l].p + N.grid_off, 0, pts * sizeof(double), s->stream);
+                }
+            }
+            if (!check_cuda(cudaMemcpyAsync(A.lthr[l].p, thr.data(), Lv.nnodes * sizeof(double),
+                                            cudaMemcpyHostToDevice, s->stream), "node thresholds"))
+                return QZ_FAILURE;
+            const long long it0 = s->stats.cg_iterations;
+            if (cg_level_adjoint(s, l, A.llam[l].p, A.lphib[l].p, A.lscr[l].p, A.lthr[l].p, skip))
+                return QZ_FAILURE;
+            *cycles += (int)(s->stats.cg_iterations - it0);
+            s->stats.cg_iterations = it0; // the forward's count stays the forward's
+            if (Lv.bdry_total > 0)
+                launch(s, QZ_PROF_OTHER, 160.0 * Lv.bdry_total, k_adj_bdry_T,
+                       dim3(blocks_for(Lv.bdry_total, 256)), dim3(256), Lv.bdry_total, Lv.bdry.p,
+                       Lv.bdry_node.p, Lv.nodes.p, P.nodes.p, A.lphib[l].p, A.llam[l].p, A0, A1,
+                       A2, pA0, pA1, pA2, pphic);
+            if (Lv.simb_total > 0)
+            {
+                launch(s, QZ_PROF_OTHER, 96.0 * Lv.simb_total, k_adj_simb_T, dim3(ADJ_RED_BLOCKS),
+                       dim3(256), Lv.simb_total, Lv.simb.p, Lv.simb_node.p, Lv.nodes.p,
+                       A.lphib[l].p, A.llam[l].p, Lv.pot, A0, A1, A2, Lv.ax, Lv.ay, Lv.az,
+                       A.red.p);
+                launch(s, QZ_PROF_OTHER, 8.0 * ADJ_RED_BLOCKS, k_adj_final, dim3(1), dim3(256),
+                       ADJ_RED_BLOCKS, A.red.p, 1.0 / s->cfg.total_mass, 1, mbar_acc(s));
+            }
+            const double Hl = 1.0 / (1 << Lv.h[0].lv);
+            const double cl = 4.0 * s->cfg.G * QZ_PI_D / (Hl * Hl * Hl * Hl * Hl * Hl);
+            launch(s, QZ_PROF_GATHER, 144.0 * n, k_adj_lvl_depT, dim3(blocks_for(n, 256)),
+                   dim3(256), n, cl, s->node_of[l].p, Lv.nodes.p, x, y, z, s->m, A.llam[l].p,
+                   A.xb.p, A.mb.p);
+        }
+    }
     const long m = (1L << L) - 1;
     launch(s, QZ_PROF_GRADIENT, 32.0 * m * m * m, k_adj_negdiv, dim3(blocks_for(m * m * m, 256)),
            dim3(256), L, D, o2h, Abx, Aby, Abz, A.phib.p);
-    if (solve_zero_bc(s, A.lam.p, A.phib.p, s->cfg.adjoint_tol, A.red.p, A.host, cycles))
+    if (amr)
+        launch(s, QZ_PROF_GRADIENT, 16.0 * m * m * m, k_adj_add_interior,
+               dim3(blocks_for(m * m * m, 256)), dim3(256), L, D, A.phic0.p, A.phib.p);
+    int hc = 0;
+    if (solve_zero_bc(s, A.lam.p, A.phib.p, s->cfg.adjoint_tol, A.red.p, A.host, &hc))
         return QZ_FAILURE;
+    *cycles += hc;
     const long nb = (1L << L) + 1;
     launch(s, QZ_PROF_OTHER, 80.0 * (nb * nb * nb - m * m * m), k_adj_shell,
            dim3(ADJ_RED_BLOCKS), dim3(256), L, D, o2h, oh2, pot, A.lam.p, Abx, Aby, Abz, s->gax,
-           s->gay, s->gaz, A.red.p);
+           s->gay, s->gaz, amr ? (const double *)A.phic0.p : nullptr, A.red.p);
     launch(s, QZ_PROF_OTHER, 8.0 * ADJ_RED_BLOCKS, k_adj_final, dim3(1), dim3(256), ADJ_RED_BLOCKS,
            A.red.p, 1.0 / s->cfg.total_mass, 1, mbar_acc(s));
     launch(s, QZ_PROF_GATHER, 112.0 * n + 32.0 * 8 * n, k_adj_gather, dim3(blocks_for(n, 256)),
-           dim3(256), n, L, D, coeff, x, y, z, s->m, ab, ab + n, ab + 2 * n, s->gax, s->gay,
+           dim3(256), n, L, D, coeff, x, y, z, s->m, abh, abh + n, abh + 2 * n, s->gax, s->gay,
            s->gaz, A.lam.p, A.xb.p, A.xb.p + n, A.xb.p + 2 * n, A.mb.p, s->flags);
     return check_cuda(cudaGetLastError(), "adjoint force") ? QZ_SUCCESS : QZ_FAILURE;
 }
@@ -560,9 +1212,14 @@ static bool h2d_any(qz_sim *s, double *dst, const double *src, long count)
 // grid fields consistent with it.
 static int restore_full(qz_sim *s, const double *rec)
 {
-    if (!load_state(s, rec) || deposit_head(s) || grid_accel_head(s))
+    if (!load_state(s, rec))
         return QZ_FAILURE;
-    return QZ_SUCCESS;
+    if (amr_adj(s))
+        return (amr_reassign(s) || deposit_head(s) || amr_deposit(s) || grid_accel_head(s) ||
+                amr_grid_accel(s))
+                   ? QZ_FAILURE
+                   : QZ_SUCCESS;
+    return (deposit_head(s) || grid_accel_head(s)) ? QZ_FAILURE : QZ_SUCCESS;
 }
 
 } // namespace qz
@@ -591,6 +1248,16 @@ int qz_force_vjp(qz_sim *s, const double *abx, const double *aby, const double *
     cudaMemsetAsync(A.mb.p, 0, n * sizeof(double), s->stream);
     cudaMemsetAsync(A.lam.p, 0, s->gpts * sizeof(double), s->stream);
     cudaMemsetAsync(mbar_acc(s), 0, sizeof(double), s->stream);
+    if (amr_adj(s))
+    {
+        if (adj_alloc_levels(s))
+        {
+            set_error("adjoint level buffers: out of device memory");
+            return QZ_FAILURE;
+        }
+        for (int l = 1; l < s->amr_nlev; l++)
+            cudaMemsetAsync(A.llam[l].p, 0, A.llam[l].cap * sizeof(double), s->stream);
+    }
     if (!h2d_any(s, A.ab.p, abx, n) || !h2d_any(s, A.ab.p + n, aby, n) ||
         !h2d_any(s, A.ab.p + 2 * n, abz, n))
         return QZ_FAILURE;
@@ -676,6 +1343,16 @@ int qz_adjoint_final_loss(qz_sim *s, int nsteps, double dt, int checkpoint_every
         cudaMemsetAsync(A.mb.p, 0, n * sizeof(double), s->stream);
         cudaMemsetAsync(A.lam.p, 0, s->gpts * sizeof(double), s->stream);
         cudaMemsetAsync(mbar_acc(s), 0, sizeof(double), s->stream);
+        if (amr_adj(s))
+        {
+            if (adj_alloc_levels(s))
+            {
+                set_error("adjoint level buffers: out of device memory");
+                break;
+            }
+            for (int l = 1; l < s->amr_nlev; l++)
+                cudaMemsetAsync(A.llam[l].p, 0, A.llam[l].cap * sizeof(double), s->stream);
+        }
         cudaEventRecord(e1, s->stream);
         // ---- reverse sweep, segment by segment
         for (int sg = nseg - 1; sg >= 0 && ok; sg--)
@@ -705,7 +1382,17 @@ int qz_adjoint_final_loss(qz_sim *s, int nsteps, double dt, int checkpoint_every
                 launch(s, QZ_PROF_LEAPFROG, 72.0 * n, k_adj_kick, dim3(blocks_for(3 * n, 256)),
                        dim3(256), 3 * n, dt, A.vb.p, A.ac.p, A.ab.p);
                 int cyc = 0;
-                if (force_vjp(s, S1, S1 + n, S1 + 2 * n, S1 + 9 * n, A.ab.p, &cyc))
+                if (amr_adj(s))
+                {
+                    // the levels' fields of the state are rebuilt in the simulation
+                    if (prepare_state(s, S1) ||
+                        force_vjp(s, s->x, s->y, s->z, s->pot, A.ab.p, &cyc))
+                    {
+                        ok = false;
+                        break;
+                    }
+                }
+                else if (force_vjp(s, S1, S1 + n, S1 + 2 * n, S1 + 9 * n, A.ab.p, &cyc))
                 {
                     ok = false;
                     break;
@@ -721,7 +1408,12 @@ int qz_adjoint_final_loss(qz_sim *s, int nsteps, double dt, int checkpoint_every
         {
             const double *S0 = A.seg.p;
             int cyc = 0;
-            if (force_vjp(s, S0, S0 + n, S0 + 2 * n, S0 + 9 * n, A.ac.p, &cyc))
+            if (amr_adj(s))
+            {
+                if (prepare_state(s, S0) || force_vjp(s, s->x, s->y, s->z, s->pot, A.ac.p, &cyc))
+                    break;
+            }
+            else if (force_vjp(s, S0, S0 + n, S0 + 2 * n, S0 + 9 * n, A.ac.p, &cyc))
                 break;
             cycles += cyc;
         }

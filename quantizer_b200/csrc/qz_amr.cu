@@ -40,55 +40,16 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include "qz_internal.cuh"
+#include "qz_amr_dev.cuh"
 
 namespace cgrp = cooperative_groups;
 
 namespace qz {
 
 #define QZ_PI_D 3.14159265358979323846
-constexpr int AMR_MAX_LEVELS = 16;
 // largest block of the conjugate gradient kernel (two blocks per SM at 64 registers)
 constexpr int CG_MAX_THREADS = 512;
 
-// ---- small device helpers --------------------------------------------------------------
-// Index of the last node whose offset (0: grid_off, 1: cls_off, 2: box_off) is <= v.
-__device__ __forceinline__ int find_node(const AmrNode *nodes, int nn, long v, int field)
-{
-    int lo = 0, hi = nn - 1;
-    while (lo < hi)
-    {
-        int mid = (lo + hi + 1) >> 1;
-        long off = field == 0 ? nodes[mid].grid_off : field == 1 ? nodes[mid].cls_off : nodes[mid].box_off;
-        if (off <= v)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ long box_index(const AmrNode &N, int cx, int cy, int cz)
-{
-    return (long)(cx - N.ts[0]) + (long)(cy - N.ts[1]) * N.rd[0] +
-           (long)(cz - N.ts[2]) * N.rd[0] * N.rd[1];
-}
-
-__device__ __forceinline__ long grid_index(const AmrNode &N, int gx, int gy, int gz)
-{
-    // box grid coordinates (not level coordinates)
-    return N.grid_off + gx + (long)gy * (N.rd[0] + 1) + (long)gz * (N.rd[0] + 1) * (N.rd[1] + 1);
-}
-
-__device__ __forceinline__ void grid_coords(const AmrNode &N, long g, int *gx, int *gy, int *gz)
-{
-    long l = g - N.grid_off;
-    const long sx = N.rd[0] + 1, sxy = sx * (N.rd[1] + 1);
-    *gz = (int)(l / sxy);
-    l -= (long)(*gz) * sxy;
-    *gy = (int)(l / sx);
-    *gx = (int)(l - (long)(*gy) * sx);
-}
 
 __device__ __forceinline__ double block_sum_d(double v, double *sh)
 {
@@ -730,6 +691,23 @@ static bool ensure_sort(qz_sim *s, long need)
 }
 
 // Rebuilds the tree below the head from the current positions.
+// Frozen tree: the nodes stay; every particle's node on each level is found
+// again from its position, level by level from the head, by the rule the
+// construction uses (k_next_node).
+int amr_reassign(qz_sim *s)
+{
+    const long n = s->n;
+    cudaMemsetAsync(s->node_of[0].p, 0, (n > 0 ? n : 1) * sizeof(int), s->stream);
+    for (int l = 0; l + 1 < s->amr_nlev; l++)
+    {
+        AmrLevel &P = s->amr[l];
+        if (n > 0)
+            launch(s, QZ_PROF_TREE, 36.0 * n, k_next_node, dim3(blocks_for(n, 256)), dim3(256), n,
+                   s->node_of[l].p, P.nodes.p, P.box.p, s->x, s->y, s->z, s->node_of[l + 1].p);
+    }
+    return check_cuda(cudaGetLastError(), "amr reassign") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
 int amr_build(qz_sim *s)
 {
     const long n = s->n;
@@ -1221,23 +1199,6 @@ int amr_deposit(qz_sim *s)
 }
 
 // ---- potential on refinement levels -----------------------------------------------------
-// Parent-interpolated start (potential_branches.c:204-331): 0.125 times the sum
-// of the 8 parent values at (c >> 1, (c + 1) >> 1) per axis, in the reference's
-// order; `field` selects potential or acceleration arrays of the parent.
-__device__ __forceinline__ double from_parent(const AmrNode &P, const double *__restrict__ pf,
-                                              int cx, int cy, int cz)
-{
-    const int x1 = (cx >> 1) - P.ts[0], x2 = ((cx + 1) >> 1) - P.ts[0];
-    const int y1 = (cy >> 1) - P.ts[1], y2 = ((cy + 1) >> 1) - P.ts[1];
-    const int z1 = (cz >> 1) - P.ts[2], z2 = ((cz + 1) >> 1) - P.ts[2];
-    const long sx = P.rd[0] + 1, sxy = sx * (P.rd[1] + 1);
-    const long o = P.grid_off;
-    return 0.125 * (pf[o + x1 + y1 * sx + z1 * sxy] + pf[o + x2 + y1 * sx + z1 * sxy] +
-                    pf[o + x1 + y2 * sx + z1 * sxy] + pf[o + x2 + y2 * sx + z1 * sxy] +
-                    pf[o + x1 + y1 * sx + z2 * sxy] + pf[o + x2 + y1 * sx + z2 * sxy] +
-                    pf[o + x1 + y2 * sx + z2 * sxy] + pf[o + x2 + y2 * sx + z2 * sxy]);
-}
-
 __global__ void k_pot_init(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
                            const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
                            const double *__restrict__ ppot, double *__restrict__ pot)
@@ -1335,6 +1296,7 @@ struct CgArgs {
     int every;
     int max_iter;
     int method; // check_method 0/1/2 of conj_grad_error (poisson_error.c:235-282)
+    const double *thr_node; // per node r.r threshold in place of the mass-based one (or null)
 };
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
@@ -1498,6 +1460,8 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
         x.thr = N.nintr * tt * tt;
         if (A.method == 2)
             x.thr = x.thr * (cbrt((double)N.nintr) * cbrt((double)N.nintr));
+        if (A.thr_node)
+            x.thr = A.thr_node[C.node];
         const long size = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
         x.cap = (int)(size < A.max_iter ? size : A.max_iter);
         x.rs_prev = x.rs_cur = 0.0;
@@ -2247,7 +2211,16 @@ static int sor_level(qz_sim *s, AmrLevel &L, int level_index, const std::vector<
     return check_cuda(cudaGetLastError(), "sor") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
-static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = true)
+// Overrides of a solve that is not the reference's (the adjoint's): per-node
+// r.r thresholds (device array), the ratio-test bound, nodes to leave out.
+struct CgOverride {
+    const double *thr;
+    double tol2;
+    std::vector<char> skip;
+};
+
+static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = true,
+                    const CgOverride *ov = nullptr)
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
@@ -2265,7 +2238,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], (const void *)k_cg1_nodes,
                                                       CG_MAX_THREADS, kCgSmem);
     });
-    const int per_sm = occ[c.cg_variant == 1 ? 1 : 0];
+    const int per_sm = occ[(c.cg_variant == 1 && !ov) ? 1 : 0];
     if (per_sm < 1)
     {
         set_error("conjugate gradient kernel cannot be resident");
@@ -2281,7 +2254,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     {
         node_chunk[2 * q] = (int)L.hchunks.size();
         const AmrNode &N = L.h[q];
-        if (!allow_sor || N.ncells > c.branch_cg_cells)
+        if (ov && ov->skip[q])
+            ; // no work for this node
+        else if (!allow_sor || N.ncells > c.branch_cg_cells)
             for (int b = N.intr_off; b < N.intr_off + N.nintr; b += chunk)
                 L.hchunks.push_back({q, b, std::min(b + chunk, N.intr_off + N.nintr)});
         else if (N.nintr > 0)
@@ -2294,7 +2269,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     if (L.nchunks == 0)
         return QZ_SUCCESS;
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
-    const bool one = c.cg_variant == 1;
+    const bool one = c.cg_variant == 1 && !ov; // the overrides are the two-phase kernel's
     const long nparts = (one ? 3L : 4L) * L.nchunks * CG_PS;
     if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, nparts) ||
         !L.nint.ensure(s->mem, 5L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
@@ -2353,6 +2328,13 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     A.every = c.check_every > 0 ? c.check_every : 1;
     A.max_iter = c.max_iter;
     A.method = c.check_method;
+    A.thr_node = nullptr;
+    if (ov)
+    {
+        A.tol2 = ov->tol2;
+        A.method = 0;
+        A.thr_node = ov->thr;
+    }
     const int blocks = (int)std::min(max_blocks, (long)L.nchunks);
     const int nslot = (L.nchunks + blocks - 1) / blocks;
     A.chunk = chunk;
@@ -2445,6 +2427,26 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         return QZ_FAILURE;
     }
     return check_cuda(cudaGetLastError(), "cg") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// The adjoint's node solves on level l: Lap_h lam = rhs on every node's interior
+// with lam = 0 on the node boundaries (the level's L.pot, L.d, L.pot_old are
+// pointed at lam, rhs and scratch for the call), until r.r <= thr[node]; nodes
+// with skip[node] are left out (their lam stays).
+int cg_level_adjoint(qz_sim *s, int l, double *lam, double *rhs, double *scratch,
+                     const double *thr_dev, const std::vector<char> &skip)
+{
+    AmrLevel &L = s->amr[l];
+    double *kp = L.pot, *kd = L.d, *ko = L.pot_old;
+    L.pot = lam;
+    L.d = rhs;
+    L.pot_old = scratch;
+    CgOverride ov{thr_dev, INFINITY, skip};
+    const int rc = cg_level(s, L, l, false, &ov);
+    L.pot = kp;
+    L.d = kd;
+    L.pot_old = ko;
+    return rc;
 }
 
 int amr_potential(qz_sim *s)
@@ -2668,12 +2670,6 @@ int amr_grid_accel(qz_sim *s)
 }
 
 // ---- gather from the finest node -----------------------------------------------------------
-struct LevelRefs {
-    const AmrNode *nodes[AMR_MAX_LEVELS];
-    const int *node_of[AMR_MAX_LEVELS];
-    const double *ax[AMR_MAX_LEVELS], *ay[AMR_MAX_LEVELS], *az[AMR_MAX_LEVELS];
-    int nlev;
-};
 
 __global__ void k_amr_gather(long n, LevelRefs R, const double *__restrict__ x,
                              const double *__restrict__ y, const double *__restrict__ z,

@@ -318,6 +318,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->adjoint_tol = 1e-10;
     c->cg_variant = 0;
     c->mg_points_per_thread = 4;
+    c->freeze_tree = 0;
     return QZ_SUCCESS;
 }
 
@@ -630,7 +631,14 @@ int qz_tree_adaptation(qz_sim *s)
 {
     if (!s)
         return QZ_FAILURE;
-    return amr_on(s) ? amr_build(s) : QZ_SUCCESS;
+    if (!amr_on(s))
+        return QZ_SUCCESS;
+    if (s->cfg.freeze_tree && s->tree_built)
+        return amr_reassign(s);
+    if (amr_build(s))
+        return QZ_FAILURE;
+    s->tree_built = true;
+    return QZ_SUCCESS;
 }
 
 int qz_grid_density(qz_sim *s)

@@ -329,6 +329,7 @@ struct qz_sim {
     long ofl_removed = 0;
     long ofl_layout_n = 0; // particle count the lists of the last step were laid out for
     int amr_nlev = 1;                  // levels in use this step
+    bool tree_built = false;           // a tree exists (freeze_tree keeps it)
     std::vector<qz::DBuf<int>> node_of; // per level: node of each particle or -1
     qz::DBuf<int> amr_tmp, amr_tmp2;   // scratch (labels, scans, compaction)
     qz::DBuf<int> zone_box;            // per zone: min x,y,z, max x,y,z
@@ -440,6 +441,8 @@ int deposit_head(qz_sim *s);
 int grid_accel_head(qz_sim *s);
 int grid_accel_head_from(qz_sim *s, const double *pot);
 int head_segments(qz_sim *s, const double *x, const double *y, const double *z, int **perm_out);
+int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
+                     unsigned **ks_out, int **perm_out);
 int gather_head(qz_sim *s);
 int kick_drift(qz_sim *s, double dt);
 int kick(qz_sim *s, double dt);
@@ -448,6 +451,9 @@ int potential_head(qz_sim *s);
 int amr_init(qz_sim *s);
 void amr_free(qz_sim *s);
 int amr_build(qz_sim *s);
+int amr_reassign(qz_sim *s); // frozen tree: particles to the existing nodes
+int cg_level_adjoint(qz_sim *s, int l, double *lam, double *rhs, double *scratch,
+                     const double *thr_dev, const std::vector<char> &skip);
 int amr_deposit(qz_sim *s);
 int amr_potential(qz_sim *s);
 int amr_grid_accel(qz_sim *s);
