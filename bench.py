@@ -82,6 +82,11 @@ WORKLOADS.update({
     "adjoint262k_head128": dict(ic="adjoint", n=262144, a=0.04, lmin=7, levels=0, ref_ptcl=9,
                                 steps=200, precision=0, cpu_steps=2, ref_steps=2, every=20,
                                 fd_coords=64, tol=1e-11),
+    # the same with two refinement levels above the head frozen to the tree built at
+    # the initial positions (a cell refines above 8 particles)
+    "adjoint262k_head128_amr2": dict(ic="adjoint", n=262144, a=0.04, lmin=7, levels=2,
+                                     ref_ptcl=9, steps=200, precision=0, cpu_steps=2,
+                                     ref_steps=2, every=20, fd_coords=64, tol=1e-11),
 })
 DEFAULT_WORKLOAD = "plummer1m_head128_amr3"
 
@@ -315,7 +320,9 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     config = {"workload": args.workload, "particles": wl["n"], "head_grid": 2 ** wl["lmin"],
-              "tree": "head node only (fixed)", "dt": "1e-3 crossing time", "precision": "fp64",
+              "tree": "head node only (fixed)" if wl["levels"] == 0 else
+              f"{wl['levels']} refinement levels frozen to the tree of the initial positions",
+              "dt": "1e-3 crossing time", "precision": "fp64",
               "residual_tol": wl["tol"], "adjoint_tol": wl["tol"],
               "checkpoint_every": wl["every"], "loss": "mean_p |x_T - x*_T|^2",
               "targets": "forward run of ICs perturbed by N(0, 1e-3^2) in x, y, z",
@@ -345,6 +352,8 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     dev = torch.device("cuda", local)
     n, L = wl["n"], wl["lmin"]
     cfg = dict(tol=wl["tol"], tol2=wl["tol"], adjoint_tol=wl["tol"])
+    if wl["levels"] > 0:
+        cfg.update(lmax=wl["lmin"] + wl["levels"], ref_ptcl=wl["ref_ptcl"], freeze_tree=1)
     ic = ics.plummer(n, a=wl["a"], seed=replicas.seed_for(rank))
     dt = 1e-3 * ics.crossing_time(wl["a"])
     rng = np.random.default_rng(100 + rank)
@@ -352,17 +361,22 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     for k in ("x", "y", "z"):
         pert[k] = pert[k] + rng.normal(0.0, 1e-3, n)
 
-    def forward(c, steps):
-        with core.Simulation(c, L, **cfg) as sm:
+    def forward(c, steps, base=None):
+        # a frozen tree is built at `base` (the unperturbed positions) and the run
+        # starts from `c` on it, as the gradient assumes
+        with core.Simulation(c if base is None else base, L, **cfg) as sm:
             sm.init_forces()
+            if base is not None:
+                sm.set_particles(c)
+                sm.init_forces()
             sm.step(dt, steps)
             return sm.particles()
 
-    pt = forward(pert, K)
+    pt = forward(pert, K, ic if wl["levels"] > 0 else None)
     tgt = {k: pt[k] for k in ("x", "y", "z")}
 
-    def loss_of(c):
-        p = forward(c, K)
+    def loss_of(c, base=None):
+        p = forward(c, K, base)
         d = sum((p[k] - tgt[k]) ** 2 for k in ("x", "y", "z"))
         return float(d.sum() / n)
 
@@ -409,7 +423,14 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
         cp, cm = {k: v.copy() for k, v in ic.items()}, {k: v.copy() for k, v in ic.items()}
         cp[field][p] += h
         cm[field][p] -= h
-        fd = (loss_of(cp) - loss_of(cm)) / (2 * h)
+        if wl["levels"] > 0:
+            # positions and velocities on the tree of ic; mass runs on their own
+            # masses (the total mass and the shell follow them; the tree is ic's)
+            bp = cp if field == "m" else ic
+            bm = cm if field == "m" else ic
+            fd = (loss_of(cp, bp) - loss_of(cm, bm)) / (2 * h)
+        else:
+            fd = (loss_of(cp) - loss_of(cm)) / (2 * h)
         scale = float(np.abs(g[key]).max())
         errs.append(abs(fd - g[key][p]) / scale)
         rels.append(abs(fd - g[key][p]) / max(abs(fd), 1e-300))
