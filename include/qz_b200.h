@@ -255,8 +255,10 @@ QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const double *dt,
                                 double *best_ms);
 
 /* Differentiation form (no reference counterpart: QUANTIZER has no adjoint).
- * Head-only FP64 runs (lmax == lmin, 3-point stencil, reflexive walls,
- * multigrid head solve).  The force F(x, m) = gather(-grad Lap^-1 deposit(x, m))
+ * FP64 runs with the 3-point stencil, reflexive walls and the multigrid head
+ * solve, head-only or with refinement levels on a frozen tree (freeze_tree:
+ * the node solves, parent averages, level deposits and finest-level gathers
+ * are differentiated with the tree held fixed).  The force F(x, m) = gather(-grad Lap^-1 deposit(x, m))
  * of grid_density.c:35-111, potential_head_node.c:99-179,
  * grid_acceleration.c:36-76 and particle_acceleration.c:33-132 is
  * differentiated with the Poisson solve taken as exact (its adjoint is a

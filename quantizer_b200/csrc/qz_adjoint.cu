@@ -1,4 +1,5 @@
-// qz_adjoint.cu -- reverse-mode derivative of the head-node particle-mesh step.
+// qz_adjoint.cu -- reverse-mode derivative of the particle-mesh step (the head
+// node, and the refinement levels of a frozen tree further below).
 //
 // The forward map of one step (particle_updating.c:39-207, 2677-2688 around
 // grid_density.c:35-111, potential_head_node.c:99-179, grid_acceleration.c:36-76
