@@ -1,6 +1,6 @@
 """GPU: energies and momentum (observables.c:661-696) against the reference's
 observables() on the same states (reference driver, both potential-energy
-forms), in the reference's units (conversion factors from the driver).
+forms), in the reference's units (conversion factors from the reference driver).
 
 Tolerances: kinetic energy 1e-12 relative and momentum 1e-12 of sum m|v| on
 identical velocities (step 0; after steps, those of the velocities); exact

@@ -4,7 +4,7 @@ the compiled reference (oracle/_ref/qz_ref_driver) and its fixtures.
 * force_stencil 1 (grid_acceleration.c:78-197, 396-692): head-only run in the
   lexicographic Gauss-Seidel mode (the reference's arithmetic order) against
   the fixture, tolerances of the 3-point pipeline test; a refinement run
-  against the driver at step 0 and after 3 steps, tolerances of the
+  against the reference driver at step 0 and after 3 steps, tolerances of the
   refinement tests (node accelerations 1e-6 of the node's max, particle
   accelerations 1e-6, positions 1e-10 box units).
 * conjugate gradient as the multigrid smoother (solver 2,
@@ -15,11 +15,11 @@ the compiled reference (oracle/_ref/qz_ref_driver) and its fixtures.
 * the head solved by the node conjugate gradient (head_pot_method 1,
   potential_head_node.c:157-171, conjugate_gradient.c:322-463): head run
   against the fixture with the cg-smoothing tolerances (the dot products are
-  added in a different order); a refinement run against the driver with the
+  added in a different order); a refinement run against the reference driver with the
   same setting, tolerances of the refinement tests.
 * red-black SOR for refinement nodes of at most branch_cg_cells cells
   (potential_branches.c:460-512; here 6000 cells, so the level-1 node takes SOR
-  and the larger ones CG): refinement run against the driver with the same
+  and the larger ones CG): refinement run against the reference driver with the same
   setting, node potentials 1e-8, particle accelerations 1e-6, positions 1e-10
   box units after 3 steps.
 """
