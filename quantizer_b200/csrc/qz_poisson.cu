@@ -751,6 +751,36 @@ template <typename T> struct MgArgs {
     GridBar bar;
 };
 
+// Work item t = a + n0 (b + n1 c) of a grid-stride loop (t = tid, tid + stride,
+// ...): the coordinates are advanced by the stride's own decomposition with
+// carries, so the loop divides only when it starts.  Requires stride > 0; the
+// loop ends when c reaches the third extent.
+struct Walk3 {
+    unsigned a, b, c, da, db, dc, n0, n1;
+    __device__ __forceinline__ Walk3(unsigned t, unsigned stride, unsigned n0_, unsigned n1_)
+        : n0(n0_), n1(n1_)
+    {
+        a = t % n0;
+        unsigned r = t / n0;
+        b = r % n1;
+        c = r / n1;
+        da = stride % n0;
+        r = stride / n0;
+        db = r % n1;
+        dc = r / n1;
+    }
+    __device__ __forceinline__ void next()
+    {
+        a += da;
+        const unsigned ca = a >= n0 ? 1u : 0u;
+        a -= ca ? n0 : 0u;
+        b += db + ca;
+        const unsigned cb = b >= n1 ? 1u : 0u;
+        b -= cb ? n1 : 0u;
+        c += dc + cb;
+    }
+};
+
 // One colour of a red-black sweep over work items t = tid, tid + nthr, ...
 template <typename T>
 __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rho, int color,
@@ -758,14 +788,12 @@ __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rh
 {
     const int m = phi.n - 2;
     const unsigned half = (unsigned)(m + 1) / 2;
-    const unsigned total = half * (unsigned)m * (unsigned)m;
     const T one_sixth = (T)(1.0 / 6.0);
 #pragma unroll 4
-    for (unsigned t = tid; t < total; t += nthr)
+    for (Walk3 x(tid, nthr, half, (unsigned)m); x.c < (unsigned)m; x.next())
     {
-        const unsigned ti = t % half, r = t / half;
-        const int j = 1 + (int)(r % (unsigned)m), k = 1 + (int)(r / (unsigned)m);
-        const int i = ((((1 + j + k) & 1) == color) ? 1 : 2) + 2 * (int)ti;
+        const int j = 1 + (int)x.b, k = 1 + (int)x.c;
+        const int i = ((((1 + j + k) & 1) == color) ? 1 : 2) + 2 * (int)x.a;
         if (i > m)
             continue;
         const long gp = phi.off + i + j * phi.sy + k * phi.sz;
@@ -783,16 +811,13 @@ __device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &r
                                             const Grid<T> &cphi, const Grid<T> &crho, T ooh2,
                                             T scale, unsigned tid, unsigned nthr)
 {
-    const unsigned nc = (unsigned)cphi.n, nc3 = nc * nc * nc;
-    for (unsigned t = tid; t < nc3; t += nthr)
+    const unsigned nc = (unsigned)cphi.n;
+    for (Walk3 x(tid, nthr, nc, nc); x.c < nc; x.next())
+        cphi.p[cphi.off + (long)x.a + (long)x.b * cphi.sy + (long)x.c * cphi.sz] = (T)0;
+    const unsigned mc = nc - 2;
+    for (Walk3 x(tid, nthr, mc, mc); x.c < mc; x.next())
     {
-        const int i = (int)(t % nc), j = (int)((t / nc) % nc), k = (int)(t / (nc * nc));
-        cphi.p[cphi.off + i + j * cphi.sy + k * cphi.sz] = (T)0;
-    }
-    const unsigned mc = nc - 2, mc3 = mc * mc * mc;
-    for (unsigned t = tid; t < mc3; t += nthr)
-    {
-        const int lx = 1 + (int)(t % mc), ly = 1 + (int)((t / mc) % mc), lz = 1 + (int)(t / (mc * mc));
+        const int lx = 1 + (int)x.a, ly = 1 + (int)x.b, lz = 1 + (int)x.c;
         const long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
         const long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
         const T *p = phi.p;
@@ -802,45 +827,76 @@ __device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &r
     }
 }
 
+// phi += the trilinear interpolation of the coarse correction c (k_prolong_add's
+// arithmetic).  A work item is the pair of fine points i = 2a+1 (odd) and
+// i + 1 (even) of one row: both draw on the coarse columns a and a + 1 only, so
+// their up to eight coarse values are loaded once, together.  Each point adds
+// its terms in k_prolong_add's z, y, x order, skipping coarse points outside
+// 1..mc; a point even in all three coordinates takes its coarse value as is.
 template <typename T>
 __device__ __forceinline__ void mg_prolong(const Grid<T> &phi, const Grid<T> &c, unsigned tid,
                                            unsigned nthr)
 {
     const int m = phi.n - 2, mc = c.n - 2;
-    const unsigned um = (unsigned)m, total = um * um * um;
-    for (unsigned t = tid; t < total; t += nthr)
+    const unsigned um = (unsigned)m, pairs = (unsigned)mc + 1; // m = 2 mc + 1
+    for (Walk3 x(tid, nthr, pairs, um); x.c < um; x.next())
     {
-        const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
-        int cx0, cx1, cy0, cy1, cz0, cz1;
-        T wx, wy, wz;
-        if (i & 1) { cx0 = (i - 1) >> 1; cx1 = cx0 + 1; wx = (T)0.5; } else { cx0 = cx1 = i >> 1; wx = (T)1; }
-        if (j & 1) { cy0 = (j - 1) >> 1; cy1 = cy0 + 1; wy = (T)0.5; } else { cy0 = cy1 = j >> 1; wy = (T)1; }
-        if (k & 1) { cz0 = (k - 1) >> 1; cz1 = cz0 + 1; wz = (T)0.5; } else { cz0 = cz1 = k >> 1; wz = (T)1; }
-        T acc;
-        if (!(i & 1) && !(j & 1) && !(k & 1))
-            acc = c.p[c.off + cx0 + cy0 * c.sy + cz0 * c.sz];
-        else
+        const int a = (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
+        const int i0 = 2 * a + 1;
+        const bool second = a < mc; // i0 + 1 <= m
+        // y and z: coarse planes and their presence (odd: (j-1)/2 and (j+1)/2, even: j/2)
+        const bool jo = j & 1, ko = k & 1;
+        const int oy0 = jo ? (j - 1) >> 1 : j >> 1, oz0 = ko ? (k - 1) >> 1 : k >> 1;
+        bool vy[2], vz[2];
+        vy[0] = jo ? oy0 >= 1 : true;
+        vy[1] = jo && oy0 + 1 <= mc;
+        vz[0] = ko ? oz0 >= 1 : true;
+        vz[1] = ko && oz0 + 1 <= mc;
+        const bool vx0 = a >= 1, vx1 = a + 1 <= mc;
+        const T wy = jo ? (T)0.5 : (T)1, wz = ko ? (T)0.5 : (T)1;
+        const long cb = c.off + a + (long)oy0 * c.sy + (long)oz0 * c.sz;
+        T v[8]; // [z][y][x] with x = column a, a + 1
+#pragma unroll
+        for (int q = 0; q < 8; q++)
         {
-            const T wgt = wx * wy * wz;
-            acc = (T)0;
-            for (int cz = cz0; cz <= cz1; cz++)
+            const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
+            const bool ok = vz[az] && vy[ay] && (ax ? vx1 : vx0);
+            v[q] = ok ? c.p[cb + ax + (long)ay * c.sy + (long)az * c.sz] : (T)0;
+        }
+        const long f0 = phi.off + i0 + (long)j * phi.sy + (long)k * phi.sz;
+        const T p0 = phi.p[f0];
+        const T p1 = second ? phi.p[f0 + 1] : (T)0;
+        // odd point i0: x weight 1/2 on both columns
+        const T w0 = (T)0.5 * wy * wz;
+        T acc0 = (T)0;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+            const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
+            if (vz[az] && vy[ay] && (ax ? vx1 : vx0))
+                acc0 += w0 * v[q];
+        }
+        phi.p[f0] = p0 + acc0;
+        if (second)
+        {
+            // even point i0 + 1: column a + 1 at x weight 1
+            T acc1;
+            if (!jo && !ko)
+                acc1 = v[1];
+            else
             {
-                if (cz < 1 || cz > mc)
-                    continue;
-                for (int cy = cy0; cy <= cy1; cy++)
+                const T w1 = (T)1 * wy * wz;
+                acc1 = (T)0;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
                 {
-                    if (cy < 1 || cy > mc)
-                        continue;
-                    for (int cx = cx0; cx <= cx1; cx++)
-                    {
-                        if (cx < 1 || cx > mc)
-                            continue;
-                        acc += wgt * c.p[c.off + cx + cy * c.sy + cz * c.sz];
-                    }
+                    const int az = q >> 1, ay = q & 1;
+                    if (vz[az] && vy[ay])
+                        acc1 += w1 * v[2 * q + 1];
                 }
             }
+            phi.p[f0 + 1] = p1 + acc1;
         }
-        phi.p[phi.off + i + j * phi.sy + k * phi.sz] += acc;
     }
 }
 
@@ -887,11 +943,18 @@ __device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsi
                                         unsigned nthr)
 {
     const unsigned n = (unsigned)a.n, n3 = n * n * n;
-    for (unsigned t = tid; t < n3; t += nthr)
+    const long nn = (long)n * n;
+    if (a.off == 0 && b.off == 0 && a.sy == n && b.sy == n && a.sz == nn && b.sz == nn)
     {
-        const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / (n * n));
-        b.p[b.off + i + j * b.sy + k * b.sz] = a.p[a.off + i + j * a.sy + k * a.sz];
+        // both dense: a flat loop, unrolled so that several loads are in flight
+#pragma unroll 4
+        for (unsigned t = tid; t < n3; t += nthr)
+            b.p[t] = a.p[t];
+        return;
     }
+    for (Walk3 x(tid, nthr, n, n); x.c < n; x.next())
+        b.p[b.off + (long)x.a + (long)x.b * b.sy + (long)x.c * b.sz] =
+            a.p[a.off + (long)x.a + (long)x.b * a.sy + (long)x.c * a.sz];
 }
 
 template <typename T>
@@ -910,13 +973,13 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             const Grid<double> &P = A.fphi, &R = A.frho;
             const int n = P.n, m = n - 2;
             const double ooh2 = (double)((n - 1) * (n - 1));
-            const unsigned um = (unsigned)m, tot = um * um * um, n3 = (unsigned)n * n * n;
+            const unsigned um = (unsigned)m, n3 = (unsigned)n * n * n;
             float *rf = (float *)A.rho[0].p, *ef = (float *)A.phi[0].p;
             for (unsigned t = gtid; t < n3; t += gn)
                 ef[t] = 0.0f;
-            for (unsigned t = gtid; t < tot; t += gn)
+            for (Walk3 x(gtid, gn, um, um); x.c < um; x.next())
             {
-                const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+                const int i = 1 + (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
                 const long gp = P.off + i + j * P.sy + k * P.sz;
                 const long gr = R.off + i + j * R.sy + k * R.sz;
                 const double *p = P.p;
@@ -991,11 +1054,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
         {
             const Grid<double> &P = A.fphi;
             const int n = P.n, m = n - 2;
-            const unsigned um = (unsigned)m, tot = um * um * um;
+            const unsigned um = (unsigned)m;
             const float *ef = (const float *)A.phi[0].p;
-            for (unsigned t = gtid; t < tot; t += gn)
+            for (Walk3 x(gtid, gn, um, um); x.c < um; x.next())
             {
-                const int i = 1 + (int)(t % um), j = 1 + (int)((t / um) % um), k = 1 + (int)(t / (um * um));
+                const int i = 1 + (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
                 P.p[P.off + i + j * P.sy + k * P.sz] += (double)ef[i + (long)j * n + (long)k * n * n];
             }
             gsync();
