@@ -735,6 +735,7 @@ int vcycle(qz_sim *s, int level, int type) { return vcycle_t<double>(s, level, t
 constexpr int MG_MAXLEV = 12;
 constexpr int MG_SMALL_N = 17;
 constexpr int MG_THREADS = 512;
+static_assert(MG_THREADS == 512, "the single-block sub-cycle maps its threads to an 8 x 8 x 8 cube");
 constexpr size_t MG_SMEM_MAX = 100 * 1024; // two resident blocks a SM
 
 template <typename T> struct MgArgs {
@@ -743,6 +744,7 @@ template <typename T> struct MgArgs {
     int nsmall; // first level of at most MG_SMALL_N points a side
     int n_pre, n_post, n_coarse;
     T w, scale;
+    T h2[MG_MAXLEV]; // (1 / (n - 1))^2 of each level, as k_gs_rb's caller computes it
     int iters; // cycles (mixed: defect-correction iterations) in this launch
     int mixed;
     Grid<double> fphi, frho; // FP64 fine grid (mixed form): phi[0] / rho[0] are ef / rf
@@ -781,6 +783,20 @@ struct Walk3 {
     }
 };
 
+// The red-black update of point (i, j, k) (k_gs_rb's arithmetic).
+template <typename T>
+__device__ __forceinline__ void mg_rb_point(const Grid<T> &phi, const Grid<T> &rho, int i, int j,
+                                            int k, T H2, T w)
+{
+    const T one_sixth = (T)(1.0 / 6.0);
+    const long gp = phi.off + i + j * phi.sy + k * phi.sz;
+    const long gr = rho.off + i + j * rho.sy + k * rho.sz;
+    T *p = phi.p;
+    T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
+                       p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
+    p[gp] = w * a + ((T)1.0 - w) * p[gp];
+}
+
 // One colour of a red-black sweep over work items t = tid, tid + nthr, ...
 template <typename T>
 __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rho, int color,
@@ -788,7 +804,6 @@ __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rh
 {
     const int m = phi.n - 2;
     const unsigned half = (unsigned)(m + 1) / 2;
-    const T one_sixth = (T)(1.0 / 6.0);
 #pragma unroll 4
     for (Walk3 x(tid, nthr, half, (unsigned)m); x.c < (unsigned)m; x.next())
     {
@@ -796,13 +811,53 @@ __device__ __forceinline__ void mg_rb_half(const Grid<T> &phi, const Grid<T> &rh
         const int i = ((((1 + j + k) & 1) == color) ? 1 : 2) + 2 * (int)x.a;
         if (i > m)
             continue;
-        const long gp = phi.off + i + j * phi.sy + k * phi.sz;
-        const long gr = rho.off + i + j * rho.sy + k * rho.sz;
-        T *p = phi.p;
-        T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
-                           p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
-        p[gp] = w * a + ((T)1.0 - w) * p[gp];
+        mg_rb_point(phi, rho, i, j, k, H2, w);
     }
+}
+
+// Block-level loops over the small grids of the single-block sub-cycle: the
+// block's MG_THREADS = 512 threads form an 8 x 8 x 8 cube and step through a
+// grid by 8 along each axis, with no index division.
+struct MgCube {
+    int x, y, z;
+};
+__device__ __forceinline__ MgCube mg_cube()
+{
+    const int t = (int)threadIdx.x;
+    return MgCube{t & 7, (t >> 3) & 7, t >> 6};
+}
+
+template <typename T>
+__device__ __forceinline__ void mg_rb_half_blk(const Grid<T> &phi, const Grid<T> &rho, int color,
+                                               T H2, T w)
+{
+    const int m = phi.n - 2, half = (m + 1) / 2;
+    const MgCube q = mg_cube();
+    for (int k = 1 + q.z; k <= m; k += 8)
+        for (int j = 1 + q.y; j <= m; j += 8)
+        {
+            const int i0 = (((1 + j + k) & 1) == color) ? 1 : 2;
+            for (int ti = q.x; ti < half; ti += 8)
+            {
+                const int i = i0 + 2 * ti;
+                if (i <= m)
+                    mg_rb_point(phi, rho, i, j, k, H2, w);
+            }
+        }
+}
+
+// rho_c at coarse point (lx, ly, lz) = scale * the residual at the injected fine point.
+template <typename T>
+__device__ __forceinline__ void mg_restrict_point(const Grid<T> &phi, const Grid<T> &rho,
+                                                  const Grid<T> &crho, T ooh2, T scale, int lx,
+                                                  int ly, int lz)
+{
+    const long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
+    const long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
+    const T *p = phi.p;
+    T rv = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
+                               p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
+    crho.p[crho.off + lx + ly * crho.sy + lz * crho.sz] = scale * rv;
 }
 
 // rho_c = scale * residual at the injected points; phi_c = 0 everywhere.
@@ -816,15 +871,24 @@ __device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &r
         cphi.p[cphi.off + (long)x.a + (long)x.b * cphi.sy + (long)x.c * cphi.sz] = (T)0;
     const unsigned mc = nc - 2;
     for (Walk3 x(tid, nthr, mc, mc); x.c < mc; x.next())
-    {
-        const int lx = 1 + (int)x.a, ly = 1 + (int)x.b, lz = 1 + (int)x.c;
-        const long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
-        const long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
-        const T *p = phi.p;
-        T rv = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
-                                   p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
-        crho.p[crho.off + lx + ly * crho.sy + lz * crho.sz] = scale * rv;
-    }
+        mg_restrict_point(phi, rho, crho, ooh2, scale, 1 + (int)x.a, 1 + (int)x.b, 1 + (int)x.c);
+}
+
+template <typename T>
+__device__ __forceinline__ void mg_restrict_blk(const Grid<T> &phi, const Grid<T> &rho,
+                                                const Grid<T> &cphi, const Grid<T> &crho, T ooh2,
+                                                T scale)
+{
+    const int nc = cphi.n, mc = nc - 2;
+    const MgCube q = mg_cube();
+    for (int k = q.z; k < nc; k += 8)
+        for (int j = q.y; j < nc; j += 8)
+            for (int i = q.x; i < nc; i += 8)
+                cphi.p[cphi.off + i + (long)j * cphi.sy + (long)k * cphi.sz] = (T)0;
+    for (int k = 1 + q.z; k <= mc; k += 8)
+        for (int j = 1 + q.y; j <= mc; j += 8)
+            for (int i = 1 + q.x; i <= mc; i += 8)
+                mg_restrict_point(phi, rho, crho, ooh2, scale, i, j, k);
 }
 
 // phi += the trilinear interpolation of the coarse correction c (k_prolong_add's
@@ -834,96 +898,112 @@ __device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &r
 // its terms in k_prolong_add's z, y, x order, skipping coarse points outside
 // 1..mc; a point even in all three coordinates takes its coarse value as is.
 template <typename T>
+__device__ __forceinline__ void mg_prolong_pair(const Grid<T> &phi, const Grid<T> &c, int mc, int a,
+                                                int j, int k)
+{
+    const int i0 = 2 * a + 1;
+    const bool second = a < mc; // i0 + 1 <= m
+    // y and z: coarse planes and their presence (odd: (j-1)/2 and (j+1)/2, even: j/2)
+    const bool jo = j & 1, ko = k & 1;
+    const int oy0 = jo ? (j - 1) >> 1 : j >> 1, oz0 = ko ? (k - 1) >> 1 : k >> 1;
+    bool vy[2], vz[2];
+    vy[0] = jo ? oy0 >= 1 : true;
+    vy[1] = jo && oy0 + 1 <= mc;
+    vz[0] = ko ? oz0 >= 1 : true;
+    vz[1] = ko && oz0 + 1 <= mc;
+    const bool vx0 = a >= 1, vx1 = a + 1 <= mc;
+    const T wy = jo ? (T)0.5 : (T)1, wz = ko ? (T)0.5 : (T)1;
+    const long cb = c.off + a + (long)oy0 * c.sy + (long)oz0 * c.sz;
+    T v[8]; // [z][y][x] with x = column a, a + 1
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+    {
+        const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
+        const bool ok = vz[az] && vy[ay] && (ax ? vx1 : vx0);
+        v[q] = ok ? c.p[cb + ax + (long)ay * c.sy + (long)az * c.sz] : (T)0;
+    }
+    const long f0 = phi.off + i0 + (long)j * phi.sy + (long)k * phi.sz;
+    const T p0 = phi.p[f0];
+    const T p1 = second ? phi.p[f0 + 1] : (T)0;
+    // odd point i0: x weight 1/2 on both columns
+    const T w0 = (T)0.5 * wy * wz;
+    T acc0 = (T)0;
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+    {
+        const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
+        if (vz[az] && vy[ay] && (ax ? vx1 : vx0))
+            acc0 += w0 * v[q];
+    }
+    phi.p[f0] = p0 + acc0;
+    if (second)
+    {
+        // even point i0 + 1: column a + 1 at x weight 1
+        T acc1;
+        if (!jo && !ko)
+            acc1 = v[1];
+        else
+        {
+            const T w1 = (T)1 * wy * wz;
+            acc1 = (T)0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+            {
+                const int az = q >> 1, ay = q & 1;
+                if (vz[az] && vy[ay])
+                    acc1 += w1 * v[2 * q + 1];
+            }
+        }
+        phi.p[f0 + 1] = p1 + acc1;
+    }
+}
+
+template <typename T>
 __device__ __forceinline__ void mg_prolong(const Grid<T> &phi, const Grid<T> &c, unsigned tid,
                                            unsigned nthr)
 {
     const int m = phi.n - 2, mc = c.n - 2;
     const unsigned um = (unsigned)m, pairs = (unsigned)mc + 1; // m = 2 mc + 1
     for (Walk3 x(tid, nthr, pairs, um); x.c < um; x.next())
-    {
-        const int a = (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
-        const int i0 = 2 * a + 1;
-        const bool second = a < mc; // i0 + 1 <= m
-        // y and z: coarse planes and their presence (odd: (j-1)/2 and (j+1)/2, even: j/2)
-        const bool jo = j & 1, ko = k & 1;
-        const int oy0 = jo ? (j - 1) >> 1 : j >> 1, oz0 = ko ? (k - 1) >> 1 : k >> 1;
-        bool vy[2], vz[2];
-        vy[0] = jo ? oy0 >= 1 : true;
-        vy[1] = jo && oy0 + 1 <= mc;
-        vz[0] = ko ? oz0 >= 1 : true;
-        vz[1] = ko && oz0 + 1 <= mc;
-        const bool vx0 = a >= 1, vx1 = a + 1 <= mc;
-        const T wy = jo ? (T)0.5 : (T)1, wz = ko ? (T)0.5 : (T)1;
-        const long cb = c.off + a + (long)oy0 * c.sy + (long)oz0 * c.sz;
-        T v[8]; // [z][y][x] with x = column a, a + 1
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-        {
-            const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
-            const bool ok = vz[az] && vy[ay] && (ax ? vx1 : vx0);
-            v[q] = ok ? c.p[cb + ax + (long)ay * c.sy + (long)az * c.sz] : (T)0;
-        }
-        const long f0 = phi.off + i0 + (long)j * phi.sy + (long)k * phi.sz;
-        const T p0 = phi.p[f0];
-        const T p1 = second ? phi.p[f0 + 1] : (T)0;
-        // odd point i0: x weight 1/2 on both columns
-        const T w0 = (T)0.5 * wy * wz;
-        T acc0 = (T)0;
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-        {
-            const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
-            if (vz[az] && vy[ay] && (ax ? vx1 : vx0))
-                acc0 += w0 * v[q];
-        }
-        phi.p[f0] = p0 + acc0;
-        if (second)
-        {
-            // even point i0 + 1: column a + 1 at x weight 1
-            T acc1;
-            if (!jo && !ko)
-                acc1 = v[1];
-            else
-            {
-                const T w1 = (T)1 * wy * wz;
-                acc1 = (T)0;
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                {
-                    const int az = q >> 1, ay = q & 1;
-                    if (vz[az] && vy[ay])
-                        acc1 += w1 * v[2 * q + 1];
-                }
-            }
-            phi.p[f0 + 1] = p1 + acc1;
-        }
-    }
+        mg_prolong_pair(phi, c, mc, (int)x.a, 1 + (int)x.b, 1 + (int)x.c);
 }
 
-template <typename T> __device__ __forceinline__ T mg_h2(int n)
+template <typename T>
+__device__ __forceinline__ void mg_prolong_blk(const Grid<T> &phi, const Grid<T> &c)
 {
-    return (T)((1.0 / (n - 1)) * (1.0 / (n - 1)));
+    const int m = phi.n - 2, mc = c.n - 2;
+    const MgCube q = mg_cube();
+    for (int k = 1 + q.z; k <= m; k += 8)
+        for (int j = 1 + q.y; j <= m; j += 8)
+            for (int a = q.x; a <= mc; a += 8)
+                mg_prolong_pair(phi, c, mc, a, j, k);
 }
 
-// Smoothing sweeps of level l; sync() separates the colours.
-template <typename T, typename Sync>
-__device__ __forceinline__ void mg_smooth_g(const Grid<T> &phi, const Grid<T> &rho, T w,
-                                            int sweeps, unsigned tid, unsigned nthr, Sync sync)
-{
-    const T H2 = mg_h2<T>(phi.n);
-    for (int it = 0; it < sweeps; it++)
-        for (int color = 0; color < 2; color++)
-        {
-            mg_rb_half(phi, rho, color, H2, w, tid, nthr);
-            sync();
-        }
-}
-
+// Smoothing sweeps of level l over the whole grid of threads; sync() separates
+// the colours.
 template <typename T, typename Sync>
 __device__ __forceinline__ void mg_smooth(const MgArgs<T> &A, int l, int sweeps, unsigned tid,
                                           unsigned nthr, Sync sync)
 {
-    mg_smooth_g(A.phi[l], A.rho[l], A.w, sweeps, tid, nthr, sync);
+    for (int it = 0; it < sweeps; it++)
+        for (int color = 0; color < 2; color++)
+        {
+            mg_rb_half(A.phi[l], A.rho[l], color, A.h2[l], A.w, tid, nthr);
+            sync();
+        }
+}
+
+// The same inside one block (grids of the single-block sub-cycle).
+template <typename T>
+__device__ __forceinline__ void mg_smooth_blk(const Grid<T> &phi, const Grid<T> &rho, T H2, T w,
+                                              int sweeps)
+{
+    for (int it = 0; it < sweeps; it++)
+        for (int color = 0; color < 2; color++)
+        {
+            mg_rb_half_blk(phi, rho, color, H2, w);
+            __syncthreads();
+        }
 }
 
 template <typename T> __device__ __forceinline__ Grid<T> mg_dense(T *p, int n)
@@ -964,7 +1044,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
     __shared__ int sh_ok;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
     auto gsync = [&]() { gbar_sync(A.bar, &sh_ok); };
-    auto bsync = [&]() { __syncthreads(); };
     for (int it = 0; it < A.iters; it++)
     {
         if (A.mixed)
@@ -1020,14 +1099,14 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             }
             for (int l = A.nsmall; l < A.nlev; l++)
             {
-                mg_smooth_g(P(l), R(l), A.w, A.n_pre, bt, bn, bsync);
+                mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_pre);
                 if (l == A.nlev - 1)
-                    mg_smooth_g(P(l), R(l), A.w, A.n_coarse, bt, bn, bsync);
+                    mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_coarse);
                 else
                 {
                     const int n = A.phi[l].n;
-                    mg_restrict(P(l), R(l), P(l + 1), R(l + 1), (T)(double)((n - 1) * (n - 1)),
-                                A.scale, bt, bn);
+                    mg_restrict_blk(P(l), R(l), P(l + 1), R(l + 1), (T)(double)((n - 1) * (n - 1)),
+                                    A.scale);
                     __syncthreads();
                 }
             }
@@ -1035,10 +1114,10 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             {
                 if (l < A.nlev - 1)
                 {
-                    mg_prolong(P(l), P(l + 1), bt, bn);
+                    mg_prolong_blk(P(l), P(l + 1));
                     __syncthreads();
                 }
-                mg_smooth_g(P(l), R(l), A.w, A.n_post, bt, bn, bsync);
+                mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_post);
             }
             if (A.smem)
                 mg_copy(P(A.nsmall), A.phi[A.nsmall], bt, bn);
@@ -1095,6 +1174,11 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     A.n_coarse = c.n_coarse;
     A.w = (T)c.w_sor;
     A.scale = (T)0.5; // red-black: half injection (see k_resid_restrict)
+    for (int l = 0; l < A.nlev; l++)
+    {
+        const int n = A.phi[l].n;
+        A.h2[l] = (T)((1.0 / (n - 1)) * (1.0 / (n - 1)));
+    }
     A.iters = iters;
     A.mixed = std::is_same<T, float>::value ? 1 : 0;
     A.fphi = s->fine_phi;
