@@ -954,14 +954,37 @@ __global__ void k_in_level(long n, const int *__restrict__ node_of, int *__restr
         flag[i] = node_of[i] >= 0 ? 1 : 0;
 }
 
-// One warp per occupied cell: CIC corner sums with the branch weights
-// (grid_density.c:166-245): w1 = x - H floor(x / H), w2 = H - w1, times
-// 4 pi G m / H^6; plus the cell's mass.
+// CIC corner sums with the branch weights (grid_density.c:166-245):
+// w1 = x - H floor(x / H), w2 = H - w1, times 4 pi G m / H^6; plus the mass.
+__device__ __forceinline__ void lvl_cic_add(int i, double H, double ooh, double coeff,
+                                            const double *__restrict__ x,
+                                            const double *__restrict__ y,
+                                            const double *__restrict__ z,
+                                            const double *__restrict__ m, double acc[9])
+{
+    int fx = (int)(x[i] * ooh), fy = (int)(y[i] * ooh), fz = (int)(z[i] * ooh);
+    double wx1 = x[i] - H * fx, wy1 = y[i] - H * fy, wz1 = z[i] - H * fz;
+    double wx2 = H - wx1, wy2 = H - wy1, wz2 = H - wz1;
+    double cm = coeff * m[i];
+    acc[0] += cm * (wx2 * wy2 * wz2);
+    acc[1] += cm * (wx1 * wy2 * wz2);
+    acc[2] += cm * (wx2 * wy1 * wz2);
+    acc[3] += cm * (wx1 * wy1 * wz2);
+    acc[4] += cm * (wx2 * wy2 * wz1);
+    acc[5] += cm * (wx1 * wy2 * wz1);
+    acc[6] += cm * (wx2 * wy1 * wz1);
+    acc[7] += cm * (wx1 * wy1 * wz1);
+    acc[8] += m[i];
+}
+
+// One warp per occupied cell of at most SEG_LONG particles (longer cells are
+// listed for k_lvl_seg_long): the corner sums and the cell's mass.
 __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ perm,
-                                 const int *__restrict__ seg_start, const int *__restrict__ flags,
-                                 const double *__restrict__ x, const double *__restrict__ y,
-                                 const double *__restrict__ z, const double *__restrict__ m,
-                                 double *__restrict__ cs, double *__restrict__ smass)
+                                 const int *__restrict__ seg_start, int *__restrict__ flags,
+                                 int *__restrict__ long_list, const double *__restrict__ x,
+                                 const double *__restrict__ y, const double *__restrict__ z,
+                                 const double *__restrict__ m, double *__restrict__ cs,
+                                 double *__restrict__ smass)
 {
     const int lane = threadIdx.x & 31;
     const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -972,27 +995,18 @@ __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ p
     for (long sg = warp0; sg < nseg; sg += nwarps)
     {
         const int b = seg_start[sg], e = seg_start[sg + 1];
+        if (e - b > SEG_LONG)
+        {
+            if (lane == 0)
+                long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+            continue;
+        }
         double acc[9];
 #pragma unroll
         for (int c = 0; c < 9; c++)
             acc[c] = 0.0;
         for (int q = b + lane; q < e; q += 32)
-        {
-            const int i = perm[q];
-            int fx = (int)(x[i] * ooh), fy = (int)(y[i] * ooh), fz = (int)(z[i] * ooh);
-            double wx1 = x[i] - H * fx, wy1 = y[i] - H * fy, wz1 = z[i] - H * fz;
-            double wx2 = H - wx1, wy2 = H - wy1, wz2 = H - wz1;
-            double cm = coeff * m[i];
-            acc[0] += cm * (wx2 * wy2 * wz2);
-            acc[1] += cm * (wx1 * wy2 * wz2);
-            acc[2] += cm * (wx2 * wy1 * wz2);
-            acc[3] += cm * (wx1 * wy1 * wz2);
-            acc[4] += cm * (wx2 * wy2 * wz1);
-            acc[5] += cm * (wx1 * wy2 * wz1);
-            acc[6] += cm * (wx2 * wy1 * wz1);
-            acc[7] += cm * (wx1 * wy1 * wz1);
-            acc[8] += m[i];
-        }
+            lvl_cic_add(perm[q], H, ooh, coeff, x, y, z, m, acc);
 #pragma unroll
         for (int c = 0; c < 9; c++)
         {
@@ -1012,6 +1026,51 @@ __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ p
         }
         if (lane == 0)
             smass[sg] = acc[8];
+    }
+}
+
+// One block per listed cell of more than SEG_LONG particles (as k_seg_long).
+__global__ void __launch_bounds__(SEG_LONG_THREADS)
+    k_lvl_seg_long(int lv, double coeff, const int *__restrict__ perm,
+                   const int *__restrict__ seg_start, const int *__restrict__ flags,
+                   const int *__restrict__ long_list, const double *__restrict__ x,
+                   const double *__restrict__ y, const double *__restrict__ z,
+                   const double *__restrict__ m, double *__restrict__ cs,
+                   double *__restrict__ smass)
+{
+    __shared__ double shw[(SEG_LONG_THREADS / 32) * 9];
+    const int nl = flags[F_NLONG];
+    const double H = 1.0 / (1 << lv);
+    const double ooh = (double)(1 << lv);
+    const int bs = (int)blockDim.x;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x)
+    {
+        const int sg = long_list[li];
+        const int b = seg_start[sg], e = seg_start[sg + 1];
+        double acc[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++)
+            acc[c] = 0.0;
+        for (int q0 = b + (int)threadIdx.x; q0 < e; q0 += 4 * bs)
+        {
+            int iq[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+            {
+                const int q = q0 + u * bs;
+                iq[u] = q < e ? perm[q] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (iq[u] >= 0)
+                    lvl_cic_add(iq[u], H, ooh, coeff, x, y, z, m, acc);
+        }
+        seg_block_sums<9>(acc, shw);
+        if (threadIdx.x < 8)
+            cs[(long)sg * 8 + threadIdx.x] = acc[0];
+        else if (threadIdx.x == 8)
+            smass[sg] = acc[0];
+        __syncthreads(); // shw is rewritten for the next cell
     }
 }
 
@@ -1164,9 +1223,13 @@ int amr_deposit(qz_sim *s)
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
         long blocks = std::min((m * 32 + 255) / 256 + 1, (long)sms * 16);
+        cudaMemsetAsync(s->flags + F_NLONG, 0, sizeof(int), s->stream);
         launch(s, QZ_PROF_DEPOSIT, 40.0 * m, k_lvl_seg_reduce, dim3((int)blocks), dim3(256),
-               L.h[0].lv, coeff, perm, s->seg_start, s->flags, s->x, s->y, s->z, s->m,
-               s->cell_sums, s->seg_mass.p);
+               L.h[0].lv, coeff, perm, s->seg_start, s->flags, s->long_seg, s->x, s->y, s->z,
+               s->m, s->cell_sums, s->seg_mass.p);
+        launch(s, QZ_PROF_DEPOSIT, 0.0, k_lvl_seg_long, dim3(sms), dim3(SEG_LONG_THREADS),
+               L.h[0].lv, coeff, perm, s->seg_start, s->flags, s->long_seg, s->x, s->y, s->z,
+               s->m, s->cell_sums, s->seg_mass.p);
         launch(s, QZ_PROF_DEPOSIT, 12.0 * L.grid_total, k_lvl_point_gather,
                dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, L.nnodes, L.nodes.p,
                L.cell_seg.p, s->cell_sums, L.d);

@@ -370,7 +370,7 @@ int qz_destroy(qz_sim *s)
                     s->pot, s->pot_old, s->d, s->gax, s->gay, s->gaz, s->sort.k0, s->sort.k1,
                     s->sort.v0, s->sort.v1, s->sort.hist, s->seg_head, s->seg_id, s->seg_start,
                     s->seg_cell, s->cell_seg, s->cell_sums, s->red, s->flags, s->d_ts,
-                    s->gbar};
+                    s->gbar, s->long_seg};
     for (void *p : ptrs)
         dfree(p);
     free_levels(s);
@@ -482,7 +482,8 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
          dmalloc(&s->sort.hist, 256 * tiles, "hist");
     ok = ok && dmalloc(&s->seg_head, cap, "seg") && dmalloc(&s->seg_id, cap, "seg") &&
          dmalloc(&s->seg_start, cap + 1, "seg") && dmalloc(&s->seg_cell, cap, "seg") &&
-         dmalloc(&s->cell_seg, B * B * B, "cell_seg") && dmalloc(&s->cell_sums, 8 * cap, "cs");
+         dmalloc(&s->cell_seg, B * B * B, "cell_seg") && dmalloc(&s->cell_sums, 8 * cap, "cs") &&
+         dmalloc(&s->long_seg, cap / SEG_LONG + 2, "long segments");
     s->red_blocks = 296;
     ok = ok && dmalloc(&s->red, s->red_blocks + 8, "red") && dmalloc(&s->flags, F_COUNT, "flags");
     ok = ok && check_cuda(cudaMallocHost((void **)&s->h_flags, F_COUNT * sizeof(int)), "pinned");

@@ -42,6 +42,46 @@ struct Level {
     float *cgrf = nullptr, *cgpf = nullptr, *cgaf = nullptr;
 };
 
+// Deposit segments (occupied cells) of more than SEG_LONG particles are reduced
+// by a whole block each instead of one warp: the densest cells of a centrally
+// concentrated system hold thousands of particles, and one warp walking them
+// would set the length of the deposit.
+constexpr int SEG_LONG = 256;
+constexpr int SEG_LONG_THREADS = 1024;
+
+#ifdef __CUDACC__
+// Block-wide sums of acc[0..NV): xor-shuffle trees in each warp, then the warps'
+// values added in warp order by thread c < NV, which receives sum c in acc[0]
+// (a fixed order: the same inputs give the same bits).  shw holds
+// (blockDim / 32) * NV doubles; the caller syncs before reusing it.
+template <int NV> __device__ __forceinline__ void seg_block_sums(double (&acc)[NV], double *shw)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+    {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[c] = v;
+    }
+    if (lane == 0)
+    {
+#pragma unroll
+        for (int c = 0; c < NV; c++)
+            shw[w * NV + c] = acc[c];
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < NV)
+    {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++)
+            t += shw[k * NV + threadIdx.x];
+        acc[0] = t;
+    }
+}
+#endif
+
 // Device-side flag words (int).
 enum Flag {
     F_RATIO_FAIL = 0, // ratio test |phi/phi_old - 1| > tol2 somewhere
@@ -50,6 +90,7 @@ enum Flag {
     F_NSEG = 3,       // number of occupied cells (deposit segments)
     F_RESID_FAIL = 4, // method-1 pointwise residual failure
     F_AMR_CONV = 5,   // refinement nodes converged in the current level solve
+    F_NLONG = 6,      // deposit segments longer than SEG_LONG (listed in long_seg)
     F_COUNT = 8
 };
 enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2, E_BARRIER = 8 };
@@ -295,6 +336,7 @@ struct qz_sim {
     int *seg_id = nullptr;    // n: exclusive scan of seg_head
     int *seg_start = nullptr; // n + 1
     int *seg_cell = nullptr;  // n
+    int *long_seg = nullptr;  // capacity / SEG_LONG + 2: deposit segments left to k_seg_long
     int *cell_seg = nullptr;  // B^3 cells: segment of the cell or -1
     double *cell_sums = nullptr; // 8 * n
     int *scan_tmp = nullptr;

@@ -252,11 +252,35 @@ __global__ void k_seg_fill(long n, const unsigned *__restrict__ k, const int *__
 
 // One warp per occupied cell: the 8 CIC corner sums of coeff * m * w over the
 // cell's particles (lane-strided partial sums, then a fixed xor-shuffle tree).
+// Particle i's CIC corner weights times 4 pi G m / H^3, added to acc.
+__device__ __forceinline__ void head_cic_add(int i, double scale, double coeff,
+                                             const double *__restrict__ x,
+                                             const double *__restrict__ y,
+                                             const double *__restrict__ z,
+                                             const double *__restrict__ m, double acc[8])
+{
+    double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
+    int fx = (int)px, fy = (int)py, fz = (int)pz;
+    double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+    double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+    double cm = coeff * m[i];
+    acc[0] += cm * (wx2 * wy2 * wz2);
+    acc[1] += cm * (wx1 * wy2 * wz2);
+    acc[2] += cm * (wx2 * wy1 * wz2);
+    acc[3] += cm * (wx1 * wy1 * wz2);
+    acc[4] += cm * (wx2 * wy2 * wz1);
+    acc[5] += cm * (wx1 * wy2 * wz1);
+    acc[6] += cm * (wx2 * wy1 * wz1);
+    acc[7] += cm * (wx1 * wy1 * wz1);
+}
+
+// One warp per occupied cell of at most SEG_LONG particles; longer cells are
+// listed for k_seg_long.
 __global__ void k_seg_reduce(int L, double coeff, const int *__restrict__ perm,
-                             const int *__restrict__ seg_start, const int *__restrict__ flags,
-                             const double *__restrict__ x, const double *__restrict__ y,
-                             const double *__restrict__ z, const double *__restrict__ m,
-                             double *__restrict__ cs)
+                             const int *__restrict__ seg_start, int *__restrict__ flags,
+                             int *__restrict__ long_list, const double *__restrict__ x,
+                             const double *__restrict__ y, const double *__restrict__ z,
+                             const double *__restrict__ m, double *__restrict__ cs)
 {
     const int lane = threadIdx.x & 31;
     const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -266,27 +290,18 @@ __global__ void k_seg_reduce(int L, double coeff, const int *__restrict__ perm,
     for (long sg = warp0; sg < nseg; sg += nwarps)
     {
         const int b = seg_start[sg], e = seg_start[sg + 1];
+        if (e - b > SEG_LONG)
+        {
+            if (lane == 0)
+                long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+            continue;
+        }
         double acc[8];
 #pragma unroll
         for (int c = 0; c < 8; c++)
             acc[c] = 0.0;
         for (int q = b + lane; q < e; q += 32)
-        {
-            const int i = perm[q];
-            double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
-            int fx = (int)px, fy = (int)py, fz = (int)pz;
-            double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
-            double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
-            double cm = coeff * m[i];
-            acc[0] += cm * (wx2 * wy2 * wz2);
-            acc[1] += cm * (wx1 * wy2 * wz2);
-            acc[2] += cm * (wx2 * wy1 * wz2);
-            acc[3] += cm * (wx1 * wy1 * wz2);
-            acc[4] += cm * (wx2 * wy2 * wz1);
-            acc[5] += cm * (wx1 * wy2 * wz1);
-            acc[6] += cm * (wx2 * wy1 * wz1);
-            acc[7] += cm * (wx1 * wy1 * wz1);
-        }
+            head_cic_add(perm[q], scale, coeff, x, y, z, m, acc);
 #pragma unroll
         for (int c = 0; c < 8; c++)
         {
@@ -304,6 +319,50 @@ __global__ void k_seg_reduce(int L, double coeff, const int *__restrict__ perm,
                     v = acc[c];
             cs[sg * 8 + lane] = v;
         }
+    }
+}
+
+// One block per occupied cell listed by k_seg_reduce (more than SEG_LONG
+// particles): thread t adds particles t, t + blockDim, ... of the cell (four at
+// a time, their loads together), then the block sums in a fixed order, so the
+// result does not depend on scheduling.
+__global__ void __launch_bounds__(SEG_LONG_THREADS)
+    k_seg_long(int L, double coeff, const int *__restrict__ perm,
+               const int *__restrict__ seg_start, const int *__restrict__ flags,
+               const int *__restrict__ long_list, const double *__restrict__ x,
+               const double *__restrict__ y, const double *__restrict__ z,
+               const double *__restrict__ m, double *__restrict__ cs)
+{
+    __shared__ double shw[(SEG_LONG_THREADS / 32) * 8];
+    const int nl = flags[F_NLONG];
+    const double scale = (double)(1 << L);
+    const int bs = (int)blockDim.x;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x)
+    {
+        const int sg = long_list[li];
+        const int b = seg_start[sg], e = seg_start[sg + 1];
+        double acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            acc[c] = 0.0;
+        for (int q0 = b + (int)threadIdx.x; q0 < e; q0 += 4 * bs)
+        {
+            int iq[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+            {
+                const int q = q0 + u * bs;
+                iq[u] = q < e ? perm[q] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (iq[u] >= 0)
+                    head_cic_add(iq[u], scale, coeff, x, y, z, m, acc);
+        }
+        seg_block_sums<8>(acc, shw);
+        if (threadIdx.x < 8)
+            cs[(long)sg * 8 + threadIdx.x] = acc[0];
+        __syncthreads(); // shw is rewritten for the next cell
     }
 }
 
@@ -405,7 +464,11 @@ int deposit_head(qz_sim *s)
     long max_blocks = (long)sms * 16;
     if (blocks > max_blocks)
         blocks = max_blocks;
-    launch(s, QZ_PROF_DEPOSIT, 36.0 * n, k_seg_reduce, dim3((int)blocks), dim3(256), L, coeff, perm, s->seg_start, s->flags, s->x, s->y, s->z, s->m, s->cell_sums);
+    cudaMemsetAsync(s->flags + F_NLONG, 0, sizeof(int), s->stream);
+    launch(s, QZ_PROF_DEPOSIT, 36.0 * n, k_seg_reduce, dim3((int)blocks), dim3(256), L, coeff, perm,
+           s->seg_start, s->flags, s->long_seg, s->x, s->y, s->z, s->m, s->cell_sums);
+    launch(s, QZ_PROF_DEPOSIT, 0.0, k_seg_long, dim3(sms), dim3(SEG_LONG_THREADS), L, coeff, perm,
+           s->seg_start, s->flags, s->long_seg, s->x, s->y, s->z, s->m, s->cell_sums);
     launch(s, QZ_PROF_DEPOSIT, 12.0 * s->gpts, k_point_gather, dim3(blocks_for(s->gpts, 256)), dim3(256), L, s->D, s->cell_seg, s->cell_sums, s->d);
     return check_cuda(cudaGetLastError(), "deposit") ? QZ_SUCCESS : QZ_FAILURE;
 }
