@@ -119,15 +119,48 @@ __global__ void k_adj_final(int nb, const double *__restrict__ partial, double s
 }
 
 // ---- deposit of a-bar (gather transpose) ------------------------------------------------
-// One warp per occupied head cell: for each of the 8 corners the sums of
-// w * abar over the cell's particles, three components.  cs: segment * 24 +
-// component * 8 + corner.
+// Particle i's CIC corner weights times its a-bar, three components, added to
+// acc (component * 8 + corner).
+__device__ __forceinline__ void adj_cic_add(int i, double scale, const double *__restrict__ x,
+                                            const double *__restrict__ y,
+                                            const double *__restrict__ z,
+                                            const double *__restrict__ abx,
+                                            const double *__restrict__ aby,
+                                            const double *__restrict__ abz, double acc[24])
+{
+    double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
+    int fx = (int)px, fy = (int)py, fz = (int)pz;
+    double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
+    double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
+    double w[8];
+    w[0] = wx2 * wy2 * wz2;
+    w[1] = wx1 * wy2 * wz2;
+    w[2] = wx2 * wy1 * wz2;
+    w[3] = wx1 * wy1 * wz2;
+    w[4] = wx2 * wy2 * wz1;
+    w[5] = wx1 * wy2 * wz1;
+    w[6] = wx2 * wy1 * wz1;
+    w[7] = wx1 * wy1 * wz1;
+    const double a0 = abx[i], a1 = aby[i], a2 = abz[i];
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+    {
+        acc[c] += a0 * w[c];
+        acc[8 + c] += a1 * w[c];
+        acc[16 + c] += a2 * w[c];
+    }
+}
+
+// One warp per occupied cell of at most SEG_LONG particles (longer cells are
+// listed for k_adj_seg_long): for each of the 8 corners the sums of w * abar
+// over the cell's particles, three components.  cs: segment * 24 + component *
+// 8 + corner.
 __global__ void k_adj_seg_reduce(int L, const int *__restrict__ perm,
-                                 const int *__restrict__ seg_start, const int *__restrict__ flags,
-                                 const double *__restrict__ x, const double *__restrict__ y,
-                                 const double *__restrict__ z, const double *__restrict__ abx,
-                                 const double *__restrict__ aby, const double *__restrict__ abz,
-                                 double *__restrict__ cs)
+                                 const int *__restrict__ seg_start, int *__restrict__ flags,
+                                 int *__restrict__ long_list, const double *__restrict__ x,
+                                 const double *__restrict__ y, const double *__restrict__ z,
+                                 const double *__restrict__ abx, const double *__restrict__ aby,
+                                 const double *__restrict__ abz, double *__restrict__ cs)
 {
     const int lane = threadIdx.x & 31;
     const long warp0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -137,35 +170,18 @@ __global__ void k_adj_seg_reduce(int L, const int *__restrict__ perm,
     for (long sg = warp0; sg < nseg; sg += nwarps)
     {
         const int b = seg_start[sg], e = seg_start[sg + 1];
+        if (e - b > SEG_LONG)
+        {
+            if (lane == 0)
+                long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+            continue;
+        }
         double acc[24];
 #pragma unroll
         for (int c = 0; c < 24; c++)
             acc[c] = 0.0;
         for (int q = b + lane; q < e; q += 32)
-        {
-            const int i = perm[q];
-            double px = x[i] * scale, py = y[i] * scale, pz = z[i] * scale;
-            int fx = (int)px, fy = (int)py, fz = (int)pz;
-            double wx1 = px - fx, wy1 = py - fy, wz1 = pz - fz;
-            double wx2 = 1.0 - wx1, wy2 = 1.0 - wy1, wz2 = 1.0 - wz1;
-            double w[8];
-            w[0] = wx2 * wy2 * wz2;
-            w[1] = wx1 * wy2 * wz2;
-            w[2] = wx2 * wy1 * wz2;
-            w[3] = wx1 * wy1 * wz2;
-            w[4] = wx2 * wy2 * wz1;
-            w[5] = wx1 * wy2 * wz1;
-            w[6] = wx2 * wy1 * wz1;
-            w[7] = wx1 * wy1 * wz1;
-            const double a0 = abx[i], a1 = aby[i], a2 = abz[i];
-#pragma unroll
-            for (int c = 0; c < 8; c++)
-            {
-                acc[c] += a0 * w[c];
-                acc[8 + c] += a1 * w[c];
-                acc[16 + c] += a2 * w[c];
-            }
-        }
+            adj_cic_add(perm[q], scale, x, y, z, abx, aby, abz, acc);
 #pragma unroll
         for (int c = 0; c < 24; c++)
         {
@@ -183,6 +199,45 @@ __global__ void k_adj_seg_reduce(int L, const int *__restrict__ perm,
                     v = acc[c];
             cs[sg * 24 + lane] = v;
         }
+    }
+}
+
+// One block per listed cell of more than SEG_LONG particles: thread t adds
+// particles t, t + blockDim, ... (two at a time), then block sums in a fixed
+// order.  512 threads: the 24 sums a thread need more than 64 registers.
+constexpr int ADJ_SEG_LONG_THREADS = 512;
+__global__ void __launch_bounds__(ADJ_SEG_LONG_THREADS)
+    k_adj_seg_long(int L, const int *__restrict__ perm, const int *__restrict__ seg_start,
+                   const int *__restrict__ flags, const int *__restrict__ long_list,
+                   const double *__restrict__ x, const double *__restrict__ y,
+                   const double *__restrict__ z, const double *__restrict__ abx,
+                   const double *__restrict__ aby, const double *__restrict__ abz,
+                   double *__restrict__ cs)
+{
+    __shared__ double shw[(ADJ_SEG_LONG_THREADS / 32) * 24];
+    const int nl = flags[F_NLONG];
+    const double scale = (double)(1 << L);
+    const int bs = (int)blockDim.x;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x)
+    {
+        const int sg = long_list[li];
+        const int b = seg_start[sg], e = seg_start[sg + 1];
+        double acc[24];
+#pragma unroll
+        for (int c = 0; c < 24; c++)
+            acc[c] = 0.0;
+        for (int q0 = b + (int)threadIdx.x; q0 < e; q0 += 2 * bs)
+        {
+            const int q1 = q0 + bs;
+            const int i0 = perm[q0], i1 = q1 < e ? perm[q1] : -1;
+            adj_cic_add(i0, scale, x, y, z, abx, aby, abz, acc);
+            if (i1 >= 0)
+                adj_cic_add(i1, scale, x, y, z, abx, aby, abz, acc);
+        }
+        seg_block_sums<24>(acc, shw);
+        if (threadIdx.x < 24)
+            cs[(long)sg * 24 + threadIdx.x] = acc[0];
+        __syncthreads(); // shw is rewritten for the next cell
     }
 }
 
@@ -1007,8 +1062,12 @@ static int adj_level_deposit(qz_sim *s, int l, const double *x, const double *y,
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     const long blocks = std::min((m * 32 + 255) / 256, (long)sms * 16);
+    cudaMemsetAsync(s->flags + F_NLONG, 0, sizeof(int), s->stream);
     launch(s, QZ_PROF_DEPOSIT, 56.0 * m, k_adj_seg_reduce, dim3((int)blocks), dim3(256),
-           L.h[0].lv, perm, s->seg_start, s->flags, x, y, z, ab, ab + n, ab + 2 * n, A.cs.p);
+           L.h[0].lv, perm, s->seg_start, s->flags, s->long_seg, x, y, z, ab, ab + n, ab + 2 * n,
+           A.cs.p);
+    launch(s, QZ_PROF_DEPOSIT, 0.0, k_adj_seg_long, dim3(2 * sms), dim3(ADJ_SEG_LONG_THREADS), L.h[0].lv,
+           perm, s->seg_start, s->flags, s->long_seg, x, y, z, ab, ab + n, ab + 2 * n, A.cs.p);
     launch(s, QZ_PROF_DEPOSIT, 24.0 * L.grid_total, k_adj_lvl_point_gather3,
            dim3(blocks_for(L.grid_total, 256)), dim3(256), L.grid_total, L.nnodes, L.nodes.p,
            L.cell_seg.p, A.cs.p, A0, A1, A2);
@@ -1063,8 +1122,11 @@ static int force_vjp(qz_sim *s, const double *x, const double *y, const double *
     const long blocks = std::min((n * 32 + 255) / 256, (long)sms * 16);
     if (!A.cs.ensure(s->mem, 24 * n + 24))
         return QZ_FAILURE;
+    cudaMemsetAsync(s->flags + F_NLONG, 0, sizeof(int), s->stream);
     launch(s, QZ_PROF_DEPOSIT, 56.0 * n, k_adj_seg_reduce, dim3((int)blocks), dim3(256), L, perm,
-           s->seg_start, s->flags, x, y, z, abh, abh + n, abh + 2 * n, A.cs.p);
+           s->seg_start, s->flags, s->long_seg, x, y, z, abh, abh + n, abh + 2 * n, A.cs.p);
+    launch(s, QZ_PROF_DEPOSIT, 0.0, k_adj_seg_long, dim3(2 * sms), dim3(ADJ_SEG_LONG_THREADS), L, perm,
+           s->seg_start, s->flags, s->long_seg, x, y, z, abh, abh + n, abh + 2 * n, A.cs.p);
     double *Abx = A.Ab.p, *Aby = A.Ab.p + s->gpts, *Abz = A.Ab.p + 2 * s->gpts;
     launch(s, QZ_PROF_DEPOSIT, 24.0 * s->gpts, k_adj_point_gather, dim3(blocks_for(s->gpts, 256)),
            dim3(256), D, s->cell_seg, A.cs.p, Abx, Aby, Abz);

@@ -266,6 +266,8 @@ int check_flags(qz_sim *s)
         cudaMemsetAsync(s->flags + F_ERROR, 0, sizeof(int), s->stream);
         if (e & E_BARRIER)
             set_error("a grid barrier wait in a cooperative kernel gave up (flags 0x%x)", e);
+        else if (e & E_SCAN)
+            set_error("a scan's wait for a preceding tile gave up (flags 0x%x)", e);
         else
             set_error("device bounds check failed (flags 0x%x): a particle left the unit box", e);
         return QZ_FAILURE;
@@ -379,7 +381,7 @@ int qz_destroy(qz_sim *s)
     s->ofl_state.release(s->mem);
     s->ofl_int.release(s->mem);
     if (s->mem.pool)
-        pool_free(s->mem, s->scan_tmp);
+        pool_free(s->mem, s->scan_st);
     if (s->stream)
         cudaStreamSynchronize(s->stream); // the pool frees are stream-ordered
     if (s->mem.pool)

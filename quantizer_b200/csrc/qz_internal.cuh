@@ -93,7 +93,7 @@ enum Flag {
     F_NLONG = 6,      // deposit segments longer than SEG_LONG (listed in long_seg)
     F_COUNT = 8
 };
-enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2, E_BARRIER = 8 };
+enum ErrorBits { E_PTCL_OUTSIDE = 1, E_SORT_RANGE = 2, E_BARRIER = 8, E_SCAN = 16 };
 
 // Grid-wide barrier of a cooperative launch with bounded waits.  word[0]
 // counts arrivals, word[2] is the generation and word[3] is set once a wait of
@@ -339,8 +339,13 @@ struct qz_sim {
     int *long_seg = nullptr;  // capacity / SEG_LONG + 2: deposit segments left to k_seg_long
     int *cell_seg = nullptr;  // B^3 cells: segment of the cell or -1
     double *cell_sums = nullptr; // 8 * n
-    int *scan_tmp = nullptr;
-    long scan_tmp_cap = 0;
+    // single-pass scan: per-tile status words (tagged with the call's epoch) and,
+    // after them, the tile counter; the host keeps the counter's value at the
+    // start of the next call (scan_base) and the epoch
+    unsigned long long *scan_st = nullptr;
+    long scan_st_cap = 0;
+    unsigned long long scan_base = 0;
+    unsigned scan_epoch = 0;
 
     double *red = nullptr; // reduction partials
     int red_blocks = 0;

@@ -135,20 +135,6 @@ __device__ __forceinline__ int block_excl_scan(int v, int *sh, int *total)
     return wprefix + x - v;
 }
 
-__global__ void k_scan_tiles(const int *__restrict__ in, long n, int *__restrict__ tile_sums)
-{
-    __shared__ int sh[32];
-    long base = (long)blockIdx.x * SC_TILE + (long)threadIdx.x * SC_ITEMS;
-    int s = 0;
-    for (int q = 0; q < SC_ITEMS; q++)
-        if (base + q < n)
-            s += in[base + q];
-    int total;
-    block_excl_scan(s, sh, &total);
-    if (threadIdx.x == 0)
-        tile_sums[blockIdx.x] = total;
-}
-
 // Single block: exclusive scan of m values in place (m may exceed the block).
 __global__ void k_scan_single(int *__restrict__ a, long m)
 {
@@ -178,49 +164,124 @@ __global__ void k_scan_single(int *__restrict__ a, long m)
     }
 }
 
-// in and out may be the same array (each block reads its tile before writing it)
-__global__ void k_scan_apply(const int *in, int *out, long n, const int *__restrict__ tile_offsets)
+// Single-pass exclusive scan (decoupled look-back, Merrill and Garland 2016).
+// A block takes the next tile number from a counter (arrival order: every
+// tile before it belongs to a block that is already running, so a wait always
+// ends), scans its tile, publishes the tile's sum in its status word, then adds
+// the published values of the tiles before it, walking back until one holds an
+// inclusive prefix, and publishes its own inclusive prefix.  A status word is
+// flag (2 bits: 1 = tile sum, 2 = inclusive prefix) | epoch (30 bits) | value
+// (32 bits): one word, so a reader sees a flag and its value together; words of
+// an earlier call carry an older epoch and read as not yet published.  Integer
+// sums: the result does not depend on the order of arrival.  A wait gives up
+// after SCAN_POLL_LIMIT polls and sets E_SCAN in flags[F_ERROR].
+constexpr long SCAN_POLL_LIMIT = 1L << 22;
+
+__device__ __forceinline__ unsigned long long scan_ld(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void scan_st(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(SC_THREADS)
+    k_scan_lookback(const int *in, int *out, long n, unsigned long long *__restrict__ st,
+                    unsigned long long *__restrict__ ctr, unsigned long long base,
+                    unsigned epoch, int *__restrict__ flags)
 {
     __shared__ int sh[32];
-    long base = (long)blockIdx.x * SC_TILE + (long)threadIdx.x * SC_ITEMS;
+    __shared__ long s_tile;
+    __shared__ int s_prefix;
+    if (threadIdx.x == 0)
+        s_tile = (long)(atomicAdd(ctr, 1ull) - base);
+    __syncthreads();
+    const long tile = s_tile;
+    const long i0 = tile * SC_TILE + (long)threadIdx.x * SC_ITEMS;
     int v[SC_ITEMS];
-    int s = 0;
+    int sum = 0;
     for (int q = 0; q < SC_ITEMS; q++)
     {
-        v[q] = (base + q < n) ? in[base + q] : 0;
-        s += v[q];
+        v[q] = (i0 + q < n) ? in[i0 + q] : 0;
+        sum += v[q];
     }
-    int ex = block_excl_scan(s, sh, nullptr);
-    int run = tile_offsets[blockIdx.x] + ex;
+    int total;
+    const int ex = block_excl_scan(sum, sh, &total);
+    if (threadIdx.x == 0)
+    {
+        const unsigned long long tag = (unsigned long long)epoch << 32;
+        int prefix = 0;
+        if (tile > 0)
+        {
+            scan_st(&st[tile], (1ull << 62) | tag | (unsigned)total);
+            long polls = 0;
+            for (long j = tile - 1; j >= 0;)
+            {
+                const unsigned long long w = scan_ld(&st[j]);
+                const unsigned fl = (unsigned)(w >> 62);
+                if (fl == 0 || (unsigned)((w >> 32) & 0x3fffffffu) != epoch)
+                {
+                    if (++polls > SCAN_POLL_LIMIT)
+                    {
+                        atomicOr(&flags[F_ERROR], E_SCAN);
+                        break;
+                    }
+                    continue;
+                }
+                prefix += (int)(unsigned)w;
+                if (fl == 2)
+                    break;
+                j--;
+            }
+        }
+        scan_st(&st[tile], (2ull << 62) | tag | (unsigned)(prefix + total));
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    int run = s_prefix + ex;
     for (int q = 0; q < SC_ITEMS; q++)
     {
-        if (base + q < n)
-            out[base + q] = run;
+        if (i0 + q < n)
+            out[i0 + q] = run;
         run += v[q];
     }
 }
 
+// in and out may be the same array (each block reads its tile before writing it)
 int scan_exclusive(qz_sim *s, const int *in, int *out, long n)
 {
     if (n <= 0)
         return QZ_SUCCESS;
-    long tiles = (n + SC_TILE - 1) / SC_TILE;
-    if (s->scan_tmp_cap < tiles)
+    const long tiles = (n + SC_TILE - 1) / SC_TILE;
+    if (s->scan_st_cap < tiles)
     {
-        pool_free(s->mem, s->scan_tmp);
-        s->scan_tmp = nullptr;
-        s->scan_tmp_cap = 0;
+        // status words and the counter start at zero (epoch 0 is never used)
+        pool_free(s->mem, s->scan_st);
+        s->scan_st = nullptr;
+        s->scan_st_cap = 0;
         const long cap = tiles + tiles / 2 + 64;
-        if (!pool_alloc(s->mem, &s->scan_tmp, cap))
+        if (!pool_alloc(s->mem, &s->scan_st, cap + 1))
         {
-            set_error("scan scratch: out of device memory");
+            set_error("scan status words: out of device memory");
             return QZ_FAILURE;
         }
-        s->scan_tmp_cap = cap;
+        cudaMemsetAsync(s->scan_st, 0, (cap + 1) * sizeof(unsigned long long), s->stream);
+        s->scan_st_cap = cap;
+        s->scan_base = 0;
     }
-    launch(s, QZ_PROF_SORT, 4.0 * n, k_scan_tiles, dim3((int)tiles), dim3(SC_THREADS), in, n, s->scan_tmp);
-    launch(s, QZ_PROF_SORT, 8.0 * 256 * tiles, k_scan_single, dim3(1), dim3(SC_THREADS), s->scan_tmp, tiles);
-    launch(s, QZ_PROF_SORT, 8.0 * n, k_scan_apply, dim3((int)tiles), dim3(SC_THREADS), in, out, n, s->scan_tmp);
+    if (++s->scan_epoch >= (1u << 30))
+    {
+        // the epoch field wraps: clear the old words once
+        cudaMemsetAsync(s->scan_st, 0, s->scan_st_cap * sizeof(unsigned long long), s->stream);
+        s->scan_epoch = 1;
+    }
+    launch(s, QZ_PROF_SORT, 8.0 * n, k_scan_lookback, dim3((int)tiles), dim3(SC_THREADS), in, out,
+           n, s->scan_st, s->scan_st + s->scan_st_cap, s->scan_base, s->scan_epoch, s->flags);
+    s->scan_base += (unsigned long long)tiles;
     return check_cuda(cudaGetLastError(), "scan") ? QZ_SUCCESS : QZ_FAILURE;
 }
 
