@@ -2,7 +2,8 @@
 // exclusive int scan, both deterministic (no order-dependent atomics on the
 // data path: per-tile digit counts use shared-memory integer atomics, whose
 // totals do not depend on order; ranks come from warp match masks in the
-// original element order).
+// original element order; the scan's tile numbers follow the blocks' arrival,
+// but its results are integer sums and do not depend on it).
 //
 // Tile = 8 warps x 8 iterations x 32 lanes = 2048 keys.  Warp w of tile t
 // owns keys [t*2048 + w*256, +256); iteration r covers 32 consecutive keys in
