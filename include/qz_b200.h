@@ -349,9 +349,10 @@ QZ_API int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, in
  * loads the library holds until the process exits; gridsize above
  * QZ_NOALLOC_MAX_GRID is rejected with an error.  phi (in/out) and rho are
  * gridsize^3 float64 device arrays; stream is a cudaStream_t (NULL for the
- * default stream); the call only enqueues work on it.  The first call on a
- * device looks up the array's device address once (make that first call before
- * any stream capture).  All calls share the array, which keeps the last call's
+ * default stream); the call only enqueues work on it.  Every call looks up the
+ * array's device address on the current device; the first call on a device
+ * also loads the library's kernels there (make that first call before any
+ * stream capture).  All calls share the array, which keeps the last call's
  * contents (each call starts by copying phi into it); calls that overlap on
  * the GPU race on it, so serialise them. */
 #define QZ_NOALLOC_MAX_GRID 65
@@ -362,6 +363,19 @@ QZ_API int qz_jacobi_noalloc(double *phi, const double *rho, int gridsize, int i
 QZ_API int qz_ptcl_idx_to_box_idx(int lv, int box_ts_x, int box_ts_y, int box_ts_z,
                            int box_real_dim_x, int box_real_dim_y, long n, const double *x,
                            const double *y, const double *z, int *out);
+
+/* Test hooks (no counterpart in the reference; used by the library's own tests).
+ * qz_test_scan: the device's single-pass exclusive scan of n ints (host arrays
+ * in / out; in_place scans one device buffer into itself; epoch != 0 first sets
+ * the scan epoch counter, so that a test can run across its wrap).
+ * qz_test_wait_gives_up: runs one bounded device wait that nothing satisfies
+ * and returns what the library returns then (QZ_FAILURE and the message):
+ * which 0 the scan's look-back on a tile that is never published, which 1 the
+ * cooperative kernels' grid barrier (out2[0], out2[1]: 1 if the first / second
+ * barrier of the probe returned true).  Each wait ends at its poll limit. */
+QZ_API int qz_test_scan(qz_sim *sim, const int *in, int *out, long n, int in_place,
+                        unsigned epoch);
+QZ_API int qz_test_wait_gives_up(qz_sim *sim, int which, int *out2);
 
 #ifdef __cplusplus
 }

@@ -134,6 +134,8 @@ def load() -> C.CDLL:
         "qz_amr_node_box": ([vp, C.c_int, C.c_int, _I], C.c_int),
         "qz_amr_node_list": ([vp, C.c_int, C.c_int, C.c_int, _I], C.c_int),
         "qz_amr_node_field": ([vp, C.c_int, C.c_int, C.c_int, _P], C.c_int),
+        "qz_test_scan": ([vp, _I, _I, C.c_long, C.c_int, C.c_uint], C.c_int),
+        "qz_test_wait_gives_up": ([vp, C.c_int, _I], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -514,6 +514,8 @@ int vcycle(qz_sim *s, int level, int type);
 int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **vals_out);
 long radix_tiles(long n);
 int scan_exclusive(qz_sim *s, const int *in, int *out, long n);
+int scan_wait_probe(qz_sim *s);
+void scan_set_epoch(qz_sim *s, unsigned epoch);
 
 // grid views
 inline Grid<double> head_view(qz_sim *s, double *field)

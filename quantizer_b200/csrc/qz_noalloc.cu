@@ -6,15 +6,18 @@
 // file-scope device array of fixed size: it is loaded with the module and
 // held by every device that loads the library until the process exits, so a
 // call allocates nothing.  Host code cannot use the array's name as a device
-// address (in host code it names a host-side stand-in), so the array's device
-// address is looked up once per device with cudaGetSymbolAddress, with that
-// device current, and passed to the kernels.
+// address (in host code it names a host-side stand-in), so every call looks up
+// the array's device address with cudaGetSymbolAddress, with the caller's
+// device current, and passes it to the kernels.  The lookup allocates nothing
+// and is not cached: an address kept from an earlier context (after
+// cudaDeviceReset, the module is loaded again elsewhere) would be stale.  On
+// the first call on a device the lookup also loads the module there, so make
+// that first call before any stream capture.
 //
 // Every call shares the array and it keeps the last call's contents: each call
 // first copies phi into it, so no state carries over between calls.  Calls
 // that overlap on the GPU (two streams, or two host threads, at the same time
 // on one device) race on the array and must be serialised by the caller.
-#include <mutex>
 #include <stdio.h>
 
 #include "qz_internal.cuh"
@@ -25,28 +28,17 @@ static __device__ __align__(256) double qz_noalloc_scratch[QZ_NOALLOC_MAX_POINTS
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-double *g_scratch[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (set-up on the
-// first call per device).
-double *scratch_address(int dev)
+// Device address of the scratch array in the current device's context.
+double *scratch_address()
 {
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch[dev])
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, qz_noalloc_scratch);
+    if (e != cudaSuccess)
     {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, qz_noalloc_scratch);
-        if (e != cudaSuccess)
-        {
-            qz::set_error("qz_jacobi_noalloc: cudaGetSymbolAddress failed: %s",
-                          cudaGetErrorString(e));
-            return nullptr;
-        }
-        g_scratch[dev] = static_cast<double *>(p);
+        qz::set_error("qz_jacobi_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return nullptr;
     }
-    return g_scratch[dev];
+    return static_cast<double *>(p);
 }
 
 __global__ void k_na_copy(const double *__restrict__ src, double *__restrict__ dst, long n)
@@ -92,12 +84,12 @@ extern "C" int qz_jacobi_noalloc(double *phi, const double *rho, int gridsize, i
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    if (e != cudaSuccess)
     {
         qz::set_error("qz_jacobi_noalloc: no usable CUDA device (%s)", cudaGetErrorString(e));
         return QZ_FAILURE;
     }
-    double *scr = scratch_address(dev);
+    double *scr = scratch_address();
     if (!scr)
         return QZ_FAILURE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);

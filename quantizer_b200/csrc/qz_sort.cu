@@ -252,12 +252,9 @@ __global__ void __launch_bounds__(SC_THREADS)
     }
 }
 
-// in and out may be the same array (each block reads its tile before writing it)
-int scan_exclusive(qz_sim *s, const int *in, int *out, long n)
+// Status words for `tiles` tiles and a fresh epoch for the next scan.
+static int scan_prepare(qz_sim *s, long tiles)
 {
-    if (n <= 0)
-        return QZ_SUCCESS;
-    const long tiles = (n + SC_TILE - 1) / SC_TILE;
     if (s->scan_st_cap < tiles)
     {
         // status words and the counter start at zero (epoch 0 is never used)
@@ -280,6 +277,17 @@ int scan_exclusive(qz_sim *s, const int *in, int *out, long n)
         cudaMemsetAsync(s->scan_st, 0, s->scan_st_cap * sizeof(unsigned long long), s->stream);
         s->scan_epoch = 1;
     }
+    return QZ_SUCCESS;
+}
+
+// in and out may be the same array (each block reads its tile before writing it)
+int scan_exclusive(qz_sim *s, const int *in, int *out, long n)
+{
+    if (n <= 0)
+        return QZ_SUCCESS;
+    const long tiles = (n + SC_TILE - 1) / SC_TILE;
+    if (scan_prepare(s, tiles))
+        return QZ_FAILURE;
     launch(s, QZ_PROF_SORT, 8.0 * n, k_scan_lookback, dim3((int)tiles), dim3(SC_THREADS), in, out,
            n, s->scan_st, s->scan_st + s->scan_st_cap, s->scan_base, s->scan_epoch, s->flags);
     s->scan_base += (unsigned long long)tiles;
@@ -323,5 +331,24 @@ int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **val
 }
 
 long radix_tiles(long n) { return (n + RS_TILE - 1) / RS_TILE; }
+
+// Test hook for the look-back's bounded wait: one block of a fresh epoch that
+// draws tile 1 (base one below the tile counter, which equals scan_base between
+// scans), whose tile 0 is never published, so its wait must run to
+// SCAN_POLL_LIMIT, set E_SCAN and return.  n = 0: the block reads and writes
+// no element.
+int scan_wait_probe(qz_sim *s)
+{
+    if (scan_prepare(s, 2))
+        return QZ_FAILURE;
+    launch(s, QZ_PROF_SORT, 0.0, k_scan_lookback, dim3(1), dim3(SC_THREADS), (const int *)nullptr,
+           (int *)nullptr, 0L, s->scan_st, s->scan_st + s->scan_st_cap, s->scan_base - 1ull,
+           s->scan_epoch, s->flags);
+    s->scan_base += 1ull; // the counter advanced by one tile
+    return check_cuda(cudaGetLastError(), "scan probe") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+// Test hook: sets the epoch the next scan increments (to reach the wrap).
+void scan_set_epoch(qz_sim *s, unsigned epoch) { s->scan_epoch = epoch; }
 
 } // namespace qz

@@ -1,16 +1,18 @@
-"""Kernel micro-benchmarks of libqzb200 at chosen sizes (device time by CUDA
-events on the library stream; the per-launch profiler books algorithmic
-bytes per kernel category).
+"""Kernel-level measurement cases of libqzb200 at chosen sizes, used to make
+the ncu summaries under profiles/ (device time by CUDA events on the library
+stream; the per-launch profiler books algorithmic bytes per kernel category).
 
-    python -m quantizer_b200.kernel_bench smooth    --n 257 --iters 4
-    python -m quantizer_b200.kernel_bench multigrid --n 257 --cycles 2
-    python -m quantizer_b200.kernel_bench step      --particles 1000000 --lmin 7 --steps 3
+    python -m tests.kernel_cases smooth    --n 257 --iters 4
+    python -m tests.kernel_cases multigrid --n 257 --cycles 2
+    python -m tests.kernel_cases step      --particles 1048576 --lmin 7 --levels 3 --steps 3
 
 `smooth` and `multigrid` run the array-level routines (gauss_saidel /
 multigrid, red-black order) on seeded random grids of n^3 points, which is
 how the smoother is profiled at sizes whose fields exceed the 126 MB L2.
-`step` runs whole head-node leapfrog steps of a Plummer sphere (refinement
-off) -- a kernel-level measurement, not the workload of bench.py.
+`step` runs whole leapfrog steps of a Plummer sphere on a 2^lmin head grid
+with `--levels` refinement levels above it (0: head only); `--precision 1`
+selects the mixed-precision form.  These are kernel-level cases, not the
+timed workload of bench.py.
 """
 from __future__ import annotations
 
@@ -20,7 +22,11 @@ import time
 
 import numpy as np
 
-from . import core, ics
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from quantizer_b200 import core, ics  # noqa: E402
 
 
 def _smooth(args) -> dict:

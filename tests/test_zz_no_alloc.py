@@ -9,7 +9,8 @@ inside the library instead.  The test calls it through the C ABI on device
 arrays owned by the test, twice in a row (the shared array keeps the previous
 call's contents, which must not leak into the next result), and compares each
 result with the allocating entry point qz_jacobi on the same inputs, bit for bit
-(the tolerance of the other Jacobi tests).  It lives in a file of its own that
+(the tolerance of the other Jacobi tests), at weights 1 and 0.7 (below 1 the
+(1 - w) term reads the ping-pong copy's previous contents).  It lives in a file of its own that
 pytest collects last.
 """
 import ctypes as C
@@ -30,18 +31,19 @@ def _lib():
     return lib
 
 
-@pytest.mark.parametrize("n,iters", [(17, 3), (33, 2), (65, 5)])
-def test_noalloc_jacobi_matches_allocating_entry_point(n, iters):
+@pytest.mark.parametrize("n,iters,w", [(17, 3, 1.0), (33, 2, 1.0), (65, 5, 1.0), (33, 3, 0.7),
+                                      (65, 4, 0.7)])
+def test_noalloc_jacobi_matches_allocating_entry_point(n, iters, w):
     import torch
     lib = _lib()
     rng = np.random.default_rng(n)
     cases = [(rng.standard_normal(n ** 3), rng.standard_normal(n ** 3) * 10.0) for _ in range(2)]
     stream = torch.cuda.current_stream()
     for phi0, rho in cases:  # two calls in a row
-        expected = core.jacobi(phi0, rho, iters, 1.0)
+        expected = core.jacobi(phi0, rho, iters, w)
         dphi = torch.tensor(phi0, dtype=torch.float64, device="cuda")
         drho = torch.tensor(rho, dtype=torch.float64, device="cuda")
-        rc = lib.qz_jacobi_noalloc(dphi.data_ptr(), drho.data_ptr(), n, iters, 1.0,
+        rc = lib.qz_jacobi_noalloc(dphi.data_ptr(), drho.data_ptr(), n, iters, w,
                                    stream.cuda_stream)
         assert rc == 0, lib.qz_last_error().decode()
         stream.synchronize()
