@@ -13,9 +13,10 @@ refinement levels, and the 512-member batching form (ensemble512: value is
 the members stepped concurrently, beside the same members stepped one after
 another).  The default workload
 is the 1M-particle Plummer sphere on a 128^3 head with 3 refinement levels in
-FP64 (the reference's arithmetic); the mixed-precision form (FP32 head
-smoothing inside FP64 defect correction) is timed on the same workload and
-reported with its force error against FP64 in "variant".
+FP64 (the reference's arithmetic); the mixed-precision form (FP32 multigrid
+cycles inside FP64 defect correction on the head and on every refinement node)
+is timed on the same workload and reported with its force error against FP64
+in "variant".
 
 * value  -- whole-job throughput with the state resident in HBM; the device
   time of exactly K steps (CUDA events on the library stream), L2 flushed
@@ -58,7 +59,7 @@ WORKLOADS = {
                               precision=0, cpu_steps=100, ref_steps=100),
     # Plummer N=1,048,576, a=0.02, head 128^3, refinement up to 3 levels above the head,
     # a cell refines when it holds more than 8 particles; FP64, with the mixed-precision
-    # head solve (FP32 smoothing inside FP64 defect correction) timed beside it
+    # form (FP32 multigrid inside FP64 defect correction) timed beside it
     "plummer1m_head128_amr3": dict(n=1048576, a=0.02, lmin=7, levels=3, ref_ptcl=9, steps=100,
                                    precision=0, variant=1, cpu_steps=3, ref_steps=10),
 }
@@ -107,6 +108,8 @@ def ensemble_members(wl: dict, seed: int = 0) -> list:
     As = rng.uniform(0.02, 0.08, m)
     return [(int(n), float(a), 5 if n < 16384 else 6) for n, a in zip(ns, As)]
 METRIC = "particle-steps/s"
+MIXED_DESC = ("fp32 multigrid cycles in fp64 defect correction (head: persistent V-cycles; "
+              "refinement nodes: one thread-block cluster per node)")
 
 
 def log(*a):
@@ -511,7 +514,7 @@ def main() -> int:
     config = {"workload": args.workload, "particles": wl["n"], "head_grid": 2 ** wl["lmin"],
               "lmax_minus_lmin": wl["levels"], "refine_above_particles": wl["ref_ptcl"] - 1,
               "dt": "1e-3 crossing time", "precision":
-              "fp64" if wl["precision"] == 0 else "fp32 head smoothing in fp64 defect correction",
+              "fp64" if wl["precision"] == 0 else MIXED_DESC,
               "residual_tol": 1e-10, "l2": "flushed between timed steps (256 MiB write)",
               "replicas": world}
 
@@ -646,7 +649,9 @@ def main() -> int:
         for _ in range(W):
             ref_sim.step(dt, 1)
         barrier()
+        sv0 = ref_sim.stats()
         ms_plain = timed_steps_on(ref_sim, lambda: ref_sim.step(dt, 1), K)
+        sv1 = ref_sim.stats()
         t_max = replicas.max_over_ranks(ms_plain, dev)
         plain_value = world * wl["n"] * K / (t_max / 1e3)
         # force error: both forms from one state, one step
@@ -663,8 +668,10 @@ def main() -> int:
         a_p = np.sqrt(sum(f64[k] ** 2 for k in ("ax", "ay", "az")))
         diff = np.sqrt(sum((mix[k] - f64[k]) ** 2 for k in ("ax", "ay", "az")))
         errs = diff / np.maximum(a_p, 1e-300)
-        plain = {"precision": "fp64" if wl["variant"] == 0 else
-                 "fp32 head smoothing in fp64 defect correction",
+        plain = {"precision": "fp64" if wl["variant"] == 0 else MIXED_DESC,
+                 "node_mg_iterations_per_step":
+                     (sv1.node_mg_iterations - sv0.node_mg_iterations) / K,
+                 "vcycles_per_step": (sv1.vcycles_total - sv0.vcycles_total) / K,
                  "value": plain_value, "ms_per_step": t_max / K,
                  "max_rel_force_err_mixed_vs_fp64": float(errs.max()),
                  "median_rel_force_err_mixed_vs_fp64": float(np.median(errs))}
@@ -686,7 +693,7 @@ def main() -> int:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if wl["precision"] == 0 else "f64 (f32 head smoothing)",
+                "dtype": "f64" if wl["precision"] == 0 else "f64 (f32 multigrid cycles)",
                 "data": "synthetic",
                 "config": config,
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 80 * n,

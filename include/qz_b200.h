@@ -126,6 +126,8 @@ typedef struct qz_stats {
     double last_dt;            /* step size of the last qz_step step */
     double sim_time;           /* sum of the qz_step step sizes */
     long long adjoint_cycles;  /* multigrid cycles of the adjoint solves */
+    long long node_mg_iterations; /* mixed form: defect-correction iterations of the
+                                     refinement-level solves (slowest node of each) */
 } qz_stats;
 
 /* Result of qz_adjoint_final_loss. */
@@ -155,7 +157,8 @@ typedef struct qz_sim qz_sim;
 #define QZ_PROF_OTHER 9      /* boundary fill, copies, mixed-precision residual */
 #define QZ_PROF_TREE 10      /* refinement tree: counts, flags, zones, children, lists */
 #define QZ_PROF_CG 11        /* refinement-node conjugate gradient */
-#define QZ_PROF_CATEGORIES 12
+#define QZ_PROF_NODE_MG 12   /* refinement-node FP32 multigrid in FP64 defect correction */
+#define QZ_PROF_CATEGORIES 13
 
 /* Configuration with the reference defaults (global_variables.c:300-341). */
 QZ_API int qz_default_config(qz_config *cfg, int lmin);
@@ -358,6 +361,20 @@ QZ_API int qz_multigrid(const qz_config *cfg, double *phi, const double *rho, in
 #define QZ_NOALLOC_MAX_GRID 65
 QZ_API int qz_jacobi_noalloc(double *phi, const double *rho, int gridsize, int iter_max,
                              double w, void *stream);
+
+/* conjugate_gradient (force_methods/conjugate_gradient.c:322-463) on one node
+ * given as HOST arrays, the fields of the reference's struct node: level lv,
+ * box_real_dim, the interior list ptr_intr_box_grid_idx (grid_intr_size
+ * entries), node_mass, cell_size, and the grid fields d, pot, pot_old of
+ * (box_real_dim + 1)^3 points.  Solved by the device's node conjugate gradient
+ * (same iterates, checks every check_every iterations with poisson_error's
+ * tests, the reference's iteration cap); pot is overwritten with the solution
+ * and pot_old as poisson_error leaves it.  QZ_FAILURE when the precision is
+ * not reached, with the reference's message. */
+QZ_API int qz_node_conjugate_gradient(qz_sim *sim, int lv, int box_real_dim_x, int box_real_dim_y,
+                                      int box_real_dim_z, int grid_intr_size,
+                                      const int *intr_box_grid_idx, double node_mass, int cell_size,
+                                      const double *d, double *pot, double *pot_old);
 
 /* Batched ptcl_idx_to_box_idx for one non-periodic node geometry. */
 QZ_API int qz_ptcl_idx_to_box_idx(int lv, int box_ts_x, int box_ts_y, int box_ts_z,

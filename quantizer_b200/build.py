@@ -21,7 +21,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["qz_capi.cu", "qz_particles.cu", "qz_poisson.cu", "qz_sort.cu", "qz_amr.cu",
                 "qz_noalloc.cu", "qz_observe.cu",
-                "qz_ensemble.cu", "qz_adjoint.cu", "qz_snapshot.cu", "qz_testhooks.cu"]
+                "qz_ensemble.cu", "qz_adjoint.cu", "qz_snapshot.cu", "qz_testhooks.cu",
+                "qz_node_mg.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include")]

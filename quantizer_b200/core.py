@@ -51,7 +51,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_longlong), ("steps", C.c_longlong), ("error_flags", C.c_int),
         ("cg_iterations", C.c_longlong), ("levels", C.c_int), ("nodes", C.c_int),
         ("last_dt", C.c_double), ("sim_time", C.c_double),
-        ("adjoint_cycles", C.c_longlong),
+        ("adjoint_cycles", C.c_longlong), ("node_mg_iterations", C.c_longlong),
     ]
 
 
@@ -135,6 +135,8 @@ def load() -> C.CDLL:
         "qz_amr_node_list": ([vp, C.c_int, C.c_int, C.c_int, _I], C.c_int),
         "qz_amr_node_field": ([vp, C.c_int, C.c_int, C.c_int, _P], C.c_int),
         "qz_test_scan": ([vp, _I, _I, C.c_long, C.c_int, C.c_uint], C.c_int),
+        "qz_node_conjugate_gradient": ([vp] + [C.c_int] * 5 + [_I, C.c_double, C.c_int] +
+                                       [_P] * 3, C.c_int),
         "qz_test_wait_gives_up": ([vp, C.c_int, _I], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -466,7 +468,7 @@ def ptcl_idx_to_box_idx(lv: int, box_ts: tuple, box_real_dim: tuple, x, y, z) ->
 
 # -- per-launch profiler ---------------------------------------------------------------
 PROF_CATEGORIES = ("smooth", "restrict", "prolong", "check", "deposit", "sort", "gradient",
-                   "gather", "leapfrog", "other", "tree", "cg")
+                   "gather", "leapfrog", "other", "tree", "cg", "node_mg")
 
 
 def _prof_sig(lib):

@@ -496,9 +496,10 @@ __global__ void k_adj_add_scalar(long n, const double *__restrict__ v, double *_
 // finest level down: the gather's transpose deposits a-bar on each particle's
 // finest level; on each level the gradient's transpose (-div over the interior
 // points), children's contributions, the node solves with zero boundary, and the
-// transposes of P (to the parent's a-bar and phi-bar: accumulated with atomic
-// adds, the only sums here whose order is not fixed), the shell (to the total
-// mass) and the deposit (to x and m).
+// transposes of P (to the parent's a-bar and phi-bar: contributions sorted by
+// parent point and added in list order), the shell (to the total mass) and the
+// deposit (to x and m).  Every sum has a fixed order: the gradient is
+// bit-reproducible.
 
 struct NodeOfPtrs {
     const int *p[AMR_MAX_LEVELS];
@@ -728,41 +729,66 @@ __device__ __forceinline__ double adj_phit(const AmrNode &N, long g, const doubl
     return phib[g] - nb / (H * H);
 }
 
-// transposes of the parent averages at the node boundary points: 0.125 of the
-// point's phi-bar (after the solve) and a-bar to each of its 8 parent points
-__global__ void k_adj_bdry_T(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
-                             const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
-                             const double *__restrict__ phib, const double *__restrict__ lam,
-                             const double *__restrict__ A0, const double *__restrict__ A1,
-                             const double *__restrict__ A2, double *__restrict__ pA0,
-                             double *__restrict__ pA1, double *__restrict__ pA2,
-                             double *__restrict__ pphic)
+// Transposes of the parent averages at the node boundary points: 0.125 of the
+// point's phi-bar (after the solve) and a-bar go to each of its 8 parent points
+// (a point on an even coordinate names the same parent point twice).  The
+// contributions are made deterministic by sorting them by target: pass 1 writes
+// one (parent point, 8 e + corner) pair per contribution, a stable radix sort
+// orders them by parent point and then by boundary-list position, and pass 2
+// adds each parent point's run in that order.
+__device__ __forceinline__ long adj_bdry_target(const AmrNode &N, const AmrNode &P, long g, int c)
 {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nlist)
-        return;
-    const long g = list[e];
-    const AmrNode N = nodes[lnode[e]];
-    const AmrNode P = pnodes[N.parent];
     int gx, gy, gz;
     grid_coords(N, g, &gx, &gy, &gz);
     const int cx = gx + N.ts[0], cy = gy + N.ts[1], cz = gz + N.ts[2];
-    const double ft = 0.125 * adj_phit(N, g, phib, lam);
-    const double a0 = 0.125 * A0[g], a1 = 0.125 * A1[g], a2 = 0.125 * A2[g];
-    const int xs[2] = {(cx >> 1) - P.ts[0], ((cx + 1) >> 1) - P.ts[0]};
-    const int ys[2] = {(cy >> 1) - P.ts[1], ((cy + 1) >> 1) - P.ts[1]};
-    const int zs[2] = {(cz >> 1) - P.ts[2], ((cz + 1) >> 1) - P.ts[2]};
+    const int ii = c & 1, jj = (c >> 1) & 1, kk = c >> 2;
+    const int x = (ii ? ((cx + 1) >> 1) : (cx >> 1)) - P.ts[0];
+    const int y = (jj ? ((cy + 1) >> 1) : (cy >> 1)) - P.ts[1];
+    const int z = (kk ? ((cz + 1) >> 1) : (cz >> 1)) - P.ts[2];
     const long sx = P.rd[0] + 1, sxy = sx * (P.rd[1] + 1);
-    for (int kk = 0; kk < 2; kk++)
-        for (int jj = 0; jj < 2; jj++)
-            for (int ii = 0; ii < 2; ii++)
-            {
-                const long q = P.grid_off + xs[ii] + ys[jj] * sx + zs[kk] * sxy;
-                atomicAdd(&pphic[q], ft);
-                atomicAdd(&pA0[q], a0);
-                atomicAdd(&pA1[q], a1);
-                atomicAdd(&pA2[q], a2);
-            }
+    return P.grid_off + x + y * sx + z * sxy;
+}
+
+__global__ void k_adj_bdry_keys(int nlist, const int *__restrict__ list, const int *__restrict__ lnode,
+                                const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ pnodes,
+                                unsigned *__restrict__ key, int *__restrict__ val)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8L * nlist)
+        return;
+    const int e = (int)(t >> 3), c = (int)(t & 7);
+    const AmrNode N = nodes[lnode[e]];
+    key[t] = (unsigned)adj_bdry_target(N, pnodes[N.parent], list[e], c);
+    val[t] = (int)t;
+}
+
+__global__ void k_adj_bdry_sum(long m, const unsigned *__restrict__ key, const int *__restrict__ val,
+                               const int *__restrict__ list, const int *__restrict__ lnode,
+                               const AmrNode *__restrict__ nodes, const double *__restrict__ phib,
+                               const double *__restrict__ lam, const double *__restrict__ A0,
+                               const double *__restrict__ A1, const double *__restrict__ A2,
+                               double *__restrict__ pA0, double *__restrict__ pA1,
+                               double *__restrict__ pA2, double *__restrict__ pphic)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || (i > 0 && key[i - 1] == key[i]))
+        return;
+    const unsigned q = key[i];
+    double sf = 0.0, s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (long j = i; j < m && key[j] == q; j++)
+    {
+        const int e = val[j] >> 3;
+        const long g = list[e];
+        const AmrNode N = nodes[lnode[e]];
+        sf += 0.125 * adj_phit(N, g, phib, lam);
+        s0 += 0.125 * A0[g];
+        s1 += 0.125 * A1[g];
+        s2 += 0.125 * A2[g];
+    }
+    pphic[q] += sf;
+    pA0[q] += s0;
+    pA1[q] += s1;
+    pA2[q] += s2;
 }
 
 // simulation-boundary points (analytic, linear in M): per block partial sums of
@@ -1212,10 +1238,28 @@ static int force_vjp(qz_sim *s, const double *x, const double *y, const double *
             *cycles += (int)(s->stats.cg_iterations - it0);
             s->stats.cg_iterations = it0; // the forward's count stays the forward's
             if (Lv.bdry_total > 0)
-                launch(s, QZ_PROF_OTHER, 160.0 * Lv.bdry_total, k_adj_bdry_T,
-                       dim3(blocks_for(Lv.bdry_total, 256)), dim3(256), Lv.bdry_total, Lv.bdry.p,
-                       Lv.bdry_node.p, Lv.nodes.p, P.nodes.p, A.lphib[l].p, A.llam[l].p, A0, A1,
-                       A2, pA0, pA1, pA2, pphic);
+            {
+                const long m8 = 8L * Lv.bdry_total;
+                if (!ensure_sort(s, m8))
+                {
+                    set_error("adjoint boundary transposes: sort buffers");
+                    return QZ_FAILURE;
+                }
+                int bits = 1;
+                while (bits < 32 && (1L << bits) < P.grid_total)
+                    bits++;
+                launch(s, QZ_PROF_OTHER, 8.0 * m8, k_adj_bdry_keys, dim3(blocks_for(m8, 256)),
+                       dim3(256), Lv.bdry_total, Lv.bdry.p, Lv.bdry_node.p, Lv.nodes.p, P.nodes.p,
+                       s->sort.k0, s->sort.v0);
+                unsigned *bk;
+                int *bv;
+                if (radix_sort_pairs(s, m8, bits, &bk, &bv))
+                    return QZ_FAILURE;
+                launch(s, QZ_PROF_OTHER, 160.0 * Lv.bdry_total, k_adj_bdry_sum,
+                       dim3(blocks_for(m8, 256)), dim3(256), m8, bk, bv, Lv.bdry.p,
+                       Lv.bdry_node.p, Lv.nodes.p, A.lphib[l].p, A.llam[l].p, A0, A1, A2, pA0,
+                       pA1, pA2, pphic);
+            }
             if (Lv.simb_total > 0)
             {
                 launch(s, QZ_PROF_OTHER, 96.0 * Lv.simb_total, k_adj_simb_T, dim3(ADJ_RED_BLOCKS),

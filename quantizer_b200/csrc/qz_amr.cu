@@ -577,6 +577,7 @@ void amr_free(qz_sim *s)
     for (auto &L : s->amr)
         free_level(s->mem, L);
     free_level(s->mem, s->head_cg);
+    free_level(s->mem, s->node_cg);
     s->amr.clear();
     for (auto &b : s->node_of)
         b.release(s->mem);
@@ -668,7 +669,7 @@ int amr_init(qz_sim *s)
     return ok ? QZ_SUCCESS : QZ_FAILURE;
 }
 
-static bool ensure_sort(qz_sim *s, long need)
+bool ensure_sort(qz_sim *s, long need)
 {
     Sort &S = s->sort;
     if (need <= S.cap)
@@ -2543,7 +2544,9 @@ int amr_potential(qz_sim *s)
                    L.intr_node.p, L.nodes.p, P.nodes.p, P.pot, L.pot);
         launch(s, QZ_PROF_OTHER, 16.0 * L.grid_total, k_copy_d, dim3(blocks_for(L.grid_total, 256)),
                dim3(256), L.grid_total, L.pot, L.pot_old);
-        if (cg_level(s, L, l))
+        // FP64: the reference's node conjugate gradient; mixed: FP32 multigrid in FP64
+        // defect correction (qz_node_mg.cu)
+        if (s->cfg.precision == QZ_PREC_MIXED ? node_mg_level(s, L, l) : cg_level(s, L, l))
             return QZ_FAILURE;
     }
     return QZ_SUCCESS;
@@ -2606,6 +2609,72 @@ int head_cg_solve(qz_sim *s)
     L.pot = s->pot;
     L.pot_old = s->pot_old;
     return cg_level(s, L, 0, false);
+}
+
+// ---- one node given as host arrays (the drop-in's conjugate_gradient(struct node *)) -----
+// conjugate_gradient.c:322-463 on one node: the node becomes a one-node level whose
+// grid fields are device copies of the host arrays, solved by k_cg_nodes, and
+// pot and pot_old are copied back.  poisson_error (poisson_error.c:339-342) copies
+// the whole pot grid to pot_old at every failed check; the device kernel copies
+// the interior points only (the only ones the ratio test reads), so the other
+// points of pot_old take pot's values here when a check failed.
+static int node_cg_host(qz_sim *s, int lv, const int rd[3], int nintr, const int *intr,
+                        double mass, int ncells, const double *d, double *pot, double *pot_old)
+{
+    AmrLevel &L = s->node_cg;
+    AmrNode N{};
+    N.lv = lv;
+    N.parent = -1;
+    for (int q = 0; q < 3; q++)
+        N.rd[q] = rd[q];
+    N.ncells = ncells;
+    N.intr_off = 0;
+    N.nintr = nintr;
+    N.grid_off = 0;
+    N.mass = mass;
+    const long gt = (long)(rd[0] + 1) * (rd[1] + 1) * (rd[2] + 1);
+    L.nnodes = 1;
+    L.h.assign(1, N);
+    L.intr_total = nintr;
+    L.grid_total = gt;
+    if (!L.intr.ensure(s->mem, nintr) || !L.gpot.ensure(s->mem, gt) ||
+        !L.gpot_old.ensure(s->mem, gt) || !L.gd.ensure(s->mem, gt) || !upload_nodes(s, L))
+    {
+        set_error("node conjugate gradient buffers");
+        return QZ_FAILURE;
+    }
+    L.pot = L.gpot.p;
+    L.pot_old = L.gpot_old.p;
+    L.d = L.gd.p;
+    if (!check_cuda(cudaMemcpyAsync(L.intr.p, intr, nintr * sizeof(int), cudaMemcpyHostToDevice,
+                                    s->stream), "node list") ||
+        !check_cuda(cudaMemcpyAsync(L.pot, pot, gt * sizeof(double), cudaMemcpyHostToDevice,
+                                    s->stream), "node pot") ||
+        !check_cuda(cudaMemcpyAsync(L.pot_old, pot_old, gt * sizeof(double),
+                                    cudaMemcpyHostToDevice, s->stream), "node pot_old") ||
+        !check_cuda(cudaMemcpyAsync(L.d, d, gt * sizeof(double), cudaMemcpyHostToDevice,
+                                    s->stream), "node density"))
+        return QZ_FAILURE;
+    const long long it0 = s->stats.cg_iterations;
+    const int rc = cg_level(s, L, 0, false);
+    const long long iters = s->stats.cg_iterations - it0;
+    if (!check_cuda(cudaMemcpyAsync(pot, L.pot, gt * sizeof(double), cudaMemcpyDeviceToHost,
+                                    s->stream), "node pot back") ||
+        !check_cuda(cudaMemcpyAsync(pot_old, L.pot_old, gt * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s->stream), "node pot_old back") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "node sync"))
+        return QZ_FAILURE;
+    const int every = s->cfg.check_every > 0 ? s->cfg.check_every : 1;
+    if (iters > every || rc != QZ_SUCCESS)
+    {
+        std::vector<char> in(gt, 0);
+        for (int e = 0; e < nintr; e++)
+            in[intr[e]] = 1;
+        for (long g = 0; g < gt; g++)
+            if (!in[g])
+                pot_old[g] = pot[g];
+    }
+    return rc;
 }
 
 // ---- gradient on refinement levels -------------------------------------------------------
@@ -2881,3 +2950,38 @@ int amr_gather(qz_sim *s)
     return check_cuda(cudaGetLastError(), "amr gather") ? QZ_SUCCESS : QZ_FAILURE;
 }
 } // namespace qz
+
+using namespace qz;
+
+extern "C" int qz_node_conjugate_gradient(qz_sim *s, int lv, int box_real_dim_x,
+                                          int box_real_dim_y, int box_real_dim_z,
+                                          int grid_intr_size, const int *intr_box_grid_idx,
+                                          double node_mass, int cell_size, const double *d,
+                                          double *pot, double *pot_old)
+{
+    if (!s || lv < 0 || lv > 30 || box_real_dim_x < 2 || box_real_dim_y < 2 || box_real_dim_z < 2 ||
+        grid_intr_size < 0 || (grid_intr_size > 0 && !intr_box_grid_idx) || !d || !pot ||
+        !pot_old || cell_size <= 0)
+    {
+        set_error("qz_node_conjugate_gradient: bad arguments");
+        return QZ_FAILURE;
+    }
+    if (grid_intr_size == 0)
+        return QZ_SUCCESS;
+    const long gt = (long)(box_real_dim_x + 1) * (box_real_dim_y + 1) * (box_real_dim_z + 1);
+    const long sy = box_real_dim_x + 1, sz = sy * (box_real_dim_y + 1);
+    for (int e = 0; e < grid_intr_size; e++)
+    {
+        const long g = intr_box_grid_idx[e];
+        if (g - sz < 0 || g + sz >= gt)
+        {
+            set_error("qz_node_conjugate_gradient: interior point %ld has a neighbour outside "
+                      "the node grid", g);
+            return QZ_FAILURE;
+        }
+    }
+    const int rd[3] = {box_real_dim_x, box_real_dim_y, box_real_dim_z};
+    return node_cg_host(s, lv, rd, grid_intr_size, intr_box_grid_idx, node_mass, cell_size, d, pot,
+                        pot_old);
+}
+

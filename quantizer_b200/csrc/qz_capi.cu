@@ -125,6 +125,9 @@ static bool build_levels(qz_sim *s, int n0)
     const bool cgs = s->cfg.smoother == 2;
     if (cgs && !s->cg_part && !dmalloc(&s->cg_part, 2 * QZ_CG_PART_MAX, "cg partials"))
         return false;
+    // mixed form: per-block partials of the in-launch convergence test, its result
+    if (mixed && !s->mg_part && !dmalloc(&s->mg_part, 2 * QZ_CG_PART_MAX + 8, "mg partials"))
+        return false;
     for (auto &l : s->levels)
     {
         size_t pts = (size_t)l.n * l.n * l.n;
@@ -188,6 +191,8 @@ static void free_levels(qz_sim *s)
     s->levels.clear();
     dfree(s->cg_part);
     s->cg_part = nullptr;
+    dfree(s->mg_part);
+    s->mg_part = nullptr;
     dfree(s->rf);
     dfree(s->ef);
     dfree(s->ef_alt);
@@ -377,6 +382,7 @@ int qz_destroy(qz_sim *s)
         dfree(p);
     free_levels(s);
     amr_free(s);
+    node_mg_free(s);
     adjoint_free(s);
     s->ofl_state.release(s->mem);
     s->ofl_int.release(s->mem);

@@ -563,13 +563,21 @@ void jacobi(double *phi, const double *rho, int gridsize, int iter_max)
         fail("jacobi");
 }
 
-/* force_methods/conjugate_gradient.c:322-463: refinement-node solver, not in
- * this build (head-only). */
+/* force_methods/conjugate_gradient.c:322-463: one node's solve on the device
+ * (the node's grid fields are copied in and back; see qz_node_conjugate_gradient). */
 int conjugate_gradient(struct node *p)
 {
-    (void)p;
-    printf("\nERROR (drop-in): conjugate_gradient (refinement nodes) is not supported by this build\n");
-    return REF_FAILURE;
+    if (!p || ensure())
+        return REF_FAILURE;
+    if (qz_node_conjugate_gradient(g_sim, p->lv, p->box_real_dim_x, p->box_real_dim_y,
+                                   p->box_real_dim_z, p->grid_intr_size, p->ptr_intr_box_grid_idx,
+                                   p->node_mass, p->cell_size, p->ptr_d, p->ptr_pot,
+                                   p->ptr_pot_old))
+    {
+        fail("conjugate_gradient");
+        return REF_FAILURE;
+    }
+    return REF_SUCCESS;
 }
 
 /* force_methods/conjugate_gradient_multigrid.c:29-176 */

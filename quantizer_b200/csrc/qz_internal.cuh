@@ -304,6 +304,7 @@ struct AmrLevel {
 
 namespace qz {
 struct Adjoint;  // qz_adjoint.cu
+struct NodeMgState; // qz_node_mg.cu
 struct Snapshot; // qz_snapshot.cu
 }
 
@@ -313,6 +314,8 @@ struct qz_sim {
     cudaStream_t stream = nullptr;
     qz::MemCtx mem; // stream-ordered pool for buffers that grow during a run
     double *cg_part = nullptr; // conjugate-gradient smoothing: 2 x QZ_CG_PART_MAX partial sums
+    double *mg_part = nullptr; // mixed head cycles: block partials of the convergence test + result
+    int mg_ran = 0, mg_conv = 0; // mixed head cycles: iterations of the last launch, converged
     unsigned *gbar = nullptr;  // grid barrier words of the cooperative launches (4)
     long n = 0, cap = 0;
     double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
@@ -363,7 +366,9 @@ struct qz_sim {
     // refinement tree (lmax > lmin): levels[0] = head, rebuilt every step
     std::vector<qz::AmrLevel> amr;
     qz::AmrLevel head_cg; // the head as a one-node level (head_pot_method 1)
+    qz::AmrLevel node_cg; // one host node solved by the node conjugate gradient (qz_node_conjugate_gradient)
     qz::Adjoint *adj = nullptr; // adjoint buffers (qz_force_vjp, qz_adjoint_final_loss)
+    qz::NodeMgState *node_mg = nullptr; // mixed-form refinement-level multigrid buffers
     qz::Snapshot *snap = nullptr; // snapshot staging and writer thread (qz_write_snapshot)
     // the head node's mass (node_mass): the configured total mass, lowered by
     // outflow removals; the convergence tests of the head solve use it
@@ -420,6 +425,8 @@ int solve_zero_bc(qz_sim *s, double *lam, double *f, double rtol, double *scratc
 int check_flags(qz_sim *s);                   // qz_capi.cu
 int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
 void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
+int node_mg_level(qz_sim *s, AmrLevel &L, int level_index); // qz_node_mg.cu
+void node_mg_free(qz_sim *s);                               // qz_node_mg.cu
 void snapshot_free(qz_sim *s);                // qz_snapshot.cu
 // A copy of the state a step reads (particles, accelerations, head potential)
 // and of the statistics, to run trial steps and put the simulation back
@@ -515,6 +522,7 @@ int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **val
 long radix_tiles(long n);
 int scan_exclusive(qz_sim *s, const int *in, int *out, long n);
 int scan_wait_probe(qz_sim *s);
+bool ensure_sort(qz_sim *s, long need); // qz_amr.cu: radix-sort buffers for need pairs
 void scan_set_epoch(qz_sim *s, unsigned epoch);
 
 // grid views

@@ -1,0 +1,871 @@
+// qz_node_mg.cu -- mixed-precision Poisson solves of the refinement nodes:
+// FP32 multigrid V-cycles inside FP64 defect correction, one thread-block
+// cluster per node.
+//
+// The reference solves every refinement node by unpreconditioned conjugate
+// gradient in FP64 (potential_branches.c:401-532 -> conjugate_gradient.c:
+// 322-463), checking the node every 5 iterations with the ratio test against
+// the previous check and the residual test of conj_grad_error
+// (poisson_error.c:36-81, 236-288).  The plain FP64 path of this library keeps
+// that solver (k_cg_nodes, qz_amr.cu).  The mixed-precision form replaces it
+// by defect correction:
+//
+//   repeat:  r = d - Lap_H(phi)                      (FP64, interior points)
+//            convergence test on phi (ratio test against the previous iterate,
+//            residual test on r: the reference's test, FP64)
+//            e ~= Lap_H^-1 r by one FP32 V-cycle      (zero on non-interior points)
+//            phi += e                                 (FP64)
+//
+// The V-cycle works on the node's grid box with a mask: level 0 is the node
+// grid ((rd + 1)^3 points, unknowns at the node's interior points, in the
+// node's colour-coded interior list), level k + 1 has ceil(c_k / 2) cells per
+// axis and a point X is an unknown when the fine point 2^k X is an interior
+// point (every other point holds zero: homogeneous Dirichlet values for the
+// correction).  Smoothing is red-black Gauss-Seidel with the arithmetic of the
+// head's sweeps (k_gs_rb: phi = (sum of neighbours - h^2 rho) / 6), restriction
+// takes half the residual at the coincident fine point (the red-black head
+// cycle's half injection), prolongation is trilinear and adds at unknowns
+// only.  The coarsest level (at most 4 cells per axis) is solved by FP64
+// red-black sweeps.
+//
+// Execution: one cluster of CS CTAs (16 where the device allows, else 8) per
+// node, all nodes of a level in one launch.  Phases are separated by hardware
+// cluster barriers (barrier.cluster arrive.release / wait.acquire); data
+// written by other CTAs of the cluster is read with L2 loads (ld.global.cg).
+// The fine level and the first coarse levels are swept by the whole cluster;
+// the levels small enough for shared memory run as a sub-cycle inside CTA 0
+// while the others wait at the next cluster barrier.  The FP64 residual pass
+// also forms the new iterate: phi_{k+1} = phi_k + e is written to the other of
+// the node's two potential buffers (pot / pot_old), so the ratio test compares
+// the two buffers without a copy; a node that stops with its iterate in
+// pot_old copies its interior points back to pot.  Residual sums: warp
+// shuffle trees, warps in order, CTAs in rank order read through distributed
+// shared memory -- every CTA obtains the same sums and takes the same
+// decisions, and runs are bit-reproducible.  A node that does not converge
+// within max_iter iterations fails the solve, as the reference's solver does.
+#include <cooperative_groups.h>
+#include <mutex>
+
+#include "qz_amr_dev.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace qz {
+
+#define QZ_PI_NMG 3.14159265358979323846
+
+constexpr int NMG_THREADS = 1024;
+constexpr int NMG_MAXLEV = 10;
+constexpr size_t NMG_SMEM_MAX = 160 * 1024; // shared-memory sub-cycle (CTA 0)
+constexpr int NMG_COARSE_SWEEPS = 24;       // FP64 red-black sweeps on the coarsest level
+
+struct NmgLev {
+    int nx, ny, nz; // points per axis
+    long off;       // first point in the coarse pools (levels >= 1)
+};
+
+struct NmgNode {
+    int q;          // node index in the level
+    int nlev;       // multigrid levels (0: the node grid)
+    int nsmall;     // first level of CTA 0's shared-memory sub-cycle (>= 1)
+    int ib, ie;     // the node's range of the level's interior list
+    long goff;      // node grid offset in the level's grid pools
+    double oh2;     // 1 / H^2
+    double thr;     // residual test: r.r threshold (check methods 0 and 2)
+    double rmt;     // check method 1: tol * (4 pi G rho_mean)
+    int cap;        // most iterations
+    int smem_need;  // bytes of the sub-cycle
+    float h2[NMG_MAXLEV];
+    NmgLev lv[NMG_MAXLEV];
+    int soff[NMG_MAXLEV]; // sub-cycle levels: byte offset of e (float), f (float), mask (uchar)
+    int coff;             // coarsest level FP64 arrays (e, f)
+};
+
+struct NmgArgs {
+    const NmgNode *tab;
+    const int *intr;       // level interior list (grid-pool indices)
+    int *cl;               // colour-coded copy of the list (~g for odd points)
+    const double *d;
+    double *pot, *pot_old; // the node's two potential buffers
+    float *ef, *rf;        // level 0 correction and residual (grid-pool layout)
+    unsigned char *msk;    // level 0 interior mask (grid-pool layout)
+    float *ec, *fc;        // coarse levels
+    unsigned char *mc;
+    int *status;           // per entry: converged, iterations
+    double tol2;
+    int method;
+    int n_pre, n_post;
+};
+
+// ---- small helpers ------------------------------------------------------------------------
+__device__ __forceinline__ float ldg_f(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ double ldg_d(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned char ldg_u8(const unsigned char *p) { return __ldcg(p); }
+
+// Items of one colour of a dense level: rows (j, k) over the interior, i of the
+// row's parity.  Item t -> (i, j, k) or false when beyond the row.
+struct ColourWalk {
+    int mx, my, mz, hmax;
+    long items;
+    __device__ ColourWalk(int nx, int ny, int nz)
+    {
+        mx = nx - 2;
+        my = ny - 2;
+        mz = nz - 2;
+        hmax = (mx + 1) / 2;
+        items = (mx > 0 && my > 0 && mz > 0) ? (long)hmax * my * mz : 0;
+    }
+    __device__ bool at(long t, int col, int &i, int &j, int &k) const
+    {
+        const int u = (int)(t % hmax);
+        const long row = t / hmax;
+        j = 1 + (int)(row % my);
+        k = 1 + (int)(row / my);
+        i = ((((1 + j + k) & 1) == col) ? 1 : 2) + 2 * u;
+        return i <= mx;
+    }
+};
+
+// One colour of a red-black sweep of a dense level.  G: arrays in global
+// memory (L2 loads).  FIRST: the level's correction starts at zero (the other
+// colour's values are not read).
+template <bool G, typename T>
+__device__ __forceinline__ void dense_sweep(T *e, const T *f, const unsigned char *m, int nx, int ny,
+                                            int nz, T h2, int col, bool first, long t0, long nt)
+{
+    const ColourWalk W(nx, ny, nz);
+    const long sy = nx, sz = (long)nx * ny;
+    const T one_sixth = (T)(1.0 / 6.0);
+    for (long t = t0; t < W.items; t += nt)
+    {
+        int i, j, k;
+        if (!W.at(t, col, i, j, k))
+            continue;
+        const long x = i + j * sy + k * sz;
+        const unsigned char a = G ? ldg_u8(m + x) : m[x];
+        if (!a)
+            continue;
+        T fx, s;
+        if constexpr (G)
+        {
+            fx = ldg_f(f + x);
+            s = first ? (T)0
+                      : ldg_f(e + x + 1) + ldg_f(e + x - 1) + ldg_f(e + x + sy) + ldg_f(e + x - sy) +
+                            ldg_f(e + x + sz) + ldg_f(e + x - sz);
+        }
+        else
+        {
+            fx = f[x];
+            s = first ? (T)0 : e[x + 1] + e[x - 1] + e[x + sy] + e[x - sy] + e[x + sz] + e[x - sz];
+        }
+        const T v = one_sixth * (-h2 * fx + s);
+        if constexpr (G)
+            __stcg(e + x, v);
+        else
+            e[x] = v;
+    }
+}
+
+// Residual of the fine level (k-1) at 2X, halved, into the coarse rhs at the
+// coarse unknowns X of a dense level k.  GF: the fine arrays are global; GC:
+// the coarse ones are.
+template <bool GF, bool GC>
+__device__ __forceinline__ void dense_restrict(const float *ef, const float *ff, int fnx, int fny,
+                                               float foh2, float *fcrs, const unsigned char *mcrs,
+                                               int nx, int ny, int nz, long t0, long nt)
+{
+    const long fsy = fnx, fsz = (long)fnx * fny;
+    const long sy = nx, sz = (long)nx * ny;
+    const int mx = nx - 2, my = ny - 2, mz = nz - 2;
+    if (mx < 1 || my < 1 || mz < 1)
+        return;
+    const long items = (long)mx * my * mz;
+    for (long t = t0; t < items; t += nt)
+    {
+        const int i = 1 + (int)(t % mx);
+        const long r = t / mx;
+        const int j = 1 + (int)(r % my), k = 1 + (int)(r / my);
+        const long x = i + j * sy + k * sz;
+        if (!(GC ? ldg_u8(mcrs + x) : mcrs[x]))
+            continue;
+        const long g = 2L * i + 2L * j * fsy + 2L * k * fsz;
+        float c, s;
+        if (GF)
+        {
+            c = ldg_f(ef + g);
+            s = ldg_f(ef + g + 1) + ldg_f(ef + g - 1) + ldg_f(ef + g + fsy) + ldg_f(ef + g - fsy) +
+                ldg_f(ef + g + fsz) + ldg_f(ef + g - fsz);
+        }
+        else
+        {
+            c = ef[g];
+            s = ef[g + 1] + ef[g - 1] + ef[g + fsy] + ef[g - fsy] + ef[g + fsz] + ef[g - fsz];
+        }
+        const float rv = (GF ? ldg_f(ff + g) : ff[g]) + foh2 * (6.0f * c - s);
+        const float v = 0.5f * rv;
+        if (GC)
+            __stcg(fcrs + x, v);
+        else
+            fcrs[x] = v;
+    }
+}
+
+// Trilinear value of the coarse correction at fine point (i, j, k).
+template <bool G>
+__device__ __forceinline__ float prolong_at(const float *ec, int cnx, int cny, int i, int j, int k)
+{
+    const long csy = cnx, csz = (long)cnx * cny;
+    const int x0 = i >> 1, x1 = (i + 1) >> 1, y0 = j >> 1, y1 = (j + 1) >> 1, z0 = k >> 1,
+              z1 = (k + 1) >> 1;
+    auto E = [&](int a, int b, int c) -> float {
+        const long x = a + b * csy + c * csz;
+        return G ? ldg_f(ec + x) : ec[x];
+    };
+    const float wx = (i & 1) ? 0.5f : 1.0f, wy = (j & 1) ? 0.5f : 1.0f, wz = (k & 1) ? 0.5f : 1.0f;
+    float acc = E(x0, y0, z0);
+    if (i & 1)
+        acc += E(x1, y0, z0);
+    if (j & 1)
+    {
+        acc += E(x0, y1, z0);
+        if (i & 1)
+            acc += E(x1, y1, z0);
+    }
+    if (k & 1)
+    {
+        acc += E(x0, y0, z1);
+        if (i & 1)
+            acc += E(x1, y0, z1);
+        if (j & 1)
+        {
+            acc += E(x0, y1, z1);
+            if (i & 1)
+                acc += E(x1, y1, z1);
+        }
+    }
+    return wx * wy * wz * acc;
+}
+
+// e_k += P e_{k+1} at the unknowns of a dense level k.
+template <bool GF, bool GC>
+__device__ __forceinline__ void dense_prolong(float *e, const unsigned char *m, int nx, int ny,
+                                              int nz, const float *ec, int cnx, int cny, long t0,
+                                              long nt)
+{
+    const long sy = nx, sz = (long)nx * ny;
+    const int mx = nx - 2, my = ny - 2, mz = nz - 2;
+    if (mx < 1 || my < 1 || mz < 1)
+        return;
+    const long items = (long)mx * my * mz;
+    for (long t = t0; t < items; t += nt)
+    {
+        const int i = 1 + (int)(t % mx);
+        const long r = t / mx;
+        const int j = 1 + (int)(r % my), k = 1 + (int)(r / my);
+        const long x = i + j * sy + k * sz;
+        if (!(GF ? ldg_u8(m + x) : m[x]))
+            continue;
+        const float add = prolong_at<GC>(ec, cnx, cny, i, j, k);
+        if (GF)
+            __stcg(e + x, ldg_f(e + x) + add);
+        else
+            e[x] += add;
+    }
+}
+
+// ---- the kernel -------------------------------------------------------------------------
+__global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constant__ NmgArgs A)
+{
+    cg::cluster_group cluster = cg::this_cluster();
+    const int CS = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int ent = (int)(blockIdx.x / CS);
+    __shared__ NmgNode N;
+    __shared__ double wsum[32];
+    __shared__ int wflag[32];
+    __shared__ double part_d;  // this CTA's partial (read by the others through DSMEM)
+    __shared__ int part_f;
+    __shared__ double tot_d;
+    __shared__ int tot_f;
+    extern __shared__ __align__(16) unsigned char nmg_dyn[];
+    const int tid = threadIdx.x, NT = blockDim.x;
+    if (tid == 0)
+        N = A.tab[ent];
+    __syncthreads();
+    const long ct = (long)rank * NT + tid, CT = (long)CS * NT;
+    const int nl = N.ie - N.ib;
+    const int sb = N.ib + (int)((long)nl * rank / CS), se = N.ib + (int)((long)nl * (rank + 1) / CS);
+    const NmgLev L0 = N.lv[0];
+    const long sy0 = L0.nx, sz0 = (long)L0.nx * L0.ny;
+    float *ef = A.ef + N.goff;
+    float *rf = A.rf + N.goff;
+    unsigned char *mk0 = A.msk + N.goff;
+
+    // set-up 1: colour-coded list and the fine mask
+    for (int e = sb + tid; e < se; e += NT)
+    {
+        const int g = A.intr[e];
+        long l = g - N.goff;
+        const int z = (int)(l / sz0);
+        l -= z * sz0;
+        const int y = (int)(l / sy0);
+        const int x = (int)(l - y * sy0);
+        A.cl[e] = ((x + y + z) & 1) ? ~g : g;
+        __stcg(A.msk + g, (unsigned char)1);
+    }
+    cluster.sync();
+    // set-up 2: coarse masks, X is an unknown where the fine point 2^k X is one
+    for (int k = 1; k < N.nlev; k++)
+    {
+        const NmgLev Lk = N.lv[k];
+        const int mx = Lk.nx - 2, my = Lk.ny - 2, mz = Lk.nz - 2;
+        if (mx < 1 || my < 1 || mz < 1)
+            continue;
+        const long items = (long)mx * my * mz;
+        for (long t = ct; t < items; t += CT)
+        {
+            const int i = 1 + (int)(t % mx);
+            const long r = t / mx;
+            const int j = 1 + (int)(r % my), kk = 1 + (int)(r / my);
+            const long g = ((long)i << k) + ((long)j << k) * sy0 + ((long)kk << k) * sz0;
+            A.mc[Lk.off + i + (long)j * Lk.nx + (long)kk * Lk.nx * Lk.ny] = ldg_u8(mk0 + g);
+        }
+    }
+    cluster.sync();
+    // CTA 0: zero the sub-cycle arrays once and copy their masks
+    if (rank == 0)
+    {
+        for (int k = N.nsmall; k < N.nlev; k++)
+        {
+            const NmgLev Lk = N.lv[k];
+            const long P = (long)Lk.nx * Lk.ny * Lk.nz;
+            float *se_ = reinterpret_cast<float *>(nmg_dyn + N.soff[k]);
+            float *sf_ = se_ + P;
+            unsigned char *sm_ = reinterpret_cast<unsigned char *>(sf_ + P);
+            for (long t = tid; t < P; t += NT)
+            {
+                se_[t] = 0.0f;
+                sf_[t] = 0.0f;
+                sm_[t] = ldg_u8(A.mc + Lk.off + t);
+            }
+        }
+        __syncthreads();
+    }
+
+    auto sub_e = [&](int k) { return reinterpret_cast<float *>(nmg_dyn + N.soff[k]); };
+    auto sub_f = [&](int k) {
+        return reinterpret_cast<float *>(nmg_dyn + N.soff[k]) + (long)N.lv[k].nx * N.lv[k].ny * N.lv[k].nz;
+    };
+    auto sub_m = [&](int k) {
+        const long P = (long)N.lv[k].nx * N.lv[k].ny * N.lv[k].nz;
+        return reinterpret_cast<unsigned char *>(reinterpret_cast<float *>(nmg_dyn + N.soff[k]) + 2 * P);
+    };
+    auto ge = [&](int k) { return k == 0 ? ef : A.ec + N.lv[k].off; };
+    auto gf = [&](int k) { return k == 0 ? rf : A.fc + N.lv[k].off; };
+
+    // one colour of a sweep of the fine level over this CTA's slice of the list
+    auto fine_sweep = [&](int col, bool first) {
+        const float h2 = N.h2[0];
+        const float one_sixth = (float)(1.0 / 6.0);
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            if ((v < 0) != (col == 1))
+                continue;
+            const long g = v < 0 ? ~v : v;
+            const float fx = ldg_f(A.rf + g);
+            float s = 0.0f;
+            if (!first)
+                s = ldg_f(A.ef + g + 1) + ldg_f(A.ef + g - 1) + ldg_f(A.ef + g + sy0) +
+                    ldg_f(A.ef + g - sy0) + ldg_f(A.ef + g + sz0) + ldg_f(A.ef + g - sz0);
+            __stcg(A.ef + g, one_sixth * (-h2 * fx + s));
+        }
+    };
+
+    double *bufs[2] = {A.pot, A.pot_old};
+    int it = 0;
+    bool conv = false;
+    for (;;)
+    {
+        // FP64: new iterate, its residual (FP32 copy for the cycle), ratio test
+        const double *ph = bufs[it & 1];
+        double *pn = bufs[(it + 1) & 1];
+        double acc = 0.0;
+        int fl = 0; // 1: ratio test failed, 2: point residual test failed (method 1)
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            const long g = v < 0 ? ~v : v;
+            auto P = [&](long x) -> double {
+                return it > 0 ? ldg_d(ph + x) + (double)ldg_f(A.ef + x) : ldg_d(ph + x);
+            };
+            const double old = ldg_d(ph + g);
+            const double c0 = P(g);
+            const double r = A.d[g] + N.oh2 * (6.0 * c0 - P(g + 1) - P(g - 1) - P(g + sy0) -
+                                              P(g - sy0) - P(g + sz0) - P(g - sz0));
+            __stcg(pn + g, c0);
+            A.rf[g] = (float)r;
+            acc += r * r;
+            const double aux = c0 / old;
+            if ((1.0 - A.tol2 > aux) || (1.0 + A.tol2 < aux))
+                fl |= 1;
+            if (A.method == 1 && fabs(r) >= N.rmt)
+                fl |= 2;
+        }
+        for (int o = 16; o > 0; o >>= 1)
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)fl);
+        if ((tid & 31) == 0)
+        {
+            wsum[tid >> 5] = acc;
+            wflag[tid >> 5] = fl;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            double t = 0.0;
+            int f = 0;
+            for (int w = 0; w < (NT >> 5); w++)
+            {
+                t += wsum[w];
+                f |= wflag[w];
+            }
+            part_d = t;
+            part_f = f;
+        }
+        cluster.sync();
+        if (tid == 0)
+        {
+            double t = 0.0;
+            int f = 0;
+            for (int r = 0; r < CS; r++)
+            {
+                t += *cluster.map_shared_rank(&part_d, r);
+                f |= *cluster.map_shared_rank(&part_f, r);
+            }
+            tot_d = t;
+            tot_f = f;
+        }
+        __syncthreads();
+        conv = it > 0 && !(tot_f & 1) && (A.method == 1 ? !(tot_f & 2) : tot_d < N.thr);
+        if (conv || it >= N.cap)
+            break;
+
+        // ---- one FP32 V-cycle on (ef, rf) -----------------------------------------
+        for (int sw = 0; sw < A.n_pre; sw++)
+            for (int col = 0; col < 2; col++)
+            {
+                fine_sweep(col, sw == 0 && col == 0);
+                cluster.sync();
+            }
+        for (int k = 1; k < N.nsmall; k++)
+        {
+            const NmgLev F = N.lv[k - 1], C = N.lv[k];
+            dense_restrict<true, true>(ge(k - 1), gf(k - 1), F.nx, F.ny, 1.0f / N.h2[k - 1],
+                                       A.fc + C.off, A.mc + C.off, C.nx, C.ny, C.nz, ct, CT);
+            cluster.sync();
+            for (int sw = 0; sw < A.n_pre; sw++)
+                for (int col = 0; col < 2; col++)
+                {
+                    dense_sweep<true, float>(A.ec + C.off, A.fc + C.off, A.mc + C.off, C.nx, C.ny,
+                                             C.nz, N.h2[k], col, sw == 0 && col == 0, ct, CT);
+                    cluster.sync();
+                }
+        }
+        if (rank == 0)
+        {
+            // sub-cycle of the small levels in shared memory
+            const int ks = N.nsmall;
+            {
+                const NmgLev F = N.lv[ks - 1], C = N.lv[ks];
+                dense_restrict<true, false>(ge(ks - 1), gf(ks - 1), F.nx, F.ny, 1.0f / N.h2[ks - 1],
+                                            sub_f(ks), sub_m(ks), C.nx, C.ny, C.nz, tid, NT);
+                __syncthreads();
+            }
+            for (int k = ks; k < N.nlev - 1; k++)
+            {
+                const NmgLev C = N.lv[k], D = N.lv[k + 1];
+                for (int sw = 0; sw < A.n_pre; sw++)
+                    for (int col = 0; col < 2; col++)
+                    {
+                        dense_sweep<false, float>(sub_e(k), sub_f(k), sub_m(k), C.nx, C.ny, C.nz,
+                                                  N.h2[k], col, sw == 0 && col == 0, tid, NT);
+                        __syncthreads();
+                    }
+                dense_restrict<false, false>(sub_e(k), sub_f(k), C.nx, C.ny, 1.0f / N.h2[k],
+                                             sub_f(k + 1), sub_m(k + 1), D.nx, D.ny, D.nz, tid, NT);
+                __syncthreads();
+            }
+            {
+                // coarsest level: FP64 red-black sweeps from zero
+                const int k = N.nlev - 1;
+                const NmgLev C = N.lv[k];
+                const long P = (long)C.nx * C.ny * C.nz;
+                double *e64 = reinterpret_cast<double *>(nmg_dyn + N.coff);
+                double *f64 = e64 + P;
+                const float *fk = sub_f(k);
+                for (long t = tid; t < P; t += NT)
+                {
+                    e64[t] = 0.0;
+                    f64[t] = (double)fk[t];
+                }
+                __syncthreads();
+                const double h2 = (double)N.h2[k];
+                for (int sw = 0; sw < NMG_COARSE_SWEEPS; sw++)
+                    for (int col = 0; col < 2; col++)
+                    {
+                        dense_sweep<false, double>(e64, f64, sub_m(k), C.nx, C.ny, C.nz, h2, col,
+                                                   false, tid, NT);
+                        __syncthreads();
+                    }
+                float *ek = sub_e(k);
+                const unsigned char *mk = sub_m(k);
+                for (long t = tid; t < P; t += NT)
+                    if (mk[t])
+                        ek[t] = (float)e64[t];
+                __syncthreads();
+            }
+            for (int k = N.nlev - 2; k >= ks; k--)
+            {
+                const NmgLev C = N.lv[k], D = N.lv[k + 1];
+                dense_prolong<false, false>(sub_e(k), sub_m(k), C.nx, C.ny, C.nz, sub_e(k + 1), D.nx,
+                                            D.ny, tid, NT);
+                __syncthreads();
+                for (int sw = 0; sw < A.n_post; sw++)
+                    for (int col = 0; col < 2; col++)
+                    {
+                        dense_sweep<false, float>(sub_e(k), sub_f(k), sub_m(k), C.nx, C.ny, C.nz,
+                                                  N.h2[k], col, false, tid, NT);
+                        __syncthreads();
+                    }
+            }
+            {
+                const NmgLev C = N.lv[ks];
+                const long P = (long)C.nx * C.ny * C.nz;
+                const float *sek = sub_e(ks);
+                const unsigned char *smk = sub_m(ks);
+                float *gek = A.ec + C.off;
+                for (long t = tid; t < P; t += NT)
+                    if (smk[t])
+                        __stcg(gek + t, sek[t]);
+            }
+        }
+        cluster.sync();
+        for (int k = N.nsmall - 1; k >= 1; k--)
+        {
+            const NmgLev C = N.lv[k], D = N.lv[k + 1];
+            dense_prolong<true, true>(A.ec + C.off, A.mc + C.off, C.nx, C.ny, C.nz, A.ec + D.off,
+                                      D.nx, D.ny, ct, CT);
+            cluster.sync();
+            for (int sw = 0; sw < A.n_post; sw++)
+                for (int col = 0; col < 2; col++)
+                {
+                    dense_sweep<true, float>(A.ec + C.off, A.fc + C.off, A.mc + C.off, C.nx, C.ny,
+                                             C.nz, N.h2[k], col, false, ct, CT);
+                    cluster.sync();
+                }
+        }
+        {
+            // prolongation to the fine unknowns (this CTA's slice of the list)
+            const NmgLev D = N.lv[1];
+            const float *e1 = A.ec + D.off;
+            for (int e = sb + tid; e < se; e += NT)
+            {
+                const int v = A.cl[e];
+                const long g = v < 0 ? ~v : v;
+                long l = g - N.goff;
+                const int z = (int)(l / sz0);
+                l -= z * sz0;
+                const int y = (int)(l / sy0);
+                const int x = (int)(l - y * sy0);
+                __stcg(A.ef + g, ldg_f(A.ef + g) + prolong_at<true>(e1, D.nx, D.ny, x, y, z));
+            }
+        }
+        cluster.sync();
+        for (int sw = 0; sw < A.n_post; sw++)
+            for (int col = 0; col < 2; col++)
+            {
+                fine_sweep(col, false);
+                cluster.sync();
+            }
+        it++;
+    }
+    // the iterate that passed the test is in bufs[(it + 1) & 1]
+    if ((it + 1) & 1)
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            const long g = v < 0 ? ~v : v;
+            A.pot[g] = ldg_d(A.pot_old + g);
+        }
+    if (rank == 0 && tid == 0)
+    {
+        A.status[2 * ent] = conv ? 1 : 0;
+        A.status[2 * ent + 1] = it;
+    }
+    // no CTA leaves while another may still read its partials
+    cluster.sync();
+}
+
+// ---- host ---------------------------------------------------------------------------------
+struct NodeMgBufs {
+    DBuf<NmgNode> tab;
+    DBuf<int> cl, status;
+    DBuf<float> ef, rf, ec, fc;
+    DBuf<unsigned char> msk, mc;
+};
+
+struct NodeMgState {
+    NodeMgBufs lv[AMR_MAX_LEVELS]; // one set per refinement level (each keeps its sizes)
+};
+
+static NodeMgBufs &bufs_of(qz_sim *s, int level)
+{
+    if (!s->node_mg)
+        s->node_mg = new NodeMgState();
+    return s->node_mg->lv[level];
+}
+
+// Cluster size and dynamic shared memory of the launch (set once).
+static int cluster_size(size_t smem)
+{
+    static int cs = 0;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        cudaFuncSetAttribute((const void *)k_node_mg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)NMG_SMEM_MAX);
+        cudaFuncSetAttribute((const void *)k_node_mg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        for (int c : {16, 8, 4, 2, 1})
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(c);
+            cfg.blockDim = dim3(NMG_THREADS);
+            cfg.dynamicSmemBytes = NMG_SMEM_MAX;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = c;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, (const void *)k_node_mg, &cfg) == cudaSuccess &&
+                n > 0)
+            {
+                cs = c;
+                break;
+            }
+        }
+        cudaGetLastError();
+    });
+    (void)smem;
+    return cs;
+}
+
+int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
+{
+    const qz_config &c = s->cfg;
+    NodeMgBufs &B = bufs_of(s, level_index);
+    std::vector<NmgNode> tab;
+    long coarse = 0;
+    size_t smem = 0;
+    for (int q = 0; q < L.nnodes; q++)
+    {
+        const AmrNode &nd = L.h[q];
+        if (nd.nintr <= 0)
+            continue;
+        NmgNode N;
+        memset(&N, 0, sizeof N);
+        N.q = q;
+        N.ib = nd.intr_off;
+        N.ie = nd.intr_off + nd.nintr;
+        N.goff = nd.grid_off;
+        const double H = 1.0 / (1 << nd.lv);
+        N.oh2 = 1.0 / (H * H);
+        const double rm = 4.0 * c.G * QZ_PI_NMG * nd.mass / (nd.ncells * H * H * H);
+        const double tt = c.tol * rm;
+        N.thr = nd.nintr * tt * tt;
+        if (c.check_method == 2)
+            N.thr = N.thr * (cbrt((double)nd.nintr) * cbrt((double)nd.nintr));
+        N.rmt = c.tol * rm;
+        N.cap = c.max_iter;
+        int cx = nd.rd[0], cy = nd.rd[1], cz = nd.rd[2];
+        int k = 0;
+        for (;;)
+        {
+            N.lv[k].nx = cx + 1;
+            N.lv[k].ny = cy + 1;
+            N.lv[k].nz = cz + 1;
+            N.h2[k] = (float)((H * (1 << k)) * (H * (1 << k)));
+            if (k > 0)
+            {
+                N.lv[k].off = coarse;
+                coarse += (long)(cx + 1) * (cy + 1) * (cz + 1);
+            }
+            if (k >= 1 && (std::max(cx, std::max(cy, cz)) <= 4 || k == NMG_MAXLEV - 1))
+                break;
+            cx = (cx + 1) / 2;
+            cy = (cy + 1) / 2;
+            cz = (cz + 1) / 2;
+            k++;
+        }
+        N.nlev = k + 1;
+        // sub-cycle levels: the longest tail of levels (from level 1 on) that fits
+        const long Plast = (long)N.lv[N.nlev - 1].nx * N.lv[N.nlev - 1].ny * N.lv[N.nlev - 1].nz;
+        int ks = N.nlev - 1;
+        size_t need = 16 * (size_t)Plast + 9 * (size_t)Plast + 64;
+        while (ks > 1)
+        {
+            const long P = (long)N.lv[ks - 1].nx * N.lv[ks - 1].ny * N.lv[ks - 1].nz;
+            if (need + 9 * (size_t)P + 64 > NMG_SMEM_MAX)
+                break;
+            need += 9 * (size_t)P + 64;
+            ks--;
+        }
+        N.nsmall = ks;
+        size_t off = 0;
+        for (int j = ks; j < N.nlev; j++)
+        {
+            N.soff[j] = (int)off;
+            const long P = (long)N.lv[j].nx * N.lv[j].ny * N.lv[j].nz;
+            off += ((9 * (size_t)P + 15) / 16) * 16;
+        }
+        N.coff = (int)off;
+        off += 16 * (size_t)Plast;
+        N.smem_need = (int)off;
+        if (off > NMG_SMEM_MAX)
+        {
+            set_error("node multigrid: the coarse levels of a node need %zu bytes of shared memory",
+                      off);
+            return QZ_FAILURE;
+        }
+        smem = std::max(smem, off);
+        tab.push_back(N);
+    }
+    if (tab.empty())
+        return QZ_SUCCESS;
+    const int nt = (int)tab.size();
+    if (!B.tab.ensure(s->mem, nt) || !B.status.ensure(s->mem, 2L * nt) ||
+        !B.cl.ensure(s->mem, L.intr_total) || !B.ef.ensure(s->mem, L.grid_total) ||
+        !B.rf.ensure(s->mem, L.grid_total) || !B.msk.ensure(s->mem, L.grid_total) ||
+        !B.ec.ensure(s->mem, coarse) || !B.fc.ensure(s->mem, coarse) || !B.mc.ensure(s->mem, coarse))
+    {
+        set_error("node multigrid buffers");
+        return QZ_FAILURE;
+    }
+    const int cs = cluster_size(smem);
+    if (cs < 1)
+    {
+        set_error("node multigrid: no cluster of the kernel can be resident");
+        return QZ_FAILURE;
+    }
+    if (!check_cuda(cudaMemcpyAsync(B.tab.p, tab.data(), nt * sizeof(NmgNode),
+                                    cudaMemcpyHostToDevice, s->stream),
+                    "node multigrid table"))
+        return QZ_FAILURE;
+    cudaMemsetAsync(B.msk.p, 0, L.grid_total, s->stream);
+    cudaMemsetAsync(B.ef.p, 0, L.grid_total * sizeof(float), s->stream);
+    cudaMemsetAsync(B.ec.p, 0, std::max(coarse, 1L) * sizeof(float), s->stream);
+    cudaMemsetAsync(B.mc.p, 0, std::max(coarse, 1L), s->stream);
+    NmgArgs A;
+    A.tab = B.tab.p;
+    A.intr = L.intr.p;
+    A.cl = B.cl.p;
+    A.d = L.d;
+    A.pot = L.pot;
+    A.pot_old = L.pot_old;
+    A.ef = B.ef.p;
+    A.rf = B.rf.p;
+    A.msk = B.msk.p;
+    A.ec = B.ec.p;
+    A.fc = B.fc.p;
+    A.mc = B.mc.p;
+    A.status = B.status.p;
+    A.tol2 = c.tol2;
+    A.method = c.check_method;
+    A.n_pre = std::max(1, c.n_pre);
+    A.n_post = std::max(0, c.n_post);
+
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nt * cs);
+    cfg.blockDim = dim3(NMG_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaEvent_t eb = nullptr, ee = nullptr;
+    if (s->prof)
+    {
+        eb = prof_event(s);
+        ee = prof_event(s);
+        cudaEventRecord(eb, s->stream);
+    }
+    if (!check_cuda(cudaLaunchKernelEx(&cfg, k_node_mg, A), "node multigrid"))
+        return QZ_FAILURE;
+    s->stats.kernel_launches++;
+    if (s->prof)
+    {
+        cudaEventRecord(ee, s->stream);
+        s->prof_pending.push_back({QZ_PROF_NODE_MG, 0.0, eb, ee});
+    }
+    std::vector<int> st(2 * nt);
+    if (!check_cuda(cudaMemcpyAsync(st.data(), B.status.p, 2L * nt * sizeof(int),
+                                    cudaMemcpyDeviceToHost, s->stream),
+                    "node multigrid status") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "node multigrid sync"))
+        return QZ_FAILURE;
+    int worst = 0, unconv = 0;
+    double pts_it = 0.0;
+    for (int e = 0; e < nt; e++)
+    {
+        worst = std::max(worst, st[2 * e + 1]);
+        unconv += st[2 * e] == 0;
+        pts_it += (double)(tab[e].ie - tab[e].ib) * st[2 * e + 1];
+    }
+    s->stats.node_mg_iterations += worst;
+    if (s->prof)
+    {
+        // per fine unknown and iteration: the FP64 pass reads d, phi, e (the 7
+        // stencil values come from cache lines shared with neighbours) and
+        // writes the new phi and r (36 B); each red-black sweep reads e, r and
+        // writes e (12 B); restriction and prolongation about 8 B; the coarse
+        // levels add about a seventh
+        const double sweeps = (double)(A.n_pre + A.n_post);
+        s->prof_pending.back().bytes = pts_it * (36.0 + 12.0 * sweeps + 8.0) * 8.0 / 7.0;
+    }
+    if (unconv)
+    {
+        set_error("the precision was not reached in refinement level %d after %d multigrid "
+                  "iterations (%d nodes)",
+                  level_index, worst, unconv);
+        return QZ_FAILURE;
+    }
+    return check_cuda(cudaGetLastError(), "node multigrid") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+void node_mg_free(qz_sim *s)
+{
+    if (!s->node_mg)
+        return;
+    for (auto &B : s->node_mg->lv)
+    {
+        B.tab.release(s->mem);
+        B.cl.release(s->mem);
+        B.status.release(s->mem);
+        B.ef.release(s->mem);
+        B.rf.release(s->mem);
+        B.ec.release(s->mem);
+        B.fc.release(s->mem);
+        B.msk.release(s->mem);
+        B.mc.release(s->mem);
+    }
+    delete s->node_mg;
+    s->node_mg = nullptr;
+}
+
+} // namespace qz

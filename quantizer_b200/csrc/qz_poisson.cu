@@ -751,6 +751,16 @@ template <typename T> struct MgArgs {
     int smem;                // the small levels live in block 0's shared memory
     int soff[MG_MAXLEV];     // their offsets there (phi, then rho), in elements
     GridBar bar;
+    // mixed form with the convergence test inside the launch (poisson_error.c:
+    // 36-133 on the fine interior, evaluated before each iteration's cycle from
+    // the second on; pot_old holds the previous iterate)
+    int check;
+    double *pold;           // FP64 pot_old, the layout of fphi's array
+    double *part;           // per block: residual partial [b], flags [QZ_CG_PART_MAX + b]
+    int *outst;             // [0] iterations run, [1] converged
+    double tm, tp, rm, tol; // 1 -/+ tol2, 4 pi G rho_mean, tol
+    int method;
+    long nintr;
 };
 
 // Work item t = a + n0 (b + n1 c) of a grid-stride loop (t = tid, tid + stride,
@@ -1056,6 +1066,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             float *rf = (float *)A.rho[0].p, *ef = (float *)A.phi[0].p;
             for (unsigned t = gtid; t < n3; t += gn)
                 ef[t] = 0.0f;
+            double acc = 0.0;
+            int fl = 0; // 1 ratio test failed, 2 point residual test failed (method 1)
             for (Walk3 x(gtid, gn, um, um); x.c < um; x.next())
             {
                 const int i = 1 + (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
@@ -1065,8 +1077,93 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
                 const double r = R.p[gr] + ooh2 * (6.0 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + P.sy] -
                                                    p[gp - P.sy] - p[gp + P.sz] - p[gp - P.sz]);
                 rf[i + (long)j * n + (long)k * n * n] = (float)r;
+                if (A.check)
+                {
+                    // k_check_partial's tests on the same points, then pot_old = phi
+                    const double pv = p[gp];
+                    const double a = pv / A.pold[gp];
+                    if ((A.tm > a) || (A.tp < a))
+                        fl |= 1;
+                    A.pold[gp] = pv;
+                    if (A.method == 1)
+                    {
+                        if (fabs(r) / A.rm >= A.tol)
+                            fl |= 2;
+                    }
+                    else
+                        acc += r * r;
+                }
+            }
+            if (A.check)
+            {
+                for (int o = 16; o > 0; o >>= 1)
+                    acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)fl);
+                __shared__ double wacc[MG_THREADS / 32];
+                __shared__ int wfl[MG_THREADS / 32];
+                if ((threadIdx.x & 31) == 0)
+                {
+                    wacc[threadIdx.x >> 5] = acc;
+                    wfl[threadIdx.x >> 5] = fl;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0)
+                {
+                    double t = 0.0;
+                    int f = 0;
+                    for (int w = 0; w < MG_THREADS / 32; w++)
+                    {
+                        t += wacc[w];
+                        f |= wfl[w];
+                    }
+                    A.part[blockIdx.x] = t;
+                    A.part[QZ_CG_PART_MAX + blockIdx.x] = (double)f;
+                }
             }
             gsync();
+            if (A.check)
+            {
+                // every block adds the partials in the same order: the same decision
+                __shared__ int s_stop;
+                if (threadIdx.x < 32)
+                {
+                    double t = 0.0;
+                    int f = 0;
+                    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
+                    {
+                        t += __ldcg(A.part + b);
+                        f |= (int)__ldcg(A.part + QZ_CG_PART_MAX + b);
+                    }
+                    for (int o = 16; o > 0; o >>= 1)
+                        t += __shfl_xor_sync(0xffffffffu, t, o);
+                    f = (int)__reduce_or_sync(0xffffffffu, (unsigned)f);
+                    if (threadIdx.x == 0)
+                    {
+                        int ok;
+                        if (A.method == 1)
+                            ok = !(f & 2);
+                        else
+                        {
+                            double err = t / A.nintr;
+                            err = sqrt(err);
+                            err = err / A.rm;
+                            if (A.method == 2)
+                                err = err / (cbrt((double)A.nintr) * cbrt((double)A.nintr));
+                            ok = err < A.tol;
+                        }
+                        s_stop = it > 0 && !(f & 1) && ok;
+                        if (s_stop && blockIdx.x == 0)
+                        {
+                            A.outst[0] = it;
+                            A.outst[1] = 1;
+                        }
+                    }
+                }
+                __syncthreads();
+                if (s_stop)
+                    return;
+                // the partials are rewritten only after the next iteration's barriers
+            }
         }
         // levels above the small ones: grid-wide phases
         for (int l = 0; l < A.nsmall; l++)
@@ -1143,6 +1240,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
             gsync();
         }
     }
+    if (A.check && gtid == 0)
+    {
+        A.outst[0] = A.iters;
+        A.outst[1] = 0;
+    }
 }
 
 // True when the head solve runs as persistent launches (red-black Gauss-Seidel
@@ -1155,7 +1257,7 @@ bool mg_persistent(const qz_sim *s)
            !s->fused_rb && (int)s->levels.size() <= MG_MAXLEV;
 }
 
-template <typename T> static int mg_launch(qz_sim *s, int iters)
+template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = false)
 {
     const qz_config &c = s->cfg;
     MgArgs<T> A;
@@ -1185,6 +1287,27 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     A.frho = s->fine_rho;
     A.bar = GridBar{s->gbar, s->flags};
     cudaMemsetAsync(s->gbar, 0, 4 * sizeof(unsigned), s->stream);
+    A.check = check && A.mixed ? 1 : 0;
+    if (A.check)
+    {
+        const int L = s->L;
+        const int nc = 1 << L;
+        const double H = 1.0 / nc;
+        A.pold = s->pot_old;
+        A.part = s->mg_part;
+        A.outst = reinterpret_cast<int *>(s->mg_part + 2 * QZ_CG_PART_MAX);
+        A.tm = 1.0 - c.tol2;
+        A.tp = 1.0 + c.tol2;
+        A.rm = 4.0 * c.G * QZ_PI_D * s->head_mass / ((double)nc * nc * nc * H * H * H);
+        A.tol = c.tol;
+        A.method = c.check_method;
+        A.nintr = (long)(nc - 1) * (nc - 1) * (nc - 1);
+        if (!s->mg_part)
+        {
+            set_error("mixed multigrid: partial-sum buffer missing");
+            return QZ_FAILURE;
+        }
+    }
     // shared memory for the small levels (phi and rho of each)
     long elems = 0;
     for (int l = A.nsmall; l < A.nlev; l++)
@@ -1241,7 +1364,7 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     if (A.mixed)
     {
         const double m = s->fine_phi.n - 2;
-        bytes += 40.0 * m * m * m;
+        bytes += (A.check ? 56.0 : 40.0) * m * m * m; // the test reads and writes pot_old
     }
     void *args[] = {&A};
     cudaEvent_t eb = nullptr, ee = nullptr;
@@ -1260,6 +1383,19 @@ template <typename T> static int mg_launch(qz_sim *s, int iters)
     {
         cudaEventRecord(ee, s->stream);
         s->prof_pending.push_back({QZ_PROF_SMOOTH, bytes * iters, eb, ee});
+    }
+    if (A.check)
+    {
+        // iterations run and the test's outcome; the profiler's bytes follow the count
+        int st[2] = {0, 0};
+        if (!check_cuda(cudaMemcpyAsync(st, A.outst, sizeof st, cudaMemcpyDeviceToHost, s->stream),
+                        "multigrid result") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "multigrid result"))
+            return QZ_FAILURE;
+        s->mg_ran = st[0];
+        s->mg_conv = st[1];
+        if (s->prof)
+            s->prof_pending.back().bytes = bytes * st[0];
     }
     return QZ_SUCCESS;
 }
@@ -1641,9 +1777,31 @@ int potential_head(qz_sim *s)
     sync_fine_alt(s);
     int iter = 0;
     bool check = false;
-    const int every = c.check_every > 0 ? c.check_every : 1;
+    // the mixed form tests after every defect-correction iteration (its FP64
+    // residual is computed anyway); the FP64 form keeps the reference's cadence
+    const int every =
+        c.precision == QZ_PREC_MIXED ? 1 : (c.check_every > 0 ? c.check_every : 1);
     const bool graphs = s->use_graphs && !s->prof;
-    if (mg_persistent(s))
+    if (mg_persistent(s) && c.precision == QZ_PREC_MIXED)
+    {
+        // mixed form: one launch runs the defect-correction iterations and takes the
+        // convergence test (FP64) before every iteration's cycle from the second on
+        if (mg_launch<float>(s, c.max_iter, true))
+            return QZ_FAILURE;
+        if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
+                                        cudaMemcpyDeviceToHost, s->stream),
+                        "flags") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "flags"))
+            return QZ_FAILURE;
+        if (s->h_flags[F_ERROR] & E_BARRIER)
+        {
+            set_error("multigrid cycles: a grid barrier wait gave up");
+            return QZ_FAILURE;
+        }
+        iter = s->mg_ran;
+        check = s->mg_conv != 0;
+    }
+    else if (mg_persistent(s))
     {
         // one cooperative launch per check block, then the convergence test
         while (iter < c.max_iter && !check)

@@ -29,6 +29,11 @@ sources (oracle/Makefile, target ``ref``):
 * ``arrays.npz`` -- direct calls into oracle/_ref/libqzref.so of the
   reference's gauss_saidel, jacobi (odd sweep count), conjugate_gradient_multigrid
   and multigrid (V, F and W cycles) on seeded random arrays.
+* ``node_cg.npz`` -- the reference's conjugate_gradient(struct node *)
+  (force_methods/conjugate_gradient.c:322-463) called through libqzref.so on a
+  synthetic node: a 30 x 32 x 34-cell box at level 7 whose interior points
+  fill an ellipsoid, a smooth positive density, boundary values of -GM/r;
+  inputs and the pot / pot_old it leaves.
 
 Run in a container that has the reference source tree:
     python tests/golden/make_golden.py [fixture-name ...]   (default: all)
@@ -158,6 +163,98 @@ def arrays_case() -> None:
     print("wrote arrays.npz")
 
 
+def node_struct():
+    """ctypes mirror of struct node (headers/initialize_node.h:63-216), the layout
+    quantizer_b200/csrc/qz_ref_abi.h declares."""
+    I, D, B, PI, PD = C.c_int, C.c_double, C.c_bool, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    V = C.c_void_p
+    fields = [("ID", I), ("lv", I), ("ptr_box", PI), ("ptr_box_old", PI), ("box_cap", I)]
+    fields += [(f"box_real_dim_{a}", I) for a in "xyz"] + [(f"box_dim_{a}", I) for a in "xyz"]
+    fields += [(f"box_ts_{a}", I) for a in "xyz"] + [(f"box_min_{a}", I) for a in "xyz"]
+    fields += [(f"box_max_{a}", I) for a in "xyz"] + [("box_check_fit", B)]
+    fields += [("ptr_cell_idx_x", PI), ("ptr_cell_idx_y", PI), ("ptr_cell_idx_z", PI),
+               ("ptr_box_idx", PI), ("cell_cap", I), ("cell_size", I), ("ptr_cell_struct", V),
+               ("ptr_cell_struct_old", V), ("cell_struct_old_cap", I), ("node_mass", D),
+               ("no_ptcl_full_node", I), ("no_ptcl_outs_ref_zones", I)]
+    for w in ("intr", "bdry", "sim_bdry"):
+        fields += [(f"ptr_{w}_grid_cell_idx_{a}", PI) for a in "xyz"]
+        fields += [(f"ptr_{w}_box_grid_idx", PI), (f"grid_{w}_cap", I), (f"grid_{w}_size", I)]
+    fields += [(f"ptr_{f}", PD) for f in ("pot", "pot_old", "ax", "ay", "az", "d")]
+    fields += [("grid_properties_cap", I), ("pptr_chn", V), ("ptr_pt", V), ("chn_cap", I),
+               ("chn_size", I), ("ptr_cell_ref", PI), ("cell_ref_cap", I), ("cell_ref_size", I),
+               ("pptr_zones", V), ("zones_cap", I), ("zones_size", I), ("ptr_zone_cap", PI),
+               ("ptr_zone_size", PI), ("ptr_aux_idx", PI), ("aux_idx_cap", I)]
+    fields += [(f"ptr_pbc_bool_bdry_anomalies_{a}", V) for a in "xyz"]
+    fields += [("pbc_bool_bdry_anomalies_cap", I)]
+    fields += [(f"ptr_pbc_min_subzones_{a}", PI) for a in "xyz"]
+    fields += [(f"ptr_pbc_max_subzones_{a}", PI) for a in "xyz"]
+    fields += [("pbc_subzones_cap", I), ("pbc_subzones_size", I)]
+    fields += [(f"ptr_links_{k}", PI) for k in ("old_ord_old", "new_ord_new", "new_ord_old",
+                                                 "old_ord_new")]
+    fields += [("links_cap", I)]
+    fields += [(n, B) for n in ("sim_bdry_contact", "sim_bdry_contact_x", "sim_bdry_contact_y",
+                                "sim_bdry_contact_z", "pbc_crosses_sim_box_bdry",
+                                "pbc_crosses_sim_box_bdry_x", "pbc_crosses_sim_box_bdry_y",
+                                "pbc_crosses_sim_box_bdry_z", "pbc_crosses_whole_sim_box",
+                                "pbc_crosses_whole_sim_box_x", "pbc_crosses_whole_sim_box_y",
+                                "pbc_crosses_whole_sim_box_z", "pbc_correction_due_pbc_flag")]
+
+    class Node(C.Structure):
+        _fields_ = fields
+    return Node
+
+
+def node_cg_case() -> None:
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libqzref.so"))
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)
+    try:
+        lib.global_variables()
+    finally:
+        os.dup2(saved, 1)
+    Node = node_struct()
+    lv, rd = 7, (30, 32, 34)
+    sx, sy, sz = rd[0] + 1, rd[1] + 1, rd[2] + 1
+    H = 1.0 / (1 << lv)
+    gz, gy, gx = np.meshgrid(np.arange(sz), np.arange(sy), np.arange(sx), indexing="ij")
+    c = np.array([rd[0] / 2, rd[1] / 2, rd[2] / 2])
+    q = ((gx - c[0]) / 12.0) ** 2 + ((gy - c[1]) / 13.0) ** 2 + ((gz - c[2]) / 14.0) ** 2
+    inside = (q < 1.0) & (gx > 0) & (gy > 0) & (gz > 0) & (gx < rd[0]) & (gy < rd[1]) & (gz < rd[2])
+    intr = np.flatnonzero(inside.ravel()).astype(np.int32)
+    # level coordinates: the box starts at cell 40 of the level (centre of mass near 0.5)
+    X = (gx + 49) * H - 0.5
+    Y = (gy + 48) * H - 0.5
+    Z = (gz + 47) * H - 0.5
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    d = (4.0 * np.pi * 3.0 / (4.0 * np.pi * 0.05 ** 3) * (1 + (r / 0.05) ** 2) ** -2.5).ravel()
+    d = np.where(inside.ravel(), d, 0.0)
+    pot = (-1.0 / np.sqrt(r * r + 0.05 ** 2)).ravel().copy()
+    pot_old = pot.copy()
+    out = {"rd": np.array(rd, dtype=np.int32), "lv": np.array([lv]), "intr": intr,
+           "d": d.copy(), "pot_in": pot.copy()}
+    cells = int(np.count_nonzero(inside)) // 2 + 1
+    mass = 0.7
+    nd = Node()
+    nd.ID, nd.lv = 1, lv
+    nd.box_real_dim_x, nd.box_real_dim_y, nd.box_real_dim_z = rd
+    nd.grid_intr_size = intr.size
+    nd.ptr_intr_box_grid_idx = intr.ctypes.data_as(C.POINTER(C.c_int))
+    nd.ptr_d = d.ctypes.data_as(C.POINTER(C.c_double))
+    nd.ptr_pot = pot.ctypes.data_as(C.POINTER(C.c_double))
+    nd.ptr_pot_old = pot_old.ctypes.data_as(C.POINTER(C.c_double))
+    nd.grid_properties_cap = sx * sy * sz
+    nd.node_mass = mass
+    nd.cell_size = cells
+    lib.conjugate_gradient.argtypes = [C.POINTER(Node)]
+    lib.conjugate_gradient.restype = C.c_int
+    rc = lib.conjugate_gradient(C.byref(nd))
+    out.update(rc=np.array([rc]), mass=np.array([mass]), cells=np.array([cells]),
+               pot_out=pot, pot_old_out=pot_old)
+    np.savez_compressed(os.path.join(HERE, "node_cg.npz"), **out)
+    print("wrote node_cg.npz", rc, intr.size)
+
+
 def main() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     want = set(sys.argv[1:])
@@ -183,6 +280,8 @@ def main() -> None:
         timestep_case(ic, dt)
     if not want or "arrays.npz" in want:
         arrays_case()
+    if not want or "node_cg.npz" in want:
+        node_cg_case()
 
 
 if __name__ == "__main__":

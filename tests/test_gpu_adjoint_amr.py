@@ -144,3 +144,18 @@ def test_adjoint_trajectory_with_refinement_against_finite_differences():
         cm["m"][p] -= em
         fd = (loss(cp, cp) - loss(cm, cm)) / (2 * em)
         assert abs(fd - g["gm"][p]) <= 1e-5 * mscale, (p, fd, g["gm"][p])
+
+
+def test_force_vjp_with_refinement_is_bit_reproducible():
+    # every sum of the pull-back has a fixed order (the parent-average transposes
+    # add their contributions sorted by parent point): two calls agree bit for bit
+    ic = _ic(seed=9)
+    n = ic["x"].size
+    ab = np.random.default_rng(2).standard_normal((3, n))
+    out = []
+    for _ in range(2):
+        with core.Simulation(ic, L, **TOL) as sim:
+            sim.init_forces()
+            out.append(sim.force_vjp(ab[0], ab[1], ab[2]))
+    for k in ("gx", "gy", "gz", "gm"):
+        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)

@@ -11,6 +11,11 @@
   leapfrog step.
 * The 4.2 M-particle merger on a 256^3 head with four levels: two steps run,
   the tree has its five levels, momentum is conserved to the same bound.
+* The same merger against the compiled reference (all host threads) after the
+  step-0 forces and one step: head potential 1e-9 of its largest value,
+  particle accelerations 1e-6 of the largest, positions 1e-10 box units; at
+  step 0 every node's geometry and particle count equal the reference's, after
+  the step the nodes per level, the particles per node and the refined cells.
 """
 import os
 
@@ -89,3 +94,47 @@ def test_merger_two_steps():
     dp = np.abs(_momentum(p, m) - _momentum(ic, m)).max()
     assert dp < 1e-3 * vscale * m.sum()
     assert np.all((p["x"] > 0) & (p["x"] < 1))
+
+
+def test_merger_one_step_against_reference(tmp_path):
+    lmin, lmax, rp = 8, 12, 9
+    ic = ics.merger(2097152, a=0.03, seed=1)
+    dt = 1e-3 * ics.crossing_time(0.03)
+    out = str(tmp_path)
+    path = os.path.join(out, "ic.bin")
+    ics.write_ic(path, ic)
+    O.run_reference(path, out, steps=1, dt=dt, dump="0,1", lmin=lmin, lmax=lmax, ref_ptcl=rp,
+                    threads=os.cpu_count() or 1)
+    ref0, ref1 = O.read_nodes(out, 0), O.read_nodes(out, 1)
+    with core.Simulation(ic, lmin, lmax=lmax, ref_ptcl=rp) as sim:
+        sim.init_forces()
+        p0 = sim.particles()
+        pot0 = sim.field("pot")
+        assert sim.levels() == max(nd["level"] for nd in ref0) + 1 == 5
+        for nd in ref0:
+            if nd["level"] == 0:
+                continue
+            info = sim.node_info(nd["level"], nd["idx"])
+            for k in ("ts", "rd", "bmin", "bmax", "ncells", "nintr", "nbdry", "nsimb", "nptcl"):
+                assert info[k] == nd[k], (nd["level"], nd["idx"], k, info[k], nd[k])
+        sim.step(dt, 1)
+        p1 = sim.particles()
+        for L in range(1, sim.levels()):
+            theirs = [nd for nd in ref1 if nd["level"] == L]
+            assert sim.num_nodes(L) == len(theirs), L
+            mine_n = sorted(sim.node_info(L, i)["nptcl"] for i in range(sim.num_nodes(L)))
+            assert mine_n == sorted(nd["nptcl"] for nd in theirs), L
+            mine = set()
+            for i in range(sim.num_nodes(L)):
+                mine |= set(map(tuple, sim.node_cells(L, i)))
+            cells = set()
+            for nd in theirs:
+                cx = [O.node_dump(out, 1, L, nd["idx"], c) for c in ("cx", "cy", "cz")]
+                cells |= set(zip(*[v.tolist() for v in cx]))
+            assert mine == cells, L
+    assert _rel(pot0, O.read_dump(out, 0, "pot")) < 1e-9
+    for k in ("ax", "ay", "az"):
+        assert _rel(p0[k], O.read_dump(out, 0, k)) < 1e-6, k
+        assert _rel(p1[k], O.read_dump(out, 1, k)) < 1e-6, k
+    for k in ("x", "y", "z"):
+        assert np.abs(p1[k] - O.read_dump(out, 1, k)).max() < 1e-10, k
