@@ -364,22 +364,29 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     for k in ("x", "y", "z"):
         pert[k] = pert[k] + rng.normal(0.0, 1e-3, n)
 
-    def forward(c, steps, base=None):
+    def forward(c, steps, base=None, record=False, replay=None):
         # a frozen tree is built at `base` (the unperturbed positions) and the run
-        # starts from `c` on it, as the gradient assumes
+        # starts from `c` on it, as the gradient assumes.  record / replay: the
+        # solver schedule (iteration count of every Poisson solve), so that the
+        # +eps and -eps runs apply the same map as the unperturbed run
         with core.Simulation(c if base is None else base, L, **cfg) as sm:
+            if record:
+                sm.record_schedule()
+            if replay is not None:
+                sm.replay_schedule(replay)
             sm.init_forces()
             if base is not None:
                 sm.set_particles(c)
                 sm.init_forces()
             sm.step(dt, steps)
-            return sm.particles()
+            sched = sm.take_schedule() if record else None
+            return sm.particles(), sched
 
-    pt = forward(pert, K, ic if wl["levels"] > 0 else None)
+    pt, _ = forward(pert, K, ic if wl["levels"] > 0 else None)
     tgt = {k: pt[k] for k in ("x", "y", "z")}
 
-    def loss_of(c, base=None):
-        p = forward(c, K, base)
+    def loss_of(c, base=None, replay=None):
+        p, _ = forward(c, K, base, replay=replay)
         d = sum((p[k] - tgt[k]) ** 2 for k in ("x", "y", "z"))
         return float(d.sum() / n)
 
@@ -421,6 +428,8 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
     kinds = kinds[:wl["fd_coords"]]
     picks = rng.choice(n, len(kinds), replace=False)
     errs, rels = [], []
+    # the unperturbed run's solver schedule: every +-eps run replays it
+    _, sched = forward(ic, K, ic if wl["levels"] > 0 else None, record=True)
     for (field, key, eps), p in zip(kinds, picks):
         h = eps if eps is not None else 1e-3 * ic["m"][p]
         cp, cm = {k: v.copy() for k, v in ic.items()}, {k: v.copy() for k, v in ic.items()}
@@ -431,9 +440,9 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
             # masses (the total mass and the shell follow them; the tree is ic's)
             bp = cp if field == "m" else ic
             bm = cm if field == "m" else ic
-            fd = (loss_of(cp, bp) - loss_of(cm, bm)) / (2 * h)
+            fd = (loss_of(cp, bp, sched) - loss_of(cm, bm, sched)) / (2 * h)
         else:
-            fd = (loss_of(cp) - loss_of(cm)) / (2 * h)
+            fd = (loss_of(cp, replay=sched) - loss_of(cm, replay=sched)) / (2 * h)
         scale = float(np.abs(g[key]).max())
         errs.append(abs(fd - g[key][p]) / scale)
         rels.append(abs(fd - g[key][p]) / max(abs(fd), 1e-300))
@@ -461,7 +470,8 @@ def run_adjoint(args, wl: dict, K: int, W: int) -> int:
                                        "median_err_over_gradient_max": float(np.median(errs)),
                                        "median_rel_err": float(np.median(rels)),
                                        "max_rel_err": float(max(rels)),
-                                       "eps": "1e-6 (x, v), 1e-3 m_p (m)"},
+                                       "eps": "1e-6 (x, v), 1e-3 m_p (m)",
+                                       "solver_schedule": "replayed from the unperturbed run"},
                 "gpu_launches": int(st1.kernel_launches - st0.kernel_launches) // 2,
                 "clocks": clk.summary(), "cpu_baseline": None}
         print(json.dumps(line), flush=True)

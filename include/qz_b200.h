@@ -310,6 +310,17 @@ QZ_API int qz_snapshot_wait(qz_sim *sim);
  * order (reproducible; equal to the reference's to rounding). */
 QZ_API int qz_observables(qz_sim *sim, int potential_type, const double *units, double *out);
 
+/* Solver schedule, for finite-difference checks of the adjoint.  A forward
+ * Poisson solve normally stops at the reference's convergence test, so runs
+ * from slightly different inputs can stop after different iteration counts and
+ * the map from inputs to outputs jumps.  mode 1 starts recording the count of
+ * every forward solve (the head: its cycles; a refinement level: one count per
+ * node); mode 0 stops and copies up to cap counts to counts (*len = how many
+ * were recorded); mode 2 replays counts[0..cap): every forward solve runs
+ * exactly its recorded count with no convergence test, in the recorded order
+ * (a run with more solves than recorded fails). */
+QZ_API int qz_solve_schedule(qz_sim *sim, int mode, int *counts, long cap, long *len);
+
 /* Synchronise the library stream and report statistics. */
 QZ_API int qz_synchronize(qz_sim *sim);
 QZ_API int qz_get_stats(qz_sim *sim, qz_stats *out);

@@ -135,6 +135,7 @@ def load() -> C.CDLL:
         "qz_amr_node_list": ([vp, C.c_int, C.c_int, C.c_int, _I], C.c_int),
         "qz_amr_node_field": ([vp, C.c_int, C.c_int, C.c_int, _P], C.c_int),
         "qz_test_scan": ([vp, _I, _I, C.c_long, C.c_int, C.c_uint], C.c_int),
+        "qz_solve_schedule": ([vp, C.c_int, _I, C.c_long, C.POINTER(C.c_long)], C.c_int),
         "qz_node_conjugate_gradient": ([vp] + [C.c_int] * 5 + [_I, C.c_double, C.c_int] +
                                        [_P] * 3, C.c_int),
         "qz_test_wait_gives_up": ([vp, C.c_int, _I], C.c_int),
@@ -370,6 +371,24 @@ class Simulation:
         out["loss"] = st.loss
         out["stats"] = {f: getattr(st, f) for f, _ in AdjointStats._fields_}
         return out
+
+    # -- solver schedule (finite-difference checks) ---------------------------------
+    def record_schedule(self) -> None:
+        """Record the iteration count of every forward Poisson solve from now on."""
+        _check(self.lib.qz_solve_schedule(self.h, 1, None, 0, None))
+
+    def take_schedule(self) -> np.ndarray:
+        """Stop recording (or replaying) and return the recorded counts."""
+        n = C.c_long()
+        _check(self.lib.qz_solve_schedule(self.h, 0, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        _check(self.lib.qz_solve_schedule(self.h, 0, _p(out), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def replay_schedule(self, counts) -> None:
+        """Every forward solve from now on runs exactly the next recorded count."""
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        _check(self.lib.qz_solve_schedule(self.h, 2, _p(c), c.size, None))
 
     def step(self, dt: float, nsteps: int = 1) -> None:
         _check(self.lib.qz_step(self.h, dt, nsteps))

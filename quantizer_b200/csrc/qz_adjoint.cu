@@ -1081,7 +1081,7 @@ static int adj_level_deposit(qz_sim *s, int l, const double *x, const double *y,
         bits++;
     unsigned *ks;
     int *perm;
-    if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm))
+    if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm, 0u))
         return QZ_FAILURE;
     if (!A.cs.ensure(s->mem, 24 * m + 24))
         return QZ_FAILURE;

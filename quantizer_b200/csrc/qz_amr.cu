@@ -1179,7 +1179,7 @@ __global__ void k_node_mass(int nn, AmrNode *nodes, const int *__restrict__ seg_
 }
 
 int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
-                     unsigned **ks_out, int **perm_out); // qz_particles.cu
+                     unsigned **ks_out, int **perm_out, unsigned morton_B); // qz_particles.cu
 
 int amr_deposit(qz_sim *s)
 {
@@ -1212,7 +1212,7 @@ int amr_deposit(qz_sim *s)
             bits++;
         unsigned *ks;
         int *perm;
-        if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm))
+        if (deposit_segments(s, m, bits, L.cell_seg.p, L.box_total, &ks, &perm, 0u))
             return QZ_FAILURE;
         if (!s->seg_mass.ensure(s->mem, m + 1))
         {
@@ -1361,6 +1361,8 @@ struct CgArgs {
     int max_iter;
     int method; // check_method 0/1/2 of conj_grad_error (poisson_error.c:235-282)
     const double *thr_node; // per node r.r threshold in place of the mass-based one (or null)
+    const int *cap_node;    // per node iteration count in place of the cap, with no
+                            // convergence (a replayed schedule), or null
 };
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
@@ -1528,6 +1530,11 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             x.thr = A.thr_node[C.node];
         const long size = (long)(N.rd[0] + 1) * (N.rd[1] + 1) * (N.rd[2] + 1);
         x.cap = (int)(size < A.max_iter ? size : A.max_iter);
+        if (A.cap_node)
+        {
+            x.cap = A.cap_node[C.node];
+            x.thr = -1.0; // r.r < -1 never holds: the node runs exactly cap iterations
+        }
         x.rs_prev = x.rs_cur = 0.0;
         x.done = 0;
         slot[s] = x;
@@ -2302,7 +2309,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], (const void *)k_cg1_nodes,
                                                       CG_MAX_THREADS, kCgSmem);
     });
-    const int per_sm = occ[(c.cg_variant == 1 && !ov) ? 1 : 0];
+    const int per_sm = occ[(c.cg_variant == 1 && !ov && s->sched_mode != 2) ? 1 : 0];
     if (per_sm < 1)
     {
         set_error("conjugate gradient kernel cannot be resident");
@@ -2328,15 +2335,38 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         node_chunk[2 * q + 1] = (int)L.hchunks.size();
     }
     L.nchunks = (int)L.hchunks.size();
+    // solver schedule (forward solves only): replay gives every node its recorded count
+    const bool replay = !ov && s->sched_mode == 2;
+    const bool record = !ov && s->sched_mode == 1;
+    std::vector<int> caps;
+    if (replay)
+    {
+        if (!sor_nodes.empty())
+        {
+            set_error("a solver schedule cannot replay red-black SOR nodes");
+            return QZ_FAILURE;
+        }
+        caps.resize(nn);
+        if (!sched_take(s, nn, caps.data()))
+            return QZ_FAILURE;
+    }
     if (!sor_nodes.empty() && sor_level(s, L, level_index, sor_nodes))
         return QZ_FAILURE;
     if (L.nchunks == 0)
+    {
+        if (record)
+        {
+            std::vector<int> z(nn, 0);
+            sched_put(s, z.data(), nn);
+        }
         return QZ_SUCCESS;
+    }
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
-    const bool one = c.cg_variant == 1 && !ov; // the overrides are the two-phase kernel's
+    // the overrides and replayed schedules are the two-phase kernel's
+    const bool one = c.cg_variant == 1 && !ov && !replay;
     const long nparts = (one ? 3L : 4L) * L.nchunks * CG_PS;
     if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, nparts) ||
-        !L.nint.ensure(s->mem, 5L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
+        !L.nint.ensure(s->mem, 6L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
         !L.p.ensure(s->mem, L.grid_total) || !L.Ap.ensure(s->mem, L.grid_total) ||
         !L.apv.ensure(s->mem, L.grid_total) ||
         (one && !L.cg1.ensure(s->mem, 4 * L.grid_total)))
@@ -2348,11 +2378,13 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     int active = 0;
     for (int q = 0; q < nn; q++)
         active += node_chunk[2 * q + 1] > node_chunk[2 * q];
-    node_chunk.resize(5L * nn + 3, 0);
+    node_chunk.resize(6L * nn + 3, 0);
     node_chunk[4L * nn + 2] = active;
+    for (int q = 0; q < (int)caps.size(); q++)
+        node_chunk[5L * nn + 3 + q] = caps[q];
     if (!check_cuda(cudaMemcpyAsync(L.chunks.p, L.hchunks.data(), L.nchunks * sizeof(AmrChunk),
                                     cudaMemcpyHostToDevice, s->stream), "chunks") ||
-        !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), (5L * nn + 3) * sizeof(int),
+        !check_cuda(cudaMemcpyAsync(L.nint.p, node_chunk.data(), (6L * nn + 3) * sizeof(int),
                                     cudaMemcpyHostToDevice, s->stream), "cg ints"))
         return QZ_FAILURE;
     // r and both p buffers are zero off the interior points; partials start unpublished
@@ -2393,6 +2425,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     A.max_iter = c.max_iter;
     A.method = c.check_method;
     A.thr_node = nullptr;
+    A.cap_node = replay ? L.nint.p + 5 * nn + 3 : nullptr;
+    if (replay)
+        A.method = 0; // decisions by the (never met) r.r threshold only
     if (ov)
     {
         A.tol2 = ov->tol2;
@@ -2484,7 +2519,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
                   level_index);
         return QZ_FAILURE;
     }
-    if (st[2] != 0)
+    if (record)
+        sched_put(s, st.data() + 3, nn);
+    if (st[2] != 0 && !replay)
     {
         set_error("the precision was not reached in refinement level %d after %d conjugate "
                   "gradient iterations", level_index, st[0]);

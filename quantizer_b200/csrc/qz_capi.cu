@@ -257,6 +257,22 @@ static bool d2h(qz_sim *s, double *dst, const double *src, long count)
     return true;
 }
 
+bool sched_take(qz_sim *s, int n, int *out)
+{
+    if (s->sched_pos + (size_t)n > s->sched.size())
+    {
+        set_error("solver schedule exhausted: the replayed run has more solves than the "
+                  "recorded one");
+        return false;
+    }
+    for (int q = 0; q < n; q++)
+        out[q] = s->sched[s->sched_pos + q];
+    s->sched_pos += n;
+    return true;
+}
+
+void sched_put(qz_sim *s, const int *v, int n) { s->sched.insert(s->sched.end(), v, v + n); }
+
 int check_flags(qz_sim *s)
 {
     if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
@@ -801,6 +817,35 @@ int qz_step(qz_sim *s, double dt, int nsteps)
             return QZ_FAILURE;
     }
     return check_flags(s);
+}
+
+int qz_solve_schedule(qz_sim *s, int mode, int *counts, long cap, long *len)
+{
+    if (!s || mode < 0 || mode > 2 || cap < 0 || (cap > 0 && !counts))
+    {
+        set_error("qz_solve_schedule: bad arguments");
+        return QZ_FAILURE;
+    }
+    if (mode == 0)
+    {
+        if (len)
+            *len = (long)s->sched.size();
+        for (long q = 0; q < cap && q < (long)s->sched.size(); q++)
+            counts[q] = s->sched[q];
+        s->sched_mode = 0;
+        return QZ_SUCCESS;
+    }
+    if (mode == 1)
+    {
+        s->sched.clear();
+        s->sched_pos = 0;
+        s->sched_mode = 1;
+        return QZ_SUCCESS;
+    }
+    s->sched.assign(counts, counts + cap);
+    s->sched_pos = 0;
+    s->sched_mode = 2;
+    return QZ_SUCCESS;
 }
 
 int qz_synchronize(qz_sim *s)

@@ -369,6 +369,13 @@ struct qz_sim {
     qz::AmrLevel node_cg; // one host node solved by the node conjugate gradient (qz_node_conjugate_gradient)
     qz::Adjoint *adj = nullptr; // adjoint buffers (qz_force_vjp, qz_adjoint_final_loss)
     qz::NodeMgState *node_mg = nullptr; // mixed-form refinement-level multigrid buffers
+    // Solver schedule (qz_solve_schedule): mode 1 records the iterations of every
+    // forward Poisson solve (head: one count; a level: one count per node), mode 2
+    // replays recorded counts -- each solve runs exactly its count, without
+    // convergence tests, so that runs from perturbed inputs apply the same map.
+    int sched_mode = 0;
+    std::vector<int> sched;
+    size_t sched_pos = 0;
     qz::Snapshot *snap = nullptr; // snapshot staging and writer thread (qz_write_snapshot)
     // the head node's mass (node_mass): the configured total mass, lowered by
     // outflow removals; the convergence tests of the head solve use it
@@ -426,6 +433,10 @@ int check_flags(qz_sim *s);                   // qz_capi.cu
 int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
 void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
 int node_mg_level(qz_sim *s, AmrLevel &L, int level_index); // qz_node_mg.cu
+// solver schedule (qz_capi.cu): counts of the next solve in replay mode (false and
+// an error when the schedule is exhausted); append in record mode
+bool sched_take(qz_sim *s, int n, int *out);
+void sched_put(qz_sim *s, const int *v, int n);
 void node_mg_free(qz_sim *s);                               // qz_node_mg.cu
 void snapshot_free(qz_sim *s);                // qz_snapshot.cu
 // A copy of the state a step reads (particles, accelerations, head potential)
@@ -496,7 +507,7 @@ int grid_accel_head(qz_sim *s);
 int grid_accel_head_from(qz_sim *s, const double *pot);
 int head_segments(qz_sim *s, const double *x, const double *y, const double *z, int **perm_out);
 int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
-                     unsigned **ks_out, int **perm_out);
+                     unsigned **ks_out, int **perm_out, unsigned morton_B);
 int gather_head(qz_sim *s);
 int kick_drift(qz_sim *s, double dt);
 int kick(qz_sim *s, double dt);

@@ -73,7 +73,8 @@ struct NmgNode {
     double oh2;     // 1 / H^2
     double thr;     // residual test: r.r threshold (check methods 0 and 2)
     double rmt;     // check method 1: tol * (4 pi G rho_mean)
-    int cap;        // most iterations
+    int cap;        // most iterations (a replayed schedule: exactly this many)
+    int replay;     // no convergence test: run cap iterations
     int smem_need;  // bytes of the sub-cycle
     float h2[NMG_MAXLEV];
     NmgLev lv[NMG_MAXLEV];
@@ -447,7 +448,8 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             tot_f = f;
         }
         __syncthreads();
-        conv = it > 0 && !(tot_f & 1) && (A.method == 1 ? !(tot_f & 2) : tot_d < N.thr);
+        conv = !N.replay && it > 0 && !(tot_f & 1) &&
+               (A.method == 1 ? !(tot_f & 2) : tot_d < N.thr);
         if (conv || it >= N.cap)
             break;
 
@@ -667,6 +669,14 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     const qz_config &c = s->cfg;
     NodeMgBufs &B = bufs_of(s, level_index);
     std::vector<NmgNode> tab;
+    // solver schedule: replay gives every node its recorded count
+    std::vector<int> caps;
+    if (s->sched_mode == 2)
+    {
+        caps.resize(L.nnodes);
+        if (!sched_take(s, L.nnodes, caps.data()))
+            return QZ_FAILURE;
+    }
     long coarse = 0;
     size_t smem = 0;
     for (int q = 0; q < L.nnodes; q++)
@@ -688,7 +698,8 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         if (c.check_method == 2)
             N.thr = N.thr * (cbrt((double)nd.nintr) * cbrt((double)nd.nintr));
         N.rmt = c.tol * rm;
-        N.cap = c.max_iter;
+        N.cap = caps.empty() ? c.max_iter : caps[q];
+        N.replay = caps.empty() ? 0 : 1;
         int cx = nd.rd[0], cy = nd.rd[1], cz = nd.rd[2];
         int k = 0;
         for (;;)
@@ -743,7 +754,14 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         tab.push_back(N);
     }
     if (tab.empty())
+    {
+        if (s->sched_mode == 1)
+        {
+            std::vector<int> z(L.nnodes, 0);
+            sched_put(s, z.data(), L.nnodes);
+        }
         return QZ_SUCCESS;
+    }
     const int nt = (int)tab.size();
     if (!B.tab.ensure(s->mem, nt) || !B.status.ensure(s->mem, 2L * nt) ||
         !B.cl.ensure(s->mem, L.intr_total) || !B.ef.ensure(s->mem, L.grid_total) ||
@@ -828,6 +846,15 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         pts_it += (double)(tab[e].ie - tab[e].ib) * st[2 * e + 1];
     }
     s->stats.node_mg_iterations += worst;
+    if (s->sched_mode == 1)
+    {
+        std::vector<int> per(L.nnodes, 0);
+        for (int e = 0; e < nt; e++)
+            per[tab[e].q] = st[2 * e + 1];
+        sched_put(s, per.data(), L.nnodes);
+    }
+    if (s->sched_mode == 2)
+        unconv = 0; // replayed counts: no convergence test
     if (s->prof)
     {
         // per fine unknown and iteration: the FP64 pass reads d, phi, e (the 7

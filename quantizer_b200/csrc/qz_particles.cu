@@ -201,7 +201,42 @@ __device__ __forceinline__ int cell_coord(double x, int L, int *err)
     return f + 1;
 }
 
-__global__ void k_head_keys(long n, int L, const double *__restrict__ x,
+// Morton (Z-order) keys of head cells: the bits of the three box coordinates
+// interleaved (x lowest), 10 bits a coordinate at most.
+__device__ __forceinline__ unsigned morton_spread(unsigned v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ unsigned morton_compact(unsigned v)
+{
+    v &= 0x09249249u;
+    v = (v ^ (v >> 2)) & 0x030c30c3u;
+    v = (v ^ (v >> 4)) & 0x0300f00fu;
+    v = (v ^ (v >> 8)) & 0x030000ffu;
+    v = (v ^ (v >> 16)) & 0x3ffu;
+    return v;
+}
+
+// Linear cell index of a key: keys are linear (morton_B == 0) or Morton codes
+// of a box of morton_B cells a side.
+__device__ __forceinline__ long key_cell(unsigned k, unsigned morton_B)
+{
+    if (!morton_B)
+        return k;
+    const long B = morton_B;
+    return morton_compact(k) + morton_compact(k >> 1) * B + morton_compact(k >> 2) * B * B;
+}
+
+// Head cell key of every particle: the Morton code of its box cell when the
+// codes fit (3 (L + 1) <= 30 bits), so that cells close in space are close in
+// the sorted order; else the linear index bx + by B + bz B^2.
+__global__ void k_head_keys(long n, int L, int morton, const double *__restrict__ x,
                             const double *__restrict__ y, const double *__restrict__ z,
                             unsigned *__restrict__ keys, int *__restrict__ vals,
                             int *__restrict__ flags)
@@ -213,7 +248,8 @@ __global__ void k_head_keys(long n, int L, const double *__restrict__ x,
     int err = 0;
     unsigned bx = cell_coord(x[i], L, &err), by = cell_coord(y[i], L, &err),
              bz = cell_coord(z[i], L, &err);
-    keys[i] = bx + by * B + bz * B * B;
+    keys[i] = morton ? morton_spread(bx) | (morton_spread(by) << 1) | (morton_spread(bz) << 2)
+                     : bx + by * B + bz * B * B;
     vals[i] = (int)i;
     if (err)
         atomicOr(&flags[F_ERROR], err);
@@ -227,10 +263,10 @@ __global__ void k_seg_heads(long n, const unsigned *__restrict__ k, int *__restr
     head[i] = (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
 }
 
-__global__ void k_seg_fill(long n, const unsigned *__restrict__ k, const int *__restrict__ head,
-                           const int *__restrict__ sid, int *__restrict__ seg_start,
-                           int *__restrict__ seg_cell, int *__restrict__ cell_seg,
-                           int *__restrict__ flags)
+__global__ void k_seg_fill(long n, unsigned morton_B, const unsigned *__restrict__ k,
+                           const int *__restrict__ head, const int *__restrict__ sid,
+                           int *__restrict__ seg_start, int *__restrict__ seg_cell,
+                           int *__restrict__ cell_seg, int *__restrict__ flags)
 {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -240,7 +276,7 @@ __global__ void k_seg_fill(long n, const unsigned *__restrict__ k, const int *__
         int sgm = sid[i];
         seg_start[sgm] = (int)i;
         seg_cell[sgm] = (int)k[i];
-        cell_seg[k[i]] = sgm;
+        cell_seg[key_cell(k[i], morton_B)] = sgm;
     }
     if (i == n - 1)
     {
@@ -402,10 +438,12 @@ __global__ void k_point_gather(int L, long D, const int *__restrict__ cell_seg,
 }
 
 // Sorts the m (cell key, particle) pairs staged in s->sort.k0 / v0 and builds
-// the cell segments: seg_start / seg_cell of every occupied cell, cell_seg
-// (ncells_box entries, -1 for empty cells) and flags[F_NSEG].
+// the cell segments: seg_start / seg_cell (the key) of every occupied cell,
+// cell_seg (ncells_box entries by linear cell index, -1 for empty cells; keys
+// are Morton codes of a box of morton_B cells a side when morton_B > 0) and
+// flags[F_NSEG].
 int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box,
-                     unsigned **ks_out, int **perm_out)
+                     unsigned **ks_out, int **perm_out, unsigned morton_B)
 {
     unsigned *ks;
     int *perm;
@@ -419,7 +457,8 @@ int deposit_segments(qz_sim *s, long m, int bits, int *cell_seg, long ncells_box
         if (scan_exclusive(s, s->seg_head, s->seg_id, m))
             return QZ_FAILURE;
         launch(s, QZ_PROF_DEPOSIT, 12.0 * m, k_seg_fill, dim3(blocks_for(m, 256)), dim3(256), m,
-               ks, s->seg_head, s->seg_id, s->seg_start, s->seg_cell, cell_seg, s->flags);
+               morton_B, ks, s->seg_head, s->seg_id, s->seg_start, s->seg_cell, cell_seg,
+               s->flags);
     }
     else
         cudaMemsetAsync(s->flags + F_NSEG, 0, sizeof(int), s->stream);
@@ -436,12 +475,19 @@ int head_segments(qz_sim *s, const double *x, const double *y, const double *z, 
     const long n = s->n;
     const int L = s->L;
     const long B = (1L << L) + 2;
-    launch(s, QZ_PROF_DEPOSIT, 32.0 * n, k_head_keys, dim3(blocks_for(n, 256)), dim3(256), n, L, x, y, z, s->sort.k0, s->sort.v0, s->flags);
+    // Morton keys need L + 1 bits a coordinate (B <= 2^(L+1))
+    const int morton = 3 * (L + 1) <= 30 ? 1 : 0;
+    launch(s, QZ_PROF_DEPOSIT, 32.0 * n, k_head_keys, dim3(blocks_for(n, 256)), dim3(256), n, L,
+           morton, x, y, z, s->sort.k0, s->sort.v0, s->flags);
     int bits = 1;
-    while ((1L << bits) < B * B * B)
-        bits++;
+    if (morton)
+        bits = 3 * (L + 1);
+    else
+        while ((1L << bits) < B * B * B)
+            bits++;
     unsigned *ks;
-    return deposit_segments(s, n, bits, s->cell_seg, B * B * B, &ks, perm_out);
+    return deposit_segments(s, n, bits, s->cell_seg, B * B * B, &ks, perm_out,
+                            morton ? (unsigned)B : 0u);
 }
 
 int deposit_head(qz_sim *s)

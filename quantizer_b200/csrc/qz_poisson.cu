@@ -1777,6 +1777,26 @@ int potential_head(qz_sim *s)
     sync_fine_alt(s);
     int iter = 0;
     bool check = false;
+    if (s->sched_mode == 2)
+    {
+        // replay: exactly the recorded number of cycles, no convergence test
+        int n = 0;
+        if (!sched_take(s, 1, &n))
+            return QZ_FAILURE;
+        if (mg_persistent(s))
+        {
+            if (n > 0 && mg_cycles(s, n))
+                return QZ_FAILURE;
+        }
+        else
+            for (int q = 0; q < n; q++)
+                if (c.precision == QZ_PREC_MIXED ? mixed_iteration(s) : vcycle(s, 0, c.cycle))
+                    return QZ_FAILURE;
+        s->stats.last_vcycles = n;
+        s->stats.vcycles_total += n;
+        s->stats.last_converged = 1;
+        return check_cuda(cudaGetLastError(), "replayed head solve") ? QZ_SUCCESS : QZ_FAILURE;
+    }
     // the mixed form tests after every defect-correction iteration (its FP64
     // residual is computed anyway); the FP64 form keeps the reference's cadence
     const int every =
@@ -1865,6 +1885,8 @@ int potential_head(qz_sim *s)
     s->stats.last_vcycles = iter;
     s->stats.vcycles_total += iter;
     s->stats.last_converged = check ? 1 : 0;
+    if (s->sched_mode == 1)
+        sched_put(s, &iter, 1);
     if (iter == c.max_iter)
     {
         set_error("the precision was not reached in the head node after %d multigrid cycles",
