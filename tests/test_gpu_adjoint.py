@@ -137,3 +137,31 @@ def test_adjoint_rejects_unsupported_configurations():
         sim.init_forces()
         with pytest.raises(core.QZError, match="head-only"):
             sim.force_vjp(np.zeros(500), np.zeros(500), np.zeros(500))
+
+
+def test_replayed_schedule_reproduces_the_recorded_run():
+    # replaying a run's own solver schedule from the same inputs gives the same bits
+    ic = _ic(n=3000, seed=4)
+    dt = 1e-3 * ics.crossing_time(0.05)
+    out, sched = [], None
+    for replay in (False, True):
+        with core.Simulation(ic, L, **TOL) as sim:
+            if replay:
+                sim.replay_schedule(sched)
+            else:
+                sim.record_schedule()
+            sim.init_forces()
+            sim.step(dt, 5)
+            out.append(sim.particles())
+            if not replay:
+                sched = sim.take_schedule()
+    assert sched.size == 6 and np.all(sched > 0)  # step-0 solve and one per step
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
+    # a run with more solves than recorded fails instead of running unchecked
+    with core.Simulation(ic, L, **TOL) as sim:
+        sim.replay_schedule(sched[:2])
+        sim.init_forces()
+        sim.step(dt, 1)
+        with pytest.raises(core.QZError, match="schedule exhausted"):
+            sim.step(dt, 1)
