@@ -58,137 +58,163 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
     p[gp] = w * a + ((T)1.0 - w) * p[gp];
 }
 
-// One whole red-black sweep per launch, tiled in 3-D: a CTA stages its tile
-// of phi_in plus a 2-point halo in shared memory (asynchronous copies), updates
-// the red points of the tile and of a 1-point ring around it (the ring values
-// are recomputed by the neighbouring CTAs too, from the same inputs, so they
-// agree bit for bit), then the black points of the tile, and writes the tile to
-// phi_out.  Reading phi_in and writing phi_out (ping-pong) keeps CTAs from
-// racing on halos.  Each thread owns x-adjacent pairs of points -- one red, one
-// black -- so every lane updates one point per row in each colour phase.  The
-// arithmetic is that of k_gs_rb: the result equals two k_gs_rb launches.
-constexpr int RBT_X = 64, RBT_Y = 8, RBT_Z = 8; // tile (points); 32 x 8 threads
-constexpr int RBS_X = RBT_X + 4, RBS_Y = RBT_Y + 4, RBS_Z = RBT_Z + 4;
-constexpr int RB_THREADS_X = 32, RB_THREADS_Y = 8;
+// One whole red-black sweep per launch (the result of a red k_gs_rb launch
+// followed by a black one, bit for bit), reading phi from `pin` and writing
+// `pout` (ping-pong: CTAs never race on halos), with every field value loaded
+// from memory once per CTA and written once.  A CTA owns a tile of ZM_TX x
+// ZM_TY interior points in (x, y) and a chunk of ZM_TZ planes in z, and marches
+// up the chunk with a ring of planes in shared memory, staged by asynchronous
+// copies (cp.async) one plane ahead of the arithmetic:
+//   step s: load plane s+1 (phi window of the tile plus 2 points a side, rho
+//           window plus 1 point a side);
+//           red points of plane s-1 over the tile and a 1-point ring around it
+//           (from the old black values of planes s-2, s-1, s);
+//           black points of plane s-2 over the tile (from the new red values
+//           of planes s-3, s-2, s-1);
+//           plane s-2 of the tile to pout.
+// A ring point is a neighbouring CTA's tile point: both compute it from the
+// same old values, so they agree bit for bit.  Algorithmic traffic: 24 B a
+// point (phi and rho read, phi written); halos add (68 x 20 + 66 x 18) /
+// (64 x 16) - 2 = 0.49 reads a point, mostly served by L2.
+constexpr int ZM_TX = 64, ZM_TY = 16, ZM_TZ = 32;
+constexpr int ZM_WX = ZM_TX + 4, ZM_WY = ZM_TY + 4; // phi window
+constexpr int ZM_RX = ZM_TX + 2, ZM_RY = ZM_TY + 2; // red ring and rho window
+constexpr int ZM_PH = 5, ZM_RH = 4;                 // planes held (one in flight)
+constexpr int ZM_THREADS = 512;
 
-template <typename T>
-__device__ __forceinline__ void rb_update(T *S, int l, T rho_v, T H2, T w)
+template <typename T> constexpr size_t zm_smem_bytes()
 {
-    constexpr int SY = RBS_X, SZ = RBS_X * RBS_Y;
-    const T one_sixth = (T)(1.0 / 6.0);
-    T a = one_sixth * (-H2 * rho_v + S[l + 1] + S[l - 1] + S[l + SY] + S[l - SY] + S[l + SZ] +
-                       S[l - SZ]);
-    S[l] = w * a + ((T)1.0 - w) * S[l];
+    return sizeof(T) * ((size_t)ZM_PH * ZM_WX * ZM_WY + (size_t)ZM_RH * ZM_RX * ZM_RY);
 }
 
+__device__ __forceinline__ int zm_slot(int z, int ring) { return ((z % ring) + ring) % ring; }
+
 template <typename T>
-__global__ void __launch_bounds__(RB_THREADS_X * RB_THREADS_Y)
-    k_gs_rb_tile(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w)
+__global__ void __launch_bounds__(ZM_THREADS)
+    k_gs_rb_zm(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w)
 {
-    extern __shared__ unsigned char smem_raw[];
-    T *S = reinterpret_cast<T *>(smem_raw);
-    constexpr int SY = RBS_X, SZ = RBS_X * RBS_Y;
-    const int m = pin.n - 2;
-    const int last = pin.n - 1;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = 1 + blockIdx.x * RBT_X, y0 = 1 + blockIdx.y * RBT_Y, z0 = 1 + blockIdx.z * RBT_Z;
-    // stage: local x in 0..67 = global x0-2 .. x0+65; lanes take x = tx, 32+tx, 64+tx (tx<4)
-#pragma unroll
-    for (int lz = 0; lz < RBS_Z; lz++)
-    {
-        const int gz = z0 - 2 + lz;
-        if (gz < 0 || gz > last)
-            continue;
-#pragma unroll
-        for (int hy = 0; hy < 2; hy++)
+    extern __shared__ __align__(16) unsigned char zm_raw[];
+    T *PH = reinterpret_cast<T *>(zm_raw);           // [ZM_PH][ZM_WY][ZM_WX]
+    T *RH = PH + (size_t)ZM_PH * ZM_WX * ZM_WY;      // [ZM_RH][ZM_RY][ZM_RX]
+    const int n = pin.n, m = n - 2, last = n - 1;
+    const int tid = threadIdx.x;
+    const int x0 = 1 + blockIdx.x * ZM_TX, y0 = 1 + blockIdx.y * ZM_TY;
+    const int kb = 1 + blockIdx.z * ZM_TZ, ke = min(m, kb + ZM_TZ - 1);
+    const T one_sixth = (T)(1.0 / 6.0);
+    // asynchronous loads of plane z: phi window (in range) and, for interior
+    // planes, the rho window (in range)
+    auto load = [&](int z) {
+        if (z >= 0 && z <= last && z >= kb - 2 && z <= ke + 2)
         {
-            const int ly = ty + RB_THREADS_Y * hy;
-            if (ly >= RBS_Y)
-                break;
-            const int gy = y0 - 2 + ly;
-            if (gy < 0 || gy > last)
-                continue;
-            const T *row = pin.p + pin.off + gy * pin.sy + (long)gz * pin.sz;
-#pragma unroll
-            for (int hx = 0; hx < 3; hx++)
+            T *dst = PH + (size_t)zm_slot(z, ZM_PH) * ZM_WX * ZM_WY;
+            for (int e = tid; e < ZM_WX * ZM_WY; e += ZM_THREADS)
             {
-                const int lx = tx + 32 * hx;
-                const int gx = x0 - 2 + lx;
-                if (lx < RBS_X && gx >= 0 && gx <= last)
-                    __pipeline_memcpy_async(&S[lx + ly * SY + lz * SZ], row + gx, sizeof(T));
+                const int wy = e / ZM_WX, wx = e - wy * ZM_WX;
+                const int gx = x0 - 2 + wx, gy = y0 - 2 + wy;
+                if (gx >= 0 && gx <= last && gy >= 0 && gy <= last)
+                    __pipeline_memcpy_async(dst + e, pin.p + pin.off + gx + gy * pin.sy + (long)z * pin.sz,
+                                            sizeof(T));
             }
         }
-    }
-    __pipeline_commit();
-    __pipeline_wait_prior(0);
-    __syncthreads();
-    // red phase over the tile and its 1-point ring: local x pairs (1+2p, 2+2p),
-    // p = 0..32 (lane tx takes p = tx, and lane 0 also p = 32)
-#pragma unroll 2
-    for (int lz = 1; lz <= RBT_Z + 2; lz++)
-    {
-        const int gz = z0 - 2 + lz;
-        if (gz < 1 || gz > m)
-            continue;
-        for (int ly = 1 + ty; ly <= RBT_Y + 2; ly += RB_THREADS_Y)
+        if (z >= 1 && z <= m && z >= kb - 1 && z <= ke + 1)
         {
-            const int gy = y0 - 2 + ly;
-            if (gy < 1 || gy > m)
-                continue;
-            const long rrow = rho.off + gy * rho.sy + (long)gz * rho.sz;
-#pragma unroll
-            for (int hp = 0; hp < 2; hp++)
+            T *dst = RH + (size_t)zm_slot(z, ZM_RH) * ZM_RX * ZM_RY;
+            for (int e = tid; e < ZM_RX * ZM_RY; e += ZM_THREADS)
             {
-                const int pidx = tx + 32 * hp;
-                if (pidx > 32)
-                    break;
-                // the red member of the pair
-                int lx = 1 + 2 * pidx;
-                int gx = x0 - 2 + lx;
-                if ((gx + gy + gz) & 1)
+                const int ry = e / ZM_RX, rx = e - ry * ZM_RX;
+                const int gx = x0 - 1 + rx, gy = y0 - 1 + ry;
+                if (gx >= 1 && gx <= m && gy >= 1 && gy <= m)
+                    __pipeline_memcpy_async(dst + e, rho.p + rho.off + gx + gy * rho.sy + (long)z * rho.sz,
+                                            sizeof(T));
+            }
+        }
+        __pipeline_commit();
+    };
+    // window index of (wx, wy) in plane z
+    auto P = [&](int z) { return PH + (size_t)zm_slot(z, ZM_PH) * ZM_WX * ZM_WY; };
+    auto R = [&](int z) { return RH + (size_t)zm_slot(z, ZM_RH) * ZM_RX * ZM_RY; };
+    load(kb - 2);
+    for (int sp = kb - 2; sp <= ke + 2; sp++)
+    {
+        load(sp + 1);
+        __pipeline_wait_prior(1); // plane sp has landed
+        __syncthreads();
+        // red points of plane zr = sp - 1: pairs (2p, 2p + 1) of ring x, one red each
+        const int zr = sp - 1;
+        if (zr >= kb - 1 && zr <= ke + 1 && zr >= 1 && zr <= m)
+        {
+            T *pc = P(zr), *pd = P(zr - 1), *pu = P(zr + 1);
+            const T *rr = R(zr);
+            for (int e = tid; e < (ZM_RX / 2) * ZM_RY; e += ZM_THREADS)
+            {
+                const int ry = e / (ZM_RX / 2), pr = e - ry * (ZM_RX / 2);
+                const int gy = y0 - 1 + ry;
+                int rx = 2 * pr;
+                int gx = x0 - 1 + rx;
+                if ((gx + gy + zr) & 1)
                 {
-                    lx++;
+                    rx++;
                     gx++;
                 }
-                if (gx >= 1 && gx <= m)
-                    rb_update(S, lx + ly * SY + lz * SZ, rho.p[rrow + gx], H2, w);
+                if (gx < 1 || gx > m || gy < 1 || gy > m)
+                    continue;
+                const int l = (rx + 1) + (ry + 1) * ZM_WX;
+                const T a = one_sixth * (-H2 * rr[rx + ry * ZM_RX] + pc[l + 1] + pc[l - 1] +
+                                         pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
+                pc[l] = w * a + ((T)1.0 - w) * pc[l];
             }
         }
-    }
-    __syncthreads();
-    // black phase over the tile: local x pairs (2+2t, 3+2t), t = tx; write both
-    const int lxa = 2 + 2 * tx;
-    const int gxa = x0 + 2 * tx; // global x of the pair's first point
-    const int gy = y0 + ty;
-    if (gy > m || gxa > m)
-        return;
-    const bool second = gxa + 1 <= m;
-    const long rrow = rho.off + gy * rho.sy;
-    const long orow = pout.off + gy * pout.sy;
-    const int ly = 2 + ty;
-#pragma unroll 2
-    for (int lz = 2; lz < RBT_Z + 2; lz++)
-    {
-        const int gz = z0 - 2 + lz;
-        if (gz > m)
-            break;
-        const int l = lxa + ly * SY + lz * SZ;
-        const int black = ((gxa + gy + gz) & 1) ? 0 : 1; // offset of the black member
-        if (black == 0 || second)
-            rb_update(S, l + black, rho.p[rrow + (long)gz * rho.sz + gxa + black], H2, w);
-        pout.p[orow + (long)gz * pout.sz + gxa] = S[l];
-        if (second)
-            pout.p[orow + (long)gz * pout.sz + gxa + 1] = S[l + 1];
+        __syncthreads();
+        // black points of plane zb = sp - 2 over the tile: pairs (2t, 2t + 1) of tile x
+        const int zb = sp - 2;
+        const bool outp = zb >= kb && zb <= ke;
+        if (outp)
+        {
+            T *pc = P(zb), *pd = P(zb - 1), *pu = P(zb + 1);
+            const T *rr = R(zb);
+            for (int e = tid; e < (ZM_TX / 2) * ZM_TY; e += ZM_THREADS)
+            {
+                const int ty = e / (ZM_TX / 2), pt = e - ty * (ZM_TX / 2);
+                const int gy = y0 + ty;
+                int tx = 2 * pt;
+                int gx = x0 + tx;
+                if (!((gx + gy + zb) & 1))
+                {
+                    tx++;
+                    gx++;
+                }
+                if (gx > m || gy > m)
+                    continue;
+                const int l = (tx + 2) + (ty + 2) * ZM_WX;
+                const T a = one_sixth * (-H2 * rr[(tx + 1) + (ty + 1) * ZM_RX] + pc[l + 1] +
+                                         pc[l - 1] + pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
+                pc[l] = w * a + ((T)1.0 - w) * pc[l];
+            }
+        }
+        __syncthreads();
+        if (outp)
+        {
+            const T *pc = P(zb);
+            for (int e = tid; e < ZM_TX * ZM_TY; e += ZM_THREADS)
+            {
+                const int ty = e / ZM_TX, tx = e - ty * ZM_TX;
+                const int gx = x0 + tx, gy = y0 + ty;
+                if (gx <= m && gy <= m)
+                    pout.p[pout.off + gx + gy * pout.sy + (long)zb * pout.sz] =
+                        pc[(tx + 2) + (ty + 2) * ZM_WX];
+            }
+        }
+        __syncthreads(); // the next step's loads reuse the slot of plane sp - 4
     }
 }
 
 // Opt the fused sweep in to more than 48 KB of dynamic shared memory.
 void init_kernel_attributes()
 {
-    cudaFuncSetAttribute(k_gs_rb_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(double) * RBS_X * RBS_Y * RBS_Z));
-    cudaFuncSetAttribute(k_gs_rb_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(float) * RBS_X * RBS_Y * RBS_Z));
+    cudaFuncSetAttribute(k_gs_rb_zm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)zm_smem_bytes<double>());
+    cudaFuncSetAttribute(k_gs_rb_zm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)zm_smem_bytes<float>());
 }
 
 template <typename T>
@@ -474,14 +500,13 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
         else if (alt.p && m >= 64 && s->fused_rb)
         {
             // fused sweeps, ping-pong phi <-> alt (alt has phi's boundary values)
-            dim3 grid((m + RBT_X - 1) / RBT_X, (m + RBT_Y - 1) / RBT_Y, (m + RBT_Z - 1) / RBT_Z);
-            size_t shm = sizeof(T) * RBS_X * RBS_Y * RBS_Z;
+            dim3 grid((m + ZM_TX - 1) / ZM_TX, (m + ZM_TY - 1) / ZM_TY, (m + ZM_TZ - 1) / ZM_TZ);
+            const size_t shm = zm_smem_bytes<T>();
             Grid<T> a = phi, b = alt;
             for (int it = 0; it < iters; it++)
             {
                 launch_shm(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m, shm,
-                           k_gs_rb_tile<T>, grid, dim3(RB_THREADS_X, RB_THREADS_Y), a, b, rho,
-                           H2, w);
+                           k_gs_rb_zm<T>, grid, dim3(ZM_THREADS), a, b, rho, H2, w);
                 Grid<T> t = a;
                 a = b;
                 b = t;
