@@ -11,15 +11,19 @@
  * reads them (timestep, observables, snapshots) always sees current values.
  *
  * Refinement runs (lmax > lmin): the tree bookkeeping stays in the reference's
- * C -- tree_adaptation and the particle moves between cell lists of
- * particle_updating.c:634-1381, so the host program links the reference's
- * particle_updating.o -- and the host particle arrays are authoritative for
- * x and v: grid_density, timestep and observables upload them first.  The
- * density, potentials, grid and particle accelerations are computed on the
- * device on its own copy of the tree (built from the same rules,
- * tree_construction.c; its refined cells equal the reference's adapted tree);
- * particle accelerations and the head node's fields are written back,
- * refinement nodes' grid fields are not.
+ * C (tree_adaptation and the rest of its bookkeeping objects) and the host
+ * particle arrays are authoritative for x and v: grid_density, timestep,
+ * observables and particle_updating_A upload them first.  particle_updating_A
+ * advances every particle on the device (kick, drift, reflection at the
+ * walls) and the shim then applies the moves between the host tree's cell
+ * lists that the reference makes in its cell loops (particle_updating.c:
+ * 634-1381): same cell, another cell of the node, a child zone, the parent or
+ * a sibling node, with the nodes' masses and particle counts.  The density,
+ * potentials, grid and particle accelerations are computed on the device on
+ * its own copy of the tree (built from the same rules, tree_construction.c;
+ * its refined cells equal the reference's adapted tree); particle
+ * accelerations and the head node's fields are written back, refinement
+ * nodes' grid fields are not.
  *
  * Supported: reflexive boundaries, one smoother for all multigrid stages or
  * the head conjugate gradient, the particle refinement criterion with n_exp
@@ -63,6 +67,12 @@ static struct {
     double *ref_mass;
     int **ptcl_id;
     double *total_mass_final;
+    /* the tree by levels and the particles' update flags (refinement runs) */
+    struct node ****tentacles;
+    int **tentacles_size;
+    int *tentacles_level_max;
+    bool **updating_flag;
+    int (*space_check)(int *, int, float, const char *, ...);
     int resolved;
 } R;
 
@@ -141,6 +151,11 @@ static int resolve(void)
     R.box_extra = need("min_box_extra_size_per_side_real", &ok);
     R.ptcl_id = need("GL_ptcl_ID", &ok);
     R.total_mass_final = need("GL_total_mass_final", &ok);
+    R.tentacles = need("GL_tentacles", &ok);
+    R.tentacles_size = need("GL_tentacles_size", &ok);
+    R.tentacles_level_max = need("GL_tentacles_level_max", &ok);
+    R.updating_flag = need("GL_ptcl_updating_flag", &ok);
+    *(void **)&R.space_check = need("space_check", &ok);
     R.resolved = ok;
     return ok;
 }
@@ -370,14 +385,98 @@ int particle_acceleration(void)
     return REF_SUCCESS;
 }
 
-/* Refinement runs move particles between the host tree's cell lists in the
- * reference's particle_updating.c, which the host program links instead. */
-static int amr_update_refused(void)
+/* Appends particle p to cell b of node nd (the host tree's cell list), with
+ * the cell's mass; capacity grows through the reference's space_check, as its
+ * own appends do. */
+static int cell_append(struct node *nd, int b, int p, double m)
 {
-    printf("\nERROR (drop-in): refinement runs keep the reference's particle_updating.o "
-           "(cell-list bookkeeping of particle_updating.c:634-1381) in the link\n");
-    g_failed = 1;
-    return REF_FAILURE;
+    struct cell_struct *c = &nd->ptr_cell_struct[b];
+    if (R.space_check(&c->ptcl_cap, c->ptcl_size + 1, 1.0f, "p1i1", &c->ptr_ptcl) == REF_FAILURE)
+    {
+        printf("Error, in space_check function\n");
+        return REF_FAILURE;
+    }
+    c->ptr_ptcl[c->ptcl_size++] = p;
+    c->cell_mass += m;
+    return REF_SUCCESS;
+}
+
+/* The moves between the host tree's cell lists after the device advanced the
+ * particles (reflexive boundaries; particle_updating.c:634-1381).  Nodes are
+ * visited from the finest level to the head, cells in each node's cell order,
+ * particles in list order; a visited particle takes the pass's update flag
+ * and is not moved twice.  A particle whose box cell in its node changed goes
+ *   into a refined cell (status >= 0):  the child zone's node, its cell there;
+ *   outside the node (status -4):       the parent's cell there, or the
+ *                                       sibling node whose zone holds it;
+ *   anywhere else:                      its new cell of the node;
+ * and leaves its old cell by taking the list's last entry into its place.
+ * Node masses and particle counts follow the particle across nodes. */
+static int apply_cell_moves(void)
+{
+    const double *mass = *R.ptcl_mass;
+    bool *flag = *R.updating_flag;
+    const bool status = !flag[0];
+    struct node ***tent = *R.tentacles;
+    const int *tsize = *R.tentacles_size;
+    for (int lv = *R.tentacles_level_max; lv >= 0; lv--)
+        for (int i = 0; i < tsize[lv]; i++)
+        {
+            struct node *nd = tent[lv][i];
+            for (int c = 0; c < nd->cell_size; c++)
+            {
+                const int bo = nd->ptr_box_idx[c];
+                if (nd->chn_size > 0 && nd->ptr_box[bo] >= 0)
+                    continue; /* a refined cell: its particles belong to the child */
+                struct cell_struct *cs = &nd->ptr_cell_struct[bo];
+                int np = cs->ptcl_size;
+                for (int j = 0; j < np; j++)
+                {
+                    const int p = cs->ptr_ptcl[j];
+                    if (flag[p] == status)
+                        continue;
+                    flag[p] = status;
+                    const int bn = ptcl_idx_to_box_idx(nd, p);
+                    if (bn == bo)
+                        continue;
+                    const double m = mass[p];
+                    const int st = nd->ptr_box[bn];
+                    if (nd->chn_size > 0 && st >= 0)
+                    {
+                        struct node *ch = nd->pptr_chn[st];
+                        if (cell_append(ch, ptcl_idx_to_box_idx(ch, p), p, m))
+                            return REF_FAILURE;
+                        ch->node_mass += m;
+                        ch->no_ptcl_full_node++;
+                    }
+                    else if (st == -4)
+                    {
+                        struct node *pt = nd->ptr_pt;
+                        const int bp = ptcl_idx_to_box_idx(pt, p);
+                        if (pt->ptr_box[bp] >= 0)
+                        {
+                            struct node *sib = pt->pptr_chn[pt->ptr_box[bp]];
+                            if (cell_append(sib, ptcl_idx_to_box_idx(sib, p), p, m))
+                                return REF_FAILURE;
+                            sib->node_mass += m;
+                            sib->no_ptcl_full_node++;
+                        }
+                        else if (cell_append(pt, bp, p, m))
+                            return REF_FAILURE;
+                        nd->node_mass -= m;
+                        nd->no_ptcl_full_node--;
+                    }
+                    else if (cell_append(nd, bn, p, m))
+                        return REF_FAILURE;
+                    cs->ptr_ptcl[j] = cs->ptr_ptcl[np - 1];
+                    np--;
+                    j--;
+                    cs->cell_mass -= m;
+                }
+                cs->ptcl_size = np;
+            }
+        }
+    return REF_SUCCESS;
 }
 
 /* Outflow removals of the last update, applied to the host's bookkeeping in
@@ -423,7 +522,16 @@ int particle_updating_A(double dt)
     if (ensure())
         return REF_FAILURE;
     if (g_amr)
-        return amr_update_refused();
+    {
+        /* the host arrays are authoritative: advance them on the device, bring
+         * x, v and a (negated on reflection) back, then move the particles
+         * between the host tree's cell lists */
+        if (sync_host_particles(1) || qz_particle_updating_A(g_sim, dt) ||
+            qz_get_particles(g_sim, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
+                             *R.ptcl_vz, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az))
+            return fail("particle_updating_A");
+        return apply_cell_moves();
+    }
     if (qz_particle_updating_A(g_sim, dt) || apply_removals() ||
         qz_get_particles(g_sim, *R.ptcl_x, *R.ptcl_y, *R.ptcl_z, *R.ptcl_vx, *R.ptcl_vy,
                          *R.ptcl_vz, *R.ptcl_ax, *R.ptcl_ay, *R.ptcl_az))
@@ -436,11 +544,10 @@ void particle_updating_B(double dt)
 {
     if (ensure())
         return;
-    if (g_amr)
-    {
-        amr_update_refused();
-        return;
-    }
+    /* every particle's half kick (refinement runs: the reference kicks each
+     * particle once, in the cell list of its finest node, particle_updating.c:
+     * 2690-2785); the device's v and a are current (grid_density uploaded v,
+     * particle_acceleration computed a) */
     if (qz_particle_updating_B(g_sim, dt) ||
         qz_get_particles(g_sim, NULL, NULL, NULL, *R.ptcl_vx, *R.ptcl_vy, *R.ptcl_vz, NULL, NULL,
                          NULL))

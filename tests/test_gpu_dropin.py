@@ -3,11 +3,13 @@ tree construction/adaptation, globals) linked with libqz_dropin.so in place of
 its hot-path objects (oracle/_ref/qz_dropin_driver), run against the
 unmodified reference (oracle/_ref/qz_ref_driver) on the same inputs.
 
-Refinement runs (oracle/_ref/qz_dropin_amr_driver, which also keeps the
-reference's particle_updating.o for the cell-list moves): positions after 4
-steps within 1e-10 box units, particle accelerations within 1e-6 of the
-largest, head potential within 1e-9, box indices equal, and the reference's
-own adapted tree (node count and particles per node) as in the plain run."""
+Refinement runs (oracle/_ref/qz_dropin_amr_driver, the same link: the
+reference's particle_updating.o is not in it -- the drop-in advances the
+particles on the device and applies the moves between the host tree's cell
+lists itself): positions after 4 steps within 1e-10 box units, particle
+accelerations within 1e-6 of the largest, head potential within 1e-9, box
+indices equal, and the reference's own adapted tree (node count and particles
+per node, in node order) as in the plain run."""
 import os
 
 import numpy as np
