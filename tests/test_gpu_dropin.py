@@ -103,3 +103,27 @@ def test_dropin_refinement_run_matches_reference(tmp_path):
         nr = O.read_nodes(str(tmp_path / "ref"), s)
         ng = O.read_nodes(str(tmp_path / "gpu"), s)
         assert [(n["lv"], n["nptcl"]) for n in nr] == [(n["lv"], n["nptcl"]) for n in ng]
+
+
+def test_dropin_refinement_throughput_at_the_bench_size(tmp_path, capsys):
+    """The bench workload (Plummer N = 1,048,576, a = 0.02, head 128^3, three
+    refinement levels) through the drop-in in the reference's main-loop order,
+    the host bookkeeping (tree_adaptation, cell lists) on all host threads:
+    the run must complete and match the reference's positions after the steps;
+    the step-loop rate of both is printed (particle-steps/s) for the record."""
+    n, steps = 1048576, 3
+    p = str(tmp_path / "ic.bin")
+    ics.write_ic(p, ics.plummer(n, a=0.02, seed=1))
+    kw = dict(lmin=7, lmax=10, ref_ptcl=9, steps=steps, dt=1e-3 * ics.crossing_time(0.02),
+              dump=f"{steps}", threads=os.cpu_count() or 1)
+    rr = _run(O.REF_DRIVER, p, str(tmp_path / "ref"), **kw)
+    rg = _run(O.DROPIN_AMR_DRIVER, p, str(tmp_path / "gpu"), **kw)
+    for f in ("x", "y", "z"):
+        g = O.read_dump(str(tmp_path / "gpu"), steps, f)
+        r = O.read_dump(str(tmp_path / "ref"), steps, f)
+        assert np.abs(g - r).max() < 1e-10, f
+    with capsys.disabled():
+        print(f"\ndrop-in refinement run, {n} particles x {steps} steps: "
+              f"drop-in {n * steps / rg['loop_s']:.4g} particle-steps/s, "
+              f"reference {n * steps / rr['loop_s']:.4g} particle-steps/s "
+              f"({os.cpu_count()} host threads)")
