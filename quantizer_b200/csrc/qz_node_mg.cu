@@ -13,8 +13,18 @@
 //   repeat:  r = d - Lap_H(phi)                      (FP64, interior points)
 //            convergence test on phi (ratio test against the previous iterate,
 //            residual test on r: the reference's test, FP64)
-//            e ~= Lap_H^-1 r by one FP32 V-cycle      (zero on non-interior points)
-//            phi += e                                 (FP64)
+//            z ~= Lap_H^-1 r by one FP32 V-cycle      (zero on non-interior points)
+//            phi += alpha p, p = z + beta p_old       (FP64)
+//
+// with alpha and beta those of the flexible conjugate gradient (Notay 2000,
+// Polak-Ribiere beta = r.(z - z_old) / (r_old.z_old), alpha = r.z / p.Lap p).
+// Plain defect correction (phi += z) converges slowly on refinement nodes: a
+// node's interior ends at odd fine-grid coordinates (zone surfaces are faces of
+// parent cells), so every coarse level places its zero boundary up to one of
+// its cells outside the true one and over-corrects the smoothest error (at
+// 1M particles, 128^3 head, three levels: 40-300 iterations, one node not
+// converging in 5000).  The conjugate-gradient step makes the cycle a
+// preconditioner and removes that sensitivity.
 //
 // The V-cycle works on the node's grid box with a mask: level 0 is the node
 // grid ((rd + 1)^3 points, unknowns at the node's interior points, in the
@@ -93,6 +103,8 @@ struct NmgArgs {
     float *ec, *fc;        // coarse levels
     unsigned char *mc;
     int *status;           // per entry: converged, iterations
+    double *pv;            // flexible CG direction (grid-pool layout, zero off the interior)
+    float *efo;            // the previous preconditioned residual (interior points)
     double tol2;
     int method;
     int n_pre, n_post;
@@ -282,11 +294,14 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     const int rank = (int)cluster.block_rank();
     const int ent = (int)(blockIdx.x / CS);
     __shared__ NmgNode N;
-    __shared__ double wsum[32];
+    __shared__ double wsum[32], wsum2[32];
     __shared__ int wflag[32];
-    __shared__ double part_d;  // this CTA's partial (read by the others through DSMEM)
-    __shared__ int part_f;
-    __shared__ double tot_d;
+    // this CTA's partials of the three reductions of an iteration (read by the
+    // others through distributed shared memory; one slot set per reduction, so a
+    // slot is rewritten only an iteration later, many cluster barriers on)
+    __shared__ double part_d[3][2];
+    __shared__ int part_f[3];
+    __shared__ double tot_d[2];
     __shared__ int tot_f;
     extern __shared__ __align__(16) unsigned char nmg_dyn[];
     const int tid = threadIdx.x, NT = blockDim.x;
@@ -383,12 +398,63 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         }
     };
 
+    // Cluster-wide sums of (a, b) and OR of f in slot set `slot`: warp trees,
+    // warps in order, CTAs in rank order; every CTA gets the same values.
+    auto reduce = [&](int slot, double a, double b, int f) {
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        f = (int)__reduce_or_sync(0xffffffffu, (unsigned)f);
+        if ((tid & 31) == 0)
+        {
+            wsum[tid >> 5] = a;
+            wsum2[tid >> 5] = b;
+            wflag[tid >> 5] = f;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            double t = 0.0, u = 0.0;
+            int g = 0;
+            for (int w = 0; w < (NT >> 5); w++)
+            {
+                t += wsum[w];
+                u += wsum2[w];
+                g |= wflag[w];
+            }
+            part_d[slot][0] = t;
+            part_d[slot][1] = u;
+            part_f[slot] = g;
+        }
+        cluster.sync();
+        if (tid == 0)
+        {
+            double t = 0.0, u = 0.0;
+            int g = 0;
+            for (int r = 0; r < CS; r++)
+            {
+                const double *pr = cluster.map_shared_rank(&part_d[slot][0], r);
+                t += pr[0];
+                u += pr[1];
+                g |= *cluster.map_shared_rank(&part_f[slot], r);
+            }
+            tot_d[0] = t;
+            tot_d[1] = u;
+            tot_f = g;
+        }
+        __syncthreads();
+    };
+
     double *bufs[2] = {A.pot, A.pot_old};
     int it = 0;
     bool conv = false;
+    double alpha = 0.0, rz_prev = 1.0;
     for (;;)
     {
-        // FP64: new iterate, its residual (FP32 copy for the cycle), ratio test
+        // FP64: new iterate phi + alpha p, its residual (FP32 copy for the cycle),
+        // ratio test against the previous iterate
         const double *ph = bufs[it & 1];
         double *pn = bufs[(it + 1) & 1];
         double acc = 0.0;
@@ -398,14 +464,14 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             const int v = A.cl[e];
             const long g = v < 0 ? ~v : v;
             auto P = [&](long x) -> double {
-                return it > 0 ? ldg_d(ph + x) + (double)ldg_f(A.ef + x) : ldg_d(ph + x);
+                return it > 0 ? ldg_d(ph + x) + alpha * ldg_d(A.pv + x) : ldg_d(ph + x);
             };
             const double old = ldg_d(ph + g);
             const double c0 = P(g);
             const double r = A.d[g] + N.oh2 * (6.0 * c0 - P(g + 1) - P(g - 1) - P(g + sy0) -
                                               P(g - sy0) - P(g + sz0) - P(g - sz0));
             __stcg(pn + g, c0);
-            A.rf[g] = (float)r;
+            __stcg(A.rf + g, (float)r);
             acc += r * r;
             const double aux = c0 / old;
             if ((1.0 - A.tol2 > aux) || (1.0 + A.tol2 < aux))
@@ -413,43 +479,9 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             if (A.method == 1 && fabs(r) >= N.rmt)
                 fl |= 2;
         }
-        for (int o = 16; o > 0; o >>= 1)
-            acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)fl);
-        if ((tid & 31) == 0)
-        {
-            wsum[tid >> 5] = acc;
-            wflag[tid >> 5] = fl;
-        }
-        __syncthreads();
-        if (tid == 0)
-        {
-            double t = 0.0;
-            int f = 0;
-            for (int w = 0; w < (NT >> 5); w++)
-            {
-                t += wsum[w];
-                f |= wflag[w];
-            }
-            part_d = t;
-            part_f = f;
-        }
-        cluster.sync();
-        if (tid == 0)
-        {
-            double t = 0.0;
-            int f = 0;
-            for (int r = 0; r < CS; r++)
-            {
-                t += *cluster.map_shared_rank(&part_d, r);
-                f |= *cluster.map_shared_rank(&part_f, r);
-            }
-            tot_d = t;
-            tot_f = f;
-        }
-        __syncthreads();
+        reduce(0, acc, 0.0, fl);
         conv = !N.replay && it > 0 && !(tot_f & 1) &&
-               (A.method == 1 ? !(tot_f & 2) : tot_d < N.thr);
+               (A.method == 1 ? !(tot_f & 2) : tot_d[0] < N.thr);
         if (conv || it >= N.cap)
             break;
 
@@ -590,6 +622,46 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                 fine_sweep(col, false);
                 cluster.sync();
             }
+
+        // ---- flexible conjugate gradient with z = ef (Notay 2000; Polak-Ribiere
+        // beta), FP64 arithmetic on the FP32 vectors r (rf) and z ------------------
+        double rz = 0.0, rzo = 0.0;
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            const long g = v < 0 ? ~v : v;
+            const double r = (double)ldg_f(A.rf + g);
+            rz += r * (double)ldg_f(A.ef + g);
+            if (it > 0)
+                rzo += r * (double)ldg_f(A.efo + g);
+        }
+        reduce(1, rz, rzo, 0);
+        rz = tot_d[0];
+        const double beta = it > 0 ? (rz - tot_d[1]) / rz_prev : 0.0;
+        rz_prev = rz;
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            const long g = v < 0 ? ~v : v;
+            const float z = ldg_f(A.ef + g);
+            const double pnew = (double)z + (it > 0 ? beta * ldg_d(A.pv + g) : 0.0);
+            __stcg(A.pv + g, pnew);
+            __stcg(A.efo + g, z);
+        }
+        cluster.sync();
+        double pq = 0.0;
+        for (int e = sb + tid; e < se; e += NT)
+        {
+            const int v = A.cl[e];
+            const long g = v < 0 ? ~v : v;
+            const double pc = ldg_d(A.pv + g);
+            const double lap = N.oh2 * (ldg_d(A.pv + g + 1) + ldg_d(A.pv + g - 1) +
+                                        ldg_d(A.pv + g + sy0) + ldg_d(A.pv + g - sy0) +
+                                        ldg_d(A.pv + g + sz0) + ldg_d(A.pv + g - sz0) - 6.0 * pc);
+            pq += pc * lap;
+        }
+        reduce(2, pq, 0.0, 0);
+        alpha = tot_d[0] != 0.0 ? rz / tot_d[0] : 0.0;
         it++;
     }
     // the iterate that passed the test is in bufs[(it + 1) & 1]
@@ -613,7 +685,8 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
 struct NodeMgBufs {
     DBuf<NmgNode> tab;
     DBuf<int> cl, status;
-    DBuf<float> ef, rf, ec, fc;
+    DBuf<float> ef, rf, ec, fc, efo;
+    DBuf<double> pv;
     DBuf<unsigned char> msk, mc;
 };
 
@@ -766,7 +839,8 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     if (!B.tab.ensure(s->mem, nt) || !B.status.ensure(s->mem, 2L * nt) ||
         !B.cl.ensure(s->mem, L.intr_total) || !B.ef.ensure(s->mem, L.grid_total) ||
         !B.rf.ensure(s->mem, L.grid_total) || !B.msk.ensure(s->mem, L.grid_total) ||
-        !B.ec.ensure(s->mem, coarse) || !B.fc.ensure(s->mem, coarse) || !B.mc.ensure(s->mem, coarse))
+        !B.ec.ensure(s->mem, coarse) || !B.fc.ensure(s->mem, coarse) || !B.mc.ensure(s->mem, coarse) ||
+        !B.pv.ensure(s->mem, L.grid_total) || !B.efo.ensure(s->mem, L.grid_total))
     {
         set_error("node multigrid buffers");
         return QZ_FAILURE;
@@ -785,6 +859,7 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     cudaMemsetAsync(B.ef.p, 0, L.grid_total * sizeof(float), s->stream);
     cudaMemsetAsync(B.ec.p, 0, std::max(coarse, 1L) * sizeof(float), s->stream);
     cudaMemsetAsync(B.mc.p, 0, std::max(coarse, 1L), s->stream);
+    cudaMemsetAsync(B.pv.p, 0, L.grid_total * sizeof(double), s->stream);
     NmgArgs A;
     A.tab = B.tab.p;
     A.intr = L.intr.p;
@@ -799,6 +874,8 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.fc = B.fc.p;
     A.mc = B.mc.p;
     A.status = B.status.p;
+    A.pv = B.pv.p;
+    A.efo = B.efo.p;
     A.tol2 = c.tol2;
     A.method = c.check_method;
     A.n_pre = std::max(1, c.n_pre);
@@ -857,13 +934,14 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         unconv = 0; // replayed counts: no convergence test
     if (s->prof)
     {
-        // per fine unknown and iteration: the FP64 pass reads d, phi, e (the 7
+        // per fine unknown and iteration: the FP64 pass reads d, phi, p (the 7
         // stencil values come from cache lines shared with neighbours) and
         // writes the new phi and r (36 B); each red-black sweep reads e, r and
-        // writes e (12 B); restriction and prolongation about 8 B; the coarse
-        // levels add about a seventh
+        // writes e (12 B); restriction and prolongation about 8 B, the coarse
+        // levels about a seventh of that; the conjugate-gradient passes read r,
+        // z, z_old (12 B), read z, p and write p, z_old (24 B), read p (8 B)
         const double sweeps = (double)(A.n_pre + A.n_post);
-        s->prof_pending.back().bytes = pts_it * (36.0 + 12.0 * sweeps + 8.0) * 8.0 / 7.0;
+        s->prof_pending.back().bytes = pts_it * (36.0 + (12.0 * sweeps + 8.0) * 8.0 / 7.0 + 44.0);
     }
     if (unconv)
     {
@@ -890,6 +968,8 @@ void node_mg_free(qz_sim *s)
         B.fc.release(s->mem);
         B.msk.release(s->mem);
         B.mc.release(s->mem);
+        B.pv.release(s->mem);
+        B.efo.release(s->mem);
     }
     delete s->node_mg;
     s->node_mg = nullptr;
