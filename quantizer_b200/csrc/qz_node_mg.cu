@@ -64,7 +64,7 @@ namespace qz {
 
 #define QZ_PI_NMG 3.14159265358979323846
 
-constexpr int NMG_THREADS = 1024;
+constexpr int NMG_THREADS = 512;
 constexpr int NMG_MAXLEV = 10;
 constexpr size_t NMG_SMEM_MAX = 160 * 1024; // shared-memory sub-cycle (CTA 0)
 constexpr int NMG_COARSE_SWEEPS = 24;       // FP64 red-black sweeps on the coarsest level
@@ -95,7 +95,7 @@ struct NmgNode {
 struct NmgArgs {
     const NmgNode *tab;
     const int *intr;       // level interior list (grid-pool indices)
-    int *cl;               // colour-coded copy of the list (~g for odd points)
+    int *cl;               // the list by colour within each CTA's slice
     const double *d;
     double *pot, *pot_old; // the node's two potential buffers
     float *ef, *rf;        // level 0 correction and residual (grid-pool layout)
@@ -317,7 +317,14 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     float *rf = A.rf + N.goff;
     unsigned char *mk0 = A.msk + N.goff;
 
-    // set-up 1: colour-coded list and the fine mask
+    // set-up 1: the fine mask, and this CTA's slice of the interior list split by
+    // colour into cl (even points from sb up, odd points from se down; the order
+    // inside a colour does not matter to a sweep, and the sums below walk the
+    // interior list itself, in its fixed order)
+    __shared__ int s_nred, s_nblk;
+    if (tid == 0)
+        s_nred = s_nblk = 0;
+    __syncthreads();
     for (int e = sb + tid; e < se; e += NT)
     {
         const int g = A.intr[e];
@@ -326,9 +333,14 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         l -= z * sz0;
         const int y = (int)(l / sy0);
         const int x = (int)(l - y * sy0);
-        A.cl[e] = ((x + y + z) & 1) ? ~g : g;
+        if ((x + y + z) & 1)
+            A.cl[se - 1 - atomicAdd(&s_nblk, 1)] = g;
+        else
+            A.cl[sb + atomicAdd(&s_nred, 1)] = g;
         __stcg(A.msk + g, (unsigned char)1);
     }
+    __syncthreads();
+    const int nred = s_nred; // cl[sb, sb + nred): even points; [sb + nred, se): odd
     cluster.sync();
     // set-up 2: coarse masks, X is an unknown where the fine point 2^k X is one
     for (int k = 1; k < N.nlev; k++)
@@ -380,21 +392,39 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     auto gf = [&](int k) { return k == 0 ? rf : A.fc + N.lv[k].off; };
 
     // one colour of a sweep of the fine level over this CTA's slice of the list
+    // one colour of a sweep of the fine level over this CTA's points of that
+    // colour, NB points a thread at a time (their loads in flight together; points
+    // of one colour are never neighbours)
+    constexpr int NB = 4;
     auto fine_sweep = [&](int col, bool first) {
         const float h2 = N.h2[0];
         const float one_sixth = (float)(1.0 / 6.0);
-        for (int e = sb + tid; e < se; e += NT)
+        const int b0 = col == 0 ? sb : sb + nred, b1 = col == 0 ? sb + nred : se;
+        for (int e0 = b0 + tid; e0 < b1; e0 += NB * NT)
         {
-            const int v = A.cl[e];
-            if ((v < 0) != (col == 1))
-                continue;
-            const long g = v < 0 ? ~v : v;
-            const float fx = ldg_f(A.rf + g);
-            float s = 0.0f;
-            if (!first)
-                s = ldg_f(A.ef + g + 1) + ldg_f(A.ef + g - 1) + ldg_f(A.ef + g + sy0) +
-                    ldg_f(A.ef + g - sy0) + ldg_f(A.ef + g + sz0) + ldg_f(A.ef + g - sz0);
-            __stcg(A.ef + g, one_sixth * (-h2 * fx + s));
+            long g[NB];
+            float fx[NB], sm[NB];
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+            {
+                const int e = e0 + u * NT;
+                g[u] = e < b1 ? (long)A.cl[e] : -1L;
+            }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                {
+                    const long x = g[u];
+                    fx[u] = ldg_f(A.rf + x);
+                    sm[u] = first ? 0.0f
+                                  : ldg_f(A.ef + x + 1) + ldg_f(A.ef + x - 1) + ldg_f(A.ef + x + sy0) +
+                                        ldg_f(A.ef + x - sy0) + ldg_f(A.ef + x + sz0) +
+                                        ldg_f(A.ef + x - sz0);
+                }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                    __stcg(A.ef + g[u], one_sixth * (-h2 * fx[u] + sm[u]));
         }
     };
 
@@ -459,25 +489,42 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         double *pn = bufs[(it + 1) & 1];
         double acc = 0.0;
         int fl = 0; // 1: ratio test failed, 2: point residual test failed (method 1)
-        for (int e = sb + tid; e < se; e += NT)
+        auto P = [&](long x) -> double {
+            return it > 0 ? ldg_d(ph + x) + alpha * ldg_d(A.pv + x) : ldg_d(ph + x);
+        };
+        for (int e0 = sb + tid; e0 < se; e0 += 2 * NT)
         {
-            const int v = A.cl[e];
-            const long g = v < 0 ? ~v : v;
-            auto P = [&](long x) -> double {
-                return it > 0 ? ldg_d(ph + x) + alpha * ldg_d(A.pv + x) : ldg_d(ph + x);
-            };
-            const double old = ldg_d(ph + g);
-            const double c0 = P(g);
-            const double r = A.d[g] + N.oh2 * (6.0 * c0 - P(g + 1) - P(g - 1) - P(g + sy0) -
-                                              P(g - sy0) - P(g + sz0) - P(g - sz0));
-            __stcg(pn + g, c0);
-            __stcg(A.rf + g, (float)r);
-            acc += r * r;
-            const double aux = c0 / old;
-            if ((1.0 - A.tol2 > aux) || (1.0 + A.tol2 < aux))
-                fl |= 1;
-            if (A.method == 1 && fabs(r) >= N.rmt)
-                fl |= 2;
+            long g[2];
+            double c0[2], r[2], old[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+            {
+                const int e = e0 + u * NT;
+                g[u] = e < se ? (long)A.intr[e] : -1L;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+                if (g[u] >= 0)
+                {
+                    const long x = g[u];
+                    old[u] = ldg_d(ph + x);
+                    c0[u] = P(x);
+                    r[u] = A.d[x] + N.oh2 * (6.0 * c0[u] - P(x + 1) - P(x - 1) - P(x + sy0) -
+                                             P(x - sy0) - P(x + sz0) - P(x - sz0));
+                }
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+                if (g[u] >= 0)
+                {
+                    __stcg(pn + g[u], c0[u]);
+                    __stcg(A.rf + g[u], (float)r[u]);
+                    acc += r[u] * r[u];
+                    const double aux = c0[u] / old[u];
+                    if ((1.0 - A.tol2 > aux) || (1.0 + A.tol2 < aux))
+                        fl |= 1;
+                    if (A.method == 1 && fabs(r[u]) >= N.rmt)
+                        fl |= 2;
+                }
         }
         reduce(0, acc, 0.0, fl);
         conv = !N.replay && it > 0 && !(tot_f & 1) &&
@@ -605,8 +652,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             const float *e1 = A.ec + D.off;
             for (int e = sb + tid; e < se; e += NT)
             {
-                const int v = A.cl[e];
-                const long g = v < 0 ? ~v : v;
+                const long g = A.cl[e];
                 long l = g - N.goff;
                 const int z = (int)(l / sz0);
                 l -= z * sz0;
@@ -628,8 +674,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         double rz = 0.0, rzo = 0.0;
         for (int e = sb + tid; e < se; e += NT)
         {
-            const int v = A.cl[e];
-            const long g = v < 0 ? ~v : v;
+            const long g = A.intr[e];
             const double r = (double)ldg_f(A.rf + g);
             rz += r * (double)ldg_f(A.ef + g);
             if (it > 0)
@@ -641,8 +686,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         rz_prev = rz;
         for (int e = sb + tid; e < se; e += NT)
         {
-            const int v = A.cl[e];
-            const long g = v < 0 ? ~v : v;
+            const long g = A.intr[e];
             const float z = ldg_f(A.ef + g);
             const double pnew = (double)z + (it > 0 ? beta * ldg_d(A.pv + g) : 0.0);
             __stcg(A.pv + g, pnew);
@@ -650,15 +694,30 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         }
         cluster.sync();
         double pq = 0.0;
-        for (int e = sb + tid; e < se; e += NT)
+        for (int e0 = sb + tid; e0 < se; e0 += 2 * NT)
         {
-            const int v = A.cl[e];
-            const long g = v < 0 ? ~v : v;
-            const double pc = ldg_d(A.pv + g);
-            const double lap = N.oh2 * (ldg_d(A.pv + g + 1) + ldg_d(A.pv + g - 1) +
-                                        ldg_d(A.pv + g + sy0) + ldg_d(A.pv + g - sy0) +
-                                        ldg_d(A.pv + g + sz0) + ldg_d(A.pv + g - sz0) - 6.0 * pc);
-            pq += pc * lap;
+            long g[2];
+            double pc[2], lap[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+            {
+                const int e = e0 + u * NT;
+                g[u] = e < se ? (long)A.intr[e] : -1L;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+                if (g[u] >= 0)
+                {
+                    const long x = g[u];
+                    pc[u] = ldg_d(A.pv + x);
+                    lap[u] = N.oh2 * (ldg_d(A.pv + x + 1) + ldg_d(A.pv + x - 1) +
+                                      ldg_d(A.pv + x + sy0) + ldg_d(A.pv + x - sy0) +
+                                      ldg_d(A.pv + x + sz0) + ldg_d(A.pv + x - sz0) - 6.0 * pc[u]);
+                }
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+                if (g[u] >= 0)
+                    pq += pc[u] * lap[u];
         }
         reduce(2, pq, 0.0, 0);
         alpha = tot_d[0] != 0.0 ? rz / tot_d[0] : 0.0;
@@ -668,8 +727,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     if ((it + 1) & 1)
         for (int e = sb + tid; e < se; e += NT)
         {
-            const int v = A.cl[e];
-            const long g = v < 0 ? ~v : v;
+            const long g = A.intr[e];
             A.pot[g] = ldg_d(A.pot_old + g);
         }
     if (rank == 0 && tid == 0)
