@@ -55,6 +55,7 @@
 // within max_iter iterations fails the solve, as the reference's solver does.
 #include <cooperative_groups.h>
 #include <mutex>
+#include <stdlib.h>
 
 #include "qz_amr_dev.cuh"
 
@@ -67,7 +68,7 @@ namespace qz {
 constexpr int NMG_THREADS = 512;
 constexpr int NMG_MAXLEV = 10;
 constexpr size_t NMG_SMEM_MAX = 160 * 1024; // shared-memory sub-cycle (CTA 0)
-constexpr int NMG_COARSE_SWEEPS = 24;       // FP64 red-black sweeps on the coarsest level
+constexpr int NMG_COARSE_SWEEPS = 8; // FP64 red-black sweeps on the coarsest level (default)
 
 struct NmgLev {
     int nx, ny, nz; // points per axis
@@ -108,6 +109,7 @@ struct NmgArgs {
     double tol2;
     int method;
     int n_pre, n_post;
+    int n_coarse; // red-black sweeps of the coarsest level
 };
 
 // ---- small helpers ------------------------------------------------------------------------
@@ -128,12 +130,15 @@ struct ColourWalk {
         hmax = (mx + 1) / 2;
         items = (mx > 0 && my > 0 && mz > 0) ? (long)hmax * my * mz : 0;
     }
+    // item counts stay below 2^31 (a level has at most the node grid's points)
     __device__ bool at(long t, int col, int &i, int &j, int &k) const
     {
-        const int u = (int)(t % hmax);
-        const long row = t / hmax;
-        j = 1 + (int)(row % my);
-        k = 1 + (int)(row / my);
+        const unsigned tt = (unsigned)t, hm = (unsigned)hmax;
+        const unsigned row = tt / hm;
+        const int u = (int)(tt - row * hm);
+        const unsigned kk = row / (unsigned)my;
+        j = 1 + (int)(row - kk * (unsigned)my);
+        k = 1 + (int)kk;
         i = ((((1 + j + k) & 1) == col) ? 1 : 2) + 2 * u;
         return i <= mx;
     }
@@ -195,9 +200,10 @@ __device__ __forceinline__ void dense_restrict(const float *ef, const float *ff,
     const long items = (long)mx * my * mz;
     for (long t = t0; t < items; t += nt)
     {
-        const int i = 1 + (int)(t % mx);
-        const long r = t / mx;
-        const int j = 1 + (int)(r % my), k = 1 + (int)(r / my);
+        const unsigned tt = (unsigned)t, r = tt / (unsigned)mx;
+        const int i = 1 + (int)(tt - r * (unsigned)mx);
+        const unsigned rk = r / (unsigned)my;
+        const int j = 1 + (int)(r - rk * (unsigned)my), k = 1 + (int)rk;
         const long x = i + j * sy + k * sz;
         if (!(GC ? ldg_u8(mcrs + x) : mcrs[x]))
             continue;
@@ -272,9 +278,10 @@ __device__ __forceinline__ void dense_prolong(float *e, const unsigned char *m, 
     const long items = (long)mx * my * mz;
     for (long t = t0; t < items; t += nt)
     {
-        const int i = 1 + (int)(t % mx);
-        const long r = t / mx;
-        const int j = 1 + (int)(r % my), k = 1 + (int)(r / my);
+        const unsigned tt = (unsigned)t, r = tt / (unsigned)mx;
+        const int i = 1 + (int)(tt - r * (unsigned)mx);
+        const unsigned rk = r / (unsigned)my;
+        const int j = 1 + (int)(r - rk * (unsigned)my), k = 1 + (int)rk;
         const long x = i + j * sy + k * sz;
         if (!(GF ? ldg_u8(m + x) : m[x]))
             continue;
@@ -352,9 +359,10 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         const long items = (long)mx * my * mz;
         for (long t = ct; t < items; t += CT)
         {
-            const int i = 1 + (int)(t % mx);
-            const long r = t / mx;
-            const int j = 1 + (int)(r % my), kk = 1 + (int)(r / my);
+            const unsigned tt = (unsigned)t, r = tt / (unsigned)mx;
+            const int i = 1 + (int)(tt - r * (unsigned)mx);
+            const unsigned rk = r / (unsigned)my;
+            const int j = 1 + (int)(r - rk * (unsigned)my), kk = 1 + (int)rk;
             const long g = ((long)i << k) + ((long)j << k) * sy0 + ((long)kk << k) * sz0;
             A.mc[Lk.off + i + (long)j * Lk.nx + (long)kk * Lk.nx * Lk.ny] = ldg_u8(mk0 + g);
         }
@@ -592,7 +600,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                 }
                 __syncthreads();
                 const double h2 = (double)N.h2[k];
-                for (int sw = 0; sw < NMG_COARSE_SWEEPS; sw++)
+                for (int sw = 0; sw < A.n_coarse; sw++)
                     for (int col = 0; col < 2; col++)
                     {
                         dense_sweep<false, double>(e64, f64, sub_m(k), C.nx, C.ny, C.nz, h2, col,
@@ -936,8 +944,13 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.efo = B.efo.p;
     A.tol2 = c.tol2;
     A.method = c.check_method;
-    A.n_pre = std::max(1, c.n_pre);
-    A.n_post = std::max(0, c.n_post);
+    // smoothing of the node cycles: the head's counts unless QZ_NODE_MG_SWEEPS
+    // (pre = post) and QZ_NODE_MG_COARSE (coarsest-level sweeps) set them
+    static const char *env_sw = getenv("QZ_NODE_MG_SWEEPS");
+    static const char *env_co = getenv("QZ_NODE_MG_COARSE");
+    A.n_pre = std::max(1, env_sw ? atoi(env_sw) : c.n_pre);
+    A.n_post = std::max(0, env_sw ? atoi(env_sw) : c.n_post);
+    A.n_coarse = std::max(1, env_co ? atoi(env_co) : NMG_COARSE_SWEEPS);
 
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nt * cs);
