@@ -40,8 +40,9 @@
 //
 // Execution: one cluster of CS CTAs (16 where the device allows, else 8) per
 // node, all nodes of a level in one launch.  Phases are separated by hardware
-// cluster barriers (barrier.cluster arrive.release / wait.acquire); data
-// written by other CTAs of the cluster is read with L2 loads (ld.global.cg).
+// cluster barriers (barrier.cluster arrive.release / wait.acquire), which make
+// every store before a barrier visible to every load after it across the
+// cluster (plain, L1-cached loads).
 // The fine level and the first coarse levels are swept by the whole cluster;
 // the levels small enough for shared memory run as a sub-cycle inside CTA 0
 // while the others wait at the next cluster barrier.  The FP64 residual pass
@@ -113,9 +114,16 @@ struct NmgArgs {
 };
 
 // ---- small helpers ------------------------------------------------------------------------
-__device__ __forceinline__ float ldg_f(const float *p) { return __ldcg(p); }
-__device__ __forceinline__ double ldg_d(const double *p) { return __ldcg(p); }
-__device__ __forceinline__ unsigned char ldg_u8(const unsigned char *p) { return __ldcg(p); }
+// Loads of data that other CTAs of the cluster wrote earlier in the launch:
+// plain (L1-cached) loads.  Every phase ends at a cluster barrier whose arrive
+// has release and whose wait has acquire semantics at cluster scope, so by the
+// PTX memory model a load after the barrier observes every store made before
+// it by any thread of the cluster; neighbouring stencil points then share L1
+// lines instead of each load going to L2.
+__device__ __forceinline__ float ldg_f(const float *p) { return *p; }
+__device__ __forceinline__ double ldg_d(const double *p) { return *p; }
+__device__ __forceinline__ unsigned char ldg_u8(const unsigned char *p) { return *p; }
+template <typename T> __device__ __forceinline__ void stg(T *p, T v) { *p = v; }
 
 // Items of one colour of a dense level: rows (j, k) over the interior, i of the
 // row's parity.  Item t -> (i, j, k) or false when beyond the row.
@@ -178,7 +186,7 @@ __device__ __forceinline__ void dense_sweep(T *e, const T *f, const unsigned cha
         }
         const T v = one_sixth * (-h2 * fx + s);
         if constexpr (G)
-            __stcg(e + x, v);
+            stg(e + x, v);
         else
             e[x] = v;
     }
@@ -223,7 +231,7 @@ __device__ __forceinline__ void dense_restrict(const float *ef, const float *ff,
         const float rv = (GF ? ldg_f(ff + g) : ff[g]) + foh2 * (6.0f * c - s);
         const float v = 0.5f * rv;
         if (GC)
-            __stcg(fcrs + x, v);
+            stg(fcrs + x, v);
         else
             fcrs[x] = v;
     }
@@ -287,7 +295,7 @@ __device__ __forceinline__ void dense_prolong(float *e, const unsigned char *m, 
             continue;
         const float add = prolong_at<GC>(ec, cnx, cny, i, j, k);
         if (GF)
-            __stcg(e + x, ldg_f(e + x) + add);
+            stg(e + x, ldg_f(e + x) + add);
         else
             e[x] += add;
     }
@@ -344,7 +352,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             A.cl[se - 1 - atomicAdd(&s_nblk, 1)] = g;
         else
             A.cl[sb + atomicAdd(&s_nred, 1)] = g;
-        __stcg(A.msk + g, (unsigned char)1);
+        stg(A.msk + g, (unsigned char)1);
     }
     __syncthreads();
     const int nred = s_nred; // cl[sb, sb + nred): even points; [sb + nred, se): odd
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
 #pragma unroll
             for (int u = 0; u < NB; u++)
                 if (g[u] >= 0)
-                    __stcg(A.ef + g[u], one_sixth * (-h2 * fx[u] + sm[u]));
+                    stg(A.ef + g[u], one_sixth * (-h2 * fx[u] + sm[u]));
         }
     };
 
@@ -524,8 +532,8 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             for (int u = 0; u < 2; u++)
                 if (g[u] >= 0)
                 {
-                    __stcg(pn + g[u], c0[u]);
-                    __stcg(A.rf + g[u], (float)r[u]);
+                    stg(pn + g[u], c0[u]);
+                    stg(A.rf + g[u], (float)r[u]);
                     acc += r[u] * r[u];
                     const double aux = c0[u] / old[u];
                     if ((1.0 - A.tol2 > aux) || (1.0 + A.tol2 < aux))
@@ -636,7 +644,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                 float *gek = A.ec + C.off;
                 for (long t = tid; t < P; t += NT)
                     if (smk[t])
-                        __stcg(gek + t, sek[t]);
+                        stg(gek + t, sek[t]);
             }
         }
         cluster.sync();
@@ -658,15 +666,32 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             // prolongation to the fine unknowns (this CTA's slice of the list)
             const NmgLev D = N.lv[1];
             const float *e1 = A.ec + D.off;
-            for (int e = sb + tid; e < se; e += NT)
+            for (int e0 = sb + tid; e0 < se; e0 += NB * NT)
             {
-                const long g = A.cl[e];
-                long l = g - N.goff;
-                const int z = (int)(l / sz0);
-                l -= z * sz0;
-                const int y = (int)(l / sy0);
-                const int x = (int)(l - y * sy0);
-                __stcg(A.ef + g, ldg_f(A.ef + g) + prolong_at<true>(e1, D.nx, D.ny, x, y, z));
+                long g[NB];
+                float add[NB], old[NB];
+#pragma unroll
+                for (int u = 0; u < NB; u++)
+                {
+                    const int e = e0 + u * NT;
+                    g[u] = e < se ? (long)A.cl[e] : -1L;
+                }
+#pragma unroll
+                for (int u = 0; u < NB; u++)
+                    if (g[u] >= 0)
+                    {
+                        const unsigned l = (unsigned)(g[u] - N.goff);
+                        const unsigned z = l / (unsigned)sz0;
+                        const unsigned rem = l - z * (unsigned)sz0;
+                        const unsigned y = rem / (unsigned)sy0;
+                        const unsigned x = rem - y * (unsigned)sy0;
+                        old[u] = ldg_f(A.ef + g[u]);
+                        add[u] = prolong_at<true>(e1, D.nx, D.ny, (int)x, (int)y, (int)z);
+                    }
+#pragma unroll
+                for (int u = 0; u < NB; u++)
+                    if (g[u] >= 0)
+                        stg(A.ef + g[u], old[u] + add[u]);
             }
         }
         cluster.sync();
@@ -680,25 +705,61 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         // ---- flexible conjugate gradient with z = ef (Notay 2000; Polak-Ribiere
         // beta), FP64 arithmetic on the FP32 vectors r (rf) and z ------------------
         double rz = 0.0, rzo = 0.0;
-        for (int e = sb + tid; e < se; e += NT)
+        for (int e0 = sb + tid; e0 < se; e0 += NB * NT)
         {
-            const long g = A.intr[e];
-            const double r = (double)ldg_f(A.rf + g);
-            rz += r * (double)ldg_f(A.ef + g);
-            if (it > 0)
-                rzo += r * (double)ldg_f(A.efo + g);
+            long g[NB];
+            float rv[NB], zv[NB], zo[NB];
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+            {
+                const int e = e0 + u * NT;
+                g[u] = e < se ? (long)A.intr[e] : -1L;
+            }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                {
+                    rv[u] = ldg_f(A.rf + g[u]);
+                    zv[u] = ldg_f(A.ef + g[u]);
+                    zo[u] = it > 0 ? ldg_f(A.efo + g[u]) : 0.0f;
+                }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                {
+                    rz += (double)rv[u] * (double)zv[u];
+                    rzo += (double)rv[u] * (double)zo[u];
+                }
         }
         reduce(1, rz, rzo, 0);
         rz = tot_d[0];
         const double beta = it > 0 ? (rz - tot_d[1]) / rz_prev : 0.0;
         rz_prev = rz;
-        for (int e = sb + tid; e < se; e += NT)
+        for (int e0 = sb + tid; e0 < se; e0 += NB * NT)
         {
-            const long g = A.intr[e];
-            const float z = ldg_f(A.ef + g);
-            const double pnew = (double)z + (it > 0 ? beta * ldg_d(A.pv + g) : 0.0);
-            __stcg(A.pv + g, pnew);
-            __stcg(A.efo + g, z);
+            long g[NB];
+            float zv[NB];
+            double po[NB];
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+            {
+                const int e = e0 + u * NT;
+                g[u] = e < se ? (long)A.intr[e] : -1L;
+            }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                {
+                    zv[u] = ldg_f(A.ef + g[u]);
+                    po[u] = it > 0 ? ldg_d(A.pv + g[u]) : 0.0;
+                }
+#pragma unroll
+            for (int u = 0; u < NB; u++)
+                if (g[u] >= 0)
+                {
+                    stg(A.pv + g[u], (double)zv[u] + (it > 0 ? beta * po[u] : 0.0));
+                    stg(A.efo + g[u], zv[u]);
+                }
         }
         cluster.sync();
         double pq = 0.0;
