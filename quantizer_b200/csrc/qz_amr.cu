@@ -2583,10 +2583,7 @@ int amr_potential(qz_sim *s)
                dim3(256), L.grid_total, L.pot, L.pot_old);
         // FP64: the reference's node conjugate gradient; mixed: FP32 multigrid in FP64
         // defect correction (qz_node_mg.cu)
-        int rc = s->cfg.precision == QZ_PREC_MIXED ? node_mg_level(s, L, l) : cg_level(s, L, l);
-        if (rc == NMG_RETRY_CG)
-            rc = cg_level(s, L, l);
-        if (rc)
+        if (s->cfg.precision == QZ_PREC_MIXED ? node_mg_level(s, L, l) : cg_level(s, L, l))
             return QZ_FAILURE;
     }
     return QZ_SUCCESS;

@@ -432,9 +432,6 @@ int solve_zero_bc(qz_sim *s, double *lam, double *f, double rtol, double *scratc
 int check_flags(qz_sim *s);                   // qz_capi.cu
 int step_core(qz_sim *s, double dt);          // qz_capi.cu: one fixed-dt step, no flag check
 void adjoint_free(qz_sim *s);                 // qz_adjoint.cu
-// QZ_SUCCESS, QZ_FAILURE, or NMG_RETRY_CG: a node group's barrier gave up, solve
-// the level by the conjugate gradient instead
-constexpr int NMG_RETRY_CG = 2;
 int node_mg_level(qz_sim *s, AmrLevel &L, int level_index); // qz_node_mg.cu
 // solver schedule (qz_capi.cu): counts of the next solve in replay mode (false and
 // an error when the schedule is exhausted); append in record mode

@@ -85,7 +85,6 @@ struct NmgNode {
     double oh2;     // 1 / H^2
     double thr;     // residual test: r.r threshold (check methods 0 and 2)
     double rmt;     // check method 1: tol * (4 pi G rho_mean)
-    int G;          // clusters working on the node (a node group)
     int cap;        // most iterations (a replayed schedule: exactly this many)
     int replay;     // no convergence test: run cap iterations
     int smem_need;  // bytes of the sub-cycle
@@ -106,11 +105,6 @@ struct NmgArgs {
     float *ec, *fc;        // coarse levels
     unsigned char *mc;
     int *status;           // per entry: converged, iterations
-    const int2 *cmap;      // per cluster: node entry, group index inside the node
-    unsigned *nbar;        // per node entry: node barrier words (count, -, generation, gave up)
-    double *gpart;         // per node entry: partials of the three reductions, per CTA
-    int gstride;           // CTAs a node entry's partial rows hold (most G x CS)
-    int *err;              // bit 0: a node barrier gave up
     double *pv;            // flexible CG direction (grid-pool layout, zero off the interior)
     float *efo;            // the previous preconditioned residual (interior points)
     double tol2;
@@ -120,44 +114,15 @@ struct NmgArgs {
 };
 
 // ---- small helpers ------------------------------------------------------------------------
-// Loads of data that other CTAs of the node group wrote earlier in the launch:
-// L2 loads (ld.global.cg), never a line an SM's L1 kept from an earlier phase.
-__device__ __forceinline__ float ldg_f(const float *p) { return __ldcg(p); }
-__device__ __forceinline__ double ldg_d(const double *p) { return __ldcg(p); }
-__device__ __forceinline__ unsigned char ldg_u8(const unsigned char *p) { return __ldcg(p); }
-
-constexpr int NMG_BAR_POLL_LIMIT = 1 << 21;
-
-// Barrier of the G cluster leaders of a node group (the arrival count and the
-// generation in global memory, the pattern of gbar_sync with G participants):
-// returns false once a wait of this node has given up (then at once).
-__device__ __forceinline__ bool node_bar_leader(unsigned *w, int G, int *err)
-{
-    unsigned long long gw = gbar_ld_acquire64(&w[2]);
-    const unsigned gen = (unsigned)gw;
-    if ((gw >> 32) != 0)
-        return false;
-    unsigned prev;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(&w[0]) : "memory");
-    if (prev == (unsigned)G - 1)
-    {
-        asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&w[0]) : "memory");
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&w[2]) : "memory");
-        return true;
-    }
-    for (int polls = 0;; polls++)
-    {
-        gw = gbar_ld_acquire64(&w[2]);
-        if ((unsigned)gw != gen)
-            return true;
-        if ((gw >> 32) != 0 || polls > NMG_BAR_POLL_LIMIT)
-        {
-            atomicExch(&w[3], 1u);
-            atomicOr(err, 1);
-            return false;
-        }
-    }
-}
+// Loads of data that other CTAs of the cluster wrote earlier in the launch:
+// plain (L1-cached) loads.  Every phase ends at a cluster barrier whose arrive
+// has release and whose wait has acquire semantics at cluster scope, so by the
+// PTX memory model a load after the barrier observes every store made before
+// it by any thread of the cluster; neighbouring stencil points then share L1
+// lines instead of each load going to L2.
+__device__ __forceinline__ float ldg_f(const float *p) { return *p; }
+__device__ __forceinline__ double ldg_d(const double *p) { return *p; }
+__device__ __forceinline__ unsigned char ldg_u8(const unsigned char *p) { return *p; }
 template <typename T> __device__ __forceinline__ void stg(T *p, T v) { *p = v; }
 
 // Items of one colour of a dense level: rows (j, k) over the interior, i of the
@@ -342,44 +307,25 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     cg::cluster_group cluster = cg::this_cluster();
     const int CS = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
-    const int2 cm = A.cmap[blockIdx.x / CS];
-    const int ent = cm.x;
+    const int ent = (int)(blockIdx.x / CS);
     __shared__ NmgNode N;
-    __shared__ int s_ok;
     __shared__ double wsum[32], wsum2[32];
     __shared__ int wflag[32];
+    // this CTA's partials of the three reductions of an iteration (read by the
+    // others through distributed shared memory; one slot set per reduction, so a
+    // slot is rewritten only an iteration later, many cluster barriers on)
+    __shared__ double part_d[3][2];
+    __shared__ int part_f[3];
     __shared__ double tot_d[2];
     __shared__ int tot_f;
     extern __shared__ __align__(16) unsigned char nmg_dyn[];
     const int tid = threadIdx.x, NT = blockDim.x;
     if (tid == 0)
-    {
         N = A.tab[ent];
-        s_ok = 1;
-    }
     __syncthreads();
-    // this CTA's place in the node group: gr of GCS CTAs
-    const int G = N.G, GCS = G * CS, gr = cm.y * CS + rank;
-    const long ct = (long)gr * NT + tid, CT = (long)GCS * NT;
+    const long ct = (long)rank * NT + tid, CT = (long)CS * NT;
     const int nl = N.ie - N.ib;
-    const int sb = N.ib + (int)((long)nl * gr / GCS), se = N.ib + (int)((long)nl * (gr + 1) / GCS);
-    // Node-wide barrier: the cluster's barrier, then (G > 1) its leader meets the
-    // other clusters' leaders, then the cluster's barrier again.  The leader's
-    // outcome reaches the whole cluster through distributed shared memory, so
-    // every CTA of a cluster takes the same branches; a node whose barrier gave
-    // up stops at its next decision (and the host solves the level again by the
-    // conjugate gradient).
-    bool abort_node = false;
-    auto nsync = [&]() {
-        cluster.sync();
-        if (G > 1)
-        {
-            if (rank == 0 && tid == 0 && s_ok)
-                s_ok = node_bar_leader(A.nbar + 4 * ent, G, A.err) ? 1 : 0;
-            cluster.sync();
-            abort_node = abort_node || *cluster.map_shared_rank(&s_ok, 0) == 0;
-        }
-    };
+    const int sb = N.ib + (int)((long)nl * rank / CS), se = N.ib + (int)((long)nl * (rank + 1) / CS);
     const NmgLev L0 = N.lv[0];
     const long sy0 = L0.nx, sz0 = (long)L0.nx * L0.ny;
     float *ef = A.ef + N.goff;
@@ -410,7 +356,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
     }
     __syncthreads();
     const int nred = s_nred; // cl[sb, sb + nred): even points; [sb + nred, se): odd
-    nsync();
+    cluster.sync();
     // set-up 2: coarse masks, X is an unknown where the fine point 2^k X is one
     for (int k = 1; k < N.nlev; k++)
     {
@@ -429,9 +375,9 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             A.mc[Lk.off + i + (long)j * Lk.nx + (long)kk * Lk.nx * Lk.ny] = ldg_u8(mk0 + g);
         }
     }
-    nsync();
-    // CTA 0 of the group: zero the sub-cycle arrays once and copy their masks
-    if (gr == 0)
+    cluster.sync();
+    // CTA 0: zero the sub-cycle arrays once and copy their masks
+    if (rank == 0)
     {
         for (int k = N.nsmall; k < N.nlev; k++)
         {
@@ -514,9 +460,6 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             wflag[tid >> 5] = f;
         }
         __syncthreads();
-        // one row of partials per node entry and reduction; a row is rewritten
-        // only an iteration later, many node barriers on
-        double *row = A.gpart + ((long)ent * 3 + slot) * 3L * A.gstride;
         if (tid == 0)
         {
             double t = 0.0, u = 0.0;
@@ -527,20 +470,21 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                 u += wsum2[w];
                 g |= wflag[w];
             }
-            stg(row + 3 * gr, t);
-            stg(row + 3 * gr + 1, u);
-            stg(row + 3 * gr + 2, (double)g);
+            part_d[slot][0] = t;
+            part_d[slot][1] = u;
+            part_f[slot] = g;
         }
-        nsync();
+        cluster.sync();
         if (tid == 0)
         {
             double t = 0.0, u = 0.0;
             int g = 0;
-            for (int r = 0; r < GCS; r++)
+            for (int r = 0; r < CS; r++)
             {
-                t += ldg_d(row + 3 * r);
-                u += ldg_d(row + 3 * r + 1);
-                g |= (int)ldg_d(row + 3 * r + 2);
+                const double *pr = cluster.map_shared_rank(&part_d[slot][0], r);
+                t += pr[0];
+                u += pr[1];
+                g |= *cluster.map_shared_rank(&part_f[slot], r);
             }
             tot_d[0] = t;
             tot_d[1] = u;
@@ -601,7 +545,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
         reduce(0, acc, 0.0, fl);
         conv = !N.replay && it > 0 && !(tot_f & 1) &&
                (A.method == 1 ? !(tot_f & 2) : tot_d[0] < N.thr);
-        if (conv || it >= N.cap || abort_node)
+        if (conv || it >= N.cap)
             break;
 
         // ---- one FP32 V-cycle on (ef, rf) -----------------------------------------
@@ -609,23 +553,23 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             for (int col = 0; col < 2; col++)
             {
                 fine_sweep(col, sw == 0 && col == 0);
-                nsync();
+                cluster.sync();
             }
         for (int k = 1; k < N.nsmall; k++)
         {
             const NmgLev F = N.lv[k - 1], C = N.lv[k];
             dense_restrict<true, true>(ge(k - 1), gf(k - 1), F.nx, F.ny, 1.0f / N.h2[k - 1],
                                        A.fc + C.off, A.mc + C.off, C.nx, C.ny, C.nz, ct, CT);
-            nsync();
+            cluster.sync();
             for (int sw = 0; sw < A.n_pre; sw++)
                 for (int col = 0; col < 2; col++)
                 {
                     dense_sweep<true, float>(A.ec + C.off, A.fc + C.off, A.mc + C.off, C.nx, C.ny,
                                              C.nz, N.h2[k], col, sw == 0 && col == 0, ct, CT);
-                    nsync();
+                    cluster.sync();
                 }
         }
-        if (gr == 0)
+        if (rank == 0)
         {
             // sub-cycle of the small levels in shared memory
             const int ks = N.nsmall;
@@ -703,19 +647,19 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                         stg(gek + t, sek[t]);
             }
         }
-        nsync();
+        cluster.sync();
         for (int k = N.nsmall - 1; k >= 1; k--)
         {
             const NmgLev C = N.lv[k], D = N.lv[k + 1];
             dense_prolong<true, true>(A.ec + C.off, A.mc + C.off, C.nx, C.ny, C.nz, A.ec + D.off,
                                       D.nx, D.ny, ct, CT);
-            nsync();
+            cluster.sync();
             for (int sw = 0; sw < A.n_post; sw++)
                 for (int col = 0; col < 2; col++)
                 {
                     dense_sweep<true, float>(A.ec + C.off, A.fc + C.off, A.mc + C.off, C.nx, C.ny,
                                              C.nz, N.h2[k], col, false, ct, CT);
-                    nsync();
+                    cluster.sync();
                 }
         }
         {
@@ -750,12 +694,12 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                         stg(A.ef + g[u], old[u] + add[u]);
             }
         }
-        nsync();
+        cluster.sync();
         for (int sw = 0; sw < A.n_post; sw++)
             for (int col = 0; col < 2; col++)
             {
                 fine_sweep(col, false);
-                nsync();
+                cluster.sync();
             }
 
         // ---- flexible conjugate gradient with z = ef (Notay 2000; Polak-Ribiere
@@ -817,7 +761,7 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
                     stg(A.efo + g[u], zv[u]);
                 }
         }
-        nsync();
+        cluster.sync();
         double pq = 0.0;
         for (int e0 = sb + tid; e0 < se; e0 += 2 * NT)
         {
@@ -855,12 +799,12 @@ __global__ void __launch_bounds__(NMG_THREADS, 1) k_node_mg(const __grid_constan
             const long g = A.intr[e];
             A.pot[g] = ldg_d(A.pot_old + g);
         }
-    if (gr == 0 && tid == 0)
+    if (rank == 0 && tid == 0)
     {
         A.status[2 * ent] = conv ? 1 : 0;
         A.status[2 * ent + 1] = it;
     }
-    // no CTA leaves while another may still read its leader's barrier outcome
+    // no CTA leaves while another may still read its partials
     cluster.sync();
 }
 
@@ -869,9 +813,7 @@ struct NodeMgBufs {
     DBuf<NmgNode> tab;
     DBuf<int> cl, status;
     DBuf<float> ef, rf, ec, fc, efo;
-    DBuf<double> pv, gpart;
-    DBuf<int2> cmap;
-    DBuf<unsigned> nbar;
+    DBuf<double> pv;
     DBuf<unsigned char> msk, mc;
 };
 
@@ -887,11 +829,9 @@ static NodeMgBufs &bufs_of(qz_sim *s, int level)
 }
 
 // Cluster size and dynamic shared memory of the launch (set once).
-// Cluster size of the launch and how many such clusters the device holds at
-// once (set once): node groups must be resident together.
-static int cluster_size(int *max_active)
+static int cluster_size(size_t smem)
 {
-    static int cs = 0, act = 0;
+    static int cs = 0;
     static std::once_flag once;
     std::call_once(once, [&] {
         cudaFuncSetAttribute((const void *)k_node_mg, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -915,19 +855,14 @@ static int cluster_size(int *max_active)
                 n > 0)
             {
                 cs = c;
-                act = n;
                 break;
             }
         }
         cudaGetLastError();
     });
-    *max_active = act;
+    (void)smem;
     return cs;
 }
-
-// Interior points a cluster takes in a node group (a node of more points gets
-// several clusters, up to what the device holds at once).
-constexpr long NMG_PTS_PER_CLUSTER = 32768;
 
 int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
 {
@@ -1037,59 +972,16 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         set_error("node multigrid buffers");
         return QZ_FAILURE;
     }
-    int max_active = 0;
-    const int cs = cluster_size(&max_active);
+    const int cs = cluster_size(smem);
     if (cs < 1)
     {
         set_error("node multigrid: no cluster of the kernel can be resident");
         return QZ_FAILURE;
     }
-    // node groups: more clusters for larger nodes while all of the launch's
-    // clusters fit on the device at once (they wait on one another)
-    static const char *env_pc = getenv("QZ_NODE_MG_POINTS_PER_CLUSTER");
-    const long ppc = env_pc ? std::max(1L, atol(env_pc)) : NMG_PTS_PER_CLUSTER;
-    int total = 0;
-    for (auto &N : tab)
-    {
-        N.G = (int)std::max(1L, std::min(16L, ((long)(N.ie - N.ib) + ppc - 1) / ppc));
-        total += N.G;
-    }
-    while (total > max_active)
-    {
-        int big = 0;
-        for (int e = 1; e < (int)tab.size(); e++)
-            if (tab[e].G > tab[big].G)
-                big = e;
-        if (tab[big].G == 1)
-            break; // every node alone: no waits between clusters
-        tab[big].G--;
-        total--;
-    }
-    int gmax = 1;
-    std::vector<int2> cmap;
-    for (int e = 0; e < (int)tab.size(); e++)
-    {
-        gmax = std::max(gmax, tab[e].G);
-        for (int g = 0; g < tab[e].G; g++)
-            cmap.push_back(make_int2(e, g));
-    }
-    const int nclusters = (int)cmap.size();
-    const int gstride = gmax * cs;
-    if (!B.cmap.ensure(s->mem, nclusters) || !B.nbar.ensure(s->mem, 4L * nt + 4) ||
-        !B.gpart.ensure(s->mem, 9L * nt * gstride))
-    {
-        set_error("node multigrid buffers");
-        return QZ_FAILURE;
-    }
     if (!check_cuda(cudaMemcpyAsync(B.tab.p, tab.data(), nt * sizeof(NmgNode),
                                     cudaMemcpyHostToDevice, s->stream),
-                    "node multigrid table") ||
-        !check_cuda(cudaMemcpyAsync(B.cmap.p, cmap.data(), nclusters * sizeof(int2),
-                                    cudaMemcpyHostToDevice, s->stream),
-                    "node multigrid cluster map"))
+                    "node multigrid table"))
         return QZ_FAILURE;
-    // barrier words and the error word (after the nodes' four words) start at zero
-    cudaMemsetAsync(B.nbar.p, 0, (4L * nt + 4) * sizeof(unsigned), s->stream);
     cudaMemsetAsync(B.msk.p, 0, L.grid_total, s->stream);
     cudaMemsetAsync(B.ef.p, 0, L.grid_total * sizeof(float), s->stream);
     cudaMemsetAsync(B.ec.p, 0, std::max(coarse, 1L) * sizeof(float), s->stream);
@@ -1111,11 +1003,6 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.status = B.status.p;
     A.pv = B.pv.p;
     A.efo = B.efo.p;
-    A.cmap = B.cmap.p;
-    A.nbar = B.nbar.p;
-    A.err = reinterpret_cast<int *>(B.nbar.p + 4L * nt);
-    A.gpart = B.gpart.p;
-    A.gstride = gstride;
     A.tol2 = c.tol2;
     A.method = c.check_method;
     // smoothing of the node cycles: the head's counts unless QZ_NODE_MG_SWEEPS
@@ -1127,7 +1014,7 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.n_coarse = std::max(1, env_co ? atoi(env_co) : NMG_COARSE_SWEEPS);
 
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nclusters * cs);
+    cfg.gridDim = dim3(nt * cs);
     cfg.blockDim = dim3(NMG_THREADS);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s->stream;
@@ -1153,23 +1040,12 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
         cudaEventRecord(ee, s->stream);
         s->prof_pending.push_back({QZ_PROF_NODE_MG, 0.0, eb, ee});
     }
-    std::vector<int> st(2 * nt + 1);
+    std::vector<int> st(2 * nt);
     if (!check_cuda(cudaMemcpyAsync(st.data(), B.status.p, 2L * nt * sizeof(int),
                                     cudaMemcpyDeviceToHost, s->stream),
                     "node multigrid status") ||
-        !check_cuda(cudaMemcpyAsync(st.data() + 2 * nt, A.err, sizeof(int),
-                                    cudaMemcpyDeviceToHost, s->stream),
-                    "node multigrid error word") ||
         !check_cuda(cudaStreamSynchronize(s->stream), "node multigrid sync"))
         return QZ_FAILURE;
-    if (st[2 * nt])
-    {
-        // a node group's barrier gave up (its clusters were not resident together):
-        // the caller solves the level again by the conjugate gradient, from the
-        // iterate in pot (pot and pot_old hold the same boundary values)
-        s->stats.error_flags |= E_BARRIER;
-        return NMG_RETRY_CG;
-    }
     int worst = 0, unconv = 0;
     double pts_it = 0.0;
     for (int e = 0; e < nt; e++)
@@ -1226,9 +1102,6 @@ void node_mg_free(qz_sim *s)
         B.mc.release(s->mem);
         B.pv.release(s->mem);
         B.efo.release(s->mem);
-        B.gpart.release(s->mem);
-        B.cmap.release(s->mem);
-        B.nbar.release(s->mem);
     }
     delete s->node_mg;
     s->node_mg = nullptr;
