@@ -108,8 +108,8 @@ def ensemble_members(wl: dict, seed: int = 0) -> list:
     As = rng.uniform(0.02, 0.08, m)
     return [(int(n), float(a), 5 if n < 16384 else 6) for n, a in zip(ns, As)]
 METRIC = "particle-steps/s"
-MIXED_DESC = ("fp32 multigrid cycles in fp64 defect correction (head: persistent V-cycles; "
-              "refinement nodes: one thread-block cluster per node)")
+MIXED_DESC = ("fp32 head multigrid cycles in fp64 defect correction (convergence test in the "
+              "launch, every iteration); refinement nodes by the fp64 node conjugate gradient")
 
 
 def log(*a):
@@ -686,6 +686,32 @@ def main() -> int:
                  "max_rel_force_err_mixed_vs_fp64": float(errs.max()),
                  "median_rel_force_err_mixed_vs_fp64": float(np.median(errs))}
         ref_sim.close()
+        # the same form with the refinement nodes solved by the FP32 node multigrid
+        # (flexible conjugate gradient preconditioned by V-cycles) instead of the
+        # reference's FP64 node conjugate gradient
+        mg_sim = core.Simulation(ic, wl["lmin"], precision=wl["variant"],
+                                 node_solver=core.QZ_NODE_MG, **simcfg)
+        mg_sim.init_forces()
+        for _ in range(W):
+            mg_sim.step(dt, 1)
+        barrier()
+        sm0 = mg_sim.stats()
+        ms_mg = timed_steps_on(mg_sim, lambda: mg_sim.step(dt, 1), K)
+        sm1 = mg_sim.stats()
+        t_mg = replicas.max_over_ranks(ms_mg, dev)
+        mg_sim.set_particles(state)
+        mg_sim.set_accelerations(state["ax"], state["ay"], state["az"])
+        mg_sim.step(dt, 1)
+        pm = mg_sim.particles()
+        diff = np.sqrt(sum((pm[k] - f64[k]) ** 2 for k in ("ax", "ay", "az")))
+        em = diff / np.maximum(a_p, 1e-300)
+        plain["node_multigrid"] = {
+            "value": world * wl["n"] * K / (t_mg / 1e3), "ms_per_step": t_mg / K,
+            "node_mg_iterations_per_step":
+                (sm1.node_mg_iterations - sm0.node_mg_iterations) / K,
+            "max_rel_force_err_vs_fp64": float(em.max()),
+            "median_rel_force_err_vs_fp64": float(np.median(em))}
+        mg_sim.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -111,7 +111,16 @@ typedef struct qz_config {
      * particles to them (each level's node of a particle from its parent's box
      * status, as the construction does) instead of rebuilding the tree */
     int freeze_tree;
+    /* solver of the refinement nodes: QZ_NODE_CG the reference's node
+     * conjugate gradient (FP64; conjugate_gradient.c:322-463), QZ_NODE_MG FP32
+     * multigrid V-cycles preconditioning a flexible conjugate gradient in FP64
+     * (one thread-block cluster per node); both stop at the reference's
+     * convergence test */
+    int node_solver;
 } qz_config;
+
+#define QZ_NODE_CG 0
+#define QZ_NODE_MG 1
 
 typedef struct qz_stats {
     long long vcycles_total;   /* V-cycles (FP64 or FP32 inner) since creation */

@@ -23,6 +23,8 @@ QZ_GS_REDBLACK = 0
 QZ_GS_LEX = 1
 QZ_PREC_FP64 = 0
 QZ_PREC_MIXED = 1
+QZ_NODE_CG = 0
+QZ_NODE_MG = 1
 FIELDS = {"pot": 0, "pot_old": 1, "d": 2, "ax": 3, "ay": 4, "az": 5}
 
 _P = C.POINTER(C.c_double)
@@ -42,6 +44,7 @@ class Config(C.Structure):
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
         ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
         ("mg_points_per_thread", C.c_int), ("freeze_tree", C.c_int),
+        ("node_solver", C.c_int),
     ]
 
 

@@ -2581,9 +2581,9 @@ int amr_potential(qz_sim *s)
                    L.intr_node.p, L.nodes.p, P.nodes.p, P.pot, L.pot);
         launch(s, QZ_PROF_OTHER, 16.0 * L.grid_total, k_copy_d, dim3(blocks_for(L.grid_total, 256)),
                dim3(256), L.grid_total, L.pot, L.pot_old);
-        // FP64: the reference's node conjugate gradient; mixed: FP32 multigrid in FP64
-        // defect correction (qz_node_mg.cu)
-        if (s->cfg.precision == QZ_PREC_MIXED ? node_mg_level(s, L, l) : cg_level(s, L, l))
+        // the reference's node conjugate gradient, or FP32 multigrid cycles
+        // preconditioning a flexible conjugate gradient (qz_node_mg.cu)
+        if (s->cfg.node_solver == QZ_NODE_MG ? node_mg_level(s, L, l) : cg_level(s, L, l))
             return QZ_FAILURE;
     }
     return QZ_SUCCESS;

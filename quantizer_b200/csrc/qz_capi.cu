@@ -342,6 +342,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->cg_variant = 0;
     c->mg_points_per_thread = 4;
     c->freeze_tree = 0;
+    c->node_solver = QZ_NODE_CG;
     return QZ_SUCCESS;
 }
 

@@ -70,6 +70,10 @@ constexpr int NMG_THREADS = 512;
 constexpr int NMG_MAXLEV = 10;
 constexpr size_t NMG_SMEM_MAX = 160 * 1024; // shared-memory sub-cycle (CTA 0)
 constexpr int NMG_COARSE_SWEEPS = 8; // FP64 red-black sweeps on the coarsest level (default)
+// Red-black sweeps before and after each coarse correction.  Measured on the
+// 1M-particle sphere with three refinement levels (node solves per step): 2
+// sweeps 69 iterations, 14.9 ms; 3 sweeps 36, 9.7 ms; 4 sweeps 27, 8.6 ms.
+constexpr int NMG_SWEEPS = 4;
 
 struct NmgLev {
     int nx, ny, nz; // points per axis
@@ -1005,12 +1009,13 @@ int node_mg_level(qz_sim *s, AmrLevel &L, int level_index)
     A.efo = B.efo.p;
     A.tol2 = c.tol2;
     A.method = c.check_method;
-    // smoothing of the node cycles: the head's counts unless QZ_NODE_MG_SWEEPS
-    // (pre = post) and QZ_NODE_MG_COARSE (coarsest-level sweeps) set them
+    // smoothing of the node cycles: NMG_SWEEPS red-black sweeps before and after
+    // the coarse correction unless QZ_NODE_MG_SWEEPS (pre = post) and
+    // QZ_NODE_MG_COARSE (coarsest-level sweeps) set them
     static const char *env_sw = getenv("QZ_NODE_MG_SWEEPS");
     static const char *env_co = getenv("QZ_NODE_MG_COARSE");
-    A.n_pre = std::max(1, env_sw ? atoi(env_sw) : c.n_pre);
-    A.n_post = std::max(0, env_sw ? atoi(env_sw) : c.n_post);
+    A.n_pre = std::max(1, env_sw ? atoi(env_sw) : NMG_SWEEPS);
+    A.n_post = std::max(0, env_sw ? atoi(env_sw) : NMG_SWEEPS);
     A.n_coarse = std::max(1, env_co ? atoi(env_co) : NMG_COARSE_SWEEPS);
 
     cudaLaunchConfig_t cfg = {};

@@ -1,7 +1,8 @@
-"""The mixed-precision form with refinement: FP32 multigrid V-cycles on every
-refinement node inside FP64 defect correction (qz_node_mg.cu), against the FP64
-pipeline whose node solves are the reference's conjugate gradient (pinned to
-the compiled reference in test_gpu_amr.py).
+"""The mixed-precision form with the node multigrid solver (node_solver =
+QZ_NODE_MG): FP32 V-cycles on every refinement node preconditioning a flexible
+conjugate gradient in FP64 (qz_node_mg.cu), with FP32 head cycles, against the
+FP64 pipeline whose node solves are the reference's conjugate gradient (pinned
+to the compiled reference in test_gpu_amr.py).
 
 Bars (relative to the field's largest magnitude, per level and node):
   node potentials          1e-8   (both solves stop at the reference's test:
@@ -9,7 +10,7 @@ Bars (relative to the field's largest magnitude, per level and node):
   particle accelerations   1e-5   largest relative force error per particle
                                   (the north-star bound for the mixed form)
   positions after 3 steps  1e-10  box units
-Also: the mixed form runs no conjugate-gradient iteration and is
+Also: the node multigrid runs no node conjugate-gradient iteration and is
 bit-reproducible (two runs equal), and the residual-test variants
 (check_poisson_error_method 1 and 2) converge with it.
 """
@@ -47,7 +48,7 @@ def test_node_multigrid_matches_fp64_conjugate_gradient(n, a, lmin, lmax, seed):
     ic = ics.plummer(n, a=a, seed=seed)
     dt = 1e-3 * ics.crossing_time(a)
     p64, pot64, st64 = _run(ic, lmin, lmax, dt, 3)
-    pmx, potmx, stmx = _run(ic, lmin, lmax, dt, 3, precision=core.QZ_PREC_MIXED)
+    pmx, potmx, stmx = _run(ic, lmin, lmax, dt, 3, precision=core.QZ_PREC_MIXED, node_solver=core.QZ_NODE_MG)
     assert stmx.levels == st64.levels and stmx.nodes == st64.nodes
     assert stmx.levels >= 3
     assert stmx.cg_iterations == 0 and stmx.node_mg_iterations > 0
@@ -65,8 +66,8 @@ def test_node_multigrid_matches_fp64_conjugate_gradient(n, a, lmin, lmax, seed):
 def test_node_multigrid_is_bit_reproducible():
     ic = ics.plummer(60000, a=0.03, seed=6)
     dt = 1e-3 * ics.crossing_time(0.03)
-    a, pa, sa = _run(ic, 6, 8, dt, 2, precision=core.QZ_PREC_MIXED)
-    b, pb, sb = _run(ic, 6, 8, dt, 2, precision=core.QZ_PREC_MIXED)
+    a, pa, sa = _run(ic, 6, 8, dt, 2, precision=core.QZ_PREC_MIXED, node_solver=core.QZ_NODE_MG)
+    b, pb, sb = _run(ic, 6, 8, dt, 2, precision=core.QZ_PREC_MIXED, node_solver=core.QZ_NODE_MG)
     assert sa.node_mg_iterations == sb.node_mg_iterations
     for k in ("x", "y", "z", "ax", "ay", "az"):
         np.testing.assert_array_equal(a[k], b[k])
@@ -79,6 +80,6 @@ def test_node_multigrid_check_methods(method):
     ic = ics.plummer(60000, a=0.03, seed=7)
     dt = 1e-3 * ics.crossing_time(0.03)
     p64, _, _ = _run(ic, 6, 8, dt, 2, check_method=method)
-    pmx, _, st = _run(ic, 6, 8, dt, 2, check_method=method, precision=core.QZ_PREC_MIXED)
+    pmx, _, st = _run(ic, 6, 8, dt, 2, check_method=method, precision=core.QZ_PREC_MIXED, node_solver=core.QZ_NODE_MG)
     assert st.node_mg_iterations > 0
     assert _force_err(pmx, p64).max() < 1e-5
