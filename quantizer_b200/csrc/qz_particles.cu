@@ -407,11 +407,12 @@ __global__ void __launch_bounds__(SEG_LONG_THREADS)
 __global__ void k_point_gather(int L, long D, const int *__restrict__ cell_seg,
                                const double *__restrict__ cs, double *__restrict__ d)
 {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= D * D * D)
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x, uD = (unsigned)D;
+    if (t >= uD * uD * uD)
         return;
     const long B = D - 1;
-    int gx = (int)(t % D), gy = (int)((t / D) % D), gz = (int)(t / (D * D));
+    const unsigned q = t / uD, r = q / uD;
+    const int gx = (int)(t - q * uD), gy = (int)(q - r * uD), gz = (int)r;
     double acc = 0.0;
     for (int c = 0; c < 2; c++)
     {
@@ -544,10 +545,12 @@ __global__ void k_grid_accel_head(int L, long D, int stencil, int periodic,
                                   double *__restrict__ ay, double *__restrict__ az)
 {
     const int m = (1 << L) - 1; // interior points per axis: box coords 2..2^L
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)m * m * m)
+    // 32-bit index arithmetic (m^3 < 2^32 for every head grid this library builds)
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x, um = (unsigned)m;
+    if (t >= um * um * um)
         return;
-    int i = 2 + (int)(t % m), j = 2 + (int)((t / m) % m), k = 2 + (int)(t / ((long)m * m));
+    const unsigned q = t / um, r = q / um;
+    const int i = 2 + (int)(t - q * um), j = 2 + (int)(q - r * um), k = 2 + (int)r;
     const long D2 = D * D;
     long g = i + j * D + k * D2;
     const double H = 1.0 / (1 << L);

@@ -60,53 +60,51 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
 
 // One whole red-black sweep per launch (the result of a red k_gs_rb launch
 // followed by a black one, bit for bit), reading phi from `pin` and writing
-// `pout` (ping-pong: CTAs never race on halos), with every field value loaded
+// `pout` (ping-pong: CTAs never race on halos), with every phi value loaded
 // from memory once per CTA and written once.  A CTA owns a tile of ZM_TX x
 // ZM_TY interior points in (x, y) and a chunk of ZM_TZ planes in z, and marches
-// up the chunk with a ring of planes in shared memory, staged by asynchronous
-// copies (cp.async) one plane ahead of the arithmetic:
-//   step s: load plane s+1 (phi window of the tile plus 2 points a side, rho
-//           window plus 1 point a side);
+// up the chunk with a ring of phi planes in shared memory, staged by
+// asynchronous copies (cp.async) one plane ahead of the arithmetic:
+//   step s: load plane s+1 (the tile plus 2 points a side);
 //           red points of plane s-1 over the tile and a 1-point ring around it
 //           (from the old black values of planes s-2, s-1, s);
 //           black points of plane s-2 over the tile (from the new red values
-//           of planes s-3, s-2, s-1);
-//           plane s-2 of the tile to pout.
-// A ring point is a neighbouring CTA's tile point: both compute it from the
-// same old values, so they agree bit for bit.  Algorithmic traffic: 24 B a
-// point (phi and rho read, phi written); halos add (68 x 20 + 66 x 18) /
-// (64 x 16) - 2 = 0.49 reads a point, mostly served by L2.
+//           of planes s-3, s-2, s-1), and both points of each x pair of plane
+//           s-2 written to pout.
+// rho is read from memory where a point is updated (coalesced along x).  A
+// ring point is a neighbouring CTA's tile point: both compute it from the same
+// old values, so they agree bit for bit.  Algorithmic traffic: 24 B a point
+// (phi and rho read, phi written); the phi halo adds (68 x 20) / (64 x 16) - 1
+// = 0.33 reads a point and the rho ring 0.16, mostly served by L2.
 constexpr int ZM_TX = 64, ZM_TY = 16, ZM_TZ = 32;
 constexpr int ZM_WX = ZM_TX + 4, ZM_WY = ZM_TY + 4; // phi window
-constexpr int ZM_RX = ZM_TX + 2, ZM_RY = ZM_TY + 2; // red ring and rho window
-constexpr int ZM_PH = 5, ZM_RH = 4;                 // planes held (one in flight)
+constexpr int ZM_RX = ZM_TX + 2, ZM_RY = ZM_TY + 2; // red ring
+constexpr int ZM_PH = 5;                            // planes held (one in flight)
 constexpr int ZM_THREADS = 512;
 
 template <typename T> constexpr size_t zm_smem_bytes()
 {
-    return sizeof(T) * ((size_t)ZM_PH * ZM_WX * ZM_WY + (size_t)ZM_RH * ZM_RX * ZM_RY);
+    return sizeof(T) * (size_t)ZM_PH * ZM_WX * ZM_WY;
 }
 
-__device__ __forceinline__ int zm_slot(int z, int ring) { return ((z % ring) + ring) % ring; }
+__device__ __forceinline__ int zm_slot(int z) { return ((z % ZM_PH) + ZM_PH) % ZM_PH; }
 
 template <typename T>
 __global__ void __launch_bounds__(ZM_THREADS)
     k_gs_rb_zm(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w)
 {
     extern __shared__ __align__(16) unsigned char zm_raw[];
-    T *PH = reinterpret_cast<T *>(zm_raw);           // [ZM_PH][ZM_WY][ZM_WX]
-    T *RH = PH + (size_t)ZM_PH * ZM_WX * ZM_WY;      // [ZM_RH][ZM_RY][ZM_RX]
+    T *PH = reinterpret_cast<T *>(zm_raw); // [ZM_PH][ZM_WY][ZM_WX]
     const int n = pin.n, m = n - 2, last = n - 1;
     const int tid = threadIdx.x;
     const int x0 = 1 + blockIdx.x * ZM_TX, y0 = 1 + blockIdx.y * ZM_TY;
     const int kb = 1 + blockIdx.z * ZM_TZ, ke = min(m, kb + ZM_TZ - 1);
     const T one_sixth = (T)(1.0 / 6.0);
-    // asynchronous loads of plane z: phi window (in range) and, for interior
-    // planes, the rho window (in range)
+    // asynchronous loads of the phi window of plane z (points in range)
     auto load = [&](int z) {
         if (z >= 0 && z <= last && z >= kb - 2 && z <= ke + 2)
         {
-            T *dst = PH + (size_t)zm_slot(z, ZM_PH) * ZM_WX * ZM_WY;
+            T *dst = PH + (size_t)zm_slot(z) * ZM_WX * ZM_WY;
             for (int e = tid; e < ZM_WX * ZM_WY; e += ZM_THREADS)
             {
                 const int wy = e / ZM_WX, wx = e - wy * ZM_WX;
@@ -116,23 +114,9 @@ __global__ void __launch_bounds__(ZM_THREADS)
                                             sizeof(T));
             }
         }
-        if (z >= 1 && z <= m && z >= kb - 1 && z <= ke + 1)
-        {
-            T *dst = RH + (size_t)zm_slot(z, ZM_RH) * ZM_RX * ZM_RY;
-            for (int e = tid; e < ZM_RX * ZM_RY; e += ZM_THREADS)
-            {
-                const int ry = e / ZM_RX, rx = e - ry * ZM_RX;
-                const int gx = x0 - 1 + rx, gy = y0 - 1 + ry;
-                if (gx >= 1 && gx <= m && gy >= 1 && gy <= m)
-                    __pipeline_memcpy_async(dst + e, rho.p + rho.off + gx + gy * rho.sy + (long)z * rho.sz,
-                                            sizeof(T));
-            }
-        }
         __pipeline_commit();
     };
-    // window index of (wx, wy) in plane z
-    auto P = [&](int z) { return PH + (size_t)zm_slot(z, ZM_PH) * ZM_WX * ZM_WY; };
-    auto R = [&](int z) { return RH + (size_t)zm_slot(z, ZM_RH) * ZM_RX * ZM_RY; };
+    auto P = [&](int z) { return PH + (size_t)zm_slot(z) * ZM_WX * ZM_WY; };
     load(kb - 2);
     for (int sp = kb - 2; sp <= ke + 2; sp++)
     {
@@ -144,7 +128,7 @@ __global__ void __launch_bounds__(ZM_THREADS)
         if (zr >= kb - 1 && zr <= ke + 1 && zr >= 1 && zr <= m)
         {
             T *pc = P(zr), *pd = P(zr - 1), *pu = P(zr + 1);
-            const T *rr = R(zr);
+            const T *rr = rho.p + rho.off + (long)zr * rho.sz;
             for (int e = tid; e < (ZM_RX / 2) * ZM_RY; e += ZM_THREADS)
             {
                 const int ry = e / (ZM_RX / 2), pr = e - ry * (ZM_RX / 2);
@@ -159,52 +143,42 @@ __global__ void __launch_bounds__(ZM_THREADS)
                 if (gx < 1 || gx > m || gy < 1 || gy > m)
                     continue;
                 const int l = (rx + 1) + (ry + 1) * ZM_WX;
-                const T a = one_sixth * (-H2 * rr[rx + ry * ZM_RX] + pc[l + 1] + pc[l - 1] +
+                const T a = one_sixth * (-H2 * rr[gx + gy * rho.sy] + pc[l + 1] + pc[l - 1] +
                                          pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
                 pc[l] = w * a + ((T)1.0 - w) * pc[l];
             }
         }
         __syncthreads();
-        // black points of plane zb = sp - 2 over the tile: pairs (2t, 2t + 1) of tile x
+        // black points of plane zb = sp - 2 over the tile: pairs (2t, 2t + 1) of tile
+        // x; the pair (its red member final since the last step) goes to pout
         const int zb = sp - 2;
-        const bool outp = zb >= kb && zb <= ke;
-        if (outp)
+        if (zb >= kb && zb <= ke)
         {
             T *pc = P(zb), *pd = P(zb - 1), *pu = P(zb + 1);
-            const T *rr = R(zb);
+            const T *rr = rho.p + rho.off + (long)zb * rho.sz;
+            T *out = pout.p + pout.off + (long)zb * pout.sz;
             for (int e = tid; e < (ZM_TX / 2) * ZM_TY; e += ZM_THREADS)
             {
                 const int ty = e / (ZM_TX / 2), pt = e - ty * (ZM_TX / 2);
                 const int gy = y0 + ty;
-                int tx = 2 * pt;
-                int gx = x0 + tx;
-                if (!((gx + gy + zb) & 1))
-                {
-                    tx++;
-                    gx++;
-                }
-                if (gx > m || gy > m)
+                const int gxa = x0 + 2 * pt;
+                if (gy > m || gxa > m)
                     continue;
-                const int l = (tx + 2) + (ty + 2) * ZM_WX;
-                const T a = one_sixth * (-H2 * rr[(tx + 1) + (ty + 1) * ZM_RX] + pc[l + 1] +
-                                         pc[l - 1] + pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
-                pc[l] = w * a + ((T)1.0 - w) * pc[l];
+                const int b = ((gxa + gy + zb) & 1) ? 0 : 1; // offset of the black member
+                const int la = (2 * pt + 2) + (ty + 2) * ZM_WX;
+                const int l = la + b;
+                if (gxa + b <= m)
+                {
+                    const T a = one_sixth * (-H2 * rr[gxa + b + gy * rho.sy] + pc[l + 1] +
+                                             pc[l - 1] + pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
+                    pc[l] = w * a + ((T)1.0 - w) * pc[l];
+                }
+                out[gxa + gy * pout.sy] = pc[la];
+                if (gxa + 1 <= m)
+                    out[gxa + 1 + gy * pout.sy] = pc[la + 1];
             }
         }
-        __syncthreads();
-        if (outp)
-        {
-            const T *pc = P(zb);
-            for (int e = tid; e < ZM_TX * ZM_TY; e += ZM_THREADS)
-            {
-                const int ty = e / ZM_TX, tx = e - ty * ZM_TX;
-                const int gx = x0 + tx, gy = y0 + ty;
-                if (gx <= m && gy <= m)
-                    pout.p[pout.off + gx + gy * pout.sy + (long)zb * pout.sz] =
-                        pc[(tx + 2) + (ty + 2) * ZM_WX];
-            }
-        }
-        __syncthreads(); // the next step's loads reuse the slot of plane sp - 4
+        __syncthreads(); // the next step's load reuses the slot of plane sp - 4
     }
 }
 
