@@ -64,14 +64,16 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
 // from memory once per CTA and written once.  A CTA owns a tile of ZM_TX x
 // ZM_TY interior points in (x, y) and a chunk of ZM_TZ planes in z, and marches
 // up the chunk with a ring of phi planes in shared memory, staged by
-// asynchronous copies (cp.async) one plane ahead of the arithmetic:
-//   step s: load plane s+1 (the tile plus 2 points a side);
+// asynchronous copies (cp.async) two planes ahead of the arithmetic:
+//   step s: load plane s+2 (the tile plus 2 points a side);
 //           red points of plane s-1 over the tile and a 1-point ring around it
 //           (from the old black values of planes s-2, s-1, s);
 //           black points of plane s-2 over the tile (from the new red values
 //           of planes s-3, s-2, s-1), and both points of each x pair of plane
 //           s-2 written to pout.
-// rho is read from memory where a point is updated (coalesced along x).  A
+// rho is read from memory where a point is updated (coalesced along x), each
+// thread's loads issued at the top of the step so that they overlap the wait
+// for the plane.  A
 // ring point is a neighbouring CTA's tile point: both compute it from the same
 // old values, so they agree bit for bit.  Algorithmic traffic: 24 B a point
 // (phi and rho read, phi written); the phi halo adds (68 x 20) / (64 x 16) - 1
@@ -79,7 +81,7 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
 constexpr int ZM_TX = 64, ZM_TY = 16, ZM_TZ = 32;
 constexpr int ZM_WX = ZM_TX + 4, ZM_WY = ZM_TY + 4; // phi window
 constexpr int ZM_RX = ZM_TX + 2, ZM_RY = ZM_TY + 2; // red ring
-constexpr int ZM_PH = 5;                            // planes held (one in flight)
+constexpr int ZM_PH = 6;                            // planes held (two in flight)
 constexpr int ZM_THREADS = 512;
 
 template <typename T> constexpr size_t zm_smem_bytes()
@@ -117,66 +119,89 @@ __global__ void __launch_bounds__(ZM_THREADS)
         __pipeline_commit();
     };
     auto P = [&](int z) { return PH + (size_t)zm_slot(z) * ZM_WX * ZM_WY; };
+    // a thread's red pairs (at most two: 33 x 18 = 594 pairs for 512 threads) and
+    // its black pair (exactly one: 32 x 16), fixed for the whole march
+    constexpr int NRP = ((ZM_RX / 2) * ZM_RY + ZM_THREADS - 1) / ZM_THREADS;
+    static_assert((ZM_TX / 2) * ZM_TY == ZM_THREADS, "one black pair a thread");
+    int rpx[NRP], rpy[NRP];
+    for (int q = 0; q < NRP; q++)
+    {
+        const int e = tid + q * ZM_THREADS;
+        rpy[q] = e / (ZM_RX / 2);
+        rpx[q] = 2 * (e - rpy[q] * (ZM_RX / 2));
+        if (e >= (ZM_RX / 2) * ZM_RY)
+            rpy[q] = -1;
+    }
+    const int bty = tid / (ZM_TX / 2), bpx = 2 * (tid - bty * (ZM_TX / 2));
     load(kb - 2);
+    load(kb - 1);
     for (int sp = kb - 2; sp <= ke + 2; sp++)
     {
-        load(sp + 1);
-        __pipeline_wait_prior(1); // plane sp has landed
+        load(sp + 2);
+        const int zr = sp - 1, zb = sp - 2;
+        const bool do_red = zr >= kb - 1 && zr <= ke + 1 && zr >= 1 && zr <= m;
+        const bool do_black = zb >= kb && zb <= ke;
+        // this step's rho values, loaded before the wait
+        T rv[NRP], bv = (T)0;
+        int rl[NRP];
+        for (int q = 0; q < NRP; q++)
+        {
+            rl[q] = -1;
+            rv[q] = (T)0;
+            if (!do_red || rpy[q] < 0)
+                continue;
+            const int gy = y0 - 1 + rpy[q];
+            int rx = rpx[q], gx = x0 - 1 + rx;
+            if ((gx + gy + zr) & 1)
+            {
+                rx++;
+                gx++;
+            }
+            if (gx < 1 || gx > m || gy < 1 || gy > m)
+                continue;
+            rl[q] = (rx + 1) + (rpy[q] + 1) * ZM_WX;
+            rv[q] = rho.p[rho.off + gx + gy * rho.sy + (long)zr * rho.sz];
+        }
+        const int bgy = y0 + bty, bgxa = x0 + bpx;
+        const bool bpair = do_black && bgy <= m && bgxa <= m;
+        const int bb = ((bgxa + bgy + zb) & 1) ? 0 : 1; // offset of the black member
+        const bool bupd = bpair && bgxa + bb <= m;
+        if (bupd)
+            bv = rho.p[rho.off + bgxa + bb + bgy * rho.sy + (long)zb * rho.sz];
+        __pipeline_wait_prior(2); // plane sp has landed
         __syncthreads();
-        // red points of plane zr = sp - 1: pairs (2p, 2p + 1) of ring x, one red each
-        const int zr = sp - 1;
-        if (zr >= kb - 1 && zr <= ke + 1 && zr >= 1 && zr <= m)
+        // red points of plane zr over the tile and its ring
+        if (do_red)
         {
             T *pc = P(zr), *pd = P(zr - 1), *pu = P(zr + 1);
-            const T *rr = rho.p + rho.off + (long)zr * rho.sz;
-            for (int e = tid; e < (ZM_RX / 2) * ZM_RY; e += ZM_THREADS)
+            for (int q = 0; q < NRP; q++)
             {
-                const int ry = e / (ZM_RX / 2), pr = e - ry * (ZM_RX / 2);
-                const int gy = y0 - 1 + ry;
-                int rx = 2 * pr;
-                int gx = x0 - 1 + rx;
-                if ((gx + gy + zr) & 1)
-                {
-                    rx++;
-                    gx++;
-                }
-                if (gx < 1 || gx > m || gy < 1 || gy > m)
+                const int l = rl[q];
+                if (l < 0)
                     continue;
-                const int l = (rx + 1) + (ry + 1) * ZM_WX;
-                const T a = one_sixth * (-H2 * rr[gx + gy * rho.sy] + pc[l + 1] + pc[l - 1] +
-                                         pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
+                const T a = one_sixth * (-H2 * rv[q] + pc[l + 1] + pc[l - 1] + pc[l + ZM_WX] +
+                                         pc[l - ZM_WX] + pu[l] + pd[l]);
                 pc[l] = w * a + ((T)1.0 - w) * pc[l];
             }
         }
         __syncthreads();
-        // black points of plane zb = sp - 2 over the tile: pairs (2t, 2t + 1) of tile
-        // x; the pair (its red member final since the last step) goes to pout
-        const int zb = sp - 2;
-        if (zb >= kb && zb <= ke)
+        // black point of this thread's pair of plane zb; the pair (its red member
+        // final since the last step) goes to pout
+        if (bpair)
         {
             T *pc = P(zb), *pd = P(zb - 1), *pu = P(zb + 1);
-            const T *rr = rho.p + rho.off + (long)zb * rho.sz;
             T *out = pout.p + pout.off + (long)zb * pout.sz;
-            for (int e = tid; e < (ZM_TX / 2) * ZM_TY; e += ZM_THREADS)
+            const int la = (bpx + 2) + (bty + 2) * ZM_WX;
+            const int l = la + bb;
+            if (bupd)
             {
-                const int ty = e / (ZM_TX / 2), pt = e - ty * (ZM_TX / 2);
-                const int gy = y0 + ty;
-                const int gxa = x0 + 2 * pt;
-                if (gy > m || gxa > m)
-                    continue;
-                const int b = ((gxa + gy + zb) & 1) ? 0 : 1; // offset of the black member
-                const int la = (2 * pt + 2) + (ty + 2) * ZM_WX;
-                const int l = la + b;
-                if (gxa + b <= m)
-                {
-                    const T a = one_sixth * (-H2 * rr[gxa + b + gy * rho.sy] + pc[l + 1] +
-                                             pc[l - 1] + pc[l + ZM_WX] + pc[l - ZM_WX] + pu[l] + pd[l]);
-                    pc[l] = w * a + ((T)1.0 - w) * pc[l];
-                }
-                out[gxa + gy * pout.sy] = pc[la];
-                if (gxa + 1 <= m)
-                    out[gxa + 1 + gy * pout.sy] = pc[la + 1];
+                const T a = one_sixth * (-H2 * bv + pc[l + 1] + pc[l - 1] + pc[l + ZM_WX] +
+                                         pc[l - ZM_WX] + pu[l] + pd[l]);
+                pc[l] = w * a + ((T)1.0 - w) * pc[l];
             }
+            out[bgxa + bgy * pout.sy] = pc[la];
+            if (bgxa + 1 <= m)
+                out[bgxa + 1 + bgy * pout.sy] = pc[la + 1];
         }
         __syncthreads(); // the next step's load reuses the slot of plane sp - 4
     }
