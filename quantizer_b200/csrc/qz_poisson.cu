@@ -78,7 +78,7 @@ __global__ void k_gs_rb(Grid<T> phi, Grid<T> rho, int color, T H2, T w)
 // old values, so they agree bit for bit.  Algorithmic traffic: 24 B a point
 // (phi and rho read, phi written); the phi halo adds (68 x 20) / (64 x 16) - 1
 // = 0.33 reads a point and the rho ring 0.16, mostly served by L2.
-constexpr int ZM_TX = 64, ZM_TY = 16, ZM_TZ = 32;
+constexpr int ZM_TX = 64, ZM_TY = 16; // z-chunks are sized by the host (zm_chunk)
 constexpr int ZM_WX = ZM_TX + 4, ZM_WY = ZM_TY + 4; // phi window
 constexpr int ZM_RX = ZM_TX + 2, ZM_RY = ZM_TY + 2; // red ring
 constexpr int ZM_PH = 6;                            // planes held (two in flight)
@@ -93,14 +93,14 @@ __device__ __forceinline__ int zm_slot(int z) { return ((z % ZM_PH) + ZM_PH) % Z
 
 template <typename T>
 __global__ void __launch_bounds__(ZM_THREADS)
-    k_gs_rb_zm(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w)
+    k_gs_rb_zm(Grid<T> pin, Grid<T> pout, Grid<T> rho, T H2, T w, int tz)
 {
     extern __shared__ __align__(16) unsigned char zm_raw[];
     T *PH = reinterpret_cast<T *>(zm_raw); // [ZM_PH][ZM_WY][ZM_WX]
     const int n = pin.n, m = n - 2, last = n - 1;
     const int tid = threadIdx.x;
     const int x0 = 1 + blockIdx.x * ZM_TX, y0 = 1 + blockIdx.y * ZM_TY;
-    const int kb = 1 + blockIdx.z * ZM_TZ, ke = min(m, kb + ZM_TZ - 1);
+    const int kb = 1 + blockIdx.z * tz, ke = min(m, kb + tz - 1);
     const T one_sixth = (T)(1.0 / 6.0);
     // asynchronous loads of the phi window of plane z (points in range)
     auto load = [&](int z) {
@@ -499,13 +499,21 @@ static int smooth_t(qz_sim *s, Grid<T> phi, Grid<T> rho, int iters, Grid<T> scra
         else if (alt.p && m >= 64 && s->fused_rb)
         {
             // fused sweeps, ping-pong phi <-> alt (alt has phi's boundary values)
-            dim3 grid((m + ZM_TX - 1) / ZM_TX, (m + ZM_TY - 1) / ZM_TY, (m + ZM_TZ - 1) / ZM_TZ);
+            // z-chunks: as many as keep the whole launch resident at once (one wave;
+            // a CTA's march is a chain of dependent plane steps)
             const size_t shm = zm_smem_bytes<T>();
+            int per_sm = 1, sms = 148;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs_rb_zm<T>, ZM_THREADS, shm);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+            const int txy = ((m + ZM_TX - 1) / ZM_TX) * ((m + ZM_TY - 1) / ZM_TY);
+            const int nch = std::max(1, std::min(m, (std::max(per_sm, 1) * sms) / txy));
+            const int tz = (m + nch - 1) / nch;
+            dim3 grid((m + ZM_TX - 1) / ZM_TX, (m + ZM_TY - 1) / ZM_TY, (m + tz - 1) / tz);
             Grid<T> a = phi, b = alt;
             for (int it = 0; it < iters; it++)
             {
                 launch_shm(s, QZ_PROF_SMOOTH, (double)sizeof(T) * 3.0 * m * m * m, shm,
-                           k_gs_rb_zm<T>, grid, dim3(ZM_THREADS), a, b, rho, H2, w);
+                           k_gs_rb_zm<T>, grid, dim3(ZM_THREADS), a, b, rho, H2, w, tz);
                 Grid<T> t = a;
                 a = b;
                 b = t;

@@ -11,7 +11,7 @@ multigrid, red-black order) on seeded random grids of n^3 points, which is
 how the smoother is profiled at sizes whose fields exceed the 126 MB L2.
 `step` runs whole leapfrog steps of a Plummer sphere on a 2^lmin head grid
 with `--levels` refinement levels above it (0: head only); `--precision 1`
-selects the mixed-precision form.  These are kernel-level cases, not the
+selects the mixed-precision form, `--node-solver 1` the node multigrid.  These are kernel-level cases, not the
 timed workload of bench.py.
 """
 from __future__ import annotations
@@ -58,7 +58,7 @@ def _step(args) -> dict:
     ic = ics.plummer(args.particles, a=args.a, seed=1)
     dt = 1e-3 * ics.crossing_time(args.a)
     with core.Simulation(ic, args.lmin, lmax=args.lmin + args.levels, ref_ptcl=args.ref_ptcl,
-                         precision=args.precision) as sim:
+                         precision=args.precision, node_solver=args.node_solver) as sim:
         sim.init_forces()
         sim.step(dt, 1)
         st0 = sim.stats()
@@ -96,6 +96,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--levels", type=int, default=0, help="refinement levels above the head")
+    ap.add_argument("--node-solver", type=int, default=0,
+                    help="refinement nodes: 0 conjugate gradient, 1 FP32 node multigrid")
     ap.add_argument("--ref-ptcl", type=int, default=9)
     args = ap.parse_args()
     fn = {"smooth": _smooth, "multigrid": _multigrid, "step": _step}[args.what]
