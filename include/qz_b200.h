@@ -100,7 +100,9 @@ typedef struct qz_config {
     double adjoint_tol;
     /* refinement-node conjugate gradient: 0 the reference's two reductions per
      * iteration, 1 one reduction per iteration (Chronopoulos-Gear arrangement:
-     * the same iterates in exact arithmetic, half the waits) */
+     * the same iterates in exact arithmetic, half the waits), 2 one reduction
+     * per iteration in the pipelined arrangement (Ghysels-Vanroose: w = A r
+     * by recurrence, one stencil and 12 loads a point) */
     int cg_variant;
     /* persistent multigrid cycles: finest-level points of one colour per thread,
      * which sets the launch's block count (at most two blocks per SM); results

@@ -1817,6 +1817,7 @@ struct Cg1Args {
     const double *d;
     double *pot, *pot_old;
     double *rb[2], *wb[2], *sb[2], *pb[2]; // r_j in rb[j & 1], ...
+    double *zv;                            // pipelined form: z = A s (rb[0], sb[0], pb[0] in place)
     double *pg[3], *pd[3];                 // per chunk: partial gamma, delta of j in [j % 3]
     int *rfail[2];
     int *status;
@@ -1910,7 +1911,41 @@ __device__ __forceinline__ double2 cg1_node_sum(const double *ga, const double *
     return t;
 }
 
+// ---- pipelined conjugate gradient (cg_variant 2) ----------------------------------------
+// Ghysels and Vanroose's arrangement (2014) of the same iterates: besides
+// w = A r and s = A p it carries z = A s, so that w_{j+1} = w_j - alpha_j z_j
+// comes from a recurrence and the one stencil of an iteration is q_j = A w_j:
+//
+//   z_j = q_j + beta_j z_{j-1};  s_j = w_j + beta_j s_{j-1};  p_j = r_j + beta_j p_{j-1}
+//   pot += alpha_j p_j;  r_{j+1} = r_j - alpha_j s_j;  w_{j+1} = w_j - alpha_j z_j
+//
+// with alpha and beta from gamma = r.r and delta = w.r as in the single-reduction
+// form.  Only w is read at neighbouring points (double-buffered by parity); r,
+// s, p and z are updated in place at the block's own points, so an iteration
+// loads w at seven points and five vectors at one (12 loads, 6 stores a point)
+// where the single-reduction form recomputes its neighbours' next residuals (23
+// loads).  One wait a iteration, as there.  The recurrence for w lets the
+// recursive residual drift from d - A pot by rounding; the convergence test
+// reads the recursive gamma as the reference's reads its recursive rsnew.
+// Points of one chunk a thread handles at once in the pipelined form (its chunks
+// hold CG2_PPT x 512 points).  Measured on the 1M-particle sphere, 128^3 head,
+// three levels (conjugate-gradient time a step): 2 points 7.09 ms, 4 points
+// 7.01 ms, 8 points 12.0 ms; the two-phase form 7.02 ms.
+constexpr int CG2_PPT = 4;
+template <bool PIPE> __device__ __forceinline__ void cg1_solve(const Cg1Args &A);
+
 __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg1_nodes(Cg1Args A)
+{
+    cg1_solve<false>(A);
+}
+
+// one block a SM: 128 registers for CG2_PPT points in flight without spills
+__global__ void __launch_bounds__(CG_MAX_THREADS, 1) k_cg2_nodes(Cg1Args A)
+{
+    cg1_solve<true>(A);
+}
+
+template <bool PIPE> __device__ __forceinline__ void cg1_solve(const Cg1Args &A)
 {
     __shared__ double2 sh2[CG_MAX_THREADS / 32];
     __shared__ int shf[CG_MAX_THREADS / 32];
@@ -2082,13 +2117,72 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg1_nodes(Cg1Args A)
             live = 1;
             const double beta = j == 0 ? 0.0 : gamma / x.g_prev;
             const double alpha = j == 0 ? gamma / delta : gamma / (delta - beta * gamma / x.a_prev);
-            const double *r = A.rb[cur], *w = A.wb[cur], *so = A.sb[prv], *po = A.pb[prv];
-            double *rn = A.rb[prv], *wn = A.wb[prv], *sn = A.sb[cur], *pn = A.pb[cur];
             const double oh2 = x.oh2;
             const int sy = x.sy, sz = x.sz;
             double ag = 0.0, ad = 0.0;
             int fail = 0;
-            for (int e = threadIdx.x; e < x.n; e += NT)
+            if constexpr (PIPE)
+            {
+                const double *w = A.wb[cur];
+                double *wn = A.wb[prv], *r = A.rb[0], *sv = A.sb[0], *pv = A.pb[0], *zv = A.zv;
+                // CG2_PPT points of a thread together: their loads are in flight at once
+                for (int e0 = threadIdx.x; e0 < x.n; e0 += CG2_PPT * NT)
+                {
+                    int g[CG2_PPT];
+                    double wc[CG2_PPT], q[CG2_PPT], rg[CG2_PPT], zo[CG2_PPT], so[CG2_PPT],
+                        po[CG2_PPT], pt[CG2_PPT];
+#pragma unroll
+                    for (int u = 0; u < CG2_PPT; u++)
+                    {
+                        const int e = e0 + u * NT;
+                        g[u] = e < x.n ? gi(s, e) : gi(s, e0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < CG2_PPT; u++)
+                    {
+                        const int gg = g[u];
+                        wc[u] = w[gg];
+                        q[u] = -oh2 * (6.0 * wc[u] - w[gg + 1] - w[gg - 1] - w[gg + sy] -
+                                       w[gg - sy] - w[gg + sz] - w[gg - sz]);
+                        rg[u] = r[gg];
+                        zo[u] = j > 0 ? zv[gg] : 0.0;
+                        so[u] = j > 0 ? sv[gg] : 0.0;
+                        po[u] = j > 0 ? pv[gg] : 0.0;
+                        pt[u] = A.pot[gg];
+                    }
+#pragma unroll
+                    for (int u = 0; u < CG2_PPT; u++)
+                    {
+                        if (e0 + u * NT >= x.n)
+                            break;
+                        const int gg = g[u];
+                        const double z = q[u] + beta * zo[u];
+                        const double sn = wc[u] + beta * so[u];
+                        const double p = rg[u] + beta * po[u];
+                        const double xv = pt[u] + alpha * p;
+                        const double rn = rg[u] - alpha * sn;
+                        const double wv = wc[u] - alpha * z;
+                        zv[gg] = z;
+                        sv[gg] = sn;
+                        pv[gg] = p;
+                        A.pot[gg] = xv;
+                        r[gg] = rn;
+                        wn[gg] = wv;
+                        ag += rn * rn;
+                        ad += wv * rn;
+                        if (check_next)
+                        {
+                            const double ratio = xv / A.pot_old[gg];
+                            if ((tm > ratio) || (tp < ratio) ||
+                                (A.method == 1 && fabs(rn) / x.rm >= A.tol))
+                                fail = 1;
+                        }
+                    }
+                }
+            }
+            const double *r = A.rb[cur], *w = A.wb[cur], *so = A.sb[prv], *po = A.pb[prv];
+            double *rn = A.rb[prv], *wn = A.wb[prv], *sn = A.sb[cur], *pn = A.pb[cur];
+            for (int e = threadIdx.x; !PIPE && e < x.n; e += NT)
             {
                 const int g = gi(s, e);
                 const Cg1Point a = cg1_point(r, w, so, po, A.pot, g, sy, sz, alpha, beta, oh2);
@@ -2296,20 +2390,25 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
     // Chunks of 1024 interior points (never across nodes), two points a thread of
-    // a 512-thread block.  Levels of up to two chunks per resident block-slot
+    // a 512-thread block (the pipelined form: 2048, four points a thread).  Levels of up to two chunks per resident block-slot
     // give every block one chunk; larger levels give blocks several.
     constexpr int kCgSmem = 40 * 1024; // slot records and cached grid indices
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    static int occ[2] = {0, 0};
+    static int occ[3] = {0, 0, 0};
     static std::once_flag occ_once;
     std::call_once(occ_once, [] {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], (const void *)k_cg_nodes,
                                                       CG_MAX_THREADS, kCgSmem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], (const void *)k_cg1_nodes,
                                                       CG_MAX_THREADS, kCgSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], (const void *)k_cg2_nodes,
+                                                      CG_MAX_THREADS, kCgSmem);
     });
-    const int per_sm = occ[(c.cg_variant == 1 && !ov && s->sched_mode != 2) ? 1 : 0];
+    // the overrides and replayed schedules are the two-phase kernel's
+    const int variant = (!ov && s->sched_mode != 2) ? c.cg_variant : 0;
+    const int per_sm = occ[variant];
+    const bool one = variant >= 1, pipe = variant == 2;
     if (per_sm < 1)
     {
         set_error("conjugate gradient kernel cannot be resident");
@@ -2317,7 +2416,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     }
     const long max_blocks = (long)per_sm * sms;
     const int nt = CG_MAX_THREADS;
-    const int chunk = 2 * nt;
+    const int chunk = (pipe ? CG2_PPT : 2) * nt;
     L.hchunks.clear();
     std::vector<int> node_chunk(2L * nn, 0);
     std::vector<int> sor_nodes; // nodes of at most branch_cg_cells cells: red-black SOR
@@ -2362,8 +2461,6 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         return QZ_SUCCESS;
     }
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
-    // the overrides and replayed schedules are the two-phase kernel's
-    const bool one = c.cg_variant == 1 && !ov && !replay;
     const long nparts = (one ? 3L : 4L) * L.nchunks * CG_PS;
     if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, nparts) ||
         !L.nint.ensure(s->mem, 6L * nn + 3) || !L.r.ensure(s->mem, L.grid_total) ||
@@ -2464,6 +2561,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     B.sb[1] = one ? L.cg1.p + L.grid_total : nullptr;
     B.pb[0] = one ? L.cg1.p + 2 * L.grid_total : nullptr;
     B.pb[1] = one ? L.cg1.p + 3 * L.grid_total : nullptr;
+    B.zv = pipe ? L.cg1.p + 3 * L.grid_total : nullptr; // the pipelined form uses no pb[1]
     for (int q = 0; q < 3; q++)
     {
         // gamma and delta of a chunk share its slot's line
@@ -2488,8 +2586,9 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         ee = prof_event(s);
         cudaEventRecord(eb, s->stream);
     }
-    if (!check_cuda(cudaLaunchCooperativeKernel(one ? (const void *)k_cg1_nodes
-                                                    : (const void *)k_cg_nodes,
+    if (!check_cuda(cudaLaunchCooperativeKernel(pipe  ? (const void *)k_cg2_nodes
+                                                : one ? (const void *)k_cg1_nodes
+                                                      : (const void *)k_cg_nodes,
                                                 dim3(blocks), dim3(nt), args, smem, s->stream),
                     "cooperative cg"))
         return QZ_FAILURE;
@@ -2507,11 +2606,12 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     {
         // bytes per iteration and interior point: the P phase reads r and p_{k-2} and
         // writes p_{k-1} (24 B), the U phase reads p, pot, r and writes pot, r (40 B);
-        // the single-reduction form reads r, w, s, p, pot and writes the five (80 B)
+        // the single-reduction form reads r, w, s, p, pot and writes the five (80 B),
+        // the pipelined form reads w, z, s, p, r, pot and writes the six (96 B)
         double pts_it = 0.0;
         for (int q = 0; q < nn; q++)
             pts_it += (double)L.h[q].nintr * st[3 + q];
-        s->prof_pending.back().bytes = (one ? 80.0 : 64.0) * pts_it;
+        s->prof_pending.back().bytes = (pipe ? 96.0 : one ? 80.0 : 64.0) * pts_it;
     }
     if (st[1])
     {

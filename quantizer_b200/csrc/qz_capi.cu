@@ -459,7 +459,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     }
     if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 2 || cfg->cycle < 0 ||
         cfg->cycle > 2 || cfg->head_pot_method < 0 || cfg->head_pot_method > 1 ||
-        cfg->cg_variant < 0 || cfg->cg_variant > 1 ||
+        cfg->cg_variant < 0 || cfg->cg_variant > 2 ||
         n_capacity > (1L << 30))
     {
         set_error("qz_create: unsupported configuration");

@@ -1,11 +1,12 @@
-"""The single-reduction conjugate gradient (cg_variant 1) against the reference.
+"""The one-reduction conjugate gradients (cg_variant 1: Chronopoulos-Gear,
+cg_variant 2: pipelined) against the reference.
 
-It produces the reference's iterates in exact arithmetic with another rounding,
+Each produces the reference's iterates in exact arithmetic with another rounding,
 so the bars are those of the refinement tests: node potentials 1e-8, node and
 particle accelerations 1e-6 of the largest, positions after 3 steps 1e-10 box
 units; the head solved by it (head_pot_method 1) against the fixture with the
-bars of the two-reduction form; the iteration counts of every level within one
-check interval (5) of the two-reduction form's.
+bars of the two-reduction form; the iteration count within one check interval
+(5) a level of the two-reduction form's.
 """
 import os
 
@@ -34,12 +35,12 @@ def test_single_reduction_cg_refinement(tmp_path, case):
                     lmax=lmax, ref_ptcl=rp)
     ref = O.read_nodes(str(tmp_path), 0)
     iters = {}
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         with core.Simulation(ic, lmin, lmax=lmax, ref_ptcl=rp, cg_variant=variant) as sim:
             sim.init_forces()
             iters[variant] = sim.stats().cg_iterations
             p0 = sim.particles()
-            if variant == 1:
+            if variant > 0:
                 for nd in ref:
                     L, i = nd["level"], nd["idx"]
                     if L == 0:
@@ -51,7 +52,7 @@ def test_single_reduction_cg_refinement(tmp_path, case):
                         assert _rel(mine, theirs) < tol, (L, i, f, _rel(mine, theirs))
             sim.step(dt, steps)
             pend = sim.particles()
-        if variant == 1:
+        if variant > 0:
             for k in ("ax", "ay", "az"):
                 assert _rel(p0[k], O.read_dump(str(tmp_path), 0, k)) < 1e-6
                 assert _rel(pend[k], O.read_dump(str(tmp_path), steps, k)) < 1e-6
@@ -59,13 +60,15 @@ def test_single_reduction_cg_refinement(tmp_path, case):
                 assert np.abs(pend[k] - O.read_dump(str(tmp_path), steps, k)).max() < 1e-10
     levels = lmax - lmin
     assert abs(iters[1] - iters[0]) <= 5 * levels, iters
+    assert abs(iters[2] - iters[0]) <= 5 * levels, iters
 
 
-def test_single_reduction_cg_head(cghead_golden):
+@pytest.mark.parametrize("variant", [1, 2])
+def test_single_reduction_cg_head(cghead_golden, variant):
     g = cghead_golden
     steps, dt = int(g["meta"][1]), float(g["meta"][2])
     ic = {k: g["ic_" + k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
-    with core.Simulation(ic, 4, head_pot_method=1, cg_variant=1) as sim:
+    with core.Simulation(ic, 4, head_pot_method=1, cg_variant=variant) as sim:
         sim.init_forces()
         pot0 = sim.field("pot")
         sim.step(dt, steps)
