@@ -74,7 +74,7 @@ WORKLOADS.update({
     # [0.02, 0.08], head 32^3 below N = 16384 else 64^3, two refinement levels, each
     # member with dt = 1e-3 of its own crossing time; stepped concurrently
     "ensemble512": dict(ic="ensemble", members=512, n=0, a=0.0, lmin=5, levels=2, ref_ptcl=9,
-                        steps=10, precision=0, cpu_steps=2, ref_steps=2, threads=16),
+                        steps=10, precision=1, cpu_steps=2, ref_steps=2, threads=16),
     # differentiation form: Plummer N = 262,144, a = 0.04, head 128^3 with the tree fixed
     # to the head node, FP64, 200 steps; loss = mean squared distance of the final
     # positions to targets from a forward run of ICs perturbed by N(0, 1e-3^2);
@@ -227,7 +227,9 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     config = {"workload": args.workload, "members": len(members), "particles": total,
               "particles_per_member": "log-uniform in [2048, 65536]", "head_grid": "32 or 64",
               "lmax_minus_lmin": wl["levels"], "refine_above_particles": wl["ref_ptcl"] - 1,
-              "dt": "1e-3 crossing time of each member", "precision": "fp64",
+              "dt": "1e-3 crossing time of each member",
+              "precision": "fp32 head multigrid cycles in fp64 defect correction, fp64 node "
+                           "conjugate gradient" if wl["precision"] else "fp64",
               "threads": wl["threads"], "replicas": world,
               "l2": "aggregate member state above L2, members interleave (no flush)"}
     if args.impl == "reference":
@@ -254,7 +256,8 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     sims, dts = [], []
     for k, (n, a, lmin) in enumerate(members):
         s = core.Simulation(ics.plummer(n, a=a, seed=1000 * rank + k), lmin,
-                            lmax=lmin + wl["levels"], ref_ptcl=wl["ref_ptcl"])
+                            lmax=lmin + wl["levels"], ref_ptcl=wl["ref_ptcl"],
+                            precision=wl["precision"])
         s.init_forces()
         sims.append(s)
         dts.append(1e-3 * ics.crossing_time(a))
@@ -275,11 +278,12 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
         return max(starts[0].elapsed_time(e) for e in ends)
 
     core.ensemble_step(sims, dts, W, threads=wl["threads"])
-    # autotuner: host threads x multigrid points per thread, one trial step each,
-    # states put back (untimed)
-    threads, ppt, tune_ms = core.ensemble_autotune(sims, dts)
+    # autotuner: host threads x multigrid points per thread x tile core of the
+    # tiled multigrid phases, one trial step each, states put back (untimed)
+    threads, ppt, tile, tune_ms = core.ensemble_autotune(sims, dts)
     config["threads"] = threads
     config["mg_points_per_thread"] = ppt
+    config["mg_tile"] = tile
     st0 = [s.stats() for s in sims]
     with ClockSampler(local) as clk:
         ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=threads))
@@ -298,13 +302,15 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config, "e2e": None,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64 (f32 head multigrid cycles)" if wl["precision"] else "f64",
+                "data": "synthetic", "config": config, "e2e": None,
                 "single_instance_loop": {"value": loop_value, "steps": Kl,
                                          "speedup_of_batching": value / world / loop_value},
-                "autotune": {"threads": threads, "mg_points_per_thread": ppt,
+                "autotune": {"threads": threads, "mg_points_per_thread": ppt, "mg_tile": tile,
                              "best_trial_ms": tune_ms,
-                             "grid": "threads {4, 8, 16, 32, 64} x points per thread {2, 4, 8}"},
+                             "grid": "threads {4, 8, 16, 32, 64} x points per thread {2, 4, 8}"
+                                     " x tile core {grid phases, 8x4x4, 8x8x8, 16x8x8}"},
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     for s in sims:

@@ -119,7 +119,20 @@ typedef struct qz_config {
      * (one thread-block cluster per node); both stop at the reference's
      * convergence test */
     int node_solver;
+    /* persistent multigrid cycles: the coarse levels above the single-block
+     * sub-cycle in tiled phases (one grid phase for a level's pre-smoothing and
+     * restriction, one for its prolongation and post-smoothing; halos
+     * recomputed, the fields bit for bit those of the grid phases) where a
+     * level's tiles take one round of the launch's blocks.  0: the first tile
+     * core of QZ_MG_TILES that fits the shared memory, k >= 1: core k - 1 (if
+     * it fits), -1: grid phases only; qz_ensemble_autotune picks it for
+     * ensembles */
+    int mg_tile;
 } qz_config;
+
+/* tile cores (x, y, z points) of the tiled multigrid phases, in mg_tile order */
+#define QZ_MG_TILES {{8, 4, 4}, {16, 4, 4}, {8, 8, 4}, {16, 8, 4}, {8, 8, 8}, {16, 8, 8}, {4, 4, 4}}
+#define QZ_MG_NTILES 7
 
 #define QZ_NODE_CG 0
 #define QZ_NODE_MG 1
@@ -257,15 +270,18 @@ QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *dt, int nste
                             int nthreads);
 
 /* Autotuner of the batching form: times one ensemble step (host wall time to
- * completion) for every pair of host thread count (thread_opts) and multigrid
- * points per thread (ppt_opts), restoring every simulation's state (particles,
- * accelerations, head potential, statistics) after each trial; sets every
- * simulation's mg_points_per_thread to the best pair's and writes the best
- * thread count, points per thread and step time.  The simulations are left as
- * they were (their results do not depend on the choice). */
+ * completion) for every combination of host thread count (thread_opts),
+ * multigrid points per thread (ppt_opts) and tile core of the tiled multigrid
+ * phases (tile_opts: mg_tile values), restoring every simulation's state
+ * (particles, accelerations, head potential, statistics) after each trial;
+ * sets every simulation's mg_points_per_thread and mg_tile to the best
+ * combination's and writes the best thread count, points per thread, tile and
+ * step time (best_tile may be NULL).  The simulations are left as they were
+ * (their results do not depend on the choice). */
 QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const double *dt,
                                 const int *thread_opts, int nthread_opts, const int *ppt_opts,
-                                int nppt_opts, int *best_threads, int *best_ppt,
+                                int nppt_opts, const int *tile_opts, int ntile_opts,
+                                int *best_threads, int *best_ppt, int *best_tile,
                                 double *best_ms);
 
 /* Differentiation form (no reference counterpart: QUANTIZER has no adjoint).

@@ -44,7 +44,7 @@ class Config(C.Structure):
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
         ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
         ("mg_points_per_thread", C.c_int), ("freeze_tree", C.c_int),
-        ("node_solver", C.c_int),
+        ("node_solver", C.c_int), ("mg_tile", C.c_int),
     ]
 
 
@@ -120,8 +120,8 @@ def load() -> C.CDLL:
         "qz_timestep": ([vp, _P], C.c_int),
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
         "qz_ensemble_step": ([C.POINTER(vp), C.c_int, _P, C.c_int, C.c_int], C.c_int),
-        "qz_ensemble_autotune": ([C.POINTER(vp), C.c_int, _P, _I, C.c_int, _I, C.c_int, _I, _I,
-                                  _P], C.c_int),
+        "qz_ensemble_autotune": ([C.POINTER(vp), C.c_int, _P, _I, C.c_int, _I, C.c_int, _I,
+                                  C.c_int, _I, _I, _I, _P], C.c_int),
         "qz_force_vjp": ([vp] + [_P] * 7, C.c_int),
         "qz_write_snapshot": ([vp, C.c_char_p, C.c_double, _P, C.c_int, C.c_int], C.c_int),
         "qz_snapshot_wait": ([vp], C.c_int),
@@ -429,20 +429,23 @@ def ensemble_step(sims: list, dt, nsteps: int = 1, threads: int = 8) -> None:
     _check(load().qz_ensemble_step(arr, len(sims), None if d is None else _p(d), nsteps, threads))
 
 
-def ensemble_autotune(sims: list, dt, thread_opts=(4, 8, 16, 32, 64), ppt_opts=(2, 4, 8)):
-    """Picks the host thread count and multigrid points per thread of the batching
-    form by timing one ensemble step per pair (qz_ensemble_autotune; the members'
-    states are put back).  Returns (threads, points_per_thread, ms)."""
+def ensemble_autotune(sims: list, dt, thread_opts=(4, 8, 16, 32, 64), ppt_opts=(2, 4, 8),
+                      tile_opts=(-1, 1, 5, 6)):
+    """Picks the host thread count, multigrid points per thread and tile core of
+    the tiled multigrid phases (mg_tile) of the batching form by timing one
+    ensemble step per combination (qz_ensemble_autotune; the members' states are
+    put back).  Returns (threads, points_per_thread, mg_tile, ms)."""
     arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
     d = None if dt is None else np.ascontiguousarray(
         np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(sims),)))
     to = (C.c_int * len(thread_opts))(*thread_opts)
     po = (C.c_int * len(ppt_opts))(*ppt_opts)
-    bt, bp, bms = C.c_int(), C.c_int(), C.c_double()
+    go = (C.c_int * len(tile_opts))(*tile_opts)
+    bt, bp, bg, bms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
     _check(load().qz_ensemble_autotune(arr, len(sims), None if d is None else _p(d), to,
-                                       len(thread_opts), po, len(ppt_opts), C.byref(bt),
-                                       C.byref(bp), C.byref(bms)))
-    return bt.value, bp.value, bms.value
+                                       len(thread_opts), po, len(ppt_opts), go, len(tile_opts),
+                                       C.byref(bt), C.byref(bp), C.byref(bg), C.byref(bms)))
+    return bt.value, bp.value, bg.value, bms.value
 
 
 def gauss_saidel(phi: np.ndarray, rho: np.ndarray, iters: int, w: float = 1.0,

@@ -343,6 +343,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->mg_points_per_thread = 4;
     c->freeze_tree = 0;
     c->node_solver = QZ_NODE_CG;
+    c->mg_tile = 0;
     return QZ_SUCCESS;
 }
 
@@ -459,7 +460,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     }
     if (cfg->force_stencil < 0 || cfg->force_stencil > 1 || cfg->smoother < 0 || cfg->smoother > 2 || cfg->cycle < 0 ||
         cfg->cycle > 2 || cfg->head_pot_method < 0 || cfg->head_pot_method > 1 ||
-        cfg->cg_variant < 0 || cfg->cg_variant > 2 ||
+        cfg->cg_variant < 0 || cfg->cg_variant > 2 || cfg->mg_tile < -1 || cfg->mg_tile > QZ_MG_NTILES ||
         n_capacity > (1L << 30))
     {
         set_error("qz_create: unsupported configuration");

@@ -84,14 +84,22 @@ extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *d
 
 extern "C" QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const double *dt,
                                            const int *thread_opts, int nthread_opts,
-                                           const int *ppt_opts, int nppt_opts, int *best_threads,
-                                           int *best_ppt, double *best_ms)
+                                           const int *ppt_opts, int nppt_opts,
+                                           const int *tile_opts, int ntile_opts, int *best_threads,
+                                           int *best_ppt, int *best_tile, double *best_ms)
 {
-    if (!sims || nsims < 1 || !thread_opts || nthread_opts < 1 || !ppt_opts || nppt_opts < 1)
+    if (!sims || nsims < 1 || !thread_opts || nthread_opts < 1 || !ppt_opts || nppt_opts < 1 ||
+        !tile_opts || ntile_opts < 1)
     {
         set_error("qz_ensemble_autotune: bad arguments");
         return QZ_FAILURE;
     }
+    for (int a = 0; a < ntile_opts; a++)
+        if (tile_opts[a] < -1 || tile_opts[a] > QZ_MG_NTILES)
+        {
+            set_error("qz_ensemble_autotune: tile option %d out of range", tile_opts[a]);
+            return QZ_FAILURE;
+        }
     std::vector<SavedState> saved(nsims);
     auto restore_all = [&]() {
         for (int k = 0; k < nsims; k++)
@@ -106,32 +114,38 @@ extern "C" QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const doubl
             !state_save(sims[k], saved[k]) || qz_synchronize(sims[k]))
             rc = QZ_FAILURE;
     }
-    int bt = thread_opts[0], bp = ppt_opts[0];
+    int bt = thread_opts[0], bp = ppt_opts[0], bl = tile_opts[0];
     double bms = 1e300;
-    for (int a = 0; a < nppt_opts && rc == QZ_SUCCESS; a++)
-    {
-        for (int k = 0; k < nsims; k++)
-            sims[k]->cfg.mg_points_per_thread = ppt_opts[a];
-        for (int b = 0; b < nthread_opts && rc == QZ_SUCCESS; b++)
+    for (int g = 0; g < ntile_opts && rc == QZ_SUCCESS; g++)
+        for (int a = 0; a < nppt_opts && rc == QZ_SUCCESS; a++)
         {
-            const auto t0 = std::chrono::steady_clock::now();
-            rc = qz_ensemble_step(sims, nsims, dt, 1, thread_opts[b]);
-            const double ms =
-                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
-                    .count();
-            if (rc == QZ_SUCCESS && ms < bms)
+            for (int k = 0; k < nsims; k++)
             {
-                bms = ms;
-                bt = thread_opts[b];
-                bp = ppt_opts[a];
+                sims[k]->cfg.mg_points_per_thread = ppt_opts[a];
+                sims[k]->cfg.mg_tile = tile_opts[g];
             }
-            if (rc == QZ_SUCCESS && !restore_all())
-                rc = QZ_FAILURE;
+            for (int b = 0; b < nthread_opts && rc == QZ_SUCCESS; b++)
+            {
+                const auto t0 = std::chrono::steady_clock::now();
+                rc = qz_ensemble_step(sims, nsims, dt, 1, thread_opts[b]);
+                const double ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                        .count();
+                if (rc == QZ_SUCCESS && ms < bms)
+                {
+                    bms = ms;
+                    bt = thread_opts[b];
+                    bp = ppt_opts[a];
+                    bl = tile_opts[g];
+                }
+                if (rc == QZ_SUCCESS && !restore_all())
+                    rc = QZ_FAILURE;
+            }
         }
-    }
     for (int k = 0; k < nsims; k++)
     {
         sims[k]->cfg.mg_points_per_thread = bp;
+        sims[k]->cfg.mg_tile = bl;
         state_free(sims[k], saved[k]);
     }
     if (rc != QZ_SUCCESS)
@@ -140,6 +154,8 @@ extern "C" QZ_API int qz_ensemble_autotune(qz_sim **sims, int nsims, const doubl
         *best_threads = bt;
     if (best_ppt)
         *best_ppt = bp;
+    if (best_tile)
+        *best_tile = bl;
     if (best_ms)
         *best_ms = bms;
     return QZ_SUCCESS;

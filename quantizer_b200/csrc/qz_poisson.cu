@@ -793,6 +793,11 @@ template <typename T> struct MgArgs {
     double tm, tp, rm, tol; // 1 -/+ tol2, 4 pi G rho_mean, tol
     int method;
     long nintr;
+    // coarse levels 1 .. nsmall-1 in tiled phases (mg_tile_down / mg_tile_up):
+    // bit l of tiled set for a tiled level, tile cores of tc[0] x tc[1] x tc[2] points
+    int tiled;
+    int tc[3];
+    Grid<T> mid[MG_MAXLEV]; // partner arrays of the tiled levels (zero boundary)
 };
 
 // Work item t = a + n0 (b + n1 c) of a grid-stride loop (t = tid, tid + stride,
@@ -1079,8 +1084,338 @@ __device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsi
             a.p[a.off + (long)x.a + (long)x.b * a.sy + (long)x.c * a.sz];
 }
 
+// ---- coarse levels in tiled phases ------------------------------------------------------
+// A coarse level's pre-smoothing and restriction (2 n_pre + 1 grid phases)
+// become one phase, and its prolongation and post-smoothing (2 n_post + 1)
+// another.  Every block takes tiles of the level's interior: it sets up a tile's
+// core with a halo deep enough for all the colour phases in shared memory,
+// runs the colour phases on regions that shrink by one point a phase, and
+// writes back the core.  A halo point is computed by every tile that holds it,
+// from the same values with the same arithmetic, so it equals the owner's; the
+// pre-smoothing halo is 2 n_pre + 1 (the residual at a restriction point needs
+// its smoothed neighbours), the post-smoothing halo 2 n_post.  A tile must not
+// read what another tile of the same phase writes, so the down phase starts
+// from zero (the restriction into a coarse level zeroes it) and writes its
+// cores to the level's partner array (mid), and the up phase reads mid and
+// writes the level's correction.  Point updates, restriction and prolongation
+// keep the arithmetic of mg_rb_point, mg_restrict_point and mg_prolong_pair,
+// so the fields equal those of the grid-phase path bit for bit.
+
+// Region [x0, x1) x [y0, y1) x [z0, z1) of a level.
+struct MgBox {
+    int x0, x1, y0, y1, z0, z1;
+};
+
+// The core [c0, c1) of each axis widened by h, clipped to [lo, hi).
+__device__ __forceinline__ MgBox mg_box(const int c0[3], const int c1[3], int h, int lo, int hi)
+{
+    MgBox b;
+    b.x0 = max(c0[0] - h, lo);
+    b.x1 = min(c1[0] + h, hi);
+    b.y0 = max(c0[1] - h, lo);
+    b.y1 = min(c1[1] + h, hi);
+    b.z0 = max(c0[2] - h, lo);
+    b.z1 = min(c1[2] + h, hi);
+    return b;
+}
+
+// A shared-memory copy of a box of a level: point (i, j, k) at
+// (i - o[0]) + (j - o[1]) sx + (k - o[2]) sxy.
+template <typename T> struct MgTile {
+    T *s;
+    int o[3];
+    int sx, sxy;
+    __device__ __forceinline__ int at(int i, int j, int k) const
+    {
+        return (i - o[0]) + (j - o[1]) * sx + (k - o[2]) * sxy;
+    }
+};
+
+// Starts asynchronous copies of box b of a level into the tile (cp.async, one
+// element each: every load of a tile is in flight at once); mg_tile_wait ends them.
 template <typename T>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant__ MgArgs<T> A)
+__device__ __forceinline__ void mg_tile_load(const Grid<T> &g, const MgBox &b, const MgTile<T> &t)
+{
+    const int nx = b.x1 - b.x0, ny = b.y1 - b.y0, nz = b.z1 - b.z0;
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return;
+    for (Walk3 w(threadIdx.x, blockDim.x, (unsigned)nx, (unsigned)ny); w.c < (unsigned)nz; w.next())
+    {
+        const int i = b.x0 + (int)w.a, j = b.y0 + (int)w.b, k = b.z0 + (int)w.c;
+        __pipeline_memcpy_async(&t.s[t.at(i, j, k)], &g.p[g.off + i + (long)j * g.sy + (long)k * g.sz],
+                                sizeof(T));
+    }
+}
+
+__device__ __forceinline__ void mg_tile_wait()
+{
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+    __syncthreads();
+}
+
+// Zero over box b of the tile.
+template <typename T> __device__ __forceinline__ void mg_tile_zero(const MgBox &b, const MgTile<T> &t)
+{
+    const int nx = b.x1 - b.x0, ny = b.y1 - b.y0, nz = b.z1 - b.z0;
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return;
+    for (Walk3 w(threadIdx.x, blockDim.x, (unsigned)nx, (unsigned)ny); w.c < (unsigned)nz; w.next())
+        t.s[t.at(b.x0 + (int)w.a, b.y0 + (int)w.b, b.z0 + (int)w.c)] = (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ void mg_tile_store(const Grid<T> &g, const MgBox &b, const MgTile<T> &t)
+{
+    const int nx = b.x1 - b.x0, ny = b.y1 - b.y0, nz = b.z1 - b.z0;
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return;
+    for (Walk3 w(threadIdx.x, blockDim.x, (unsigned)nx, (unsigned)ny); w.c < (unsigned)nz; w.next())
+    {
+        const int i = b.x0 + (int)w.a, j = b.y0 + (int)w.b, k = b.z0 + (int)w.c;
+        g.p[g.off + i + (long)j * g.sy + (long)k * g.sz] = t.s[t.at(i, j, k)];
+    }
+}
+
+// One colour of a red-black sweep over the points of box u (mg_rb_point's
+// arithmetic; colour (i + j + k) & 1 as in mg_rb_half).
+template <typename T>
+__device__ __forceinline__ void mg_tile_rb(const MgTile<T> &P, const MgTile<T> &R, const MgBox &u,
+                                           int color, T H2, T w)
+{
+    const int nx = u.x1 - u.x0, ny = u.y1 - u.y0, nz = u.z1 - u.z0;
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return;
+    const T one_sixth = (T)(1.0 / 6.0);
+    const unsigned hw = (unsigned)(nx + 1) / 2;
+    T *p = P.s;
+    for (Walk3 x(threadIdx.x, blockDim.x, hw, (unsigned)ny); x.c < (unsigned)nz; x.next())
+    {
+        const int j = u.y0 + (int)x.b, k = u.z0 + (int)x.c;
+        const int i = ((((u.x0 + j + k) & 1) == color) ? u.x0 : u.x0 + 1) + 2 * (int)x.a;
+        if (i >= u.x1)
+            continue;
+        const int q = P.at(i, j, k);
+        const T a = one_sixth * (-H2 * R.s[R.at(i, j, k)] + p[q + 1] + p[q - 1] + p[q + P.sx] +
+                                 p[q - P.sx] + p[q + P.sxy] + p[q - P.sxy]);
+        p[q] = w * a + ((T)1.0 - w) * p[q];
+    }
+}
+
+// The correction k_prolong_add (mg_prolong_pair) adds at fine point (i, j, k),
+// from coarse values at(a, b, c): the odd point of a pair adds its up to eight
+// terms in z, y, x order, the even point takes its column's value as is (j, k
+// even) or adds its up to four terms in z, y order.
+template <typename T, typename CF>
+__device__ __forceinline__ T mg_prolong_value(CF cv, int mc, int i, int j, int k)
+{
+    const bool jo = j & 1, ko = k & 1;
+    const int oy0 = jo ? (j - 1) >> 1 : j >> 1, oz0 = ko ? (k - 1) >> 1 : k >> 1;
+    bool vy[2], vz[2];
+    vy[0] = jo ? oy0 >= 1 : true;
+    vy[1] = jo && oy0 + 1 <= mc;
+    vz[0] = ko ? oz0 >= 1 : true;
+    vz[1] = ko && oz0 + 1 <= mc;
+    const T wy = jo ? (T)0.5 : (T)1, wz = ko ? (T)0.5 : (T)1;
+    if (i & 1)
+    {
+        const int a = (i - 1) >> 1;
+        const bool vx0 = a >= 1, vx1 = a + 1 <= mc;
+        const T w0 = (T)0.5 * wy * wz;
+        T acc = (T)0;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+            const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
+            if (vz[az] && vy[ay] && (ax ? vx1 : vx0))
+                acc += w0 * cv(a + ax, oy0 + ay, oz0 + az);
+        }
+        return acc;
+    }
+    const int b = i >> 1;
+    if (!jo && !ko)
+        return cv(b, oy0, oz0);
+    const T w1 = (T)1 * wy * wz;
+    T acc = (T)0;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+    {
+        const int az = q >> 1, ay = q & 1;
+        if (vz[az] && vy[ay])
+            acc += w1 * cv(b, oy0 + ay, oz0 + az);
+    }
+    return acc;
+}
+
+// Tiles of a level's interior [1, m]^3 with cores of tc points per axis.
+struct MgTiling {
+    int nt[3];
+    __device__ __forceinline__ MgTiling(int m, const int tc[3])
+    {
+        for (int d = 0; d < 3; d++)
+            nt[d] = (m + tc[d] - 1) / tc[d];
+    }
+    __device__ __forceinline__ int count() const { return nt[0] * nt[1] * nt[2]; }
+    __device__ __forceinline__ void core(int t, int m, const int tc[3], int c0[3], int c1[3]) const
+    {
+        const int tt[3] = {t % nt[0], (t / nt[0]) % nt[1], t / (nt[0] * nt[1])};
+        for (int d = 0; d < 3; d++)
+        {
+            c0[d] = 1 + tt[d] * tc[d];
+            c1[d] = min(c0[d] + tc[d], m + 1);
+        }
+    }
+};
+
+// Shared-memory elements of the two tiled phases (the host sizes the launch with it).
+__host__ __device__ inline long mg_tile_elems(const int tc[3], int n_pre, int n_post)
+{
+    auto vol = [&](int h) { return (long)(tc[0] + 2 * h) * (tc[1] + 2 * h) * (tc[2] + 2 * h); };
+    const int hd = 2 * n_pre + 1, hu = 2 * n_post;
+    const long down = vol(hd) + vol(hd - 1);
+    long coarse = 1;
+    for (int d = 0; d < 3; d++)
+        coarse *= (tc[d] + 2 * hu + 1) / 2 + 2;
+    const long up = vol(hu) + vol(hu > 0 ? hu - 1 : 0) + coarse;
+    return down > up ? down : up;
+}
+
+// Level l (zero at the start): n_pre sweeps into mid_l, the restriction into level
+// l + 1 (phi_{l+1} = 0).
+template <typename T>
+__device__ __noinline__ void mg_tile_down(const MgArgs<T> &A, int l, T *sm, unsigned gtid, unsigned gn)
+{
+    const Grid<T> &R = A.rho[l], &CP = A.phi[l + 1], &CR = A.rho[l + 1];
+    const int n = A.phi[l].n, m = n - 2, nc = CP.n, mc = nc - 2;
+    const unsigned unc = (unsigned)nc;
+    for (Walk3 x(gtid, gn, unc, unc); x.c < unc; x.next())
+        CP.p[CP.off + (long)x.a + (long)x.b * CP.sy + (long)x.c * CP.sz] = (T)0;
+    const int hd = 2 * A.n_pre + 1, hr = hd - 1;
+    MgTile<T> tp, tr;
+    tp.s = sm;
+    tp.sx = A.tc[0] + 2 * hd;
+    tp.sxy = tp.sx * (A.tc[1] + 2 * hd);
+    tr.s = sm + (long)tp.sxy * (A.tc[2] + 2 * hd);
+    tr.sx = A.tc[0] + 2 * hr;
+    tr.sxy = tr.sx * (A.tc[1] + 2 * hr);
+    const T H2 = A.h2[l], w = A.w, ooh2 = (T)(double)((n - 1) * (n - 1)), scale = A.scale;
+    const MgTiling tl(m, A.tc);
+    for (int t = blockIdx.x; t < tl.count(); t += gridDim.x)
+    {
+        int c0[3], c1[3];
+        tl.core(t, m, A.tc, c0, c1);
+        for (int d = 0; d < 3; d++)
+        {
+            tp.o[d] = c0[d] - hd;
+            tr.o[d] = c0[d] - hr;
+        }
+        mg_tile_zero(mg_box(c0, c1, hd, 0, n), tp); // the level starts at zero
+        mg_tile_load(R, mg_box(c0, c1, hr, 1, m + 1), tr);
+        mg_tile_wait();
+        for (int c = 0; c < 2 * A.n_pre; c++)
+        {
+            mg_tile_rb(tp, tr, mg_box(c0, c1, hd - 1 - c, 1, m + 1), c & 1, H2, w);
+            __syncthreads();
+        }
+        // coarse points whose injected fine point 2X lies in the core
+        MgBox cb;
+        cb.x0 = max((c0[0] + 1) >> 1, 1);
+        cb.x1 = min((c1[0] + 1) >> 1, mc + 1);
+        cb.y0 = max((c0[1] + 1) >> 1, 1);
+        cb.y1 = min((c1[1] + 1) >> 1, mc + 1);
+        cb.z0 = max((c0[2] + 1) >> 1, 1);
+        cb.z1 = min((c1[2] + 1) >> 1, mc + 1);
+        const int nx = cb.x1 - cb.x0, ny = cb.y1 - cb.y0, nz = cb.z1 - cb.z0;
+        if (nx > 0 && ny > 0 && nz > 0)
+        {
+            const T *p = tp.s;
+            for (Walk3 x(threadIdx.x, blockDim.x, (unsigned)nx, (unsigned)ny); x.c < (unsigned)nz;
+                 x.next())
+            {
+                const int lx = cb.x0 + (int)x.a, ly = cb.y0 + (int)x.b, lz = cb.z0 + (int)x.c;
+                const int q = tp.at(2 * lx, 2 * ly, 2 * lz);
+                const T rv = tr.s[tr.at(2 * lx, 2 * ly, 2 * lz)] +
+                             ooh2 * ((T)6 * p[q] - p[q + 1] - p[q - 1] - p[q + tp.sx] - p[q - tp.sx] -
+                                     p[q + tp.sxy] - p[q - tp.sxy]);
+                CR.p[CR.off + lx + (long)ly * CR.sy + (long)lz * CR.sz] = scale * rv;
+            }
+        }
+        mg_tile_store(A.mid[l], mg_box(c0, c1, 0, 1, m + 1), tp);
+        __syncthreads(); // the next tile reloads the arrays
+    }
+}
+
+// Level l: phi_l = mid_l + the prolonged correction of level l + 1, then n_post
+// sweeps.
+template <typename T> __device__ __noinline__ void mg_tile_up(const MgArgs<T> &A, int l, T *sm)
+{
+    const Grid<T> &P = A.phi[l], &R = A.rho[l], &C = A.phi[l + 1];
+    const int n = P.n, m = n - 2, nc = C.n, mc = nc - 2;
+    const int hu = 2 * A.n_post, hr = hu > 0 ? hu - 1 : 0;
+    MgTile<T> tp, tr, tc;
+    tp.s = sm;
+    tp.sx = A.tc[0] + 2 * hu;
+    tp.sxy = tp.sx * (A.tc[1] + 2 * hu);
+    tr.s = sm + (long)tp.sxy * (A.tc[2] + 2 * hu);
+    tr.sx = A.tc[0] + 2 * hr;
+    tr.sxy = tr.sx * (A.tc[1] + 2 * hr);
+    tc.s = tr.s + (long)tr.sxy * (A.tc[2] + 2 * hr);
+    tc.sx = (A.tc[0] + 2 * hu + 1) / 2 + 2;
+    tc.sxy = tc.sx * ((A.tc[1] + 2 * hu + 1) / 2 + 2);
+    const T H2 = A.h2[l], w = A.w;
+    const MgTiling tl(m, A.tc);
+    for (int t = blockIdx.x; t < tl.count(); t += gridDim.x)
+    {
+        int c0[3], c1[3];
+        tl.core(t, m, A.tc, c0, c1);
+        for (int d = 0; d < 3; d++)
+        {
+            tp.o[d] = c0[d] - hu;
+            tr.o[d] = c0[d] - hr;
+        }
+        const MgBox pb = mg_box(c0, c1, hu, 0, n), ib = mg_box(c0, c1, hu, 1, m + 1);
+        // coarse columns of the interior points of the box: [(f0 - 1) >> 1, (f1 + 1) >> 1]
+        MgBox cb;
+        cb.x0 = (ib.x0 - 1) >> 1;
+        cb.x1 = min(((ib.x1 - 1 + 1) >> 1) + 1, nc);
+        cb.y0 = (ib.y0 - 1) >> 1;
+        cb.y1 = min(((ib.y1 - 1 + 1) >> 1) + 1, nc);
+        cb.z0 = (ib.z0 - 1) >> 1;
+        cb.z1 = min(((ib.z1 - 1 + 1) >> 1) + 1, nc);
+        tc.o[0] = cb.x0;
+        tc.o[1] = cb.y0;
+        tc.o[2] = cb.z0;
+        mg_tile_load(A.mid[l], pb, tp);
+        if (hu > 0)
+            mg_tile_load(R, mg_box(c0, c1, hr, 1, m + 1), tr);
+        mg_tile_load(C, cb, tc);
+        mg_tile_wait();
+        {
+            const int nx = ib.x1 - ib.x0, ny = ib.y1 - ib.y0, nz = ib.z1 - ib.z0;
+            const T *cs = tc.s;
+            auto cv = [&](int a, int b, int c) -> T { return cs[tc.at(a, b, c)]; };
+            if (nx > 0 && ny > 0 && nz > 0)
+                for (Walk3 x(threadIdx.x, blockDim.x, (unsigned)nx, (unsigned)ny); x.c < (unsigned)nz;
+                     x.next())
+                {
+                    const int i = ib.x0 + (int)x.a, j = ib.y0 + (int)x.b, k = ib.z0 + (int)x.c;
+                    const int q = tp.at(i, j, k);
+                    tp.s[q] = tp.s[q] + mg_prolong_value<T>(cv, mc, i, j, k);
+                }
+        }
+        __syncthreads();
+        for (int c = 0; c < hu; c++)
+        {
+            mg_tile_rb(tp, tr, mg_box(c0, c1, hu - 1 - c, 1, m + 1), c & 1, H2, w);
+            __syncthreads();
+        }
+        mg_tile_store(P, mg_box(c0, c1, 0, 1, m + 1), tp);
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_constant__ MgArgs<T> A)
 {
     extern __shared__ __align__(16) unsigned char mg_dyn[];
     __shared__ int sh_ok;
@@ -1197,9 +1532,15 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
                 // the partials are rewritten only after the next iteration's barriers
             }
         }
-        // levels above the small ones: grid-wide phases
+        // levels above the small ones: grid-wide phases (coarse ones tiled)
         for (int l = 0; l < A.nsmall; l++)
         {
+            if ((A.tiled >> l) & 1)
+            {
+                mg_tile_down(A, l, reinterpret_cast<T *>(mg_dyn), gtid, gn);
+                gsync();
+                continue;
+            }
             mg_smooth(A, l, A.n_pre, gtid, gn, gsync);
             const int n = A.phi[l].n;
             mg_restrict(A.phi[l], A.rho[l], A.phi[l + 1], A.rho[l + 1], (T)(double)((n - 1) * (n - 1)),
@@ -1254,6 +1595,12 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_cycles(const __grid_constant_
         gsync();
         for (int l = A.nsmall - 1; l >= 0; l--)
         {
+            if ((A.tiled >> l) & 1)
+            {
+                mg_tile_up(A, l, reinterpret_cast<T *>(mg_dyn));
+                gsync();
+                continue;
+            }
             mg_prolong(A.phi[l], A.phi[l + 1], gtid, gn);
             gsync();
             mg_smooth(A, l, A.n_post, gtid, gn, gsync);
@@ -1380,6 +1727,38 @@ template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = fa
     const long ppt = c.mg_points_per_thread > 0 ? c.mg_points_per_thread : 4;
     const int blocks = (int)std::max(1L, std::min((long)std::min(ps, 2) * sms,
                                                   (work + ppt * MG_THREADS - 1) / (ppt * MG_THREADS)));
+    // tiled coarse levels: the first core (or the configured one) whose two
+    // phases fit the shared memory (shared with the sub-cycle's arrays); a level
+    // is tiled when its tiles take one round of the launch's blocks
+    A.tiled = 0;
+    if (c.mg_tile >= 0 && A.nsmall > 1)
+    {
+        static const int cores[QZ_MG_NTILES][3] = QZ_MG_TILES;
+        for (int k = c.mg_tile > 0 ? c.mg_tile - 1 : 0; k < (c.mg_tile > 0 ? c.mg_tile : QZ_MG_NTILES);
+             k++)
+        {
+            const size_t need = (size_t)mg_tile_elems(cores[k], c.n_pre, c.n_post) * sizeof(T);
+            if (need > MG_SMEM_MAX)
+                continue;
+            for (int d = 0; d < 3; d++)
+                A.tc[d] = cores[k][d];
+            for (int l = 1; l < A.nsmall; l++)
+            {
+                const long m = A.phi[l].n - 2;
+                long nt = 1;
+                for (int d = 0; d < 3; d++)
+                    nt *= (m + cores[k][d] - 1) / cores[k][d];
+                if (nt <= blocks)
+                {
+                    A.tiled |= 1 << l;
+                    A.mid[l] = LevelViews<T>::alt(s, l);
+                }
+            }
+            if (A.tiled)
+                smem = std::max(smem, need);
+            break;
+        }
+    }
     // algorithmic bytes of one cycle, as the launch-per-phase path counts them
     double bytes = 0.0;
     for (int l = 0; l < A.nlev; l++)

@@ -48,7 +48,8 @@ def test_ensemble_equals_members_alone(dt):
 def test_autotune_leaves_members_unchanged():
     """The autotuner's trial steps are put back: stepping after it gives the
     states of members stepped without it, for any multigrid points per thread
-    (the multigrid launch's block count does not change its arithmetic)."""
+    and tile core (neither the multigrid launch's block count nor its tiled
+    phases change its arithmetic)."""
     dts = [1e-4 * (1 + 0.1 * k) for k in range(len(MEMBERS))]
     ref = _make()
     core.ensemble_step(ref, dts, 2, threads=4)
@@ -56,8 +57,9 @@ def test_autotune_leaves_members_unchanged():
     for s in ref:
         s.close()
     ens = _make()
-    threads, ppt, ms = core.ensemble_autotune(ens, dts, thread_opts=(1, 4), ppt_opts=(1, 16))
-    assert threads in (1, 4) and ppt in (1, 16) and ms > 0
+    threads, ppt, tile, ms = core.ensemble_autotune(ens, dts, thread_opts=(1, 4),
+                                                    ppt_opts=(1, 16), tile_opts=(-1, 6))
+    assert threads in (1, 4) and ppt in (1, 16) and tile in (-1, 6) and ms > 0
     for s in ens:
         st = s.stats()
         assert st.steps == 0
