@@ -98,6 +98,7 @@ __global__ void k_rs_downsweep(const unsigned *__restrict__ kin, const int *__re
 // ---- exclusive scan (three phases, fixed tiling) -----------------------------
 constexpr int SC_THREADS = 1024;
 constexpr int SC_ITEMS = 4;
+static_assert(SC_ITEMS == 4, "k_scan_lookback moves a thread's items as one int4");
 constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
 
 __device__ __forceinline__ int block_excl_scan(int v, int *sh, int *total)
@@ -170,10 +171,13 @@ __global__ void k_scan_single(int *__restrict__ a, long m)
 // tile before it belongs to a block that is already running, so a wait always
 // ends), scans its tile, publishes the tile's sum in its status word, then adds
 // the published values of the tiles before it, walking back until one holds an
-// inclusive prefix, and publishes its own inclusive prefix.  A status word is
-// flag (2 bits: 1 = tile sum, 2 = inclusive prefix) | epoch (30 bits) | value
-// (32 bits): one word, so a reader sees a flag and its value together; words of
-// an earlier call carry an older epoch and read as not yet published.  Integer
+// inclusive prefix, and publishes its own inclusive prefix.  The walk is one
+// warp's: lane l reads the status of the l-th tile back, so a window of 32
+// predecessors costs one round trip; a window is used once every tile in it up
+// to the nearest inclusive prefix has published.  A status word is flag (2
+// bits: 1 = tile sum, 2 = inclusive prefix) | epoch (30 bits) | value (32
+// bits): one word, so a reader sees a flag and its value together; words of an
+// earlier call carry an older epoch and read as not yet published.  Integer
 // sums: the result does not depend on the order of arrival.  A wait gives up
 // after SCAN_POLL_LIMIT polls and sets E_SCAN in flags[F_ERROR].
 constexpr long SCAN_POLL_LIMIT = 1L << 22;
@@ -188,6 +192,51 @@ __device__ __forceinline__ unsigned long long scan_ld(const unsigned long long *
 __device__ __forceinline__ void scan_st(unsigned long long *p, unsigned long long v)
 {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Sum of the published values of the tiles before `tile` (warp 0 of the block).
+__device__ __forceinline__ int scan_lookback_warp(const unsigned long long *st, long tile,
+                                                  unsigned epoch, int *flags)
+{
+    const int lane = threadIdx.x & 31;
+    int prefix = 0;
+    long polls = 0;
+    for (long j = tile - 1; j >= 0;)
+    {
+        const long idx = j - lane;
+        unsigned fl = 2, val = 0; // before tile 0: an inclusive zero (never reached past it)
+        if (idx >= 0)
+        {
+            const unsigned long long w = scan_ld(&st[idx]);
+            fl = (unsigned)(w >> 62);
+            if ((unsigned)((w >> 32) & 0x3fffffffu) != epoch)
+                fl = 0;
+            val = (unsigned)w;
+        }
+        const unsigned m2 = __ballot_sync(0xffffffffu, fl == 2);
+        const unsigned m0 = __ballot_sync(0xffffffffu, fl == 0);
+        const int first2 = m2 ? __ffs(m2) - 1 : 32;
+        // lanes up to the nearest inclusive prefix must all have published
+        const unsigned need = first2 == 32 ? 0xffffffffu : ((2u << first2) - 1u);
+        if (m0 & need)
+        {
+            if (++polls > SCAN_POLL_LIMIT)
+            {
+                if (lane == 0)
+                    atomicOr(&flags[F_ERROR], E_SCAN);
+                break;
+            }
+            continue;
+        }
+        int add = (lane <= first2) ? (int)val : 0;
+        for (int o = 16; o > 0; o >>= 1)
+            add += __shfl_xor_sync(0xffffffffu, add, o);
+        prefix += add;
+        if (first2 < 32)
+            break;
+        j -= 32;
+    }
+    return prefix;
 }
 
 __global__ void __launch_bounds__(SC_THREADS)
@@ -205,51 +254,51 @@ __global__ void __launch_bounds__(SC_THREADS)
     const long i0 = tile * SC_TILE + (long)threadIdx.x * SC_ITEMS;
     int v[SC_ITEMS];
     int sum = 0;
-    for (int q = 0; q < SC_ITEMS; q++)
+    if (i0 + SC_ITEMS <= n && ((reinterpret_cast<unsigned long long>(in + i0) & 15) == 0))
     {
-        v[q] = (i0 + q < n) ? in[i0 + q] : 0;
-        sum += v[q];
+        const int4 q4 = *reinterpret_cast<const int4 *>(in + i0);
+        v[0] = q4.x;
+        v[1] = q4.y;
+        v[2] = q4.z;
+        v[3] = q4.w;
     }
+    else
+        for (int q = 0; q < SC_ITEMS; q++)
+            v[q] = (i0 + q < n) ? in[i0 + q] : 0;
+    for (int q = 0; q < SC_ITEMS; q++)
+        sum += v[q];
     int total;
     const int ex = block_excl_scan(sum, sh, &total);
-    if (threadIdx.x == 0)
+    if (threadIdx.x < 32)
     {
         const unsigned long long tag = (unsigned long long)epoch << 32;
         int prefix = 0;
         if (tile > 0)
         {
-            scan_st(&st[tile], (1ull << 62) | tag | (unsigned)total);
-            long polls = 0;
-            for (long j = tile - 1; j >= 0;)
-            {
-                const unsigned long long w = scan_ld(&st[j]);
-                const unsigned fl = (unsigned)(w >> 62);
-                if (fl == 0 || (unsigned)((w >> 32) & 0x3fffffffu) != epoch)
-                {
-                    if (++polls > SCAN_POLL_LIMIT)
-                    {
-                        atomicOr(&flags[F_ERROR], E_SCAN);
-                        break;
-                    }
-                    continue;
-                }
-                prefix += (int)(unsigned)w;
-                if (fl == 2)
-                    break;
-                j--;
-            }
+            if (threadIdx.x == 0)
+                scan_st(&st[tile], (1ull << 62) | tag | (unsigned)total);
+            prefix = scan_lookback_warp(st, tile, epoch, flags);
         }
-        scan_st(&st[tile], (2ull << 62) | tag | (unsigned)(prefix + total));
-        s_prefix = prefix;
+        if (threadIdx.x == 0)
+        {
+            scan_st(&st[tile], (2ull << 62) | tag | (unsigned)(prefix + total));
+            s_prefix = prefix;
+        }
     }
     __syncthreads();
     int run = s_prefix + ex;
+    int o[SC_ITEMS];
     for (int q = 0; q < SC_ITEMS; q++)
     {
-        if (i0 + q < n)
-            out[i0 + q] = run;
+        o[q] = run;
         run += v[q];
     }
+    if (i0 + SC_ITEMS <= n && ((reinterpret_cast<unsigned long long>(out + i0) & 15) == 0))
+        *reinterpret_cast<int4 *>(out + i0) = make_int4(o[0], o[1], o[2], o[3]);
+    else
+        for (int q = 0; q < SC_ITEMS; q++)
+            if (i0 + q < n)
+                out[i0 + q] = o[q];
 }
 
 // Status words for `tiles` tiles and a fresh epoch for the next scan.

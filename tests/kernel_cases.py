@@ -58,16 +58,17 @@ def _step(args) -> dict:
     ic = ics.plummer(args.particles, a=args.a, seed=1)
     dt = 1e-3 * ics.crossing_time(args.a)
     with core.Simulation(ic, args.lmin, lmax=args.lmin + args.levels, ref_ptcl=args.ref_ptcl,
-                         precision=args.precision, node_solver=args.node_solver) as sim:
+                         precision=args.precision, node_solver=args.node_solver,
+                         cg_variant=args.cg_variant) as sim:
         sim.init_forces()
         sim.step(dt, 1)
         st0 = sim.stats()
         t0 = time.perf_counter()
-        sim.step(dt, args.steps)  # timed: CUDA graphs on, profiler off
+        sim.step(dt, args.steps)  # timed, profiler off
         sim.synchronize()
         t = time.perf_counter() - t0
         st1 = sim.stats()
-        core.profile_reset(sim)  # separate profiled pass (per-launch events, no graphs)
+        core.profile_reset(sim)  # separate profiled pass (per-launch events)
         core.profile_enable(sim, True)
         sim.step(dt, args.steps)
         prof = core.profile_read(sim)
@@ -99,6 +100,9 @@ def main() -> None:
     ap.add_argument("--node-solver", type=int, default=0,
                     help="refinement nodes: 0 conjugate gradient, 1 FP32 node multigrid")
     ap.add_argument("--ref-ptcl", type=int, default=9)
+    ap.add_argument("--cg-variant", type=int, default=0,
+                    help="node conjugate gradient: 0 two reductions, 1 single reduction, "
+                         "2 pipelined")
     args = ap.parse_args()
     fn = {"smooth": _smooth, "multigrid": _multigrid, "step": _step}[args.what]
     print(json.dumps(fn(args)))
