@@ -256,6 +256,16 @@ QZ_API int qz_amr_node_field(qz_sim *sim, int level, int node, int which, double
 QZ_API int qz_init_forces(qz_sim *sim);
 QZ_API int qz_step(qz_sim *sim, double dt, int nsteps);
 
+/* One step (dt > 0) on host-resident state, as the reference's main loop keeps
+ * it: x..vz, m and ax..az (length qz_num_particles) are copied in, the step is
+ * qz_step's, and x..vz, ax..az are copied back before the call returns.  With
+ * page-locked arrays the copies overlap the step (masses in during the
+ * kick-drift and tree, positions out during the force computation); with
+ * pageable ones they go through the staging buffer before and after it. */
+QZ_API int qz_step_host(qz_sim *sim, double dt, double *x, double *y, double *z, double *vx,
+                        double *vy, double *vz, const double *m, double *ax, double *ay,
+                        double *az);
+
 /* timestep (timestep.c:589-700, headers/timestep.h): the CFL time step of the
  * current velocities and accelerations, each particle with the cell size of its
  * finest node; reduced on the device (exact, order-independent min / max). */

@@ -120,6 +120,7 @@ def load() -> C.CDLL:
         "qz_timestep": ([vp, _P], C.c_int),
         "qz_observables": ([vp, C.c_int, _P, _P], C.c_int),
         "qz_ensemble_step": ([C.POINTER(vp), C.c_int, _P, C.c_int, C.c_int], C.c_int),
+        "qz_step_host": ([vp, C.c_double] + [_P] * 10, C.c_int),
         "qz_ensemble_autotune": ([C.POINTER(vp), C.c_int, _P, _I, C.c_int, _I, C.c_int, _I,
                                   C.c_int, _I, _I, _I, _P], C.c_int),
         "qz_force_vjp": ([vp] + [_P] * 7, C.c_int),
@@ -210,14 +211,18 @@ class Simulation:
         _check(self.lib.qz_set_particle_accel(self.h, *[_p(v) for v in a]))
 
     def step_host(self, state: dict, dt: float) -> None:
-        """One leapfrog step on host arrays, as the drop-in serves the
-        reference's main loop: the state (x..vz, ax..az, m) is copied to the
-        device, advanced, and x..vz, ax..az are copied back into `state`."""
-        self.set_particles(state)
-        self.set_accelerations(state["ax"], state["ay"], state["az"])
-        _check(self.lib.qz_step(self.h, dt, 1))
-        _check(self.lib.qz_get_particles(self.h, *[_p(state[k]) for k in
-                                                   ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]))
+        """One leapfrog step on host arrays (qz_step_host), as the reference's
+        main loop keeps its state: x..vz, m, ax..az are copied to the device,
+        advanced, and x..vz, ax..az are copied back into `state` (contiguous
+        float64 arrays of length n; page-locked ones overlap the copies with
+        the step)."""
+        for k in ("x", "y", "z", "vx", "vy", "vz", "m", "ax", "ay", "az"):
+            a = state[k]
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size != self.n:
+                raise QZError(f"step_host: {k} must be a contiguous float64 array of length n")
+        _check(self.lib.qz_step_host(self.h, dt, *[_p(state[k]) for k in
+                                                   ("x", "y", "z", "vx", "vy", "vz", "m", "ax",
+                                                    "ay", "az")]))
 
     @property
     def n(self) -> int:

@@ -418,6 +418,15 @@ int qz_destroy(qz_sim *s)
         cudaFreeHost(s->h_ts);
     if (s->h_stage)
         cudaFreeHost(s->h_stage);
+    if (s->xfer)
+    {
+        cudaStreamSynchronize(s->xfer);
+        cudaStreamDestroy(s->xfer);
+    }
+    if (s->ev_mass)
+        cudaEventDestroy(s->ev_mass);
+    if (s->ev_drift)
+        cudaEventDestroy(s->ev_drift);
     if (s->stream)
         cudaStreamDestroy(s->stream);
     delete s;
@@ -818,6 +827,82 @@ int qz_step(qz_sim *s, double dt, int nsteps)
         if (step_core(s, h))
             return QZ_FAILURE;
     }
+    return check_flags(s);
+}
+
+// One step on host-resident state.  Page-locked arrays (every one of the ten):
+// x..vz and ax..az go in on the simulation's stream, the masses on a second
+// stream while the kick-drift and the tree run (the deposit is the first stage
+// that reads them), and the drifted positions come back on the second stream
+// while the forces are computed; velocities and accelerations come back after
+// the kick.  Pageable arrays: the staged copies of qz_set_particles /
+// qz_get_particles around qz_step.  The arithmetic is qz_step's either way.
+int qz_step_host(qz_sim *s, double dt, double *x, double *y, double *z, double *vx, double *vy,
+                 double *vz, const double *m, double *ax, double *ay, double *az)
+{
+    if (!s || !(dt > 0.0) || !x || !y || !z || !vx || !vy || !vz || !m || !ax || !ay || !az)
+    {
+        set_error("qz_step_host: bad arguments (dt must be > 0)");
+        return QZ_FAILURE;
+    }
+    const long n = s->n;
+    const void *arrays[10] = {x, y, z, vx, vy, vz, m, ax, ay, az};
+    bool pinned = true;
+    for (const void *p : arrays)
+    {
+        cudaPointerAttributes at;
+        pinned = pinned && cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+                 at.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+    }
+    // outflow boundaries remove particles in the kick-drift: the plain sequence
+    if (!pinned || s->cfg.bdry == 2 || n == 0)
+        return (qz_set_particles(s, n, x, y, z, vx, vy, vz, m) ||
+                qz_set_particle_accel(s, ax, ay, az) || qz_step(s, dt, 1) ||
+                qz_get_particles(s, x, y, z, vx, vy, vz, ax, ay, az))
+                   ? QZ_FAILURE
+                   : QZ_SUCCESS;
+    if (!s->xfer &&
+        (!check_cuda(cudaStreamCreateWithFlags(&s->xfer, cudaStreamNonBlocking), "copy stream") ||
+         !check_cuda(cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming), "event") ||
+         !check_cuda(cudaEventCreateWithFlags(&s->ev_drift, cudaEventDisableTiming), "event")))
+        return QZ_FAILURE;
+    const size_t b = (size_t)n * sizeof(double);
+    double *dst[9] = {s->x, s->y, s->z, s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    const double *src[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    for (int q = 0; q < 9; q++)
+        if (!check_cuda(cudaMemcpyAsync(dst[q], src[q], b, cudaMemcpyHostToDevice, s->stream), "h2d"))
+            return QZ_FAILURE;
+    // the masses on the second stream: nothing before the deposit reads them
+    if (!check_cuda(cudaMemcpyAsync(s->m, m, b, cudaMemcpyHostToDevice, s->xfer), "h2d mass") ||
+        !check_cuda(cudaEventRecord(s->ev_mass, s->xfer), "event"))
+        return QZ_FAILURE;
+    s->head_mass = s->cfg.total_mass;
+    s->ofl_removed = 0;
+    s->forces_ready = true;
+    if (kick_drift(s, dt) || !check_cuda(cudaEventRecord(s->ev_drift, s->stream), "event") ||
+        !check_cuda(cudaStreamWaitEvent(s->xfer, s->ev_drift, 0), "wait"))
+        return QZ_FAILURE;
+    double *hx[3] = {x, y, z};
+    const double *dx[3] = {s->x, s->y, s->z};
+    for (int q = 0; q < 3; q++)
+        if (!check_cuda(cudaMemcpyAsync(hx[q], dx[q], b, cudaMemcpyDeviceToHost, s->xfer), "d2h"))
+            return QZ_FAILURE;
+    if (qz_reset(s) || qz_tree_adaptation(s) ||
+        !check_cuda(cudaStreamWaitEvent(s->stream, s->ev_mass, 0), "wait") || qz_grid_density(s) ||
+        qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, dt))
+        return QZ_FAILURE;
+    s->stats.steps++;
+    s->stats.last_dt = dt;
+    s->stats.sim_time += dt;
+    double *ho[6] = {vx, vy, vz, ax, ay, az};
+    const double *dout[6] = {s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    for (int q = 0; q < 6; q++)
+        if (!check_cuda(cudaMemcpyAsync(ho[q], dout[q], b, cudaMemcpyDeviceToHost, s->stream), "d2h"))
+            return QZ_FAILURE;
+    if (!check_cuda(cudaStreamSynchronize(s->xfer), "copy stream sync") ||
+        !check_cuda(cudaStreamSynchronize(s->stream), "step sync"))
+        return QZ_FAILURE;
     return check_flags(s);
 }
 

@@ -359,6 +359,10 @@ struct qz_sim {
     double *h_red = nullptr; // pinned scalar readback
     double *h_stage = nullptr; // pinned staging for host copies
     size_t h_stage_bytes = 0;
+    // qz_step_host: second stream for the copies that overlap the step, and its
+    // events (masses in, drifted positions ready)
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t ev_mass = nullptr, ev_drift = nullptr;
 
     qz_stats stats{};
     bool forces_ready = false;
