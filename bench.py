@@ -692,32 +692,37 @@ def main() -> int:
                  "max_rel_force_err_mixed_vs_fp64": float(errs.max()),
                  "median_rel_force_err_mixed_vs_fp64": float(np.median(errs))}
         ref_sim.close()
-        # the same form with the refinement nodes solved by the FP32 node multigrid
-        # (flexible conjugate gradient preconditioned by V-cycles) instead of the
-        # reference's FP64 node conjugate gradient
-        mg_sim = core.Simulation(ic, wl["lmin"], precision=wl["variant"],
-                                 node_solver=core.QZ_NODE_MG, **simcfg)
-        mg_sim.init_forces()
-        for _ in range(W):
-            mg_sim.step(dt, 1)
-        barrier()
-        sm0 = mg_sim.stats()
-        ms_mg = timed_steps_on(mg_sim, lambda: mg_sim.step(dt, 1), K)
-        sm1 = mg_sim.stats()
-        t_mg = replicas.max_over_ranks(ms_mg, dev)
-        mg_sim.set_particles(state)
-        mg_sim.set_accelerations(state["ax"], state["ay"], state["az"])
-        mg_sim.step(dt, 1)
-        pm = mg_sim.particles()
-        diff = np.sqrt(sum((pm[k] - f64[k]) ** 2 for k in ("ax", "ay", "az")))
-        em = diff / np.maximum(a_p, 1e-300)
-        plain["node_multigrid"] = {
-            "value": world * wl["n"] * K / (t_mg / 1e3), "ms_per_step": t_mg / K,
-            "node_mg_iterations_per_step":
-                (sm1.node_mg_iterations - sm0.node_mg_iterations) / K,
-            "max_rel_force_err_vs_fp64": float(em.max()),
-            "median_rel_force_err_vs_fp64": float(np.median(em))}
-        mg_sim.close()
+        def extra_form(**kw) -> dict:
+            """The variant's form with other node-solve settings: K timed steps and
+            the force error against FP64 after one step from `state`."""
+            xs = core.Simulation(ic, wl["lmin"], precision=wl["variant"], **kw, **simcfg)
+            xs.init_forces()
+            for _ in range(W):
+                xs.step(dt, 1)
+            barrier()
+            s0 = xs.stats()
+            ms_x = timed_steps_on(xs, lambda: xs.step(dt, 1), K)
+            s1 = xs.stats()
+            t_x = replicas.max_over_ranks(ms_x, dev)
+            xs.set_particles(state)
+            xs.set_accelerations(state["ax"], state["ay"], state["az"])
+            xs.step(dt, 1)
+            px = xs.particles()
+            xs.close()
+            ex = np.sqrt(sum((px[k] - f64[k]) ** 2 for k in ("ax", "ay", "az"))) / \
+                np.maximum(a_p, 1e-300)
+            return {"value": world * wl["n"] * K / (t_x / 1e3), "ms_per_step": t_x / K,
+                    "node_mg_iterations_per_step":
+                        (s1.node_mg_iterations - s0.node_mg_iterations) / K,
+                    "cg_iterations_per_step": (s1.cg_iterations - s0.cg_iterations) / K,
+                    "max_rel_force_err_vs_fp64": float(ex.max()),
+                    "median_rel_force_err_vs_fp64": float(np.median(ex))}
+
+        # the refinement nodes solved by the FP32 node multigrid (flexible conjugate
+        # gradient preconditioned by V-cycles) instead of the FP64 node CG
+        plain["node_multigrid"] = extra_form(node_solver=core.QZ_NODE_MG)
+        # the node CG started from the previous step's solution (node_warm)
+        plain["warm_nodes"] = extra_form(node_warm=1)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

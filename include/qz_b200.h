@@ -128,6 +128,12 @@ typedef struct qz_config {
      * it fits), -1: grid phases only; qz_ensemble_autotune picks it for
      * ensembles */
     int mg_tile;
+    /* refinement-node solves start from the previous solve's solution where the
+     * previous tree's node of the same index held the point as an interior
+     * point (1), instead of the parent interpolation alone as the reference
+     * does (0, default): fewer iterations, the same convergence test, results
+     * that differ from the reference's by the solve tolerance */
+    int node_warm;
 } qz_config;
 
 /* tile cores (x, y, z points) of the tiled multigrid phases, in mg_tile order */

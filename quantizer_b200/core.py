@@ -44,7 +44,7 @@ class Config(C.Structure):
         ("time_step_method", C.c_int), ("head_pot_method", C.c_int),
         ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
         ("mg_points_per_thread", C.c_int), ("freeze_tree", C.c_int),
-        ("node_solver", C.c_int), ("mg_tile", C.c_int),
+        ("node_solver", C.c_int), ("mg_tile", C.c_int), ("node_warm", C.c_int),
     ]
 
 

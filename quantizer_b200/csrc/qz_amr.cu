@@ -569,6 +569,9 @@ static void free_level(const MemCtx &m, AmrLevel &L)
         b->release(m);
     L.nodes.release(m);
     L.chunks.release(m);
+    L.wpot.release(m);
+    L.wnodes.release(m);
+    L.wmask.release(m);
     L = AmrLevel();
 }
 
@@ -2650,6 +2653,43 @@ int cg_level_adjoint(qz_sim *s, int l, double *lam, double *rhs, double *scratch
     return rc;
 }
 
+// Warm start: interior point g of node q takes the previous solve's value at the
+// same level coordinates when node q of the previous tree holds that point as an
+// interior point (the parent interpolation stays elsewhere).
+__global__ void k_pot_warm(int n, const int *__restrict__ intr, const int *__restrict__ intr_node,
+                           const AmrNode *__restrict__ nodes, const AmrNode *__restrict__ wnodes,
+                           int wnn, const unsigned char *__restrict__ wmask,
+                           const double *__restrict__ wpot, double *__restrict__ pot)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    const int q = intr_node[t];
+    if (q >= wnn)
+        return;
+    const AmrNode N = nodes[q], W = wnodes[q];
+    const long g = intr[t];
+    const long sy = N.rd[0] + 1, sz = sy * (N.rd[1] + 1);
+    long l = g - N.grid_off;
+    const long k = l / sz;
+    l -= k * sz;
+    const long j = l / sy, i = l - j * sy;
+    const long pi = i + N.ts[0] - W.ts[0], pj = j + N.ts[1] - W.ts[1], pk = k + N.ts[2] - W.ts[2];
+    if (pi < 0 || pj < 0 || pk < 0 || pi > W.rd[0] || pj > W.rd[1] || pk > W.rd[2])
+        return;
+    const long wsy = W.rd[0] + 1, wsz = wsy * (W.rd[1] + 1);
+    const long pg = W.grid_off + pi + pj * wsy + pk * wsz;
+    if (wmask[pg])
+        pot[g] = wpot[pg];
+}
+
+__global__ void k_mark(int n, const int *__restrict__ idx, unsigned char *__restrict__ mask)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n)
+        mask[idx[t]] = 1;
+}
+
 int amr_potential(qz_sim *s)
 {
     const double coeff = -s->cfg.G * s->cfg.total_mass;
@@ -2679,12 +2719,37 @@ int amr_potential(qz_sim *s)
             launch(s, QZ_PROF_OTHER, 80.0 * L.intr_total, k_pot_init,
                    dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
                    L.intr_node.p, L.nodes.p, P.nodes.p, P.pot, L.pot);
+        const bool warm = s->cfg.node_warm && s->sched_mode == 0;
+        if (warm && L.wnn > 0 && L.intr_total > 0)
+            launch(s, QZ_PROF_OTHER, 40.0 * L.intr_total, k_pot_warm,
+                   dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
+                   L.intr_node.p, L.nodes.p, L.wnodes.p, L.wnn, L.wmask.p, L.wpot.p, L.pot);
         launch(s, QZ_PROF_OTHER, 16.0 * L.grid_total, k_copy_d, dim3(blocks_for(L.grid_total, 256)),
                dim3(256), L.grid_total, L.pot, L.pot_old);
         // the reference's node conjugate gradient, or FP32 multigrid cycles
         // preconditioning a flexible conjugate gradient (qz_node_mg.cu)
         if (s->cfg.node_solver == QZ_NODE_MG ? node_mg_level(s, L, l) : cg_level(s, L, l))
             return QZ_FAILURE;
+        if (warm)
+        {
+            // keep this solve for the next one
+            if (!L.wpot.ensure(s->mem, L.grid_total) || !L.wmask.ensure(s->mem, L.grid_total) ||
+                !L.wnodes.ensure(s->mem, L.nnodes))
+            {
+                set_error("warm-start buffers");
+                return QZ_FAILURE;
+            }
+            cudaMemcpyAsync(L.wpot.p, L.pot, L.grid_total * sizeof(double), cudaMemcpyDeviceToDevice,
+                            s->stream);
+            cudaMemcpyAsync(L.wnodes.p, L.nodes.p, L.nnodes * sizeof(AmrNode),
+                            cudaMemcpyDeviceToDevice, s->stream);
+            cudaMemsetAsync(L.wmask.p, 0, L.grid_total, s->stream);
+            if (L.intr_total > 0)
+                launch(s, QZ_PROF_OTHER, 5.0 * L.intr_total, k_mark,
+                       dim3(blocks_for(L.intr_total, 256)), dim3(256), L.intr_total, L.intr.p,
+                       L.wmask.p);
+            L.wnn = L.nnodes;
+        }
     }
     return QZ_SUCCESS;
 }

@@ -344,6 +344,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->freeze_tree = 0;
     c->node_solver = QZ_NODE_CG;
     c->mg_tile = 0;
+    c->node_warm = 0;
     return QZ_SUCCESS;
 }
 

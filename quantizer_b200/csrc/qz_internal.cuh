@@ -296,6 +296,12 @@ struct AmrLevel {
     int nchunks = 0;
     int h_active = 0; // host copy of the unconverged-node count at the start of a solve
     std::vector<AmrChunk> hchunks;
+    // warm start (node_warm): the level's solution, nodes and interior mask of the
+    // previous solve
+    DBuf<double> wpot;
+    DBuf<AmrNode> wnodes;
+    DBuf<unsigned char> wmask;
+    int wnn = 0;
 };
 
 } // namespace qz
