@@ -688,7 +688,7 @@ bool ensure_sort(qz_sim *s, long need)
               check_cuda(cudaMalloc(&S.k1, need * sizeof(unsigned)), "sort") &&
               check_cuda(cudaMalloc(&S.v0, need * sizeof(int)), "sort") &&
               check_cuda(cudaMalloc(&S.v1, need * sizeof(int)), "sort") &&
-              check_cuda(cudaMalloc(&S.hist, 256L * tiles * sizeof(int)), "sort");
+              check_cuda(cudaMalloc(&S.hist, 256L * std::max(tiles, 4L) * sizeof(int)), "sort");
     S.cap = ok ? need : 0;
     S.tiles_cap = ok ? tiles : 0;
     return ok;

@@ -515,7 +515,7 @@ int qz_create(const qz_config *cfg, long n_capacity, qz_sim **out)
     long tiles = radix_tiles(cap);
     ok = ok && dmalloc(&s->sort.k0, cap, "keys") && dmalloc(&s->sort.k1, cap, "keys") &&
          dmalloc(&s->sort.v0, cap, "vals") && dmalloc(&s->sort.v1, cap, "vals") &&
-         dmalloc(&s->sort.hist, 256 * tiles, "hist");
+         dmalloc(&s->sort.hist, 256 * std::max(tiles, 4L), "hist");
     ok = ok && dmalloc(&s->seg_head, cap, "seg") && dmalloc(&s->seg_id, cap, "seg") &&
          dmalloc(&s->seg_start, cap + 1, "seg") && dmalloc(&s->seg_cell, cap, "seg") &&
          dmalloc(&s->cell_seg, B * B * B, "cell_seg") && dmalloc(&s->cell_sums, 8 * cap, "cs") &&

@@ -8,8 +8,13 @@
 // Tile = 8 warps x 8 iterations x 32 lanes = 2048 keys.  Warp w of tile t
 // owns keys [t*2048 + w*256, +256); iteration r covers 32 consecutive keys in
 // lane order, so (warp, iteration, lane) order is the input order and the
-// scatter is stable.  Histograms are stored digit-major (digit * tiles + tile)
-// so that one exclusive scan yields every (digit, tile) output base.
+// scatter is stable.  One pass per 8-bit digit, each a single launch
+// (Adinets and Merrill's one-sweep arrangement, 2022): the digit counts of all
+// passes come from one histogram launch, and a pass's tile finds the keys of
+// its digits in earlier tiles by a decoupled look-back (one thread a digit)
+// instead of an upsweep and a scan of per-tile counts.
+#include <algorithm>
+
 #include "qz_internal.cuh"
 
 namespace qz {
@@ -19,83 +24,7 @@ constexpr int RS_ITEMS = 8;
 constexpr int RS_TILE = RS_WARPS * RS_ITEMS * 32; // 2048
 constexpr int RS_RADIX = 256;
 
-__global__ void k_rs_upsweep(const unsigned *__restrict__ keys, long n, int shift, int tiles,
-                             int *__restrict__ hist)
-{
-    __shared__ int cnt[RS_RADIX];
-    for (int i = threadIdx.x; i < RS_RADIX; i += blockDim.x)
-        cnt[i] = 0;
-    __syncthreads();
-    long base = (long)blockIdx.x * RS_TILE;
-    for (int it = threadIdx.x; it < RS_TILE; it += blockDim.x)
-    {
-        long i = base + it;
-        if (i < n)
-            atomicAdd(&cnt[(keys[i] >> shift) & 0xFF], 1);
-    }
-    __syncthreads();
-    for (int dgt = threadIdx.x; dgt < RS_RADIX; dgt += blockDim.x)
-        hist[(long)dgt * tiles + blockIdx.x] = cnt[dgt];
-}
-
-__global__ void k_rs_downsweep(const unsigned *__restrict__ kin, const int *__restrict__ vin,
-                               unsigned *__restrict__ kout, int *__restrict__ vout, long n,
-                               int shift, int tiles, const int *__restrict__ hist)
-{
-    __shared__ int woff[RS_WARPS][RS_RADIX];
-    __shared__ int bbase[RS_RADIX];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = threadIdx.x; i < RS_WARPS * RS_RADIX; i += blockDim.x)
-        (&woff[0][0])[i] = 0;
-    for (int dgt = threadIdx.x; dgt < RS_RADIX; dgt += blockDim.x)
-        bbase[dgt] = hist[(long)dgt * tiles + blockIdx.x];
-    __syncthreads();
-    const long wbase = (long)blockIdx.x * RS_TILE + (long)warp * RS_ITEMS * 32;
-    // per-warp digit counts
-    for (int r = 0; r < RS_ITEMS; r++)
-    {
-        long i = wbase + r * 32 + lane;
-        if (i < n)
-            atomicAdd(&woff[warp][(kin[i] >> shift) & 0xFF], 1);
-    }
-    __syncthreads();
-    // exclusive prefix over warps, per digit
-    for (int dgt = threadIdx.x; dgt < RS_RADIX; dgt += blockDim.x)
-    {
-        int run = 0;
-        for (int w = 0; w < RS_WARPS; w++)
-        {
-            int c = woff[w][dgt];
-            woff[w][dgt] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-    const unsigned lt = (1u << lane) - 1u;
-    for (int r = 0; r < RS_ITEMS; r++)
-    {
-        long i = wbase + r * 32 + lane;
-        bool valid = i < n;
-        unsigned active = __ballot_sync(0xffffffffu, valid);
-        if (valid)
-        {
-            unsigned k = kin[i];
-            int v = vin[i];
-            int dgt = (k >> shift) & 0xFF;
-            unsigned peers = __match_any_sync(active, dgt);
-            int rank = __popc(peers & lt);
-            int pos = bbase[dgt] + woff[warp][dgt] + rank;
-            kout[pos] = k;
-            vout[pos] = v;
-            __syncwarp(active);
-            if (rank == 0)
-                woff[warp][dgt] += __popc(peers);
-        }
-        __syncwarp();
-    }
-}
-
-// ---- exclusive scan (three phases, fixed tiling) -----------------------------
+// ---- exclusive scan -------------------------------------------------------------------
 constexpr int SC_THREADS = 1024;
 constexpr int SC_ITEMS = 4;
 static_assert(SC_ITEMS == 4, "k_scan_lookback moves a thread's items as one int4");
@@ -135,35 +64,6 @@ __device__ __forceinline__ int block_excl_scan(int v, int *sh, int *total)
     if (total)
         *total = t;
     return wprefix + x - v;
-}
-
-// Single block: exclusive scan of m values in place (m may exceed the block).
-__global__ void k_scan_single(int *__restrict__ a, long m)
-{
-    __shared__ int sh[32];
-    int carry = 0;
-    for (long base = 0; base < m; base += (long)SC_THREADS * SC_ITEMS)
-    {
-        long i0 = base + (long)threadIdx.x * SC_ITEMS;
-        int v[SC_ITEMS];
-        int s = 0;
-        for (int q = 0; q < SC_ITEMS; q++)
-        {
-            v[q] = (i0 + q < m) ? a[i0 + q] : 0;
-            s += v[q];
-        }
-        int total;
-        int ex = block_excl_scan(s, sh, &total);
-        int run = carry + ex;
-        for (int q = 0; q < SC_ITEMS; q++)
-        {
-            if (i0 + q < m)
-                a[i0 + q] = run;
-            run += v[q];
-        }
-        carry += total;
-        __syncthreads();
-    }
 }
 
 // Single-pass exclusive scan (decoupled look-back, Merrill and Garland 2016).
@@ -301,6 +201,130 @@ __global__ void __launch_bounds__(SC_THREADS)
                 out[i0 + q] = o[q];
 }
 
+// ---- radix sort ----------------------------------------------------------------------
+// Digit counts of every pass (passes x 256, zeroed by the caller): block-local
+// counts in shared memory, then one integer add per digit and block.
+__global__ void k_rs_hist(const unsigned *__restrict__ keys, long n, int passes,
+                          int *__restrict__ ghist)
+{
+    __shared__ int cnt[4][RS_RADIX];
+    for (int i = threadIdx.x; i < 4 * RS_RADIX; i += blockDim.x)
+        (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+    {
+        const unsigned k = keys[i];
+        for (int p = 0; p < passes; p++)
+            atomicAdd(&cnt[p][(k >> (8 * p)) & 0xFF], 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * RS_RADIX; i += blockDim.x)
+    {
+        const int c = (&cnt[0][0])[i];
+        if (c)
+            atomicAdd(&ghist[i], c);
+    }
+}
+
+// One pass on the digit at `shift`.  A block takes the next tile number from
+// the counter (arrival order, as the scan), counts its keys per warp and digit,
+// publishes its per-digit counts in the status words of its tile (flag | epoch
+// | value, as the scan's), and thread d adds the counts of digit d in the tiles
+// before it, walking back to the first inclusive prefix; the digit's output
+// base is the exclusive scan of the pass's global counts plus that prefix.  The
+// scatter is the stable warp-ordered one.
+__global__ void __launch_bounds__(RS_WARPS * 32)
+    k_rs_onesweep(const unsigned *__restrict__ kin, const int *__restrict__ vin,
+                  unsigned *__restrict__ kout, int *__restrict__ vout, long n, int shift,
+                  const int *__restrict__ ghist, unsigned long long *__restrict__ st,
+                  unsigned long long *__restrict__ ctr, unsigned long long base, unsigned epoch,
+                  int *__restrict__ flags)
+{
+    static_assert(RS_WARPS * 32 == RS_RADIX, "one thread a digit");
+    __shared__ int woff[RS_WARPS][RS_RADIX];
+    __shared__ int bbase[RS_RADIX];
+    __shared__ int sh[32];
+    __shared__ long s_tile;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0)
+        s_tile = (long)(atomicAdd(ctr, 1ull) - base);
+    for (int i = tid; i < RS_WARPS * RS_RADIX; i += blockDim.x)
+        (&woff[0][0])[i] = 0;
+    // exclusive scan of the pass's global digit counts
+    int total;
+    const int gex = block_excl_scan(ghist[tid], sh, &total);
+    __syncthreads();
+    const long tile = s_tile;
+    const long wbase = tile * RS_TILE + (long)warp * RS_ITEMS * 32;
+    for (int r = 0; r < RS_ITEMS; r++)
+    {
+        const long i = wbase + r * 32 + lane;
+        if (i < n)
+            atomicAdd(&woff[warp][(kin[i] >> shift) & 0xFF], 1);
+    }
+    __syncthreads();
+    // thread d: exclusive prefix over warps of digit d, the tile's count of d
+    const int d = tid;
+    int cnt = 0;
+    for (int w = 0; w < RS_WARPS; w++)
+    {
+        const int c = woff[w][d];
+        woff[w][d] = cnt;
+        cnt += c;
+    }
+    const unsigned long long tag = (unsigned long long)epoch << 32;
+    int prefix = 0;
+    if (tile > 0)
+    {
+        scan_st(&st[tile * RS_RADIX + d], (1ull << 62) | tag | (unsigned)cnt);
+        long polls = 0;
+        for (long j = tile - 1; j >= 0;)
+        {
+            const unsigned long long w = scan_ld(&st[j * RS_RADIX + d]);
+            const unsigned fl = (unsigned)(w >> 62);
+            if (fl == 0 || (unsigned)((w >> 32) & 0x3fffffffu) != epoch)
+            {
+                if (++polls > SCAN_POLL_LIMIT)
+                {
+                    atomicOr(&flags[F_ERROR], E_SCAN);
+                    break;
+                }
+                continue;
+            }
+            prefix += (int)(unsigned)w;
+            if (fl == 2)
+                break;
+            j--;
+        }
+    }
+    scan_st(&st[tile * RS_RADIX + d], (2ull << 62) | tag | (unsigned)(prefix + cnt));
+    bbase[d] = gex + prefix;
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < RS_ITEMS; r++)
+    {
+        const long i = wbase + r * 32 + lane;
+        const bool valid = i < n;
+        const unsigned active = __ballot_sync(0xffffffffu, valid);
+        if (valid)
+        {
+            const unsigned k = kin[i];
+            const int v = vin[i];
+            const int dg = (k >> shift) & 0xFF;
+            const unsigned peers = __match_any_sync(active, dg);
+            const int rank = __popc(peers & lt);
+            const int pos = bbase[dg] + woff[warp][dg] + rank;
+            kout[pos] = k;
+            vout[pos] = v;
+            __syncwarp(active);
+            if (rank == 0)
+                woff[warp][dg] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
 // Status words for `tiles` tiles and a fresh epoch for the next scan.
 static int scan_prepare(qz_sim *s, long tiles)
 {
@@ -356,17 +380,27 @@ int radix_sort_pairs(qz_sim *s, long n, int bits, unsigned **keys_out, int **val
         *vals_out = vi;
         return QZ_SUCCESS;
     }
-    int tiles = (int)((n + RS_TILE - 1) / RS_TILE);
-    for (int shift = 0; shift < bits; shift += 8)
+    const long tiles = (n + RS_TILE - 1) / RS_TILE;
+    const int passes = (bits + 7) / 8;
+    if (passes > 4)
     {
-        launch(s, QZ_PROF_SORT, 4.0 * n, k_rs_upsweep, dim3(tiles), dim3(RS_WARPS * 32), ki, n, shift, tiles, S.hist);
-        // digit-major counts of all tiles: exclusive scan in place (one block when small)
-        const long hm = (long)RS_RADIX * tiles;
-        if (hm <= 4L * SC_TILE)
-            launch(s, QZ_PROF_SORT, 8.0 * hm, k_scan_single, dim3(1), dim3(SC_THREADS), S.hist, hm);
-        else if (scan_exclusive(s, S.hist, S.hist, hm))
+        set_error("radix sort: %d key bits (at most 32)", bits);
+        return QZ_FAILURE;
+    }
+    // global digit counts of every pass (S.hist holds at least 4 x 256 ints)
+    cudaMemsetAsync(S.hist, 0, (size_t)passes * RS_RADIX * sizeof(int), s->stream);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    const int hb = (int)std::min<long>(2L * sms, (n + 1023) / 1024);
+    launch(s, QZ_PROF_SORT, 4.0 * n, k_rs_hist, dim3(hb), dim3(256), ki, n, passes, S.hist);
+    for (int p = 0; p < passes; p++)
+    {
+        if (scan_prepare(s, tiles * RS_RADIX))
             return QZ_FAILURE;
-        launch(s, QZ_PROF_SORT, 16.0 * n, k_rs_downsweep, dim3(tiles), dim3(RS_WARPS * 32), ki, vi, ko, vo, n, shift, tiles, S.hist);
+        launch(s, QZ_PROF_SORT, 16.0 * n, k_rs_onesweep, dim3((int)tiles), dim3(RS_WARPS * 32), ki,
+               vi, ko, vo, n, 8 * p, S.hist + p * RS_RADIX, s->scan_st, s->scan_st + s->scan_st_cap,
+               s->scan_base, s->scan_epoch, s->flags);
+        s->scan_base += (unsigned long long)tiles;
         unsigned *tk = ki;
         ki = ko;
         ko = tk;
