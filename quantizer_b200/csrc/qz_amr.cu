@@ -1369,6 +1369,7 @@ struct CgArgs {
 };
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
+constexpr int CG_FILL = 148;         // chunks a level's CG points are cut into (B200's SMs)
 // Partial-sum slots are 128 bytes apart (one L2 line each): every block of a
 // node polls every slot of the node, so slots sharing lines would serialise the
 // polls and the publications of many chunks on a few lines.
@@ -2392,9 +2393,10 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
-    // Chunks of 1024 interior points (never across nodes), two points a thread of
-    // a 512-thread block (the pipelined form: 2048, four points a thread).  Levels of up to two chunks per resident block-slot
-    // give every block one chunk; larger levels give blocks several.
+    // Chunks of at most 1024 interior points (never across nodes), up to two
+    // points a thread of a 512-thread block (the pipelined form: 2048, four
+    // points a thread).  Levels of up to two chunks per resident block-slot give
+    // every block one chunk; larger levels give blocks several.
     constexpr int kCgSmem = 40 * 1024; // slot records and cached grid indices
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
@@ -2419,7 +2421,26 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     }
     const long max_blocks = (long)per_sm * sms;
     const int nt = CG_MAX_THREADS;
-    const int chunk = (pipe ? CG2_PPT : 2) * nt;
+    // The level's CG points are cut into about CG_FILL chunks (one block a SM),
+    // or 2 CG_FILL when a chunk would exceed the two points a thread the update
+    // phase holds: the slowest SM sets every phase's length, so chunks fill the
+    // SMs evenly.  Measured on the 1M-particle sphere (CG time a step): fixed
+    // 1024-point chunks 6.98 ms, CG_FILL 148 6.86 ms, 74 6.89, 222 7.88, 296
+    // 7.60.  CG_FILL is fixed, not the device's SM count, so the partial sums
+    // and the results do not depend on the device.
+    int chunk = (pipe ? CG2_PPT : 2) * nt;
+    if (!pipe)
+    {
+        long tot = 0;
+        for (int q = 0; q < nn; q++)
+            if (!(ov && ov->skip[q]) && (!allow_sor || L.h[q].ncells > c.branch_cg_cells))
+                tot += L.h[q].nintr;
+        long cs = (tot + CG_FILL - 1) / CG_FILL;
+        if (cs > 2L * nt)
+            cs = (tot + 2L * CG_FILL - 1) / (2L * CG_FILL);
+        cs = (cs + 31) / 32 * 32;
+        chunk = (int)std::max(64L, std::min(cs, 2L * nt));
+    }
     L.hchunks.clear();
     std::vector<int> node_chunk(2L * nn, 0);
     std::vector<int> sor_nodes; // nodes of at most branch_cg_cells cells: red-black SOR
