@@ -996,40 +996,84 @@ __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ p
     const int nseg = flags[F_NSEG];
     const double H = 1.0 / (1 << lv);
     const double ooh = (double)(1 << lv);
-    for (long sg = warp0; sg < nseg; sg += nwarps)
+    // A warp takes four consecutive cells.  When each holds at most 8 particles,
+    // lanes 8g..8g+7 sum cell g (one particle a lane): the xor tree over those 8
+    // lanes is the tree the whole warp would apply to them (the other lanes hold
+    // zeros), so the sums are bit for bit those of one warp a cell.
+    for (long s4 = warp0 * 4; s4 < nseg; s4 += nwarps * 4)
     {
-        const int b = seg_start[sg], e = seg_start[sg + 1];
-        if (e - b > SEG_LONG)
+        const int g = lane >> 3, gl = lane & 7;
+        const long sgg = s4 + g;
+        int bg = 0, eg = 0;
+        if (sgg < nseg)
         {
-            if (lane == 0)
-                long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+            bg = seg_start[sgg];
+            eg = seg_start[sgg + 1];
+        }
+        if (__all_sync(0xffffffffu, eg - bg <= 8))
+        {
+            double acc[9];
+#pragma unroll
+            for (int c = 0; c < 9; c++)
+                acc[c] = 0.0;
+            if (gl < eg - bg)
+                lvl_cic_add(perm[bg + gl], H, ooh, coeff, x, y, z, m, acc);
+#pragma unroll
+            for (int c = 0; c < 9; c++)
+            {
+                double v = acc[c];
+                for (int o = 4; o > 0; o >>= 1)
+                    v += __shfl_xor_sync(0xffffffffu, v, o);
+                acc[c] = v;
+            }
+            if (sgg < nseg)
+            {
+                double v = acc[0];
+#pragma unroll
+                for (int c = 1; c < 8; c++)
+                    if (gl == c)
+                        v = acc[c];
+                cs[sgg * 8 + gl] = v;
+                if (gl == 0)
+                    smass[sgg] = acc[8];
+            }
             continue;
         }
-        double acc[9];
-#pragma unroll
-        for (int c = 0; c < 9; c++)
-            acc[c] = 0.0;
-        for (int q = b + lane; q < e; q += 32)
-            lvl_cic_add(perm[q], H, ooh, coeff, x, y, z, m, acc);
-#pragma unroll
-        for (int c = 0; c < 9; c++)
+        for (long sg = s4; sg < s4 + 4 && sg < nseg; sg++)
         {
-            double v = acc[c];
-            for (int o = 16; o > 0; o >>= 1)
-                v += __shfl_xor_sync(0xffffffffu, v, o);
-            acc[c] = v;
-        }
-        if (lane < 8)
-        {
-            double v = acc[0];
+            const int b = seg_start[sg], e = seg_start[sg + 1];
+            if (e - b > SEG_LONG)
+            {
+                if (lane == 0)
+                    long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+                continue;
+            }
+            double acc[9];
 #pragma unroll
-            for (int c = 1; c < 8; c++)
-                if (lane == c)
-                    v = acc[c];
-            cs[sg * 8 + lane] = v;
+            for (int c = 0; c < 9; c++)
+                acc[c] = 0.0;
+            for (int q = b + lane; q < e; q += 32)
+                lvl_cic_add(perm[q], H, ooh, coeff, x, y, z, m, acc);
+#pragma unroll
+            for (int c = 0; c < 9; c++)
+            {
+                double v = acc[c];
+                for (int o = 16; o > 0; o >>= 1)
+                    v += __shfl_xor_sync(0xffffffffu, v, o);
+                acc[c] = v;
+            }
+            if (lane < 8)
+            {
+                double v = acc[0];
+#pragma unroll
+                for (int c = 1; c < 8; c++)
+                    if (lane == c)
+                        v = acc[c];
+                cs[sg * 8 + lane] = v;
+            }
+            if (lane == 0)
+                smass[sg] = acc[8];
         }
-        if (lane == 0)
-            smass[sg] = acc[8];
     }
 }
 
