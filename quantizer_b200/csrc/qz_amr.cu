@@ -999,7 +999,8 @@ __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ p
     // A warp takes four consecutive cells.  When each holds at most 8 particles,
     // lanes 8g..8g+7 sum cell g (one particle a lane): the xor tree over those 8
     // lanes is the tree the whole warp would apply to them (the other lanes hold
-    // zeros), so the sums are bit for bit those of one warp a cell.
+    // zeros, which add exactly), so the sums are bit for bit those of one warp a
+    // cell.
     for (long s4 = warp0 * 4; s4 < nseg; s4 += nwarps * 4)
     {
         const int g = lane >> 3, gl = lane & 7;
@@ -1039,40 +1040,83 @@ __global__ void k_lvl_seg_reduce(int lv, double coeff, const int *__restrict__ p
             }
             continue;
         }
-        for (long sg = s4; sg < s4 + 4 && sg < nseg; sg++)
+        // else pairs of cells of at most 16 particles, 16 lanes a cell (again the
+        // warp's tree), and one warp a cell for the others
+        for (int h = 0; h < 2; h++)
         {
-            const int b = seg_start[sg], e = seg_start[sg + 1];
-            if (e - b > SEG_LONG)
+            const long p0 = s4 + 2 * h;
+            const int gh = lane >> 4, hl = lane & 15;
+            const long sgp = p0 + gh;
+            int bp = 0, ep = 0;
+            if (sgp < nseg)
             {
-                if (lane == 0)
-                    long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+                bp = seg_start[sgp];
+                ep = seg_start[sgp + 1];
+            }
+            if (__all_sync(0xffffffffu, ep - bp <= 16))
+            {
+                double acc[9];
+#pragma unroll
+                for (int c = 0; c < 9; c++)
+                    acc[c] = 0.0;
+                if (hl < ep - bp)
+                    lvl_cic_add(perm[bp + hl], H, ooh, coeff, x, y, z, m, acc);
+#pragma unroll
+                for (int c = 0; c < 9; c++)
+                {
+                    double v = acc[c];
+                    for (int o = 8; o > 0; o >>= 1)
+                        v += __shfl_xor_sync(0xffffffffu, v, o);
+                    acc[c] = v;
+                }
+                if (sgp < nseg && hl < 8)
+                {
+                    double v = acc[0];
+#pragma unroll
+                    for (int c = 1; c < 8; c++)
+                        if (hl == c)
+                            v = acc[c];
+                    cs[sgp * 8 + hl] = v;
+                    if (hl == 0)
+                        smass[sgp] = acc[8];
+                }
                 continue;
             }
-            double acc[9];
-#pragma unroll
-            for (int c = 0; c < 9; c++)
-                acc[c] = 0.0;
-            for (int q = b + lane; q < e; q += 32)
-                lvl_cic_add(perm[q], H, ooh, coeff, x, y, z, m, acc);
-#pragma unroll
-            for (int c = 0; c < 9; c++)
+            for (long sg = p0; sg < p0 + 2 && sg < nseg; sg++)
             {
-                double v = acc[c];
-                for (int o = 16; o > 0; o >>= 1)
-                    v += __shfl_xor_sync(0xffffffffu, v, o);
-                acc[c] = v;
-            }
-            if (lane < 8)
-            {
-                double v = acc[0];
+                const int b = seg_start[sg], e = seg_start[sg + 1];
+                if (e - b > SEG_LONG)
+                {
+                    if (lane == 0)
+                        long_list[atomicAdd(&flags[F_NLONG], 1)] = (int)sg;
+                    continue;
+                }
+                double acc[9];
 #pragma unroll
-                for (int c = 1; c < 8; c++)
-                    if (lane == c)
-                        v = acc[c];
-                cs[sg * 8 + lane] = v;
+                for (int c = 0; c < 9; c++)
+                    acc[c] = 0.0;
+                for (int q = b + lane; q < e; q += 32)
+                    lvl_cic_add(perm[q], H, ooh, coeff, x, y, z, m, acc);
+#pragma unroll
+                for (int c = 0; c < 9; c++)
+                {
+                    double v = acc[c];
+                    for (int o = 16; o > 0; o >>= 1)
+                        v += __shfl_xor_sync(0xffffffffu, v, o);
+                    acc[c] = v;
+                }
+                if (lane < 8)
+                {
+                    double v = acc[0];
+#pragma unroll
+                    for (int c = 1; c < 8; c++)
+                        if (lane == c)
+                            v = acc[c];
+                    cs[sg * 8 + lane] = v;
+                }
+                if (lane == 0)
+                    smass[sg] = acc[8];
             }
-            if (lane == 0)
-                smass[sg] = acc[8];
         }
     }
 }
