@@ -1458,6 +1458,11 @@ struct CgArgs {
 
 constexpr long long CG_EMPTY = -1LL; // all-ones word: partial not yet published
 constexpr int CG_FILL = 148;         // chunks a level's CG points are cut into (B200's SMs)
+// Interior points a thread in a chunk's update phase (chunks of up to CG_UPT x
+// 512 points), with one block a SM and the registers of one (128 a thread).
+// Measured on the 1M-particle sphere in one run (CG time a step): 2 points a
+// thread and two blocks a SM 6.64 ms, 4 points and one block 6.33 ms.
+constexpr int CG_UPT = 4;
 // Partial-sum slots are 128 bytes apart (one L2 line each): every block of a
 // node polls every slot of the node, so slots sharing lines would serialise the
 // polls and the publications of many chunks on a few lines.
@@ -1584,7 +1589,7 @@ __device__ __forceinline__ double cg_node_sum(const double *part, int cb, int ce
     return t.x;
 }
 
-__global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
+__global__ void __launch_bounds__(CG_MAX_THREADS, 1) k_cg_nodes(CgArgs A)
 {
     __shared__ double sh[32];
     __shared__ double2 sh2[CG_MAX_THREADS / 32];
@@ -1789,28 +1794,27 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             CgSlot &x = slot[s];
             if (x.done)
                 continue;
-            const int e0 = threadIdx.x, e1 = threadIdx.x + NT;
-            const bool h0 = e0 < x.n, h1 = e1 < x.n;
-            const int ga = h0 ? gi(s, e0) : 0, gb = h1 ? gi(s, e1) : 0;
-            double apa = 0.0, apb = 0.0, pva = 0.0, pvb = 0.0, pota = 0.0, potb = 0.0,
-                   rva = 0.0, rvb = 0.0, olda = 1.0, oldb = 1.0;
-            if (h0)
+            // up to CG_UPT points a thread (chunks of up to CG_UPT x 512 points)
+            int g[CG_UPT];
+            bool h[CG_UPT];
+            double apv[CG_UPT], pvv[CG_UPT], potv[CG_UPT], rvv[CG_UPT], oldv[CG_UPT];
+#pragma unroll
+            for (int u = 0; u < CG_UPT; u++)
             {
-                apa = A.apv[ga];
-                pva = pn[ga];
-                pota = A.pot[ga];
-                rva = A.r[ga];
-                if (check)
-                    olda = A.pot_old[ga];
-            }
-            if (h1)
-            {
-                apb = A.apv[gb];
-                pvb = pn[gb];
-                potb = A.pot[gb];
-                rvb = A.r[gb];
-                if (check)
-                    oldb = A.pot_old[gb];
+                const int e = threadIdx.x + u * NT;
+                h[u] = e < x.n;
+                g[u] = h[u] ? gi(s, e) : 0;
+                apv[u] = pvv[u] = potv[u] = rvv[u] = 0.0;
+                oldv[u] = 1.0;
+                if (h[u])
+                {
+                    apv[u] = A.apv[g[u]];
+                    pvv[u] = pn[g[u]];
+                    potv[u] = A.pot[g[u]];
+                    rvv[u] = A.r[g[u]];
+                    if (check)
+                        oldv[u] = A.pot_old[g[u]];
+                }
             }
             if (x.q != cq)
             {
@@ -1825,34 +1829,22 @@ __global__ void __launch_bounds__(CG_MAX_THREADS, 2) k_cg_nodes(CgArgs A)
             const double alpha = x.rs_cur / pap;
             double acc = 0.0;
             int fail = 0;
-            if (h0)
-            {
-                const double pv = pota + alpha * pva;
-                A.pot[ga] = pv;
-                const double rv = rva - alpha * apa;
-                A.r[ga] = rv;
-                acc += rv * rv;
-                if (check)
+#pragma unroll
+            for (int u = 0; u < CG_UPT; u++)
+                if (h[u])
                 {
-                    const double ratio = pv / olda;
-                    if ((tm > ratio) || (tp < ratio) || (res1 && fabs(rv) / x.rm >= A.tol))
-                        fail = 1;
+                    const double pv = potv[u] + alpha * pvv[u];
+                    A.pot[g[u]] = pv;
+                    const double rv = rvv[u] - alpha * apv[u];
+                    A.r[g[u]] = rv;
+                    acc += rv * rv;
+                    if (check)
+                    {
+                        const double ratio = pv / oldv[u];
+                        if ((tm > ratio) || (tp < ratio) || (res1 && fabs(rv) / x.rm >= A.tol))
+                            fail = 1;
+                    }
                 }
-            }
-            if (h1)
-            {
-                const double pv = potb + alpha * pvb;
-                A.pot[gb] = pv;
-                const double rv = rvb - alpha * apb;
-                A.r[gb] = rv;
-                acc += rv * rv;
-                if (check)
-                {
-                    const double ratio = pv / oldb;
-                    if ((tm > ratio) || (tp < ratio) || (res1 && fabs(rv) / x.rm >= A.tol))
-                        fail = 1;
-                }
-            }
             const double t = block_sum_d(acc, sh);
             fail = __syncthreads_or(fail);
             if (threadIdx.x == 0)
@@ -2481,10 +2473,10 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
-    // Chunks of at most 1024 interior points (never across nodes), up to two
-    // points a thread of a 512-thread block (the pipelined form: 2048, four
-    // points a thread).  Levels of up to two chunks per resident block-slot give
-    // every block one chunk; larger levels give blocks several.
+    // Chunks of at most CG_UPT x 512 interior points (never across nodes), up to
+    // CG_UPT points a thread of a 512-thread block (the pipelined form: 2048,
+    // four points a thread).  Levels of up to one chunk per resident block-slot
+    // give every block one chunk; larger levels give blocks several.
     constexpr int kCgSmem = 40 * 1024; // slot records and cached grid indices
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
@@ -2510,12 +2502,12 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     const long max_blocks = (long)per_sm * sms;
     const int nt = CG_MAX_THREADS;
     // The level's CG points are cut into about CG_FILL chunks (one block a SM),
-    // or 2 CG_FILL when a chunk would exceed the two points a thread the update
-    // phase holds: the slowest SM sets every phase's length, so chunks fill the
-    // SMs evenly.  Measured on the 1M-particle sphere (CG time a step): fixed
-    // 1024-point chunks 6.98 ms, CG_FILL 148 6.86 ms, 74 6.89, 222 7.88, 296
-    // 7.60.  CG_FILL is fixed, not the device's SM count, so the partial sums
-    // and the results do not depend on the device.
+    // or 2 CG_FILL when a chunk would exceed the CG_UPT points a thread the
+    // update phase holds: the slowest SM sets every phase's length, so chunks fill
+    // the SMs evenly.  Measured on the 1M-particle sphere with two points a
+    // thread (CG time a step): fixed 1024-point chunks 6.98 ms, CG_FILL 148
+    // 6.86 ms, 74 6.89, 222 7.88, 296 7.60.  CG_FILL is fixed, not the device's
+    // SM count, so the partial sums and the results do not depend on the device.
     int chunk = (pipe ? CG2_PPT : 2) * nt;
     if (!pipe)
     {
@@ -2524,10 +2516,10 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
             if (!(ov && ov->skip[q]) && (!allow_sor || L.h[q].ncells > c.branch_cg_cells))
                 tot += L.h[q].nintr;
         long cs = (tot + CG_FILL - 1) / CG_FILL;
-        if (cs > 2L * nt)
+        if (cs > (long)CG_UPT * nt)
             cs = (tot + 2L * CG_FILL - 1) / (2L * CG_FILL);
         cs = (cs + 31) / 32 * 32;
-        chunk = (int)std::max(64L, std::min(cs, 2L * nt));
+        chunk = (int)std::max(64L, std::min(cs, (long)CG_UPT * nt));
     }
     L.hchunks.clear();
     std::vector<int> node_chunk(2L * nn, 0);
