@@ -830,14 +830,16 @@ struct Walk3 {
     }
 };
 
-// The red-black update of point (i, j, k) (k_gs_rb's arithmetic).
-template <typename T>
-__device__ __forceinline__ void mg_rb_point(const Grid<T> &phi, const Grid<T> &rho, int i, int j,
-                                            int k, T H2, T w)
+// The red-black update of point (i, j, k) (k_gs_rb's arithmetic).  G: Grid<T>
+// (64-bit strides) or DGrid<T> (a dense grid of the single-block sub-cycle in
+// shared memory, 32-bit index arithmetic).
+template <typename T, typename G>
+__device__ __forceinline__ void mg_rb_point(const G &phi, const G &rho, int i, int j, int k, T H2,
+                                            T w)
 {
     const T one_sixth = (T)(1.0 / 6.0);
-    const long gp = phi.off + i + j * phi.sy + k * phi.sz;
-    const long gr = rho.off + i + j * rho.sy + k * rho.sz;
+    const auto gp = phi.off + i + j * phi.sy + k * phi.sz;
+    const auto gr = rho.off + i + j * rho.sy + k * rho.sz;
     T *p = phi.p;
     T a = one_sixth * (-H2 * rho.p[gr] + p[gp + 1] + p[gp - 1] + p[gp + phi.sy] +
                        p[gp - phi.sy] + p[gp + phi.sz] + p[gp - phi.sz]);
@@ -874,9 +876,8 @@ __device__ __forceinline__ MgCube mg_cube()
     return MgCube{t & 7, (t >> 3) & 7, t >> 6};
 }
 
-template <typename T>
-__device__ __forceinline__ void mg_rb_half_blk(const Grid<T> &phi, const Grid<T> &rho, int color,
-                                               T H2, T w)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_rb_half_blk(const G &phi, const G &rho, int color, T H2, T w)
 {
     const int m = phi.n - 2, half = (m + 1) / 2;
     const MgCube q = mg_cube();
@@ -894,13 +895,12 @@ __device__ __forceinline__ void mg_rb_half_blk(const Grid<T> &phi, const Grid<T>
 }
 
 // rho_c at coarse point (lx, ly, lz) = scale * the residual at the injected fine point.
-template <typename T>
-__device__ __forceinline__ void mg_restrict_point(const Grid<T> &phi, const Grid<T> &rho,
-                                                  const Grid<T> &crho, T ooh2, T scale, int lx,
-                                                  int ly, int lz)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_restrict_point(const G &phi, const G &rho, const G &crho, T ooh2,
+                                                  T scale, int lx, int ly, int lz)
 {
-    const long gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
-    const long gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
+    const auto gp = phi.off + 2 * lx + 2 * ly * phi.sy + 2 * lz * phi.sz;
+    const auto gr = rho.off + 2 * lx + 2 * ly * rho.sy + 2 * lz * rho.sz;
     const T *p = phi.p;
     T rv = rho.p[gr] + ooh2 * ((T)6 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + phi.sy] -
                                p[gp - phi.sy] - p[gp + phi.sz] - p[gp - phi.sz]);
@@ -921,17 +921,16 @@ __device__ __forceinline__ void mg_restrict(const Grid<T> &phi, const Grid<T> &r
         mg_restrict_point(phi, rho, crho, ooh2, scale, 1 + (int)x.a, 1 + (int)x.b, 1 + (int)x.c);
 }
 
-template <typename T>
-__device__ __forceinline__ void mg_restrict_blk(const Grid<T> &phi, const Grid<T> &rho,
-                                                const Grid<T> &cphi, const Grid<T> &crho, T ooh2,
-                                                T scale)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_restrict_blk(const G &phi, const G &rho, const G &cphi,
+                                                const G &crho, T ooh2, T scale)
 {
     const int nc = cphi.n, mc = nc - 2;
     const MgCube q = mg_cube();
     for (int k = q.z; k < nc; k += 8)
         for (int j = q.y; j < nc; j += 8)
             for (int i = q.x; i < nc; i += 8)
-                cphi.p[cphi.off + i + (long)j * cphi.sy + (long)k * cphi.sz] = (T)0;
+                cphi.p[cphi.off + i + j * cphi.sy + k * cphi.sz] = (T)0;
     for (int k = 1 + q.z; k <= mc; k += 8)
         for (int j = 1 + q.y; j <= mc; j += 8)
             for (int i = 1 + q.x; i <= mc; i += 8)
@@ -944,9 +943,9 @@ __device__ __forceinline__ void mg_restrict_blk(const Grid<T> &phi, const Grid<T
 // their up to eight coarse values are loaded once, together.  Each point adds
 // its terms in k_prolong_add's z, y, x order, skipping coarse points outside
 // 1..mc; a point even in all three coordinates takes its coarse value as is.
-template <typename T>
-__device__ __forceinline__ void mg_prolong_pair(const Grid<T> &phi, const Grid<T> &c, int mc, int a,
-                                                int j, int k)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_prolong_pair(const G &phi, const G &c, int mc, int a, int j,
+                                                int k)
 {
     const int i0 = 2 * a + 1;
     const bool second = a < mc; // i0 + 1 <= m
@@ -960,16 +959,16 @@ __device__ __forceinline__ void mg_prolong_pair(const Grid<T> &phi, const Grid<T
     vz[1] = ko && oz0 + 1 <= mc;
     const bool vx0 = a >= 1, vx1 = a + 1 <= mc;
     const T wy = jo ? (T)0.5 : (T)1, wz = ko ? (T)0.5 : (T)1;
-    const long cb = c.off + a + (long)oy0 * c.sy + (long)oz0 * c.sz;
+    const auto cb = c.off + a + oy0 * c.sy + oz0 * c.sz;
     T v[8]; // [z][y][x] with x = column a, a + 1
 #pragma unroll
     for (int q = 0; q < 8; q++)
     {
         const int az = q >> 2, ay = (q >> 1) & 1, ax = q & 1;
         const bool ok = vz[az] && vy[ay] && (ax ? vx1 : vx0);
-        v[q] = ok ? c.p[cb + ax + (long)ay * c.sy + (long)az * c.sz] : (T)0;
+        v[q] = ok ? c.p[cb + ax + ay * c.sy + az * c.sz] : (T)0;
     }
-    const long f0 = phi.off + i0 + (long)j * phi.sy + (long)k * phi.sz;
+    const auto f0 = phi.off + i0 + j * phi.sy + k * phi.sz;
     const T p0 = phi.p[f0];
     const T p1 = second ? phi.p[f0 + 1] : (T)0;
     // odd point i0: x weight 1/2 on both columns
@@ -1012,18 +1011,18 @@ __device__ __forceinline__ void mg_prolong(const Grid<T> &phi, const Grid<T> &c,
     const int m = phi.n - 2, mc = c.n - 2;
     const unsigned um = (unsigned)m, pairs = (unsigned)mc + 1; // m = 2 mc + 1
     for (Walk3 x(tid, nthr, pairs, um); x.c < um; x.next())
-        mg_prolong_pair(phi, c, mc, (int)x.a, 1 + (int)x.b, 1 + (int)x.c);
+        mg_prolong_pair<T>(phi, c, mc, (int)x.a, 1 + (int)x.b, 1 + (int)x.c);
 }
 
-template <typename T>
-__device__ __forceinline__ void mg_prolong_blk(const Grid<T> &phi, const Grid<T> &c)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_prolong_blk(const G &phi, const G &c)
 {
     const int m = phi.n - 2, mc = c.n - 2;
     const MgCube q = mg_cube();
     for (int k = 1 + q.z; k <= m; k += 8)
         for (int j = 1 + q.y; j <= m; j += 8)
             for (int a = q.x; a <= mc; a += 8)
-                mg_prolong_pair(phi, c, mc, a, j, k);
+                mg_prolong_pair<T>(phi, c, mc, a, j, k);
 }
 
 // Smoothing sweeps of level l over the whole grid of threads; sync() separates
@@ -1041,9 +1040,8 @@ __device__ __forceinline__ void mg_smooth(const MgArgs<T> &A, int l, int sweeps,
 }
 
 // The same inside one block (grids of the single-block sub-cycle).
-template <typename T>
-__device__ __forceinline__ void mg_smooth_blk(const Grid<T> &phi, const Grid<T> &rho, T H2, T w,
-                                              int sweeps)
+template <typename T, typename G>
+__device__ __forceinline__ void mg_smooth_blk(const G &phi, const G &rho, T H2, T w, int sweeps)
 {
     for (int it = 0; it < sweeps; it++)
         for (int color = 0; color < 2; color++)
@@ -1053,27 +1051,57 @@ __device__ __forceinline__ void mg_smooth_blk(const Grid<T> &phi, const Grid<T> 
         }
 }
 
-template <typename T> __device__ __forceinline__ Grid<T> mg_dense(T *p, int n)
+// A dense n^3 grid in shared memory (the single-block sub-cycle): 32-bit strides.
+template <typename T> struct DGrid {
+    T *p;
+    static constexpr int off = 0;
+    int sy, sz, n;
+};
+
+template <typename T> __device__ __forceinline__ DGrid<T> mg_dense(T *p, int n)
 {
-    Grid<T> g;
+    DGrid<T> g;
     g.p = p;
-    g.off = 0;
     g.sy = n;
-    g.sz = (long)n * n;
+    g.sz = n * n;
     g.n = n;
     return g;
 }
 
-// Copies all points of grid a into grid b (same size), block-wide.
+// Block-wide copies between a level's grid and its shared-memory copy.  A
+// dense level (offset 0, strides n and n^2: every level below the finest) moves
+// as a flat array, by asynchronous copies in, all in flight at once.
+template <typename T> __device__ __forceinline__ bool mg_is_dense(const Grid<T> &a)
+{
+    return a.off == 0 && a.sy == a.n && a.sz == (long)a.n * a.n;
+}
+
 template <typename T>
-__device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsigned tid,
-                                        unsigned nthr)
+__device__ __forceinline__ void mg_copy_in(const Grid<T> &a, const DGrid<T> &b, unsigned tid,
+                                           unsigned nthr)
 {
     const unsigned n = (unsigned)a.n, n3 = n * n * n;
-    const long nn = (long)n * n;
-    if (a.off == 0 && b.off == 0 && a.sy == n && b.sy == n && a.sz == nn && b.sz == nn)
+    if (mg_is_dense(a))
     {
-        // both dense: a flat loop, unrolled so that several loads are in flight
+        for (unsigned t = tid; t < n3; t += nthr)
+            __pipeline_memcpy_async(&b.p[t], &a.p[t], sizeof(T));
+        __pipeline_commit();
+        __pipeline_wait_prior(0);
+        return;
+    }
+    for (Walk3 x(tid, nthr, n, n); x.c < n; x.next())
+        b.p[x.a + x.b * b.sy + x.c * b.sz] =
+            a.p[a.off + (long)x.a + (long)x.b * a.sy + (long)x.c * a.sz];
+}
+
+template <typename T>
+__device__ __forceinline__ void mg_copy_out(const DGrid<T> &a, const Grid<T> &b, unsigned tid,
+                                            unsigned nthr)
+{
+    const unsigned n = (unsigned)a.n;
+    if (mg_is_dense(b))
+    {
+        const unsigned n3 = n * n * n;
 #pragma unroll 4
         for (unsigned t = tid; t < n3; t += nthr)
             b.p[t] = a.p[t];
@@ -1081,7 +1109,35 @@ __device__ __forceinline__ void mg_copy(const Grid<T> &a, const Grid<T> &b, unsi
     }
     for (Walk3 x(tid, nthr, n, n); x.c < n; x.next())
         b.p[b.off + (long)x.a + (long)x.b * b.sy + (long)x.c * b.sz] =
-            a.p[a.off + (long)x.a + (long)x.b * a.sy + (long)x.c * a.sz];
+            a.p[x.a + x.b * a.sy + x.c * a.sz];
+}
+
+// The levels of the single-block sub-cycle (P(l), R(l): a level's phi and rho,
+// in shared or global memory).
+template <typename T, typename PF, typename RF>
+__device__ __forceinline__ void mg_subcycle_levels(const MgArgs<T> &A, PF P, RF R)
+{
+    for (int l = A.nsmall; l < A.nlev; l++)
+    {
+        mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_pre);
+        if (l == A.nlev - 1)
+            mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_coarse);
+        else
+        {
+            const int n = A.phi[l].n;
+            mg_restrict_blk(P(l), R(l), P(l + 1), R(l + 1), (T)(double)((n - 1) * (n - 1)), A.scale);
+            __syncthreads();
+        }
+    }
+    for (int l = A.nlev - 1; l >= A.nsmall; l--)
+    {
+        if (l < A.nlev - 1)
+        {
+            mg_prolong_blk<T>(P(l), P(l + 1));
+            __syncthreads();
+        }
+        mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_post);
+    }
 }
 
 // ---- coarse levels in tiled phases ------------------------------------------------------
@@ -1552,45 +1608,33 @@ __global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_consta
         if (blockIdx.x == 0)
         {
             const unsigned bt = threadIdx.x, bn = blockDim.x;
-            T *sm = reinterpret_cast<T *>(mg_dyn);
-            auto P = [&](int l) {
-                return A.smem ? mg_dense(sm + A.soff[l], A.phi[l].n) : A.phi[l];
-            };
-            auto R = [&](int l) {
-                return A.smem ? mg_dense(sm + A.soff[l] + A.phi[l].n * A.phi[l].n * A.phi[l].n,
-                                         A.phi[l].n)
-                              : A.rho[l];
-            };
             if (A.smem)
             {
-                mg_copy(A.phi[A.nsmall], P(A.nsmall), bt, bn);
-                mg_copy(A.rho[A.nsmall], R(A.nsmall), bt, bn);
-                __syncthreads();
-            }
-            for (int l = A.nsmall; l < A.nlev; l++)
-            {
-                mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_pre);
-                if (l == A.nlev - 1)
-                    mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_coarse);
-                else
-                {
+                T *sm = reinterpret_cast<T *>(mg_dyn);
+                auto P = [&](int l) { return mg_dense(sm + A.soff[l], A.phi[l].n); };
+                auto R = [&](int l) {
                     const int n = A.phi[l].n;
-                    mg_restrict_blk(P(l), R(l), P(l + 1), R(l + 1), (T)(double)((n - 1) * (n - 1)),
-                                    A.scale);
-                    __syncthreads();
-                }
-            }
-            for (int l = A.nlev - 1; l >= A.nsmall; l--)
-            {
-                if (l < A.nlev - 1)
+                    return mg_dense(sm + A.soff[l] + n * n * n, n);
+                };
+                // a coarse level's correction starts at zero (the restriction into
+                // it zeroed it): only its rho is copied in
+                const int ns = A.nsmall, n = A.phi[ns].n;
+                if (ns > 0)
                 {
-                    mg_prolong_blk(P(l), P(l + 1));
-                    __syncthreads();
+                    const DGrid<T> p0 = P(ns);
+                    for (int t = bt; t < n * n * n; t += bn)
+                        p0.p[t] = (T)0;
                 }
-                mg_smooth_blk(P(l), R(l), A.h2[l], A.w, A.n_post);
+                else
+                    mg_copy_in(A.phi[ns], P(ns), bt, bn);
+                mg_copy_in(A.rho[ns], R(ns), bt, bn);
+                __syncthreads();
+                mg_subcycle_levels(A, P, R);
+                mg_copy_out(P(ns), A.phi[ns], bt, bn);
             }
-            if (A.smem)
-                mg_copy(P(A.nsmall), A.phi[A.nsmall], bt, bn);
+            else
+                mg_subcycle_levels(A, [&](int l) { return A.phi[l]; },
+                                   [&](int l) { return A.rho[l]; });
         }
         gsync();
         for (int l = A.nsmall - 1; l >= 0; l--)
