@@ -1144,9 +1144,9 @@ static qz_sim *dense_context(const qz_config *cfg, int gridsize, double **dphi, 
 static int run_dense(const qz_config *cfg, double *phi, const double *rho, int gridsize,
                      int (*body)(qz_sim *, void *), void *arg)
 {
-    if (!phi || !rho || gridsize < 3)
+    if (!phi || !rho || gridsize < 3 || (long)gridsize * gridsize * gridsize >= (1L << 31))
     {
-        set_error("bad grid arguments");
+        set_error("bad grid arguments (3 <= gridsize, gridsize^3 < 2^31)");
         return QZ_FAILURE;
     }
     double *dphi = nullptr, *drho = nullptr;

@@ -21,12 +21,15 @@
 namespace qz {
 
 // Strided view of an n^3 multigrid level: point (i,j,k) at p[off + i + j*sy + k*sz].
+// Every grid has fewer than 2^31 points (head grids of at most (2^9 + 3)^3,
+// array-level grids checked at entry), so offsets and strides are 32-bit and
+// index arithmetic stays in 32 bits unless a kernel widens it.
 template <typename T>
 struct Grid {
     T *p;
-    long off;
-    long sy;
-    long sz;
+    int off;
+    int sy;
+    int sz;
     int n;
 };
 
