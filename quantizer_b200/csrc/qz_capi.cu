@@ -125,8 +125,8 @@ static bool build_levels(qz_sim *s, int n0)
     const bool cgs = s->cfg.smoother == 2;
     if (cgs && !s->cg_part && !dmalloc(&s->cg_part, 2 * QZ_CG_PART_MAX, "cg partials"))
         return false;
-    // mixed form: per-block partials of the in-launch convergence test, its result
-    if (mixed && !s->mg_part && !dmalloc(&s->mg_part, 2 * QZ_CG_PART_MAX + 8, "mg partials"))
+    // persistent cycles: per-block partials of the in-launch convergence test, its result
+    if (!s->mg_part && !dmalloc(&s->mg_part, 2 * QZ_CG_PART_MAX + 8, "mg partials"))
         return false;
     for (auto &l : s->levels)
     {

@@ -793,6 +793,7 @@ template <typename T> struct MgArgs {
     double tm, tp, rm, tol; // 1 -/+ tol2, 4 pi G rho_mean, tol
     int method;
     long nintr;
+    int every; // FP64 form: the test after every `every` cycles (the reference's cadence)
     // coarse levels 1 .. nsmall-1 in tiled phases (mg_tile_down / mg_tile_up):
     // bit l of tiled set for a tiled level, tile cores of tc[0] x tc[1] x tc[2] points
     int tiled;
@@ -1470,6 +1471,111 @@ template <typename T> __device__ __noinline__ void mg_tile_up(const MgArgs<T> &A
     }
 }
 
+// The FP64 form's convergence test inside the launch after `it` cycles
+// (k_check_partial / k_check_final / k_copy_if_unconverged on the fine
+// interior): per-block residual partials and ratio-test flags, one grid
+// barrier, the decision taken by every block from the partials in the same
+// order; unconverged: pot_old = pot on the interior (its boundary equals pot's
+// for the whole solve).  True when converged (block 0 records it in outst).
+template <typename Sync>
+__device__ bool mg_check64(const MgArgs<double> &A, int it, unsigned gtid, unsigned gn, Sync gsync)
+{
+    const Grid<double> &P = A.phi[0], &R = A.rho[0];
+    const int n = P.n, m = n - 2;
+    const double ooh2 = (double)((n - 1) * (n - 1));
+    const unsigned um = (unsigned)m;
+    double acc = 0.0;
+    int fl = 0; // 1 ratio test failed, 2 point residual test failed (method 1)
+    for (Walk3 x(gtid, gn, um, um); x.c < um; x.next())
+    {
+        const int i = 1 + (int)x.a, j = 1 + (int)x.b, k = 1 + (int)x.c;
+        const int gp = P.off + i + j * P.sy + k * P.sz;
+        const double *p = P.p;
+        const double r = R.p[R.off + i + j * R.sy + k * R.sz] +
+                         ooh2 * (6.0 * p[gp] - p[gp + 1] - p[gp - 1] - p[gp + P.sy] - p[gp - P.sy] -
+                                 p[gp + P.sz] - p[gp - P.sz]);
+        const double a = p[gp] / A.pold[gp];
+        if ((A.tm > a) || (A.tp < a))
+            fl |= 1;
+        if (A.method == 1)
+        {
+            if (fabs(r) / A.rm >= A.tol)
+                fl |= 2;
+        }
+        else
+            acc += r * r;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    fl = (int)__reduce_or_sync(0xffffffffu, (unsigned)fl);
+    __shared__ double wacc[MG_THREADS / 32];
+    __shared__ int wfl[MG_THREADS / 32];
+    __shared__ int s_stop;
+    if ((threadIdx.x & 31) == 0)
+    {
+        wacc[threadIdx.x >> 5] = acc;
+        wfl[threadIdx.x >> 5] = fl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0.0;
+        int f = 0;
+        for (int w = 0; w < MG_THREADS / 32; w++)
+        {
+            t += wacc[w];
+            f |= wfl[w];
+        }
+        A.part[blockIdx.x] = t;
+        A.part[QZ_CG_PART_MAX + blockIdx.x] = (double)f;
+    }
+    gsync();
+    if (threadIdx.x < 32)
+    {
+        double t = 0.0;
+        int f = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
+        {
+            t += __ldcg(A.part + b);
+            f |= (int)__ldcg(A.part + QZ_CG_PART_MAX + b);
+        }
+        for (int o = 16; o > 0; o >>= 1)
+            t += __shfl_xor_sync(0xffffffffu, t, o);
+        f = (int)__reduce_or_sync(0xffffffffu, (unsigned)f);
+        if (threadIdx.x == 0)
+        {
+            int ok;
+            if (A.method == 1)
+                ok = !(f & 2);
+            else
+            {
+                double err = t / A.nintr;
+                err = sqrt(err);
+                err = err / A.rm;
+                if (A.method == 2)
+                    err = err / (cbrt((double)A.nintr) * cbrt((double)A.nintr));
+                ok = err < A.tol;
+            }
+            s_stop = !(f & 1) && ok;
+            if (s_stop && blockIdx.x == 0)
+            {
+                A.outst[0] = it;
+                A.outst[1] = 1;
+            }
+        }
+    }
+    __syncthreads();
+    if (s_stop)
+        return true;
+    for (Walk3 x(gtid, gn, um, um); x.c < um; x.next())
+    {
+        const int gp = P.off + 1 + (int)x.a + (1 + (int)x.b) * P.sy + (1 + (int)x.c) * P.sz;
+        A.pold[gp] = P.p[gp];
+    }
+    // the partials are rewritten only after the next cycle's barriers
+    return false;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_constant__ MgArgs<T> A)
 {
@@ -1479,6 +1585,9 @@ __global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_consta
     auto gsync = [&]() { gbar_sync(A.bar, &sh_ok); };
     for (int it = 0; it < A.iters; it++)
     {
+        if constexpr (std::is_same<T, double>::value)
+            if (A.check && it > 0 && it % A.every == 0 && mg_check64(A, it, gtid, gn, gsync))
+                return;
         if (A.mixed)
         {
             // rf = (float)(rho + ooh2 (6 phi - sum)) on the fine interior (FP64), ef = 0
@@ -1663,6 +1772,9 @@ __global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_consta
             gsync();
         }
     }
+    if constexpr (std::is_same<T, double>::value)
+        if (A.check && A.iters > 0 && A.iters % A.every == 0 && mg_check64(A, A.iters, gtid, gn, gsync))
+            return;
     if (A.check && gtid == 0)
     {
         A.outst[0] = A.iters;
@@ -1710,7 +1822,8 @@ template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = fa
     A.frho = s->fine_rho;
     A.bar = GridBar{s->gbar, s->flags};
     cudaMemsetAsync(s->gbar, 0, 4 * sizeof(unsigned), s->stream);
-    A.check = check && A.mixed ? 1 : 0;
+    A.check = check ? 1 : 0;
+    A.every = A.mixed ? 1 : (c.check_every > 0 ? c.check_every : 1);
     if (A.check)
     {
         const int L = s->L;
@@ -2278,29 +2391,22 @@ int potential_head(qz_sim *s)
     }
     else if (mg_persistent(s))
     {
-        // one cooperative launch per check block, then the convergence test
-        while (iter < c.max_iter && !check)
+        // FP64 form: one launch runs the cycles and takes the convergence test
+        // after every `every` cycles, as the host loop of check blocks did
+        if (mg_launch<double>(s, c.max_iter, true))
+            return QZ_FAILURE;
+        if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
+                                        cudaMemcpyDeviceToHost, s->stream),
+                        "flags") ||
+            !check_cuda(cudaStreamSynchronize(s->stream), "flags"))
+            return QZ_FAILURE;
+        if (s->h_flags[F_ERROR] & E_BARRIER)
         {
-            int k = every - (iter % every);
-            if (k > c.max_iter - iter)
-                k = c.max_iter - iter;
-            if (mg_cycles(s, k))
-                return QZ_FAILURE;
-            iter += k;
-            if (iter % every == 0)
-            {
-                if (launch_check(s, s->head_mass))
-                    return QZ_FAILURE;
-                if (!check_cuda(cudaStreamSynchronize(s->stream), "convergence readback"))
-                    return QZ_FAILURE;
-                check = s->h_flags[F_CONVERGED] != 0;
-                if (s->h_flags[F_ERROR] & E_BARRIER)
-                {
-                    set_error("multigrid cycles: a grid barrier wait gave up");
-                    return QZ_FAILURE;
-                }
-            }
+            set_error("multigrid cycles: a grid barrier wait gave up");
+            return QZ_FAILURE;
         }
+        iter = s->mg_ran;
+        check = s->mg_conv != 0;
     }
     while (iter < c.max_iter && !check)
     {
