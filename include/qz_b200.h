@@ -134,6 +134,13 @@ typedef struct qz_config {
      * does (0, default): fewer iterations, the same convergence test, results
      * that differ from the reference's by the solve tolerance */
     int node_warm;
+    /* refinement steps whose head solve is one persistent launch: 1 (default)
+     * runs that launch on a second stream of higher priority while the tree
+     * construction and the level deposits, which read only the particles, run
+     * on the simulation's stream; the level solves start when both are done.
+     * 0 runs the stages one after another in main.c's order.  Results are the
+     * same bit for bit either way. */
+    int tree_overlap;
 } qz_config;
 
 /* tile cores (x, y, z points) of the tiled multigrid phases, in mg_tile order */

@@ -345,6 +345,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->node_solver = QZ_NODE_CG;
     c->mg_tile = 0;
     c->node_warm = 0;
+    c->tree_overlap = 1;
     return QZ_SUCCESS;
 }
 
@@ -428,6 +429,15 @@ int qz_destroy(qz_sim *s)
         cudaEventDestroy(s->ev_mass);
     if (s->ev_drift)
         cudaEventDestroy(s->ev_drift);
+    if (s->head_stream)
+    {
+        cudaStreamSynchronize(s->head_stream);
+        cudaStreamDestroy(s->head_stream);
+    }
+    if (s->ev_fork)
+        cudaEventDestroy(s->ev_fork);
+    if (s->ev_head)
+        cudaEventDestroy(s->ev_head);
     if (s->stream)
         cudaStreamDestroy(s->stream);
     delete s;
@@ -762,12 +772,66 @@ int qz_init_forces(qz_sim *s)
 } // extern "C"
 
 namespace qz {
+// Tree, densities and potentials of a step (main.c:417-447).  The tree and the
+// level deposits read only the particles, and the head solve reads only the
+// head density, so in refinement runs whose head solve is one persistent
+// launch (tree_overlap) that launch runs on a stream of higher priority (its
+// blocks are placed before the tree kernels' waiting blocks) while the tree is
+// built and the levels deposited on the simulation's stream, with the host
+// waits of the tree construction overlapping the solve; the level solves wait
+// for both.  Every kernel computes what it computes in the sequential order.
+// Measured on the 1M-particle sphere (128^3 head, three levels), ms a step:
+// sequential 10.54-10.59; overlapped with 4 points a thread (two blocks on
+// every SM: the tree kernels wait for the solve) 10.61, 8 points 9.66-9.80,
+// 10 points 9.57, 12 points 9.53, 16 points 9.95.
+constexpr int OVERLAP_PPT = 12;
+
+static int tree_density_potential(qz_sim *s)
+{
+    if (!amr_on(s) || !s->cfg.tree_overlap || s->no_overlap || !head_one_launch(s))
+        return (qz_tree_adaptation(s) || qz_grid_density(s) || qz_potential(s)) ? QZ_FAILURE
+                                                                                : QZ_SUCCESS;
+    if (!s->head_stream)
+    {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (!check_cuda(cudaStreamCreateWithPriority(&s->head_stream, cudaStreamNonBlocking,
+                                                     greatest),
+                        "head-solve stream") ||
+            !check_cuda(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming), "event") ||
+            !check_cuda(cudaEventCreateWithFlags(&s->ev_head, cudaEventDisableTiming), "event"))
+            return QZ_FAILURE;
+    }
+    bool issued = false;
+    if (deposit_head(s) || !check_cuda(cudaEventRecord(s->ev_fork, s->stream), "fork") ||
+        !check_cuda(cudaStreamWaitEvent(s->head_stream, s->ev_fork, 0), "fork"))
+        return QZ_FAILURE;
+    // the head launch takes at least OVERLAP_PPT points a thread: fewer blocks,
+    // so that SMs keep room for the tree's kernels (128^3 head: 177 blocks of
+    // 512 threads instead of two on every SM)
+    s->mg_ppt_floor = OVERLAP_PPT;
+    const int rc_issue = potential_head_issue(s, s->head_stream, &issued);
+    s->mg_ppt_floor = 0;
+    if (rc_issue || !check_cuda(cudaEventRecord(s->ev_head, s->head_stream), "join"))
+    {
+        cudaStreamSynchronize(s->head_stream);
+        return QZ_FAILURE;
+    }
+    const bool tree_ok = !qz_tree_adaptation(s) && !amr_deposit(s);
+    // the head launch is always waited for, whatever the tree's outcome
+    const bool head_ok = !potential_head_finish(s, s->head_stream);
+    if (!check_cuda(cudaStreamWaitEvent(s->stream, s->ev_head, 0), "join") || !tree_ok ||
+        !head_ok)
+        return QZ_FAILURE;
+    return amr_potential(s);
+}
+
 // main.c:375-481 with a given dt: kick-drift, reset, tree, deposit, potential,
 // gradient, gather, kick.
 int step_core(qz_sim *s, double h)
 {
-    if (kick_drift(s, h) || qz_reset(s) || qz_tree_adaptation(s) || qz_grid_density(s) ||
-        qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, h))
+    if (kick_drift(s, h) || qz_reset(s) || tree_density_potential(s) ||
+        qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, h))
         return QZ_FAILURE;
     s->stats.steps++;
     s->stats.last_dt = h;
@@ -833,8 +897,8 @@ int qz_step(qz_sim *s, double dt, int nsteps)
 
 // One step on host-resident state.  Page-locked arrays (every one of the ten):
 // x..vz and ax..az go in on the simulation's stream, the masses on a second
-// stream while the kick-drift and the tree run (the deposit is the first stage
-// that reads them), and the drifted positions come back on the second stream
+// stream beside them and the kick-drift (the deposit is the first stage that
+// reads them), and the drifted positions come back on the second stream
 // while the forces are computed; velocities and accelerations come back after
 // the kick.  Pageable arrays: the staged copies of qz_set_particles /
 // qz_get_particles around qz_step.  The arithmetic is qz_step's either way.
@@ -889,9 +953,9 @@ int qz_step_host(qz_sim *s, double dt, double *x, double *y, double *z, double *
     for (int q = 0; q < 3; q++)
         if (!check_cuda(cudaMemcpyAsync(hx[q], dx[q], b, cudaMemcpyDeviceToHost, s->xfer), "d2h"))
             return QZ_FAILURE;
-    if (qz_reset(s) || qz_tree_adaptation(s) ||
-        !check_cuda(cudaStreamWaitEvent(s->stream, s->ev_mass, 0), "wait") || qz_grid_density(s) ||
-        qz_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, dt))
+    if (qz_reset(s) || !check_cuda(cudaStreamWaitEvent(s->stream, s->ev_mass, 0), "wait") ||
+        tree_density_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) ||
+        kick(s, dt))
         return QZ_FAILURE;
     s->stats.steps++;
     s->stats.last_dt = dt;

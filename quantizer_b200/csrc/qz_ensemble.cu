@@ -40,6 +40,9 @@ extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *d
         nthreads = 1;
     if (nthreads > nsims)
         nthreads = nsims > 0 ? nsims : 1;
+    // members run side by side already: each keeps its stages on its own stream
+    for (int k = 0; k < nsims; k++)
+        sims[k]->no_overlap = true;
     std::atomic<int> next{0};
     std::atomic<int> failed{-1};
     std::mutex mu;
@@ -74,6 +77,8 @@ extern "C" QZ_API int qz_ensemble_step(qz_sim **sims, int nsims, const double *d
     worker();
     for (auto &th : pool)
         th.join();
+    for (int k = 0; k < nsims; k++)
+        sims[k]->no_overlap = false;
     if (failed.load() >= 0)
     {
         set_error("qz_ensemble_step: simulation %d: %s", failed.load(), first_error.c_str());

@@ -325,6 +325,14 @@ struct qz_sim {
     double *cg_part = nullptr; // conjugate-gradient smoothing: 2 x QZ_CG_PART_MAX partial sums
     double *mg_part = nullptr; // mixed head cycles: block partials of the convergence test + result
     int mg_ran = 0, mg_conv = 0; // mixed head cycles: iterations of the last launch, converged
+    double mg_cycle_bytes = 0.0; // deferred head launch: profiler bytes of one cycle
+    int mg_prof_idx = -1;        // deferred head launch: its profiler record, or -1
+    // refinement steps: higher-priority stream of the head solve while the tree
+    // and the level deposits run on `stream`, and the fork / join events
+    cudaStream_t head_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_head = nullptr;
+    bool no_overlap = false; // set by qz_ensemble_step: members stay on one stream
+    int mg_ppt_floor = 0;    // fewest finest-level points a thread of the head launch takes
     unsigned *gbar = nullptr;  // grid barrier words of the cooperative launches (4)
     long n = 0, cap = 0;
     double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
@@ -537,6 +545,9 @@ int amr_potential(qz_sim *s);
 int amr_grid_accel(qz_sim *s);
 int amr_gather(qz_sim *s);
 int poisson_error_head(qz_sim *s, int *converged);
+bool head_one_launch(const qz_sim *s);
+int potential_head_issue(qz_sim *s, cudaStream_t st, bool *issued);
+int potential_head_finish(qz_sim *s, cudaStream_t st);
 int smooth(qz_sim *s, Grid<double> phi, Grid<double> rho, int iters);
 void sync_fine_alt(qz_sim *s);
 void init_kernel_attributes();

@@ -1792,7 +1792,10 @@ bool mg_persistent(const qz_sim *s)
            !s->fused_rb && (int)s->levels.size() <= MG_MAXLEV;
 }
 
-template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = false)
+// check: the convergence test inside the launch; defer: no host wait for the
+// launch's outcome (potential_head_finish reads it)
+template <typename T>
+static int mg_launch(qz_sim *s, int iters, bool check = false, bool defer = false)
 {
     const qz_config &c = s->cfg;
     MgArgs<T> A;
@@ -1881,7 +1884,8 @@ template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = fa
     // independent simulations can run their cycles side by side
     const long m0 = A.phi[0].n - 2;
     const long work = (m0 + 1) / 2 * m0 * m0;
-    const long ppt = c.mg_points_per_thread > 0 ? c.mg_points_per_thread : 4;
+    const long ppt = std::max((long)(c.mg_points_per_thread > 0 ? c.mg_points_per_thread : 4),
+                              (long)s->mg_ppt_floor);
     const int blocks = (int)std::max(1L, std::min((long)std::min(ps, 2) * sms,
                                                   (work + ppt * MG_THREADS - 1) / (ppt * MG_THREADS)));
     // tiled coarse levels: the first core (or the configured one) whose two
@@ -1952,7 +1956,12 @@ template <typename T> static int mg_launch(qz_sim *s, int iters, bool check = fa
         cudaEventRecord(ee, s->stream);
         s->prof_pending.push_back({QZ_PROF_SMOOTH, bytes * iters, eb, ee});
     }
-    if (A.check)
+    if (A.check && defer)
+    {
+        s->mg_cycle_bytes = bytes;
+        s->mg_prof_idx = s->prof ? (int)s->prof_pending.size() - 1 : -1;
+    }
+    else if (A.check)
     {
         // iterations run and the test's outcome; the profiler's bytes follow the count
         int st[2] = {0, 0};
@@ -2335,9 +2344,92 @@ int poisson_error_head(qz_sim *s, int *converged)
     return QZ_SUCCESS;
 }
 
+// The head solve is one persistent launch with the convergence test inside it
+// (multigrid cycles of the red-black V-cycle, FP64 or the mixed form, no
+// replayed schedule).
+bool head_one_launch(const qz_sim *s)
+{
+    return s->cfg.head_pot_method != 1 && s->sched_mode != 2 && mg_persistent(s);
+}
+
+// Iteration count, outcome and statistics of a head solve (potential_head_node.c:151-155:
+// reaching the cap is a failure).
+static int head_tail(qz_sim *s, int iter, bool check)
+{
+    const qz_config &c = s->cfg;
+    s->stats.last_vcycles = iter;
+    s->stats.vcycles_total += iter;
+    s->stats.last_converged = check ? 1 : 0;
+    if (s->sched_mode == 1)
+        sched_put(s, &iter, 1);
+    if (iter == c.max_iter)
+    {
+        set_error("the precision was not reached in the head node after %d multigrid cycles",
+                  iter);
+        return QZ_FAILURE;
+    }
+    return QZ_SUCCESS;
+}
+
+// First half of a one-launch head solve: pot_old, the fine-level views and the
+// cooperative launch, all on stream st, with no host wait.  *issued is false
+// (and nothing is queued) when the head solve is not one launch.
+int potential_head_issue(qz_sim *s, cudaStream_t st, bool *issued)
+{
+    *issued = false;
+    if (!head_one_launch(s))
+        return QZ_SUCCESS;
+    const qz_config &c = s->cfg;
+    cudaStream_t keep = s->stream;
+    s->stream = st;
+    cudaMemcpyAsync(s->pot_old, s->pot, s->gpts * sizeof(double), cudaMemcpyDeviceToDevice,
+                    s->stream);
+    sync_fine_alt(s);
+    // the mixed form tests after every defect-correction iteration (its FP64
+    // residual is computed anyway); the FP64 form keeps the reference's cadence
+    const int rc = c.precision == QZ_PREC_MIXED ? mg_launch<float>(s, c.max_iter, true, true)
+                                                : mg_launch<double>(s, c.max_iter, true, true);
+    s->stream = keep;
+    *issued = rc == QZ_SUCCESS;
+    return rc;
+}
+
+// Second half: waits for the launch on stream st and reads its iteration count,
+// the test's outcome and the barrier status.
+int potential_head_finish(qz_sim *s, cudaStream_t st)
+{
+    int out[2] = {0, 0};
+    const int *outst = reinterpret_cast<const int *>(s->mg_part + 2 * QZ_CG_PART_MAX);
+    if (!check_cuda(cudaMemcpyAsync(out, outst, sizeof out, cudaMemcpyDeviceToHost, st),
+                    "multigrid result") ||
+        !check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
+                                    cudaMemcpyDeviceToHost, st),
+                    "flags") ||
+        !check_cuda(cudaStreamSynchronize(st), "multigrid result"))
+        return QZ_FAILURE;
+    s->mg_ran = out[0];
+    s->mg_conv = out[1];
+    if (s->mg_prof_idx >= 0 && s->mg_prof_idx < (int)s->prof_pending.size())
+        s->prof_pending[s->mg_prof_idx].bytes = s->mg_cycle_bytes * out[0];
+    s->mg_prof_idx = -1;
+    if (s->h_flags[F_ERROR] & E_BARRIER)
+    {
+        set_error("multigrid cycles: a grid barrier wait gave up");
+        return QZ_FAILURE;
+    }
+    return head_tail(s, s->mg_ran, s->mg_conv != 0);
+}
+
 int potential_head(qz_sim *s)
 {
     const qz_config &c = s->cfg;
+    if (head_one_launch(s))
+    {
+        bool issued = false;
+        if (potential_head_issue(s, s->stream, &issued))
+            return QZ_FAILURE;
+        return potential_head_finish(s, s->stream);
+    }
     cudaMemcpyAsync(s->pot_old, s->pot, s->gpts * sizeof(double), cudaMemcpyDeviceToDevice,
                     s->stream);
     if (c.head_pot_method == 1)
@@ -2370,44 +2462,6 @@ int potential_head(qz_sim *s)
     const int every =
         c.precision == QZ_PREC_MIXED ? 1 : (c.check_every > 0 ? c.check_every : 1);
     const bool graphs = s->use_graphs && !s->prof;
-    if (mg_persistent(s) && c.precision == QZ_PREC_MIXED)
-    {
-        // mixed form: one launch runs the defect-correction iterations and takes the
-        // convergence test (FP64) before every iteration's cycle from the second on
-        if (mg_launch<float>(s, c.max_iter, true))
-            return QZ_FAILURE;
-        if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
-                                        cudaMemcpyDeviceToHost, s->stream),
-                        "flags") ||
-            !check_cuda(cudaStreamSynchronize(s->stream), "flags"))
-            return QZ_FAILURE;
-        if (s->h_flags[F_ERROR] & E_BARRIER)
-        {
-            set_error("multigrid cycles: a grid barrier wait gave up");
-            return QZ_FAILURE;
-        }
-        iter = s->mg_ran;
-        check = s->mg_conv != 0;
-    }
-    else if (mg_persistent(s))
-    {
-        // FP64 form: one launch runs the cycles and takes the convergence test
-        // after every `every` cycles, as the host loop of check blocks did
-        if (mg_launch<double>(s, c.max_iter, true))
-            return QZ_FAILURE;
-        if (!check_cuda(cudaMemcpyAsync(s->h_flags, s->flags, F_COUNT * sizeof(int),
-                                        cudaMemcpyDeviceToHost, s->stream),
-                        "flags") ||
-            !check_cuda(cudaStreamSynchronize(s->stream), "flags"))
-            return QZ_FAILURE;
-        if (s->h_flags[F_ERROR] & E_BARRIER)
-        {
-            set_error("multigrid cycles: a grid barrier wait gave up");
-            return QZ_FAILURE;
-        }
-        iter = s->mg_ran;
-        check = s->mg_conv != 0;
-    }
     while (iter < c.max_iter && !check)
     {
         if (graphs && iter % every == 0 && c.max_iter - iter >= every)
@@ -2443,18 +2497,7 @@ int potential_head(qz_sim *s)
             check = s->h_flags[F_CONVERGED] != 0;
         }
     }
-    s->stats.last_vcycles = iter;
-    s->stats.vcycles_total += iter;
-    s->stats.last_converged = check ? 1 : 0;
-    if (s->sched_mode == 1)
-        sched_put(s, &iter, 1);
-    if (iter == c.max_iter)
-    {
-        set_error("the precision was not reached in the head node after %d multigrid cycles",
-                  iter);
-        return QZ_FAILURE;
-    }
-    return QZ_SUCCESS;
+    return head_tail(s, iter, check);
 }
 
 } // namespace qz
