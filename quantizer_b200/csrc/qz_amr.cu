@@ -2468,8 +2468,13 @@ struct CgOverride {
     std::vector<char> skip;
 };
 
-static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = true,
-                    const CgOverride *ov = nullptr)
+static int cg_level_collect(qz_sim *s, AmrLevel &L, int level_index, const CgPending &pd);
+
+// Queues the set-up and the cooperative launch of a level's node solves on the
+// simulation's stream with no host wait (red-black SOR nodes, if any, are
+// solved first, with their own waits); cg_level_collect reads the outcome.
+static int cg_level_issue(qz_sim *s, AmrLevel &L, int level_index, CgPending &pd,
+                          bool allow_sor = true, const CgOverride *ov = nullptr)
 {
     const qz_config &c = s->cfg;
     const int nn = L.nnodes;
@@ -2522,7 +2527,8 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         chunk = (int)std::max(64L, std::min(cs, (long)CG_UPT * nt));
     }
     L.hchunks.clear();
-    std::vector<int> node_chunk(2L * nn, 0);
+    std::vector<int> &node_chunk = L.hnode_chunk;
+    node_chunk.assign(2L * nn, 0);
     std::vector<int> sor_nodes; // nodes of at most branch_cg_cells cells: red-black SOR
     for (int q = 0; q < nn; q++)
     {
@@ -2555,15 +2561,14 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     }
     if (!sor_nodes.empty() && sor_level(s, L, level_index, sor_nodes))
         return QZ_FAILURE;
+    pd = CgPending();
+    pd.record = record;
+    pd.replay = replay;
+    pd.one = one;
+    pd.pipe = pipe;
+    pd.nn = nn;
     if (L.nchunks == 0)
-    {
-        if (record)
-        {
-            std::vector<int> z(nn, 0);
-            sched_put(s, z.data(), nn);
-        }
         return QZ_SUCCESS;
-    }
     // nint: node_chunk (2 nn) | rfail[0] (nn) | rfail[1] (nn) | status (3) | iterations (nn)
     const long nparts = (one ? 3L : 4L) * L.nchunks * CG_PS;
     if (!L.chunks.ensure(s->mem, L.nchunks) || !L.chunk_part.ensure(s->mem, nparts) ||
@@ -2701,12 +2706,33 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
     {
         cudaEventRecord(ee, s->stream);
         s->prof_pending.push_back({QZ_PROF_CG, 0.0, eb, ee});
+        pd.prof_idx = (int)s->prof_pending.size() - 1;
+    }
+    pd.launched = true;
+    pd.status = A.status;
+    return QZ_SUCCESS;
+}
+
+// Reads a level's solve outcome (waits for the stream up to its launch): iteration
+// counts, the schedule record, the profiler's bytes and the failure messages.
+static int cg_level_collect(qz_sim *s, AmrLevel &L, int level_index, const CgPending &pd)
+{
+    const int nn = pd.nn;
+    const bool record = pd.record, replay = pd.replay, one = pd.one, pipe = pd.pipe;
+    if (!pd.launched)
+    {
+        if (record)
+        {
+            std::vector<int> z(nn, 0);
+            sched_put(s, z.data(), nn);
+        }
+        return QZ_SUCCESS;
     }
     std::vector<int> st(3 + nn);
-    if (!read_ints(s, A.status, 3 + nn, st.data()))
+    if (!read_ints(s, pd.status, 3 + nn, st.data()))
         return QZ_FAILURE;
     s->stats.cg_iterations += st[0];
-    if (s->prof)
+    if (pd.prof_idx >= 0 && pd.prof_idx < (int)s->prof_pending.size())
     {
         // bytes per iteration and interior point: the P phase reads r and p_{k-2} and
         // writes p_{k-1} (24 B), the U phase reads p, pot, r and writes pot, r (40 B);
@@ -2715,7 +2741,7 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         double pts_it = 0.0;
         for (int q = 0; q < nn; q++)
             pts_it += (double)L.h[q].nintr * st[3 + q];
-        s->prof_pending.back().bytes = (pipe ? 96.0 : one ? 80.0 : 64.0) * pts_it;
+        s->prof_pending[pd.prof_idx].bytes = (pipe ? 96.0 : one ? 80.0 : 64.0) * pts_it;
     }
     if (st[1])
     {
@@ -2732,6 +2758,15 @@ static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = tr
         return QZ_FAILURE;
     }
     return check_cuda(cudaGetLastError(), "cg") ? QZ_SUCCESS : QZ_FAILURE;
+}
+
+static int cg_level(qz_sim *s, AmrLevel &L, int level_index, bool allow_sor = true,
+                    const CgOverride *ov = nullptr)
+{
+    CgPending pd;
+    if (cg_level_issue(s, L, level_index, pd, allow_sor, ov))
+        return QZ_FAILURE;
+    return cg_level_collect(s, L, level_index, pd);
 }
 
 // The adjoint's node solves on level l: Lap_h lam = rhs on every node's interior
@@ -2791,9 +2826,39 @@ __global__ void k_mark(int n, const int *__restrict__ idx, unsigned char *__rest
         mask[idx[t]] = 1;
 }
 
+// Node CG without a recorded or replayed schedule: every level's set-up and
+// solve are queued before any outcome is read back, so the GPU goes from one
+// level's solve to the next without waiting for the host (a level's start
+// values read its parent's solution in stream order).
+bool amr_potential_queues(const qz_sim *s)
+{
+    return s->cfg.node_solver != QZ_NODE_MG && s->sched_mode == 0;
+}
+
 int amr_potential(qz_sim *s)
 {
+    std::vector<CgPending> pend;
+    if (amr_potential_issue(s, pend))
+        return QZ_FAILURE;
+    return amr_potential_collect(s, pend);
+}
+
+int amr_potential_collect(qz_sim *s, const std::vector<CgPending> &pend)
+{
+    if (amr_potential_queues(s))
+        for (int l = 1; l < s->amr_nlev && l < (int)pend.size() && s->amr[l].nnodes > 0; l++)
+            if (cg_level_collect(s, s->amr[l], l, pend[l]))
+                return QZ_FAILURE;
+    return QZ_SUCCESS;
+}
+
+// The levels' potentials in order: start values, then the node solves (queued,
+// or solved with their waits when amr_potential_queues is false).
+int amr_potential_issue(qz_sim *s, std::vector<CgPending> &pend)
+{
     const double coeff = -s->cfg.G * s->cfg.total_mass;
+    const bool queue = amr_potential_queues(s);
+    pend.assign(s->amr_nlev, CgPending());
     for (int l = 1; l < s->amr_nlev; l++)
     {
         AmrLevel &L = s->amr[l];
@@ -2829,7 +2894,8 @@ int amr_potential(qz_sim *s)
                dim3(256), L.grid_total, L.pot, L.pot_old);
         // the reference's node conjugate gradient, or FP32 multigrid cycles
         // preconditioning a flexible conjugate gradient (qz_node_mg.cu)
-        if (s->cfg.node_solver == QZ_NODE_MG ? node_mg_level(s, L, l) : cg_level(s, L, l))
+        if (queue ? cg_level_issue(s, L, l, pend[l])
+                  : s->cfg.node_solver == QZ_NODE_MG ? node_mg_level(s, L, l) : cg_level(s, L, l))
             return QZ_FAILURE;
         if (warm)
         {

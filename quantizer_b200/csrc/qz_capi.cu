@@ -817,13 +817,20 @@ static int tree_density_potential(qz_sim *s)
         cudaStreamSynchronize(s->head_stream);
         return QZ_FAILURE;
     }
-    const bool tree_ok = !qz_tree_adaptation(s) && !amr_deposit(s);
-    // the head launch is always waited for, whatever the tree's outcome
+    bool ok = !qz_tree_adaptation(s) && !amr_deposit(s) &&
+              check_cuda(cudaStreamWaitEvent(s->stream, s->ev_head, 0), "join");
+    // queued level solves: their set-up is issued before the host waits for the
+    // head launch, so the first level starts as soon as the head solve ends; the
+    // head's outcome is still read (and reported) before the levels'
+    std::vector<CgPending> pend;
+    const bool queue = ok && amr_potential_queues(s);
+    if (queue)
+        ok = !amr_potential_issue(s, pend);
+    // the head launch is always waited for, whatever the other stages' outcome
     const bool head_ok = !potential_head_finish(s, s->head_stream);
-    if (!check_cuda(cudaStreamWaitEvent(s->stream, s->ev_head, 0), "join") || !tree_ok ||
-        !head_ok)
+    if (!ok || !head_ok)
         return QZ_FAILURE;
-    return amr_potential(s);
+    return queue ? amr_potential_collect(s, pend) : amr_potential(s);
 }
 
 // main.c:375-481 with a given dt: kick-drift, reset, tree, deposit, potential,

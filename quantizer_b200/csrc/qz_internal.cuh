@@ -299,6 +299,7 @@ struct AmrLevel {
     int nchunks = 0;
     int h_active = 0; // host copy of the unconverged-node count at the start of a solve
     std::vector<AmrChunk> hchunks;
+    std::vector<int> hnode_chunk; // node chunk ranges and flags uploaded with the chunks
     // warm start (node_warm): the level's solution, nodes and interior mask of the
     // previous solve
     DBuf<double> wpot;
@@ -542,6 +543,18 @@ int cg_level_adjoint(qz_sim *s, int l, double *lam, double *rhs, double *scratch
                      const double *thr_dev, const std::vector<char> &skip);
 int amr_deposit(qz_sim *s);
 int amr_potential(qz_sim *s);
+// What the host needs after a level's conjugate-gradient launch: where its
+// status words are and how its outcome is booked.
+struct CgPending {
+    bool launched = false; // a cooperative launch was queued (else nothing to read)
+    bool record = false, replay = false, one = false, pipe = false;
+    int nn = 0;
+    const int *status = nullptr; // status (3) then iterations (nn)
+    int prof_idx = -1;           // the launch's profiler record, or -1
+};
+bool amr_potential_queues(const qz_sim *s);
+int amr_potential_issue(qz_sim *s, std::vector<CgPending> &pend);
+int amr_potential_collect(qz_sim *s, const std::vector<CgPending> &pend);
 int amr_grid_accel(qz_sim *s);
 int amr_gather(qz_sim *s);
 int poisson_error_head(qz_sim *s, int *converged);
