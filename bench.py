@@ -74,7 +74,8 @@ WORKLOADS.update({
     # [0.02, 0.08], head 32^3 below N = 16384 else 64^3, two refinement levels, each
     # member with dt = 1e-3 of its own crossing time; stepped concurrently
     "ensemble512": dict(ic="ensemble", members=512, n=0, a=0.0, lmin=5, levels=2, ref_ptcl=9,
-                        steps=10, precision=1, cpu_steps=2, ref_steps=2, threads=16),
+                        steps=10, precision=1, cpu_steps=2, ref_steps=2, threads=16,
+                        cg_chunk_min=2048),
     # differentiation form: Plummer N = 262,144, a = 0.04, head 128^3 with the tree fixed
     # to the head node, FP64, 200 steps; loss = mean squared distance of the final
     # positions to targets from a forward run of ICs perturbed by N(0, 1e-3^2);
@@ -257,7 +258,7 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     for k, (n, a, lmin) in enumerate(members):
         s = core.Simulation(ics.plummer(n, a=a, seed=1000 * rank + k), lmin,
                             lmax=lmin + wl["levels"], ref_ptcl=wl["ref_ptcl"],
-                            precision=wl["precision"])
+                            precision=wl["precision"], cg_chunk_min=wl["cg_chunk_min"])
         s.init_forces()
         sims.append(s)
         dts.append(1e-3 * ics.crossing_time(a))
@@ -284,6 +285,7 @@ def run_ensemble(args, wl: dict, K: int, W: int) -> int:
     config["threads"] = threads
     config["mg_points_per_thread"] = ppt
     config["mg_tile"] = tile
+    config["cg_chunk_min"] = wl["cg_chunk_min"]
     st0 = [s.stats() for s in sims]
     with ClockSampler(local) as clk:
         ms = makespan(lambda: core.ensemble_step(sims, dts, K, threads=threads))

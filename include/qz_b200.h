@@ -141,6 +141,15 @@ typedef struct qz_config {
      * 0 runs the stages one after another in main.c's order.  Results are the
      * same bit for bit either way. */
     int tree_overlap;
+    /* refinement-node conjugate gradient: fewest interior points in a chunk
+     * (one 512-thread block works a chunk; chunks never cross nodes).  0
+     * (default): a level's points are cut into about 148 chunks, one a SM,
+     * which suits one simulation on the GPU.  Many simulations side by side
+     * (qz_ensemble_step) want larger chunks, e.g. 2048, so that a small
+     * member's level takes a few SMs instead of all of them.  The chunks set
+     * the order of the dot products' partial sums, so results depend on it at
+     * rounding level (deterministically). */
+    int cg_chunk_min;
 } qz_config;
 
 /* tile cores (x, y, z points) of the tiled multigrid phases, in mg_tile order */

@@ -45,7 +45,7 @@ class Config(C.Structure):
         ("adjoint_tol", C.c_double), ("cg_variant", C.c_int),
         ("mg_points_per_thread", C.c_int), ("freeze_tree", C.c_int),
         ("node_solver", C.c_int), ("mg_tile", C.c_int), ("node_warm", C.c_int),
-        ("tree_overlap", C.c_int),
+        ("tree_overlap", C.c_int), ("cg_chunk_min", C.c_int),
     ]
 
 

@@ -2520,11 +2520,30 @@ static int cg_level_issue(qz_sim *s, AmrLevel &L, int level_index, CgPending &pd
         for (int q = 0; q < nn; q++)
             if (!(ov && ov->skip[q]) && (!allow_sor || L.h[q].ncells > c.branch_cg_cells))
                 tot += L.h[q].nintr;
+        long target = CG_FILL;
         long cs = (tot + CG_FILL - 1) / CG_FILL;
         if (cs > (long)CG_UPT * nt)
+        {
+            target = 2L * CG_FILL;
             cs = (tot + 2L * CG_FILL - 1) / (2L * CG_FILL);
+        }
         cs = (cs + 31) / 32 * 32;
-        chunk = (int)std::max(64L, std::min(cs, (long)CG_UPT * nt));
+        // chunks never cross nodes: on a level of several nodes the rounding
+        // per node can push the count past the target, and the blocks given one
+        // chunk more than the others would set every phase's length; grow the
+        // chunk (by 32 points) until the count is within the target
+        const long cap = (long)CG_UPT * nt;
+        auto count = [&](long size) {
+            long k = 0;
+            for (int q = 0; q < nn; q++)
+                if (!(ov && ov->skip[q]) && (!allow_sor || L.h[q].ncells > c.branch_cg_cells))
+                    k += (L.h[q].nintr + size - 1) / size;
+            return k;
+        };
+        while (cs < cap && count(cs) > target)
+            cs += 32;
+        cs = std::max(cs, (long)c.cg_chunk_min);
+        chunk = (int)std::max(64L, std::min(cs, cap));
     }
     L.hchunks.clear();
     std::vector<int> &node_chunk = L.hnode_chunk;

@@ -346,6 +346,7 @@ int qz_default_config(qz_config *c, int lmin)
     c->mg_tile = 0;
     c->node_warm = 0;
     c->tree_overlap = 1;
+    c->cg_chunk_min = 0;
     return QZ_SUCCESS;
 }
 
