@@ -787,7 +787,28 @@ namespace qz {
 // 10 points 9.57, 12 points 9.53, 16 points 9.95.
 constexpr int OVERLAP_PPT = 12;
 
-static int tree_density_potential(qz_sim *s)
+// Outcomes a step reads at its end: the head launch (when it ran on the second
+// stream) and the queued level solves.
+struct StepPending {
+    bool head = false;
+    bool levels = false;
+    std::vector<CgPending> pend;
+};
+
+// Reads the outcomes in the order the stages ran (head, then levels); the head
+// stream is always waited for.
+static int step_finish(qz_sim *s, StepPending &sp)
+{
+    int rc = QZ_SUCCESS;
+    if (sp.head && potential_head_finish(s, s->head_stream))
+        rc = QZ_FAILURE;
+    if (rc == QZ_SUCCESS && sp.levels && amr_potential_collect(s, sp.pend))
+        rc = QZ_FAILURE;
+    sp = StepPending();
+    return rc;
+}
+
+static int tree_density_potential(qz_sim *s, StepPending &sp)
 {
     if (!amr_on(s) || !s->cfg.tree_overlap || s->no_overlap || !head_one_launch(s))
         return (qz_tree_adaptation(s) || qz_grid_density(s) || qz_potential(s)) ? QZ_FAILURE
@@ -820,26 +841,33 @@ static int tree_density_potential(qz_sim *s)
     }
     bool ok = !qz_tree_adaptation(s) && !amr_deposit(s) &&
               check_cuda(cudaStreamWaitEvent(s->stream, s->ev_head, 0), "join");
-    // queued level solves: their set-up is issued before the host waits for the
-    // head launch, so the first level starts as soon as the head solve ends; the
-    // head's outcome is still read (and reported) before the levels'
-    std::vector<CgPending> pend;
-    const bool queue = ok && amr_potential_queues(s);
-    if (queue)
-        ok = !amr_potential_issue(s, pend);
+    // queued level solves: issued with no host wait, so the first level starts as
+    // soon as the head solve ends and the gradient, gather and kick follow the
+    // last level on the stream; the outcomes (head, then levels) are read at
+    // the end of the step (step_finish)
+    sp.head = true;
+    if (ok && amr_potential_queues(s))
+    {
+        sp.levels = true;
+        ok = !amr_potential_issue(s, sp.pend);
+        return ok ? QZ_SUCCESS : QZ_FAILURE;
+    }
     // the head launch is always waited for, whatever the other stages' outcome
+    sp.head = false;
     const bool head_ok = !potential_head_finish(s, s->head_stream);
     if (!ok || !head_ok)
         return QZ_FAILURE;
-    return queue ? amr_potential_collect(s, pend) : amr_potential(s);
+    return amr_potential(s);
 }
 
 // main.c:375-481 with a given dt: kick-drift, reset, tree, deposit, potential,
 // gradient, gather, kick.
 int step_core(qz_sim *s, double h)
 {
-    if (kick_drift(s, h) || qz_reset(s) || tree_density_potential(s) ||
-        qz_grid_acceleration(s) || qz_particle_acceleration(s) || kick(s, h))
+    StepPending sp;
+    const bool ok = !kick_drift(s, h) && !qz_reset(s) && !tree_density_potential(s, sp) &&
+                    !qz_grid_acceleration(s) && !qz_particle_acceleration(s) && !kick(s, h);
+    if (step_finish(s, sp) || !ok)
         return QZ_FAILURE;
     s->stats.steps++;
     s->stats.last_dt = h;
@@ -961,18 +989,27 @@ int qz_step_host(qz_sim *s, double dt, double *x, double *y, double *z, double *
     for (int q = 0; q < 3; q++)
         if (!check_cuda(cudaMemcpyAsync(hx[q], dx[q], b, cudaMemcpyDeviceToHost, s->xfer), "d2h"))
             return QZ_FAILURE;
-    if (qz_reset(s) || !check_cuda(cudaStreamWaitEvent(s->stream, s->ev_mass, 0), "wait") ||
-        tree_density_potential(s) || qz_grid_acceleration(s) || qz_particle_acceleration(s) ||
-        kick(s, dt))
+    StepPending sp;
+    const bool ok = !qz_reset(s) &&
+                    check_cuda(cudaStreamWaitEvent(s->stream, s->ev_mass, 0), "wait") &&
+                    !tree_density_potential(s, sp) && !qz_grid_acceleration(s) &&
+                    !qz_particle_acceleration(s) && !kick(s, dt);
+    // the copies back are queued before the step's outcomes are read
+    double *ho[6] = {vx, vy, vz, ax, ay, az};
+    const double *dout[6] = {s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
+    bool copied = ok;
+    for (int q = 0; q < 6 && copied; q++)
+        copied = check_cuda(cudaMemcpyAsync(ho[q], dout[q], b, cudaMemcpyDeviceToHost, s->stream),
+                            "d2h");
+    if (step_finish(s, sp) || !copied)
+    {
+        cudaStreamSynchronize(s->xfer);
+        cudaStreamSynchronize(s->stream);
         return QZ_FAILURE;
+    }
     s->stats.steps++;
     s->stats.last_dt = dt;
     s->stats.sim_time += dt;
-    double *ho[6] = {vx, vy, vz, ax, ay, az};
-    const double *dout[6] = {s->vx, s->vy, s->vz, s->ax, s->ay, s->az};
-    for (int q = 0; q < 6; q++)
-        if (!check_cuda(cudaMemcpyAsync(ho[q], dout[q], b, cudaMemcpyDeviceToHost, s->stream), "d2h"))
-            return QZ_FAILURE;
     if (!check_cuda(cudaStreamSynchronize(s->xfer), "copy stream sync") ||
         !check_cuda(cudaStreamSynchronize(s->stream), "step sync"))
         return QZ_FAILURE;
