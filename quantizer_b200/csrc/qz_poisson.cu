@@ -769,6 +769,7 @@ constexpr int MG_SMALL_N = 17;
 constexpr int MG_THREADS = 512;
 static_assert(MG_THREADS == 512, "the single-block sub-cycle maps its threads to an 8 x 8 x 8 cube");
 constexpr size_t MG_SMEM_MAX = 100 * 1024; // two resident blocks a SM
+constexpr int MG_CLUSTER_MAX = 16;          // largest (non-portable) thread-block cluster
 
 template <typename T> struct MgArgs {
     Grid<T> phi[MG_MAXLEV], rho[MG_MAXLEV];
@@ -799,6 +800,9 @@ template <typename T> struct MgArgs {
     int tiled;
     int tc[3];
     Grid<T> mid[MG_MAXLEV]; // partner arrays of the tiled levels (zero boundary)
+    // the launch is one thread-block cluster (at most MG_CLUSTER_MAX blocks):
+    // its grid-wide barrier is the hardware cluster barrier
+    int cluster;
 };
 
 // Work item t = a + n0 (b + n1 c) of a grid-stride loop (t = tid, tid + stride,
@@ -1582,7 +1586,15 @@ __global__ void __launch_bounds__(MG_THREADS, 2) k_mg_cycles(const __grid_consta
     extern __shared__ __align__(16) unsigned char mg_dyn[];
     __shared__ int sh_ok;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
-    auto gsync = [&]() { gbar_sync(A.bar, &sh_ok); };
+    // every block reaches the same barriers in the same order (all decisions
+    // come from values every block computes alike), so the cluster barrier,
+    // which has no time limit, is met as surely as the bounded grid barrier
+    auto gsync = [&]() {
+        if (A.cluster)
+            cooperative_groups::this_cluster().sync();
+        else
+            gbar_sync(A.bar, &sh_ok);
+    };
     for (int it = 0; it < A.iters; it++)
     {
         if constexpr (std::is_same<T, double>::value)
@@ -1792,6 +1804,34 @@ bool mg_persistent(const qz_sim *s)
            !s->fused_rb && (int)s->levels.size() <= MG_MAXLEV;
 }
 
+// Whether one cluster of lc's shape (blocks, threads, shared memory) can be
+// resident on the device: cudaOccupancyMaxActiveClusters once per shape (the
+// first query also allows cluster sizes above the portable 8).
+template <typename T> static bool mg_cluster_fits(const cudaLaunchConfig_t &lc)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<long, bool>> known; // (blocks << 32 | smem, fits)
+    static bool attr_set = false;
+    const long key = ((long)lc.gridDim.x << 32) | (long)lc.dynamicSmemBytes;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto &k : known)
+        if (k.first == key)
+            return k.second;
+    if (!attr_set)
+    {
+        cudaFuncSetAttribute((const void *)k_mg_cycles<T>,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        attr_set = true;
+    }
+    int nc = 0;
+    const bool fits = cudaOccupancyMaxActiveClusters(&nc, (const void *)k_mg_cycles<T>, &lc) ==
+                          cudaSuccess &&
+                      nc > 0;
+    cudaGetLastError();
+    known.push_back({key, fits});
+    return fits;
+}
+
 // check: the convergence test inside the launch; defer: no host wait for the
 // launch's outcome (potential_head_finish reads it)
 template <typename T>
@@ -1938,6 +1978,26 @@ static int mg_launch(qz_sim *s, int iters, bool check = false, bool defer = fals
         const double m = s->fine_phi.n - 2;
         bytes += (A.check ? 56.0 : 40.0) * m * m * m; // the test reads and writes pot_old
     }
+    // launches of at most MG_CLUSTER_MAX blocks (small heads: 9 blocks on 33^3)
+    // run as one thread-block cluster whose barrier is the hardware's, where
+    // the device can place such a cluster with this shared memory
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute la[1];
+    A.cluster = 0;
+    if (blocks <= MG_CLUSTER_MAX)
+    {
+        lc.gridDim = dim3(blocks);
+        lc.blockDim = dim3(MG_THREADS);
+        lc.dynamicSmemBytes = smem;
+        lc.stream = s->stream;
+        la[0].id = cudaLaunchAttributeClusterDimension;
+        la[0].val.clusterDim.x = blocks;
+        la[0].val.clusterDim.y = 1;
+        la[0].val.clusterDim.z = 1;
+        lc.attrs = la;
+        lc.numAttrs = 1;
+        A.cluster = mg_cluster_fits<T>(lc) ? 1 : 0;
+    }
     void *args[] = {&A};
     cudaEvent_t eb = nullptr, ee = nullptr;
     if (s->prof)
@@ -1946,9 +2006,15 @@ static int mg_launch(qz_sim *s, int iters, bool check = false, bool defer = fals
         ee = prof_event(s);
         cudaEventRecord(eb, s->stream);
     }
-    if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_mg_cycles<T>, dim3(blocks),
-                                                dim3(MG_THREADS), args, smem, s->stream),
-                    "multigrid cycles"))
+    if (A.cluster)
+    {
+        if (!check_cuda(cudaLaunchKernelExC(&lc, (const void *)k_mg_cycles<T>, args),
+                        "multigrid cycles (cluster)"))
+            return QZ_FAILURE;
+    }
+    else if (!check_cuda(cudaLaunchCooperativeKernel((const void *)k_mg_cycles<T>, dim3(blocks),
+                                                     dim3(MG_THREADS), args, smem, s->stream),
+                         "multigrid cycles"))
         return QZ_FAILURE;
     s->stats.kernel_launches++;
     if (s->prof)
