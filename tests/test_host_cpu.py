@@ -61,6 +61,16 @@ def test_default_config_matches_reference_defaults():
     assert (c.tol, c.tol2, c.w_sor, c.bdry, c.cycle, c.smoother) == (1e-10, 1e-10, 1.0, 1, 0, 0)
 
 
+def test_default_config_schedule_options():
+    # the last fields of qz_config, as the library fills them: a misaligned
+    # ctypes mirror would read other fields' bytes here
+    c = core.config(7)
+    assert (c.node_warm, c.tree_overlap, c.cg_chunk_min) == (0, 1, 0)
+    assert (c.mg_points_per_thread, c.mg_tile, c.freeze_tree) == (4, 0, 0)
+    c2 = core.config(7, tree_overlap=0, cg_chunk_min=2048)
+    assert (c2.tree_overlap, c2.cg_chunk_min) == (0, 2048)
+
+
 def test_no_cpu_fallback_without_a_device():
     import torch
     if torch.cuda.is_available():
